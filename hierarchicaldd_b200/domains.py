@@ -1,0 +1,153 @@
+"""Synthetic Poisson domains for the DD-PCG solver.
+
+The flag rules follow the reference's domain generator
+(demos/SPGrid_Create_Simple_Domain/Create_3D_Domain/main.cpp):
+
+* a grid of ``size`` cells per axis, where ``size`` is the cell count plus one
+  (the reference's ``-size`` convention), cells indexed ``0 .. size-1``;
+* cells on the outer layer (index 0 or size-1) are Dirichlet (main.cpp:118);
+* Dirichlet cells without an Active face neighbour become exterior, flag 0
+  (main.cpp:126-140);
+* Active and Interface cells carry face bits for neighbours that are
+  Active|Interface|Dirichlet (main.cpp:299, SPGrid_Flag_Helper.h).
+
+The reference's own generator carves a Neumann (exterior) bubble; the workloads
+here place Dirichlet spheres instead, with every seed and shape fixed below.
+Random numbers come from numpy's Philox bit generator so that the inputs are the
+same on every host.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+ACTIVE = 0x00010000
+DIRICHLET = 0x00020000
+BOUNDARY = 0x00040000
+INTERFACE = 0x00080000
+FACE_MX = 0x00100000
+FACE_ALL = 0x03F00000
+
+
+@dataclass
+class Domain:
+    """One Poisson problem: cell flags and right-hand side on a dense grid."""
+
+    size: tuple          # cells per axis (reference -size, i.e. cell count + 1)
+    flags: np.ndarray    # uint32 [size]: Active / Dirichlet / 0, plus face bits
+    rhs: np.ndarray      # float32 [size]
+    sub_size: tuple = (16, 16, 16)
+    name: str = ""
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n_active(self) -> int:
+        return int(np.count_nonzero(self.flags & ACTIVE))
+
+
+def face_bits(flags: np.ndarray) -> np.ndarray:
+    """OR face bits into Active|Interface cells (SPGrid_Flag_Helper.h:74-106)."""
+    f = flags.copy()
+    typ = f & (ACTIVE | INTERFACE | DIRICHLET)
+    nb_ok = typ != 0
+    solve = (f & (ACTIVE | INTERFACE)) != 0
+    pad = np.pad(nb_ok, 1, constant_values=False)
+    n0, n1, n2 = f.shape
+    shifts = [(-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1)]
+    for k, (a, b, c) in enumerate(shifts):
+        nb = pad[1 + a:1 + a + n0, 1 + b:1 + b + n1, 1 + c:1 + c + n2]
+        f[solve & nb] |= np.uint32(FACE_MX << k)
+    return f
+
+
+def _finish(active: np.ndarray, dirichlet: np.ndarray) -> np.ndarray:
+    """Apply the generator's exterior rule and face bits."""
+    flags = np.zeros(active.shape, np.uint32)
+    flags[active] = ACTIVE
+    flags[dirichlet & ~active] = DIRICHLET
+    # Dirichlet cells with no Active face neighbour become exterior (flag 0).
+    pad = np.pad(active, 1, constant_values=False)
+    n0, n1, n2 = active.shape
+    has_active_nb = np.zeros_like(active)
+    for a, b, c in [(-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1)]:
+        has_active_nb |= pad[1 + a:1 + a + n0, 1 + b:1 + b + n1, 1 + c:1 + c + n2]
+    flags[(flags == DIRICHLET) & ~has_active_nb] = 0
+    return face_bits(flags)
+
+
+def box_with_spheres(size, spheres) -> np.ndarray:
+    """Flags for a box with Dirichlet outer layer and Dirichlet spheres.
+
+    ``spheres`` is a list of ``(centre_xyz, radius)``; a cell (i, j, k) is inside
+    when ``|(i, j, k) - centre|^2 <= radius^2``.
+    """
+    n = tuple(int(s) for s in size)
+    i, j, k = np.ogrid[0:n[0], 0:n[1], 0:n[2]]
+    outer = (i == 0) | (i == n[0] - 1) | (j == 0) | (j == n[1] - 1) | (k == 0) | (k == n[2] - 1)
+    inside = np.zeros(n, bool)
+    for (cx, cy, cz), r in spheres:
+        inside |= (i - cx) ** 2 + (j - cy) ** 2 + (k - cz) ** 2 <= r * r
+    dirichlet = outer | inside
+    active = ~dirichlet
+    return _finish(active, dirichlet)
+
+
+def config1() -> Domain:
+    """64^3 cells (size 65), Dirichlet sphere c=(32,32,32) r=12, delta 1.0 at (16,16,16)."""
+    size = (65, 65, 65)
+    flags = box_with_spheres(size, [((32, 32, 32), 12)])
+    rhs = np.zeros(size, np.float32)
+    rhs[16, 16, 16] = 1.0
+    return Domain(size, flags, rhs, (16, 16, 16), "c1_64cube_sub16",
+                  dict(vlevels=3, nVcycles=1, interior_smoothing=3, boundary_smoothing=3,
+                       sigma_levels=3, sigma_smoothing=3, sigma_mg=1))
+
+
+def config2() -> Domain:
+    """256^3 cells (size 257), sphere c=(128,128,128) r=48, delta at (64,64,64) + U[-1e-3,1e-3]."""
+    size = (257, 257, 257)
+    flags = box_with_spheres(size, [((128, 128, 128), 48)])
+    rng = np.random.Generator(np.random.Philox(2))
+    noise = rng.uniform(-1e-3, 1e-3, size).astype(np.float32)
+    rhs = np.where((flags & ACTIVE) != 0, noise, np.float32(0)).astype(np.float32)
+    rhs[64, 64, 64] += np.float32(1.0)
+    return Domain(size, flags, rhs, (32, 32, 32), "c2_256cube_sub32",
+                  dict(vlevels=4, nVcycles=1, interior_smoothing=4, boundary_smoothing=4,
+                       sigma_levels=4, sigma_smoothing=3, sigma_mg=1))
+
+
+def config3() -> Domain:
+    """384^3 cells (size 385), sphere scaled from config 2 (r=72), 8 Gaussian sources (sigma 6)."""
+    size = (385, 385, 385)
+    flags = box_with_spheres(size, [((192, 192, 192), 72)])
+    rng = np.random.Generator(np.random.Philox(3))
+    act = np.argwhere((flags & ACTIVE) != 0)
+    centres = act[rng.integers(0, len(act), 8)]
+    i, j, k = np.ogrid[0:size[0], 0:size[1], 0:size[2]]
+    rhs = np.zeros(size, np.float32)
+    for c in centres:
+        rhs += np.exp(-((i - c[0]) ** 2 + (j - c[1]) ** 2 + (k - c[2]) ** 2) / (2 * 36.0)).astype(np.float32)
+    rhs[(flags & ACTIVE) == 0] = 0
+    return Domain(size, flags, rhs, (32, 32, 32), "c3_384cube_sub32",
+                  dict(vlevels=4, nVcycles=1, interior_smoothing=4, boundary_smoothing=4,
+                       sigma_levels=4, sigma_smoothing=3, sigma_mg=1, true_residual_every=20))
+
+
+def small(n_cells=32, sub=8, radius=6, seed=0, delta=None) -> Domain:
+    """A small test domain: n_cells^3 box, one centred Dirichlet sphere, random RHS."""
+    size = (n_cells + 1,) * 3
+    c = n_cells // 2
+    flags = box_with_spheres(size, [((c, c, c), radius)] if radius > 0 else [])
+    rng = np.random.Generator(np.random.Philox(seed))
+    rhs = rng.uniform(-1, 1, size).astype(np.float32)
+    rhs[(flags & ACTIVE) == 0] = 0
+    if delta is not None:
+        rhs[:] = 0
+        rhs[delta] = 1.0
+    return Domain(size, flags, rhs, (sub, sub, sub), f"small{n_cells}_sub{sub}",
+                  dict(vlevels=3, nVcycles=1, interior_smoothing=3, boundary_smoothing=3,
+                       sigma_levels=2, sigma_smoothing=3, sigma_mg=1))
+
+
+CONFIGS = {"c1": config1, "c2": config2, "c3": config3}

@@ -1,0 +1,338 @@
+// ORACLE (test infrastructure only) -- solver object and C entry points used by
+// tests/ (through ctypes), __graft_entry__.smoke() and bench.py's cpu_baseline.
+//
+// Restates the CPU dd_pcg driver:
+//   CPU/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Decomposition_Solver.h:121-197
+//   CPU/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Decomposition_Preconditioner.h:88-128
+//   CPU/SPGrid_Domain_Decomposition_Solver/CG_SYSTEM.cpp:28-119
+//   PB/Public_Library/PhysBAM_Tools/Krylov_Solvers/CONJUGATE_GRADIENT.cpp:22-67
+//   PB/Public_Library/PhysBAM_Tools/Krylov_Solvers/KRYLOV_SYSTEM_BASE.cpp:100-106
+// Vectors are dense x-slowest/z-fastest arrays over the level-0 grid.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <string>
+
+#include "oracle_core.h"
+#include "oracle_interface.h"
+
+namespace oracle {
+
+struct SolverBase {
+    virtual ~SolverBase() {}
+    Dims d0;
+    int sub[3];
+    int vlevels, nvcycles, interior, boundary, sigma_levels, sigma_smoothing, sigma_mg;
+    std::vector<uint32_t> flags_in;
+    virtual int num_levels() const = 0;
+    virtual const Dims& level_dims(int l) const = 0;
+    virtual const uint32_t* level_flags(int l) const = 0;
+};
+
+template <class T>
+struct Solver : SolverBase {
+    std::vector<MGLevel<T>> lv;
+    InterfaceSystem<T> sys;
+    SigmaSolver<T> sigma;
+    std::vector<T> k_tmp;  // preconditioner tmp channel (CG_SYSTEM's preconditioner_tmp_field)
+
+    int num_levels() const override { return (int)lv.size(); }
+    const Dims& level_dims(int l) const override { return lv[l].d; }
+    const uint32_t* level_flags(int l) const override { return lv[l].flags.data(); }
+
+    void setup() {
+        // SPGrid_Domain_Decomposition_Solver.h:121-155.
+        build_interface_system<T>(d0, flags_in.data(), sub, sigma_levels, sys);
+        lv.resize(vlevels);
+        lv[0].d = d0;
+        lv[0].flags = flags_in;
+        divide_domain(d0, lv[0].flags.data(), sub);
+        flag_faces(d0, lv[0].flags.data());
+        for (int l = 0; l + 1 < vlevels; ++l) {
+            for (int a = 0; a < 3; ++a) lv[l + 1].d.n[a] = lv[l].d.n[a] / 2 + 1;
+            lv[l + 1].flags.assign(lv[l + 1].d.count(), 0u);
+            downsample_topology(lv[l].d, lv[l].flags.data(), lv[l + 1].d, lv[l + 1].flags.data());
+        }
+        for (int l = 0; l < vlevels; ++l) {
+            flag_faces(lv[l].d, lv[l].flags.data());
+            flag_boundary(lv[l].d, lv[l].flags.data());
+            if (l > 0) {
+                lv[l].u.assign(lv[l].d.count(), T(0));
+                lv[l].r.assign(lv[l].d.count(), T(0));
+                lv[l].b.assign(lv[l].d.count(), T(0));
+            }
+        }
+        sigma.initialize(sys, sigma_smoothing);
+        k_tmp.assign(d0.count(), T(0));
+    }
+
+    void project(T* v) const {
+        const uint32_t* f = lv[0].flags.data();
+        for (size_t x = 0; x < d0.count(); ++x)
+            if (!(f[x] & (ACTIVE | INTERFACE))) v[x] = T(0);
+    }
+
+    // SPGrid_Domain_Decomposition_Preconditioner.h:88-128 (debug residual prints dropped).
+    void apply_preconditioner(T* result, const T* rhs, T* tmp) {
+        const size_t n = d0.count();
+        const uint32_t* f = lv[0].flags.data();
+        std::fill(result, result + n, T(0));
+        std::fill(tmp, tmp + n, T(0));
+        for (int i = 0; i < nvcycles; ++i) v_cycle<T>(lv, result, tmp, rhs, interior, boundary);
+        std::copy(rhs, rhs + n, tmp);
+        laplace_ri<T>(d0, f, result, tmp);
+        std::vector<T>& b0 = sigma.b[0];
+        std::fill(b0.begin(), b0.end(), T(0));
+        for (size_t i = 0; i < sys.iface_map.size(); ++i) {
+            auto& c = sys.iface_map[i];
+            size_t x = d0.at(c[0], c[1], c[2]);
+            if (f[x] & INTERFACE) b0[i] = tmp[x];
+        }
+        std::fill(sigma.u[0].begin(), sigma.u[0].end(), T(0));
+        for (int i = 0; i < sigma_mg; ++i) sigma.v_cycle();
+        std::fill(result, result + n, T(0));
+        std::fill(tmp, tmp + n, T(0));
+        for (size_t i = 0; i < sys.iface_map.size(); ++i) {
+            auto& c = sys.iface_map[i];
+            size_t x = d0.at(c[0], c[1], c[2]);
+            if (f[x] & INTERFACE) result[x] = sigma.u[0][i];
+        }
+        for (int i = 0; i < nvcycles; ++i) v_cycle<T>(lv, result, tmp, rhs, interior, boundary);
+    }
+
+    double dot(const T* a, const T* b) const {
+        double s = 0;
+        for (size_t x = 0; x < d0.count(); ++x) s += (double)(a[x] * b[x]);
+        return s;
+    }
+    T max_abs(const T* a) const {
+        T m = 0;
+        for (size_t x = 0; x < d0.count(); ++x) m = (std::fabs(a[x]) > m) ? std::fabs(a[x]) : m;
+        return m;
+    }
+
+    // CONJUGATE_GRADIENT.cpp:22-67 with KRYLOV_SYSTEM_BASE::Precondition.  The
+    // stop test is max|r| <= tol (relative=0, the reference's test) or
+    // max|r| <= tol * max|b| over Active|Interface cells (relative=1).
+    int solve(const T* b_in, T* x, double tol, bool relative, int min_it, int max_it, double* norms,
+              double* history, int history_len) {
+        const size_t n = d0.count();
+        std::vector<T> b(b_in, b_in + n), q(n, T(0)), s(n, T(0)), r(n, T(0)), z(n, T(0));
+        project(b.data());
+        std::fill(x, x + n, T(0));
+        const T small_number = std::numeric_limits<T>::epsilon();
+        const double bnorm = (double)max_abs(b.data());
+        const T threshold = relative ? (T)(tol * bnorm) : (T)tol;
+        T rho_old = (T)FLT_MAX, convergence_norm = 0;
+        int it;
+        for (it = 0;; ++it) {
+            if (it == 0) {
+                r = b;
+                laplace_ai<T>(d0, lv[0].flags.data(), x, q.data());
+                for (size_t i = 0; i < n; ++i) r[i] -= q[i];
+                project(r.data());
+            }
+            convergence_norm = max_abs(r.data());
+            if (history && it < history_len) history[it] = (double)convergence_norm;
+            if (convergence_norm <= threshold && (it >= min_it || convergence_norm < small_number)) break;
+            if (it == max_it) break;
+            apply_preconditioner(z.data(), r.data(), k_tmp.data());
+            project(z.data());
+            T rho = (T)dot(z.data(), r.data());
+            if (it == 0) s = z;
+            else {
+                T beta = rho / rho_old;
+                for (size_t i = 0; i < n; ++i) s[i] = s[i] * beta + z[i];
+            }
+            laplace_ai<T>(d0, lv[0].flags.data(), s.data(), q.data());
+            project(q.data());
+            T sdq = (T)dot(s.data(), q.data());
+            T alpha = sdq ? rho / sdq : (T)FLT_MAX;
+            for (size_t i = 0; i < n; ++i) x[i] = s[i] * alpha + x[i];
+            for (size_t i = 0; i < n; ++i) r[i] = q[i] * (-alpha) + r[i];
+            rho_old = rho;
+        }
+        if (norms) {
+            norms[0] = (double)convergence_norm;
+            norms[1] = bnorm;
+            // True residual of the returned x.
+            std::vector<T> ax(n, T(0));
+            laplace_ai<T>(d0, lv[0].flags.data(), x, ax.data());
+            double tmax = 0, t2 = 0, b2 = 0;
+            const uint32_t* f = lv[0].flags.data();
+            for (size_t i = 0; i < n; ++i)
+                if (f[i] & (ACTIVE | INTERFACE)) {
+                    double rr = (double)b[i] - (double)ax[i];
+                    tmax = std::max(tmax, std::fabs(rr));
+                    t2 += rr * rr;
+                    b2 += (double)b[i] * (double)b[i];
+                }
+            norms[2] = tmax;
+            norms[3] = std::sqrt(t2);
+            norms[4] = std::sqrt(b2);
+        }
+        return it;
+    }
+};
+
+}  // namespace oracle
+
+using namespace oracle;
+
+namespace {
+struct Handle {
+    std::unique_ptr<SolverBase> s;
+    bool dbl = false;
+    std::string err;
+};
+template <class T>
+Solver<T>& S(Handle* h) { return *static_cast<Solver<T>*>(h->s.get()); }
+}  // namespace
+
+#define DISPATCH(h, expr) ((h)->dbl ? ([&](Solver<double>& s) { return expr; })(S<double>(h)) \
+                                     : ([&](Solver<float>& s) { return expr; })(S<float>(h)))
+
+extern "C" {
+
+void* hddo_create(const int size[3], const int sub[3], const uint32_t* flags, int vlevels, int nvcycles,
+                  int interior, int boundary, int sigma_levels, int sigma_smoothing, int sigma_mg,
+                  int use_double, char* err, int errlen) {
+    Handle* h = new Handle();
+    h->dbl = use_double != 0;
+    try {
+        SolverBase* base;
+        if (h->dbl) base = new Solver<double>(); else base = new Solver<float>();
+        h->s.reset(base);
+        for (int a = 0; a < 3; ++a) { base->d0.n[a] = size[a]; base->sub[a] = sub[a]; }
+        base->vlevels = vlevels;
+        base->nvcycles = nvcycles;
+        base->interior = interior;
+        base->boundary = boundary;
+        base->sigma_levels = sigma_levels;
+        base->sigma_smoothing = sigma_smoothing;
+        base->sigma_mg = sigma_mg;
+        base->flags_in.assign(flags, flags + base->d0.count());
+        if (h->dbl) S<double>(h).setup(); else S<float>(h).setup();
+    } catch (const std::exception& e) {
+        if (err && errlen > 0) snprintf(err, errlen, "%s", e.what());
+        delete h;
+        return nullptr;
+    }
+    return h;
+}
+
+void hddo_destroy(void* hp) { delete static_cast<Handle*>(hp); }
+
+int hddo_num_levels(void* hp) { return static_cast<Handle*>(hp)->s->num_levels(); }
+void hddo_level_dims(void* hp, int l, int* out) {
+    const Dims& d = static_cast<Handle*>(hp)->s->level_dims(l);
+    for (int a = 0; a < 3; ++a) out[a] = d.n[a];
+}
+void hddo_level_flags(void* hp, int l, uint32_t* out) {
+    SolverBase* s = static_cast<Handle*>(hp)->s.get();
+    const Dims& d = s->level_dims(l);
+    std::memcpy(out, s->level_flags(l), d.count() * sizeof(uint32_t));
+}
+
+int hddo_num_subdomains(void* hp) {
+    Handle* h = static_cast<Handle*>(hp);
+    return DISPATCH(h, s.sys.n_sub);
+}
+int hddo_num_interface(void* hp, int level) {
+    Handle* h = static_cast<Handle*>(hp);
+    return DISPATCH(h, s.sys.n_iface[level]);
+}
+void hddo_interface_map(void* hp, int* out) {
+    Handle* h = static_cast<Handle*>(hp);
+    DISPATCH(h, ([&] { for (size_t i = 0; i < s.sys.iface_map.size(); ++i)
+                           for (int a = 0; a < 3; ++a) out[3 * i + a] = s.sys.iface_map[i][a];
+                       return 0; })());
+}
+
+// kind: 0 = Arr[level], 1 = Aii[level][sub], 2 = Air[level][sub], 3 = Prr[level]
+int hddo_matrix_shape(void* hp, int kind, int level, int sub, int* rows, int* cols, int* nnz) {
+    Handle* h = static_cast<Handle*>(hp);
+    return DISPATCH(h, ([&] {
+        const auto* m = kind == 0 ? &s.sys.Arr[level] : kind == 1 ? &s.sys.Aii[level][sub]
+                      : kind == 2 ? &s.sys.Air[level][sub] : &s.sys.Prr[level];
+        *rows = m->rows; *cols = m->cols; *nnz = (int)m->col.size();
+        return 0; })());
+}
+int hddo_matrix_get(void* hp, int kind, int level, int sub, int* ptr, int* col, double* val) {
+    Handle* h = static_cast<Handle*>(hp);
+    return DISPATCH(h, ([&] {
+        const auto* m = kind == 0 ? &s.sys.Arr[level] : kind == 1 ? &s.sys.Aii[level][sub]
+                      : kind == 2 ? &s.sys.Air[level][sub] : &s.sys.Prr[level];
+        std::copy(m->ptr.begin(), m->ptr.end(), ptr);
+        std::copy(m->col.begin(), m->col.end(), col);
+        for (size_t i = 0; i < m->val.size(); ++i) val[i] = (double)m->val[i];
+        return 0; })());
+}
+
+void hddo_vcycle(void* hp, void* u, void* r, const void* b) {
+    Handle* h = static_cast<Handle*>(hp);
+    DISPATCH(h, ([&] {
+        using T = typename std::remove_reference<decltype(s.lv[0].u[0])>::type;
+        v_cycle<T>(s.lv, (T*)u, (T*)r, (const T*)b, s.interior, s.boundary);
+        return 0; })());
+}
+
+void hddo_apply_preconditioner(void* hp, const void* rhs, void* result) {
+    Handle* h = static_cast<Handle*>(hp);
+    DISPATCH(h, ([&] {
+        using T = typename std::remove_reference<decltype(s.lv[0].u[0])>::type;
+        s.apply_preconditioner((T*)result, (const T*)rhs, s.k_tmp.data());
+        s.project((T*)result);
+        return 0; })());
+}
+
+// y = project(A x) with the CG system's Laplacian.
+void hddo_multiply(void* hp, const void* x, void* y) {
+    Handle* h = static_cast<Handle*>(hp);
+    DISPATCH(h, ([&] {
+        using T = typename std::remove_reference<decltype(s.lv[0].u[0])>::type;
+        laplace_ai<T>(s.d0, s.lv[0].flags.data(), (const T*)x, (T*)y);
+        s.project((T*)y);
+        return 0; })());
+}
+
+// One sigma V-cycle from u = 0 for the level-0 interface right-hand side b0.
+void hddo_sigma_vcycle(void* hp, const void* b0, void* u0) {
+    Handle* h = static_cast<Handle*>(hp);
+    DISPATCH(h, ([&] {
+        using T = typename std::remove_reference<decltype(s.lv[0].u[0])>::type;
+        const T* bb = (const T*)b0;
+        std::copy(bb, bb + s.sigma.b[0].size(), s.sigma.b[0].begin());
+        std::fill(s.sigma.u[0].begin(), s.sigma.u[0].end(), T(0));
+        s.sigma.v_cycle();
+        std::copy(s.sigma.u[0].begin(), s.sigma.u[0].end(), (T*)u0);
+        return 0; })());
+}
+
+// One sigma smoothing step at the given level, in place on u.
+void hddo_sigma_smooth(void* hp, int level, void* u, const void* b) {
+    Handle* h = static_cast<Handle*>(hp);
+    DISPATCH(h, ([&] {
+        using T = typename std::remove_reference<decltype(s.lv[0].u[0])>::type;
+        int n = s.sys.n_iface[level];
+        std::vector<T> uu((T*)u, (T*)u + n), tmp(n), bb((const T*)b, (const T*)b + n);
+        s.sigma.smooth(level, uu, tmp, bb);
+        std::copy(uu.begin(), uu.end(), (T*)u);
+        return 0; })());
+}
+
+int hddo_solve(void* hp, const void* b, void* x, double tol, int relative, int min_it, int max_it,
+               double* norms, double* history, int history_len) {
+    Handle* h = static_cast<Handle*>(hp);
+    return DISPATCH(h, ([&] {
+        using T = typename std::remove_reference<decltype(s.lv[0].u[0])>::type;
+        return s.solve((const T*)b, (T*)x, tol, relative != 0, min_it, max_it, norms, history, history_len);
+    })());
+}
+
+}  // extern "C"
