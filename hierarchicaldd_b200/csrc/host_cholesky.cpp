@@ -1,0 +1,306 @@
+// Supernodal multifrontal Cholesky of (A + eps I) on the host.
+//
+// Stands in for MKL PARDISO (SPD, mtype 2) that the reference uses for the
+// interface matrix and every subdomain interior matrix
+// (CPU/Interface_Solver/SIGMA_SMOOTHER.cpp:175-237 builds A + 1e-5 I with a
+// 1e-5 diagonal for empty rows; phases 11/22 factor it).  The ordering is a
+// nested dissection by breadth-first level structures; every separator (and
+// every leaf block) is one dense front, so the factor is a tree of dense
+// blocks that the GPU solves level by level.
+#include <algorithm>
+#include <cmath>
+#include <functional>
+#include <numeric>
+
+#include "sigma.h"
+
+namespace hdd {
+
+namespace {
+constexpr int kLeaf = 32;
+}
+
+void SnFactor::analyze(const CsrF& A) {
+    n = A.rows;
+    std::vector<std::vector<int>> nb(n);
+    for (int r = 0; r < n; ++r)
+        for (int p = A.ptr[r]; p < A.ptr[r + 1]; ++p) {
+            const int c = A.col[p];
+            if (c == r) continue;
+            nb[r].push_back(c);
+            nb[c].push_back(r);
+        }
+    std::vector<int> adjp(n + 1, 0), adj;
+    for (int r = 0; r < n; ++r) {
+        std::sort(nb[r].begin(), nb[r].end());
+        nb[r].erase(std::unique(nb[r].begin(), nb[r].end()), nb[r].end());
+        adjp[r + 1] = adjp[r] + (int)nb[r].size();
+    }
+    adj.reserve(adjp[n]);
+    for (int r = 0; r < n; ++r) adj.insert(adj.end(), nb[r].begin(), nb[r].end());
+    nb.clear();
+
+    perm.clear();
+    perm.reserve(n);
+    col0.clear(); ncol.clear(); parent.clear(); rows.clear();
+    std::vector<int> part(n, 0), level(n, -1), queue(n);
+    int next_part = 1;
+    auto bfs = [&](int src, int pid, std::vector<int>& seen) {
+        int qh = 0, qt = 0, last = src;
+        queue[qt++] = src;
+        level[src] = 0;
+        seen.push_back(src);
+        while (qh < qt) {
+            const int v = queue[qh++];
+            last = v;
+            for (int p = adjp[v]; p < adjp[v + 1]; ++p) {
+                const int w = adj[p];
+                if (part[w] != pid || level[w] >= 0) continue;
+                level[w] = level[v] + 1;
+                queue[qt++] = w;
+                seen.push_back(w);
+            }
+        }
+        return last;
+    };
+    auto make_node = [&](const std::vector<int>& cols, const std::vector<int>& children) {
+        const int id = (int)col0.size();
+        col0.push_back((int)perm.size());
+        ncol.push_back((int)cols.size());
+        parent.push_back(-1);
+        for (int c : children) parent[c] = id;
+        perm.insert(perm.end(), cols.begin(), cols.end());
+        return id;
+    };
+    // Returns the roots of the supernode forest covering `verts`.
+    std::function<std::vector<int>(std::vector<int>&, int)> rec = [&](std::vector<int>& verts, int pid) {
+        if ((int)verts.size() <= kLeaf) return std::vector<int>{make_node(verts, {})};
+        std::vector<int> comp;
+        const int far = bfs(verts[0], pid, comp);
+        for (int v : comp) level[v] = -1;
+        if (comp.size() < verts.size()) {
+            const int pa = next_part++, pb = next_part++;
+            for (int v : verts) part[v] = pb;
+            for (int v : comp) part[v] = pa;
+            std::vector<int> rest;
+            for (int v : verts)
+                if (part[v] == pb) rest.push_back(v);
+            std::vector<int> ra = rec(comp, pa), rb = rec(rest, pb);
+            ra.insert(ra.end(), rb.begin(), rb.end());
+            return ra;
+        }
+        comp.clear();
+        bfs(far, pid, comp);
+        int h = 0;
+        for (int v : comp) h = std::max(h, level[v]);
+        if (h < 2) {
+            for (int v : comp) level[v] = -1;
+            return std::vector<int>{make_node(verts, {})};
+        }
+        std::vector<int> cnt(h + 1, 0);
+        for (int v : comp) cnt[level[v]]++;
+        // Separator level: the smallest level set in the middle half.
+        const int total = (int)verts.size();
+        int best = -1, best_size = 0, acc = 0;
+        for (int l = 1; l < h; ++l) {
+            acc += cnt[l - 1];
+            if (acc < total / 4 || acc > (3 * total) / 4) continue;
+            if (best < 0 || cnt[l] < best_size) { best = l; best_size = cnt[l]; }
+        }
+        if (best < 0) {
+            acc = 0;
+            for (int l = 0; l <= h; ++l) {
+                acc += cnt[l];
+                if (acc >= total / 2) { best = std::max(1, std::min(l, h - 1)); break; }
+            }
+        }
+        std::vector<int> Av, Sv, Bv;
+        for (int v : comp) {
+            if (level[v] < best) Av.push_back(v);
+            else if (level[v] == best) Sv.push_back(v);
+            else Bv.push_back(v);
+            level[v] = -1;
+        }
+        const int pa = next_part++, pb = next_part++;
+        for (int v : Av) part[v] = pa;
+        for (int v : Bv) part[v] = pb;
+        for (int v : Sv) part[v] = -1;
+        std::vector<int> children = rec(Av, pa), rb = rec(Bv, pb);
+        children.insert(children.end(), rb.begin(), rb.end());
+        return std::vector<int>{make_node(Sv, children)};
+    };
+    std::vector<int> all(n);
+    std::iota(all.begin(), all.end(), 0);
+    if (n > 0) rec(all, 0);
+
+    // Row structure of every front (symbolic factorisation).
+    std::vector<int> iperm(n);
+    for (int i = 0; i < n; ++i) iperm[perm[i]] = i;
+    const int ns = (int)col0.size();
+    rows.assign(ns, {});
+    std::vector<std::vector<int>> kids(ns);
+    for (int j = 0; j < ns; ++j)
+        if (parent[j] >= 0) kids[parent[j]].push_back(j);
+    std::vector<int> mark(n, -1);
+    for (int j = 0; j < ns; ++j) {
+        const int last = col0[j] + ncol[j] - 1;
+        std::vector<int>& R = rows[j];
+        for (int c = col0[j]; c <= last; ++c) {
+            const int old = perm[c];
+            for (int p = A.ptr[old]; p < A.ptr[old + 1]; ++p) {
+                const int i = iperm[A.col[p]];
+                if (i > last && mark[i] != j) { mark[i] = j; R.push_back(i); }
+            }
+        }
+        for (int c : kids[j])
+            for (int i : rows[c])
+                if (i > last && mark[i] != j) { mark[i] = j; R.push_back(i); }
+        std::sort(R.begin(), R.end());
+    }
+}
+
+void SnFactor::factor(const CsrF& A, double eps) {
+    const int ns = (int)col0.size();
+    std::vector<int> iperm(n);
+    for (int i = 0; i < n; ++i) iperm[perm[i]] = i;
+    std::vector<std::vector<int>> kids(ns);
+    for (int j = 0; j < ns; ++j)
+        if (parent[j] >= 0) kids[parent[j]].push_back(j);
+    Ljj.assign(ns, {});
+    Lrj.assign(ns, {});
+    std::vector<std::vector<double>> upd(ns);
+    std::vector<int> pos(n, -1);
+    for (int j = 0; j < ns; ++j) {
+        const int nj = ncol[j], nr = (int)rows[j].size(), f = nj + nr;
+        std::vector<double> F((size_t)f * f, 0.0);  // col-major, lower triangle used
+        for (int a = 0; a < nj; ++a) pos[col0[j] + a] = a;
+        for (int k = 0; k < nr; ++k) pos[rows[j][k]] = nj + k;
+        for (int a = 0; a < nj; ++a) {
+            const int cnew = col0[j] + a, old = perm[cnew];
+            for (int p = A.ptr[old]; p < A.ptr[old + 1]; ++p) {
+                const int i = iperm[A.col[p]];
+                if (i < cnew) continue;
+                F[(size_t)a * f + pos[i]] += (double)A.val[p];
+            }
+            F[(size_t)a * f + a] += eps;
+        }
+        for (int c : kids[j]) {
+            const std::vector<int>& rc = rows[c];
+            const int m = (int)rc.size();
+            const std::vector<double>& U = upd[c];
+            for (int b = 0; b < m; ++b) {
+                const int pb = pos[rc[b]];
+                for (int a = b; a < m; ++a) {
+                    const int pa = pos[rc[a]];
+                    // U is lower (a >= b); the front position order is monotone in the
+                    // new index, so pa >= pb.
+                    F[(size_t)pb * f + pa] += U[(size_t)b * m + a];
+                }
+            }
+            upd[c].clear();
+            upd[c].shrink_to_fit();
+        }
+        // Dense Cholesky of the pivot block, then the off-diagonal block.
+        for (int k = 0; k < nj; ++k) {
+            double d = F[(size_t)k * f + k];
+            if (!(d > 0)) throw Error(HDD_ERR_INTERNAL, "interface matrix is not positive definite");
+            d = std::sqrt(d);
+            F[(size_t)k * f + k] = d;
+            for (int i = k + 1; i < f; ++i) F[(size_t)k * f + i] /= d;
+            // Right-looking update of the trailing columns.
+#pragma omp parallel for schedule(static) if (f - k > 256)
+            for (int c = k + 1; c < f; ++c) {
+                const double lck = F[(size_t)k * f + c];
+                if (lck == 0.0) continue;
+                double* colc = &F[(size_t)c * f];
+                const double* colk = &F[(size_t)k * f];
+                for (int i = c; i < f; ++i) colc[i] -= colk[i] * lck;
+            }
+        }
+        Ljj[j].assign((size_t)nj * nj, 0.0);
+        Lrj[j].assign((size_t)nr * nj, 0.0);
+        for (int a = 0; a < nj; ++a) {
+            for (int i = a; i < nj; ++i) Ljj[j][(size_t)a * nj + i] = F[(size_t)a * f + i];
+            for (int k = 0; k < nr; ++k) Lrj[j][(size_t)a * nr + k] = F[(size_t)a * f + nj + k];
+        }
+        if (nr > 0) {
+            upd[j].assign((size_t)nr * nr, 0.0);
+            for (int b = 0; b < nr; ++b)
+                for (int a = b; a < nr; ++a) upd[j][(size_t)b * nr + a] = F[(size_t)(nj + b) * f + nj + a];
+        }
+        for (int a = 0; a < nj; ++a) pos[col0[j] + a] = -1;
+        for (int k = 0; k < nr; ++k) pos[rows[j][k]] = -1;
+    }
+}
+
+void SnFactor::solve(double* x) const {
+    const int ns = (int)col0.size();
+    std::vector<double> y(n);
+    for (int i = 0; i < n; ++i) y[i] = x[perm[i]];
+    for (int j = 0; j < ns; ++j) {
+        const int nj = ncol[j], nr = (int)rows[j].size();
+        double* yj = &y[col0[j]];
+        for (int a = 0; a < nj; ++a) {
+            yj[a] /= Ljj[j][(size_t)a * nj + a];
+            for (int i = a + 1; i < nj; ++i) yj[i] -= Ljj[j][(size_t)a * nj + i] * yj[a];
+            for (int k = 0; k < nr; ++k) y[rows[j][k]] -= Lrj[j][(size_t)a * nr + k] * yj[a];
+        }
+    }
+    for (int j = ns - 1; j >= 0; --j) {
+        const int nj = ncol[j], nr = (int)rows[j].size();
+        double* yj = &y[col0[j]];
+        for (int a = nj - 1; a >= 0; --a) {
+            double acc = yj[a];
+            for (int k = 0; k < nr; ++k) acc -= Lrj[j][(size_t)a * nr + k] * y[rows[j][k]];
+            for (int i = a + 1; i < nj; ++i) acc -= Ljj[j][(size_t)a * nj + i] * yj[i];
+            yj[a] = acc / Ljj[j][(size_t)a * nj + a];
+        }
+    }
+    for (int i = 0; i < n; ++i) x[perm[i]] = y[i];
+}
+
+void dense_spd_inverse(std::vector<double>& a, int n) {
+    // Cholesky A = L L^T (row-major, lower), then A^{-1} = L^{-T} L^{-1}.
+    for (int k = 0; k < n; ++k) {
+        double d = a[(size_t)k * n + k];
+        for (int p = 0; p < k; ++p) d -= a[(size_t)k * n + p] * a[(size_t)k * n + p];
+        if (!(d > 0)) throw Error(HDD_ERR_INTERNAL, "coarse Schur complement is not positive definite");
+        d = std::sqrt(d);
+        a[(size_t)k * n + k] = d;
+#pragma omp parallel for schedule(static) if (n - k > 128)
+        for (int i = k + 1; i < n; ++i) {
+            double s = a[(size_t)i * n + k];
+            const double* ri = &a[(size_t)i * n];
+            const double* rk = &a[(size_t)k * n];
+            for (int p = 0; p < k; ++p) s -= ri[p] * rk[p];
+            a[(size_t)i * n + k] = s / d;
+        }
+    }
+    // Wt = (L^{-1})^T: row c of Wt is column c of L^{-1}, so both loops below
+    // read contiguous rows.
+    std::vector<double> Wt((size_t)n * n, 0.0);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int c = 0; c < n; ++c) {
+        double* w = &Wt[(size_t)c * n];
+        w[c] = 1.0 / a[(size_t)c * n + c];
+        for (int i = c + 1; i < n; ++i) {
+            const double* ri = &a[(size_t)i * n];
+            double s = 0;
+            for (int p = c; p < i; ++p) s -= ri[p] * w[p];
+            w[i] = s / ri[i];
+        }
+    }
+    // A^{-1}[i][j] = sum_{p >= max(i,j)} Wt[i][p] Wt[j][p].
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j <= i; ++j) {
+            const double* wi = &Wt[(size_t)i * n];
+            const double* wj = &Wt[(size_t)j * n];
+            double s = 0;
+            for (int p = i; p < n; ++p) s += wi[p] * wj[p];
+            a[(size_t)i * n + j] = s;
+            a[(size_t)j * n + i] = s;
+        }
+}
+
+}  // namespace hdd

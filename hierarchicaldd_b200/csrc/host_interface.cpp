@@ -1,0 +1,650 @@
+// Interface system assembly (host, parallel over subdomains).
+//
+// Restates CPU/Interface_Solver/INTERFACE_MATRIX_GENERATOR.h:130-735 with its
+// helpers STRIDE_GENERATOR.h:70-101, CELL_PROLONGATION_BAKER.h:125-152,
+// GALERKIN_PROCESS.h:183-224 and PROLONGATION_MATRIX_HELPER.cpp:268-294, and
+// the subdomain flag extraction of SPGrid_Subdomain_Splitter.h:123-154 /
+// SPGrid_Subdomain_Rasterizer.h:253-300.
+//
+// Data structures differ from the reference: every subdomain works on dense
+// box-local arrays per hierarchy level instead of SPGrid allocators and hash
+// tables, Galerkin-coarsened element matrices are memoised per (level, cell),
+// and subdomains are processed concurrently.  Global interface DOF numbers are
+// then assigned in a serial pass in the reference's first-encounter order, and
+// interface-interface contributions are summed per key in the reference's
+// (subdomain, cell) order, so the assembled matrices follow the reference's
+// numbering and float summation order.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <string>
+#include <unordered_map>
+
+#include "host_setup.h"
+#include "sigma.h"
+
+namespace hdd {
+namespace {
+
+// Adaptive-hierarchy flags, CPU/Interface_Solver/ADAPTIVE_SUBDOMAIN_POISSON_FLAGS.h:11-26.
+enum : uint32_t {
+    N_INTERFACE = 0x40u,
+    CELL_INTERIOR = 0x1u,
+    N_DEGREE = 0x10000000u,
+    N_TJUNCTION = 0x100u,
+    N_COARSE_SHARED = 0x200u,
+    N_ACTIVE = 0x400u,
+};
+
+typedef std::array<int, 3> I3;
+typedef std::array<float, 64> M8;
+
+// SPGrid page order (4x8x8 pages of a 16-byte struct, interleaved page bits):
+// the order in which the reference walks hierarchy cells.
+inline uint64_t spread_bits(uint64_t v, uint64_t mask) {
+    uint64_t r = 0;
+    for (uint64_t bit = 1; mask; bit <<= 1) {
+        const uint64_t low = mask & (~mask + 1);
+        if (v & bit) r |= low;
+        mask &= mask - 1;
+    }
+    return r;
+}
+inline uint64_t page_key(const I3& c) {
+    return spread_bits((uint64_t)c[0], 0x9249249249249000ull | 0x300ull) |
+           spread_bits((uint64_t)c[1], 0x4924924924924000ull | 0x0e0ull) |
+           spread_bits((uint64_t)c[2], 0x2492492492492000ull | 0x01cull);
+}
+
+struct Stride {
+    int lo[3];
+    std::vector<int> q[3];
+    int at(int axis, int i) const { return q[axis][i - lo[axis]]; }
+};
+
+// STRIDE_GENERATOR::Generate_Adaptive_Stride: graded node spacing per axis
+// (1 next to the box faces, doubling toward the centre); returns the number
+// of adaptation levels.
+int adaptive_stride(const I3& lo, const I3& hi, Stride& st) {
+    int level = INT_MAX;
+    for (int a = 0; a < 3; ++a) {
+        const int count = hi[a] - lo[a];
+        int axis_level = 0;
+        std::vector<std::pair<int, int>> steps{{2, 1}};
+        int cur = 1, covered = 2;
+        while (covered < count) {
+            const int qn = std::min(2, (count - covered) / cur);
+            if (qn <= 0) throw Error(HDD_ERR_UNSUPPORTED, "adaptive stride: subdomain size must be a power of two");
+            steps.push_back({qn, cur});
+            covered += qn * cur;
+            if ((count - covered) % (2 * cur) == 0) { cur *= 2; ++axis_level; }
+        }
+        st.lo[a] = lo[a];
+        std::vector<int>& q = st.q[a];
+        q.clear();
+        std::vector<int> pending;
+        for (size_t i = 0; i < steps.size(); ++i) {
+            q.insert(q.end(), steps[i].second, steps[i].second);
+            if (steps[i].first == 1 || i + 1 == steps.size()) q.push_back(steps[i].second);
+            if (steps[i].first != 1) pending.push_back(steps[i].second);
+        }
+        while (!pending.empty()) {
+            q.insert(q.end(), pending.back(), pending.back());
+            pending.pop_back();
+        }
+        if ((int)q.size() != count + 1) throw Error(HDD_ERR_INTERNAL, "adaptive stride length mismatch");
+        level = std::min(level, axis_level);
+    }
+    return level;
+}
+
+typedef std::vector<std::pair<I3, float>> Parents;
+
+// Embedding_Helper: hanging nodes are linear interpolants of the aligned nodes
+// on either side, recursively.
+void embed(const I3& idx, Parents& out, float w, const Stride& q) {
+    int qs = INT_MAX;
+    for (int a = 0; a < 3; ++a) qs = std::min(qs, q.at(a, idx[a]));
+    for (int a = 0; a < 3; ++a) {
+        const int cur = idx[a] - q.lo[a];
+        if (cur % qs != 0) {
+            I3 i1 = idx, i2 = idx;
+            i1[a] = (cur / qs) * qs + q.lo[a];
+            i2[a] = (cur / qs + 1) * qs + q.lo[a];
+            const float w1 = w * (float)(i2[a] - idx[a]) / (float)(i2[a] - i1[a]);
+            const float w2 = w * (float)(idx[a] - i1[a]) / (float)(i2[a] - i1[a]);
+            embed(i1, out, w1, q);
+            embed(i2, out, w2, q);
+            return;
+        }
+    }
+    for (auto& p : out)
+        if (p.first == idx) { p.second += w; return; }
+    out.push_back({idx, w});
+}
+
+// Trilinear node prolongation of one cell to its 8 children, indexed by the
+// child offset o = 4*ox+2*oy+oz; rows are the child's local nodes, columns the
+// parent's local nodes (both 4*x+2*y+z).
+std::array<M8, 8> bake_prolongation() {
+    std::array<M8, 8> P;
+    for (int o = 0; o < 8; ++o) {
+        P[o].fill(0.0f);
+        const int off[3] = {o >> 2, (o >> 1) & 1, o & 1};
+        for (int fi = 0; fi < 8; ++fi) {
+            const int fn[3] = {(fi >> 2) + off[0], ((fi >> 1) & 1) + off[1], (fi & 1) + off[2]};
+            int base[3];
+            for (int v = 0; v < 3; ++v) base[v] = (int)std::floor(fn[v] / 2.0);
+            for (int ci = 0; ci < 8; ++ci) {
+                const int cn[3] = {base[0] + (ci >> 2), base[1] + ((ci >> 1) & 1), base[2] + (ci & 1)};
+                float w = 1.0f;
+                for (int v = 0; v < 3; ++v) w *= (2.0f - std::abs(cn[v] * 2 - fn[v])) / 2.0;
+                if (w == 0) continue;
+                P[o][fi * 8 + cn[0] * 4 + cn[1] * 2 + cn[2]] = w;
+            }
+        }
+    }
+    return P;
+}
+
+struct BoxWork {
+    I3 lo, hi;
+    int levels = 0;
+    std::vector<uint32_t> sub_flags;       // (sub+1)^3 node flags of the box
+    int e1[3];
+    uint32_t sf(const I3& n) const {
+        for (int a = 0; a < 3; ++a)
+            if (n[a] < lo[a] || n[a] > hi[a]) return 0u;
+        return sub_flags[((size_t)(n[0] - lo[0]) * e1[1] + (n[1] - lo[1])) * e1[2] + (n[2] - lo[2])];
+    }
+    // Results per sigma level m (0-based).
+    std::vector<std::vector<I3>> iface_nodes;   // first-encounter list of interface nodes (level coords)
+    std::vector<std::vector<std::pair<std::pair<int, int>, float>>> arr_terms;  // (local iface ids), value
+    std::vector<CsrF> aii;
+    std::vector<std::vector<std::pair<std::pair<int, int>, float>>> air_terms;  // (row, local iface id)
+    std::vector<int> n_int;
+};
+
+struct LevelArrays {
+    int lo[3], e[3];
+    std::vector<uint32_t> flags;
+    std::vector<int> index;
+    bool inside(const I3& n) const {
+        for (int a = 0; a < 3; ++a)
+            if (n[a] < lo[a] || n[a] >= lo[a] + e[a]) return false;
+        return true;
+    }
+    size_t at(const I3& n) const {
+        if (!inside(n)) throw Error(HDD_ERR_INTERNAL, "hierarchy index outside its subdomain box");
+        return ((size_t)(n[0] - lo[0]) * e[1] + (n[1] - lo[1])) * e[2] + (n[2] - lo[2]);
+    }
+};
+
+void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
+    const I3 lo = W.lo, hi = W.hi;
+    Stride qtop;
+    const int levels = adaptive_stride(lo, hi, qtop);
+    if (M > levels) throw Error(HDD_ERR_INVALID_ARGUMENT, "sigma_levels exceeds the adaptive levels of a subdomain");
+    W.levels = levels;
+    std::vector<Stride> q(levels + 1);
+    for (int L = 1; L <= levels; ++L) {
+        I3 l2, h2;
+        for (int a = 0; a < 3; ++a) { l2[a] = lo[a] >> (L - 1); h2[a] = hi[a] >> (L - 1); }
+        adaptive_stride(l2, h2, q[L]);
+    }
+    // H[m][L] for m = 1..M, L = 1..levels.
+    std::vector<std::vector<LevelArrays>> H(M + 1, std::vector<LevelArrays>(levels + 1));
+    for (int m = 1; m <= M; ++m)
+        for (int L = 1; L <= levels; ++L) {
+            LevelArrays& A = H[m][L];
+            size_t cnt = 1;
+            for (int a = 0; a < 3; ++a) {
+                A.lo[a] = lo[a] >> (L - 1);
+                A.e[a] = (hi[a] >> (L - 1)) - A.lo[a] + 1;
+                cnt *= (size_t)A.e[a];
+            }
+            A.flags.assign(cnt, 0u);
+            A.index.assign(cnt, 0);
+        }
+
+    // Graded cell activation (INTERFACE_MATRIX_GENERATOR.h:184-239).
+    {
+        const int ec[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+        std::vector<uint8_t> traversed((size_t)ec[0] * ec[1] * ec[2], 0);
+        auto ntype = [&](const I3& n) {
+            const uint32_t s = W.sf(n);
+            return (uint32_t)(((s & (F_ACTIVE | F_INTERFACE)) ? 1u : 0u) | ((s & F_DIRICHLET) ? 2u : 0u));
+        };
+        for (int x = lo[0]; x <= hi[0]; ++x)
+            for (int y = lo[1]; y <= hi[1]; ++y)
+                for (int z = lo[2]; z <= hi[2]; ++z) {
+                    if (W.sf({x, y, z}) == 0) continue;
+                    for (int ci = 0; ci < 8; ++ci) {
+                        const I3 c = {x + (ci >> 2), y + ((ci >> 1) & 1), z + (ci & 1)};
+                        if (c[0] > hi[0] || c[1] > hi[1] || c[2] > hi[2]) continue;
+                        if (c[0] - 1 < lo[0] || c[1] - 1 < lo[1] || c[2] - 1 < lo[2]) continue;
+                        uint8_t& tv = traversed[((size_t)(c[0] - lo[0] - 1) * ec[1] + (c[1] - lo[1] - 1)) * ec[2] +
+                                                (c[2] - lo[2] - 1)];
+                        if (tv) continue;
+                        tv = 1;
+                        bool contributes = false;
+                        for (int v = 0; v < 3 && !contributes; ++v) {
+                            const int a = (v == 0) ? 1 : 0, b = (v == 2) ? 1 : 2;
+                            for (int e = 0; e < 4 && !contributes; ++e) {
+                                I3 l, u;
+                                l[v] = c[v] - 1; u[v] = c[v];
+                                l[a] = u[a] = c[a] - 1 + (e >> 1);
+                                l[b] = u[b] = c[b] - 1 + (e & 1);
+                                const uint32_t lt = ntype(l), ut = ntype(u);
+                                if ((lt & ut & 1u) || (((lt | ut) & 1u) && ((lt | ut) & 2u))) contributes = true;
+                            }
+                        }
+                        if (!contributes) continue;
+                        I3 cur = c, rlo = {c[0] - 1, c[1] - 1, c[2] - 1}, rhi = c;
+                        for (int cl = 1; cl <= levels; ++cl) {
+                            const int s1 = 1 << cl, s0 = 1 << (cl - 1);
+                            bool in1 = true, in0 = true;
+                            for (int a = 0; a < 3; ++a) {
+                                if (!(lo[a] + s1 <= rlo[a] && rhi[a] <= hi[a] - s1)) in1 = false;
+                                if (!(lo[a] + s0 <= rlo[a] && rhi[a] <= hi[a] - s0)) in0 = false;
+                            }
+                            for (int m = 1; m <= M; ++m)
+                                if ((cl == m && !in1) || (cl > m && in0 && !in1))
+                                    H[m][cl].flags[H[m][cl].at(cur)] |= CELL_INTERIOR;
+                            for (int a = 0; a < 3; ++a) {
+                                rlo[a] = (rlo[a] / s1) * s1;
+                                rhi[a] = rlo[a] + s1;
+                                cur[a] = (cur[a] + 1) / 2;
+                            }
+                        }
+                    }
+                }
+    }
+
+    auto interior_cells = [&](int m, int L) {
+        const LevelArrays& A = H[m][L];
+        std::vector<std::pair<uint64_t, I3>> cells;
+        for (int x = 0; x < A.e[0]; ++x)
+            for (int y = 0; y < A.e[1]; ++y)
+                for (int z = 0; z < A.e[2]; ++z)
+                    if (A.flags[((size_t)x * A.e[1] + y) * A.e[2] + z] & CELL_INTERIOR) {
+                        const I3 c = {A.lo[0] + x, A.lo[1] + y, A.lo[2] + z};
+                        cells.push_back({page_key(c), c});
+                    }
+        std::sort(cells.begin(), cells.end(), [](const auto& p, const auto& r) { return p.first < r.first; });
+        std::vector<I3> out(cells.size());
+        for (size_t i = 0; i < cells.size(); ++i) out[i] = cells[i].second;
+        return out;
+    };
+
+    W.iface_nodes.assign(M, {});
+    W.arr_terms.assign(M, {});
+    W.air_terms.assign(M, {});
+    W.aii.assign(M, CsrF());
+    W.n_int.assign(M, 0);
+    std::vector<int> node_count(M + 1, 0);
+
+    for (int m = 1; m <= M; ++m) {
+        // Interface DOFs (lines 249-312), numbered locally in encounter order.
+        std::unordered_map<uint64_t, int> local_id;
+        auto add_iface = [&](const I3& node) {
+            const uint64_t key = ((uint64_t)node[0] << 42) | ((uint64_t)node[1] << 21) | (uint64_t)node[2];
+            auto it = local_id.find(key);
+            int id;
+            if (it == local_id.end()) {
+                id = (int)W.iface_nodes[m - 1].size();
+                local_id.emplace(key, id);
+                W.iface_nodes[m - 1].push_back(node);
+            } else id = it->second;
+            LevelArrays& A = H[m][m];
+            const size_t p = A.at(node);
+            A.index[p] = id;
+            A.flags[p] |= N_INTERFACE | N_DEGREE;
+        };
+        if (m == 1) {
+            for (int axis = 0; axis < 3; ++axis)
+                for (int face = 0; face <= 1; ++face) {
+                    const int a = (axis == 0) ? 1 : 0, b = (axis == 2) ? 1 : 2;
+                    for (int va = lo[a]; va <= hi[a]; ++va)
+                        for (int vb = lo[b]; vb <= hi[b]; ++vb) {
+                            I3 node;
+                            node[axis] = face ? hi[axis] : lo[axis];
+                            node[a] = va;
+                            node[b] = vb;
+                            if (W.sf(node) & F_INTERFACE) add_iface(node);
+                        }
+                }
+        } else {
+            I3 clo, chi;
+            for (int a = 0; a < 3; ++a) { clo[a] = lo[a] >> (m - 1); chi[a] = hi[a] >> (m - 1); }
+            for (const I3& c : interior_cells(m, m))
+                for (int li = 0; li < 8; ++li) {
+                    const I3 node = {c[0] - 1 + (li >> 2), c[1] - 1 + ((li >> 1) & 1), c[2] - 1 + (li & 1)};
+                    bool on_face = false;
+                    for (int a = 0; a < 3; ++a)
+                        if (node[a] == clo[a] || node[a] == chi[a]) on_face = true;
+                    if (on_face) add_iface(node);
+                }
+        }
+        // Interior DOFs (lines 315-375).
+        int count = 0;
+        for (int L = m; L <= levels; ++L) {
+            LevelArrays& A = H[m][L];
+            for (const I3& c : interior_cells(m, L))
+                for (int li = 0; li < 8; ++li) {
+                    const I3 N = {c[0] - 1 + (li >> 2), c[1] - 1 + ((li >> 1) & 1), c[2] - 1 + (li & 1)};
+                    if (L == 1 && !(W.sf(N) & F_ACTIVE)) continue;
+                    const size_t pn = A.at(N);
+                    if (L == m && (A.flags[pn] & N_INTERFACE)) continue;
+                    int qs = INT_MAX;
+                    for (int a = 0; a < 3; ++a) qs = std::min(qs, q[L].at(a, N[a]));
+                    bool tj = false;
+                    for (int a = 0; a < 3; ++a)
+                        if ((N[a] - q[L].lo[a]) % qs != 0) tj = true;
+                    if (!tj) {
+                        if (L > m) {
+                            const LevelArrays& F = H[m][L - 1];
+                            const I3 fine = {2 * N[0], 2 * N[1], 2 * N[2]};
+                            const size_t pf = F.at(fine);
+                            if (F.flags[pf] & N_DEGREE) {
+                                A.index[pn] = F.index[pf];
+                                A.flags[pn] |= N_DEGREE | N_COARSE_SHARED;
+                            }
+                        }
+                        if (!(A.flags[pn] & N_DEGREE)) {
+                            A.flags[pn] |= N_DEGREE | N_ACTIVE;
+                            A.index[pn] = count++;
+                        }
+                    } else {
+                        A.flags[pn] |= N_TJUNCTION;
+                        Parents par;
+                        embed(N, par, 1.0f, q[L]);
+                        for (auto& p : par) {
+                            const size_t pp = A.at(p.first);
+                            if (!(A.flags[pp] & N_DEGREE)) {
+                                A.flags[pp] |= N_DEGREE | N_ACTIVE;
+                                A.index[pp] = count++;
+                            }
+                        }
+                    }
+                }
+        }
+        node_count[m] = count;
+    }
+
+    // Galerkin-coarsened cell matrices, memoised per (level, cell).
+    std::vector<std::unordered_map<uint64_t, M8>> memo(levels + 1);
+    std::function<const M8&(const I3&, int)> galerkin = [&](const I3& C, int level) -> const M8& {
+        const uint64_t key = ((uint64_t)C[0] << 42) | ((uint64_t)C[1] << 21) | (uint64_t)C[2];
+        auto it = memo[level].find(key);
+        if (it != memo[level].end()) return it->second;
+        M8 m;
+        m.fill(0.0f);
+        if (level == 1) {
+            const float w = (float)(1.0 / (1 << 2));
+            uint32_t nf[8];
+            for (int li = 0; li < 8; ++li) {
+                const I3 node = {C[0] - 1 + (li >> 2), C[1] - 1 + ((li >> 1) & 1), C[2] - 1 + (li & 1)};
+                const uint32_t s = W.sf(node);
+                nf[li] = (s & (F_ACTIVE | F_INTERFACE)) ? 1u : ((s & F_DIRICHLET) ? 2u : 0u);
+            }
+            for (int v = 0; v < 3; ++v) {
+                const int a = (v == 0) ? 1 : 0, b = (v == 2) ? 1 : 2;
+                for (int e = 0; e < 4; ++e) {
+                    int lb[3], ub[3];
+                    lb[v] = 0; ub[v] = 1;
+                    lb[a] = ub[a] = e >> 1;
+                    lb[b] = ub[b] = e & 1;
+                    const int l = lb[0] * 4 + lb[1] * 2 + lb[2], u = ub[0] * 4 + ub[1] * 2 + ub[2];
+                    if (nf[l] == 1u && nf[u] == 1u) {
+                        m[l * 8 + u] -= w; m[l * 8 + l] += w; m[u * 8 + u] += w; m[u * 8 + l] -= w;
+                    }
+                    if (nf[l] == 1u && nf[u] == 2u) m[l * 8 + l] += w;
+                    if (nf[l] == 2u && nf[u] == 1u) m[u * 8 + u] += w;
+                }
+            }
+        } else {
+            for (int o = 0; o < 8; ++o) {
+                const I3 child = {2 * C[0] - 1 + (o >> 2), 2 * C[1] - 1 + ((o >> 1) & 1), 2 * C[2] - 1 + (o & 1)};
+                const M8 g = galerkin(child, level - 1);
+                const M8& p = P[o];
+                M8 t;
+                for (int i = 0; i < 8; ++i)
+                    for (int j = 0; j < 8; ++j) {
+                        float acc = 0;
+                        for (int k = 0; k < 8; ++k) acc += g[i * 8 + k] * p[k * 8 + j];
+                        t[i * 8 + j] = acc;
+                    }
+                for (int i = 0; i < 8; ++i)
+                    for (int j = 0; j < 8; ++j) {
+                        float acc = 0;
+                        for (int k = 0; k < 8; ++k) acc += p[k * 8 + i] * t[k * 8 + j];
+                        m[i * 8 + j] += acc;
+                    }
+            }
+        }
+        return memo[level].emplace(key, m).first->second;
+    };
+
+    // Assembly (lines 554-655).
+    for (int m = 1; m <= M; ++m) {
+        std::unordered_map<uint64_t, float> aii;
+        std::unordered_map<uint64_t, size_t> air_pos;
+        auto resolve = [&](int L, const I3& p, uint32_t& f, int& id) {
+            I3 idx = p;
+            int cur = L;
+            {
+                const LevelArrays& A = H[m][cur];
+                const size_t pp = A.at(idx);
+                f = A.flags[pp];
+                id = A.index[pp];
+            }
+            while (!(f & N_DEGREE)) {
+                if (++cur > levels) throw Error(HDD_ERR_INTERNAL, "interface DOF lookup past the coarsest level");
+                for (int a = 0; a < 3; ++a) idx[a] /= 2;
+                const LevelArrays& A = H[m][cur];
+                const size_t pp = A.at(idx);
+                f = A.flags[pp];
+                id = A.index[pp];
+            }
+        };
+        for (int L = m; L <= levels; ++L)
+            for (const I3& c : interior_cells(m, L)) {
+                const M8& cm = galerkin(c, L);
+                Parents par[8];
+                for (int li = 0; li < 8; ++li) {
+                    const I3 N = {c[0] - 1 + (li >> 2), c[1] - 1 + ((li >> 1) & 1), c[2] - 1 + (li & 1)};
+                    embed(N, par[li], 1.0f, q[L]);
+                }
+                for (int n1 = 0; n1 < 8; ++n1)
+                    for (int n2 = 0; n2 < 8; ++n2) {
+                        const float e = cm[n1 * 8 + n2];
+                        if (e == 0) continue;
+                        for (auto& p1 : par[n1])
+                            for (auto& p2 : par[n2]) {
+                                uint32_t f1, f2;
+                                int id1, id2;
+                                resolve(L, p1.first, f1, id1);
+                                resolve(L, p2.first, f2, id2);
+                                const float v = p1.second * p2.second * e;
+                                const bool a1 = f1 & (N_ACTIVE | N_COARSE_SHARED), a2 = f2 & (N_ACTIVE | N_COARSE_SHARED);
+                                if ((f1 & N_INTERFACE) && (f2 & N_INTERFACE))
+                                    W.arr_terms[m - 1].push_back({{id1, id2}, v});
+                                if (a1 && a2) aii[((uint64_t)(uint32_t)id1 << 32) | (uint32_t)id2] += v;
+                                if (a1 && (f2 & N_INTERFACE)) {
+                                    const uint64_t key = ((uint64_t)(uint32_t)id1 << 32) | (uint32_t)id2;
+                                    auto it = air_pos.find(key);
+                                    if (it == air_pos.end()) {
+                                        air_pos.emplace(key, W.air_terms[m - 1].size());
+                                        W.air_terms[m - 1].push_back({{id1, id2}, v});
+                                    } else W.air_terms[m - 1][it->second].second += v;
+                                }
+                            }
+                    }
+            }
+        const int ni = node_count[m];
+        W.n_int[m - 1] = ni;
+        // Aii in CSR with explicit zeros dropped (Convert_To_Eigen, lines 687-705).
+        std::vector<std::pair<uint64_t, float>> e(aii.begin(), aii.end());
+        e.erase(std::remove_if(e.begin(), e.end(), [](const auto& t) { return t.second == 0.0f; }), e.end());
+        std::sort(e.begin(), e.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        CsrF& A = W.aii[m - 1];
+        A.rows = A.cols = ni;
+        A.ptr.assign(ni + 1, 0);
+        for (auto& t : e) A.ptr[(int)(t.first >> 32) + 1]++;
+        for (int r = 0; r < ni; ++r) A.ptr[r + 1] += A.ptr[r];
+        A.col.resize(e.size());
+        A.val.resize(e.size());
+        for (size_t i = 0; i < e.size(); ++i) { A.col[i] = (int)(uint32_t)e[i].first; A.val[i] = e[i].second; }
+    }
+}
+
+CsrF csr_from_pairs(int rows, int cols, std::vector<std::pair<uint64_t, float>>& e) {
+    e.erase(std::remove_if(e.begin(), e.end(), [](const auto& t) { return t.second == 0.0f; }), e.end());
+    std::sort(e.begin(), e.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    CsrF A;
+    A.rows = rows;
+    A.cols = cols;
+    A.ptr.assign(rows + 1, 0);
+    for (auto& t : e) A.ptr[(int)(t.first >> 32) + 1]++;
+    for (int r = 0; r < rows; ++r) A.ptr[r + 1] += A.ptr[r];
+    A.col.resize(e.size());
+    A.val.resize(e.size());
+    for (size_t i = 0; i < e.size(); ++i) { A.col[i] = (int)(uint32_t)e[i].first; A.val[i] = e[i].second; }
+    return A;
+}
+
+}  // namespace
+
+void build_interface(const DomainLayout& L, int M, InterfaceHost& out) {
+    const int* size = L.opt.size;
+    const int* sub = L.opt.sub;
+    int ns[3];
+    number_of_subdomains(size, sub, ns);
+    const int nsub = ns[0] * ns[1] * ns[2];
+    static const std::array<M8, 8> P = bake_prolongation();
+    std::vector<BoxWork> work(nsub);
+    std::vector<std::string> errors(nsub);
+#pragma omp parallel for schedule(dynamic)
+    for (int s = 0; s < nsub; ++s) {
+        try {
+            const int i = s / (ns[1] * ns[2]), j = (s / ns[2]) % ns[1], k = s % ns[2];
+            BoxWork& W = work[s];
+            W.lo = {i * sub[0], j * sub[1], k * sub[2]};
+            W.hi = {W.lo[0] + sub[0], W.lo[1] + sub[1], W.lo[2] + sub[2]};
+            for (int a = 0; a < 3; ++a) W.e1[a] = sub[a] + 1;
+            // Subdomain node flags: Active cells of the box (the splitter's temporary
+            // Boundary marks), other non-zero flags kept; cells without an Active
+            // face neighbour inside the box dropped; box-face Active cells become
+            // Interface (Domain_Divider on the box).
+            std::vector<uint32_t> t((size_t)W.e1[0] * W.e1[1] * W.e1[2], 0u);
+            auto lid = [&](int x, int y, int z) { return ((size_t)x * W.e1[1] + y) * W.e1[2] + z; };
+            for (int x = 0; x < W.e1[0]; ++x)
+                for (int y = 0; y < W.e1[1]; ++y)
+                    for (int z = 0; z < W.e1[2]; ++z) {
+                        const int gi = W.lo[0] + x, gj = W.lo[1] + y, gk = W.lo[2] + z;
+                        uint32_t f0 = 0;
+                        if (gi < size[0] && gj < size[1] && gk < size[2]) f0 = L.flags_in[L.dense_index(gi, gj, gk)];
+                        t[lid(x, y, z)] = (f0 & F_ACTIVE) ? F_ACTIVE : f0;
+                    }
+            W.sub_flags.assign(t.size(), 0u);
+            for (int x = 0; x < W.e1[0]; ++x)
+                for (int y = 0; y < W.e1[1]; ++y)
+                    for (int z = 0; z < W.e1[2]; ++z) {
+                        uint32_t v = t[lid(x, y, z)];
+                        if (!v) continue;
+                        bool nb = false;
+                        const int d[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+                        for (int f = 0; f < 6 && !nb; ++f) {
+                            const int a = x + d[f][0], b = y + d[f][1], c = z + d[f][2];
+                            if (a < 0 || b < 0 || c < 0 || a >= W.e1[0] || b >= W.e1[1] || c >= W.e1[2]) continue;
+                            if (t[lid(a, b, c)] & F_ACTIVE) nb = true;
+                        }
+                        if (!nb) continue;
+                        const int gi = W.lo[0] + x, gj = W.lo[1] + y, gk = W.lo[2] + z;
+                        if ((v & F_ACTIVE) && (gi % sub[0] == 0 || gj % sub[1] == 0 || gk % sub[2] == 0))
+                            v = (v - F_ACTIVE) | F_INTERFACE;
+                        W.sub_flags[lid(x, y, z)] = v;
+                    }
+            process_box(W, M, P);
+        } catch (const std::exception& e) {
+            errors[s] = e.what();
+        }
+    }
+    for (auto& e : errors)
+        if (!e.empty()) throw Error(HDD_ERR_UNSUPPORTED, "interface assembly: " + e);
+
+    // Serial merge in subdomain order: global interface numbering (first
+    // encounter) and the per-key summation of Arr across subdomains.
+    out.M = M;
+    out.n_sub = nsub;
+    out.n_iface.assign(M, 0);
+    out.iface_map.clear();
+    out.Arr.assign(M, CsrF());
+    out.Aii.assign(M, std::vector<CsrF>(nsub));
+    out.Air.assign(M, std::vector<CsrF>(nsub));
+    std::vector<std::unordered_map<uint64_t, int>> gid(M);
+    std::vector<std::unordered_map<uint64_t, float>> arr(M);
+    std::vector<std::vector<std::pair<uint64_t, float>>> air_pairs(nsub);
+    for (int m = 0; m < M; ++m) {
+        for (int s = 0; s < nsub; ++s) {
+            BoxWork& W = work[s];
+            std::vector<int> to_g(W.iface_nodes[m].size());
+            for (size_t i = 0; i < W.iface_nodes[m].size(); ++i) {
+                const I3& nd = W.iface_nodes[m][i];
+                const uint64_t key = ((uint64_t)nd[0] << 42) | ((uint64_t)nd[1] << 21) | (uint64_t)nd[2];
+                auto it = gid[m].find(key);
+                if (it == gid[m].end()) {
+                    it = gid[m].emplace(key, out.n_iface[m]++).first;
+                    if (m == 0) out.iface_map.push_back(nd);
+                }
+                to_g[i] = it->second;
+            }
+            for (auto& tv : W.arr_terms[m])
+                arr[m][((uint64_t)(uint32_t)to_g[tv.first.first] << 32) | (uint32_t)to_g[tv.first.second]] += tv.second;
+            std::vector<std::pair<uint64_t, float>> ap;
+            ap.reserve(W.air_terms[m].size());
+            for (auto& tv : W.air_terms[m])
+                ap.push_back({((uint64_t)(uint32_t)tv.first.first << 32) | (uint32_t)to_g[tv.first.second], tv.second});
+            air_pairs[s].swap(ap);
+            out.Aii[m][s] = std::move(W.aii[m]);
+            W.arr_terms[m].clear();
+        }
+        for (int s = 0; s < nsub; ++s) out.Air[m][s] = csr_from_pairs(work[s].n_int[m], 0, air_pairs[s]);
+        std::vector<std::pair<uint64_t, float>> ae(arr[m].begin(), arr[m].end());
+        out.Arr[m] = csr_from_pairs(out.n_iface[m], out.n_iface[m], ae);
+        for (int s = 0; s < nsub; ++s) out.Air[m][s].cols = out.n_iface[m];
+        if (m == 0)
+            for (int r = 0; r < out.Arr[0].rows; ++r) {
+                bool diag = false;
+                for (int p = out.Arr[0].ptr[r]; p < out.Arr[0].ptr[r + 1]; ++p)
+                    if (out.Arr[0].col[p] == r) diag = true;
+                if (!diag) throw Error(HDD_ERR_INTERNAL, "zero diagonal in the level-0 interface matrix");
+            }
+    }
+    // Interface prolongation Prr[m]: fine level m -> coarse level m+1.
+    out.Prr.assign(M > 1 ? M - 1 : 0, CsrF());
+    for (int m = 0; m + 1 < M; ++m) {
+        std::vector<std::pair<uint64_t, float>> pe;
+        for (auto& kv : gid[m]) {
+            const I3 F = {(int)(kv.first >> 42), (int)((kv.first >> 21) & 0x1fffff), (int)(kv.first & 0x1fffff)};
+            int base[3];
+            for (int v = 0; v < 3; ++v) base[v] = (int)std::floor(F[v] / 2.0);
+            for (int ci = 0; ci < 8; ++ci) {
+                const I3 C = {base[0] + (ci >> 2), base[1] + ((ci >> 1) & 1), base[2] + (ci & 1)};
+                float w = 1.0f;
+                for (int v = 0; v < 3; ++v) w *= (2.0f - std::abs(C[v] * 2 - F[v])) / 2.0;
+                if (!(w > 0)) continue;
+                const uint64_t ck = ((uint64_t)C[0] << 42) | ((uint64_t)C[1] << 21) | (uint64_t)C[2];
+                auto it = gid[m + 1].find(ck);
+                if (it == gid[m + 1].end()) continue;
+                pe.push_back({((uint64_t)(uint32_t)kv.second << 32) | (uint32_t)it->second, w});
+            }
+        }
+        out.Prr[m] = csr_from_pairs(out.n_iface[m], out.n_iface[m + 1], pe);
+    }
+}
+
+}  // namespace hdd

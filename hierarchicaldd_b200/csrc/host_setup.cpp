@@ -1,0 +1,284 @@
+// Host-side domain setup (see host_setup.h).
+#include "host_setup.h"
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+
+namespace hdd {
+
+static const int kFace[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+
+static inline size_t at3(const int n[3], int i, int j, int k) { return ((size_t)i * n[1] + j) * n[2] + k; }
+static inline bool in3(const int n[3], int i, int j, int k) {
+    return i >= 0 && j >= 0 && k >= 0 && i < n[0] && j < n[1] && k < n[2];
+}
+
+void number_of_subdomains(const int size[3], const int sub[3], int out[3]) {
+    // SPGrid_Domain_Divider_Helper.h:192-196 (origin 0).
+    for (int a = 0; a < 3; ++a) out[a] = (size[a] - 1) / sub[a] + (((size[a] - 1) % sub[a]) ? 1 : 0);
+}
+
+void divide_domain(const int size[3], const int sub[3], uint32_t* f) {
+    // SPGrid_Domain_Divider_Helper.h:210-241: Active cells on planes index % sub == 0
+    // become Interface; the others carry the 1-based partition id.
+    int ns[3];
+    number_of_subdomains(size, sub, ns);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < size[0]; ++i)
+        for (int j = 0; j < size[1]; ++j)
+            for (int k = 0; k < size[2]; ++k) {
+                uint32_t& v = f[at3(size, i, j, k)];
+                if (!(v & F_ACTIVE)) continue;
+                if (i % sub[0] == 0 || j % sub[1] == 0 || k % sub[2] == 0) v = (v - F_ACTIVE) | F_INTERFACE;
+                else v |= (uint32_t)((((i / sub[0]) * ns[1] + (j / sub[1])) * ns[2] + (k / sub[2])) + 1);
+            }
+}
+
+void flag_faces(const int n[3], uint32_t* f) {
+    // SPGrid_Flag_Helper.h:74-106.
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n[0]; ++i)
+        for (int j = 0; j < n[1]; ++j)
+            for (int k = 0; k < n[2]; ++k) {
+                uint32_t& v = f[at3(n, i, j, k)];
+                if (!(v & (F_ACTIVE | F_INTERFACE))) continue;
+                for (int q = 0; q < 6; ++q) {
+                    int a = i + kFace[q][0], b = j + kFace[q][1], c = k + kFace[q][2];
+                    if (in3(n, a, b, c) && (f[at3(n, a, b, c)] & (F_ACTIVE | F_INTERFACE | F_DIRICHLET)))
+                        v |= (F_FACE_MX << q);
+                }
+            }
+}
+
+void flag_boundary(const int n[3], uint32_t* f) {
+    // SPGrid_Flag_Boundary_Helper.h:238-307: Active cells within Manhattan
+    // distance 3 of an exterior (flag 0, or outside the grid), Interface or
+    // Dirichlet cell are Boundary.  Computed as a separable distance transform.
+    const size_t N = (size_t)n[0] * n[1] * n[2];
+    std::vector<uint8_t> dist(N);
+#pragma omp parallel for schedule(static)
+    for (long long x = 0; x < (long long)N; ++x) {
+        uint32_t v = f[x];
+        dist[x] = (v == 0u || (v & (F_INTERFACE | F_DIRICHLET))) ? 0 : 4;
+    }
+    // Cells outside the grid are sources: seed distances from the grid edges.
+    auto relax_axis = [&](int axis) {
+        int o1 = (axis == 0) ? 1 : 0, o2 = (axis == 2) ? 1 : 2;
+#pragma omp parallel for schedule(static)
+        for (int a = 0; a < n[o1]; ++a)
+            for (int b = 0; b < n[o2]; ++b) {
+                int idx[3];
+                auto cell = [&](int t) -> uint8_t& {
+                    idx[axis] = t; idx[o1] = a; idx[o2] = b;
+                    return dist[at3(n, idx[0], idx[1], idx[2])];
+                };
+                int d = 1;  // distance to the virtual source just before index 0
+                for (int t = 0; t < n[axis]; ++t) {
+                    uint8_t& c = cell(t);
+                    if (c > d) c = (uint8_t)d;
+                    d = std::min<int>(c + 1, 4);
+                }
+                d = 1;
+                for (int t = n[axis] - 1; t >= 0; --t) {
+                    uint8_t& c = cell(t);
+                    if (c > d) c = (uint8_t)d;
+                    d = std::min<int>(c + 1, 4);
+                }
+            }
+    };
+    // L1 distance = successive 1D passes (min-plus convolution is separable).
+    relax_axis(0);
+    relax_axis(1);
+    relax_axis(2);
+#pragma omp parallel for schedule(static)
+    for (long long x = 0; x < (long long)N; ++x)
+        if ((f[x] & F_ACTIVE) && dist[x] <= 3) f[x] |= F_BOUNDARY;
+}
+
+void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& L) {
+    L.opt = opt;
+    for (int a = 0; a < 3; ++a) {
+        if (opt.size[a] < 3) throw Error(HDD_ERR_INVALID_ARGUMENT, "size must be >= 3 on every axis");
+        int s = opt.sub[a];
+        if (s < 4 || (s & (s - 1))) throw Error(HDD_ERR_UNSUPPORTED, "sub_size must be a power of two >= 4");
+        if ((s >> (opt.vlevels - 1)) < 2)
+            throw Error(HDD_ERR_INVALID_ARGUMENT, "vlevels too deep for sub_size (needs sub_size >> (vlevels-1) >= 2)");
+    }
+    if (opt.vlevels < 1) throw Error(HDD_ERR_INVALID_ARGUMENT, "vlevels must be >= 1");
+    const size_t N = (size_t)opt.size[0] * opt.size[1] * opt.size[2];
+    L.flags_in.assign(flags, flags + N);
+    L.flags0 = L.flags_in;
+    const int* n = opt.size;
+    // Input check: an exterior cell (no type bit) may not touch an Active cell
+    // across a face.  This is the rule the reference generator enforces for
+    // Dirichlet layers (Create_3D_Domain/main.cpp:126-140); it keeps the
+    // per-subdomain V-cycles of the GPU path decoupled at every coarse level.
+    {
+        long long bad = 0;
+#pragma omp parallel for schedule(static) reduction(+ : bad)
+        for (int i = 0; i < n[0]; ++i)
+            for (int j = 0; j < n[1]; ++j)
+                for (int k = 0; k < n[2]; ++k) {
+                    uint32_t v = L.flags0[at3(n, i, j, k)];
+                    if (v & (F_INTERFACE | F_BOUNDARY)) { ++bad; continue; }
+                    if (v & (F_ACTIVE | F_DIRICHLET)) continue;
+                    for (int q = 0; q < 6; ++q) {
+                        int a = i + kFace[q][0], b = j + kFace[q][1], c = k + kFace[q][2];
+                        if (in3(n, a, b, c) && (L.flags0[at3(n, a, b, c)] & F_ACTIVE)) { ++bad; break; }
+                    }
+                }
+        if (bad)
+            throw Error(HDD_ERR_UNSUPPORTED,
+                        "domain has exterior cells face-adjacent to Active cells (or pre-set Interface/"
+                        "Boundary bits): " + std::to_string(bad) + " cells");
+    }
+    // Reference order: global Domain_Divider, Flaging, then the topology's
+    // Flaging (faces again) and Flaging_Boundary on level 0.
+    divide_domain(opt.size, opt.sub, L.flags0.data());
+    flag_faces(n, L.flags0.data());
+    flag_boundary(n, L.flags0.data());
+
+    number_of_subdomains(opt.size, opt.sub, L.ns);
+    for (int a = 0; a < 3; ++a) L.nt[a] = (opt.size[a] + opt.sub[a] - 1) / opt.sub[a];
+    L.tile_cells = opt.sub[0] * opt.sub[1] * opt.sub[2];
+    const size_t ntiles = (size_t)L.nt[0] * L.nt[1] * L.nt[2];
+    std::vector<uint8_t> used(ntiles, 0);
+    for (int i = 0; i < n[0]; ++i)
+        for (int j = 0; j < n[1]; ++j)
+            for (int k = 0; k < n[2]; ++k)
+                if (L.flags0[at3(n, i, j, k)] & (F_ACTIVE | F_INTERFACE))
+                    used[((size_t)(i / opt.sub[0]) * L.nt[1] + j / opt.sub[1]) * L.nt[2] + k / opt.sub[2]] = 1;
+    L.tile_of.assign(ntiles, -1);
+    L.tiles.clear();
+    for (int a = 0; a < L.nt[0]; ++a)
+        for (int b = 0; b < L.nt[1]; ++b)
+            for (int c = 0; c < L.nt[2]; ++c) {
+                size_t t = ((size_t)a * L.nt[1] + b) * L.nt[2] + c;
+                if (used[t]) {
+                    L.tile_of[t] = (int)L.tiles.size();
+                    L.tiles.push_back({a, b, c});
+                }
+            }
+    L.tile_flags.assign(L.tiled_count(), 0);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n[0]; ++i)
+        for (int j = 0; j < n[1]; ++j)
+            for (int k = 0; k < n[2]; ++k) {
+                long long s = L.tile_slot(i, j, k);
+                if (s >= 0) L.tile_flags[s] = compact16(L.flags0[at3(n, i, j, k)]);
+            }
+
+    // Per-box V-cycle levels.
+    const int V = opt.vlevels;
+    L.level_e.assign(3 * V, 0);
+    L.level_off.assign(V + 1, 0);
+    for (int l = 0; l < V; ++l) {
+        size_t cnt = 1;
+        for (int a = 0; a < 3; ++a) {
+            L.level_e[3 * l + a] = (opt.sub[a] >> l) + 1;
+            cnt *= (size_t)L.level_e[3 * l + a];
+        }
+        L.level_off[l + 1] = L.level_off[l] + ((cnt + 15) / 16) * 16;
+    }
+    L.box_stride = L.level_off[V];
+    L.boxes.clear();
+    for (int a = 0; a < L.ns[0]; ++a)
+        for (int b = 0; b < L.ns[1]; ++b)
+            for (int c = 0; c < L.ns[2]; ++c) {
+                bool work = false;
+                for (int i = a * opt.sub[0] + 1; i < (a + 1) * opt.sub[0] && i < n[0] && !work; ++i)
+                    for (int j = b * opt.sub[1] + 1; j < (b + 1) * opt.sub[1] && j < n[1] && !work; ++j)
+                        for (int k = c * opt.sub[2] + 1; k < (c + 1) * opt.sub[2] && k < n[2]; ++k)
+                            if (L.flags0[at3(n, i, j, k)] & F_ACTIVE) { work = true; break; }
+                if (!work) continue;
+                Box bx;
+                bx.k = {a, b, c};
+                bx.tile = L.tile_of[((size_t)a * L.nt[1] + b) * L.nt[2] + c];
+                if (bx.tile < 0) throw Error(HDD_ERR_INTERNAL, "box without a stored tile");
+                int nbk[3][3] = {{a + 1, b, c}, {a, b + 1, c}, {a, b, c + 1}};
+                for (int q = 0; q < 3; ++q) {
+                    int* t = nbk[q];
+                    bx.nb_tile[q] = (t[0] < L.nt[0] && t[1] < L.nt[1] && t[2] < L.nt[2])
+                                        ? L.tile_of[((size_t)t[0] * L.nt[1] + t[1]) * L.nt[2] + t[2]]
+                                        : -1;
+                }
+                L.boxes.push_back(bx);
+            }
+    L.box_flags.assign(L.boxes.size() * L.box_stride, 0);
+#pragma omp parallel for schedule(dynamic)
+    for (long long bi = 0; bi < (long long)L.boxes.size(); ++bi) {
+        const Box& bx = L.boxes[bi];
+        uint8_t* rec = L.box_flags.data() + bi * L.box_stride;
+        // Level 0: reference flags of the box [o, o+sub] (cells outside the grid are 0).
+        std::vector<uint32_t> fine, coarse;
+        int fe[3] = {L.level_e[0], L.level_e[1], L.level_e[2]};
+        fine.assign((size_t)fe[0] * fe[1] * fe[2], 0u);
+        for (int x = 0; x < fe[0]; ++x)
+            for (int y = 0; y < fe[1]; ++y)
+                for (int z = 0; z < fe[2]; ++z) {
+                    int gi = bx.k[0] * opt.sub[0] + x, gj = bx.k[1] * opt.sub[1] + y, gk = bx.k[2] * opt.sub[2] + z;
+                    if (in3(n, gi, gj, gk)) fine[at3(fe, x, y, z)] = L.flags0[at3(n, gi, gj, gk)];
+                }
+        for (size_t x = 0; x < fine.size(); ++x) rec[x] = compact8(fine[x]);
+        for (int l = 1; l < V; ++l) {
+            int ce[3] = {L.level_e[3 * l], L.level_e[3 * l + 1], L.level_e[3 * l + 2]};
+            coarse.assign((size_t)ce[0] * ce[1] * ce[2], 0u);
+            // V_Cycle_Topology.h:35-67: Dirichlet if any child is Dirichlet|Interface,
+            // else Active if any child is Active.  Children of c are 2c-1 and 2c.
+            for (int x = 0; x < ce[0]; ++x)
+                for (int y = 0; y < ce[1]; ++y)
+                    for (int z = 0; z < ce[2]; ++z) {
+                        uint32_t out = 0;
+                        for (int ci = 0; ci < 8; ++ci) {
+                            int fx = 2 * x - 1 + (ci >> 2), fy = 2 * y - 1 + ((ci >> 1) & 1), fz = 2 * z - 1 + (ci & 1);
+                            if (!in3(fe, fx, fy, fz)) continue;
+                            uint32_t v = fine[at3(fe, fx, fy, fz)];
+                            if (v & (F_DIRICHLET | F_INTERFACE)) out = F_DIRICHLET;
+                            else if ((v & F_ACTIVE) && out != F_DIRICHLET) out = F_ACTIVE;
+                        }
+                        coarse[at3(ce, x, y, z)] = out;
+                    }
+            flag_faces(ce, coarse.data());
+            flag_boundary(ce, coarse.data());
+            // Halo planes of a coarse box are never Active under the input check;
+            // verify, since the per-box V-cycle relies on it.
+            for (int x = 0; x < ce[0]; ++x)
+                for (int y = 0; y < ce[1]; ++y)
+                    for (int z = 0; z < ce[2]; ++z) {
+                        bool halo = x == 0 || y == 0 || z == 0 || x == ce[0] - 1 || y == ce[1] - 1 || z == ce[2] - 1;
+                        if (halo && (coarse[at3(ce, x, y, z)] & F_ACTIVE))
+                            throw Error(HDD_ERR_UNSUPPORTED, "coarse level couples subdomains");
+                    }
+            uint8_t* dst = rec + L.level_off[l];
+            for (size_t x = 0; x < coarse.size(); ++x) dst[x] = compact8(coarse[x]);
+            fine.swap(coarse);
+            for (int a = 0; a < 3; ++a) fe[a] = ce[a];
+        }
+    }
+}
+
+void dense_to_tiles(const DomainLayout& L, const float* dense, float* tiled) {
+    const int* n = L.opt.size;
+    std::memset(tiled, 0, L.tiled_count() * sizeof(float));
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n[0]; ++i)
+        for (int j = 0; j < n[1]; ++j)
+            for (int k = 0; k < n[2]; ++k) {
+                long long s = L.tile_slot(i, j, k);
+                if (s >= 0) tiled[s] = dense[at3(n, i, j, k)];
+            }
+}
+
+void tiles_to_dense(const DomainLayout& L, const float* tiled, float* dense) {
+    const int* n = L.opt.size;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n[0]; ++i)
+        for (int j = 0; j < n[1]; ++j)
+            for (int k = 0; k < n[2]; ++k) {
+                long long s = L.tile_slot(i, j, k);
+                dense[at3(n, i, j, k)] = s >= 0 ? tiled[s] : 0.0f;
+            }
+}
+
+}  // namespace hdd

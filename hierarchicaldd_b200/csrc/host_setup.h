@@ -1,0 +1,79 @@
+// Host-side domain setup: reference flag pipeline, subdomain tiles in HBM and
+// per-subdomain coarse levels for the resident V-cycle kernel.
+//
+// Layout.  The grid is cut into tiles of sub_size cells per axis; tile t holds
+// cells [t*sub, (t+1)*sub) per axis, z fastest inside a tile.  Tile k coincides
+// with the reference's subdomain box k ([k*sub, (k+1)*sub], inclusive,
+// SPGrid_Domain_Divider_Helper.h:197-201) minus its upper interface planes,
+// which are the lower planes of tiles k+1.  Only tiles holding Active or
+// Interface cells are stored; absent tiles read as zero.
+#pragma once
+#include <array>
+#include <cstdint>
+#include <vector>
+
+#include "hdd_common.h"
+
+namespace hdd {
+
+struct Options {
+    int size[3];
+    int sub[3];
+    int vlevels, nvcycles, interior, boundary, sigma_levels, sigma_smoothing, sigma_mg;
+};
+
+// One subdomain box with work for the V-cycle.
+struct Box {
+    std::array<int, 3> k;    // box coordinates (== its tile coordinates)
+    int tile;                // stored tile index of the box's own tile
+    int nb_tile[3];          // stored tile index of the +x/+y/+z neighbour tiles (-1 if absent)
+};
+
+struct DomainLayout {
+    Options opt;
+    int nt[3] = {0, 0, 0};   // tiles per axis
+    int ns[3] = {0, 0, 0};   // reference subdomain count per axis
+    int tile_cells = 0;
+    std::vector<int> tile_of;                 // nt0*nt1*nt2 -> stored tile or -1
+    std::vector<std::array<int, 3>> tiles;    // stored tile coordinates
+    std::vector<uint32_t> flags_in;           // caller flags (dense)
+    std::vector<uint32_t> flags0;             // level-0 flags after divider/faces/boundary (dense)
+    std::vector<uint16_t> tile_flags;         // compact16 per stored tile cell
+    std::vector<Box> boxes;
+    // Per-box V-cycle flags: level l box has e_l = (sub >> l) + 1 cells per
+    // axis (including the two halo planes); all levels of a box are stored
+    // back to back, boxes at a fixed stride.
+    std::vector<int> level_e;                 // [vlevels][3]
+    std::vector<size_t> level_off;            // offset of level l inside a box record
+    size_t box_stride = 0;
+    std::vector<uint8_t> box_flags;           // boxes.size() * box_stride
+
+    size_t cell_count() const { return (size_t)opt.size[0] * opt.size[1] * opt.size[2]; }
+    size_t dense_index(int i, int j, int k) const {
+        return ((size_t)i * opt.size[1] + j) * opt.size[2] + k;
+    }
+    // Tile slot of a dense cell, or -1 when its tile is not stored.
+    long long tile_slot(int i, int j, int k) const {
+        int t = tile_of[((size_t)(i / opt.sub[0]) * nt[1] + (j / opt.sub[1])) * nt[2] + (k / opt.sub[2])];
+        if (t < 0) return -1;
+        int l = ((i % opt.sub[0]) * opt.sub[1] + (j % opt.sub[1])) * opt.sub[2] + (k % opt.sub[2]);
+        return (long long)t * tile_cells + l;
+    }
+    size_t tiled_count() const { return tiles.size() * (size_t)tile_cells; }
+};
+
+// Validates options and flags, runs the level-0 flag pipeline and builds the
+// tile layout and per-box coarse levels.  Throws hdd::Error.
+void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& out);
+
+// Dense <-> tiled copies of a float field.
+void dense_to_tiles(const DomainLayout& L, const float* dense, float* tiled);
+void tiles_to_dense(const DomainLayout& L, const float* tiled, float* dense);
+
+// Level-0 flag pipeline pieces (same semantics as the reference passes).
+void divide_domain(const int size[3], const int sub[3], uint32_t* f);
+void flag_faces(const int n[3], uint32_t* f);
+void flag_boundary(const int n[3], uint32_t* f);
+void number_of_subdomains(const int size[3], const int sub[3], int out[3]);
+
+}  // namespace hdd

@@ -1,0 +1,91 @@
+// Launch interfaces of the sm_100a kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace hdd {
+
+constexpr int kMaxLevels = 8;
+
+struct VcycleArgs {
+    float* u;                  // tiled level-0 solution (read halos, write interiors)
+    const float* b;            // tiled level-0 right-hand side
+    const uint8_t* box_flags;  // per-box flag records (all levels)
+    const int* box_tile;       // [nbox]
+    const int* box_nb;         // [nbox*3] +x/+y/+z neighbour tiles (-1 absent)
+    int nbox;
+    int sub;                   // cubic subdomain edge
+    int levels;
+    size_t box_stride;
+    size_t level_off[kMaxLevels];
+    int n_vcycles, interior_itr, boundary_itr, bottom_itr;
+    int halo_from_u;           // 1: halo planes hold interface values read from u
+    int zero_init;             // 1: interior u starts at zero
+    float inv_diag[8];         // omega / face_count (float division on the host)
+    float restrict_w[64];      // (1/8,3/8,3/8,1/8)^3 tensor weights
+    float prolong_w[8];        // 4 * (3/4,1/4)^3 tensor weights
+};
+
+cudaError_t launch_vcycle(const VcycleArgs& a, cudaStream_t stream);
+
+// ---------------------------------------------------------------------------
+// PCG kernels over tiled vectors
+// ---------------------------------------------------------------------------
+struct TileGeom {
+    int sub;                   // cubic tile edge
+    int ntiles;
+    const int* nbr;            // [ntiles*6] face-neighbour tiles (-x,+x,-y,+y,-z,+z), -1 absent
+    const uint16_t* flags;     // compact16 per tile cell
+};
+
+// q = Project(A s) (double accumulation, CG_SYSTEM::Multiply + Project);
+// partial[tile] = sum over the tile of (double)(s*q) (float products).
+cudaError_t launch_laplace_dot(const TileGeom& g, const float* s, float* q, double* partial,
+                               cudaStream_t stream);
+
+// Deterministic final sums of per-tile partials into out[slot] (double).
+cudaError_t launch_reduce_sum(const double* partial, int n, double* out, cudaStream_t stream);
+cudaError_t launch_reduce_max(const float* partial, int n, float* out, cudaStream_t stream);
+
+// Scalar state of the PCG loop on the device.
+struct PcgScalars {
+    double rho_d, rho_old_d, sdq_d;   // raw FP64 sums
+    double alpha_d, beta_d;           // mixed-precision scalars
+    float rho, rho_old, alpha, beta;  // reference FP32 scalars
+    float rmax;                       // max|r|
+    int iteration;
+    int status;                       // 0 ok, 1 non-finite scalar
+};
+
+// partial[tile] = sum (double)(a*b) with project(a) applied in place.
+cudaError_t launch_project_dot(const TileGeom& g, float* a, const float* b, double* partial,
+                               cudaStream_t stream);
+// s = beta*s + z (first: s = z); beta from scalars (mode 0 float, 1 double).
+cudaError_t launch_update_s(const TileGeom& g, float* s, const float* z, const PcgScalars* sc, int first,
+                            int mode, cudaStream_t stream);
+// x += alpha s; r -= alpha q; partial max|r| per tile.
+cudaError_t launch_update_xr(const TileGeom& g, float* x, float* r, const float* s, const float* q,
+                             const PcgScalars* sc, int mode, float* partial_max, cudaStream_t stream);
+// Scalar steps (single thread).
+cudaError_t launch_scalar_rho(PcgScalars* sc, const double* rho_sum, int first, cudaStream_t stream);
+cudaError_t launch_scalar_alpha(PcgScalars* sc, const double* sdq_sum, cudaStream_t stream);
+// r = Project(b - A x); partial max|r|.
+cudaError_t launch_residual(const TileGeom& g, const float* b, const float* x, float* r, float* partial_max,
+                            cudaStream_t stream);
+// v = Project(v).
+cudaError_t launch_project(const TileGeom& g, float* v, cudaStream_t stream);
+
+// ---------------------------------------------------------------------------
+// Interface coupling (Laplace_ri gather and the interface scatter)
+// ---------------------------------------------------------------------------
+// b0[i] = r[c_i] - (float)(-sum over active-face Active neighbours of z)  at Interface cells.
+cudaError_t launch_interface_gather(const TileGeom& g, const long long* iface_slot, const int* iface_nb_slots,
+                                    int n_iface, const float* r, const float* z, float* b0,
+                                    cudaStream_t stream);
+// z[c_i] = u0[i].
+cudaError_t launch_interface_scatter(const long long* iface_slot, int n_iface, const float* u0, float* z,
+                                     cudaStream_t stream);
+
+}  // namespace hdd

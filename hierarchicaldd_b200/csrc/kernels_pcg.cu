@@ -1,0 +1,305 @@
+// PCG vector kernels over tiled vectors (HBM-streaming), sm_100a.
+//
+// Semantics follow CG_SYSTEM / CG_VECTOR / CONJUGATE_GRADIENT of the reference
+// (CPU/SPGrid_Domain_Decomposition_Solver/CG_SYSTEM.cpp:28-119,
+//  CG_VECTOR.cpp:56-74, PB/.../Krylov_Solvers/CONJUGATE_GRADIENT.cpp:30-60):
+// the Laplacian accumulates in FP64 and rounds to FP32, dot products sum FP32
+// products in FP64, and vector updates are FP32 a*c+b without contraction.
+// Per-tile partial sums are reduced in a fixed order, so every sum is
+// deterministic for a given layout.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstdint>
+
+#include "hdd_common.h"
+#include "kernels.h"
+
+namespace hdd {
+
+namespace {
+
+constexpr int kNT = 256;
+
+// Value of the face neighbour `face` of local cell (x,y,z) of tile t.
+__device__ __forceinline__ float nb_value(const TileGeom& g, const float* v, int t, int x, int y, int z,
+                                          int face) {
+    const int S = g.sub;
+    int nx = x, ny = y, nz = z, tt = t;
+    switch (face) {
+        case 0: if (x > 0) nx = x - 1; else { tt = g.nbr[6 * t + 0]; nx = S - 1; } break;
+        case 1: if (x < S - 1) nx = x + 1; else { tt = g.nbr[6 * t + 1]; nx = 0; } break;
+        case 2: if (y > 0) ny = y - 1; else { tt = g.nbr[6 * t + 2]; ny = S - 1; } break;
+        case 3: if (y < S - 1) ny = y + 1; else { tt = g.nbr[6 * t + 3]; ny = 0; } break;
+        case 4: if (z > 0) nz = z - 1; else { tt = g.nbr[6 * t + 4]; nz = S - 1; } break;
+        default: if (z < S - 1) nz = z + 1; else { tt = g.nbr[6 * t + 5]; nz = 0; } break;
+    }
+    if (tt < 0) return 0.0f;
+    return v[(size_t)tt * S * S * S + (nx * S + ny) * S + nz];
+}
+
+__device__ __forceinline__ double laplace_cell(const TileGeom& g, const float* v, int t, int x, int y, int z,
+                                               uint32_t fl, float c) {
+    const double cd = (double)c;
+    double result = 0.0;
+#pragma unroll
+    for (int face = 0; face < 6; ++face)
+        if (fl & (1u << face)) result -= ((double)nb_value(g, v, t, x, y, z, face) - cd);
+    return result;
+}
+
+template <class T>
+__device__ __forceinline__ T block_sum(T v) {
+    __shared__ T red[32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = (l < (int)(blockDim.x >> 5)) ? red[l] : T(0);
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+
+__device__ __forceinline__ float block_max(float v) {
+    __shared__ float red[32];
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = (l < (int)(blockDim.x >> 5)) ? red[l] : 0.0f;
+        for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(kNT) laplace_dot_kernel(TileGeom g, const float* __restrict__ s,
+                                                          float* __restrict__ q, double* partial) {
+    const int t = blockIdx.x;
+    const int S = g.sub, TC = S * S * S;
+    const size_t base = (size_t)t * TC;
+    double acc = 0.0;
+    for (int c = threadIdx.x; c < TC; c += kNT) {
+        const uint32_t fl = g.flags[base + c];
+        float out = 0.0f;
+        const float sv = s[base + c];
+        if (fl & (C_ACTIVE | C_INTERFACE)) {
+            const int z = c % S, tmp = c / S, y = tmp % S, x = tmp / S;
+            out = (float)laplace_cell(g, s, t, x, y, z, fl, sv);
+        }
+        q[base + c] = out;
+        acc += (double)(sv * out);
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) partial[t] = acc;
+}
+
+__global__ void __launch_bounds__(kNT) residual_kernel(TileGeom g, const float* __restrict__ b,
+                                                       const float* __restrict__ x, float* __restrict__ r,
+                                                       float* partial_max) {
+    const int t = blockIdx.x;
+    const int S = g.sub, TC = S * S * S;
+    const size_t base = (size_t)t * TC;
+    float m = 0.0f;
+    for (int c = threadIdx.x; c < TC; c += kNT) {
+        const uint32_t fl = g.flags[base + c];
+        float out = 0.0f;
+        if (fl & (C_ACTIVE | C_INTERFACE)) {
+            const int z = c % S, tmp = c / S, y = tmp % S, xx = tmp / S;
+            const float ax = (float)laplace_cell(g, x, t, xx, y, z, fl, x[base + c]);
+            out = __fsub_rn(b[base + c], ax);
+        }
+        r[base + c] = out;
+        m = fmaxf(m, fabsf(out));
+    }
+    m = block_max(m);
+    if (threadIdx.x == 0) partial_max[t] = m;
+}
+
+__global__ void __launch_bounds__(kNT) project_dot_kernel(TileGeom g, float* __restrict__ a,
+                                                          const float* __restrict__ bv, double* partial) {
+    const int t = blockIdx.x;
+    const int TC = g.sub * g.sub * g.sub;
+    const size_t base = (size_t)t * TC;
+    double acc = 0.0;
+    for (int c = threadIdx.x; c < TC; c += kNT) {
+        const uint32_t fl = g.flags[base + c];
+        float av = a[base + c];
+        if (!(fl & (C_ACTIVE | C_INTERFACE))) { av = 0.0f; a[base + c] = 0.0f; }
+        acc += (double)(av * bv[base + c]);
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) partial[t] = acc;
+}
+
+__global__ void __launch_bounds__(kNT) project_kernel(TileGeom g, float* __restrict__ a) {
+    const int t = blockIdx.x;
+    const int TC = g.sub * g.sub * g.sub;
+    const size_t base = (size_t)t * TC;
+    for (int c = threadIdx.x; c < TC; c += kNT)
+        if (!(g.flags[base + c] & (C_ACTIVE | C_INTERFACE))) a[base + c] = 0.0f;
+}
+
+__global__ void __launch_bounds__(kNT) update_s_kernel(size_t n, float* __restrict__ s,
+                                                       const float* __restrict__ z, const PcgScalars* sc,
+                                                       int first, int mode) {
+    const float beta = sc->beta;
+    const double beta_d = sc->beta_d;
+    for (size_t i = blockIdx.x * (size_t)kNT + threadIdx.x; i < n; i += (size_t)gridDim.x * kNT) {
+        if (first) s[i] = z[i];
+        else if (mode == 0) s[i] = __fadd_rn(__fmul_rn(s[i], beta), z[i]);
+        else s[i] = (float)((double)s[i] * beta_d + (double)z[i]);
+    }
+}
+
+__global__ void __launch_bounds__(kNT) update_xr_kernel(int TC, float* __restrict__ x, float* __restrict__ r,
+                                                        const float* __restrict__ s, const float* __restrict__ q,
+                                                        const PcgScalars* sc, int mode, float* partial_max) {
+    const int t = blockIdx.x;
+    const size_t base = (size_t)t * TC;
+    const float alpha = sc->alpha;
+    const double alpha_d = sc->alpha_d;
+    float m = 0.0f;
+    for (int c = threadIdx.x; c < TC; c += kNT) {
+        const size_t i = base + c;
+        float xv, rv;
+        if (mode == 0) {
+            xv = __fadd_rn(__fmul_rn(s[i], alpha), x[i]);
+            rv = __fadd_rn(__fmul_rn(q[i], -alpha), r[i]);
+        } else {
+            xv = (float)((double)x[i] + alpha_d * (double)s[i]);
+            rv = (float)((double)r[i] - alpha_d * (double)q[i]);
+        }
+        x[i] = xv;
+        r[i] = rv;
+        m = fmaxf(m, fabsf(rv));
+    }
+    m = block_max(m);
+    if (threadIdx.x == 0) partial_max[t] = m;
+}
+
+__global__ void reduce_sum_kernel(const double* partial, int n, double* out) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) *out = acc;
+}
+
+__global__ void reduce_max_kernel(const float* partial, int n, float* out) {
+    float m = 0.0f;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, partial[i]);
+    m = block_max(m);
+    if (threadIdx.x == 0) *out = m;
+}
+
+__global__ void scalar_rho_kernel(PcgScalars* sc, const double* rho_sum, int first) {
+    const double rd = *rho_sum;
+    sc->rho_d = rd;
+    sc->rho = (float)rd;
+    if (!first) {
+        sc->beta = sc->rho / sc->rho_old;
+        sc->beta_d = rd / sc->rho_old_d;
+        if (!isfinite(sc->beta) || !isfinite(sc->beta_d)) sc->status = 1;
+    }
+    if (!isfinite(rd)) sc->status = 1;
+}
+
+__global__ void scalar_alpha_kernel(PcgScalars* sc, const double* sdq_sum) {
+    const double sd = *sdq_sum;
+    sc->sdq_d = sd;
+    const float sdq = (float)sd;
+    sc->alpha = sdq != 0.0f ? sc->rho / sdq : FLT_MAX;  // CONJUGATE_GRADIENT.cpp:57
+    sc->alpha_d = sd != 0.0 ? sc->rho_d / sd : (double)FLT_MAX;
+    sc->rho_old = sc->rho;
+    sc->rho_old_d = sc->rho_d;
+    sc->iteration += 1;
+    if (!isfinite(sd) || !isfinite(sc->alpha)) sc->status = 1;
+}
+
+__global__ void __launch_bounds__(kNT) interface_gather_kernel(const long long* slot, const int* nbs, int n,
+                                                               const float* r, const float* z, float* b0) {
+    const int i = blockIdx.x * kNT + threadIdx.x;
+    if (i >= n) return;
+    double result = 0.0;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        const int s = nbs[6 * i + q];
+        if (s >= 0) result -= (double)z[s];
+    }
+    b0[i] = __fsub_rn(r[slot[i]], (float)result);
+}
+
+__global__ void __launch_bounds__(kNT) interface_scatter_kernel(const long long* slot, int n, const float* u0,
+                                                                float* z) {
+    const int i = blockIdx.x * kNT + threadIdx.x;
+    if (i < n) z[slot[i]] = u0[i];
+}
+
+}  // namespace
+
+cudaError_t launch_laplace_dot(const TileGeom& g, const float* s, float* q, double* partial, cudaStream_t st) {
+    if (g.ntiles == 0) return cudaSuccess;
+    laplace_dot_kernel<<<g.ntiles, kNT, 0, st>>>(g, s, q, partial);
+    return cudaGetLastError();
+}
+cudaError_t launch_residual(const TileGeom& g, const float* b, const float* x, float* r, float* pm, cudaStream_t st) {
+    if (g.ntiles == 0) return cudaSuccess;
+    residual_kernel<<<g.ntiles, kNT, 0, st>>>(g, b, x, r, pm);
+    return cudaGetLastError();
+}
+cudaError_t launch_project_dot(const TileGeom& g, float* a, const float* b, double* partial, cudaStream_t st) {
+    if (g.ntiles == 0) return cudaSuccess;
+    project_dot_kernel<<<g.ntiles, kNT, 0, st>>>(g, a, b, partial);
+    return cudaGetLastError();
+}
+cudaError_t launch_project(const TileGeom& g, float* v, cudaStream_t st) {
+    if (g.ntiles == 0) return cudaSuccess;
+    project_kernel<<<g.ntiles, kNT, 0, st>>>(g, v);
+    return cudaGetLastError();
+}
+cudaError_t launch_update_s(const TileGeom& g, float* s, const float* z, const PcgScalars* sc, int first, int mode,
+                            cudaStream_t st) {
+    const size_t n = (size_t)g.ntiles * g.sub * g.sub * g.sub;
+    if (n == 0) return cudaSuccess;
+    int blocks = (int)((n + kNT - 1) / kNT);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    update_s_kernel<<<blocks, kNT, 0, st>>>(n, s, z, sc, first, mode);
+    return cudaGetLastError();
+}
+cudaError_t launch_update_xr(const TileGeom& g, float* x, float* r, const float* s, const float* q,
+                             const PcgScalars* sc, int mode, float* pm, cudaStream_t st) {
+    if (g.ntiles == 0) return cudaSuccess;
+    update_xr_kernel<<<g.ntiles, kNT, 0, st>>>(g.sub * g.sub * g.sub, x, r, s, q, sc, mode, pm);
+    return cudaGetLastError();
+}
+cudaError_t launch_reduce_sum(const double* partial, int n, double* out, cudaStream_t st) {
+    reduce_sum_kernel<<<1, 1024, 0, st>>>(partial, n, out);
+    return cudaGetLastError();
+}
+cudaError_t launch_reduce_max(const float* partial, int n, float* out, cudaStream_t st) {
+    reduce_max_kernel<<<1, 1024, 0, st>>>(partial, n, out);
+    return cudaGetLastError();
+}
+cudaError_t launch_scalar_rho(PcgScalars* sc, const double* rho_sum, int first, cudaStream_t st) {
+    scalar_rho_kernel<<<1, 1, 0, st>>>(sc, rho_sum, first);
+    return cudaGetLastError();
+}
+cudaError_t launch_scalar_alpha(PcgScalars* sc, const double* sdq_sum, cudaStream_t st) {
+    scalar_alpha_kernel<<<1, 1, 0, st>>>(sc, sdq_sum);
+    return cudaGetLastError();
+}
+cudaError_t launch_interface_gather(const TileGeom&, const long long* slot, const int* nbs, int n, const float* r,
+                                    const float* z, float* b0, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    interface_gather_kernel<<<(n + kNT - 1) / kNT, kNT, 0, st>>>(slot, nbs, n, r, z, b0);
+    return cudaGetLastError();
+}
+cudaError_t launch_interface_scatter(const long long* slot, int n, const float* u0, float* z, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    interface_scatter_kernel<<<(n + kNT - 1) / kNT, kNT, 0, st>>>(slot, n, u0, z);
+    return cudaGetLastError();
+}
+
+}  // namespace hdd

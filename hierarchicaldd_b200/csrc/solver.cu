@@ -1,0 +1,357 @@
+// Solver orchestration: host setup, device residency and the PCG loop.
+//
+// PCG follows PB/Public_Library/PhysBAM_Tools/Krylov_Solvers/CONJUGATE_GRADIENT.cpp:22-67
+// with KRYLOV_SYSTEM_BASE::Precondition (Apply_Preconditioner then Project) and
+// the preconditioner of
+// CPU/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Decomposition_Preconditioner.h:88-128:
+//   pass 1: z_i = V-cycles(r) with interface values 0          (vcycle kernel)
+//   b_G    = r_G - A_Gi z_i                                      (interface gather, Laplace_ri)
+//   u_G    = sigma V-cycle(b_G)                                  (sigma.cu)
+//   pass 2: z_G = u_G, z_i = V-cycles(r) with z_G as boundary     (scatter + vcycle kernel)
+// All vectors stay resident in HBM in the tile layout; scalars live on the
+// device and only max|r| (and a status word) return to the host per iteration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "solver.h"
+
+namespace hdd {
+
+static Options to_options(const hdd_options& o) {
+    Options p;
+    for (int a = 0; a < 3; ++a) { p.size[a] = o.size[a]; p.sub[a] = o.sub_size[a]; }
+    p.vlevels = o.vlevels;
+    p.nvcycles = o.nVcycles;
+    p.interior = o.interior_smoothing;
+    p.boundary = o.boundary_smoothing;
+    p.sigma_levels = o.sigma_levels;
+    p.sigma_smoothing = o.sigma_smoothing;
+    p.sigma_mg = o.sigma_mg;
+    return p;
+}
+
+Solver::Solver(const hdd_options& o) : opts(o) {
+    for (int a = 0; a < 3; ++a)
+        if (o.size[a] < 3 || o.sub_size[a] < 1) throw Error(HDD_ERR_INVALID_ARGUMENT, "invalid size or sub_size");
+    if (o.sub_size[0] != o.sub_size[1] || o.sub_size[0] != o.sub_size[2])
+        throw Error(HDD_ERR_UNSUPPORTED, "sub_size must be equal on all axes");
+    if (o.vlevels < 1 || o.vlevels > kMaxLevels) throw Error(HDD_ERR_INVALID_ARGUMENT, "vlevels out of range");
+    if (o.sigma_levels < 1 || o.nVcycles < 0 || o.sigma_mg < 0 || o.interior_smoothing < 0 ||
+        o.boundary_smoothing < 0 || o.sigma_smoothing < 0)
+        throw Error(HDD_ERR_INVALID_ARGUMENT, "negative iteration counts");
+    int ndev = 0;
+    cuda_check(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+    if (o.device < 0 || o.device >= ndev) throw Error(HDD_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    cuda_check(cudaSetDevice(o.device), "cudaSetDevice");
+    cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+}
+
+Solver::~Solver() {
+    if (stream) {
+        cudaStreamSynchronize(stream);
+        sigma.release();
+        cudaStreamDestroy(stream);
+    }
+}
+
+void Solver::set_domain(const uint32_t* flags, const float* rhs) {
+    const size_t n = (size_t)opts.size[0] * opts.size[1] * opts.size[2];
+    flags_in.assign(flags, flags + n);
+    rhs_dense.assign(rhs, rhs + n);
+    have_domain = true;
+    initialized = false;
+    solved = false;
+}
+
+TileGeom Solver::geom() const {
+    TileGeom g;
+    g.sub = L.opt.sub[0];
+    g.ntiles = (int)L.tiles.size();
+    g.nbr = tile_nbr.p;
+    g.flags = tflags.p;
+    return g;
+}
+
+void Solver::initialize() {
+    if (!have_domain) throw Error(HDD_ERR_NOT_INITIALIZED, "no domain set");
+    cuda_check(cudaSetDevice(opts.device), "cudaSetDevice");
+    const auto t0 = std::chrono::steady_clock::now();
+    build_layout(to_options(opts), flags_in.data(), L);
+    const int S = L.opt.sub[0];
+    const size_t nt = L.tiles.size(), tc = (size_t)L.tile_cells, N = nt * tc;
+    // Tile neighbour table (-x,+x,-y,+y,-z,+z).
+    std::vector<int> nbr(nt * 6, -1);
+    for (size_t t = 0; t < nt; ++t) {
+        const auto& c = L.tiles[t];
+        const int d[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+        for (int q = 0; q < 6; ++q) {
+            const int a = c[0] + d[q][0], b = c[1] + d[q][1], e = c[2] + d[q][2];
+            if (a < 0 || b < 0 || e < 0 || a >= L.nt[0] || b >= L.nt[1] || e >= L.nt[2]) continue;
+            nbr[6 * t + q] = L.tile_of[((size_t)a * L.nt[1] + b) * L.nt[2] + e];
+        }
+    }
+    tile_nbr.upload(nbr.data(), nbr.size(), stream);
+    tflags.upload(L.tile_flags.data(), L.tile_flags.size(), stream);
+    std::vector<int> btile(L.boxes.size()), bnb(3 * L.boxes.size());
+    for (size_t i = 0; i < L.boxes.size(); ++i) {
+        btile[i] = L.boxes[i].tile;
+        for (int q = 0; q < 3; ++q) bnb[3 * i + q] = L.boxes[i].nb_tile[q];
+    }
+    box_tile.upload(btile.data(), btile.size(), stream);
+    box_nb.upload(bnb.data(), bnb.size(), stream);
+    box_flags.upload(L.box_flags.data(), L.box_flags.size(), stream);
+    for (DevBuf<float>* v : {&x, &b, &r, &z, &s, &q}) { v->alloc(std::max<size_t>(N, 1)); v->zero(stream); }
+    partial.alloc(std::max<size_t>(nt, 1));
+    partial_max.alloc(std::max<size_t>(nt, 1));
+    sums.alloc(8);
+    scalars_f.alloc(8);
+    scal.alloc(1);
+    (void)S;
+
+    // Interface system (host assembly + factorisations) and its device solver.
+    build_interface(L, opts.sigma_levels, ih);
+    sigma.setup(ih, opts.sigma_smoothing, stream);
+    // Level-0 interface DOFs: cell slots and their Active face neighbours.
+    const int n_if = ih.n_iface.empty() ? 0 : ih.n_iface[0];
+    std::vector<long long> slot(n_if);
+    std::vector<int> nbs(6 * (size_t)n_if, -1);
+    const int* n = L.opt.size;
+    const int d6[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+    for (int i = 0; i < n_if; ++i) {
+        const auto& c = ih.iface_map[i];
+        slot[i] = L.tile_slot(c[0], c[1], c[2]);
+        const uint32_t f = L.flags0[L.dense_index(c[0], c[1], c[2])];
+        if (slot[i] < 0 || !(f & F_INTERFACE)) throw Error(HDD_ERR_INTERNAL, "interface DOF outside the tile layout");
+        for (int qf = 0; qf < 6; ++qf) {
+            if (!(f & (F_FACE_MX << qf))) continue;
+            const int a = c[0] + d6[qf][0], bb = c[1] + d6[qf][1], e = c[2] + d6[qf][2];
+            if (a < 0 || bb < 0 || e < 0 || a >= n[0] || bb >= n[1] || e >= n[2]) continue;
+            if (!(L.flags0[L.dense_index(a, bb, e)] & F_ACTIVE)) continue;
+            const long long sl = L.tile_slot(a, bb, e);
+            if (sl > INT32_MAX) throw Error(HDD_ERR_UNSUPPORTED, "domain too large for 32-bit neighbour slots");
+            nbs[6 * (size_t)i + qf] = (int)sl;
+        }
+    }
+    iface_slot.upload(slot.data(), slot.size(), stream);
+    iface_nb.upload(nbs.data(), nbs.size(), stream);
+    set_rhs(rhs_dense.data());
+    sync();
+    initialized = true;
+    setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void Solver::set_rhs(const float* rhs) {
+    if (rhs != rhs_dense.data()) rhs_dense.assign(rhs, rhs + L.cell_count());
+    std::vector<float> t(L.tiled_count());
+    dense_to_tiles(L, rhs_dense.data(), t.data());
+    cuda_check(cudaMemcpyAsync(b.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D rhs");
+    sync();
+}
+
+VcycleArgs Solver::vcycle_args(float* u, const float* bb, int halo_from_u, int zero_init, int nv) const {
+    VcycleArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.u = u;
+    a.b = bb;
+    a.box_flags = box_flags.p;
+    a.box_tile = box_tile.p;
+    a.box_nb = box_nb.p;
+    a.nbox = (int)L.boxes.size();
+    a.sub = L.opt.sub[0];
+    a.levels = L.opt.vlevels;
+    a.box_stride = L.box_stride;
+    for (int l = 0; l < L.opt.vlevels; ++l) a.level_off[l] = L.level_off[l];
+    a.n_vcycles = nv;
+    a.interior_itr = L.opt.interior;
+    a.boundary_itr = L.opt.boundary;
+    a.bottom_itr = 200;  // CPU/SPGrid_Library/SPGrid_V_Cycle_Helper.h:179
+    a.halo_from_u = halo_from_u;
+    a.zero_init = zero_init;
+    // Correction weights omega/face_count with omega = (float)(2/3)
+    // (SPGrid_Correction_Legacy.h:149,190), divided in float on the host.
+    const float omega = (float)(2. / 3.);
+    a.inv_diag[0] = 0.0f;
+    for (int k = 1; k < 8; ++k) a.inv_diag[k] = omega / (float)k;
+    // Restriction tensor weights (SPGrid_Restriction_Legacy.h:49-57).
+    const float s1[4] = {(float)(1. / 8.), (float)(3. / 8.), (float)(3. / 8.), (float)(1. / 8.)};
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j)
+            for (int k = 0; k < 4; ++k) a.restrict_w[(i * 4 + j) * 4 + k] = s1[i] * s1[j] * s1[k];
+    // Prolongation tensor weights (SPGrid_Prolongation_Legacy.h:48-53).
+    const float p1[2] = {(float)(3. / 4.f), (float)(1. / 4.f)};
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j)
+            for (int k = 0; k < 2; ++k) a.prolong_w[(i * 2 + j) * 2 + k] = p1[i] * p1[j] * p1[k] * 4.0f;
+    return a;
+}
+
+void Solver::run_vcycle(float* u, const float* bb, int halo_from_u, int zero_init, int nv) {
+    VcycleArgs a = vcycle_args(u, bb, halo_from_u, zero_init, nv);
+    cuda_check(launch_vcycle(a, stream), "vcycle kernel");
+    count();
+}
+
+void Solver::apply_preconditioner(const float* rr, float* zz) {
+    const TileGeom g = geom();
+    run_vcycle(zz, rr, 0, 1, opts.nVcycles);
+    const int n_if = ih.n_iface.empty() ? 0 : ih.n_iface[0];
+    cuda_check(launch_interface_gather(g, iface_slot.p, iface_nb.p, n_if, rr, zz, sigma.b0(), stream), "gather");
+    count();
+    // u_G = 0 then sigma_mg V-cycles (Preconditioner.h:105,110-117).
+    cuda_check(cudaMemsetAsync(sigma.u0(), 0, sizeof(float) * std::max(n_if, 1), stream), "memset u0");
+    for (int i = 0; i < opts.sigma_mg; ++i) sigma.vcycle(stream, launches);
+    cuda_check(launch_interface_scatter(iface_slot.p, n_if, sigma.u0(), zz, stream), "scatter");
+    count();
+    run_vcycle(zz, rr, 1, 1, opts.nVcycles);
+}
+
+void Solver::solve(hdd_result* res) {
+    if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+    cuda_check(cudaSetDevice(opts.device), "cudaSetDevice");
+    const TileGeom g = geom();
+    const int nt = g.ntiles;
+    const int mode = opts.precision_mode == HDD_PRECISION_MIXED ? 1 : 0;
+    PcgScalars init;
+    std::memset(&init, 0, sizeof(init));
+    init.rho_old = 3.402823466e+38f;
+    init.rho_old_d = 3.402823466e+38;
+    cuda_check(cudaMemcpyAsync(scal.p, &init, sizeof(init), cudaMemcpyHostToDevice, stream), "init scalars");
+    x.zero(stream);
+    cudaEvent_t e0, e1;
+    cuda_check(cudaEventCreate(&e0), "event");
+    cuda_check(cudaEventCreate(&e1), "event");
+    cuda_check(cudaEventRecord(e0, stream), "event record");
+    // r = Project(b - A x) with x = 0 (restart branch, CONJUGATE_GRADIENT.cpp:36).
+    cuda_check(launch_residual(g, b.p, x.p, r.p, partial_max.p, stream), "residual"); count();
+    cuda_check(launch_reduce_max(partial_max.p, nt, scalars_f.p, stream), "reduce"); count();
+    float rmax = 0;
+    PcgScalars hs;
+    cuda_check(cudaMemcpyAsync(&rmax, scalars_f.p, sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    const double b_inf = rmax;
+    const float threshold = opts.relative_tol ? (float)(opts.tol * b_inf) : (float)opts.tol;
+    const float small_number = 1.1920929e-07f;
+    int it = 0;
+    bool converged = false, breakdown = false;
+    for (;; ++it) {
+        if (rmax <= threshold && (it >= opts.min_iters || rmax < small_number)) { converged = true; break; }
+        if (it >= opts.max_iters) break;
+        apply_preconditioner(r.p, z.p);
+        cuda_check(launch_project_dot(g, z.p, r.p, partial.p, stream), "project_dot"); count();
+        cuda_check(launch_reduce_sum(partial.p, nt, sums.p + 0, stream), "reduce"); count();
+        cuda_check(launch_scalar_rho(scal.p, sums.p + 0, it == 0, stream), "rho"); count();
+        cuda_check(launch_update_s(g, s.p, z.p, scal.p, it == 0, mode, stream), "update_s"); count();
+        cuda_check(launch_laplace_dot(g, s.p, q.p, partial.p, stream), "laplace"); count();
+        cuda_check(launch_reduce_sum(partial.p, nt, sums.p + 1, stream), "reduce"); count();
+        cuda_check(launch_scalar_alpha(scal.p, sums.p + 1, stream), "alpha"); count();
+        cuda_check(launch_update_xr(g, x.p, r.p, s.p, q.p, scal.p, mode, partial_max.p, stream), "update_xr"); count();
+        if (mode == 1 && opts.true_residual_every > 0 && (it + 1) % opts.true_residual_every == 0) {
+            cuda_check(launch_residual(g, b.p, x.p, r.p, partial_max.p, stream), "true residual"); count();
+        }
+        cuda_check(launch_reduce_max(partial_max.p, nt, scalars_f.p, stream), "reduce"); count();
+        cuda_check(cudaMemcpyAsync(&rmax, scalars_f.p, sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
+        cuda_check(cudaMemcpyAsync(&hs, scal.p, sizeof(hs), cudaMemcpyDeviceToHost, stream), "D2H");
+        sync();
+        if (hs.status != 0 || !std::isfinite(rmax)) { breakdown = true; ++it; break; }
+    }
+    cuda_check(cudaEventRecord(e1, stream), "event record");
+    cuda_check(cudaEventSynchronize(e1), "event sync");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // True residual of the returned x (reported, not used for stopping).
+    cuda_check(launch_residual(g, b.p, x.p, q.p, partial_max.p, stream), "true residual"); count();
+    cuda_check(launch_reduce_max(partial_max.p, nt, scalars_f.p + 1, stream), "reduce"); count();
+    cuda_check(launch_project_dot(g, q.p, q.p, partial.p, stream), "dot"); count();
+    cuda_check(launch_reduce_sum(partial.p, nt, sums.p + 2, stream), "reduce"); count();
+    cuda_check(launch_project_dot(g, b.p, b.p, partial.p, stream), "dot"); count();
+    cuda_check(launch_reduce_sum(partial.p, nt, sums.p + 3, stream), "reduce"); count();
+    float tmax = 0;
+    double d2[2] = {0, 0};
+    cuda_check(cudaMemcpyAsync(&tmax, scalars_f.p + 1, sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
+    cuda_check(cudaMemcpyAsync(d2, sums.p + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    solved = true;
+    if (res) {
+        res->iterations = it;
+        res->converged = converged ? 1 : 0;
+        res->final_norm = rmax;
+        res->b_inf = b_inf;
+        res->true_residual_inf = b_inf > 0 ? tmax / b_inf : tmax;
+        res->true_residual_l2 = d2[1] > 0 ? std::sqrt(d2[0] / d2[1]) : std::sqrt(d2[0]);
+        res->solve_ms = ms;
+        res->setup_ms = setup_ms;
+    }
+    if (breakdown) throw Error(HDD_ERR_BREAKDOWN, "PCG breakdown: non-finite scalar");
+    if (!converged) throw Error(HDD_ERR_NOT_CONVERGED, "PCG did not converge within max_iters");
+}
+
+void Solver::get_solution(float* out) {
+    if (!solved) throw Error(HDD_ERR_NOT_INITIALIZED, "no solution available");
+    std::vector<float> t(L.tiled_count());
+    cuda_check(cudaMemcpyAsync(t.data(), x.p, t.size() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H x");
+    sync();
+    tiles_to_dense(L, t.data(), out);
+}
+
+void Solver::apply_preconditioner_dense(const float* rin, float* zout) {
+    if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+    std::vector<float> t(L.tiled_count());
+    dense_to_tiles(L, rin, t.data());
+    cuda_check(cudaMemcpyAsync(r.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
+    z.zero(stream);
+    apply_preconditioner(r.p, z.p);
+    cuda_check(launch_project(geom(), z.p, stream), "project"); count();
+    cuda_check(cudaMemcpyAsync(t.data(), z.p, t.size() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    tiles_to_dense(L, t.data(), zout);
+}
+
+void Solver::vcycle_dense(float* u, const float* bb, int nv) {
+    if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+    std::vector<float> t(L.tiled_count());
+    dense_to_tiles(L, u, t.data());
+    cuda_check(cudaMemcpyAsync(z.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
+    std::vector<float> tb(L.tiled_count());
+    dense_to_tiles(L, bb, tb.data());
+    cuda_check(cudaMemcpyAsync(q.p, tb.data(), tb.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
+    run_vcycle(z.p, q.p, 1, 0, nv);
+    cuda_check(cudaMemcpyAsync(t.data(), z.p, t.size() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    // Cells outside stored tiles keep the caller's values.
+    std::vector<float> dense(L.cell_count());
+    tiles_to_dense(L, t.data(), dense.data());
+    const int* n = L.opt.size;
+    for (int i = 0; i < n[0]; ++i)
+        for (int j = 0; j < n[1]; ++j)
+            for (int k = 0; k < n[2]; ++k)
+                if (L.tile_slot(i, j, k) >= 0) u[L.dense_index(i, j, k)] = dense[L.dense_index(i, j, k)];
+}
+
+void Solver::multiply_dense(const float* xin, float* yout) {
+    if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+    std::vector<float> t(L.tiled_count());
+    dense_to_tiles(L, xin, t.data());
+    cuda_check(cudaMemcpyAsync(s.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
+    cuda_check(launch_laplace_dot(geom(), s.p, q.p, partial.p, stream), "laplace"); count();
+    cuda_check(cudaMemcpyAsync(t.data(), q.p, t.size() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    tiles_to_dense(L, t.data(), yout);
+}
+
+void Solver::sigma_vcycle_host(const float* b0, float* u0) {
+    if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+    const int n_if = ih.n_iface.empty() ? 0 : ih.n_iface[0];
+    cuda_check(cudaMemcpyAsync(sigma.b0(), b0, n_if * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
+    cuda_check(cudaMemsetAsync(sigma.u0(), 0, n_if * sizeof(float), stream), "memset");
+    sigma.vcycle(stream, launches);
+    cuda_check(cudaMemcpyAsync(u0, sigma.u0(), n_if * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+}
+
+}  // namespace hdd

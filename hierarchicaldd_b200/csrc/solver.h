@@ -1,0 +1,104 @@
+// Solver object behind the C ABI: host setup, device buffers and the PCG
+// orchestration on one stream.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "hdd_common.h"
+#include "host_setup.h"
+#include "kernels.h"
+#include "sigma.h"
+
+namespace hdd {
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        release();
+        if (count == 0) return;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            throw Error(e == cudaErrorMemoryAllocation ? HDD_ERR_OUT_OF_MEMORY : HDD_ERR_CUDA,
+                        std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        n = count;
+    }
+    void upload(const T* h, size_t count, cudaStream_t s) {
+        alloc(count);
+        if (count) check(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void zero(cudaStream_t s) {
+        if (n) check(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+    }
+    static void check(cudaError_t e) {
+        if (e != cudaSuccess) throw Error(HDD_ERR_CUDA, cudaGetErrorString(e));
+    }
+};
+
+inline void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw Error(HDD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+struct Solver {
+    hdd_options opts;
+    std::string last_error;
+    long long launches = 0;
+
+    bool have_domain = false, initialized = false, solved = false;
+    DomainLayout L;
+    std::vector<uint32_t> flags_in;
+    std::vector<float> rhs_dense;
+
+    cudaStream_t stream = nullptr;
+    DevBuf<float> x, b, r, z, s, q;
+    DevBuf<uint16_t> tflags;
+    DevBuf<int> tile_nbr, box_tile, box_nb;
+    DevBuf<uint8_t> box_flags;
+    DevBuf<double> partial, sums;
+    DevBuf<float> partial_max, scalars_f;
+    DevBuf<PcgScalars> scal;
+    // Level-0 interface DOFs (sigma level 0 order).
+    DevBuf<long long> iface_slot;
+    DevBuf<int> iface_nb;
+    SigmaGpu sigma;
+    InterfaceHost ih;
+    double setup_ms = 0;
+
+    explicit Solver(const hdd_options& o);
+    ~Solver();
+
+    void set_domain(const uint32_t* flags, const float* rhs);
+    void set_rhs(const float* rhs);
+    void initialize();
+    void solve(hdd_result* res);
+    void get_solution(float* out);
+    void apply_preconditioner_dense(const float* r, float* zout);
+    void vcycle_dense(float* u, const float* bb, int nv);
+    void multiply_dense(const float* xin, float* yout);
+    void sigma_vcycle_host(const float* b0, float* u0);
+
+    // Device pieces.
+    TileGeom geom() const;
+    VcycleArgs vcycle_args(float* u, const float* bb, int halo_from_u, int zero_init, int nv) const;
+    void run_vcycle(float* u, const float* bb, int halo_from_u, int zero_init, int nv);
+    void apply_preconditioner(const float* rr, float* zz);   // device tiled vectors
+    void count(int n = 1) { launches += n; }
+    void sync() { cuda_check(cudaStreamSynchronize(stream), "stream sync"); }
+};
+
+}  // namespace hdd

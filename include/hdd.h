@@ -1,0 +1,150 @@
+/*
+ * hdd.h -- C ABI of the B200 hierarchical domain-decomposition PCG Poisson solver.
+ *
+ * Drop-in boundary for the reference's solver API (uwgraphics/hierarchicaldd,
+ * class SPGrid_Domain_Decomposition_Solver and the Test_Bench options).  Every
+ * entry point returns an hdd_status; no C++ exception crosses this boundary.
+ * The caller owns host buffers; the library owns all device memory.  A solver
+ * handle is used from one host thread at a time.
+ *
+ * Dense arrays ("*_dense") cover the whole grid of size[0]*size[1]*size[2]
+ * cells, x slowest and z fastest: element (i,j,k) is at (i*size[1]+j)*size[2]+k.
+ * Flags use the reference bit layout (Active 0x10000, Dirichlet 0x20000, face
+ * bits 0x100000<<k); cells with flag 0 are exterior.
+ */
+#ifndef HDD_B200_H
+#define HDD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    HDD_OK = 0,
+    HDD_ERR_INVALID_ARGUMENT = 1,
+    HDD_ERR_CUDA = 2,
+    HDD_ERR_OUT_OF_MEMORY = 3,
+    HDD_ERR_NOT_INITIALIZED = 4,
+    HDD_ERR_UNSUPPORTED = 5,     /* input outside what the GPU path implements */
+    HDD_ERR_NOT_CONVERGED = 6,   /* max_iters reached; the solution is still returned */
+    HDD_ERR_BREAKDOWN = 7,       /* non-finite scalars in PCG (e.g. NaN right-hand side) */
+    HDD_ERR_TIMEOUT = 8,         /* a bounded device wait ran out */
+    HDD_ERR_IO = 9,
+    HDD_ERR_BUSY = 10,
+    HDD_ERR_NOT_FOUND = 11,
+    HDD_ERR_INTERNAL = 12
+} hdd_status;
+
+/* Precision modes of the PCG outer loop (the preconditioner is FP32 in all). */
+enum {
+    HDD_PRECISION_REFERENCE = 0, /* FP32 vectors, FP64 dot accumulation, FP32 alpha/beta (as the reference) */
+    HDD_PRECISION_MIXED = 1      /* FP32 vectors, FP64 dots and alpha/beta, periodic FP64 true residual */
+};
+
+typedef struct {
+    int size[3];            /* reference -size (cells per axis + 1) */
+    int sub_size[3];        /* reference -sub_size */
+    int vlevels;            /* reference -vlevels */
+    int nVcycles;           /* reference -nVcycles */
+    int interior_smoothing; /* reference -interior_smoothing */
+    int boundary_smoothing; /* reference -boundary_smoothing */
+    int sigma_levels;       /* reference -sigma_levels */
+    int sigma_smoothing;    /* reference -sigma_smoothing */
+    int sigma_mg;           /* reference -sigma_mg */
+    double tol;             /* stop tolerance on max|r| */
+    int relative_tol;       /* 1: max|r| <= tol*max|b|; 0: max|r| <= tol (reference test) */
+    int max_iters;          /* reference passes 5000 */
+    int min_iters;
+    int precision_mode;     /* HDD_PRECISION_* */
+    int true_residual_every;/* mixed mode: recompute r = b - A x every N iterations (0 = never) */
+    int device;             /* CUDA device ordinal */
+} hdd_options;
+
+typedef struct {
+    int iterations;
+    int converged;
+    double final_norm;        /* max|r| of the recursively updated residual */
+    double b_inf;             /* max|b| over Active|Interface cells */
+    double true_residual_inf; /* max|b - A x| / max|b| of the returned x */
+    double true_residual_l2;  /* ||b - A x||_2 / ||b||_2 of the returned x */
+    double solve_ms;          /* device time of the PCG loop */
+    double setup_ms;          /* host+device time of hdd_initialize_preconditioner */
+} hdd_result;
+
+typedef struct hdd_solver hdd_solver;
+
+/* Defaults equal the reference Test_Bench defaults
+ * (demos/Domain_Decomposition_CPU_Only/Test_Bench_3D/main.cpp:236-251) with
+ * tol 1e-6 relative. */
+void hdd_options_default(hdd_options* opts);
+
+/* Replaces constructing SPGrid_Domain_Decomposition_Solver
+ * (demos/Domain_Decomposition_CPU_Only/SPGrid_Domain_Decomposition_Solver/
+ *  SPGrid_Domain_Decomposition_Solver.h:40). */
+hdd_status hdd_create(const hdd_options* opts, hdd_solver** out);
+
+/* Replaces Read_SPGrid / Convert (SPGrid_Domain_Decomposition_Solver.h:73-105):
+ * loads cell flags and the right-hand side b. */
+hdd_status hdd_set_domain_dense(hdd_solver* s, const uint32_t* flags, const float* rhs);
+
+/* Reads the reference's SPGrid directory format (size, block_offset, flags,
+ * data) written by SPGRID_READ_WRITE::Write_SPGrid
+ * (demos/SPGrid_Create_Simple_Domain/SPGRID_READ_WRITE.h:43-51). */
+hdd_status hdd_load_spgrid_dir(hdd_solver* s, const char* directory);
+
+/* Replaces Initialize_Preconditioner (SPGrid_Domain_Decomposition_Solver.h:121-161):
+ * flags, subdomains, V-cycle topology, interface matrices and factorisations. */
+hdd_status hdd_initialize_preconditioner(hdd_solver* s);
+
+/* Replaces the right-hand side only (same domain and preconditioner). */
+hdd_status hdd_set_rhs_dense(hdd_solver* s, const float* rhs);
+
+/* Replaces Solve (SPGrid_Domain_Decomposition_Solver.h:165-197). */
+hdd_status hdd_solve(hdd_solver* s, hdd_result* result);
+
+/* Copies the solution x of the last solve. */
+hdd_status hdd_get_solution_dense(hdd_solver* s, float* x);
+
+/* Test seam: z = Project(Apply_Preconditioner(r)), replacing
+ * SPGrid_Domain_Decomposition_Preconditioner::Apply_Preconditioner
+ * (SPGrid_Domain_Decomposition_Preconditioner.h:88-128) followed by
+ * CG_SYSTEM::Project. */
+hdd_status hdd_apply_preconditioner_dense(hdd_solver* s, const float* r, float* z);
+
+/* Test seam: nV V-cycles of V_Cycle_Helper::v_cycle
+ * (SPGrid_Library/SPGrid_V_Cycle_Helper.h:156-195) on the level-0 arrays u
+ * (in/out) and b, with the interface values of u held fixed. */
+hdd_status hdd_vcycle_dense(hdd_solver* s, float* u, const float* b, int n_vcycles);
+
+/* Test seam: y = Project(A x), replacing CG_SYSTEM::Multiply + Project
+ * (CG_SYSTEM.cpp:28-44,100-119). */
+hdd_status hdd_multiply_dense(hdd_solver* s, const float* x, float* y);
+
+/* Test seam: one sigma V-cycle (SIGMA_MULTIGRID_SOLVER.cpp:70-82) from u = 0
+ * on the level-0 interface right-hand side b0 (interface DOF order). */
+hdd_status hdd_sigma_vcycle(hdd_solver* s, const float* b0, float* u0);
+
+/* Interface DOF count at a sigma level and the level-0 DOF -> cell map
+ * (INTERFACE_MATRIX_GENERATOR::interface_map). */
+hdd_status hdd_interface_size(hdd_solver* s, int level, int* n);
+hdd_status hdd_interface_map(hdd_solver* s, int* cells_xyz);
+
+/* Assembled interface matrices for inspection (kind: 0 Arr, 1 Aii, 2 Air,
+ * 3 Prr).  Call first with ptr == NULL to get rows/cols/nnz. */
+hdd_status hdd_interface_matrix(hdd_solver* s, int kind, int level, int subdomain, int* rows,
+                                int* cols, int* nnz, int* ptr, int* col, double* val);
+
+/* Number of our CUDA kernel launches issued since the handle was created. */
+hdd_status hdd_kernel_launch_count(hdd_solver* s, long long* count);
+
+const char* hdd_status_string(hdd_status status);
+const char* hdd_last_error(const hdd_solver* s);
+void hdd_destroy(hdd_solver* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HDD_B200_H */
