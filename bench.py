@@ -1,0 +1,299 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 DD-PCG Poisson solver.
+
+One step = one Poisson solve (PCG to 1e-6 relative residual, preconditioner
+already initialised) of the workload's domain.  The default workload is the
+256^3-cell domain with a Dirichlet sphere and 32^3 subdomains (sub_size 32,
+vlevels 4, interior/boundary smoothing 4, sigma_levels 4, sigma_mg 1);
+``--config c1`` selects the 64^3-cell, 16^3-subdomain case.
+
+``--impl reference`` times the CPU restatement of the reference dd_pcg path
+(the oracle) on the host cores instead.
+
+The output is one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Poisson solves/sec @1e-6 rel. residual"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--config", choices=["c1", "c2", "c3"], default="c2")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--precision", choices=["reference", "mixed"], default="reference")
+    return p.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def workload(cfg):
+    from hierarchicaldd_b200 import domains
+    return {"c1": domains.config1, "c2": domains.config2, "c3": domains.config3}[cfg]()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(d, threads_note):
+    """Oracle (CPU restatement of the reference dd_pcg) on a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_ffi import Oracle
+    m = d.meta
+    t0 = time.time()
+    o = Oracle(d.size, d.sub_size, d.flags, vlevels=m["vlevels"], nVcycles=m["nVcycles"],
+               interior_smoothing=m["interior_smoothing"], boundary_smoothing=m["boundary_smoothing"],
+               sigma_levels=m["sigma_levels"], sigma_smoothing=m["sigma_smoothing"], sigma_mg=m["sigma_mg"])
+    setup_s = time.time() - t0
+    t0 = time.time()
+    _, it, info = o.solve(d.rhs, tol=1e-6, max_it=500)
+    dt = time.time() - t0
+    return {"value": 1.0 / dt, "unit": "solves/s", "cores": threads_note, "kind": "port",
+            "sample": f"one full solve of {d.name} ({it} PCG iterations, {dt:.2f} s; setup {setup_s:.1f} s untimed)"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    d = workload(args.config)
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_ffi import Oracle
+    m = d.meta
+    o = Oracle(d.size, d.sub_size, d.flags, vlevels=m["vlevels"], nVcycles=m["nVcycles"],
+               interior_smoothing=m["interior_smoothing"], boundary_smoothing=m["boundary_smoothing"],
+               sigma_levels=m["sigma_levels"], sigma_smoothing=m["sigma_smoothing"], sigma_mg=m["sigma_mg"])
+    for _ in range(args.warmup):
+        o.solve(d.rhs, tol=1e-6, max_it=500)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.time()
+        o.solve(d.rhs, tol=1e-6, max_it=500)
+        times.append(time.time() - t0)
+    tot = sum(times)
+    v = args.steps / tot
+    line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": 0, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": d.name, "size": list(d.size), "sub_size": list(d.sub_size)},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} full solves of {d.name} on the host cores"},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from hierarchicaldd_b200 import _lib
+    from hierarchicaldd_b200.solver import SPGrid_Domain_Decomposition_Solver
+
+    d = workload(args.config)
+    m = d.meta
+    s = SPGrid_Domain_Decomposition_Solver(device=local_rank)
+    s.Set_Domain(d.flags, d.rhs)
+    t0 = time.time()
+    s.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"],
+                                m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"],
+                                m["sigma_mg"], tol=1e-6,
+                                precision_mode=1 if args.precision == "mixed" else 0)
+    setup_s = time.time() - t0
+    print(f"[bench] {d.name}: setup {setup_s:.1f} s", file=sys.stderr, flush=True)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for i in range(args.warmup):
+        r0 = s.Solve()
+        print(f"[bench] warmup {i}: {r0['solve_ms']:.2f} ms, {r0['iterations']} iterations", file=sys.stderr, flush=True)
+    launches0 = s.Kernel_Launches()
+    barrier()
+    res = []
+    with ClockSampler(local_rank) as clk:
+        t_wall = time.time()
+        for _ in range(args.steps):
+            res.append(s.Solve())
+        barrier()
+        t_wall = time.time() - t_wall
+    launches = s.Kernel_Launches() - launches0
+    dev_ms = np.array([r["solve_ms"] for r in res])
+    total_ms = float(dev_ms.sum())
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps / (total_ms / 1000.0)
+
+    # End to end through the C ABI with pinned host buffers: H2D of b, solve, D2H of x.
+    cells = int(np.prod(d.size))
+    pin_b = torch.empty(cells, dtype=torch.float32, pin_memory=True)
+    pin_x = torch.empty(cells, dtype=torch.float32, pin_memory=True)
+    pin_b.numpy()[:] = d.rhs.ravel()
+    lib = _lib.load()
+    fp = lambda t: C.cast(t.data_ptr(), C.POINTER(C.c_float))
+    barrier()
+    t_e2e = time.time()
+    for _ in range(args.steps):
+        st = lib.hdd_set_rhs_dense(s.h, fp(pin_b))
+        assert st == 0, st
+        s.Solve()
+        st = lib.hdd_get_solution_dense(s.h, fp(pin_x))
+        assert st == 0, st
+    barrier()
+    t_e2e = time.time() - t_e2e
+    e2e_val = world * args.steps / t_e2e
+    if dist is not None:
+        t = torch.tensor([t_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_val = world * args.steps / float(t.item())
+
+    # Per-phase device timing (separate, instrumented solve).
+    ms = (C.c_double * 8)()
+    cnt = (C.c_longlong * 8)()
+    lib.hdd_set_kernel_timing(s.h, 1)
+    prof = s.Solve()
+    lib.hdd_get_kernel_timing(s.h, ms, cnt)
+    lib.hdd_set_kernel_timing(s.h, 0)
+    phases = ["vcycle", "laplace", "pcg_vector", "interface", "sigma_vcycle", "dense_tile_copy"]
+    phase_ms = {n: float(ms[i]) for i, n in enumerate(phases)}
+    phase_n = {n: int(cnt[i]) for i, n in enumerate(phases)}
+
+    # Roofline of the Laplacian kernel (HBM-bound): algorithmic bytes = 12 B per
+    # Active|Interface cell (read s and flags, write q).
+    from hierarchicaldd_b200.domains import ACTIVE
+    n_solve_cells = int(np.count_nonzero(d.flags & ACTIVE))  # Active before the divider = Active|Interface after
+    lap_ms = phase_ms["laplace"] / max(phase_n["laplace"], 1)
+    hbm, peak_kind = peaks()
+    achieved = 12.0 * n_solve_cells / (lap_ms * 1e-3) / 1e9 if lap_ms > 0 else None
+
+    its = [r["iterations"] for r in res]
+    lat = np.sort(dev_ms)
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": d.name, "size": list(d.size), "sub_size": list(d.sub_size),
+                   "vlevels": m["vlevels"], "interior_smoothing": m["interior_smoothing"],
+                   "boundary_smoothing": m["boundary_smoothing"], "sigma_levels": m["sigma_levels"],
+                   "sigma_smoothing": m["sigma_smoothing"], "sigma_mg": m["sigma_mg"],
+                   "tol": 1e-6, "precision": args.precision, "l2": "working set > L2 (no flush)",
+                   "parallelism": f"replicas{world}"},
+        "iterations": its[0] if its else None,
+        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+        "true_residual_inf": res[-1]["true_residual_inf"] if res else None,
+        "setup_s": setup_s,
+        "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": 4 * cells, "d2h_bytes_per_step": 4 * cells},
+        "gpu_launches": int(launches),
+        "phase_ms_per_solve": phase_ms, "phase_launches_per_solve": phase_n,
+        "roofline": {"kernel": "laplace_dot_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": (achieved / hbm) if achieved else None, "traffic": None,
+                     "peak_kind": peak_kind},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from hierarchicaldd_b200 import domains
+        try:
+            line["cpu_baseline"] = cpu_baseline(domains.config1(), os.cpu_count())
+        except Exception as e:  # reported, not fatal
+            line["cpu_baseline"] = {"error": str(e)}
+    s.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

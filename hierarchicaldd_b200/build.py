@@ -22,6 +22,7 @@ SOURCES = [
     "kernels_vcycle.cu",
     "kernels_pcg.cu",
     "sigma.cu",
+    "sn_solve.cu",
     "solver.cu",
 ]
 

@@ -231,6 +231,22 @@ hdd_status hdd_interface_matrix(hdd_solver* s, int kind, int level, int sub, int
     });
 }
 
+hdd_status hdd_set_kernel_timing(hdd_solver* s, int enable) {
+    return guard(s, [&](Solver& v) {
+        v.collect_timing();
+        v.timing = enable != 0;
+        for (int c = 0; c < Solver::kCats; ++c) { v.cat_ms[c] = 0; v.cat_n[c] = 0; }
+    });
+}
+
+hdd_status hdd_get_kernel_timing(hdd_solver* s, double* ms, long long* launches) {
+    if (!ms || !launches) return HDD_ERR_INVALID_ARGUMENT;
+    return guard(s, [&](Solver& v) {
+        v.collect_timing();
+        for (int c = 0; c < Solver::kCats; ++c) { ms[c] = v.cat_ms[c]; launches[c] = v.cat_n[c]; }
+    });
+}
+
 hdd_status hdd_kernel_launch_count(hdd_solver* s, long long* count) {
     if (!count) return HDD_ERR_INVALID_ARGUMENT;
     return guard(s, [&](Solver& v) { *count = v.launches; });

@@ -200,21 +200,45 @@ void SnFactor::factor(const CsrF& A, double eps) {
             upd[c].clear();
             upd[c].shrink_to_fit();
         }
-        // Dense Cholesky of the pivot block, then the off-diagonal block.
-        for (int k = 0; k < nj; ++k) {
-            double d = F[(size_t)k * f + k];
-            if (!(d > 0)) throw Error(HDD_ERR_INTERNAL, "interface matrix is not positive definite");
-            d = std::sqrt(d);
-            F[(size_t)k * f + k] = d;
-            for (int i = k + 1; i < f; ++i) F[(size_t)k * f + i] /= d;
-            // Right-looking update of the trailing columns.
-#pragma omp parallel for schedule(static) if (f - k > 256)
-            for (int c = k + 1; c < f; ++c) {
-                const double lck = F[(size_t)k * f + c];
-                if (lck == 0.0) continue;
+        // Dense partial Cholesky of the front (first nj columns), blocked in
+        // panels of kPanel columns: factor the panel, then update the trailing
+        // columns with row-major copies of the panel so every update is a
+        // contiguous dot product.
+        constexpr int kPanel = 48;
+        std::vector<double> Pn;
+        for (int k0 = 0; k0 < nj; k0 += kPanel) {
+            const int kb = std::min(kPanel, nj - k0);
+            for (int k = k0; k < k0 + kb; ++k) {
+                double d = F[(size_t)k * f + k];
+                if (!(d > 0)) throw Error(HDD_ERR_INTERNAL, "interface matrix is not positive definite");
+                d = std::sqrt(d);
+                F[(size_t)k * f + k] = d;
+                for (int i = k + 1; i < f; ++i) F[(size_t)k * f + i] /= d;
+                for (int c = k + 1; c < k0 + kb; ++c) {
+                    const double lck = F[(size_t)k * f + c];
+                    if (lck == 0.0) continue;
+                    double* colc = &F[(size_t)c * f];
+                    const double* colk = &F[(size_t)k * f];
+                    for (int i = c; i < f; ++i) colc[i] -= colk[i] * lck;
+                }
+            }
+            const int t0 = k0 + kb;
+            if (t0 >= f) continue;
+            Pn.assign((size_t)(f - t0) * kb, 0.0);
+            for (int kk = 0; kk < kb; ++kk) {
+                const double* colk = &F[(size_t)(k0 + kk) * f];
+                for (int i = t0; i < f; ++i) Pn[(size_t)(i - t0) * kb + kk] = colk[i];
+            }
+#pragma omp parallel for schedule(dynamic, 8) if ((size_t)(f - t0) * (f - t0) * kb > 4000000)
+            for (int c = t0; c < f; ++c) {
+                const double* lc = &Pn[(size_t)(c - t0) * kb];
                 double* colc = &F[(size_t)c * f];
-                const double* colk = &F[(size_t)k * f];
-                for (int i = c; i < f; ++i) colc[i] -= colk[i] * lck;
+                for (int i = c; i < f; ++i) {
+                    const double* li = &Pn[(size_t)(i - t0) * kb];
+                    double acc = 0.0;
+                    for (int kk = 0; kk < kb; ++kk) acc += li[kk] * lc[kk];
+                    colc[i] -= acc;
+                }
             }
         }
         Ljj[j].assign((size_t)nj * nj, 0.0);
@@ -231,6 +255,48 @@ void SnFactor::factor(const CsrF& A, double eps) {
         for (int a = 0; a < nj; ++a) pos[col0[j] + a] = -1;
         for (int k = 0; k < nr; ++k) pos[rows[j][k]] = -1;
     }
+}
+
+void SnFactor::build_solve_blocks() {
+    // Per front: Fw = [Linv; -W] ((nj+nr) x nj, col-major) with Linv = L_JJ^{-1}
+    // (lower triangular) and W = L_RJ Linv, so that the forward substitution of a
+    // front is one product [y_J; v_J] = Fw f_J (+ f_R on the update rows) and the
+    // backward substitution is x_J = Fw^T [y_J; x_R].  Column c of Fw needs only
+    // column c of L^{-1}, so columns are computed independently.
+    const int ns = (int)col0.size();
+    Fw.assign(ns, {});
+    auto work = [&](int j, bool inner_par) {
+        const int nj = ncol[j], nr = (int)rows[j].size(), m = nj + nr;
+        std::vector<double>& F = Fw[j];
+        F.assign((size_t)m * nj, 0.0);
+        const std::vector<double>& L = Ljj[j];
+        const std::vector<double>& R = Lrj[j];
+#pragma omp parallel for schedule(dynamic, 4) if (inner_par)
+        for (int c = 0; c < nj; ++c) {
+            double* x = &F[(size_t)c * m];
+            x[c] = 1.0;
+            for (int jj = c; jj < nj; ++jj) {
+                const double* Lc = &L[(size_t)jj * nj];
+                const double xj = x[jj] / Lc[jj];
+                x[jj] = xj;
+                if (xj == 0.0) continue;
+                for (int i = jj + 1; i < nj; ++i) x[i] -= Lc[i] * xj;
+            }
+            double* w = x + nj;
+            for (int a = c; a < nj; ++a) {
+                const double la = x[a];
+                if (la == 0.0) continue;
+                const double* Ra = &R[(size_t)a * nr];
+                for (int k = 0; k < nr; ++k) w[k] -= Ra[k] * la;
+            }
+        }
+    };
+    std::vector<int> small;
+    for (int j = 0; j < ns; ++j)
+        if (ncol[j] >= 128) work(j, true);
+        else small.push_back(j);
+#pragma omp parallel for schedule(dynamic)
+    for (long t = 0; t < (long)small.size(); ++t) work(small[t], false);
 }
 
 void SnFactor::solve(double* x) const {
@@ -257,50 +323,6 @@ void SnFactor::solve(double* x) const {
         }
     }
     for (int i = 0; i < n; ++i) x[perm[i]] = y[i];
-}
-
-void dense_spd_inverse(std::vector<double>& a, int n) {
-    // Cholesky A = L L^T (row-major, lower), then A^{-1} = L^{-T} L^{-1}.
-    for (int k = 0; k < n; ++k) {
-        double d = a[(size_t)k * n + k];
-        for (int p = 0; p < k; ++p) d -= a[(size_t)k * n + p] * a[(size_t)k * n + p];
-        if (!(d > 0)) throw Error(HDD_ERR_INTERNAL, "coarse Schur complement is not positive definite");
-        d = std::sqrt(d);
-        a[(size_t)k * n + k] = d;
-#pragma omp parallel for schedule(static) if (n - k > 128)
-        for (int i = k + 1; i < n; ++i) {
-            double s = a[(size_t)i * n + k];
-            const double* ri = &a[(size_t)i * n];
-            const double* rk = &a[(size_t)k * n];
-            for (int p = 0; p < k; ++p) s -= ri[p] * rk[p];
-            a[(size_t)i * n + k] = s / d;
-        }
-    }
-    // Wt = (L^{-1})^T: row c of Wt is column c of L^{-1}, so both loops below
-    // read contiguous rows.
-    std::vector<double> Wt((size_t)n * n, 0.0);
-#pragma omp parallel for schedule(dynamic, 16)
-    for (int c = 0; c < n; ++c) {
-        double* w = &Wt[(size_t)c * n];
-        w[c] = 1.0 / a[(size_t)c * n + c];
-        for (int i = c + 1; i < n; ++i) {
-            const double* ri = &a[(size_t)i * n];
-            double s = 0;
-            for (int p = c; p < i; ++p) s -= ri[p] * w[p];
-            w[i] = s / ri[i];
-        }
-    }
-    // A^{-1}[i][j] = sum_{p >= max(i,j)} Wt[i][p] Wt[j][p].
-#pragma omp parallel for schedule(dynamic, 16)
-    for (int i = 0; i < n; ++i)
-        for (int j = 0; j <= i; ++j) {
-            const double* wi = &Wt[(size_t)i * n];
-            const double* wj = &Wt[(size_t)j * n];
-            double s = 0;
-            for (int p = i; p < n; ++p) s += wi[p] * wj[p];
-            a[(size_t)i * n + j] = s;
-            a[(size_t)j * n + i] = s;
-        }
 }
 
 }  // namespace hdd

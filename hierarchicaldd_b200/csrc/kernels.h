@@ -23,6 +23,7 @@ struct VcycleArgs {
     int n_vcycles, interior_itr, boundary_itr, bottom_itr;
     int halo_from_u;           // 1: halo planes hold interface values read from u
     int zero_init;             // 1: interior u starts at zero
+    int cluster;               // CTAs per subdomain for sub 16 (1 or 2); sub 32 always uses 4
     float inv_diag[8];         // omega / face_count (float division on the host)
     float restrict_w[64];      // (1/8,3/8,3/8,1/8)^3 tensor weights
     float prolong_w[8];        // 4 * (3/4,1/4)^3 tensor weights
@@ -76,6 +77,12 @@ cudaError_t launch_residual(const TileGeom& g, const float* b, const float* x, f
                             cudaStream_t stream);
 // v = Project(v).
 cudaError_t launch_project(const TileGeom& g, float* v, cudaStream_t stream);
+// Dense (x-slowest grid of size[0..2]) <-> tiled copies on the device;
+// tile_xyz holds the tile coordinates of every stored tile.
+cudaError_t launch_dense_to_tiles(const TileGeom& g, const int* tile_xyz, int sx, int sy, int sz, const float* dense,
+                                  float* tiled, cudaStream_t stream);
+cudaError_t launch_tiles_to_dense(const TileGeom& g, const int* tile_xyz, int sx, int sy, int sz, const float* tiled,
+                                  float* dense, cudaStream_t stream);
 
 // ---------------------------------------------------------------------------
 // Interface coupling (Laplace_ri gather and the interface scatter)

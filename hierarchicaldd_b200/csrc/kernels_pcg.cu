@@ -237,7 +237,35 @@ __global__ void __launch_bounds__(kNT) interface_scatter_kernel(const long long*
     if (i < n) z[slot[i]] = u0[i];
 }
 
+__global__ void __launch_bounds__(kNT) dense_tiles_kernel(int S, const int* tile_xyz, int sx, int sy, int sz,
+                                                          const float* __restrict__ src, float* __restrict__ dst,
+                                                          int to_tiles) {
+    const int t = blockIdx.x, TC = S * S * S;
+    const int ox = tile_xyz[3 * t] * S, oy = tile_xyz[3 * t + 1] * S, oz = tile_xyz[3 * t + 2] * S;
+    for (int c = threadIdx.x; c < TC; c += kNT) {
+        const int z = c % S, tmp = c / S, y = tmp % S, x = tmp / S;
+        const int gx = ox + x, gy = oy + y, gz = oz + z;
+        const bool in = gx < sx && gy < sy && gz < sz;
+        const size_t di = ((size_t)gx * sy + gy) * sz + gz, ti = (size_t)t * TC + c;
+        if (to_tiles) dst[ti] = in ? src[di] : 0.0f;
+        else if (in) dst[di] = src[ti];
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_dense_to_tiles(const TileGeom& g, const int* txyz, int sx, int sy, int sz, const float* dense,
+                                  float* tiled, cudaStream_t st) {
+    if (g.ntiles == 0) return cudaSuccess;
+    dense_tiles_kernel<<<g.ntiles, kNT, 0, st>>>(g.sub, txyz, sx, sy, sz, dense, tiled, 1);
+    return cudaGetLastError();
+}
+cudaError_t launch_tiles_to_dense(const TileGeom& g, const int* txyz, int sx, int sy, int sz, const float* tiled,
+                                  float* dense, cudaStream_t st) {
+    if (g.ntiles == 0) return cudaSuccess;
+    dense_tiles_kernel<<<g.ntiles, kNT, 0, st>>>(g.sub, txyz, sx, sy, sz, tiled, dense, 0);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_laplace_dot(const TileGeom& g, const float* s, float* q, double* partial, cudaStream_t st) {
     if (g.ntiles == 0) return cudaSuccess;

@@ -15,6 +15,7 @@
 //                                                 SPGrid_Prolongation_Legacy.h:46-128)
 // Smoothing is Jacobi: every residual of a sweep is computed from the old u
 // (held in registers) before any update.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -23,6 +24,8 @@
 #include "kernels.h"
 
 namespace hdd {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -279,6 +282,354 @@ size_t vcycle_smem_bytes(int levels) {
     return total;
 }
 
+// ---------------------------------------------------------------------------
+// Cluster variant: one subdomain per thread-block cluster of C CTAs.
+//
+// Level 0 is cut into C slabs along x; CTA `rank` owns interior planes
+// x0..x1 and keeps one halo plane on each side.  After every Jacobi update a
+// CTA stores its first/last owned planes straight into its neighbours'
+// shared memory (distributed shared memory), double-buffered by sweep parity,
+// and one cluster barrier per sweep orders the exchange.  The coarse levels
+// are small and live in rank 0; the restriction into rank 0 and the
+// prolongation out of it are spread over all ranks through DSMEM.  Every CTA
+// executes the same sequence of cluster barriers.
+// ---------------------------------------------------------------------------
+template <int SUB, int C>
+struct SlabGeom {
+    static constexpr int E = SUB + 1;
+    static constexpr int PS = E * E;
+    static constexpr int P = (SUB - 1 + C - 1) / C;
+    static constexpr int M2 = (SUB - 1) * (SUB - 1);
+};
+
+template <int SUB, int C>
+size_t vcycle_cluster_smem_bytes(int levels) {
+    using G = SlabGeom<SUB, C>;
+    size_t floats = (size_t)(G::P + 2) * G::PS + 2 * (size_t)G::P * G::PS + 4 * (size_t)G::PS;
+    size_t total = floats * 4 + (((size_t)G::P * G::PS + 15) & ~size_t(15));
+    for (int l = 1; l < levels; ++l) {
+        const int e = (SUB >> l) + 1;
+        const size_t n4 = ((size_t)e * e * e + 3) & ~size_t(3);
+        total += n4 * 13;
+    }
+    return total;
+}
+
+template <int SUB, int C, int NT>
+__global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
+    using G = SlabGeom<SUB, C>;
+    constexpr int E = G::E, PS = G::PS, P = G::P, M2 = G::M2;
+    constexpr int CH = (P * M2 + NT - 1) / NT;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ float s_inv[8];
+    __shared__ float s_sc64[64];
+    __shared__ float s_sc8[8];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const int box = blockIdx.x / C;
+    if (box >= a.nbox) return;  // uniform across the cluster
+    if (threadIdx.x < 8) s_inv[threadIdx.x] = a.inv_diag[threadIdx.x];
+    if (threadIdx.x < 64) s_sc64[threadIdx.x] = a.restrict_w[threadIdx.x];
+    if (threadIdx.x < 8) s_sc8[threadIdx.x] = a.prolong_w[threadIdx.x];
+
+    const int x0 = 1 + rank * P;
+    const int x1 = min(x0 + P - 1, SUB - 1);
+    const int np = x1 - x0 + 1;
+    const int ncell = np * M2;
+
+    float* u0 = reinterpret_cast<float*>(smem);            // (P+2) planes, plane lx <-> x = x0-1+lx
+    float* b0 = u0 + (P + 2) * PS;                          // P planes, plane k <-> x = x0+k
+    float* r0 = b0 + P * PS;
+    float* nxt = r0 + P * PS;                               // [parity][side][PS], side 0 = low halo
+    uint8_t* f0 = reinterpret_cast<uint8_t*>(nxt + 4 * PS);
+    LevelSmem lv[kMaxLevels];
+    {
+        unsigned char* p = reinterpret_cast<unsigned char*>(f0) + (((size_t)P * PS + 15) & ~size_t(15));
+        for (int l = 1; l < a.levels; ++l) {
+            const int e = (SUB >> l) + 1;
+            const int n4 = (e * e * e + 3) & ~3;
+            lv[l].e = e;
+            lv[l].u = reinterpret_cast<float*>(p); p += n4 * 4;
+            lv[l].b = reinterpret_cast<float*>(p); p += n4 * 4;
+            lv[l].r = reinterpret_cast<float*>(p); p += n4 * 4;
+            lv[l].f = p; p += n4;
+        }
+    }
+    const uint8_t* rec = a.box_flags + (size_t)box * a.box_stride;
+    const int tile = a.box_tile[box];
+    constexpr int TC = SUB * SUB * SUB;
+    const float* gu = a.u + (size_t)tile * TC;
+    const float* gb = a.b + (size_t)tile * TC;
+
+    // Load level 0: halo planes / rows from u (interface values) or zero.
+    auto load_u = [&](int x, int y, int z) -> float {
+        const bool halo = (x == 0) || (y == 0) || (z == 0) || (x == SUB) || (y == SUB) || (z == SUB);
+        if (halo && !a.halo_from_u) return 0.0f;
+        if (!halo && a.zero_init) return 0.0f;
+        const int hi = (x == SUB) + (y == SUB) + (z == SUB);
+        if (hi == 0) return gu[(x * SUB + y) * SUB + z];
+        if (hi > 1) return 0.0f;  // edge cells are never read by the stencil
+        const int axis = (x == SUB) ? 0 : ((y == SUB) ? 1 : 2);
+        const int nt = a.box_nb[3 * box + axis];
+        if (nt < 0) return 0.0f;
+        const int lx = (axis == 0) ? 0 : x, ly = (axis == 1) ? 0 : y, lz = (axis == 2) ? 0 : z;
+        return a.u[(size_t)nt * TC + (lx * SUB + ly) * SUB + lz];
+    };
+    for (int q = threadIdx.x; q < (np + 2) * PS; q += NT) {
+        const int lx = q / PS, rem = q % PS, y = rem / E, z = rem % E;
+        u0[q] = load_u(x0 - 1 + lx, y, z);
+    }
+    for (int q = threadIdx.x; q < P * PS; q += NT) {
+        const int k = q / PS, rem = q % PS, y = rem / E, z = rem % E;
+        const int x = x0 + k;
+        float bv = 0.0f;
+        uint8_t fv = 0;
+        if (k < np && y >= 1 && y < SUB && z >= 1 && z < SUB) {
+            bv = gb[(x * SUB + y) * SUB + z];
+            fv = rec[box_index(E, x, y, z)];
+        }
+        b0[q] = bv;
+        r0[q] = 0.0f;
+        f0[q] = fv;
+    }
+    if (rank == 0) {
+        for (int l = 1; l < a.levels; ++l) {
+            const int e = lv[l].e, n = e * e * e;
+            for (int i = threadIdx.x; i < n; i += NT) {
+                lv[l].u[i] = 0.0f; lv[l].b[i] = 0.0f; lv[l].r[i] = 0.0f;
+                lv[l].f[i] = rec[a.level_off[l] + i];
+            }
+        }
+    }
+    __syncthreads();
+    cluster.sync();  // every CTA's shared memory is initialised before remote access
+
+    float* nb_lo = (rank > 0) ? cluster.map_shared_rank(nxt, rank - 1) : nullptr;   // left neighbour's buffers
+    float* nb_hi = (rank < C - 1) ? cluster.map_shared_rank(nxt, rank + 1) : nullptr;
+    int par = 0;
+
+    auto cell_of = [&](int q, int& i, int& j, int& lx, int& y, int& z) {
+        lx = q / M2 + 1;
+        const int rem = q % M2;
+        y = rem / (SUB - 1) + 1;
+        z = rem % (SUB - 1) + 1;
+        i = (lx * E + y) * E + z;
+        j = i - PS;
+    };
+    // Store owned boundary planes into the neighbours' next-halo buffers, then
+    // barrier, then adopt the buffers written into this CTA.
+    auto finish_exchange = [&]() {
+        cluster.sync();
+        float* my_lo = nxt + (par * 2 + 0) * PS;
+        float* my_hi = nxt + (par * 2 + 1) * PS;
+        for (int q = threadIdx.x; q < M2; q += NT) {
+            const int y = q / (SUB - 1) + 1, z = q % (SUB - 1) + 1, o = y * E + z;
+            if (rank > 0) u0[o] = my_lo[o];
+            if (rank < C - 1) u0[(np + 1) * PS + o] = my_hi[o];
+        }
+        par ^= 1;
+        __syncthreads();
+    };
+    auto push_boundary = [&](int lx, int o, float v) {
+        // The low neighbour's high halo is this CTA's first plane, and vice versa.
+        if (lx == 1 && rank > 0) nb_lo[(par * 2 + 1) * PS + o] = v;
+        if (lx == np && rank < C - 1) nb_hi[(par * 2 + 0) * PS + o] = v;
+    };
+    auto slab_sweep = [&](int mode) {
+        static_assert(CH <= 32, "take mask holds 32 cells per thread");
+        float rr[CH];
+        uint32_t tk = 0;
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int q = threadIdx.x + c * NT;
+            rr[c] = 0.0f;
+            if (q < ncell) {
+                int i, j, lx, y, z;
+                cell_of(q, i, j, lx, y, z);
+                const uint32_t fl = f0[j];
+                const bool act = fl & C_ACTIVE, bnd = fl & C_BOUNDARY8;
+                const bool take = act && ((mode == 3) || (mode == 1 && bnd) || (mode == 2 && !bnd));
+                if (take) {
+                    tk |= 1u << c;
+                    const float cc = u0[i];
+                    float res = 0.0f, n;
+                    n = u0[i - PS]; if (fl & 0x01u) res = __fsub_rn(res, __fsub_rn(n, cc));
+                    n = u0[i + PS]; if (fl & 0x02u) res = __fsub_rn(res, __fsub_rn(n, cc));
+                    n = u0[i - E];  if (fl & 0x04u) res = __fsub_rn(res, __fsub_rn(n, cc));
+                    n = u0[i + E];  if (fl & 0x08u) res = __fsub_rn(res, __fsub_rn(n, cc));
+                    n = u0[i - 1];  if (fl & 0x10u) res = __fsub_rn(res, __fsub_rn(n, cc));
+                    n = u0[i + 1];  if (fl & 0x20u) res = __fsub_rn(res, __fsub_rn(n, cc));
+                    rr[c] = __fsub_rn(b0[j], res);
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int q = threadIdx.x + c * NT;
+            if (q < ncell) {
+                int i, j, lx, y, z;
+                cell_of(q, i, j, lx, y, z);
+                float v = u0[i];
+                if (tk & (1u << c)) {
+                    v = __fadd_rn(v, __fmul_rn(s_inv[__popc((uint32_t)f0[j] & C_FACES)], rr[c]));
+                    u0[i] = v;
+                }
+                push_boundary(lx, y * E + z, v);
+            }
+        }
+        finish_exchange();
+    };
+
+    const int Lm = a.levels;
+    for (int cycle = 0; cycle < a.n_vcycles; ++cycle) {
+        if (Lm == 1) {
+            for (int i = 0; i < a.bottom_itr; ++i) slab_sweep(3);
+            continue;
+        }
+        for (int i = 0; i < a.boundary_itr; ++i) slab_sweep(1);
+        for (int i = 0; i < a.interior_itr; ++i) slab_sweep(2);
+        for (int i = 0; i < a.boundary_itr; ++i) slab_sweep(1);
+        // r = b - A u on owned Active cells (halos are current after the last exchange).
+        for (int q = threadIdx.x; q < ncell; q += NT) {
+            int i, j, lx, y, z;
+            cell_of(q, i, j, lx, y, z);
+            const uint32_t fl = f0[j];
+            if (!(fl & C_ACTIVE)) continue;
+            const float cc = u0[i];
+            float res = 0.0f, n;
+            n = u0[i - PS]; if (fl & 0x01u) res = __fsub_rn(res, __fsub_rn(n, cc));
+            n = u0[i + PS]; if (fl & 0x02u) res = __fsub_rn(res, __fsub_rn(n, cc));
+            n = u0[i - E];  if (fl & 0x04u) res = __fsub_rn(res, __fsub_rn(n, cc));
+            n = u0[i + E];  if (fl & 0x08u) res = __fsub_rn(res, __fsub_rn(n, cc));
+            n = u0[i - 1];  if (fl & 0x10u) res = __fsub_rn(res, __fsub_rn(n, cc));
+            n = u0[i + 1];  if (fl & 0x20u) res = __fsub_rn(res, __fsub_rn(n, cc));
+            r0[j] = __fsub_rn(b0[j], res);
+        }
+        __syncthreads();
+        cluster.sync();  // r0 of every slab is complete
+        // Restriction into rank 0's level-1 b, coarse cells interleaved over ranks.
+        {
+            constexpr int E1 = SUB / 2 + 1, m1 = SUB / 2 - 1;
+            float* b1 = cluster.map_shared_rank(lv[1].b, 0);
+            float* r0r[C];
+#pragma unroll
+            for (int k = 0; k < C; ++k) r0r[k] = cluster.map_shared_rank(r0, k);
+            const uint8_t* f1 = rec + a.level_off[1];
+            for (int q = threadIdx.x + rank * NT; q < m1 * m1 * m1; q += NT * C) {
+                const int cz = q % m1 + 1, t = q / m1, cy = t % m1 + 1, cx = t / m1 + 1;
+                const int ci = box_index(E1, cx, cy, cz);
+                if (!(f1[ci] & C_ACTIVE)) continue;
+                float acc = 0.0f;
+#pragma unroll
+                for (int i2 = 0; i2 < 4; ++i2) {
+                    const int x = 2 * cx - 2 + i2;
+                    const int owner = (x - 1) / P;           // x >= 1 when owner is used
+                    const float* rp = (x == 0) ? nullptr : r0r[owner] + (x - 1 - owner * P) * PS;
+#pragma unroll
+                    for (int j2 = 0; j2 < 4; ++j2)
+#pragma unroll
+                        for (int k2 = 0; k2 < 4; ++k2) {
+                            const float v = rp ? rp[(2 * cy - 2 + j2) * E + (2 * cz - 2 + k2)] : 0.0f;
+                            acc = __fadd_rn(acc, __fmul_rn(s_sc64[(i2 * 4 + j2) * 4 + k2], v));
+                        }
+                }
+                b1[ci] = acc;
+            }
+        }
+        cluster.sync();  // level-1 b complete in rank 0
+        if (rank == 0) {
+            {
+                const int e = lv[1].e, n = e * e * e;
+                for (int i = threadIdx.x; i < n; i += NT) lv[1].u[i] = 0.0f;
+            }
+            __syncthreads();
+            for (int l = 1; l < Lm - 1; ++l) {
+                for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(lv[l], 1, s_inv);
+                for (int i = 0; i < a.interior_itr; ++i) jacobi_sweep<CH>(lv[l], 2, s_inv);
+                for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(lv[l], 1, s_inv);
+                residual_store(lv[l]);
+                {
+                    const int e = lv[l + 1].e, n = e * e * e;
+                    for (int i = threadIdx.x; i < n; i += NT) lv[l + 1].u[i] = 0.0f;
+                }
+                __syncthreads();
+                restrict_level(lv[l], lv[l + 1], s_sc64);
+            }
+            for (int i = 0; i < a.bottom_itr; ++i) jacobi_sweep<CH>(lv[Lm - 1], 3, s_inv);
+            for (int l = Lm - 2; l >= 1; --l) {
+                prolongate_level(lv[l], lv[l + 1], s_sc8);
+                for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(lv[l], 1, s_inv);
+                for (int i = 0; i < a.interior_itr; ++i) jacobi_sweep<CH>(lv[l], 2, s_inv);
+                for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(lv[l], 1, s_inv);
+            }
+        }
+        cluster.sync();  // level-1 u final
+        // Prolongation of rank 0's level-1 u into every slab.
+        {
+            constexpr int E1 = SUB / 2 + 1;
+            const float* u1 = cluster.map_shared_rank(lv[1].u, 0);
+            for (int q = threadIdx.x; q < ncell; q += NT) {
+                int i, j, lx, y, z;
+                cell_of(q, i, j, lx, y, z);
+                float v = u0[i];
+                if (f0[j] & C_ACTIVE) {
+                    const int x = x0 - 1 + lx;
+                    const int cx = (x + 1) >> 1, cy = (y + 1) >> 1, cz = (z + 1) >> 1;
+                    const int px = 1 - (x - (2 * cx - 1)), py = 1 - (y - (2 * cy - 1)), pz = 1 - (z - (2 * cz - 1));
+                    const int cbase = box_index(E1, cx, cy, cz);
+#pragma unroll
+                    for (int aa = 0; aa < 2; ++aa)
+#pragma unroll
+                        for (int bq = 0; bq < 2; ++bq)
+#pragma unroll
+                            for (int cq = 0; cq < 2; ++cq) {
+                                const float w = s_sc8[((aa ^ px) * 2 + (bq ^ py)) * 2 + (cq ^ pz)];
+                                const float cu = u1[cbase + (aa - px) * E1 * E1 + (bq - py) * E1 + (cq - pz)];
+                                v = __fadd_rn(v, __fmul_rn(w, cu));
+                            }
+                    u0[i] = v;
+                }
+                push_boundary(lx, y * E + z, v);
+            }
+            finish_exchange();
+        }
+        for (int i = 0; i < a.boundary_itr; ++i) slab_sweep(1);
+        for (int i = 0; i < a.interior_itr; ++i) slab_sweep(2);
+        for (int i = 0; i < a.boundary_itr; ++i) slab_sweep(1);
+    }
+
+    float* gw = a.u + (size_t)tile * TC;
+    for (int q = threadIdx.x; q < ncell; q += NT) {
+        int i, j, lx, y, z;
+        cell_of(q, i, j, lx, y, z);
+        const int x = x0 - 1 + lx;
+        gw[(x * SUB + y) * SUB + z] = u0[i];
+    }
+    cluster.sync();  // no CTA leaves while a peer may still address its shared memory
+}
+
+template <int SUB, int C, int NT>
+cudaError_t launch_cluster(const VcycleArgs& a, cudaStream_t stream) {
+    const size_t smem = vcycle_cluster_smem_bytes<SUB, C>(a.levels);
+    auto kern = vcycle_cluster_kernel<SUB, C, NT>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(a.nbox * C), 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, a);
+}
+
 }  // namespace
 
 cudaError_t launch_vcycle(const VcycleArgs& a, cudaStream_t stream) {
@@ -292,6 +643,7 @@ cudaError_t launch_vcycle(const VcycleArgs& a, cudaStream_t stream) {
             return cudaGetLastError();
         }
         case 16: {
+            if (a.cluster == 2) return launch_cluster<16, 2, 256>(a, stream);
             constexpr int NT = 512;
             const size_t smem = vcycle_smem_bytes<16>(a.levels);
             cudaError_t e = cudaFuncSetAttribute(vcycle_kernel<16, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -299,6 +651,8 @@ cudaError_t launch_vcycle(const VcycleArgs& a, cudaStream_t stream) {
             vcycle_kernel<16, NT><<<a.nbox, NT, smem, stream>>>(a);
             return cudaGetLastError();
         }
+        case 32:
+            return launch_cluster<32, 4, 512>(a, stream);
         default:
             return cudaErrorNotSupported;
     }

@@ -44,38 +44,47 @@ struct SnFactor {
     std::vector<int> col0, ncol, parent;       // per supernode, post-order
     std::vector<std::vector<int>> rows;        // below-diagonal rows (new indices), sorted
     std::vector<std::vector<double>> Ljj, Lrj; // col-major dense blocks
+    std::vector<std::vector<double>> Fw;       // [Linv; -L_RJ Linv], (nj+nr) x nj col-major
     void analyze(const CsrF& A);
     void factor(const CsrF& A, double eps);
+    void build_solve_blocks();
     void solve(double* x) const;               // host reference solve (tests)
 };
 
-// Dense inverse of an SPD matrix (row-major, in place, double).
-void dense_spd_inverse(std::vector<double>& a, int n);
+// One unit of device work of a supernodal solve: rows [rb, re) of one front,
+// streamed as a contiguous block of ncols columns x kTaskRows rows.
+struct SnTask {
+    int front, rb, re, kind;  // kind 0: forward L^{-1} rows, 1: forward update rows, 2: backward
+    int col_base, ncols, pad0, pad1;
+    long long blk;            // float offset of the task's block
+};
 
-// Device plan for a batch of independent supernodal triangular solves.
+// Device plan for a batch of independent supernodal triangular solves
+// (sn_solve.cu).
 struct SolvePlan {
     int n = 0;                       // total unknowns (concatenated)
     int nsn = 0;
     int max_front = 0;
-    std::vector<int> height_ptr, height_nodes;   // forward schedule (leaves first)
-    std::vector<int> depth_ptr, depth_nodes;     // backward schedule (roots first)
-    // device arrays
+    std::vector<int> fwd_ptr, bwd_ptr;           // task ranges per tree level
     int *d_col0 = nullptr, *d_ncol = nullptr, *d_nrow = nullptr;
-    long long *d_linv = nullptr, *d_lrj = nullptr; // offsets into d_val (Linv, LinvT, Lrj, LrjT)
     int *d_rows = nullptr; long long *d_rows_off = nullptr;
     int *d_child_ptr = nullptr, *d_child = nullptr;
     long long* d_relmap_off = nullptr; int* d_relmap = nullptr;
     long long* d_upd_off = nullptr;
     int* d_perm = nullptr;           // new -> old (concatenated)
-    int *d_height_nodes = nullptr, *d_depth_nodes = nullptr;
-    float* d_val = nullptr;
+    SnTask *d_fwd = nullptr, *d_bwd = nullptr;
+    float* d_val = nullptr;          // task blocks
     float* d_upd = nullptr;          // update vectors
     float* d_ynew = nullptr;         // forward result in new order
+    float* d_xnew = nullptr;         // backward result in new order
+    int* d_err = nullptr;            // set when a bounded wait gives up
     size_t bytes = 0;
     void build(const std::vector<const SnFactor*>& factors, const std::vector<int>& offsets, cudaStream_t s);
     void release();
     // x_old = (A+eps I)^{-1} b_old (both in the concatenated original order).
     void solve(const float* b_old, float* x_old, cudaStream_t s, long long& launches) const;
+    int error_flag(cudaStream_t s) const;
+    ~SolvePlan() { release(); }
 };
 
 struct DeviceCsr {
@@ -100,14 +109,20 @@ struct SigmaLevel {
 struct SigmaGpu {
     int M = 0, smoothing = 3;
     std::vector<SigmaLevel> lv;
-    float* bottom_inv = nullptr;     // dense S^{-1} of the coarsest level (row-major)
-    int n_bottom = 0;
+    // Coarsest level: sparse Cholesky of K = [Aii+eps, -Air; -Air^T, Arr+eps]
+    // (all subdomain interiors first, then the interface), whose interface block
+    // solves the Schur complement S exactly.
+    SolvePlan bottom;
+    float *kb = nullptr, *kx = nullptr;
+    int n_bottom = 0, n_bottom_int = 0;
     double bottom_contraction = 0;   // estimated spectral radius of the bottom smoother
     size_t device_bytes = 0;
     void setup(const InterfaceHost& ih, int smoothing_iterations, cudaStream_t s);
     void release();
     // u[0] = sigma V-cycle(b[0]) (SIGMA_MULTIGRID_SOLVER.cpp:70-82), u[0] starting at 0.
     void vcycle(cudaStream_t s, long long& launches);
+    // Nonzero when a bounded wait inside a supernodal solve gave up.
+    int error_flag(cudaStream_t s) const;
     float* b0() const { return lv.empty() ? nullptr : lv[0].b; }
     float* u0() const { return lv.empty() ? nullptr : lv[0].u; }
     ~SigmaGpu() { release(); }

@@ -15,6 +15,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "solver.h"
@@ -58,6 +60,20 @@ Solver::~Solver() {
     }
 }
 
+void Solver::collect_timing() {
+    if (pending.empty()) return;
+    cuda_check(cudaStreamSynchronize(stream), "timing sync");
+    for (auto& p : pending) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p.a, p.b);
+        cat_ms[p.cat] += ms;
+        cat_n[p.cat] += 1;
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    pending.clear();
+}
+
 void Solver::set_domain(const uint32_t* flags, const float* rhs) {
     const size_t n = (size_t)opts.size[0] * opts.size[1] * opts.size[2];
     flags_in.assign(flags, flags + n);
@@ -95,6 +111,13 @@ void Solver::initialize() {
         }
     }
     tile_nbr.upload(nbr.data(), nbr.size(), stream);
+    {
+        std::vector<int> txyz(3 * nt);
+        for (size_t t = 0; t < nt; ++t)
+            for (int a = 0; a < 3; ++a) txyz[3 * t + a] = L.tiles[t][a];
+        tile_xyz.upload(txyz.data(), txyz.size(), stream);
+    }
+    dense.alloc(std::max<size_t>(L.cell_count(), 1));
     tflags.upload(L.tile_flags.data(), L.tile_flags.size(), stream);
     std::vector<int> btile(L.boxes.size()), bnb(3 * L.boxes.size());
     for (size_t i = 0; i < L.boxes.size(); ++i) {
@@ -113,7 +136,14 @@ void Solver::initialize() {
     (void)S;
 
     // Interface system (host assembly + factorisations) and its device solver.
+    if (std::getenv("HDD_VERBOSE"))
+        std::fprintf(stderr, "[hdd setup] layout %.2f s (%zu tiles, %zu boxes)\n",
+                     std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(), L.tiles.size(),
+                     L.boxes.size());
     build_interface(L, opts.sigma_levels, ih);
+    if (std::getenv("HDD_VERBOSE"))
+        std::fprintf(stderr, "[hdd setup] interface assembly done at %.2f s\n",
+                     std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
     sigma.setup(ih, opts.sigma_smoothing, stream);
     // Level-0 interface DOFs: cell slots and their Active face neighbours.
     const int n_if = ih.n_iface.empty() ? 0 : ih.n_iface[0];
@@ -145,10 +175,13 @@ void Solver::initialize() {
 }
 
 void Solver::set_rhs(const float* rhs) {
-    if (rhs != rhs_dense.data()) rhs_dense.assign(rhs, rhs + L.cell_count());
-    std::vector<float> t(L.tiled_count());
-    dense_to_tiles(L, rhs_dense.data(), t.data());
-    cuda_check(cudaMemcpyAsync(b.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D rhs");
+    // H2D of the dense right-hand side, then a device gather into the tiles.
+    if (rhs != rhs_dense.data()) rhs_dense.clear();
+    Tm tm(this, 5);
+    cuda_check(cudaMemcpyAsync(dense.p, rhs, L.cell_count() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D rhs");
+    cuda_check(launch_dense_to_tiles(geom(), tile_xyz.p, L.opt.size[0], L.opt.size[1], L.opt.size[2], dense.p, b.p,
+                                     stream), "dense_to_tiles");
+    count();
     sync();
 }
 
@@ -171,6 +204,8 @@ VcycleArgs Solver::vcycle_args(float* u, const float* bb, int halo_from_u, int z
     a.bottom_itr = 200;  // CPU/SPGrid_Library/SPGrid_V_Cycle_Helper.h:179
     a.halo_from_u = halo_from_u;
     a.zero_init = zero_init;
+    a.cluster = 1;
+    if (const char* e = std::getenv("HDD_VCYCLE_CLUSTER")) a.cluster = std::atoi(e);
     // Correction weights omega/face_count with omega = (float)(2/3)
     // (SPGrid_Correction_Legacy.h:149,190), divided in float on the host.
     const float omega = (float)(2. / 3.);
@@ -191,6 +226,7 @@ VcycleArgs Solver::vcycle_args(float* u, const float* bb, int halo_from_u, int z
 
 void Solver::run_vcycle(float* u, const float* bb, int halo_from_u, int zero_init, int nv) {
     VcycleArgs a = vcycle_args(u, bb, halo_from_u, zero_init, nv);
+    Tm tm(this, 0);
     cuda_check(launch_vcycle(a, stream), "vcycle kernel");
     count();
 }
@@ -199,13 +235,22 @@ void Solver::apply_preconditioner(const float* rr, float* zz) {
     const TileGeom g = geom();
     run_vcycle(zz, rr, 0, 1, opts.nVcycles);
     const int n_if = ih.n_iface.empty() ? 0 : ih.n_iface[0];
-    cuda_check(launch_interface_gather(g, iface_slot.p, iface_nb.p, n_if, rr, zz, sigma.b0(), stream), "gather");
-    count();
-    // u_G = 0 then sigma_mg V-cycles (Preconditioner.h:105,110-117).
-    cuda_check(cudaMemsetAsync(sigma.u0(), 0, sizeof(float) * std::max(n_if, 1), stream), "memset u0");
-    for (int i = 0; i < opts.sigma_mg; ++i) sigma.vcycle(stream, launches);
-    cuda_check(launch_interface_scatter(iface_slot.p, n_if, sigma.u0(), zz, stream), "scatter");
-    count();
+    {
+        Tm tm(this, 3);
+        cuda_check(launch_interface_gather(g, iface_slot.p, iface_nb.p, n_if, rr, zz, sigma.b0(), stream), "gather");
+        count();
+    }
+    {
+        // u_G = 0 then sigma_mg V-cycles (Preconditioner.h:105,110-117).
+        Tm tm(this, 4);
+        cuda_check(cudaMemsetAsync(sigma.u0(), 0, sizeof(float) * std::max(n_if, 1), stream), "memset u0");
+        for (int i = 0; i < opts.sigma_mg; ++i) sigma.vcycle(stream, launches);
+    }
+    {
+        Tm tm(this, 3);
+        cuda_check(launch_interface_scatter(iface_slot.p, n_if, sigma.u0(), zz, stream), "scatter");
+        count();
+    }
     run_vcycle(zz, rr, 1, 1, opts.nVcycles);
 }
 
@@ -241,14 +286,23 @@ void Solver::solve(hdd_result* res) {
         if (rmax <= threshold && (it >= opts.min_iters || rmax < small_number)) { converged = true; break; }
         if (it >= opts.max_iters) break;
         apply_preconditioner(r.p, z.p);
-        cuda_check(launch_project_dot(g, z.p, r.p, partial.p, stream), "project_dot"); count();
-        cuda_check(launch_reduce_sum(partial.p, nt, sums.p + 0, stream), "reduce"); count();
-        cuda_check(launch_scalar_rho(scal.p, sums.p + 0, it == 0, stream), "rho"); count();
-        cuda_check(launch_update_s(g, s.p, z.p, scal.p, it == 0, mode, stream), "update_s"); count();
-        cuda_check(launch_laplace_dot(g, s.p, q.p, partial.p, stream), "laplace"); count();
-        cuda_check(launch_reduce_sum(partial.p, nt, sums.p + 1, stream), "reduce"); count();
-        cuda_check(launch_scalar_alpha(scal.p, sums.p + 1, stream), "alpha"); count();
-        cuda_check(launch_update_xr(g, x.p, r.p, s.p, q.p, scal.p, mode, partial_max.p, stream), "update_xr"); count();
+        {
+            Tm tm(this, 2);
+            cuda_check(launch_project_dot(g, z.p, r.p, partial.p, stream), "project_dot"); count();
+            cuda_check(launch_reduce_sum(partial.p, nt, sums.p + 0, stream), "reduce"); count();
+            cuda_check(launch_scalar_rho(scal.p, sums.p + 0, it == 0, stream), "rho"); count();
+            cuda_check(launch_update_s(g, s.p, z.p, scal.p, it == 0, mode, stream), "update_s"); count();
+        }
+        {
+            Tm tm(this, 1);
+            cuda_check(launch_laplace_dot(g, s.p, q.p, partial.p, stream), "laplace"); count();
+        }
+        {
+            Tm tm(this, 2);
+            cuda_check(launch_reduce_sum(partial.p, nt, sums.p + 1, stream), "reduce"); count();
+            cuda_check(launch_scalar_alpha(scal.p, sums.p + 1, stream), "alpha"); count();
+            cuda_check(launch_update_xr(g, x.p, r.p, s.p, q.p, scal.p, mode, partial_max.p, stream), "update_xr"); count();
+        }
         if (mode == 1 && opts.true_residual_every > 0 && (it + 1) % opts.true_residual_every == 0) {
             cuda_check(launch_residual(g, b.p, x.p, r.p, partial_max.p, stream), "true residual"); count();
         }
@@ -277,6 +331,7 @@ void Solver::solve(hdd_result* res) {
     cuda_check(cudaMemcpyAsync(d2, sums.p + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream), "D2H");
     sync();
     solved = true;
+    check_waits();
     if (res) {
         res->iterations = it;
         res->converged = converged ? 1 : 0;
@@ -293,10 +348,13 @@ void Solver::solve(hdd_result* res) {
 
 void Solver::get_solution(float* out) {
     if (!solved) throw Error(HDD_ERR_NOT_INITIALIZED, "no solution available");
-    std::vector<float> t(L.tiled_count());
-    cuda_check(cudaMemcpyAsync(t.data(), x.p, t.size() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H x");
+    Tm tm(this, 5);
+    cuda_check(cudaMemsetAsync(dense.p, 0, L.cell_count() * sizeof(float), stream), "memset");
+    cuda_check(launch_tiles_to_dense(geom(), tile_xyz.p, L.opt.size[0], L.opt.size[1], L.opt.size[2], x.p, dense.p,
+                                     stream), "tiles_to_dense");
+    count();
+    cuda_check(cudaMemcpyAsync(out, dense.p, L.cell_count() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H x");
     sync();
-    tiles_to_dense(L, t.data(), out);
 }
 
 void Solver::apply_preconditioner_dense(const float* rin, float* zout) {
@@ -309,6 +367,7 @@ void Solver::apply_preconditioner_dense(const float* rin, float* zout) {
     cuda_check(launch_project(geom(), z.p, stream), "project"); count();
     cuda_check(cudaMemcpyAsync(t.data(), z.p, t.size() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
     sync();
+    check_waits();
     tiles_to_dense(L, t.data(), zout);
 }
 
@@ -352,6 +411,12 @@ void Solver::sigma_vcycle_host(const float* b0, float* u0) {
     sigma.vcycle(stream, launches);
     cuda_check(cudaMemcpyAsync(u0, sigma.u0(), n_if * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
     sync();
+    check_waits();
+}
+
+void Solver::check_waits() {
+    if (sigma.error_flag(stream))
+        throw Error(HDD_ERR_TIMEOUT, "a bounded device wait in the sigma solve gave up; results are invalid");
 }
 
 }  // namespace hdd

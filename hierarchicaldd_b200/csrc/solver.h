@@ -67,7 +67,8 @@ struct Solver {
     cudaStream_t stream = nullptr;
     DevBuf<float> x, b, r, z, s, q;
     DevBuf<uint16_t> tflags;
-    DevBuf<int> tile_nbr, box_tile, box_nb;
+    DevBuf<int> tile_nbr, box_tile, box_nb, tile_xyz;
+    DevBuf<float> dense;   // staging buffer in the caller's dense layout
     DevBuf<uint8_t> box_flags;
     DevBuf<double> partial, sums;
     DevBuf<float> partial_max, scalars_f;
@@ -78,6 +79,30 @@ struct Solver {
     SigmaGpu sigma;
     InterfaceHost ih;
     double setup_ms = 0;
+
+    // Optional per-phase device timing with CUDA events on the solver stream
+    // (categories: 0 V-cycle kernel, 1 Laplacian kernel, 2 PCG vector kernels,
+    // 3 interface gather/scatter, 4 sigma V-cycle, 5 dense<->tile copies).
+    static constexpr int kCats = 8;
+    bool timing = false;
+    double cat_ms[kCats] = {0};
+    long long cat_n[kCats] = {0};
+    struct Pending { int cat; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    struct Tm {
+        Solver* s; int cat; cudaEvent_t a = nullptr, b = nullptr;
+        Tm(Solver* sv, int c) : s(sv), cat(c) {
+            if (!s->timing) return;
+            cudaEventCreate(&a); cudaEventCreate(&b);
+            cudaEventRecord(a, s->stream);
+        }
+        ~Tm() {
+            if (!a) return;
+            cudaEventRecord(b, s->stream);
+            s->pending.push_back({cat, a, b});
+        }
+    };
+    void collect_timing();
 
     explicit Solver(const hdd_options& o);
     ~Solver();
@@ -91,6 +116,8 @@ struct Solver {
     void vcycle_dense(float* u, const float* bb, int nv);
     void multiply_dense(const float* xin, float* yout);
     void sigma_vcycle_host(const float* b0, float* u0);
+    // Throws HDD_ERR_TIMEOUT when a device-side bounded wait gave up.
+    void check_waits();
 
     // Device pieces.
     TileGeom geom() const;

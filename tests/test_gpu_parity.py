@@ -153,3 +153,46 @@ def test_pcg_config1_against_fp64_oracle():
     err7 = np.linalg.norm(x7.astype(np.float64) - x64) / nrm
     assert res7["converged"] == 1
     assert err7 <= 1e-5, err7
+
+
+@pytest.mark.parametrize("cluster", ["1", "2"])
+def test_vcycle_sub16_cluster_variants_bitexact(cluster, monkeypatch):
+    """The 16^3 V-cycle runs either in one CTA or split over a 2-CTA cluster."""
+    monkeypatch.setenv("HDD_VCYCLE_CLUSTER", cluster)
+    d = domains.small(48, 16, 8, seed=7)
+    s, o = make_pair(d)
+    rng = np.random.default_rng(8)
+    f0 = o.level_flags(0)
+    u = rng.standard_normal(d.size).astype(np.float32)
+    u[(f0 & (ACTIVE | INTERFACE)) == 0] = 0
+    b = rng.standard_normal(d.size).astype(np.float32)
+    b[(f0 & ACTIVE) == 0] = 0
+    ug = s.V_Cycle(u, b, 1)
+    s.close()
+    uo, _ = o.vcycle(u, np.zeros_like(u), b)
+    assert np.array_equal(ug, uo), np.max(np.abs(ug - uo))
+
+
+def test_sub32_cluster_vcycle_and_pcg():
+    """32^3 subdomains use the 4-CTA cluster kernel: bit-exact V-cycle, PCG parity."""
+    d = domains.small(64, 32, 10, seed=9)
+    d.meta.update(vlevels=4, interior_smoothing=4, boundary_smoothing=4, sigma_levels=4)
+    s, o = make_pair(d)
+    rng = np.random.default_rng(10)
+    f0 = o.level_flags(0)
+    u = rng.standard_normal(d.size).astype(np.float32)
+    u[(f0 & (ACTIVE | INTERFACE)) == 0] = 0
+    b = rng.standard_normal(d.size).astype(np.float32)
+    b[(f0 & ACTIVE) == 0] = 0
+    for nv in (1, 2):
+        ug = s.V_Cycle(u, b, nv)
+        uo, r = u.copy(), np.zeros_like(u)
+        for _ in range(nv):
+            uo, r = o.vcycle(uo, r, b)
+        assert np.array_equal(ug, uo), (nv, np.max(np.abs(ug - uo)))
+    res = s.Solve()
+    x = s.Solution()
+    s.close()
+    xo, it_o, _ = o.solve(d.rhs, tol=1e-6)
+    assert res["converged"] == 1 and abs(res["iterations"] - it_o) <= 1, (res["iterations"], it_o)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-5
