@@ -4,9 +4,10 @@
 // interface matrix and every subdomain interior matrix
 // (CPU/Interface_Solver/SIGMA_SMOOTHER.cpp:175-237 builds A + 1e-5 I with a
 // 1e-5 diagonal for empty rows; phases 11/22 factor it).  The ordering is a
-// nested dissection by breadth-first level structures; every separator (and
-// every leaf block) is one dense front, so the factor is a tree of dense
-// blocks that the GPU solves level by level.
+// nested dissection: median planes through the DOF positions when they are
+// known, breadth-first level structures otherwise; every separator (and every
+// leaf block) is one dense front, so the factor is a tree of dense blocks that
+// the GPU solves level by level.
 #include <algorithm>
 #include <cmath>
 #include <functional>
@@ -20,7 +21,7 @@ namespace {
 constexpr int kLeaf = 32;
 }
 
-void SnFactor::analyze(const CsrF& A) {
+void SnFactor::analyze(const CsrF& A, const std::vector<std::array<int, 3>>* xyz) {
     n = A.rows;
     std::vector<std::vector<int>> nb(n);
     for (int r = 0; r < n; ++r)
@@ -88,6 +89,75 @@ void SnFactor::analyze(const CsrF& A) {
             std::vector<int> ra = rec(comp, pa), rb = rec(rest, pb);
             ra.insert(ra.end(), rb.begin(), rb.end());
             return ra;
+        }
+        if (xyz) {
+            // Geometric split: for each axis, cut at the median position; the
+            // separator is the smaller of the two one-sided boundary layers.
+            // Keep the axis with the smallest separator.
+            int best_axis = -1;
+            size_t best_sep = 0;
+            int best_cut = 0, best_side = 0;
+            std::vector<int> pos(verts.size());
+            for (int ax = 0; ax < 3; ++ax) {
+                for (size_t i = 0; i < verts.size(); ++i) pos[i] = (*xyz)[verts[i]][ax];
+                const size_t mid = pos.size() / 2;
+                std::nth_element(pos.begin(), pos.begin() + mid, pos.end());
+                int cut = pos[mid];
+                size_t nleft = 0, nle = 0;
+                for (int v : verts) {
+                    nleft += (*xyz)[v][ax] < cut;
+                    nle += (*xyz)[v][ax] <= cut;
+                }
+                if (nleft == 0) {
+                    if (nle == verts.size()) continue;  // all at one position along this axis
+                    cut += 1;                           // left = positions <= median
+                }
+                size_t sl = 0, sr = 0;
+                for (int v : verts) {
+                    const bool left = (*xyz)[v][ax] < cut;
+                    for (int p = adjp[v]; p < adjp[v + 1]; ++p) {
+                        const int w = adj[p];
+                        if (part[w] != pid) continue;
+                        if (((*xyz)[w][ax] < cut) != left) {
+                            (left ? sl : sr)++;
+                            break;
+                        }
+                    }
+                }
+                const size_t sep = std::min(sl, sr);
+                if (best_axis < 0 || sep < best_sep) {
+                    best_axis = ax;
+                    best_sep = sep;
+                    best_cut = cut;
+                    best_side = sl <= sr ? 0 : 1;
+                }
+            }
+            if (best_axis >= 0) {
+                // best_side 0: separator taken from the left layer.
+                std::vector<int> Av, Sv, Bv;
+                for (int v : verts) {
+                    const bool left = (*xyz)[v][best_axis] < best_cut;
+                    const bool on_sep_side = (best_side == 0) == left;
+                    bool boundary = false;
+                    if (on_sep_side)
+                        for (int p = adjp[v]; p < adjp[v + 1] && !boundary; ++p) {
+                            const int w = adj[p];
+                            if (part[w] == pid && ((*xyz)[w][best_axis] < best_cut) != left) boundary = true;
+                        }
+                    if (boundary) Sv.push_back(v);
+                    else if (left) Av.push_back(v);
+                    else Bv.push_back(v);
+                }
+                if (!Av.empty() && !Bv.empty()) {
+                    const int pa = next_part++, pb = next_part++;
+                    for (int v : Av) part[v] = pa;
+                    for (int v : Bv) part[v] = pb;
+                    for (int v : Sv) part[v] = -1;
+                    std::vector<int> children = rec(Av, pa), rb = rec(Bv, pb);
+                    children.insert(children.end(), rb.begin(), rb.end());
+                    return std::vector<int>{make_node(Sv, children)};
+                }
+            }
         }
         comp.clear();
         bfs(far, pid, comp);

@@ -165,6 +165,7 @@ struct BoxWork {
     std::vector<CsrF> aii;
     std::vector<std::vector<std::pair<std::pair<int, int>, float>>> air_terms;  // (row, local iface id)
     std::vector<int> n_int;
+    std::vector<std::vector<I3>> int_xyz;       // interior DOF -> position in finest-level units
 };
 
 struct LevelArrays {
@@ -284,6 +285,7 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
     W.air_terms.assign(M, {});
     W.aii.assign(M, CsrF());
     W.n_int.assign(M, 0);
+    W.int_xyz.assign(M, {});
     std::vector<int> node_count(M + 1, 0);
 
     for (int m = 1; m <= M; ++m) {
@@ -356,6 +358,7 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
                         if (!(A.flags[pn] & N_DEGREE)) {
                             A.flags[pn] |= N_DEGREE | N_ACTIVE;
                             A.index[pn] = count++;
+                            W.int_xyz[m - 1].push_back({N[0] << (L - 1), N[1] << (L - 1), N[2] << (L - 1)});
                         }
                     } else {
                         A.flags[pn] |= N_TJUNCTION;
@@ -366,6 +369,8 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
                             if (!(A.flags[pp] & N_DEGREE)) {
                                 A.flags[pp] |= N_DEGREE | N_ACTIVE;
                                 A.index[pp] = count++;
+                                const I3& q2 = p.first;
+                                W.int_xyz[m - 1].push_back({q2[0] << (L - 1), q2[1] << (L - 1), q2[2] << (L - 1)});
                             }
                         }
                     }
@@ -585,6 +590,8 @@ void build_interface(const DomainLayout& L, int M, InterfaceHost& out) {
     out.Arr.assign(M, CsrF());
     out.Aii.assign(M, std::vector<CsrF>(nsub));
     out.Air.assign(M, std::vector<CsrF>(nsub));
+    out.iface_xyz.assign(M, {});
+    out.aii_xyz.assign(M, std::vector<std::vector<std::array<int, 3>>>(nsub));
     std::vector<std::unordered_map<uint64_t, int>> gid(M);
     std::vector<std::unordered_map<uint64_t, float>> arr(M);
     std::vector<std::vector<std::pair<uint64_t, float>>> air_pairs(nsub);
@@ -599,6 +606,7 @@ void build_interface(const DomainLayout& L, int M, InterfaceHost& out) {
                 if (it == gid[m].end()) {
                     it = gid[m].emplace(key, out.n_iface[m]++).first;
                     if (m == 0) out.iface_map.push_back(nd);
+                    out.iface_xyz[m].push_back({nd[0] << m, nd[1] << m, nd[2] << m});
                 }
                 to_g[i] = it->second;
             }
@@ -610,6 +618,7 @@ void build_interface(const DomainLayout& L, int M, InterfaceHost& out) {
                 ap.push_back({((uint64_t)(uint32_t)tv.first.first << 32) | (uint32_t)to_g[tv.first.second], tv.second});
             air_pairs[s].swap(ap);
             out.Aii[m][s] = std::move(W.aii[m]);
+            out.aii_xyz[m][s] = std::move(W.int_xyz[m]);
             W.arr_terms[m].clear();
         }
         for (int s = 0; s < nsub; ++s) out.Air[m][s] = csr_from_pairs(work[s].n_int[m], 0, air_pairs[s]);

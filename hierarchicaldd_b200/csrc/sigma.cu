@@ -39,6 +39,13 @@ constexpr int kNT = 256;
 
 using dev::ck;
 
+// DOF positions of one subdomain's interior block, when assembly recorded them.
+const std::vector<std::array<int, 3>>* positions(const std::vector<std::vector<std::vector<std::array<int, 3>>>>& xyz,
+                                                int l, int sd, int rows) {
+    if (l >= (int)xyz.size() || sd >= (int)xyz[l].size() || (int)xyz[l][sd].size() != rows) return nullptr;
+    return &xyz[l][sd];
+}
+
 // ---------------------------------------------------------------------------
 // Kernels
 // ---------------------------------------------------------------------------
@@ -190,7 +197,7 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
         for (int sd = 0; sd < ih.n_sub; ++sd) {
             try {
                 if (ih.Aii[l][sd].rows == 0) continue;
-                aii[sd].analyze(ih.Aii[l][sd]);
+                aii[sd].analyze(ih.Aii[l][sd], positions(ih.aii_xyz, l, sd, ih.Aii[l][sd].rows));
                 aii[sd].factor(ih.Aii[l][sd], eps);
                 if (l + 1 < M) aii[sd].build_solve_blocks();
             } catch (const std::exception& e) { err[sd] = e.what(); }
@@ -199,7 +206,9 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
             if (!e.empty()) throw Error(HDD_ERR_INTERNAL, "subdomain factorisation: " + e);
         stamp("subdomain factors", l);
         SnFactor arrf;
-        arrf.analyze(ih.Arr[l]);
+        const std::vector<std::array<int, 3>>* ixyz =
+            (l < (int)ih.iface_xyz.size() && (int)ih.iface_xyz[l].size() == ih.Arr[l].rows) ? &ih.iface_xyz[l] : nullptr;
+        arrf.analyze(ih.Arr[l], ixyz);
         arrf.factor(ih.Arr[l], eps);
         if (l + 1 < M) arrf.build_solve_blocks();
         stamp("interface factor", l);
@@ -273,8 +282,17 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
                 for (auto& e : row) { K.col.push_back(e.first); K.val.push_back(e.second); }
                 K.ptr.push_back((int)K.col.size());
             }
+            // Positions of K's DOFs: subdomain interiors, then the interface.
+            std::vector<std::array<int, 3>> kxyz;
+            bool have_xyz = ixyz != nullptr;
+            for (int sd = 0; sd < ih.n_sub && have_xyz; ++sd) {
+                const auto* px = positions(ih.aii_xyz, l, sd, ih.Aii[l][sd].rows);
+                if (!px) have_xyz = false;
+                else kxyz.insert(kxyz.end(), px->begin(), px->end());
+            }
+            if (have_xyz) kxyz.insert(kxyz.end(), ixyz->begin(), ixyz->end());
             SnFactor kf;
-            kf.analyze(K);
+            kf.analyze(K, have_xyz ? &kxyz : nullptr);
             kf.factor(K, eps);
             kf.build_solve_blocks();
             bottom.build({&kf}, {0}, s);

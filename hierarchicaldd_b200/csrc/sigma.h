@@ -28,6 +28,10 @@ struct InterfaceHost {
     std::vector<std::array<int, 3>> iface_map;      // level-0 interface DOF -> cell
     std::vector<CsrF> Arr, Prr;                     // [level]
     std::vector<std::vector<CsrF>> Aii, Air;        // [level][subdomain]
+    // DOF positions in finest-level grid units (used only for the fill-reducing
+    // ordering of the factorisations).
+    std::vector<std::vector<std::array<int, 3>>> iface_xyz;             // [level][dof]
+    std::vector<std::vector<std::vector<std::array<int, 3>>>> aii_xyz;  // [level][subdomain][dof]
 };
 
 // Builds the interface system from the caller's flags (before the global
@@ -45,7 +49,10 @@ struct SnFactor {
     std::vector<std::vector<int>> rows;        // below-diagonal rows (new indices), sorted
     std::vector<std::vector<double>> Ljj, Lrj; // col-major dense blocks
     std::vector<std::vector<double>> Fw;       // [Linv; -L_RJ Linv], (nj+nr) x nj col-major
-    void analyze(const CsrF& A);
+    // Nested-dissection ordering and symbolic factorisation.  With DOF
+    // positions the separators are planes cut at the median along the axis
+    // that gives the smallest separator; without them, breadth-first level sets.
+    void analyze(const CsrF& A, const std::vector<std::array<int, 3>>* xyz = nullptr);
     void factor(const CsrF& A, double eps);
     void build_solve_blocks();
     void solve(double* x) const;               // host reference solve (tests)
