@@ -62,6 +62,7 @@ SIGNATURES = {
     "hdd_apply_preconditioner_dense": (C.c_int, [_vp, _fp, _fp]),
     "hdd_vcycle_dense": (C.c_int, [_vp, _fp, _fp, C.c_int]),
     "hdd_multiply_dense": (C.c_int, [_vp, _fp, _fp]),
+    "hdd_multiply_dot_dense_device_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "hdd_sigma_vcycle": (C.c_int, [_vp, _fp, _fp]),
     "hdd_interface_size": (C.c_int, [_vp, C.c_int, _ip]),
     "hdd_interface_map": (C.c_int, [_vp, _ip]),

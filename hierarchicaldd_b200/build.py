@@ -24,6 +24,7 @@ SOURCES = [
     "sigma.cu",
     "sn_solve.cu",
     "solver.cu",
+    "noalloc.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -5,6 +5,7 @@
 #include <string>
 #include <vector>
 
+#include "noalloc.h"
 #include "solver.h"
 
 using hdd::Error;
@@ -181,6 +182,18 @@ hdd_status hdd_vcycle_dense(hdd_solver* s, float* u, const float* b, int n_vcycl
 hdd_status hdd_multiply_dense(hdd_solver* s, const float* x, float* y) {
     if (!x || !y) return HDD_ERR_INVALID_ARGUMENT;
     return guard(s, [&](Solver& v) { v.multiply_dense(x, y); });
+}
+
+hdd_status hdd_multiply_dot_dense_device_noalloc(hdd_solver* s, const float* x, float* y, double* dot,
+                                                 void* stream) {
+    if (!x || !y || !dot) return HDD_ERR_INVALID_ARGUMENT;
+    return guard(s, [&](Solver& v) {
+        if (!v.initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+        hdd::cuda_check(cudaSetDevice(v.opts.device), "cudaSetDevice");
+        hdd::multiply_dot_dense_device_noalloc(v.geom(), v.tile_xyz.p, v.L.opt.size, v.opts.device, x, y, dot,
+                                               static_cast<cudaStream_t>(stream));
+        v.count(2);
+    });
 }
 
 hdd_status hdd_sigma_vcycle(hdd_solver* s, const float* b0, float* u0) {

@@ -123,6 +123,24 @@ hdd_status hdd_vcycle_dense(hdd_solver* s, float* u, const float* b, int n_vcycl
  * (CG_SYSTEM.cpp:28-44,100-119). */
 hdd_status hdd_multiply_dense(hdd_solver* s, const float* x, float* y);
 
+/* Allocation-free y = Project(A x) plus dot = sum(x*y), for callers that
+ * cannot allocate device memory when they need the operator (a framework
+ * whose own allocator holds the device memory, or a loop that must not stall
+ * on an allocation).  No counterpart in the reference.
+ *   x, y:  DEVICE arrays in the dense layout of hdd_multiply_dense
+ *          (size[0]*size[1]*size[2] floats, z fastest); cells outside the
+ *          stored tiles are read as zero and left unwritten in y.
+ *   dot:   DEVICE pointer to one double.
+ *   stream: cudaStream_t to run on (NULL = legacy default stream); the call
+ *          returns without synchronising.
+ * Per-tile partial sums go to one fixed device array of 32768 doubles
+ * (256 KiB, held by every GPU that loads the library); domains with more
+ * stored tiles get HDD_ERR_INVALID_ARGUMENT.  The first call on a device looks
+ * up that array's device address, so make it before any stream capture.
+ * Calls that overlap on the GPU share the array and race. */
+hdd_status hdd_multiply_dot_dense_device_noalloc(hdd_solver* s, const float* x, float* y, double* dot,
+                                                 void* stream);
+
 /* Test seam: one sigma V-cycle (SIGMA_MULTIGRID_SOLVER.cpp:70-82) from u = 0
  * on the level-0 interface right-hand side b0 (interface DOF order). */
 hdd_status hdd_sigma_vcycle(hdd_solver* s, const float* b0, float* u0);
