@@ -23,4 +23,7 @@ def gpu_available() -> bool:
 @pytest.fixture(scope="session")
 def hdd_lib():
     from hierarchicaldd_b200 import _lib
+    if not os.path.exists(_lib.LIB_PATH):
+        from hierarchicaldd_b200 import build
+        build.build()
     return _lib.load()
