@@ -62,16 +62,35 @@ __device__ __forceinline__ int interior_cell(int e, int q) {
     return box_index(e, x + 1, y + 1, z + 1);
 }
 
+// Thread groups that run a level: the whole CTA, or one warp for the small
+// coarse levels, where a CTA-wide barrier per half-sweep costs far more than
+// the few hundred cells it orders.
+struct CtaGroup {
+    __device__ int rank() const { return threadIdx.x; }
+    __device__ int size() const { return blockDim.x; }
+    __device__ void sync() const { __syncthreads(); }
+};
+struct WarpGroup {
+    __device__ int rank() const { return threadIdx.x & 31; }
+    __device__ int size() const { return 32; }
+    __device__ void sync() const { __syncwarp(); }
+};
+
+// Coarse levels with at most this many cells per axis (halos included) run
+// in one warp: (5-2)^3 = 27 cells, one per lane.
+constexpr int kWarpLevelE = 5;
+constexpr int kWarpCH = 1;
+
 // mode: 1 = boundary cells, 2 = interior (non-boundary) cells, 3 = all Active.
-template <int CH>
-__device__ void jacobi_sweep(const LevelSmem& L, int mode, const float* inv_diag) {
+template <int CH, class G>
+__device__ void jacobi_sweep(const G& g, const LevelSmem& L, int mode, const float* inv_diag) {
     const int m = L.e - 2;
     const int ncell = m * m * m;
     float rr[CH];
     int idx[CH];
 #pragma unroll
     for (int c = 0; c < CH; ++c) {
-        const int q = threadIdx.x + c * blockDim.x;
+        const int q = g.rank() + c * g.size();
         idx[c] = -1;
         if (q < ncell) {
             const int i = interior_cell(L.e, q);
@@ -85,7 +104,7 @@ __device__ void jacobi_sweep(const LevelSmem& L, int mode, const float* inv_diag
             }
         }
     }
-    __syncthreads();
+    g.sync();
 #pragma unroll
     for (int c = 0; c < CH; ++c) {
         if (idx[c] >= 0) {
@@ -94,26 +113,35 @@ __device__ void jacobi_sweep(const LevelSmem& L, int mode, const float* inv_diag
             L.u[i] = __fadd_rn(L.u[i], __fmul_rn(w, rr[c]));
         }
     }
-    __syncthreads();
+    g.sync();
 }
 
 // r = b - A u at Active cells (other cells of r keep their zero).
-__device__ void residual_store(const LevelSmem& L) {
+template <class G>
+__device__ void residual_store(const G& g, const LevelSmem& L) {
     const int m = L.e - 2;
     const int ncell = m * m * m;
-    for (int q = threadIdx.x; q < ncell; q += blockDim.x) {
+    for (int q = g.rank(); q < ncell; q += g.size()) {
         const int i = interior_cell(L.e, q);
         const uint32_t fl = L.f[i];
         if (fl & C_ACTIVE) L.r[i] = cell_residual(L, i, fl);
     }
-    __syncthreads();
+    g.sync();
 }
 
-__device__ void restrict_level(const LevelSmem& F, const LevelSmem& Cc, const float* sc64) {
+template <class G>
+__device__ void zero_u(const G& g, const LevelSmem& L) {
+    const int n = L.e * L.e * L.e;
+    for (int i = g.rank(); i < n; i += g.size()) L.u[i] = 0.0f;
+    g.sync();
+}
+
+template <class G>
+__device__ void restrict_level(const G& g, const LevelSmem& F, const LevelSmem& Cc, const float* sc64) {
     const int m = Cc.e - 2;
     const int ncell = m * m * m;
     const int sx = F.e * F.e, sy = F.e;
-    for (int q = threadIdx.x; q < ncell; q += blockDim.x) {
+    for (int q = g.rank(); q < ncell; q += g.size()) {
         const int z = q % m, t = q / m;
         const int y = t % m, x = t / m;
         const int ci = box_index(Cc.e, x + 1, y + 1, z + 1);
@@ -130,14 +158,15 @@ __device__ void restrict_level(const LevelSmem& F, const LevelSmem& Cc, const fl
                     acc = __fadd_rn(acc, __fmul_rn(sc64[(i2 * 4 + j2) * 4 + k2], F.r[f0 + i2 * sx + j2 * sy + k2]));
         Cc.b[ci] = acc;
     }
-    __syncthreads();
+    g.sync();
 }
 
-__device__ void prolongate_level(const LevelSmem& F, const LevelSmem& Cc, const float* sc8) {
+template <class G>
+__device__ void prolongate_level(const G& g, const LevelSmem& F, const LevelSmem& Cc, const float* sc8) {
     const int m = F.e - 2;
     const int ncell = m * m * m;
     const int csx = Cc.e * Cc.e, csy = Cc.e;
-    for (int q = threadIdx.x; q < ncell; q += blockDim.x) {
+    for (int q = g.rank(); q < ncell; q += g.size()) {
         const int z = q % m + 1, t = q / m;
         const int y = t % m + 1, x = t / m + 1;
         const int fi = box_index(F.e, x, y, z);
@@ -160,11 +189,44 @@ __device__ void prolongate_level(const LevelSmem& F, const LevelSmem& Cc, const 
                 }
         F.u[fi] = acc;
     }
-    __syncthreads();
+    g.sync();
+}
+
+// Pre/post smoothing of one level: boundary, interior, boundary sweeps.
+template <int CH, class G>
+__device__ void smooth_level(const G& g, const LevelSmem& L, const VcycleArgs& a, const float* inv_diag) {
+    for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(g, L, 1, inv_diag);
+    for (int i = 0; i < a.interior_itr; ++i) jacobi_sweep<CH>(g, L, 2, inv_diag);
+    for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(g, L, 1, inv_diag);
+}
+
+// Levels T..Lm-1 of one V-cycle with group g: down-leg from T, bottom
+// smoothing at Lm-1, up-leg back to T (the caller has restricted into T).
+template <int CH, class G>
+__device__ void vcycle_tail(const G& g, LevelSmem* lv, int T, int Lm, const VcycleArgs& a, const float* inv_diag,
+                            const float* sc64, const float* sc8) {
+    for (int l = T; l < Lm - 1; ++l) {
+        smooth_level<CH>(g, lv[l], a, inv_diag);
+        residual_store(g, lv[l]);
+        zero_u(g, lv[l + 1]);
+        restrict_level(g, lv[l], lv[l + 1], sc64);
+    }
+    for (int i = 0; i < a.bottom_itr; ++i) jacobi_sweep<CH>(g, lv[Lm - 1], 3, inv_diag);
+    for (int l = Lm - 2; l >= T; --l) {
+        prolongate_level(g, lv[l], lv[l + 1], sc8);
+        smooth_level<CH>(g, lv[l], a, inv_diag);
+    }
+}
+
+// First level (>= 1) small enough for one warp, or Lm when there is none.
+__device__ __forceinline__ int first_warp_level(int sub, int Lm) {
+    for (int l = 1; l < Lm; ++l)
+        if ((sub >> l) + 1 <= kWarpLevelE) return l;
+    return Lm;
 }
 
 template <int SUB, int NT>
-__global__ void __launch_bounds__(NT) vcycle_kernel(VcycleArgs a) {
+__global__ void __launch_bounds__(NT, 1) vcycle_kernel(VcycleArgs a) {
     constexpr int E0 = SUB + 1;
     constexpr int CH = ((SUB - 1) * (SUB - 1) * (SUB - 1) + NT - 1) / NT;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -239,25 +301,25 @@ __global__ void __launch_bounds__(NT) vcycle_kernel(VcycleArgs a) {
     __syncthreads();
 
     const int Lm = a.levels;
+    const int T = first_warp_level(SUB, Lm);  // levels T..Lm-1 run in warp 0
+    const CtaGroup cta;
     for (int cycle = 0; cycle < a.n_vcycles; ++cycle) {
-        for (int l = 0; l < Lm - 1; ++l) {
-            for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(lv[l], 1, s_inv);
-            for (int i = 0; i < a.interior_itr; ++i) jacobi_sweep<CH>(lv[l], 2, s_inv);
-            for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(lv[l], 1, s_inv);
-            residual_store(lv[l]);
-            {
-                const int e = lv[l + 1].e, n = e * e * e;
-                for (int i = threadIdx.x; i < n; i += NT) lv[l + 1].u[i] = 0.0f;
-            }
-            __syncthreads();
-            restrict_level(lv[l], lv[l + 1], s_sc64);
+        const int Tc = T < Lm ? T : Lm - 1;
+        for (int l = 0; l < Tc; ++l) {
+            smooth_level<CH>(cta, lv[l], a, s_inv);
+            residual_store(cta, lv[l]);
+            zero_u(cta, lv[l + 1]);
+            restrict_level(cta, lv[l], lv[l + 1], s_sc64);
         }
-        for (int i = 0; i < a.bottom_itr; ++i) jacobi_sweep<CH>(lv[Lm - 1], 3, s_inv);
-        for (int l = Lm - 2; l >= 0; --l) {
-            prolongate_level(lv[l], lv[l + 1], s_sc8);
-            for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(lv[l], 1, s_inv);
-            for (int i = 0; i < a.interior_itr; ++i) jacobi_sweep<CH>(lv[l], 2, s_inv);
-            for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(lv[l], 1, s_inv);
+        if (T < Lm) {
+            if (threadIdx.x < 32) vcycle_tail<kWarpCH>(WarpGroup(), lv, T, Lm, a, s_inv, s_sc64, s_sc8);
+            __syncthreads();
+        } else {
+            for (int i = 0; i < a.bottom_itr; ++i) jacobi_sweep<CH>(cta, lv[Lm - 1], 3, s_inv);
+        }
+        for (int l = Tc - 1; l >= 0; --l) {
+            prolongate_level(cta, lv[l], lv[l + 1], s_sc8);
+            smooth_level<CH>(cta, lv[l], a, s_inv);
         }
     }
 
@@ -539,29 +601,25 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
         }
         cluster.sync();  // level-1 b complete in rank 0
         if (rank == 0) {
-            {
-                const int e = lv[1].e, n = e * e * e;
-                for (int i = threadIdx.x; i < n; i += NT) lv[1].u[i] = 0.0f;
+            const CtaGroup cta;
+            zero_u(cta, lv[1]);
+            const int T = first_warp_level(SUB, Lm);  // levels T..Lm-1 run in warp 0
+            const int Tc = T < Lm ? T : Lm - 1;
+            for (int l = 1; l < Tc; ++l) {
+                smooth_level<CH>(cta, lv[l], a, s_inv);
+                residual_store(cta, lv[l]);
+                zero_u(cta, lv[l + 1]);
+                restrict_level(cta, lv[l], lv[l + 1], s_sc64);
             }
-            __syncthreads();
-            for (int l = 1; l < Lm - 1; ++l) {
-                for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(lv[l], 1, s_inv);
-                for (int i = 0; i < a.interior_itr; ++i) jacobi_sweep<CH>(lv[l], 2, s_inv);
-                for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(lv[l], 1, s_inv);
-                residual_store(lv[l]);
-                {
-                    const int e = lv[l + 1].e, n = e * e * e;
-                    for (int i = threadIdx.x; i < n; i += NT) lv[l + 1].u[i] = 0.0f;
-                }
+            if (T < Lm) {
+                if (threadIdx.x < 32) vcycle_tail<kWarpCH>(WarpGroup(), lv, T, Lm, a, s_inv, s_sc64, s_sc8);
                 __syncthreads();
-                restrict_level(lv[l], lv[l + 1], s_sc64);
+            } else {
+                for (int i = 0; i < a.bottom_itr; ++i) jacobi_sweep<CH>(cta, lv[Lm - 1], 3, s_inv);
             }
-            for (int i = 0; i < a.bottom_itr; ++i) jacobi_sweep<CH>(lv[Lm - 1], 3, s_inv);
-            for (int l = Lm - 2; l >= 1; --l) {
-                prolongate_level(lv[l], lv[l + 1], s_sc8);
-                for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(lv[l], 1, s_inv);
-                for (int i = 0; i < a.interior_itr; ++i) jacobi_sweep<CH>(lv[l], 2, s_inv);
-                for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(lv[l], 1, s_inv);
+            for (int l = Tc - 1; l >= 1; --l) {
+                prolongate_level(cta, lv[l], lv[l + 1], s_sc8);
+                smooth_level<CH>(cta, lv[l], a, s_inv);
             }
         }
         cluster.sync();  // level-1 u final

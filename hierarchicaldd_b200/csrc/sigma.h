@@ -66,6 +66,14 @@ struct SnTask {
     long long blk;            // float offset of the task's block
 };
 
+// One warp task of a small front: its Fw block (m x nj, column-major, leading
+// dimension m) at float offset `off`; `part` selects the rows (forward) or
+// columns (backward) the warp computes.
+struct SnFront {
+    int front, m, nj, part;
+    long long off;
+};
+
 // Device plan for a batch of independent supernodal triangular solves
 // (sn_solve.cu).
 struct SolvePlan {
@@ -73,6 +81,9 @@ struct SolvePlan {
     int nsn = 0;
     int max_front = 0;
     std::vector<int> fwd_ptr, bwd_ptr;           // task ranges per tree level
+    std::vector<int> sfwd_ptr, sbwd_ptr;         // warp-front ranges per tree level
+    SnFront *d_sfwd = nullptr, *d_sbwd = nullptr;
+    float* d_fw = nullptr;                       // warp-front coefficient blocks
     int *d_col0 = nullptr, *d_ncol = nullptr, *d_nrow = nullptr;
     int *d_rows = nullptr; long long *d_rows_off = nullptr;
     int *d_child_ptr = nullptr, *d_child = nullptr;

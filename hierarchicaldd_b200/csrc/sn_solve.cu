@@ -5,11 +5,19 @@
 // W = L_RJ L_JJ^{-1}, so
 //   forward   [y_J; v_J] = Fw f_J + [0; f_R]    (f assembled from b and the children's v)
 //   backward  x_J        = Fw^T [y_J; x_R]
-// are single dense products.  A front is cut into tasks of kTR rows; a task's
-// coefficients are stored as one contiguous block (column-major, kTR rows per
-// column) and streamed into shared memory with 1D bulk async copies
-// (cp.async.bulk, no multicast) through a kNS-stage mbarrier pipeline while the
-// CTA assembles its input vector.  Tasks of one tree level form one launch.
+// are single dense products.
+//
+// Fronts with at most kSmallM rows (nearly all fronts of the subdomain-interior
+// factors) keep Fw column-major with leading dimension m and no padding, and
+// are split into warp tasks: 32 rows each in the forward solve (lanes own
+// rows), kBwdCols columns each in the backward solve (lanes stride down the
+// columns, then reduce by shuffles); the loads of several columns are in
+// flight at once.
+// Larger fronts are cut into tasks of kTR rows; a task's coefficients are one
+// contiguous block (column-major, kTR rows per column) streamed into shared
+// memory with 1D bulk async copies (cp.async.bulk, no multicast) through a
+// kNS-stage mbarrier pipeline while the CTA assembles its input vector.
+// The fronts and tasks of one tree level form one launch of each kernel.
 // Every mbarrier wait is bounded; on timeout the kernel raises the plan's error
 // word, drains its own copies (bounded) and returns.
 #include <cuda_runtime.h>
@@ -29,6 +37,8 @@ constexpr int kTR = 64;   // rows per task = threads per CTA
 constexpr int kCB = 32;   // columns per pipeline stage
 constexpr int kNS = 4;    // pipeline stages
 constexpr long kWaitLimit = 1L << 22;
+constexpr int kSmallM = 256;   // rows of a warp-resident front
+constexpr int kWarps = 8;      // warps (fronts) per CTA of the warp-front kernels
 
 struct PlanView {
     const int *col0, *ncol, *nrow;
@@ -40,6 +50,7 @@ struct PlanView {
     const long long* upd_off;
     const int* perm;
     const float* val;
+    const float* fw;
     float* upd;
     float* ynew;
     float* xnew;
@@ -169,6 +180,86 @@ __global__ void __launch_bounds__(kTR) sn_task_kernel(PlanView P, const SnTask* 
     }
 }
 
+constexpr int kBwdCols = 8;   // columns per backward warp task
+
+// Forward rows [32*part, 32*part+32) of a warp-resident front: y (rows < nj)
+// or the update vector f_R - W f_J (rows >= nj).  Linv is lower triangular,
+// so rows below 32*part+32 need columns < 32*part+32 only.
+__global__ void __launch_bounds__(32 * kWarps) sn_front_forward_kernel(PlanView P, const SnFront* __restrict__ fronts,
+                                                                      int nf, const float* __restrict__ b_old) {
+    __shared__ float sf[kWarps][kSmallM];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int idx = blockIdx.x * kWarps + w;
+    if (idx >= nf) return;
+    const SnFront F = fronts[idx];
+    const int J = F.front, m = F.m, nj = F.nj, c0 = P.col0[J];
+    float* f = sf[w];
+    for (int i = lane; i < m; i += 32) f[i] = (i < nj) ? b_old[P.perm[c0 + i]] : 0.0f;
+    __syncwarp();
+    for (int c = P.child_ptr[J]; c < P.child_ptr[J + 1]; ++c) {
+        const int C = P.child[c];
+        const int mc = P.nrow[C];
+        const float* uc = P.upd + P.upd_off[C];
+        const int* rm = P.relmap + P.relmap_off[C];
+        for (int k = lane; k < mc; k += 32) f[rm[k]] += uc[k];
+        __syncwarp();
+    }
+    const float* A = P.fw + F.off;
+    const int r = 32 * F.part + lane;
+    const bool rv = r < m;
+    const int cend = min(nj, 32 * F.part + 32);
+    float acc = 0.0f;
+#pragma unroll 2
+    for (int c = 0; c < cend; c += 8) {
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+            if (rv && c + t < cend) acc = fmaf(A[(size_t)(c + t) * m + r], f[c + t], acc);
+    }
+    if (!rv) return;
+    if (r < nj) P.ynew[c0 + r] = acc;
+    else P.upd[P.upd_off[J] + (r - nj)] = f[r] + acc;
+}
+
+// Backward columns [kBwdCols*part, +kBwdCols) of a warp-resident front:
+// x_a = sum_{r >= a} Fw(r, a) g_r with g = [y_J; x_R].
+__global__ void __launch_bounds__(32 * kWarps) sn_front_backward_kernel(PlanView P, const SnFront* __restrict__ fronts,
+                                                                       int nf, float* __restrict__ x_old) {
+    __shared__ float sg[kWarps][kSmallM];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int idx = blockIdx.x * kWarps + w;
+    if (idx >= nf) return;
+    const SnFront F = fronts[idx];
+    const int J = F.front, m = F.m, nj = F.nj, c0 = P.col0[J];
+    const int* rows = P.rows + P.rows_off[J];
+    float* g = sg[w];
+    const int a0 = kBwdCols * F.part;
+    for (int i = (a0 & ~31) + lane; i < m; i += 32) g[i] = (i < nj) ? P.ynew[c0 + i] : P.xnew[rows[i - nj]];
+    __syncwarp();
+    const float* A = P.fw + F.off;
+    float sacc[kBwdCols];
+#pragma unroll
+    for (int t = 0; t < kBwdCols; ++t) sacc[t] = 0.0f;
+    for (int r0 = a0 & ~31; r0 < m; r0 += 32) {
+        const int r = r0 + lane;
+        if (r >= m) continue;
+        const float gr = g[r];
+#pragma unroll
+        for (int t = 0; t < kBwdCols; ++t)
+            if (a0 + t < nj && r >= a0 + t) sacc[t] = fmaf(A[(size_t)(a0 + t) * m + r], gr, sacc[t]);
+    }
+#pragma unroll
+    for (int t = 0; t < kBwdCols; ++t)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sacc[t] += __shfl_xor_sync(0xffffffffu, sacc[t], o);
+#pragma unroll
+    for (int t = 0; t < kBwdCols; ++t) {
+        if (lane == t && a0 + t < nj) {
+            P.xnew[c0 + a0 + t] = sacc[t];
+            x_old[P.perm[c0 + a0 + t]] = sacc[t];
+        }
+    }
+}
+
 size_t task_smem(int max_front) {
     return (size_t)kNS * kCB * kTR * sizeof(float) + kNS * sizeof(uint64_t) + (size_t)max_front * sizeof(float);
 }
@@ -235,24 +326,62 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
         total += (long long)nc * kTR;
         v.push_back(t);
     };
+    // Warp-resident fronts: one Fw block each, 16-byte aligned.
+    std::vector<long long> small_off(nsn, -1);
+    long long fw_total = 0;
+    int big_front = 0;
+    for (int g = 0; g < nsn; ++g) {
+        const int m = ncol[g] + nrow[g];
+        if (m <= kSmallM) {
+            small_off[g] = fw_total;
+            fw_total += ((long long)m * ncol[g] + 3) & ~3LL;
+        } else big_front = std::max(big_front, m);
+    }
+    std::vector<SnFront> sfwd, sbwd;
+    auto small_front = [&](int g, int part) {
+        SnFront f;
+        f.front = g; f.m = ncol[g] + nrow[g]; f.nj = ncol[g]; f.part = part; f.off = small_off[g];
+        return f;
+    };
     fwd_ptr.assign(1, 0);
+    sfwd_ptr.assign(1, 0);
     for (int h = 0; h <= hmax; ++h) {
         for (int g = 0; g < nsn; ++g) {
             if (height[g] != h) continue;
             const int nj = ncol[g], nr = nrow[g];
+            if (small_off[g] >= 0) {
+                for (int q = 0; q * 32 < nj + nr; ++q) sfwd.push_back(small_front(g, q));
+                continue;
+            }
             for (int r0 = 0; r0 < nj; r0 += kTR) add(ftasks, g, r0, std::min(r0 + kTR, nj), 0, 0, std::min(r0 + kTR, nj));
             for (int r0 = nj; r0 < nj + nr; r0 += kTR) add(ftasks, g, r0, std::min(r0 + kTR, nj + nr), 1, 0, nj);
         }
         fwd_ptr.push_back((int)ftasks.size());
+        sfwd_ptr.push_back((int)sfwd.size());
     }
     bwd_ptr.assign(1, 0);
+    sbwd_ptr.assign(1, 0);
     for (int d = 0; d <= dmax; ++d) {
         for (int g = 0; g < nsn; ++g) {
             if (depth[g] != d) continue;
             const int nj = ncol[g], nr = nrow[g];
+            if (small_off[g] >= 0) {
+                for (int q = 0; q * kBwdCols < nj; ++q) sbwd.push_back(small_front(g, q));
+                continue;
+            }
             for (int r0 = 0; r0 < nj; r0 += kTR) add(btasks, g, r0, std::min(r0 + kTR, nj), 2, r0, nj + nr - r0);
         }
         bwd_ptr.push_back((int)btasks.size());
+        sbwd_ptr.push_back((int)sbwd.size());
+    }
+    std::vector<float> fw((size_t)std::max<long long>(fw_total, 4), 0.0f);
+#pragma omp parallel for schedule(dynamic)
+    for (int g = 0; g < nsn; ++g) {
+        if (small_off[g] < 0) continue;
+        const SnFactor& F = *factors[where[g].first];
+        const std::vector<double>& W = F.Fw[where[g].second];
+        float* dst = &fw[(size_t)small_off[g]];
+        for (size_t i = 0; i < W.size(); ++i) dst[i] = (float)W[i];
     }
     std::vector<float> val((size_t)total, 0.0f);
     auto fill = [&](const std::vector<SnTask>& v, bool forward) {
@@ -302,6 +431,7 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
         }
     }
     if (nsn == 0) return;
+    max_front = std::max(big_front, 1);
     if (task_smem(max_front) > 227 * 1024)
         throw Error(HDD_ERR_UNSUPPORTED, "supernodal front too large for shared memory: " + std::to_string(max_front));
     bytes = 0;
@@ -316,9 +446,12 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
     d_relmap = dev::upload(relmap.empty() ? std::vector<int>{0} : relmap, s, bytes);
     d_upd_off = dev::upload(upd_off, s, bytes);
     d_perm = dev::upload(perm, s, bytes);
-    d_fwd = dev::upload(ftasks, s, bytes);
-    d_bwd = dev::upload(btasks, s, bytes);
-    d_val = dev::upload(val, s, bytes);
+    d_fwd = dev::upload(ftasks.empty() ? std::vector<SnTask>(1) : ftasks, s, bytes);
+    d_bwd = dev::upload(btasks.empty() ? std::vector<SnTask>(1) : btasks, s, bytes);
+    d_val = dev::upload(val.empty() ? std::vector<float>(4, 0.0f) : val, s, bytes);
+    d_sfwd = dev::upload(sfwd.empty() ? std::vector<SnFront>(1) : sfwd, s, bytes);
+    d_sbwd = dev::upload(sbwd.empty() ? std::vector<SnFront>(1) : sbwd, s, bytes);
+    d_fw = dev::upload(fw, s, bytes);
     d_upd = dev::alloc_zero<float>(std::max<long long>(upd_total, 1), bytes);
     d_ynew = dev::alloc_zero<float>(std::max(n, 1), bytes);
     d_xnew = dev::alloc_zero<float>(std::max(n, 1), bytes);
@@ -332,6 +465,7 @@ void SolvePlan::release() {
     dev::release(d_relmap_off); dev::release(d_relmap); dev::release(d_upd_off); dev::release(d_perm);
     dev::release(d_fwd); dev::release(d_bwd); dev::release(d_val); dev::release(d_upd); dev::release(d_ynew);
     dev::release(d_xnew); dev::release(d_err);
+    dev::release(d_sfwd); dev::release(d_sbwd); dev::release(d_fw);
     nsn = 0;
     n = 0;
 }
@@ -339,13 +473,19 @@ void SolvePlan::release() {
 void SolvePlan::solve(const float* b_old, float* x_old, cudaStream_t s, long long& launches) const {
     if (nsn == 0) return;
     PlanView P{d_col0, d_ncol, d_nrow, d_rows, d_rows_off, d_child_ptr, d_child, d_relmap_off, d_relmap,
-               d_upd_off, d_perm, d_val, d_upd, d_ynew, d_xnew, d_err};
+               d_upd_off, d_perm, d_val, d_fw, d_upd, d_ynew, d_xnew, d_err};
     const size_t smem = task_smem(max_front);
     if (smem > 48 * 1024) {
         dev::ck(cudaFuncSetAttribute(sn_task_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attr");
         dev::ck(cudaFuncSetAttribute(sn_task_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attr");
     }
     for (size_t h = 0; h + 1 < fwd_ptr.size(); ++h) {
+        const int ns = sfwd_ptr[h + 1] - sfwd_ptr[h];
+        if (ns) {
+            sn_front_forward_kernel<<<(ns + kWarps - 1) / kWarps, 32 * kWarps, 0, s>>>(P, d_sfwd + sfwd_ptr[h], ns, b_old);
+            dev::ck(cudaGetLastError(), "sn front forward");
+            ++launches;
+        }
         const int cnt = fwd_ptr[h + 1] - fwd_ptr[h];
         if (!cnt) continue;
         sn_task_kernel<0><<<cnt, kTR, smem, s>>>(P, d_fwd + fwd_ptr[h], b_old, x_old);
@@ -353,6 +493,12 @@ void SolvePlan::solve(const float* b_old, float* x_old, cudaStream_t s, long lon
         ++launches;
     }
     for (size_t d = 0; d + 1 < bwd_ptr.size(); ++d) {
+        const int ns = sbwd_ptr[d + 1] - sbwd_ptr[d];
+        if (ns) {
+            sn_front_backward_kernel<<<(ns + kWarps - 1) / kWarps, 32 * kWarps, 0, s>>>(P, d_sbwd + sbwd_ptr[d], ns, x_old);
+            dev::ck(cudaGetLastError(), "sn front backward");
+            ++launches;
+        }
         const int cnt = bwd_ptr[d + 1] - bwd_ptr[d];
         if (!cnt) continue;
         sn_task_kernel<1><<<cnt, kTR, smem, s>>>(P, d_bwd + bwd_ptr[d], b_old, x_old);
