@@ -58,43 +58,42 @@ struct SnFactor {
     void solve(double* x) const;               // host reference solve (tests)
 };
 
-// One unit of device work of a supernodal solve: rows [rb, re) of one front,
-// streamed as a contiguous block of ncols columns x kTaskRows rows.
+// One unit of device work of a supernodal solve, taken by a CTA of the
+// persistent solve kernels (sn_solve.cu).  With front >= 0, forward: rows
+// [r0, r0+rows) of front `front` times its columns [c0, c0+ncols); when a row
+// block is split into nk > 1 column blocks, the partial sums go to `part` and
+// the last task of the block (counter `chunk`) adds them in order; backward:
+// columns [r0, r0+rows) of the front.  With front < 0, a bundle of `rows`
+// small fronts (listed from index r0 of the plan's bundle list), one per warp.
 struct SnTask {
-    int front, rb, re, kind;  // kind 0: forward L^{-1} rows, 1: forward update rows, 2: backward
-    int col_base, ncols, pad0, pad1;
-    long long blk;            // float offset of the task's block
+    int front, r0, rows, c0, ncols, k, nk, chunk;
+    long long part;
 };
 
-// One warp task of a small front: its Fw block (m x nj, column-major, leading
-// dimension m) at float offset `off`; `part` selects the rows (forward) or
-// columns (backward) the warp computes.
-struct SnFront {
-    int front, m, nj, part;
-    long long off;
-};
-
-// Device plan for a batch of independent supernodal triangular solves
-// (sn_solve.cu).
+// Device plan for a batch of independent supernodal triangular solves.
 struct SolvePlan {
     int n = 0;                       // total unknowns (concatenated)
     int nsn = 0;
     int max_front = 0;
-    std::vector<int> fwd_ptr, bwd_ptr;           // task ranges per tree level
-    std::vector<int> sfwd_ptr, sbwd_ptr;         // warp-front ranges per tree level
-    SnFront *d_sfwd = nullptr, *d_sbwd = nullptr;
-    float* d_fw = nullptr;                       // warp-front coefficient blocks
-    int *d_col0 = nullptr, *d_ncol = nullptr, *d_nrow = nullptr;
+    int n_fwd = 0, n_bwd = 0;        // task counts
+    int n_ctr = 0;                   // ints in the counter block
+    int grid = 0;                    // persistent CTAs per launch
+    int *d_col0 = nullptr, *d_ncol = nullptr, *d_nrow = nullptr, *d_parent = nullptr;
     int *d_rows = nullptr; long long *d_rows_off = nullptr;
     int *d_child_ptr = nullptr, *d_child = nullptr;
     long long* d_relmap_off = nullptr; int* d_relmap = nullptr;
     long long* d_upd_off = nullptr;
+    long long* d_fw_off = nullptr;   // per front: float offset of Fw (leading dimension round4(m))
+    int *d_ntf = nullptr, *d_ntb = nullptr;  // tasks per front, forward / backward
     int* d_perm = nullptr;           // new -> old (concatenated)
     SnTask *d_fwd = nullptr, *d_bwd = nullptr;
-    float* d_val = nullptr;          // task blocks
+    int *d_bfwd = nullptr, *d_bbwd = nullptr;  // fronts of the forward / backward bundles
+    float* d_fw = nullptr;           // Fw blocks of all fronts
+    float* d_part = nullptr;         // partial sums of split row blocks
     float* d_upd = nullptr;          // update vectors
     float* d_ynew = nullptr;         // forward result in new order
     float* d_xnew = nullptr;         // backward result in new order
+    int* d_ctr = nullptr;            // tickets, completion and chunk counters
     int* d_err = nullptr;            // set when a bounded wait gives up
     size_t bytes = 0;
     void build(const std::vector<const SnFactor*>& factors, const std::vector<int>& offsets, cudaStream_t s);

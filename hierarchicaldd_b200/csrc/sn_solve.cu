@@ -1,29 +1,36 @@
 // Supernodal triangular solves on the GPU (the device half of the PARDISO
 // stand-in, SIGMA_SMOOTHER.cpp:433-449 phase 33).
 //
-// Every front J of the nested-dissection tree carries Fw = [L_JJ^{-1}; -W],
-// W = L_RJ L_JJ^{-1}, so
-//   forward   [y_J; v_J] = Fw f_J + [0; f_R]    (f assembled from b and the children's v)
+// Every front J of the nested-dissection forest carries
+// Fw = [L_JJ^{-1}; -L_RJ L_JJ^{-1}] (m = nj + nr rows, nj columns), stored once,
+// column-major with leading dimension round4(m), so
+//   forward   [y_J; v_J] = Fw f_J + [0; f_R]   (f assembled from b and the children's v)
 //   backward  x_J        = Fw^T [y_J; x_R]
-// are single dense products.
+// are dense products over the same coefficients.
 //
-// Fronts with at most kSmallM rows (nearly all fronts of the subdomain-interior
-// factors) keep Fw column-major with leading dimension m and no padding, and
-// are split into warp tasks: 32 rows each in the forward solve (lanes own
-// rows), kBwdCols columns each in the backward solve (lanes stride down the
-// columns, then reduce by shuffles); the loads of several columns are in
-// flight at once.
-// Larger fronts are cut into tasks of kTR rows; a task's coefficients are one
-// contiguous block (column-major, kTR rows per column) streamed into shared
-// memory with 1D bulk async copies (cp.async.bulk, no multicast) through a
-// kNS-stage mbarrier pipeline while the CTA assembles its input vector.
-// The fronts and tasks of one tree level form one launch of each kernel.
-// Every mbarrier wait is bounded; on timeout the kernel raises the plan's error
-// word, drains its own copies (bounded) and returns.
+// Each direction is ONE persistent launch.  Its work is a list of tasks in
+// topological order (forward: children before parents; backward: parents
+// before children); CTAs take tasks by ticket and, before starting one, wait
+// on per-front completion counters of the fronts it depends on.  A task only
+// ever waits on tasks with smaller tickets, which running CTAs already hold,
+// so the walk always progresses; every wait is bounded anyway and raises the
+// plan's error word when it gives up.  Data produced by other CTAs in the same
+// launch is read with L2-coherent loads after an acquire of the counter.
+//
+// Small fronts (a few row chunks times few columns) go in bundles of eight,
+// one warp per front, so eight short dependency chains run per CTA.  Other
+// forward tasks are row blocks of up to kRB rows; a CTA splits its threads
+// into row lanes x column slices and adds the slices in a fixed order.  Tall
+// fronts whose row block needs more than kCC columns are split into column
+// blocks: each writes its partial sums and the last one to finish adds them in
+// column order, so every result is independent of scheduling.  Backward tasks
+// are blocks of kBC columns, one warp per column group, lanes striding down
+// the contiguous columns.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -33,235 +40,337 @@
 namespace hdd {
 namespace {
 
-constexpr int kTR = 64;   // rows per task = threads per CTA
-constexpr int kCB = 32;   // columns per pipeline stage
-constexpr int kNS = 4;    // pipeline stages
-constexpr long kWaitLimit = 1L << 22;
-constexpr int kSmallM = 256;   // rows of a warp-resident front
-constexpr int kWarps = 8;      // warps (fronts) per CTA of the warp-front kernels
+constexpr int kNT = 256;                 // threads per CTA
+constexpr int kRB = 256;                 // rows per forward row block
+constexpr int kCC = 256;                 // columns per forward column block
+constexpr int kBC = 32;                  // columns per backward task (8 warps x 4)
+constexpr long kSpinLimit = 1L << 22;    // polls (with ~128 ns sleeps) before a wait gives up
+constexpr int kWarps = kNT / 32;         // small fronts per bundle (one per warp)
+constexpr int kSmallM = 256;             // rows of a front solved by one warp
+constexpr int kSmallLoads = 64;          // ... when its row chunks x columns stay below this
+
+constexpr int kBundleLevel = 2048;       // bundle only on levels with at least this many small fronts
+
+bool small_front(int m, int nj) { return m <= kSmallM && ((m + 31) / 32) * nj <= kSmallLoads; }
 
 struct PlanView {
-    const int *col0, *ncol, *nrow;
+    int nsn, max_m;
+    const int *col0, *ncol, *nrow, *parent;
     const int* rows;
     const long long* rows_off;
     const int *child_ptr, *child;
     const long long* relmap_off;
     const int* relmap;
     const long long* upd_off;
+    const long long* fw_off;
+    const int *ntf, *ntb;
     const int* perm;
-    const float* val;
+    const int *bfwd, *bbwd;
     const float* fw;
+    float* part;
     float* upd;
     float* ynew;
     float* xnew;
+    int* ctr;
     int* err;
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    for (long i = 0; i < kWaitLimit; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
+// Waits until *p >= target; false when the wait gave up, or at once when an
+// earlier wait of this launch already gave up (so one failure cannot turn
+// into a long chain of timeouts).
+__device__ bool wait_at_least(const int* p, int target, const int* err) {
+    for (long i = 0; i < kSpinLimit; ++i) {
+        if (ld_acquire(p) >= target) return true;
+        if (ld_acquire(err) != 0) return false;
+        __nanosleep(128);
+    }
     return false;
 }
 
-template <int DIR>
-__global__ void __launch_bounds__(kTR) sn_task_kernel(PlanView P, const SnTask* __restrict__ tasks,
-                                                      const float* __restrict__ b_old, float* __restrict__ x_old) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    float* stage = reinterpret_cast<float*>(smem_raw);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(stage + kNS * kCB * kTR);
-    float* vec = reinterpret_cast<float*>(bar + kNS);
-    const SnTask t = tasks[blockIdx.x];
-    const int J = t.front, nj = P.ncol[J], nr = P.nrow[J], c0 = P.col0[J];
-    const int tid = threadIdx.x;
-    const int nchunks = (t.ncols + kCB - 1) / kCB;
-    const float* src = P.val + t.blk;
-    if (tid == 0) {
-        for (int s = 0; s < kNS; ++s) mbar_init(&bar[s], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-    if (tid == 0) {
-        for (int k = 0; k < kNS && k < nchunks; ++k) {
-            const uint32_t bytes = (uint32_t)min(kCB, t.ncols - k * kCB) * kTR * 4u;
-            mbar_expect_tx(&bar[k], bytes);
-            bulk_g2s(stage + k * kCB * kTR, src + (size_t)k * kCB * kTR, bytes, &bar[k]);
+// Forward solve of one small front by one warp (MQ row chunks of 32 rows).
+template <int MQ>
+__device__ __forceinline__ void warp_forward_rows(const PlanView& P, int J, int m, int nj, const float* f, int lane) {
+    const size_t ld = (size_t)((m + 3) & ~3);
+    const float* A = P.fw + P.fw_off[J];
+    float acc[MQ];
+#pragma unroll
+    for (int q = 0; q < MQ; ++q) acc[q] = 0.0f;
+#pragma unroll 2
+    for (int c = 0; c < nj; c += 4) {
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            if (c + t >= nj) break;
+            const float fc = f[c + t];
+            const float* col = A + (size_t)(c + t) * ld;
+#pragma unroll
+            for (int q = 0; q < MQ; ++q) {
+                const int r = q * 32 + lane;
+                if (r < m && r >= c + t) acc[q] = fmaf(__ldg(col + r), fc, acc[q]);
+            }
         }
     }
-    // Input vector, assembled while the first stages are in flight.
-    if (DIR == 0) {
-        for (int i = tid; i < nj; i += kTR) vec[i] = b_old[P.perm[c0 + i]];
-        for (int k = tid; k < nr; k += kTR) vec[nj + k] = 0.0f;
-        __syncthreads();
-        for (int c = P.child_ptr[J]; c < P.child_ptr[J + 1]; ++c) {
-            const int C = P.child[c];
-            const int mc = P.nrow[C];
-            const float* uc = P.upd + P.upd_off[C];
-            const int* rm = P.relmap + P.relmap_off[C];
-            for (int k = tid; k < mc; k += kTR) vec[rm[k]] += uc[k];
-            __syncthreads();
-        }
-    } else {
-        const int* rows = P.rows + P.rows_off[J];
-        for (int a = tid; a < nj; a += kTR) vec[a] = P.ynew[c0 + a];
-        for (int k = tid; k < nr; k += kTR) vec[nj + k] = P.xnew[rows[k]];
-        __syncthreads();
-    }
-    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-    int k = 0;
-    bool ok = true;
-    for (; k < nchunks; ++k) {
-        const int st = k % kNS;
-        int done = 1;
-        if (tid == 0) done = mbar_wait_bounded(&bar[st], (uint32_t)((k / kNS) & 1)) ? 1 : 0;
-        if (!__syncthreads_and(done)) { ok = false; break; }
-        // The copy has landed for thread 0's observation; every thread reads
-        // after the barrier above.
-        const int nc = min(kCB, t.ncols - k * kCB);
-        const float* sp = stage + st * kCB * kTR + tid;
-        const float* vp = vec + t.col_base + k * kCB;
-        int j = 0;
-        for (; j + 3 < nc; j += 4) {
-            s0 = fmaf(sp[(j + 0) * kTR], vp[j + 0], s0);
-            s1 = fmaf(sp[(j + 1) * kTR], vp[j + 1], s1);
-            s2 = fmaf(sp[(j + 2) * kTR], vp[j + 2], s2);
-            s3 = fmaf(sp[(j + 3) * kTR], vp[j + 3], s3);
-        }
-        for (; j < nc; ++j) s0 = fmaf(sp[j * kTR], vp[j], s0);
-        __syncthreads();  // stage st is free again
-        if (tid == 0 && k + kNS < nchunks) {
-            const uint32_t bytes = (uint32_t)min(kCB, t.ncols - (k + kNS) * kCB) * kTR * 4u;
-            fence_proxy_async();
-            mbar_expect_tx(&bar[st], bytes);
-            bulk_g2s(stage + st * kCB * kTR, src + (size_t)(k + kNS) * kCB * kTR, bytes, &bar[st]);
-        }
-    }
-    if (!ok) {
-        if (tid == 0) {
-            atomicExch(P.err, 1);
-            // Drain the copies this CTA still has in flight (bounded) before leaving.
-            for (int q = k; q < nchunks && q < k + kNS; ++q) mbar_wait_bounded(&bar[q % kNS], (uint32_t)((q / kNS) & 1));
-        }
-        return;
-    }
-    const float acc = (s0 + s1) + (s2 + s3);
-    const int row = t.rb + tid;
-    if (row >= t.re) return;
-    if (DIR == 0) {
-        if (t.kind == 0) P.ynew[c0 + row] = acc;
-        else P.upd[P.upd_off[J] + (row - nj)] = vec[row] + acc;
-    } else {
-        P.xnew[c0 + row] = acc;
-        x_old[P.perm[c0 + row]] = acc;
+    const int c0 = P.col0[J];
+    const long long uo = P.upd_off[J];
+#pragma unroll
+    for (int q = 0; q < MQ; ++q) {
+        const int r = q * 32 + lane;
+        if (r >= m) continue;
+        if (r < nj) P.ynew[c0 + r] = acc[q];
+        else P.upd[uo + (r - nj)] = f[r] + acc[q];
     }
 }
 
-constexpr int kBwdCols = 8;   // columns per backward warp task
-
-// Forward rows [32*part, 32*part+32) of a warp-resident front: y (rows < nj)
-// or the update vector f_R - W f_J (rows >= nj).  Linv is lower triangular,
-// so rows below 32*part+32 need columns < 32*part+32 only.
-__global__ void __launch_bounds__(32 * kWarps) sn_front_forward_kernel(PlanView P, const SnFront* __restrict__ fronts,
-                                                                      int nf, const float* __restrict__ b_old) {
-    __shared__ float sf[kWarps][kSmallM];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int idx = blockIdx.x * kWarps + w;
-    if (idx >= nf) return;
-    const SnFront F = fronts[idx];
-    const int J = F.front, m = F.m, nj = F.nj, c0 = P.col0[J];
-    float* f = sf[w];
+__device__ void warp_forward(const PlanView& P, int J, float* f, int lane, const float* b_old, int* done) {
+    const int nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
+    const int cb = P.child_ptr[J], ce = P.child_ptr[J + 1];
+    if (lane == 0) {
+        bool ok = true;
+        for (int c = cb; c < ce; ++c) ok &= wait_at_least(done + P.child[c], P.ntf[P.child[c]], P.err);
+        if (!ok) atomicExch(P.err, 1);
+    }
+    __syncwarp();
     for (int i = lane; i < m; i += 32) f[i] = (i < nj) ? b_old[P.perm[c0 + i]] : 0.0f;
     __syncwarp();
-    for (int c = P.child_ptr[J]; c < P.child_ptr[J + 1]; ++c) {
+    for (int c = cb; c < ce; ++c) {
         const int C = P.child[c];
         const int mc = P.nrow[C];
         const float* uc = P.upd + P.upd_off[C];
         const int* rm = P.relmap + P.relmap_off[C];
-        for (int k = lane; k < mc; k += 32) f[rm[k]] += uc[k];
+        for (int k = lane; k < mc; k += 32) f[rm[k]] += __ldcg(uc + k);
         __syncwarp();
     }
-    const float* A = P.fw + F.off;
-    const int r = 32 * F.part + lane;
-    const bool rv = r < m;
-    const int cend = min(nj, 32 * F.part + 32);
-    float acc = 0.0f;
-#pragma unroll 2
-    for (int c = 0; c < cend; c += 8) {
-#pragma unroll
-        for (int t = 0; t < 8; ++t)
-            if (rv && c + t < cend) acc = fmaf(A[(size_t)(c + t) * m + r], f[c + t], acc);
-    }
-    if (!rv) return;
-    if (r < nj) P.ynew[c0 + r] = acc;
-    else P.upd[P.upd_off[J] + (r - nj)] = f[r] + acc;
+    if (m <= 64) warp_forward_rows<2>(P, J, m, nj, f, lane);
+    else if (m <= 128) warp_forward_rows<4>(P, J, m, nj, f, lane);
+    else warp_forward_rows<8>(P, J, m, nj, f, lane);
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) atomicAdd(done + J, 1);
 }
 
-// Backward columns [kBwdCols*part, +kBwdCols) of a warp-resident front:
-// x_a = sum_{r >= a} Fw(r, a) g_r with g = [y_J; x_R].
-__global__ void __launch_bounds__(32 * kWarps) sn_front_backward_kernel(PlanView P, const SnFront* __restrict__ fronts,
-                                                                       int nf, float* __restrict__ x_old) {
-    __shared__ float sg[kWarps][kSmallM];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int idx = blockIdx.x * kWarps + w;
-    if (idx >= nf) return;
-    const SnFront F = fronts[idx];
-    const int J = F.front, m = F.m, nj = F.nj, c0 = P.col0[J];
-    const int* rows = P.rows + P.rows_off[J];
-    float* g = sg[w];
-    const int a0 = kBwdCols * F.part;
-    for (int i = (a0 & ~31) + lane; i < m; i += 32) g[i] = (i < nj) ? P.ynew[c0 + i] : P.xnew[rows[i - nj]];
-    __syncwarp();
-    const float* A = P.fw + F.off;
-    float sacc[kBwdCols];
-#pragma unroll
-    for (int t = 0; t < kBwdCols; ++t) sacc[t] = 0.0f;
-    for (int r0 = a0 & ~31; r0 < m; r0 += 32) {
-        const int r = r0 + lane;
-        if (r >= m) continue;
-        const float gr = g[r];
-#pragma unroll
-        for (int t = 0; t < kBwdCols; ++t)
-            if (a0 + t < nj && r >= a0 + t) sacc[t] = fmaf(A[(size_t)(a0 + t) * m + r], gr, sacc[t]);
+// Backward solve of one small front by one warp: x_a = sum_{r >= a} Fw(r, a) g_r.
+__device__ void warp_backward(const PlanView& P, int J, float* g, int lane, float* x_old, int* done) {
+    const int nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
+    if (lane == 0) {
+        const int p = P.parent[J];
+        if (p >= 0 && !wait_at_least(done + p, P.ntb[p], P.err)) atomicExch(P.err, 1);
     }
+    __syncwarp();
+    const int* rows = P.rows + P.rows_off[J];
+    for (int i = lane; i < m; i += 32) g[i] = (i < nj) ? P.ynew[c0 + i] : __ldcg(P.xnew + rows[i - nj]);
+    __syncwarp();
+    const size_t ld = (size_t)((m + 3) & ~3);
+    const float* A = P.fw + P.fw_off[J];
+    for (int a = 0; a < nj; a += 4) {
+        float s4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll 4
+        for (int r = (a & ~31) + lane; r < m; r += 32) {
+            const float gr = g[r];
 #pragma unroll
-    for (int t = 0; t < kBwdCols; ++t)
+            for (int j = 0; j < 4; ++j)
+                if (a + j < nj && r >= a + j) s4[j] = fmaf(__ldg(A + (size_t)(a + j) * ld + r), gr, s4[j]);
+        }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) sacc[t] += __shfl_xor_sync(0xffffffffu, sacc[t], o);
+        for (int j = 0; j < 4; ++j)
 #pragma unroll
-    for (int t = 0; t < kBwdCols; ++t) {
-        if (lane == t && a0 + t < nj) {
-            P.xnew[c0 + a0 + t] = sacc[t];
-            x_old[P.perm[c0 + a0 + t]] = sacc[t];
+            for (int o = 16; o > 0; o >>= 1) s4[j] += __shfl_xor_sync(0xffffffffu, s4[j], o);
+        if (lane == 0) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (a + j < nj) {
+                    P.xnew[c0 + a + j] = s4[j];
+                    x_old[P.perm[c0 + a + j]] = s4[j];
+                }
         }
     }
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) atomicAdd(done + J, 1);
 }
 
-size_t task_smem(int max_front) {
-    return (size_t)kNS * kCB * kTR * sizeof(float) + kNS * sizeof(uint64_t) + (size_t)max_front * sizeof(float);
+__global__ void __launch_bounds__(kNT) sn_forward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks,
+                                                         const float* __restrict__ b_old) {
+    extern __shared__ float sh[];
+    float* f = sh;                 // the front's input vector, m entries
+    float* red = sh + P.max_m;     // column-slice partial sums, kNT entries
+    __shared__ int s_ticket, s_last;
+    int* done = P.ctr + 2;
+    int* chunk_ctr = P.ctr + 2 + 2 * P.nsn;
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) s_ticket = atomicAdd(P.ctr + 0, 1);
+        __syncthreads();
+        const int t = s_ticket;
+        if (t >= ntasks) break;
+        const SnTask T = tasks[t];
+        if (T.front < 0) {
+            const int w = tid >> 5;
+            if (w < T.rows) warp_forward(P, P.bfwd[T.r0 + w], sh + w * kSmallM, tid & 31, b_old, done);
+            __syncthreads();
+            continue;
+        }
+        const int J = T.front, nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
+        const int cb = P.child_ptr[J], ce = P.child_ptr[J + 1];
+        if (tid == 0) {
+            bool ok = true;
+            for (int c = cb; c < ce; ++c) ok &= wait_at_least(done + P.child[c], P.ntf[P.child[c]], P.err);
+            if (!ok) atomicExch(P.err, 1);
+        }
+        __syncthreads();
+        for (int i = tid; i < m; i += kNT) f[i] = (i < nj) ? b_old[P.perm[c0 + i]] : 0.0f;
+        __syncthreads();
+        for (int c = cb; c < ce; ++c) {
+            const int C = P.child[c];
+            const int mc = P.nrow[C];
+            const float* uc = P.upd + P.upd_off[C];
+            const int* rm = P.relmap + P.relmap_off[C];
+            for (int k = tid; k < mc; k += kNT) f[rm[k]] += __ldcg(uc + k);
+            __syncthreads();
+        }
+        // Row lanes x column slices.
+        const int mr = (T.rows + 31) & ~31;
+        const int ks = kNT / mr;
+        const int sl = tid / mr, lr = tid - sl * mr;
+        const int row = T.r0 + lr;
+        const bool active = sl < ks && lr < T.rows;
+        float acc = 0.0f;
+        if (active) {
+            const int cs = (T.ncols + ks - 1) / ks;
+            const int cbeg = T.c0 + sl * cs;
+            int cend = min(T.c0 + T.ncols, cbeg + cs);
+            if (row < nj) cend = min(cend, row + 1);  // L_JJ^{-1} is lower triangular
+            const size_t ld = (size_t)((m + 3) & ~3);
+            const float* A = P.fw + P.fw_off[J] + row;
+            int c = cbeg;
+            for (; c + 8 <= cend; c += 8) {
+                float v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) v[u] = __ldg(A + (size_t)(c + u) * ld);
+#pragma unroll
+                for (int u = 0; u < 8; ++u) acc = fmaf(v[u], f[c + u], acc);
+            }
+            for (; c < cend; ++c) acc = fmaf(__ldg(A + (size_t)c * ld), f[c], acc);
+        }
+        if (ks > 1) {
+            if (sl < ks) red[tid] = acc;
+            __syncthreads();
+            if (sl == 0 && lr < T.rows) {
+                float s2 = red[lr];
+                for (int q = 1; q < ks; ++q) s2 += red[q * mr + lr];
+                acc = s2;
+            }
+        }
+        const bool mine = sl == 0 && lr < T.rows;
+        if (T.nk == 1) {
+            if (mine) {
+                if (row < nj) P.ynew[c0 + row] = acc;
+                else P.upd[P.upd_off[J] + (row - nj)] = f[row] + acc;
+            }
+        } else {
+            if (mine) P.part[T.part + (size_t)T.k * kRB + lr] = acc;
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) s_last = (atomicAdd(chunk_ctr + T.chunk, 1) == T.nk - 1);
+            __syncthreads();
+            if (s_last) {
+                __threadfence();
+                if (mine) {
+                    float s2 = 0.0f;
+                    for (int k = 0; k < T.nk; ++k) s2 += __ldcg(P.part + T.part + (size_t)k * kRB + lr);
+                    if (row < nj) P.ynew[c0 + row] = s2;
+                    else P.upd[P.upd_off[J] + (row - nj)] = f[row] + s2;
+                }
+            }
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) atomicAdd(done + J, 1);
+    }
+}
+
+__global__ void __launch_bounds__(kNT) sn_backward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks,
+                                                          float* __restrict__ x_old) {
+    extern __shared__ float g[];   // [y_J; x_R], m entries
+    __shared__ int s_ticket;
+    int* done = P.ctr + 2 + P.nsn;
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    for (;;) {
+        if (tid == 0) s_ticket = atomicAdd(P.ctr + 1, 1);
+        __syncthreads();
+        const int t = s_ticket;
+        if (t >= ntasks) break;
+        const SnTask T = tasks[t];
+        if (T.front < 0) {
+            if (w < T.rows) warp_backward(P, P.bbwd[T.r0 + w], g + w * kSmallM, lane, x_old, done);
+            __syncthreads();
+            continue;
+        }
+        const int J = T.front, nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
+        if (tid == 0) {
+            const int p = P.parent[J];
+            if (p >= 0 && !wait_at_least(done + p, P.ntb[p], P.err)) atomicExch(P.err, 1);
+        }
+        __syncthreads();
+        const int a0 = T.r0, na = T.rows;
+        const int rs = a0 & ~31;
+        const int* rows = P.rows + P.rows_off[J];
+        for (int i = rs + tid; i < m; i += kNT) g[i] = (i < nj) ? P.ynew[c0 + i] : __ldcg(P.xnew + rows[i - nj]);
+        __syncthreads();
+        const size_t ld = (size_t)((m + 3) & ~3);
+        const float* A = P.fw + P.fw_off[J];
+        float s4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        const int amin = a0 + w;
+        if (amin < a0 + na) {
+#pragma unroll 4
+            for (int r = (amin & ~31) + lane; r < m; r += 32) {
+                const float gr = g[r];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int a = amin + 8 * j;
+                    if (a < a0 + na && r >= a) s4[j] = fmaf(__ldg(A + (size_t)a * ld + r), gr, s4[j]);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s4[j] += __shfl_xor_sync(0xffffffffu, s4[j], o);
+        if (lane == 0) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int a = amin + 8 * j;
+                if (a < a0 + na) {
+                    P.xnew[c0 + a] = s4[j];
+                    x_old[P.perm[c0 + a]] = s4[j];
+                }
+            }
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) atomicAdd(done + J, 1);
+    }
+}
+
+size_t forward_smem(int max_m) { return (size_t)std::max(max_m + kNT, kWarps * kSmallM) * sizeof(float); }
+size_t backward_smem(int max_m) { return (size_t)std::max(max_m, kWarps * kSmallM) * sizeof(float); }
+
+// The dynamic shared-memory limit of the two kernels only ever grows, so a
+// plan built later with smaller fronts cannot invalidate an earlier plan's
+// launches.
+std::mutex g_smem_mu;
+int g_smem_limit[64] = {0};
+void raise_smem_limit(int device, int bytes) {
+    std::lock_guard<std::mutex> lock(g_smem_mu);
+    if (device < 0 || device >= 64) throw Error(HDD_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    if (bytes <= g_smem_limit[device]) return;
+    dev::ck(cudaFuncSetAttribute(sn_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "smem attr");
+    dev::ck(cudaFuncSetAttribute(sn_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "smem attr");
+    g_smem_limit[device] = bytes;
 }
 
 }  // namespace
@@ -269,7 +378,7 @@ size_t task_smem(int max_front) {
 void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::vector<int>& offsets, cudaStream_t s) {
     release();
     std::vector<int> col0, ncol, nrow, rows, child_ptr{0}, child, relmap, perm, height, depth, parent_g;
-    std::vector<long long> rows_off, relmap_off, upd_off;
+    std::vector<long long> rows_off, relmap_off, upd_off, fw_off;
     n = 0;
     for (size_t f = 0; f < factors.size(); ++f) n = std::max(n, offsets[f] + factors[f]->n);
     perm.assign(n, 0);
@@ -293,117 +402,113 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
             }
         }
     }
+    if (nsn == 0) return;
     height.assign(nsn, 0);
     depth.assign(nsn, 0);
     for (int g = 0; g < nsn; ++g)
         if (parent_g[g] >= 0) height[parent_g[g]] = std::max(height[parent_g[g]], height[g] + 1);
     for (int g = nsn - 1; g >= 0; --g)
         if (parent_g[g] >= 0) depth[g] = depth[parent_g[g]] + 1;
-    long long upd_total = 0;
+    long long upd_total = 0, fw_total = 0;
     max_front = 0;
     for (int g = 0; g < nsn; ++g) {
         const SnFactor& F = *factors[where[g].first];
         const int j = where[g].second, off = offsets[where[g].first];
-        const int nj = F.ncol[j], nr = (int)F.rows[j].size();
+        const int nj = F.ncol[j], nr = (int)F.rows[j].size(), m = nj + nr;
         col0.push_back(off + F.col0[j]);
         ncol.push_back(nj);
         nrow.push_back(nr);
-        max_front = std::max(max_front, nj + nr);
+        max_front = std::max(max_front, m);
         rows_off.push_back((long long)rows.size());
         for (int r : F.rows[j]) rows.push_back(off + r);
         upd_off.push_back(upd_total);
         upd_total += nr;
+        fw_off.push_back(fw_total);
+        fw_total += (long long)((m + 3) & ~3) * nj;
     }
-    // Tasks per level and their blocks.
-    int hmax = 0, dmax = 0;
-    for (int g = 0; g < nsn; ++g) { hmax = std::max(hmax, height[g]); dmax = std::max(dmax, depth[g]); }
+    // Tasks in topological order.
+    std::vector<int> order(nsn);
+    for (int g = 0; g < nsn; ++g) order[g] = g;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return height[a] < height[b]; });
     std::vector<SnTask> ftasks, btasks;
-    long long total = 0;
-    auto add = [&](std::vector<SnTask>& v, int g, int rb, int re, int kind, int cb, int nc) {
+    std::vector<int> ntf(nsn, 0), ntb(nsn, 0), bfwd, bbwd;
+    int nchunk = 0;
+    long long part_total = 0;
+    // Small fronts of one level go in bundles of kWarps, one warp each.
+    auto flush = [](std::vector<SnTask>& tasks, std::vector<int>& list, int& first) {
+        if ((int)list.size() == first) return;
         SnTask t;
-        t.front = g; t.rb = rb; t.re = re; t.kind = kind; t.col_base = cb; t.ncols = nc; t.pad0 = t.pad1 = 0;
-        t.blk = total;
-        total += (long long)nc * kTR;
-        v.push_back(t);
+        t.front = -1; t.r0 = first; t.rows = (int)list.size() - first; t.c0 = 0; t.ncols = 0;
+        t.k = 0; t.nk = 1; t.chunk = -1; t.part = 0;
+        tasks.push_back(t);
+        first = (int)list.size();
     };
-    // Warp-resident fronts: one Fw block each, 16-byte aligned.
-    std::vector<long long> small_off(nsn, -1);
-    long long fw_total = 0;
-    int big_front = 0;
-    for (int g = 0; g < nsn; ++g) {
-        const int m = ncol[g] + nrow[g];
-        if (m <= kSmallM) {
-            small_off[g] = fw_total;
-            fw_total += ((long long)m * ncol[g] + 3) & ~3LL;
-        } else big_front = std::max(big_front, m);
-    }
-    std::vector<SnFront> sfwd, sbwd;
-    auto small_front = [&](int g, int part) {
-        SnFront f;
-        f.front = g; f.m = ncol[g] + nrow[g]; f.nj = ncol[g]; f.part = part; f.off = small_off[g];
-        return f;
-    };
-    fwd_ptr.assign(1, 0);
-    sfwd_ptr.assign(1, 0);
-    for (int h = 0; h <= hmax; ++h) {
-        for (int g = 0; g < nsn; ++g) {
-            if (height[g] != h) continue;
-            const int nj = ncol[g], nr = nrow[g];
-            if (small_off[g] >= 0) {
-                for (int q = 0; q * 32 < nj + nr; ++q) sfwd.push_back(small_front(g, q));
-                continue;
-            }
-            for (int r0 = 0; r0 < nj; r0 += kTR) add(ftasks, g, r0, std::min(r0 + kTR, nj), 0, 0, std::min(r0 + kTR, nj));
-            for (int r0 = nj; r0 < nj + nr; r0 += kTR) add(ftasks, g, r0, std::min(r0 + kTR, nj + nr), 1, 0, nj);
+    // Bundles pay off where a level has many small fronts (throughput); on
+    // narrow levels a whole CTA per front keeps the dependency chain short.
+    std::vector<int> small_h(nsn + 1, 0), small_d(nsn + 1, 0);
+    for (int g = 0; g < nsn; ++g)
+        if (small_front(ncol[g] + nrow[g], ncol[g])) { ++small_h[height[g]]; ++small_d[depth[g]]; }
+    int bfirst = 0, blevel = -1;
+    for (int g : order) {
+        const int nj = ncol[g], m = nj + nrow[g];
+        if (height[g] != blevel) { flush(ftasks, bfwd, bfirst); blevel = height[g]; }
+        if (small_front(m, nj) && small_h[height[g]] >= kBundleLevel) {
+            bfwd.push_back(g);
+            ntf[g] = 1;
+            if ((int)bfwd.size() - bfirst == kWarps) flush(ftasks, bfwd, bfirst);
+            continue;
         }
-        fwd_ptr.push_back((int)ftasks.size());
-        sfwd_ptr.push_back((int)sfwd.size());
-    }
-    bwd_ptr.assign(1, 0);
-    sbwd_ptr.assign(1, 0);
-    for (int d = 0; d <= dmax; ++d) {
-        for (int g = 0; g < nsn; ++g) {
-            if (depth[g] != d) continue;
-            const int nj = ncol[g], nr = nrow[g];
-            if (small_off[g] >= 0) {
-                for (int q = 0; q * kBwdCols < nj; ++q) sbwd.push_back(small_front(g, q));
-                continue;
+        for (int r0 = 0; r0 < m; r0 += kRB) {
+            const int rowsb = std::min(kRB, m - r0);
+            const int cend = std::min(nj, r0 + kRB);
+            const int nk = std::max(1, (cend + kCC - 1) / kCC);
+            const int chunk = nk > 1 ? nchunk++ : -1;
+            const long long part = nk > 1 ? part_total : 0;
+            if (nk > 1) part_total += (long long)nk * kRB;
+            for (int k = 0; k < nk; ++k) {
+                SnTask t;
+                t.front = g; t.r0 = r0; t.rows = rowsb; t.c0 = k * kCC;
+                t.ncols = std::min(kCC, cend - k * kCC); t.k = k; t.nk = nk; t.chunk = chunk; t.part = part;
+                ftasks.push_back(t);
+                ++ntf[g];
             }
-            for (int r0 = 0; r0 < nj; r0 += kTR) add(btasks, g, r0, std::min(r0 + kTR, nj), 2, r0, nj + nr - r0);
         }
-        bwd_ptr.push_back((int)btasks.size());
-        sbwd_ptr.push_back((int)sbwd.size());
     }
+    flush(ftasks, bfwd, bfirst);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return depth[a] < depth[b]; });
+    bfirst = 0;
+    blevel = -1;
+    for (int g : order) {
+        const int nj = ncol[g], m = nj + nrow[g];
+        if (depth[g] != blevel) { flush(btasks, bbwd, bfirst); blevel = depth[g]; }
+        if (small_front(m, nj) && small_d[depth[g]] >= kBundleLevel) {
+            bbwd.push_back(g);
+            ntb[g] = 1;
+            if ((int)bbwd.size() - bfirst == kWarps) flush(btasks, bbwd, bfirst);
+            continue;
+        }
+        for (int a0 = 0; a0 < nj; a0 += kBC) {
+            SnTask t;
+            t.front = g; t.r0 = a0; t.rows = std::min(kBC, nj - a0); t.c0 = 0; t.ncols = 0;
+            t.k = 0; t.nk = 1; t.chunk = -1; t.part = 0;
+            btasks.push_back(t);
+            ++ntb[g];
+        }
+    }
+    flush(btasks, bbwd, bfirst);
+    n_fwd = (int)ftasks.size();
+    n_bwd = (int)btasks.size();
+    n_ctr = 2 + 2 * nsn + nchunk;
     std::vector<float> fw((size_t)std::max<long long>(fw_total, 4), 0.0f);
 #pragma omp parallel for schedule(dynamic)
     for (int g = 0; g < nsn; ++g) {
-        if (small_off[g] < 0) continue;
         const SnFactor& F = *factors[where[g].first];
-        const std::vector<double>& W = F.Fw[where[g].second];
-        float* dst = &fw[(size_t)small_off[g]];
-        for (size_t i = 0; i < W.size(); ++i) dst[i] = (float)W[i];
+        const std::vector<double>& W = F.Fw[where[g].second];  // m x nj, col-major
+        const int nj = ncol[g], m = nj + nrow[g], ld = (m + 3) & ~3;
+        float* dst = &fw[(size_t)fw_off[g]];
+        for (int c = 0; c < nj; ++c)
+            for (int r = 0; r < m; ++r) dst[(size_t)c * ld + r] = (float)W[(size_t)c * m + r];
     }
-    std::vector<float> val((size_t)total, 0.0f);
-    auto fill = [&](const std::vector<SnTask>& v, bool forward) {
-#pragma omp parallel for schedule(dynamic)
-        for (long q = 0; q < (long)v.size(); ++q) {
-            const SnTask& t = v[q];
-            const SnFactor& F = *factors[where[t.front].first];
-            const int j = where[t.front].second;
-            const int m = ncol[t.front] + nrow[t.front];
-            const std::vector<double>& W = F.Fw[j];  // (m x nj), col-major: W[c*m + r]
-            float* blk = &val[(size_t)t.blk];
-            for (int c = 0; c < t.ncols; ++c)
-                for (int r = t.rb; r < t.re; ++r) {
-                    const int a = t.col_base + c;
-                    // forward: M(r, a) = Fw(r, a); backward: M(r, a) = Fw(a, r)
-                    const double v2 = forward ? W[(size_t)a * m + r] : W[(size_t)r * m + a];
-                    blk[(size_t)c * kTR + (r - t.rb)] = (float)v2;
-                }
-        }
-    };
-    fill(ftasks, true);
-    fill(btasks, false);
     // Children lists and relative maps (child row -> position in parent's front).
     relmap_off.assign(nsn, 0);
     for (int g = 0; g < nsn; ++g) {
@@ -430,14 +535,13 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
             relmap.push_back(posn);
         }
     }
-    if (nsn == 0) return;
-    max_front = std::max(big_front, 1);
-    if (task_smem(max_front) > 227 * 1024)
+    if (forward_smem(max_front) > 200 * 1024)
         throw Error(HDD_ERR_UNSUPPORTED, "supernodal front too large for shared memory: " + std::to_string(max_front));
     bytes = 0;
     d_col0 = dev::upload(col0, s, bytes);
     d_ncol = dev::upload(ncol, s, bytes);
     d_nrow = dev::upload(nrow, s, bytes);
+    d_parent = dev::upload(parent_g, s, bytes);
     d_rows = dev::upload(rows.empty() ? std::vector<int>{0} : rows, s, bytes);
     d_rows_off = dev::upload(rows_off, s, bytes);
     d_child_ptr = dev::upload(child_ptr, s, bytes);
@@ -445,66 +549,57 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
     d_relmap_off = dev::upload(relmap_off, s, bytes);
     d_relmap = dev::upload(relmap.empty() ? std::vector<int>{0} : relmap, s, bytes);
     d_upd_off = dev::upload(upd_off, s, bytes);
+    d_fw_off = dev::upload(fw_off, s, bytes);
+    d_ntf = dev::upload(ntf, s, bytes);
+    d_ntb = dev::upload(ntb, s, bytes);
     d_perm = dev::upload(perm, s, bytes);
-    d_fwd = dev::upload(ftasks.empty() ? std::vector<SnTask>(1) : ftasks, s, bytes);
-    d_bwd = dev::upload(btasks.empty() ? std::vector<SnTask>(1) : btasks, s, bytes);
-    d_val = dev::upload(val.empty() ? std::vector<float>(4, 0.0f) : val, s, bytes);
-    d_sfwd = dev::upload(sfwd.empty() ? std::vector<SnFront>(1) : sfwd, s, bytes);
-    d_sbwd = dev::upload(sbwd.empty() ? std::vector<SnFront>(1) : sbwd, s, bytes);
+    d_fwd = dev::upload(ftasks, s, bytes);
+    d_bwd = dev::upload(btasks, s, bytes);
+    d_bfwd = dev::upload(bfwd.empty() ? std::vector<int>{0} : bfwd, s, bytes);
+    d_bbwd = dev::upload(bbwd.empty() ? std::vector<int>{0} : bbwd, s, bytes);
     d_fw = dev::upload(fw, s, bytes);
+    d_part = dev::alloc_zero<float>(std::max<long long>(part_total, 1), bytes);
     d_upd = dev::alloc_zero<float>(std::max<long long>(upd_total, 1), bytes);
     d_ynew = dev::alloc_zero<float>(std::max(n, 1), bytes);
     d_xnew = dev::alloc_zero<float>(std::max(n, 1), bytes);
+    d_ctr = dev::alloc_zero<int>(n_ctr, bytes);
     d_err = dev::alloc_zero<int>(1, bytes);
+    // Persistent grid: as many CTAs as fit on the device, but no more than tasks.
+    int dev_id = 0, nsm = 0, bf = 0, bb = 0;
+    dev::ck(cudaGetDevice(&dev_id), "cudaGetDevice");
+    dev::ck(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev_id), "SM count");
+    const size_t smf = forward_smem(max_front), smb = backward_smem(max_front);
+    raise_smem_limit(dev_id, (int)smf);
+    dev::ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, sn_forward_kernel, kNT, smf), "occupancy");
+    dev::ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, sn_backward_kernel, kNT, smb), "occupancy");
+    grid = std::max(1, nsm * std::max(1, std::min(bf, bb)));
     dev::ck(cudaStreamSynchronize(s), "plan upload");
 }
 
 void SolvePlan::release() {
-    dev::release(d_col0); dev::release(d_ncol); dev::release(d_nrow);
+    dev::release(d_col0); dev::release(d_ncol); dev::release(d_nrow); dev::release(d_parent);
     dev::release(d_rows); dev::release(d_rows_off); dev::release(d_child_ptr); dev::release(d_child);
-    dev::release(d_relmap_off); dev::release(d_relmap); dev::release(d_upd_off); dev::release(d_perm);
-    dev::release(d_fwd); dev::release(d_bwd); dev::release(d_val); dev::release(d_upd); dev::release(d_ynew);
-    dev::release(d_xnew); dev::release(d_err);
-    dev::release(d_sfwd); dev::release(d_sbwd); dev::release(d_fw);
+    dev::release(d_relmap_off); dev::release(d_relmap); dev::release(d_upd_off); dev::release(d_fw_off);
+    dev::release(d_ntf); dev::release(d_ntb); dev::release(d_perm);
+    dev::release(d_fwd); dev::release(d_bwd); dev::release(d_bfwd); dev::release(d_bbwd); dev::release(d_fw); dev::release(d_part); dev::release(d_upd);
+    dev::release(d_ynew); dev::release(d_xnew); dev::release(d_ctr); dev::release(d_err);
     nsn = 0;
     n = 0;
+    n_fwd = n_bwd = n_ctr = 0;
 }
 
 void SolvePlan::solve(const float* b_old, float* x_old, cudaStream_t s, long long& launches) const {
     if (nsn == 0) return;
-    PlanView P{d_col0, d_ncol, d_nrow, d_rows, d_rows_off, d_child_ptr, d_child, d_relmap_off, d_relmap,
-               d_upd_off, d_perm, d_val, d_fw, d_upd, d_ynew, d_xnew, d_err};
-    const size_t smem = task_smem(max_front);
-    if (smem > 48 * 1024) {
-        dev::ck(cudaFuncSetAttribute(sn_task_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attr");
-        dev::ck(cudaFuncSetAttribute(sn_task_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attr");
-    }
-    for (size_t h = 0; h + 1 < fwd_ptr.size(); ++h) {
-        const int ns = sfwd_ptr[h + 1] - sfwd_ptr[h];
-        if (ns) {
-            sn_front_forward_kernel<<<(ns + kWarps - 1) / kWarps, 32 * kWarps, 0, s>>>(P, d_sfwd + sfwd_ptr[h], ns, b_old);
-            dev::ck(cudaGetLastError(), "sn front forward");
-            ++launches;
-        }
-        const int cnt = fwd_ptr[h + 1] - fwd_ptr[h];
-        if (!cnt) continue;
-        sn_task_kernel<0><<<cnt, kTR, smem, s>>>(P, d_fwd + fwd_ptr[h], b_old, x_old);
-        dev::ck(cudaGetLastError(), "sn forward");
-        ++launches;
-    }
-    for (size_t d = 0; d + 1 < bwd_ptr.size(); ++d) {
-        const int ns = sbwd_ptr[d + 1] - sbwd_ptr[d];
-        if (ns) {
-            sn_front_backward_kernel<<<(ns + kWarps - 1) / kWarps, 32 * kWarps, 0, s>>>(P, d_sbwd + sbwd_ptr[d], ns, x_old);
-            dev::ck(cudaGetLastError(), "sn front backward");
-            ++launches;
-        }
-        const int cnt = bwd_ptr[d + 1] - bwd_ptr[d];
-        if (!cnt) continue;
-        sn_task_kernel<1><<<cnt, kTR, smem, s>>>(P, d_bwd + bwd_ptr[d], b_old, x_old);
-        dev::ck(cudaGetLastError(), "sn backward");
-        ++launches;
-    }
+    PlanView P{nsn, max_front, d_col0, d_ncol, d_nrow, d_parent, d_rows, d_rows_off, d_child_ptr, d_child,
+               d_relmap_off, d_relmap, d_upd_off, d_fw_off, d_ntf, d_ntb, d_perm, d_bfwd, d_bbwd, d_fw, d_part, d_upd,
+               d_ynew,
+               d_xnew, d_ctr, d_err};
+    dev::ck(cudaMemsetAsync(d_ctr, 0, sizeof(int) * n_ctr, s), "reset counters");
+    sn_forward_kernel<<<std::min(grid, n_fwd), kNT, forward_smem(max_front), s>>>(P, d_fwd, n_fwd, b_old);
+    dev::ck(cudaGetLastError(), "sn forward");
+    sn_backward_kernel<<<std::min(grid, n_bwd), kNT, backward_smem(max_front), s>>>(P, d_bwd, n_bwd, x_old);
+    dev::ck(cudaGetLastError(), "sn backward");
+    launches += 2;
 }
 
 int SolvePlan::error_flag(cudaStream_t s) const {
