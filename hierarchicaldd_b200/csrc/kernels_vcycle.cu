@@ -83,7 +83,7 @@ constexpr int kWarpCH = 1;
 
 // mode: 1 = boundary cells, 2 = interior (non-boundary) cells, 3 = all Active.
 template <int CH, class G>
-__device__ void jacobi_sweep(const G& g, const LevelSmem& L, int mode, const float* inv_diag) {
+__device__ __noinline__ void jacobi_sweep(const G& g, const LevelSmem& L, int mode, const float* inv_diag) {
     const int m = L.e - 2;
     const int ncell = m * m * m;
     float rr[CH];
@@ -114,6 +114,65 @@ __device__ void jacobi_sweep(const G& g, const LevelSmem& L, int mode, const flo
         }
     }
     g.sync();
+}
+
+// Jacobi sweep of a whole box level with one x-line (NX cells) per thread of
+// g: no index division per cell and the line's residuals in registers.  The
+// per-cell arithmetic is cell_residual's, so results equal jacobi_sweep's.
+template <int NX, class G>
+__device__ __noinline__ void box_line_sweep(const G& g, const LevelSmem& L, int mode, const float* inv_diag) {
+    constexpr int e = NX + 2, PS = e * e;
+    const int t = g.rank();
+    float rr[NX];
+    uint32_t tk = 0;
+    int base = 0;
+    if (t < NX * NX) {
+        const int y = t / NX + 1, z = t % NX + 1;
+        base = PS + y * e + z;
+#pragma unroll
+        for (int k = 0; k < NX; ++k) {
+            const int i = base + k * PS;
+            const uint32_t fl = L.f[i];
+            const bool active = fl & C_ACTIVE;
+            const bool bnd = fl & C_BOUNDARY8;
+            const bool take = active && ((mode == 3) || (mode == 1 && bnd) || (mode == 2 && !bnd));
+            rr[k] = 0.0f;
+            if (take) {
+                tk |= 1u << k;
+                rr[k] = cell_residual(L, i, fl);
+            }
+        }
+    }
+    g.sync();
+    if (tk) {
+#pragma unroll
+        for (int k = 0; k < NX; ++k) {
+            if (tk & (1u << k)) {
+                const int i = base + k * PS;
+                const float w = inv_diag[__popc((uint32_t)L.f[i] & C_FACES)];
+                L.u[i] = __fadd_rn(L.u[i], __fmul_rn(w, rr[k]));
+            }
+        }
+    }
+    g.sync();
+}
+
+// One Jacobi sweep of a box level; levels up to 17^3 cells use one x-line
+// per thread, larger ones the chunked sweep.
+template <int CH, class G>
+__device__ void sweep_box(const G& g, const LevelSmem& L, int mode, const float* inv_diag) {
+    const int m = L.e - 2;
+    if (m * m > g.size()) {  // more lines than threads
+        jacobi_sweep<CH>(g, L, mode, inv_diag);
+        return;
+    }
+    switch (L.e) {
+        case 3: box_line_sweep<1>(g, L, mode, inv_diag); break;
+        case 5: box_line_sweep<3>(g, L, mode, inv_diag); break;
+        case 9: box_line_sweep<7>(g, L, mode, inv_diag); break;
+        case 17: box_line_sweep<15>(g, L, mode, inv_diag); break;
+        default: jacobi_sweep<CH>(g, L, mode, inv_diag); break;
+    }
 }
 
 // r = b - A u at Active cells (other cells of r keep their zero).
@@ -195,9 +254,58 @@ __device__ void prolongate_level(const G& g, const LevelSmem& F, const LevelSmem
 // Pre/post smoothing of one level: boundary, interior, boundary sweeps.
 template <int CH, class G>
 __device__ void smooth_level(const G& g, const LevelSmem& L, const VcycleArgs& a, const float* inv_diag) {
-    for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(g, L, 1, inv_diag);
-    for (int i = 0; i < a.interior_itr; ++i) jacobi_sweep<CH>(g, L, 2, inv_diag);
-    for (int i = 0; i < a.boundary_itr; ++i) jacobi_sweep<CH>(g, L, 1, inv_diag);
+    for (int i = 0; i < a.boundary_itr; ++i) sweep_box<CH>(g, L, 1, inv_diag);
+    for (int i = 0; i < a.interior_itr; ++i) sweep_box<CH>(g, L, 2, inv_diag);
+    for (int i = 0; i < a.boundary_itr; ++i) sweep_box<CH>(g, L, 1, inv_diag);
+}
+
+// n all-Active Jacobi sweeps of a 5^3 box (3^3 interior cells) by one warp:
+// lane q < 27 holds cell q in a register and takes interior neighbours by
+// shuffle; halo neighbours never change during the sweeps (only Active
+// interior cells are updated), so they are read once.  Same arithmetic and
+// face order as cell_residual, so the result equals n jacobi_sweep calls.
+__device__ __noinline__ void bottom_sweeps_3(const LevelSmem& L, int n, const float* inv_diag) {
+    const int lane = threadIdx.x & 31;
+    const bool own = lane < 27;
+    const int q = own ? lane : 0;
+    const int x = q / 9 + 1, y = (q / 3) % 3 + 1, z = q % 3 + 1;
+    const int i = (x * 5 + y) * 5 + z;
+    const uint32_t fl = own ? (uint32_t)L.f[i] : 0u;
+    const bool act = own && (fl & C_ACTIVE);
+    const float bb = own ? L.b[i] : 0.0f;
+    const float w = inv_diag[__popc(fl & C_FACES)];
+    float u = own ? L.u[i] : 0.0f;
+    // Per face: source lane for an interior neighbour, or the fixed halo value.
+    const int d[6] = {-25, 25, -5, 5, -1, 1};
+    const int dl[6] = {-9, 9, -3, 3, -1, 1};
+    const int cpos[6] = {x, x, y, y, z, z};
+    int src[6];
+    float halo[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int np = cpos[f] + ((f & 1) ? 1 : -1);
+        const bool inside = np >= 1 && np <= 3;
+        src[f] = inside ? q + dl[f] : q;
+        halo[f] = (!inside && own) ? L.u[i + d[f]] : 0.0f;
+        if (inside) halo[f] = 0.0f;
+        src[f] = inside ? src[f] : -1;
+    }
+    for (int it = 0; it < n; ++it) {
+        float nb[6];
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            const float v = __shfl_sync(0xffffffffu, u, src[f] < 0 ? q : src[f]);
+            nb[f] = src[f] < 0 ? halo[f] : v;
+        }
+        float res = 0.0f;
+#pragma unroll
+        for (int f = 0; f < 6; ++f)
+            if (fl & (1u << f)) res = __fsub_rn(res, __fsub_rn(nb[f], u));
+        const float r = __fsub_rn(bb, res);
+        if (act) u = __fadd_rn(u, __fmul_rn(w, r));
+    }
+    if (own) L.u[i] = u;
+    __syncwarp();
 }
 
 // Levels T..Lm-1 of one V-cycle with group g: down-leg from T, bottom
@@ -211,7 +319,9 @@ __device__ void vcycle_tail(const G& g, LevelSmem* lv, int T, int Lm, const Vcyc
         zero_u(g, lv[l + 1]);
         restrict_level(g, lv[l], lv[l + 1], sc64);
     }
-    for (int i = 0; i < a.bottom_itr; ++i) jacobi_sweep<CH>(g, lv[Lm - 1], 3, inv_diag);
+    if (lv[Lm - 1].e == 5 && g.size() == 32) bottom_sweeps_3(lv[Lm - 1], a.bottom_itr, inv_diag);
+    else
+        for (int i = 0; i < a.bottom_itr; ++i) sweep_box<CH>(g, lv[Lm - 1], 3, inv_diag);
     for (int l = Lm - 2; l >= T; --l) {
         prolongate_level(g, lv[l], lv[l + 1], sc8);
         smooth_level<CH>(g, lv[l], a, inv_diag);
@@ -315,7 +425,7 @@ __global__ void __launch_bounds__(NT, 1) vcycle_kernel(VcycleArgs a) {
             if (threadIdx.x < 32) vcycle_tail<kWarpCH>(WarpGroup(), lv, T, Lm, a, s_inv, s_sc64, s_sc8);
             __syncthreads();
         } else {
-            for (int i = 0; i < a.bottom_itr; ++i) jacobi_sweep<CH>(cta, lv[Lm - 1], 3, s_inv);
+            for (int i = 0; i < a.bottom_itr; ++i) sweep_box<CH>(cta, lv[Lm - 1], 3, s_inv);
         }
         for (int l = Tc - 1; l >= 0; --l) {
             prolongate_level(cta, lv[l], lv[l + 1], s_sc8);
@@ -470,77 +580,108 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
     float* nb_hi = (rank < C - 1) ? cluster.map_shared_rank(nxt, rank + 1) : nullptr;
     int par = 0;
 
-    auto cell_of = [&](int q, int& i, int& j, int& lx, int& y, int& z) {
-        lx = q / M2 + 1;
-        const int rem = q % M2;
-        y = rem / (SUB - 1) + 1;
-        z = rem % (SUB - 1) + 1;
-        i = (lx * E + y) * E + z;
-        j = i - PS;
+    // Each thread owns LPT x-lines (y, z) of the slab, np <= P cells each, and
+    // keeps their u, b and flags in registers for the whole V-cycle; shared
+    // memory holds u for the y/z neighbours of other threads.
+    constexpr int LPT = (M2 + NT - 1) / NT;
+    int off[LPT];                 // (y, z) offset within a plane; -1 if no line
+    float uu[LPT][P];             // u of the owned cells (shared memory keeps a copy)
+    float hlo[LPT], hhi[LPT];     // u at x0-1 and x1+1 of the line
+    auto load_lines = [&]() {
+#pragma unroll
+        for (int l = 0; l < LPT; ++l) {
+#pragma unroll
+            for (int k = 0; k < P; ++k) uu[l][k] = (off[l] >= 0 && k < np) ? u0[(k + 1) * PS + off[l]] : 0.0f;
+        }
     };
-    // Store owned boundary planes into the neighbours' next-halo buffers, then
-    // barrier, then adopt the buffers written into this CTA.
-    auto finish_exchange = [&]() {
+#pragma unroll
+    for (int l = 0; l < LPT; ++l) {
+        const int q = threadIdx.x + l * NT;
+        off[l] = -1;
+        hlo[l] = hhi[l] = 0.0f;
+        if (q < M2) {
+            const int y = q / (SUB - 1) + 1, z = q % (SUB - 1) + 1;
+            off[l] = y * E + z;
+            hlo[l] = u0[off[l]];
+            hhi[l] = u0[(np + 1) * PS + off[l]];
+        }
+    }
+    load_lines();
+    auto flag = [&](int l, int k) -> uint32_t { return f0[k * PS + off[l]]; };
+    // b - A u at owned cell k of line l (reference face order -x,+x,-y,+y,-z,+z).
+    auto residual = [&](int l, int k, uint32_t fl) -> float {
+        const float cc = uu[l][k];
+        float xm = hlo[l], xp = hhi[l];
+#pragma unroll
+        for (int kk = 0; kk < P; ++kk) {
+            if (kk == k - 1) xm = uu[l][kk];
+            if (kk == k + 1 && kk < np) xp = uu[l][kk];
+        }
+        const int i = (k + 1) * PS + off[l];
+        float res = 0.0f;
+        if (fl & 0x01u) res = __fsub_rn(res, __fsub_rn(xm, cc));
+        if (fl & 0x02u) res = __fsub_rn(res, __fsub_rn(xp, cc));
+        if (fl & 0x04u) res = __fsub_rn(res, __fsub_rn(u0[i - E], cc));
+        if (fl & 0x08u) res = __fsub_rn(res, __fsub_rn(u0[i + E], cc));
+        if (fl & 0x10u) res = __fsub_rn(res, __fsub_rn(u0[i - 1], cc));
+        if (fl & 0x20u) res = __fsub_rn(res, __fsub_rn(u0[i + 1], cc));
+        return __fsub_rn(b0[k * PS + off[l]], res);
+    };
+    // Send the first/last owned values to the neighbours' halo buffers,
+    // barrier, then take this CTA's new halos.
+    auto exchange = [&]() {
+#pragma unroll
+        for (int l = 0; l < LPT; ++l) {
+            if (off[l] < 0) continue;
+            float last = uu[l][0];
+#pragma unroll
+            for (int k = 0; k < P; ++k)
+                if (k == np - 1) last = uu[l][k];
+            // The low neighbour's high halo is this CTA's first plane, and vice versa.
+            if (rank > 0) nb_lo[(par * 2 + 1) * PS + off[l]] = uu[l][0];
+            if (rank < C - 1) nb_hi[(par * 2 + 0) * PS + off[l]] = last;
+        }
         cluster.sync();
-        float* my_lo = nxt + (par * 2 + 0) * PS;
-        float* my_hi = nxt + (par * 2 + 1) * PS;
-        for (int q = threadIdx.x; q < M2; q += NT) {
-            const int y = q / (SUB - 1) + 1, z = q % (SUB - 1) + 1, o = y * E + z;
-            if (rank > 0) u0[o] = my_lo[o];
-            if (rank < C - 1) u0[(np + 1) * PS + o] = my_hi[o];
+#pragma unroll
+        for (int l = 0; l < LPT; ++l) {
+            if (off[l] < 0) continue;
+            if (rank > 0) hlo[l] = nxt[(par * 2 + 0) * PS + off[l]];
+            if (rank < C - 1) hhi[l] = nxt[(par * 2 + 1) * PS + off[l]];
         }
         par ^= 1;
-        __syncthreads();
-    };
-    auto push_boundary = [&](int lx, int o, float v) {
-        // The low neighbour's high halo is this CTA's first plane, and vice versa.
-        if (lx == 1 && rank > 0) nb_lo[(par * 2 + 1) * PS + o] = v;
-        if (lx == np && rank < C - 1) nb_hi[(par * 2 + 0) * PS + o] = v;
     };
     auto slab_sweep = [&](int mode) {
-        static_assert(CH <= 32, "take mask holds 32 cells per thread");
-        float rr[CH];
-        uint32_t tk = 0;
+        float rr[LPT][P];
+        uint32_t tk[LPT];
 #pragma unroll
-        for (int c = 0; c < CH; ++c) {
-            const int q = threadIdx.x + c * NT;
-            rr[c] = 0.0f;
-            if (q < ncell) {
-                int i, j, lx, y, z;
-                cell_of(q, i, j, lx, y, z);
-                const uint32_t fl = f0[j];
+        for (int l = 0; l < LPT; ++l) {
+            tk[l] = 0u;
+            if (off[l] < 0) continue;
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                rr[l][k] = 0.0f;
+                if (k >= np) continue;
+                const uint32_t fl = flag(l, k);
                 const bool act = fl & C_ACTIVE, bnd = fl & C_BOUNDARY8;
-                const bool take = act && ((mode == 3) || (mode == 1 && bnd) || (mode == 2 && !bnd));
-                if (take) {
-                    tk |= 1u << c;
-                    const float cc = u0[i];
-                    float res = 0.0f, n;
-                    n = u0[i - PS]; if (fl & 0x01u) res = __fsub_rn(res, __fsub_rn(n, cc));
-                    n = u0[i + PS]; if (fl & 0x02u) res = __fsub_rn(res, __fsub_rn(n, cc));
-                    n = u0[i - E];  if (fl & 0x04u) res = __fsub_rn(res, __fsub_rn(n, cc));
-                    n = u0[i + E];  if (fl & 0x08u) res = __fsub_rn(res, __fsub_rn(n, cc));
-                    n = u0[i - 1];  if (fl & 0x10u) res = __fsub_rn(res, __fsub_rn(n, cc));
-                    n = u0[i + 1];  if (fl & 0x20u) res = __fsub_rn(res, __fsub_rn(n, cc));
-                    rr[c] = __fsub_rn(b0[j], res);
+                if (act && ((mode == 3) || (mode == 1 && bnd) || (mode == 2 && !bnd))) {
+                    tk[l] |= 1u << k;
+                    rr[l][k] = residual(l, k, fl);
                 }
             }
         }
         __syncthreads();
 #pragma unroll
-        for (int c = 0; c < CH; ++c) {
-            const int q = threadIdx.x + c * NT;
-            if (q < ncell) {
-                int i, j, lx, y, z;
-                cell_of(q, i, j, lx, y, z);
-                float v = u0[i];
-                if (tk & (1u << c)) {
-                    v = __fadd_rn(v, __fmul_rn(s_inv[__popc((uint32_t)f0[j] & C_FACES)], rr[c]));
-                    u0[i] = v;
+        for (int l = 0; l < LPT; ++l) {
+            if (!tk[l]) continue;
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                if (tk[l] & (1u << k)) {
+                    uu[l][k] = __fadd_rn(uu[l][k], __fmul_rn(s_inv[__popc(flag(l, k) & C_FACES)], rr[l][k]));
+                    u0[(k + 1) * PS + off[l]] = uu[l][k];
                 }
-                push_boundary(lx, y * E + z, v);
             }
         }
-        finish_exchange();
+        exchange();
     };
 
     const int Lm = a.levels;
@@ -553,20 +694,15 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
         for (int i = 0; i < a.interior_itr; ++i) slab_sweep(2);
         for (int i = 0; i < a.boundary_itr; ++i) slab_sweep(1);
         // r = b - A u on owned Active cells (halos are current after the last exchange).
-        for (int q = threadIdx.x; q < ncell; q += NT) {
-            int i, j, lx, y, z;
-            cell_of(q, i, j, lx, y, z);
-            const uint32_t fl = f0[j];
-            if (!(fl & C_ACTIVE)) continue;
-            const float cc = u0[i];
-            float res = 0.0f, n;
-            n = u0[i - PS]; if (fl & 0x01u) res = __fsub_rn(res, __fsub_rn(n, cc));
-            n = u0[i + PS]; if (fl & 0x02u) res = __fsub_rn(res, __fsub_rn(n, cc));
-            n = u0[i - E];  if (fl & 0x04u) res = __fsub_rn(res, __fsub_rn(n, cc));
-            n = u0[i + E];  if (fl & 0x08u) res = __fsub_rn(res, __fsub_rn(n, cc));
-            n = u0[i - 1];  if (fl & 0x10u) res = __fsub_rn(res, __fsub_rn(n, cc));
-            n = u0[i + 1];  if (fl & 0x20u) res = __fsub_rn(res, __fsub_rn(n, cc));
-            r0[j] = __fsub_rn(b0[j], res);
+#pragma unroll
+        for (int l = 0; l < LPT; ++l) {
+            if (off[l] < 0) continue;
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                if (k >= np) continue;
+                const uint32_t fl = flag(l, k);
+                if (fl & C_ACTIVE) r0[k * PS + off[l]] = residual(l, k, fl);
+            }
         }
         __syncthreads();
         cluster.sync();  // r0 of every slab is complete
@@ -615,7 +751,7 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
                 if (threadIdx.x < 32) vcycle_tail<kWarpCH>(WarpGroup(), lv, T, Lm, a, s_inv, s_sc64, s_sc8);
                 __syncthreads();
             } else {
-                for (int i = 0; i < a.bottom_itr; ++i) jacobi_sweep<CH>(cta, lv[Lm - 1], 3, s_inv);
+                for (int i = 0; i < a.bottom_itr; ++i) sweep_box<CH>(cta, lv[Lm - 1], 3, s_inv);
             }
             for (int l = Tc - 1; l >= 1; --l) {
                 prolongate_level(cta, lv[l], lv[l + 1], s_sc8);
@@ -623,19 +759,24 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
             }
         }
         cluster.sync();  // level-1 u final
-        // Prolongation of rank 0's level-1 u into every slab.
+        // Prolongation of rank 0's level-1 u into every owned cell.
         {
             constexpr int E1 = SUB / 2 + 1;
             const float* u1 = cluster.map_shared_rank(lv[1].u, 0);
-            for (int q = threadIdx.x; q < ncell; q += NT) {
-                int i, j, lx, y, z;
-                cell_of(q, i, j, lx, y, z);
-                float v = u0[i];
-                if (f0[j] & C_ACTIVE) {
-                    const int x = x0 - 1 + lx;
-                    const int cx = (x + 1) >> 1, cy = (y + 1) >> 1, cz = (z + 1) >> 1;
-                    const int px = 1 - (x - (2 * cx - 1)), py = 1 - (y - (2 * cy - 1)), pz = 1 - (z - (2 * cz - 1));
+#pragma unroll
+            for (int l = 0; l < LPT; ++l) {
+                if (off[l] < 0) continue;
+                const int y = off[l] / E, z = off[l] % E;
+                const int cy = (y + 1) >> 1, cz = (z + 1) >> 1;
+                const int py = 1 - (y - (2 * cy - 1)), pz = 1 - (z - (2 * cz - 1));
+#pragma unroll
+                for (int k = 0; k < P; ++k) {
+                    if (k >= np || !(flag(l, k) & C_ACTIVE)) continue;
+                    const int x = x0 + k;
+                    const int cx = (x + 1) >> 1;
+                    const int px = 1 - (x - (2 * cx - 1));
                     const int cbase = box_index(E1, cx, cy, cz);
+                    float v = u0[(k + 1) * PS + off[l]];
 #pragma unroll
                     for (int aa = 0; aa < 2; ++aa)
 #pragma unroll
@@ -646,11 +787,11 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
                                 const float cu = u1[cbase + (aa - px) * E1 * E1 + (bq - py) * E1 + (cq - pz)];
                                 v = __fadd_rn(v, __fmul_rn(w, cu));
                             }
-                    u0[i] = v;
+                    u0[(k + 1) * PS + off[l]] = v;
                 }
-                push_boundary(lx, y * E + z, v);
             }
-            finish_exchange();
+            load_lines();
+            exchange();
         }
         for (int i = 0; i < a.boundary_itr; ++i) slab_sweep(1);
         for (int i = 0; i < a.interior_itr; ++i) slab_sweep(2);
@@ -658,11 +799,13 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
     }
 
     float* gw = a.u + (size_t)tile * TC;
-    for (int q = threadIdx.x; q < ncell; q += NT) {
-        int i, j, lx, y, z;
-        cell_of(q, i, j, lx, y, z);
-        const int x = x0 - 1 + lx;
-        gw[(x * SUB + y) * SUB + z] = u0[i];
+#pragma unroll
+    for (int l = 0; l < LPT; ++l) {
+        if (off[l] < 0) continue;
+        const int y = off[l] / E, z = off[l] % E;
+#pragma unroll
+        for (int k = 0; k < P; ++k)
+            if (k < np) gw[((x0 + k) * SUB + y) * SUB + z] = uu[l][k];
     }
     cluster.sync();  // no CTA leaves while a peer may still address its shared memory
 }
