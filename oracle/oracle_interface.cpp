@@ -149,8 +149,78 @@ static void nd_order(int n, const std::vector<int>& adjp, const std::vector<int>
     rec(all, 0);
 }
 
+// Nested dissection by median planes through DOF positions: for each axis
+// the cut is at the median position and the separator is the smaller
+// one-sided boundary layer; the axis with the smallest separator wins.  Falls
+// back to the level-structure split when no axis separates.
+static void nd_order_xyz(int n, const std::vector<int>& adjp, const std::vector<int>& adji,
+                         const std::vector<std::array<int, 3>>& xyz, std::vector<int>& order) {
+    std::vector<int> part(n, 0);
+    int next_part = 1;
+    order.clear();
+    order.reserve(n);
+    std::function<void(std::vector<int>&, int)> rec = [&](std::vector<int>& verts, int pid) {
+        if (verts.size() <= 48) {
+            for (int v : verts) order.push_back(v);
+            return;
+        }
+        int best_axis = -1, best_cut = 0, best_side = 0;
+        size_t best_sep = 0;
+        std::vector<int> pos(verts.size());
+        for (int ax = 0; ax < 3; ++ax) {
+            for (size_t i = 0; i < verts.size(); ++i) pos[i] = xyz[verts[i]][ax];
+            const size_t mid = pos.size() / 2;
+            std::nth_element(pos.begin(), pos.begin() + mid, pos.end());
+            int cut = pos[mid];
+            size_t nleft = 0, nle = 0;
+            for (int v : verts) { nleft += xyz[v][ax] < cut; nle += xyz[v][ax] <= cut; }
+            if (nleft == 0) {
+                if (nle == verts.size()) continue;
+                cut += 1;
+            }
+            size_t sl = 0, sr = 0;
+            for (int v : verts) {
+                const bool left = xyz[v][ax] < cut;
+                for (int p = adjp[v]; p < adjp[v + 1]; ++p) {
+                    const int w = adji[p];
+                    if (part[w] == pid && (xyz[w][ax] < cut) != left) { (left ? sl : sr)++; break; }
+                }
+            }
+            const size_t sep = std::min(sl, sr);
+            if (best_axis < 0 || sep < best_sep) { best_axis = ax; best_sep = sep; best_cut = cut; best_side = sl <= sr ? 0 : 1; }
+        }
+        if (best_axis < 0) {
+            for (int v : verts) order.push_back(v);
+            return;
+        }
+        std::vector<int> A, S, B;
+        for (int v : verts) {
+            const bool left = xyz[v][best_axis] < best_cut;
+            bool boundary = false;
+            if ((best_side == 0) == left)
+                for (int p = adjp[v]; p < adjp[v + 1] && !boundary; ++p) {
+                    const int w = adji[p];
+                    if (part[w] == pid && (xyz[w][best_axis] < best_cut) != left) boundary = true;
+                }
+            if (boundary) S.push_back(v);
+            else if (left) A.push_back(v);
+            else B.push_back(v);
+        }
+        const int pa = next_part++, pb = next_part++;
+        for (int v : A) part[v] = pa;
+        for (int v : B) part[v] = pb;
+        for (int v : S) part[v] = -1;
+        rec(A, pa);
+        rec(B, pb);
+        for (int v : S) order.push_back(v);
+    };
+    std::vector<int> all(n);
+    for (int i = 0; i < n; ++i) all[i] = i;
+    rec(all, 0);
+}
+
 template <class T>
-void Cholesky::factor(const Csr<T>& A, double eps) {
+void Cholesky::factor(const Csr<T>& A, double eps, const std::vector<std::array<int, 3>>* xyz) {
     n = A.rows;
     // Symmetric pattern without the diagonal.
     std::vector<std::vector<int>> nb(n);
@@ -169,7 +239,8 @@ void Cholesky::factor(const Csr<T>& A, double eps) {
     }
     adji.reserve(adjp[n]);
     for (int r = 0; r < n; ++r) adji.insert(adji.end(), nb[r].begin(), nb[r].end());
-    nd_order(n, adjp, adji, perm);
+    if (xyz && (int)xyz->size() == n) nd_order_xyz(n, adjp, adji, *xyz, perm);
+    else nd_order(n, adjp, adji, perm);
     std::vector<int> iperm(n);
     for (int i = 0; i < n; ++i) iperm[perm[i]] = i;
     // Upper triangle of C = P (A + eps I) P^T by columns: entries (i <= k).
@@ -423,8 +494,14 @@ struct SubsetFlags {
 
 // CPU/Interface_Solver/GALERKIN_PROCESS.h:183-224.
 template <class T>
+using GalerkinMemo = std::vector<std::unordered_map<uint64_t, M8<T>>>;
+
+template <class T>
 static M8<T> galerkin_coarsen(const SubsetFlags& sf, const std::array<M8<T>, 8>& P, const I3& C,
-                              int level) {
+                              int level, GalerkinMemo<T>& memo) {
+    // The coarsened matrix is a pure function of (cell, level): memoised.
+    auto hit = memo[level].find(pack3(C));
+    if (hit != memo[level].end()) return hit->second;
     M8<T> m;
     m.fill(T(0));
     if (level == 1) {
@@ -454,7 +531,7 @@ static M8<T> galerkin_coarsen(const SubsetFlags& sf, const std::array<M8<T>, 8>&
     } else {
         for (int o = 0; o < 8; ++o) {
             I3 child = {2 * C[0] - 1 + (o >> 2), 2 * C[1] - 1 + ((o >> 1) & 1), 2 * C[2] - 1 + (o & 1)};
-            M8<T> g = galerkin_coarsen(sf, P, child, level - 1);
+            M8<T> g = galerkin_coarsen(sf, P, child, level - 1, memo);
             const M8<T>& p = P[o];
             M8<T> t;  // t = g * p
             for (int i = 0; i < 8; ++i)
@@ -471,6 +548,7 @@ static M8<T> galerkin_coarsen(const SubsetFlags& sf, const std::array<M8<T>, 8>&
                 }
         }
     }
+    memo[level].emplace(pack3(C), m);
     return m;
 }
 
@@ -501,7 +579,8 @@ static bool range_contains(const I3& lo, const I3& hi, const I3& rlo, const I3& 
 template <class T>
 static void create_subdomain_hierarchy(const SubsetFlags& sf, BuildState<T>& st,
                                        std::vector<Csr<T>>& Aii_out, std::vector<Csr<T>>& Air_out,
-                                       std::vector<int>& n_interior_out) {
+                                       std::vector<int>& n_interior_out,
+                                       std::vector<std::vector<std::array<int, 3>>>& pos_out) {
     const int M = st.M;
     const I3 lo = sf.lo, hi = sf.hi;
     static const std::array<M8<T>, 8> P = bake_cell_prolongation<T>();
@@ -643,6 +722,7 @@ static void create_subdomain_hierarchy(const SubsetFlags& sf, BuildState<T>& st,
         }
         // Interior DOFs (lines 315-375).
         int node_count = 0;
+        std::vector<std::array<int, 3>>& pos = pos_out[m - 1];
         for (int L = m; L <= levels; ++L) {
             for (const I3& c : sorted_interior_cells(m, L))
                 for (int li = 0; li < 8; ++li) {
@@ -665,6 +745,7 @@ static void create_subdomain_hierarchy(const SubsetFlags& sf, BuildState<T>& st,
                         if (!(rec.flags & NODE_DEGREE)) {
                             rec.flags |= NODE_DEGREE | NODE_ACTIVE;
                             rec.index = node_count++;
+                            pos.push_back({N[0] << (L - 1), N[1] << (L - 1), N[2] << (L - 1)});
                         }
                     } else {
                         H[m][L][pack3(N)].flags |= NODE_TJUNCTION;
@@ -675,6 +756,8 @@ static void create_subdomain_hierarchy(const SubsetFlags& sf, BuildState<T>& st,
                             if (!(rec.flags & NODE_DEGREE)) {
                                 rec.flags |= NODE_DEGREE | NODE_ACTIVE;
                                 rec.index = node_count++;
+                                const I3& pn = p.first;
+                                pos.push_back({pn[0] << (L - 1), pn[1] << (L - 1), pn[2] << (L - 1)});
                             }
                         }
                     }
@@ -684,6 +767,7 @@ static void create_subdomain_hierarchy(const SubsetFlags& sf, BuildState<T>& st,
     }
 
     // Galerkin assembly (lines 554-655, the compiled #else branch).
+    GalerkinMemo<T> memo(levels + 1);
     for (int m = 1; m <= M; ++m) {
         std::unordered_map<uint64_t, T> Aii, Air;
         auto resolve = [&](int L, const I3& p, uint32_t& f, int& id) {
@@ -703,7 +787,7 @@ static void create_subdomain_hierarchy(const SubsetFlags& sf, BuildState<T>& st,
         };
         for (int L = m; L <= levels; ++L)
             for (const I3& c : sorted_interior_cells(m, L)) {
-                M8<T> cm = galerkin_coarsen<T>(sf, P, c, L);
+                M8<T> cm = galerkin_coarsen<T>(sf, P, c, L, memo);
                 Parents<T> par[8];
                 for (int li = 0; li < 8; ++li) {
                     I3 N = {c[0] - 1 + (li >> 2), c[1] - 1 + ((li >> 1) & 1), c[2] - 1 + (li & 1)};
@@ -794,6 +878,7 @@ void build_interface_system(const Dims& gd, const uint32_t* gflags_in, const int
     out.Aii.assign(M, std::vector<Csr<T>>(out.n_sub));
     out.Air.assign(M, std::vector<Csr<T>>(out.n_sub));
     out.n_interior.assign(M, std::vector<int>(out.n_sub, 0));
+    out.aii_xyz.assign(M, std::vector<std::vector<std::array<int, 3>>>(out.n_sub));
     int s = 0;
     for (int i = 0; i < ns[0]; ++i)
         for (int j = 0; j < ns[1]; ++j)
@@ -803,8 +888,10 @@ void build_interface_system(const Dims& gd, const uint32_t* gflags_in, const int
                 SubsetFlags sf = extract_subset(gd, gflags_in, lo, hi, sub);
                 std::vector<Csr<T>> aii, air;
                 std::vector<int> ni;
-                create_subdomain_hierarchy<T>(sf, st, aii, air, ni);
+                std::vector<std::vector<std::array<int, 3>>> pos(M);
+                create_subdomain_hierarchy<T>(sf, st, aii, air, ni, pos);
                 for (int m = 0; m < M; ++m) {
+                    out.aii_xyz[m][s] = std::move(pos[m]);
                     out.Aii[m][s] = std::move(aii[m]);
                     out.Air[m][s] = std::move(air[m]);
                     out.n_interior[m][s] = ni[m];
@@ -812,6 +899,14 @@ void build_interface_system(const Dims& gd, const uint32_t* gflags_in, const int
             }
     out.n_iface = st.iface_counter;
     out.iface_map = st.iface_map;
+    out.iface_xyz.assign(M, {});
+    for (int m = 0; m < M; ++m) {
+        out.iface_xyz[m].assign(out.n_iface[m], {0, 0, 0});
+        for (auto& kv : st.iface_hash[m]) {
+            const I3 nd = unpack3(kv.first);
+            out.iface_xyz[m][kv.second] = {nd[0] << m, nd[1] << m, nd[2] << m};
+        }
+    }
     out.Arr.resize(M);
     for (int m = 0; m < M; ++m) {
         out.Arr[m] = csr_from_map<T>(out.n_iface[m], out.n_iface[m], st.Arr[m]);
@@ -857,9 +952,10 @@ void SigmaSolver<T>::initialize(const InterfaceSystem<T>& s, int smoothing_itera
     arr.resize(s.M);
     aii.assign(s.M, std::vector<Cholesky>(s.n_sub));
     for (int l = 0; l < s.M; ++l) {
-        arr[l].factor(s.Arr[l], eps);
+        arr[l].factor(s.Arr[l], eps, &s.iface_xyz[l]);
+#pragma omp parallel for schedule(dynamic)
         for (int sd = 0; sd < s.n_sub; ++sd)
-            if (s.n_interior[l][sd] > 0) aii[l][sd].factor(s.Aii[l][sd], eps);
+            if (s.n_interior[l][sd] > 0) aii[l][sd].factor(s.Aii[l][sd], eps, &s.aii_xyz[l][sd]);
     }
     u.resize(s.M);
     r.resize(s.M);
@@ -874,18 +970,21 @@ void SigmaSolver<T>::initialize(const InterfaceSystem<T>& s, int smoothing_itera
 template <class T>
 static void schur_accumulate(const InterfaceSystem<T>& s, const std::vector<std::vector<Cholesky>>& aii,
                              int l, const std::vector<T>& u, std::vector<T>& acc) {
-    std::vector<T> vb;
-    std::vector<double> vx;
+    // The subdomain solves are independent; their contributions are added
+    // in subdomain order afterwards.
+    std::vector<std::vector<T>> vxt(s.n_sub);
+#pragma omp parallel for schedule(dynamic)
     for (int sd = 0; sd < s.n_sub; ++sd) {
         int ni = s.n_interior[l][sd];
         if (ni == 0) continue;
-        vb.assign(ni, T(0));
+        std::vector<T> vb(ni, T(0));
         s.Air[l][sd].spmv(u.data(), vb.data());
-        vx.assign(vb.begin(), vb.end());
+        std::vector<double> vx(vb.begin(), vb.end());
         aii[l][sd].solve(vx.data());
-        std::vector<T> vxt(vx.begin(), vx.end());
-        s.Air[l][sd].spmv_t_add(vxt.data(), acc.data());
+        vxt[sd].assign(vx.begin(), vx.end());
     }
+    for (int sd = 0; sd < s.n_sub; ++sd)
+        if (s.n_interior[l][sd] > 0) s.Air[l][sd].spmv_t_add(vxt[sd].data(), acc.data());
 }
 
 template <class T>
@@ -928,8 +1027,8 @@ void SigmaSolver<T>::v_cycle() {
 
 template struct Csr<float>;
 template struct Csr<double>;
-template void Cholesky::factor<float>(const Csr<float>&, double);
-template void Cholesky::factor<double>(const Csr<double>&, double);
+template void Cholesky::factor<float>(const Csr<float>&, double, const std::vector<std::array<int, 3>>*);
+template void Cholesky::factor<double>(const Csr<double>&, double, const std::vector<std::array<int, 3>>*);
 template void build_interface_system<float>(const Dims&, const uint32_t*, const int*, int, InterfaceSystem<float>&);
 template void build_interface_system<double>(const Dims&, const uint32_t*, const int*, int, InterfaceSystem<double>&);
 template struct SigmaSolver<float>;

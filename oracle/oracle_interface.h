@@ -39,8 +39,9 @@ struct Cholesky {
     std::vector<int> perm;          // new -> old
     std::vector<int> Lp, Li;        // CSC of L, diagonal first in each column
     std::vector<double> Lx;
+    // xyz: DOF positions for the fill-reducing ordering (optional).
     template <class T>
-    void factor(const Csr<T>& A, double eps);
+    void factor(const Csr<T>& A, double eps, const std::vector<std::array<int, 3>>* xyz = nullptr);
     void solve(double* x) const;    // x <- (A+eps I)^{-1} x
     size_t nnz() const { return Li.size(); }
 };
@@ -55,6 +56,9 @@ struct InterfaceSystem {
     std::vector<std::vector<Csr<T>>> Aii, Air;   // [level][subdomain]
     std::vector<Csr<T>> Prr;           // [level] (fine rows, coarse cols)
     std::vector<std::vector<int>> n_interior;    // [level][subdomain]
+    // DOF positions (finest-level units), used only to order the factorisations.
+    std::vector<std::vector<std::array<int, 3>>> iface_xyz;               // [level][dof]
+    std::vector<std::vector<std::vector<std::array<int, 3>>>> aii_xyz;    // [level][subdomain][dof]
 };
 
 // Build the interface system.  gflags_in are the caller's flags before the
