@@ -37,7 +37,10 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--config", choices=["c1", "c2", "c3"], default="c2")
+    p.add_argument("--config", choices=["c1", "c2", "c3", "p128"], default="c2")
+    p.add_argument("--one-solve", action="store_true",
+                   help="set up, run one solve with per-phase timing and print the phase table "
+                        "(the command profiled under ncu; prints no JSON line)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--precision", choices=["reference", "mixed"], default="reference")
     return p.parse_args()
@@ -99,7 +102,39 @@ class ClockSampler:
 
 def workload(cfg):
     from hierarchicaldd_b200 import domains
-    return {"c1": domains.config1, "c2": domains.config2, "c3": domains.config3}[cfg]()
+    return domains.CONFIGS[cfg]()
+
+
+PHASES = ["vcycle", "laplace", "pcg_vector", "interface", "sigma_vcycle", "dense_tile_copy",
+          "sn_forward", "sn_backward"]
+
+
+def one_solve(args):
+    """Setup and a single timed solve: the command profiled under ncu."""
+    from hierarchicaldd_b200 import _lib
+    from hierarchicaldd_b200.solver import SPGrid_Domain_Decomposition_Solver
+    d = workload(args.config)
+    m = d.meta
+    s = SPGrid_Domain_Decomposition_Solver()
+    s.Set_Domain(d.flags, d.rhs)
+    t0 = time.time()
+    s.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"],
+                                m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"],
+                                m["sigma_mg"], tol=1e-6)
+    print(f"{d.name}: setup {time.time() - t0:.1f} s", flush=True)
+    lib = _lib.load()
+    lib.hdd_set_kernel_timing(s.h, 1)
+    r = s.Solve()
+    ms = (C.c_double * 8)()
+    cnt = (C.c_longlong * 8)()
+    nbytes = (C.c_double * 8)()
+    lib.hdd_get_kernel_timing(s.h, ms, cnt)
+    lib.hdd_get_kernel_bytes(s.h, nbytes)
+    print(f"solve: {r['iterations']} iterations, {r['solve_ms']:.2f} ms, true residual {r['true_residual_inf']:.3e}")
+    for i, n in enumerate(PHASES):
+        print(f"phase {n:16s} {ms[i]:10.3f} ms {cnt[i]:6d} launches {nbytes[i]:.6e} algorithmic bytes")
+    print(f"kernel launches {s.Kernel_Launches()}")
+    s.close()
 
 
 def peaks():
@@ -109,6 +144,21 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def measured_traffic(kernel, workload):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
+    `kernel` on `workload` from the committed ncu summaries, or None."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 3 and not line.startswith("#") and parts[0] == kernel and parts[1] == workload:
+                    return float(parts[2])
+    except OSError:
+        pass
+    return None
 
 
 def cpu_baseline(d, threads_note):
@@ -167,6 +217,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.one_solve:
+        one_solve(args)
         return
     import torch
     torch.cuda.set_device(local_rank)
@@ -239,24 +292,38 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_val = world * args.steps / float(t.item())
 
-    # Per-phase device timing (separate, instrumented solve).
+    # Per-phase device timing (separate, instrumented solve): CUDA events on
+    # the solver's stream around each phase's launches, with the phase's
+    # algorithmic bytes accounted by the library.
     ms = (C.c_double * 8)()
     cnt = (C.c_longlong * 8)()
+    nbytes = (C.c_double * 8)()
     lib.hdd_set_kernel_timing(s.h, 1)
     prof = s.Solve()
     lib.hdd_get_kernel_timing(s.h, ms, cnt)
+    lib.hdd_get_kernel_bytes(s.h, nbytes)
     lib.hdd_set_kernel_timing(s.h, 0)
-    phases = ["vcycle", "laplace", "pcg_vector", "interface", "sigma_vcycle", "dense_tile_copy"]
+    phases = PHASES
     phase_ms = {n: float(ms[i]) for i, n in enumerate(phases)}
     phase_n = {n: int(cnt[i]) for i, n in enumerate(phases)}
 
-    # Roofline of the Laplacian kernel (HBM-bound): algorithmic bytes = 12 B per
-    # Active|Interface cell (read s and flags, write q).
-    from hierarchicaldd_b200.domains import ACTIVE
-    n_solve_cells = int(np.count_nonzero(d.flags & ACTIVE))  # Active before the divider = Active|Interface after
-    lap_ms = phase_ms["laplace"] / max(phase_n["laplace"], 1)
+    # Roofline (HBM-bound kernels) of every timed kernel; the dominant one by
+    # device time is the headline.
     hbm, peak_kind = peaks()
-    achieved = 12.0 * n_solve_cells / (lap_ms * 1e-3) / 1e9 if lap_ms > 0 else None
+    kernels = {0: "vcycle_cluster_kernel" if d.sub_size[0] == 32 else "vcycle_kernel", 1: "laplace_dot_kernel",
+               6: "sn_forward_kernel", 7: "sn_backward_kernel"}
+    per_kernel = {}
+    for i, kname in kernels.items():
+        if cnt[i] == 0 or ms[i] <= 0:
+            continue
+        gbs = nbytes[i] / (ms[i] * 1e-3) / 1e9
+        per_kernel[kname] = {"ms": float(ms[i]), "launches": int(cnt[i]),
+                             "bytes_per_launch": float(nbytes[i] / cnt[i]), "achieved_gbs": gbs,
+                             "frac": gbs / hbm}
+    top = max(kernels, key=lambda i: ms[i])
+    top_name = kernels[top]
+    achieved = per_kernel.get(top_name, {}).get("achieved_gbs")
+    traffic = measured_traffic(top_name, d.name)
 
     its = [r["iterations"] for r in res]
     lat = np.sort(dev_ms)
@@ -277,9 +344,11 @@ def main():
         "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": 4 * cells, "d2h_bytes_per_step": 4 * cells},
         "gpu_launches": int(launches),
         "phase_ms_per_solve": phase_ms, "phase_launches_per_solve": phase_n,
-        "roofline": {"kernel": "laplace_dot_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm,
-                     "unit": "GB/s", "frac": (achieved / hbm) if achieved else None, "traffic": None,
-                     "peak_kind": peak_kind},
+        "roofline": {"kernel": top_name, "bound": "hbm", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
+                     "peak_kind": peak_kind,
+                     "bytes_per_launch": per_kernel.get(top_name, {}).get("bytes_per_launch")},
+        "kernels": per_kernel,
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -71,6 +71,7 @@ SIGNATURES = {
     "hdd_kernel_launch_count": (C.c_int, [_vp, C.POINTER(C.c_longlong)]),
     "hdd_set_kernel_timing": (C.c_int, [_vp, C.c_int]),
     "hdd_get_kernel_timing": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
+    "hdd_get_kernel_bytes": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "hdd_status_string": (C.c_char_p, [C.c_int]),
     "hdd_last_error": (C.c_char_p, [_vp]),
     "hdd_destroy": (None, [_vp]),

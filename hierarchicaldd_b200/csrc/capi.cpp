@@ -248,7 +248,7 @@ hdd_status hdd_set_kernel_timing(hdd_solver* s, int enable) {
     return guard(s, [&](Solver& v) {
         v.collect_timing();
         v.timing = enable != 0;
-        for (int c = 0; c < Solver::kCats; ++c) { v.cat_ms[c] = 0; v.cat_n[c] = 0; }
+        for (int c = 0; c < Solver::kCats; ++c) { v.cat_ms[c] = 0; v.cat_n[c] = 0; v.cat_bytes[c] = 0; }
     });
 }
 
@@ -257,6 +257,14 @@ hdd_status hdd_get_kernel_timing(hdd_solver* s, double* ms, long long* launches)
     return guard(s, [&](Solver& v) {
         v.collect_timing();
         for (int c = 0; c < Solver::kCats; ++c) { ms[c] = v.cat_ms[c]; launches[c] = v.cat_n[c]; }
+    });
+}
+
+hdd_status hdd_get_kernel_bytes(hdd_solver* s, double* bytes) {
+    if (!bytes) return HDD_ERR_INVALID_ARGUMENT;
+    return guard(s, [&](Solver& v) {
+        v.collect_timing();
+        for (int c = 0; c < Solver::kCats; ++c) bytes[c] = v.cat_bytes[c];
     });
 }
 

@@ -307,17 +307,17 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
     ck(cudaStreamSynchronize(s), "sigma setup");
 }
 
-void SigmaGpu::vcycle(cudaStream_t s, long long& launches) {
+void SigmaGpu::vcycle(cudaStream_t s, long long& launches, PhaseHook* hook) {
     auto schur_apply = [&](int l, const float* u, float* out_tmp) {
         SigmaLevel& L = lv[l];
         launch_csr(L.air, u, nullptr, L.vb, 0, s, launches);
-        L.aii.solve(L.vb, L.vx, s, launches);
+        L.aii.solve(L.vb, L.vx, s, launches, hook);
         launch_csr(L.airT, L.vx, L.b, out_tmp, 1, s, launches);  // tmp = b + Air^T vx
     };
     auto smooth = [&](int l) {
         SigmaLevel& L = lv[l];
         schur_apply(l, L.u, L.tmp);
-        L.arr_solve.solve(L.tmp, L.u, s, launches);
+        L.arr_solve.solve(L.tmp, L.u, s, launches, hook);
     };
     for (int l = 0; l + 1 < M; ++l) {
         SigmaLevel& L = lv[l];
@@ -333,7 +333,7 @@ void SigmaGpu::vcycle(cudaStream_t s, long long& launches) {
             // Right-hand side [0; b], solution's interface block -> u.
             if (n_bottom_int > 0) ck(cudaMemsetAsync(kb, 0, sizeof(float) * n_bottom_int, s), "memset kb");
             ck(cudaMemcpyAsync(kb + n_bottom_int, B.b, sizeof(float) * n_bottom, cudaMemcpyDeviceToDevice, s), "copy b");
-            bottom.solve(kb, kx, s, launches);
+            bottom.solve(kb, kx, s, launches, hook);
             ck(cudaMemcpyAsync(B.u, kx + n_bottom_int, sizeof(float) * n_bottom, cudaMemcpyDeviceToDevice, s), "copy u");
         }
     }

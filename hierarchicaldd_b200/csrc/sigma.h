@@ -58,6 +58,20 @@ struct SnFactor {
     void solve(double* x) const;               // host reference solve (tests)
 };
 
+// Optional per-phase device timing: the caller records events around the
+// launches of a phase and accumulates the phase's algorithmic bytes.
+struct PhaseHook {
+    virtual void begin(int phase) = 0;
+    virtual void end(int phase, double bytes) = 0;
+
+protected:
+    ~PhaseHook() = default;
+};
+
+// Timing phases of the supernodal solve kernels.
+constexpr int kPhaseSnForward = 6;
+constexpr int kPhaseSnBackward = 7;
+
 // One unit of device work of a supernodal solve, taken by a CTA of the
 // persistent solve kernels (sn_solve.cu).  With front >= 0, forward: rows
 // [r0, r0+rows) of front `front` times its columns [c0, c0+ncols); when a row
@@ -78,6 +92,7 @@ struct SolvePlan {
     int n_fwd = 0, n_bwd = 0;        // task counts
     int n_ctr = 0;                   // ints in the counter block
     int grid = 0;                    // persistent CTAs per launch
+    double fwd_bytes = 0, bwd_bytes = 0;  // algorithmic bytes of one forward / backward launch
     int *d_col0 = nullptr, *d_ncol = nullptr, *d_nrow = nullptr, *d_parent = nullptr;
     int *d_rows = nullptr; long long *d_rows_off = nullptr;
     int *d_child_ptr = nullptr, *d_child = nullptr;
@@ -99,7 +114,8 @@ struct SolvePlan {
     void build(const std::vector<const SnFactor*>& factors, const std::vector<int>& offsets, cudaStream_t s);
     void release();
     // x_old = (A+eps I)^{-1} b_old (both in the concatenated original order).
-    void solve(const float* b_old, float* x_old, cudaStream_t s, long long& launches) const;
+    void solve(const float* b_old, float* x_old, cudaStream_t s, long long& launches,
+               PhaseHook* hook = nullptr) const;
     int error_flag(cudaStream_t s) const;
     ~SolvePlan() { release(); }
 };
@@ -137,7 +153,7 @@ struct SigmaGpu {
     void setup(const InterfaceHost& ih, int smoothing_iterations, cudaStream_t s);
     void release();
     // u[0] = sigma V-cycle(b[0]) (SIGMA_MULTIGRID_SOLVER.cpp:70-82), u[0] starting at 0.
-    void vcycle(cudaStream_t s, long long& launches);
+    void vcycle(cudaStream_t s, long long& launches, PhaseHook* hook = nullptr);
     // Nonzero when a bounded wait inside a supernodal solve gave up.
     int error_flag(cudaStream_t s) const;
     float* b0() const { return lv.empty() ? nullptr : lv[0].b; }

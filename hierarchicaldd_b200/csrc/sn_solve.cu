@@ -496,6 +496,12 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
         }
     }
     flush(btasks, bbwd, bfirst);
+    // Algorithmic bytes: each stored coefficient of L_JJ^{-1} (lower triangle)
+    // and of -L_RJ L_JJ^{-1} read once per direction, plus b read and x written.
+    double coef = 0;
+    for (int g = 0; g < nsn; ++g) coef += 0.5 * ncol[g] * (ncol[g] + 1.0) + (double)nrow[g] * ncol[g];
+    fwd_bytes = 4.0 * coef + 8.0 * n;
+    bwd_bytes = 4.0 * coef + 8.0 * n;
     n_fwd = (int)ftasks.size();
     n_bwd = (int)btasks.size();
     n_ctr = 2 + 2 * nsn + nchunk;
@@ -588,17 +594,21 @@ void SolvePlan::release() {
     n_fwd = n_bwd = n_ctr = 0;
 }
 
-void SolvePlan::solve(const float* b_old, float* x_old, cudaStream_t s, long long& launches) const {
+void SolvePlan::solve(const float* b_old, float* x_old, cudaStream_t s, long long& launches, PhaseHook* hook) const {
     if (nsn == 0) return;
     PlanView P{nsn, max_front, d_col0, d_ncol, d_nrow, d_parent, d_rows, d_rows_off, d_child_ptr, d_child,
                d_relmap_off, d_relmap, d_upd_off, d_fw_off, d_ntf, d_ntb, d_perm, d_bfwd, d_bbwd, d_fw, d_part, d_upd,
                d_ynew,
                d_xnew, d_ctr, d_err};
     dev::ck(cudaMemsetAsync(d_ctr, 0, sizeof(int) * n_ctr, s), "reset counters");
+    if (hook) hook->begin(kPhaseSnForward);
     sn_forward_kernel<<<std::min(grid, n_fwd), kNT, forward_smem(max_front), s>>>(P, d_fwd, n_fwd, b_old);
     dev::ck(cudaGetLastError(), "sn forward");
+    if (hook) hook->end(kPhaseSnForward, fwd_bytes);
+    if (hook) hook->begin(kPhaseSnBackward);
     sn_backward_kernel<<<std::min(grid, n_bwd), kNT, backward_smem(max_front), s>>>(P, d_bwd, n_bwd, x_old);
     dev::ck(cudaGetLastError(), "sn backward");
+    if (hook) hook->end(kPhaseSnBackward, bwd_bytes);
     launches += 2;
 }
 

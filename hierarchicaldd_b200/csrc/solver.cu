@@ -37,6 +37,7 @@ static Options to_options(const hdd_options& o) {
 }
 
 Solver::Solver(const hdd_options& o) : opts(o) {
+    hook.s = this;
     for (int a = 0; a < 3; ++a)
         if (o.size[a] < 3 || o.sub_size[a] < 1) throw Error(HDD_ERR_INVALID_ARGUMENT, "invalid size or sub_size");
     if (o.sub_size[0] != o.sub_size[1] || o.sub_size[0] != o.sub_size[2])
@@ -68,6 +69,7 @@ void Solver::collect_timing() {
         cudaEventElapsedTime(&ms, p.a, p.b);
         cat_ms[p.cat] += ms;
         cat_n[p.cat] += 1;
+        cat_bytes[p.cat] += p.bytes;
         cudaEventDestroy(p.a);
         cudaEventDestroy(p.b);
     }
@@ -119,6 +121,17 @@ void Solver::initialize() {
     }
     dense.alloc(std::max<size_t>(L.cell_count(), 1));
     tflags.upload(L.tile_flags.data(), L.tile_flags.size(), stream);
+    {
+        // Algorithmic HBM bytes of one launch: the Laplacian reads s and the
+        // flags and writes q at each Active|Interface cell (4 + 2 + 4 + the
+        // per-tile partial, rounded to 12 B per cell); the V-cycle reads u, b
+        // and the level-0 flags and writes u once per box cell (13 B).
+        size_t nsolve = 0;
+        for (uint16_t f : L.tile_flags) nsolve += (f & (C_ACTIVE | C_INTERFACE)) ? 1 : 0;
+        const double sub3 = (double)L.opt.sub[0] * L.opt.sub[0] * L.opt.sub[0];
+        laplace_bytes = 12.0 * (double)nsolve;
+        vcycle_bytes = 13.0 * sub3 * (double)L.boxes.size();
+    }
     std::vector<int> btile(L.boxes.size()), bnb(3 * L.boxes.size());
     for (size_t i = 0; i < L.boxes.size(); ++i) {
         btile[i] = L.boxes[i].tile;
@@ -226,7 +239,7 @@ VcycleArgs Solver::vcycle_args(float* u, const float* bb, int halo_from_u, int z
 
 void Solver::run_vcycle(float* u, const float* bb, int halo_from_u, int zero_init, int nv) {
     VcycleArgs a = vcycle_args(u, bb, halo_from_u, zero_init, nv);
-    Tm tm(this, 0);
+    Tm tm(this, 0, vcycle_bytes);
     cuda_check(launch_vcycle(a, stream), "vcycle kernel");
     count();
 }
@@ -244,7 +257,7 @@ void Solver::apply_preconditioner(const float* rr, float* zz) {
         // u_G = 0 then sigma_mg V-cycles (Preconditioner.h:105,110-117).
         Tm tm(this, 4);
         cuda_check(cudaMemsetAsync(sigma.u0(), 0, sizeof(float) * std::max(n_if, 1), stream), "memset u0");
-        for (int i = 0; i < opts.sigma_mg; ++i) sigma.vcycle(stream, launches);
+        for (int i = 0; i < opts.sigma_mg; ++i) sigma.vcycle(stream, launches, &hook);
     }
     {
         Tm tm(this, 3);
@@ -294,7 +307,7 @@ void Solver::solve(hdd_result* res) {
             cuda_check(launch_update_s(g, s.p, z.p, scal.p, it == 0, mode, stream), "update_s"); count();
         }
         {
-            Tm tm(this, 1);
+            Tm tm(this, 1, laplace_bytes);
             cuda_check(launch_laplace_dot(g, s.p, q.p, partial.p, stream), "laplace"); count();
         }
         {

@@ -82,16 +82,20 @@ struct Solver {
 
     // Optional per-phase device timing with CUDA events on the solver stream
     // (categories: 0 V-cycle kernel, 1 Laplacian kernel, 2 PCG vector kernels,
-    // 3 interface gather/scatter, 4 sigma V-cycle, 5 dense<->tile copies).
+    // 3 interface gather/scatter, 4 sigma V-cycle (includes 6 and 7),
+    // 5 dense<->tile copies, 6 supernodal forward, 7 supernodal backward),
+    // with each phase's algorithmic bytes.
     static constexpr int kCats = 8;
     bool timing = false;
     double cat_ms[kCats] = {0};
     long long cat_n[kCats] = {0};
-    struct Pending { int cat; cudaEvent_t a, b; };
+    double cat_bytes[kCats] = {0};
+    double vcycle_bytes = 0, laplace_bytes = 0;  // algorithmic bytes of one launch
+    struct Pending { int cat; cudaEvent_t a, b; double bytes; };
     std::vector<Pending> pending;
     struct Tm {
-        Solver* s; int cat; cudaEvent_t a = nullptr, b = nullptr;
-        Tm(Solver* sv, int c) : s(sv), cat(c) {
+        Solver* s; int cat; double bytes; cudaEvent_t a = nullptr, b = nullptr;
+        Tm(Solver* sv, int c, double by = 0) : s(sv), cat(c), bytes(by) {
             if (!s->timing) return;
             cudaEventCreate(&a); cudaEventCreate(&b);
             cudaEventRecord(a, s->stream);
@@ -99,9 +103,27 @@ struct Solver {
         ~Tm() {
             if (!a) return;
             cudaEventRecord(b, s->stream);
-            s->pending.push_back({cat, a, b});
+            s->pending.push_back({cat, a, b, bytes});
         }
     };
+    // Phase hook for the sigma solver's supernodal launches.
+    struct Hook : PhaseHook {
+        Solver* s = nullptr;
+        cudaEvent_t a = nullptr;
+        void begin(int) override {
+            if (!s->timing) return;
+            cudaEventCreate(&a);
+            cudaEventRecord(a, s->stream);
+        }
+        void end(int phase, double bytes) override {
+            if (!s->timing || !a) return;
+            cudaEvent_t b;
+            cudaEventCreate(&b);
+            cudaEventRecord(b, s->stream);
+            s->pending.push_back({phase, a, b, bytes});
+            a = nullptr;
+        }
+    } hook;
     void collect_timing();
 
     explicit Solver(const hdd_options& o);

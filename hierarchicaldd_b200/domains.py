@@ -134,6 +134,15 @@ def config3() -> Domain:
                        sigma_levels=4, sigma_smoothing=3, sigma_mg=1, true_residual_every=20))
 
 
+def profile_case() -> Domain:
+    """128^3 cells (size 129), centred Dirichlet sphere r=24, 32^3 subdomains:
+    the 256^3 workload's kernels (sub 32, vlevels 4, smoothing 4/4) on an eighth
+    of its cells, small enough for multi-pass profiler captures."""
+    d = small(128, 32, 24, seed=5)
+    d.meta.update(vlevels=4, interior_smoothing=4, boundary_smoothing=4, sigma_levels=3)
+    return Domain(d.size, d.flags, d.rhs, d.sub_size, "p128_128cube_sub32", d.meta)
+
+
 def small(n_cells=32, sub=8, radius=6, seed=0, delta=None) -> Domain:
     """A small test domain: n_cells^3 box, one centred Dirichlet sphere, random RHS."""
     size = (n_cells + 1,) * 3
@@ -150,4 +159,4 @@ def small(n_cells=32, sub=8, radius=6, seed=0, delta=None) -> Domain:
                        sigma_levels=2, sigma_smoothing=3, sigma_mg=1))
 
 
-CONFIGS = {"c1": config1, "c2": config2, "c3": config3}
+CONFIGS = {"c1": config1, "c2": config2, "c3": config3, "p128": profile_case}

@@ -155,12 +155,17 @@ hdd_status hdd_interface_map(hdd_solver* s, int* cells_xyz);
 hdd_status hdd_interface_matrix(hdd_solver* s, int kind, int level, int subdomain, int* rows,
                                 int* cols, int* nnz, int* ptr, int* col, double* val);
 
-/* Per-phase device timing (CUDA events on the solver stream) for profiling.
+/* Per-phase device timing (CUDA events on the solver stream) for profiling;
+ * no reference counterpart (the reference prints wall-clock times).
  * Phases: 0 V-cycle kernel, 1 Laplacian kernel, 2 PCG vector kernels,
- * 3 interface gather/scatter, 4 sigma V-cycle, 5 dense<->tile copies,
- * 6-7 unused.  Enabling clears the accumulators; ms/launches hold 8 entries. */
+ * 3 interface gather/scatter, 4 sigma V-cycle (includes 6 and 7), 5 dense<->
+ * tile copies, 6 supernodal forward solves, 7 supernodal backward solves.
+ * Enabling clears the accumulators; ms/launches/bytes hold 8 entries.
+ * hdd_get_kernel_bytes gives each phase's algorithmic bytes (the data the
+ * kernels must move at minimum) for phases 0, 1, 6 and 7, 0 for the others. */
 hdd_status hdd_set_kernel_timing(hdd_solver* s, int enable);
 hdd_status hdd_get_kernel_timing(hdd_solver* s, double* ms, long long* launches);
+hdd_status hdd_get_kernel_bytes(hdd_solver* s, double* bytes);
 
 /* Number of our CUDA kernel launches issued since the handle was created. */
 hdd_status hdd_kernel_launch_count(hdd_solver* s, long long* count);

@@ -8,6 +8,9 @@
 //   PB/Public_Library/PhysBAM_Tools/Krylov_Solvers/CONJUGATE_GRADIENT.cpp:22-67
 //   PB/Public_Library/PhysBAM_Tools/Krylov_Solvers/KRYLOV_SYSTEM_BASE.cpp:100-106
 // Vectors are dense x-slowest/z-fastest arrays over the level-0 grid.
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -47,7 +50,15 @@ struct Solver : SolverBase {
 
     void setup() {
         // SPGrid_Domain_Decomposition_Solver.h:121-155.
+        const bool verbose = std::getenv("HDDO_VERBOSE") != nullptr;
+        auto t0 = std::chrono::steady_clock::now();
+        auto stamp = [&](const char* what) {
+            if (!verbose) return;
+            const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            std::fprintf(stderr, "[oracle setup] %s at %.2f s\n", what, s);
+        };
         build_interface_system<T>(d0, flags_in.data(), sub, sigma_levels, sys);
+        stamp("interface system");
         lv.resize(vlevels);
         lv[0].d = d0;
         lv[0].flags = flags_in;
@@ -67,7 +78,9 @@ struct Solver : SolverBase {
                 lv[l].b.assign(lv[l].d.count(), T(0));
             }
         }
+        stamp("topology");
         sigma.initialize(sys, sigma_smoothing);
+        stamp("factorisations");
         k_tmp.assign(d0.count(), T(0));
     }
 
