@@ -161,51 +161,74 @@ def measured_traffic(kernel, workload):
     return None
 
 
-def cpu_baseline(d, threads_note):
-    """Oracle (CPU restatement of the reference dd_pcg) on a bounded sample."""
+# PCG iterations one full solve of each workload takes in the oracle (the CPU
+# restatement of the reference dd_pcg path) at 1e-6 relative residual, from a
+# full oracle run of each workload.  A CPU sample of a few iterations is scaled
+# to one solve with it; c1 is timed as whole solves.
+ORACLE_ITERATIONS = {"c1": 12, "c2": 34, "p128": 23}
+SAMPLE_ITERATIONS = {"c1": 12, "c2": 1, "p128": 4}
+
+
+def make_oracle(d):
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from oracle_ffi import Oracle
     m = d.meta
+    return Oracle(d.size, d.sub_size, d.flags, vlevels=m["vlevels"], nVcycles=m["nVcycles"],
+                  interior_smoothing=m["interior_smoothing"], boundary_smoothing=m["boundary_smoothing"],
+                  sigma_levels=m["sigma_levels"], sigma_smoothing=m["sigma_smoothing"], sigma_mg=m["sigma_mg"])
+
+
+def oracle_sample(o, d, iters):
+    """Seconds for `iters` PCG iterations of the oracle from x = 0."""
     t0 = time.time()
-    o = Oracle(d.size, d.sub_size, d.flags, vlevels=m["vlevels"], nVcycles=m["nVcycles"],
-               interior_smoothing=m["interior_smoothing"], boundary_smoothing=m["boundary_smoothing"],
-               sigma_levels=m["sigma_levels"], sigma_smoothing=m["sigma_smoothing"], sigma_mg=m["sigma_mg"])
+    o.solve(d.rhs, tol=0.0, max_it=iters, min_it=iters)
+    return time.time() - t0
+
+
+def cpu_baseline(args, d):
+    """The oracle on the host cores, on a bounded sample of the same workload."""
+    cores = os.cpu_count() or 1
+    t0 = time.time()
+    o = make_oracle(d)
     setup_s = time.time() - t0
-    t0 = time.time()
-    _, it, info = o.solve(d.rhs, tol=1e-6, max_it=500)
-    dt = time.time() - t0
-    return {"value": 1.0 / dt, "unit": "solves/s", "cores": threads_note, "kind": "port",
-            "sample": f"one full solve of {d.name} ({it} PCG iterations, {dt:.2f} s; setup {setup_s:.1f} s untimed)"}
+    iters = SAMPLE_ITERATIONS[args.config]
+    dt = oracle_sample(o, d, iters)
+    per_solve = dt / iters * ORACLE_ITERATIONS[args.config]
+    return {"value": 1.0 / per_solve, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": (f"{iters} PCG iteration(s) of {d.name} on the oracle ({dt:.2f} s, OpenMP over "
+                       f"{cores} threads), scaled to a {ORACLE_ITERATIONS[args.config]}-iteration solve; "
+                       f"oracle setup {setup_s:.1f} s untimed")}
 
 
 def run_reference(args, rank):
+    """The reference's CPU path (its restatement in oracle/, since the reference
+    itself cannot be built here) on this workload: each step is a bounded sample
+    of PCG iterations, scaled to solves/s by the full-solve iteration count."""
     if rank != 0:
         return
     d = workload(args.config)
     cores = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from oracle_ffi import Oracle
-    m = d.meta
-    o = Oracle(d.size, d.sub_size, d.flags, vlevels=m["vlevels"], nVcycles=m["nVcycles"],
-               interior_smoothing=m["interior_smoothing"], boundary_smoothing=m["boundary_smoothing"],
-               sigma_levels=m["sigma_levels"], sigma_smoothing=m["sigma_smoothing"], sigma_mg=m["sigma_mg"])
+    t0 = time.time()
+    o = make_oracle(d)
+    print(f"[bench reference] {d.name}: oracle setup {time.time() - t0:.1f} s", file=sys.stderr, flush=True)
+    iters = SAMPLE_ITERATIONS[args.config]
     for _ in range(args.warmup):
-        o.solve(d.rhs, tol=1e-6, max_it=500)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.time()
-        o.solve(d.rhs, tol=1e-6, max_it=500)
-        times.append(time.time() - t0)
-    tot = sum(times)
-    v = args.steps / tot
+        oracle_sample(o, d, iters)
+    times = [oracle_sample(o, d, iters) for _ in range(args.steps)]
+    per_solve = [t / iters * ORACLE_ITERATIONS[args.config] for t in times]
+    v = len(per_solve) / sum(per_solve)
+    lat = np.sort(np.array(per_solve) * 1000.0)
     line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": 0, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": float(np.mean(per_solve)) * 1000.0, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": d.name, "size": list(d.size), "sub_size": list(d.sub_size)},
+            "config": {"workload": d.name, "size": list(d.size), "sub_size": list(d.sub_size),
+                       "vlevels": d.meta["vlevels"], "sigma_levels": d.meta["sigma_levels"], "tol": 1e-6},
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
-                             "sample": f"{args.steps} full solves of {d.name} on the host cores"},
+                             "sample": (f"each step: {iters} PCG iteration(s) of {d.name} on the oracle "
+                                        f"(OpenMP, {cores} threads), scaled to a "
+                                        f"{ORACLE_ITERATIONS[args.config]}-iteration solve")},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -351,10 +374,9 @@ def main():
         "kernels": per_kernel,
         "clocks": clk.summary(),
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from hierarchicaldd_b200 import domains
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.config in ORACLE_ITERATIONS:
         try:
-            line["cpu_baseline"] = cpu_baseline(domains.config1(), os.cpu_count())
+            line["cpu_baseline"] = cpu_baseline(args, d)
         except Exception as e:  # reported, not fatal
             line["cpu_baseline"] = {"error": str(e)}
     s.close()

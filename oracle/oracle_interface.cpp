@@ -3,6 +3,7 @@
 // reference's third-party solvers.
 #include "oracle_interface.h"
 
+#include <string>
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -569,6 +570,18 @@ struct BuildState {
 
 static inline uint64_t rc(int r, int c) { return ((uint64_t)(uint32_t)r << 32) | (uint32_t)c; }
 
+// One subdomain's interface contributions with subdomain-local interface
+// numbers: the nodes in local first-encounter order and every Arr addition in
+// traversal order, so a serial merge in subdomain order reproduces the global
+// first-encounter numbering and the per-key summation order exactly.
+template <class T>
+struct LocalIface {
+    int M = 0;
+    std::vector<std::unordered_map<uint64_t, int>> hash;     // [level] node -> local id
+    std::vector<std::vector<I3>> nodes;                      // [level] local id -> node
+    std::vector<std::vector<std::pair<uint64_t, T>>> arr;    // [level] (rc(local, local), value)
+};
+
 static bool range_contains(const I3& lo, const I3& hi, const I3& rlo, const I3& rhi) {
     for (int a = 0; a < 3; ++a)
         if (!(lo[a] <= rlo[a] && rhi[a] <= hi[a])) return false;
@@ -577,11 +590,15 @@ static bool range_contains(const I3& lo, const I3& hi, const I3& rlo, const I3& 
 
 // CPU/Interface_Solver/INTERFACE_MATRIX_GENERATOR.h:130-659 for one subdomain.
 template <class T>
-static void create_subdomain_hierarchy(const SubsetFlags& sf, BuildState<T>& st,
-                                       std::vector<Csr<T>>& Aii_out, std::vector<Csr<T>>& Air_out,
+static void create_subdomain_hierarchy(const SubsetFlags& sf, LocalIface<T>& li,
+                                       std::vector<Csr<T>>& Aii_out,
+                                       std::vector<std::unordered_map<uint64_t, T>>& Air_out,
                                        std::vector<int>& n_interior_out,
                                        std::vector<std::vector<std::array<int, 3>>>& pos_out) {
-    const int M = st.M;
+    const int M = li.M;
+    li.hash.assign(M, {});
+    li.nodes.assign(M, {});
+    li.arr.assign(M, {});
     const I3 lo = sf.lo, hi = sf.hi;
     static const std::array<M8<T>, 8> P = bake_cell_prolongation<T>();
     Stride3 qtop;
@@ -673,21 +690,21 @@ static void create_subdomain_hierarchy(const SubsetFlags& sf, BuildState<T>& st,
     };
 
     Aii_out.assign(M, Csr<T>());
-    Air_out.assign(M, Csr<T>());
+    Air_out.assign(M, {});
     n_interior_out.assign(M, 0);
     std::vector<int> node_counts(M + 1, 0);
 
     for (int m = 1; m <= M; ++m) {
         // Interface DOFs (lines 249-312).
-        auto add_iface = [&](const I3& node, bool record_map) {
-            auto& hash = st.iface_hash[m - 1];
+        auto add_iface = [&](const I3& node, bool) {
+            auto& hash = li.hash[m - 1];
             uint64_t key = pack3(node);
             auto it = hash.find(key);
             int id;
             if (it == hash.end()) {
-                id = st.iface_counter[m - 1]++;
+                id = (int)li.nodes[m - 1].size();
                 hash.emplace(key, id);
-                if (record_map) st.iface_map.push_back(node);
+                li.nodes[m - 1].push_back(node);
             } else id = it->second;
             NodeRec& rec = H[m][m][key];
             rec.index = id;
@@ -805,7 +822,7 @@ static void create_subdomain_hierarchy(const SubsetFlags& sf, BuildState<T>& st,
                                 resolve(L, p2.first, f2, id2);
                                 T v = p1.second * p2.second * e;
                                 if ((f1 & U_NODE_INTERFACE) && (f2 & U_NODE_INTERFACE))
-                                    st.Arr[m - 1][rc(id1, id2)] += v;
+                                    li.arr[m - 1].push_back({rc(id1, id2), v});
                                 if ((f1 & (NODE_ACTIVE | NODE_COARSE_SHARED)) &&
                                     (f2 & (NODE_ACTIVE | NODE_COARSE_SHARED)))
                                     Aii[rc(id1, id2)] += v;
@@ -817,8 +834,8 @@ static void create_subdomain_hierarchy(const SubsetFlags& sf, BuildState<T>& st,
         int ni = node_counts[m];
         n_interior_out[m - 1] = ni;
         Aii_out[m - 1] = csr_from_map<T>(ni, ni, Aii);
-        // Interface column count is fixed after all subdomains; patched later.
-        Air_out[m - 1] = csr_from_map<T>(ni, INT_MAX, Air);
+        // Columns are local interface numbers until the merge.
+        Air_out[m - 1] = std::move(Air);
     }
 }
 
@@ -879,24 +896,61 @@ void build_interface_system(const Dims& gd, const uint32_t* gflags_in, const int
     out.Air.assign(M, std::vector<Csr<T>>(out.n_sub));
     out.n_interior.assign(M, std::vector<int>(out.n_sub, 0));
     out.aii_xyz.assign(M, std::vector<std::vector<std::array<int, 3>>>(out.n_sub));
-    int s = 0;
-    for (int i = 0; i < ns[0]; ++i)
-        for (int j = 0; j < ns[1]; ++j)
-            for (int k = 0; k < ns[2]; ++k, ++s) {
+    // Subdomains are built concurrently in chunks, then merged serially in
+    // subdomain order (the reference's traversal order).
+    const int nsub = out.n_sub;
+    const int chunk = 64;
+    for (int s0 = 0; s0 < nsub; s0 += chunk) {
+        const int s1 = std::min(nsub, s0 + chunk);
+        std::vector<LocalIface<T>> li(s1 - s0);
+        std::vector<std::vector<std::unordered_map<uint64_t, T>>> air(s1 - s0);
+        std::vector<std::string> err(s1 - s0);
+#pragma omp parallel for schedule(dynamic)
+        for (int s = s0; s < s1; ++s) {
+            try {
+                const int i = s / (ns[1] * ns[2]), j = (s / ns[2]) % ns[1], k = s % ns[2];
                 I3 lo = {i * sub[0], j * sub[1], k * sub[2]};
                 I3 hi = {lo[0] + sub[0], lo[1] + sub[1], lo[2] + sub[2]};
                 SubsetFlags sf = extract_subset(gd, gflags_in, lo, hi, sub);
-                std::vector<Csr<T>> aii, air;
+                std::vector<Csr<T>> aii;
                 std::vector<int> ni;
                 std::vector<std::vector<std::array<int, 3>>> pos(M);
-                create_subdomain_hierarchy<T>(sf, st, aii, air, ni, pos);
+                li[s - s0].M = M;
+                create_subdomain_hierarchy<T>(sf, li[s - s0], aii, air[s - s0], ni, pos);
                 for (int m = 0; m < M; ++m) {
                     out.aii_xyz[m][s] = std::move(pos[m]);
                     out.Aii[m][s] = std::move(aii[m]);
-                    out.Air[m][s] = std::move(air[m]);
                     out.n_interior[m][s] = ni[m];
                 }
+            } catch (const std::exception& e) {
+                err[s - s0] = e.what();
             }
+        }
+        for (auto& e : err)
+            if (!e.empty()) throw std::runtime_error(e);
+        for (int s = s0; s < s1; ++s) {
+            LocalIface<T>& L = li[s - s0];
+            for (int m = 0; m < M; ++m) {
+                std::vector<int> to_g(L.nodes[m].size());
+                for (size_t q = 0; q < L.nodes[m].size(); ++q) {
+                    const uint64_t key = pack3(L.nodes[m][q]);
+                    auto it = st.iface_hash[m].find(key);
+                    if (it == st.iface_hash[m].end()) {
+                        it = st.iface_hash[m].emplace(key, st.iface_counter[m]++).first;
+                        if (m == 0) st.iface_map.push_back(L.nodes[m][q]);
+                    }
+                    to_g[q] = it->second;
+                }
+                for (auto& t : L.arr[m])
+                    st.Arr[m][rc(to_g[(int)(t.first >> 32)], to_g[(int)(uint32_t)t.first])] += t.second;
+                std::unordered_map<uint64_t, T> ag;
+                ag.reserve(air[s - s0][m].size());
+                for (auto& kv : air[s - s0][m])
+                    ag.emplace(rc((int)(kv.first >> 32), to_g[(int)(uint32_t)kv.first]), kv.second);
+                out.Air[m][s] = csr_from_map<T>(out.n_interior[m][s], INT_MAX, ag);
+            }
+        }
+    }
     out.n_iface = st.iface_counter;
     out.iface_map = st.iface_map;
     out.iface_xyz.assign(M, {});
