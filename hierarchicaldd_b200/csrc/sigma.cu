@@ -253,9 +253,33 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
                     xv.swap(yv);
                 }
                 bottom_contraction = rho;
-                if (std::pow(rho, 200.0) > 1e-7)
-                    throw Error(HDD_ERR_UNSUPPORTED,
-                                "coarsest sigma smoother does not converge in 200 steps (rho=" + std::to_string(rho) + ")");
+                bottom_exact = std::pow(rho, 200.0) <= 1e-7;
+                if (verbose)
+                    std::fprintf(stderr, "[hdd setup] coarsest sigma smoother: rho %.4f, %s\n", rho,
+                                 bottom_exact ? "exact Schur solve" : "200 literal smoothing steps");
+            }
+            if (!bottom_exact) {
+                // The 200 steps have not converged to S^{-1} b: run them as the
+                // reference does, with this level's solve plans.
+                std::vector<std::string> err2(ih.n_sub);
+#pragma omp parallel for schedule(dynamic)
+                for (int sd = 0; sd < ih.n_sub; ++sd) {
+                    try {
+                        if (aii[sd].n > 0) aii[sd].build_solve_blocks();
+                    } catch (const std::exception& e) { err2[sd] = e.what(); }
+                }
+                for (auto& e : err2)
+                    if (!e.empty()) throw Error(HDD_ERR_INTERNAL, "subdomain solve blocks: " + e);
+                arrf.build_solve_blocks();
+                std::vector<const SnFactor*> fs;
+                std::vector<int> offs;
+                for (int sd = 0; sd < ih.n_sub; ++sd)
+                    if (aii[sd].n > 0) { fs.push_back(&aii[sd]); offs.push_back(off[sd]); }
+                L.aii.build(fs, offs, s);
+                L.arr_solve.build({&arrf}, {0}, s);
+                device_bytes += L.aii.bytes + L.arr_solve.bytes;
+                stamp("device plans (coarsest level, literal smoothing)", l);
+                continue;
             }
             // K = [Aii (block diagonal) , -Air ; -Air^T , Arr]; factor() adds eps to the diagonal.
             const int ni = L.n_int;
@@ -327,7 +351,9 @@ void SigmaGpu::vcycle(cudaStream_t s, long long& launches, PhaseHook* hook) {
         launch_fill(lv[l + 1].u, lv[l + 1].n_iface, 0.0f, s, launches);
         launch_csr(L.prrT, L.r, nullptr, lv[l + 1].b, 0, s, launches); // b_{l+1} = Prr^T r
     }
-    {
+    if (!bottom_exact) {
+        for (int i = 0; i < kBottomSmoothing; ++i) smooth(M - 1);
+    } else {
         SigmaLevel& B = lv[M - 1];
         if (n_bottom > 0) {
             // Right-hand side [0; b], solution's interface block -> u.

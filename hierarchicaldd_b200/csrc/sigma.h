@@ -149,6 +149,10 @@ struct SigmaGpu {
     float *kb = nullptr, *kx = nullptr;
     int n_bottom = 0, n_bottom_int = 0;
     double bottom_contraction = 0;   // estimated spectral radius of the bottom smoother
+    // True when 200 bottom smoothing steps have converged to S^{-1} b (rho^200 <=
+    // 1e-7), so the coarsest level is one solve of K; false runs the 200 steps.
+    bool bottom_exact = true;
+    static constexpr int kBottomSmoothing = 200;  // SIGMA_MULTIGRID_SOLVER.cpp:78
     size_t device_bytes = 0;
     void setup(const InterfaceHost& ih, int smoothing_iterations, cudaStream_t s);
     void release();

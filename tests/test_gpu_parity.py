@@ -196,3 +196,20 @@ def test_sub32_cluster_vcycle_and_pcg():
     xo, it_o, _ = o.solve(d.rhs, tol=1e-6)
     assert res["converged"] == 1 and abs(res["iterations"] - it_o) <= 1, (res["iterations"], it_o)
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-5
+
+
+def test_sigma_literal_bottom_smoothing(capfd, monkeypatch):
+    """A coarsest sigma level whose smoother contracts slowly (rho ~0.96 here):
+    the 200 bottom smoothing steps have not converged to the Schur solve, so the
+    GPU runs them literally, as the reference does; it must match the oracle."""
+    monkeypatch.setenv("HDD_VERBOSE", "1")
+    d = domains.profile_case()
+    s, o = make_pair(d, sigma_levels=2)
+    try:
+        err = capfd.readouterr().err
+        assert "200 literal smoothing steps" in err, err[-2000:]
+        rng = np.random.default_rng(7)
+        b0 = rng.standard_normal(o.num_interface(0)).astype(np.float32)
+        assert rel_inf(s.Sigma_V_Cycle(b0), o.sigma_vcycle(b0)) < PRECOND_RTOL
+    finally:
+        s.close()
