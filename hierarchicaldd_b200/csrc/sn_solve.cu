@@ -41,8 +41,8 @@ namespace hdd {
 namespace {
 
 constexpr int kNT = 256;                 // threads per CTA
-constexpr int kRB = 256;                 // rows per forward row block
-constexpr int kCC = 256;                 // columns per forward column block
+constexpr int kRB = 128;                 // rows per forward row block
+constexpr int kCC = 128;                 // columns per forward column block
 constexpr int kBC = 32;                  // columns per backward task (8 warps x 4)
 constexpr long kSpinLimit = 1L << 22;    // polls (with ~128 ns sleeps) before a wait gives up
 constexpr int kWarps = kNT / 32;         // small fronts per bundle (one per warp)
@@ -193,7 +193,7 @@ __device__ void warp_backward(const PlanView& P, int J, float* g, int lane, floa
     if (lane == 0) atomicAdd(done + J, 1);
 }
 
-__global__ void __launch_bounds__(kNT) sn_forward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks,
+__global__ void __launch_bounds__(kNT, 8) sn_forward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks,
                                                          const float* __restrict__ b_old) {
     extern __shared__ float sh[];
     float* f = sh;                 // the front's input vector, m entries
@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(kNT) sn_forward_kernel(PlanView P, const SnTas
     }
 }
 
-__global__ void __launch_bounds__(kNT) sn_backward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks,
+__global__ void __launch_bounds__(kNT, 8) sn_backward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks,
                                                           float* __restrict__ x_old) {
     extern __shared__ float g[];   // [y_J; x_R], m entries
     __shared__ int s_ticket;
