@@ -116,63 +116,79 @@ __device__ __noinline__ void jacobi_sweep(const G& g, const LevelSmem& L, int mo
     g.sync();
 }
 
-// Jacobi sweep of a whole box level with one x-line (NX cells) per thread of
-// g: no index division per cell and the line's residuals in registers.  The
-// per-cell arithmetic is cell_residual's, so results equal jacobi_sweep's.
-template <int NX, class G>
+// Jacobi sweep of a whole box level: each of the NX*NX x-lines (NX cells) is
+// cut into PARTS contiguous pieces, one per thread of g, so there is no index
+// division per cell and a piece's residuals stay in registers.  The per-cell
+// arithmetic is cell_residual's, so results equal jacobi_sweep's.
+template <int NX, int PARTS, class G>
 __device__ __noinline__ void box_line_sweep(const G& g, const LevelSmem& L, int mode, const float* inv_diag) {
     constexpr int e = NX + 2, PS = e * e;
+    constexpr int CPT = (NX + PARTS - 1) / PARTS;   // cells per thread
     const int t = g.rank();
-    float rr[NX];
+    float rr[CPT];
     uint32_t tk = 0;
-    int base = 0;
-    if (t < NX * NX) {
-        const int y = t / NX + 1, z = t % NX + 1;
+    int base = 0, k0 = 0;
+    if (t < NX * NX * PARTS) {
+        const int line = t % (NX * NX), part = t / (NX * NX);
+        const int y = line / NX + 1, z = line % NX + 1;
+        k0 = part * CPT;
         base = PS + y * e + z;
 #pragma unroll
-        for (int k = 0; k < NX; ++k) {
+        for (int c = 0; c < CPT; ++c) {
+            rr[c] = 0.0f;
+            const int k = k0 + c;
+            if (k >= NX) continue;
             const int i = base + k * PS;
             const uint32_t fl = L.f[i];
             const bool active = fl & C_ACTIVE;
             const bool bnd = fl & C_BOUNDARY8;
             const bool take = active && ((mode == 3) || (mode == 1 && bnd) || (mode == 2 && !bnd));
-            rr[k] = 0.0f;
             if (take) {
-                tk |= 1u << k;
-                rr[k] = cell_residual(L, i, fl);
+                tk |= 1u << c;
+                rr[c] = cell_residual(L, i, fl);
             }
         }
     }
     g.sync();
     if (tk) {
 #pragma unroll
-        for (int k = 0; k < NX; ++k) {
-            if (tk & (1u << k)) {
-                const int i = base + k * PS;
+        for (int c = 0; c < CPT; ++c) {
+            if (tk & (1u << c)) {
+                const int i = base + (k0 + c) * PS;
                 const float w = inv_diag[__popc((uint32_t)L.f[i] & C_FACES)];
-                L.u[i] = __fadd_rn(L.u[i], __fmul_rn(w, rr[k]));
+                L.u[i] = __fadd_rn(L.u[i], __fmul_rn(w, rr[c]));
             }
         }
     }
     g.sync();
 }
 
-// One Jacobi sweep of a box level; levels up to 17^3 cells use one x-line
-// per thread, larger ones the chunked sweep.
+// One Jacobi sweep of a box level; levels up to 17^3 cells cut their x-lines
+// over as many threads as the group has, larger ones use the chunked sweep.
 template <int CH, class G>
 __device__ void sweep_box(const G& g, const LevelSmem& L, int mode, const float* inv_diag) {
-    const int m = L.e - 2;
-    if (m * m > g.size()) {  // more lines than threads
-        jacobi_sweep<CH>(g, L, mode, inv_diag);
-        return;
-    }
+    const int n = g.size();
     switch (L.e) {
-        case 3: box_line_sweep<1>(g, L, mode, inv_diag); break;
-        case 5: box_line_sweep<3>(g, L, mode, inv_diag); break;
-        case 9: box_line_sweep<7>(g, L, mode, inv_diag); break;
-        case 17: box_line_sweep<15>(g, L, mode, inv_diag); break;
-        default: jacobi_sweep<CH>(g, L, mode, inv_diag); break;
+        case 3: box_line_sweep<1, 1>(g, L, mode, inv_diag); return;
+        case 5:
+            if (n >= 27) box_line_sweep<3, 3>(g, L, mode, inv_diag);
+            else if (n >= 9) box_line_sweep<3, 1>(g, L, mode, inv_diag);
+            else break;
+            return;
+        case 9:
+            if (n >= 343) box_line_sweep<7, 7>(g, L, mode, inv_diag);
+            else if (n >= 98) box_line_sweep<7, 2>(g, L, mode, inv_diag);
+            else if (n >= 49) box_line_sweep<7, 1>(g, L, mode, inv_diag);
+            else break;
+            return;
+        case 17:
+            if (n >= 450) box_line_sweep<15, 2>(g, L, mode, inv_diag);
+            else if (n >= 225) box_line_sweep<15, 1>(g, L, mode, inv_diag);
+            else break;
+            return;
+        default: break;
     }
+    jacobi_sweep<CH>(g, L, mode, inv_diag);
 }
 
 // r = b - A u at Active cells (other cells of r keep their zero).
