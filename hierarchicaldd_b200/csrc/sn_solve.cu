@@ -129,13 +129,12 @@ __device__ __forceinline__ void warp_forward_rows(const PlanView& P, int J, int 
 __device__ void warp_forward(const PlanView& P, int J, float* f, int lane, const float* b_old, int* done) {
     const int nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
     const int cb = P.child_ptr[J], ce = P.child_ptr[J + 1];
+    for (int i = lane; i < m; i += 32) f[i] = (i < nj) ? b_old[P.perm[c0 + i]] : 0.0f;
     if (lane == 0) {
         bool ok = true;
         for (int c = cb; c < ce; ++c) ok &= wait_at_least(done + P.child[c], P.ntf[P.child[c]], P.err);
         if (!ok) atomicExch(P.err, 1);
     }
-    __syncwarp();
-    for (int i = lane; i < m; i += 32) f[i] = (i < nj) ? b_old[P.perm[c0 + i]] : 0.0f;
     __syncwarp();
     for (int c = cb; c < ce; ++c) {
         const int C = P.child[c];
@@ -156,13 +155,14 @@ __device__ void warp_forward(const PlanView& P, int J, float* f, int lane, const
 // Backward solve of one small front by one warp: x_a = sum_{r >= a} Fw(r, a) g_r.
 __device__ void warp_backward(const PlanView& P, int J, float* g, int lane, float* x_old, int* done) {
     const int nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
+    const int* rows = P.rows + P.rows_off[J];
+    for (int i = lane; i < nj; i += 32) g[i] = P.ynew[c0 + i];   // from the forward launch
     if (lane == 0) {
         const int p = P.parent[J];
         if (p >= 0 && !wait_at_least(done + p, P.ntb[p], P.err)) atomicExch(P.err, 1);
     }
     __syncwarp();
-    const int* rows = P.rows + P.rows_off[J];
-    for (int i = lane; i < m; i += 32) g[i] = (i < nj) ? P.ynew[c0 + i] : __ldcg(P.xnew + rows[i - nj]);
+    for (int i = nj + lane; i < m; i += 32) g[i] = __ldcg(P.xnew + rows[i - nj]);
     __syncwarp();
     const size_t ld = (size_t)((m + 3) & ~3);
     const float* A = P.fw + P.fw_off[J];
@@ -216,13 +216,32 @@ __global__ void __launch_bounds__(kNT, 8) sn_forward_kernel(PlanView P, const Sn
         }
         const int J = T.front, nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
         const int cb = P.child_ptr[J], ce = P.child_ptr[J + 1];
+        // Row lanes x column slices; each thread's first eight coefficients
+        // are requested before the dependency wait and the assembly.
+        const int mr = (T.rows + 31) & ~31;
+        const int ks = kNT / mr;
+        const int sl = tid / mr, lr = tid - sl * mr;
+        const int row = T.r0 + lr;
+        const bool active = sl < ks && lr < T.rows;
+        int cbeg = 0, cend = 0;
+        const size_t ld = (size_t)((m + 3) & ~3);
+        const float* A = P.fw + P.fw_off[J] + row;
+        float v0[8];
+        if (active) {
+            const int cs = (T.ncols + ks - 1) / ks;
+            cbeg = T.c0 + sl * cs;
+            cend = min(T.c0 + T.ncols, cbeg + cs);
+            if (row < nj) cend = min(cend, row + 1);  // L_JJ^{-1} is lower triangular
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v0[u] = (cbeg + u < cend) ? __ldg(A + (size_t)(cbeg + u) * ld) : 0.0f;
+        // b's part of the input vector does not depend on other fronts.
+        for (int i = tid; i < m; i += kNT) f[i] = (i < nj) ? b_old[P.perm[c0 + i]] : 0.0f;
         if (tid == 0) {
             bool ok = true;
             for (int c = cb; c < ce; ++c) ok &= wait_at_least(done + P.child[c], P.ntf[P.child[c]], P.err);
             if (!ok) atomicExch(P.err, 1);
         }
-        __syncthreads();
-        for (int i = tid; i < m; i += kNT) f[i] = (i < nj) ? b_old[P.perm[c0 + i]] : 0.0f;
         __syncthreads();
         for (int c = cb; c < ce; ++c) {
             const int C = P.child[c];
@@ -232,21 +251,12 @@ __global__ void __launch_bounds__(kNT, 8) sn_forward_kernel(PlanView P, const Sn
             for (int k = tid; k < mc; k += kNT) f[rm[k]] += __ldcg(uc + k);
             __syncthreads();
         }
-        // Row lanes x column slices.
-        const int mr = (T.rows + 31) & ~31;
-        const int ks = kNT / mr;
-        const int sl = tid / mr, lr = tid - sl * mr;
-        const int row = T.r0 + lr;
-        const bool active = sl < ks && lr < T.rows;
         float acc = 0.0f;
         if (active) {
-            const int cs = (T.ncols + ks - 1) / ks;
-            const int cbeg = T.c0 + sl * cs;
-            int cend = min(T.c0 + T.ncols, cbeg + cs);
-            if (row < nj) cend = min(cend, row + 1);  // L_JJ^{-1} is lower triangular
-            const size_t ld = (size_t)((m + 3) & ~3);
-            const float* A = P.fw + P.fw_off[J] + row;
-            int c = cbeg;
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (cbeg + u < cend) acc = fmaf(v0[u], f[cbeg + u], acc);
+            int c = cbeg + 8;
             for (; c + 8 <= cend; c += 8) {
                 float v[8];
 #pragma unroll
@@ -311,15 +321,16 @@ __global__ void __launch_bounds__(kNT, 8) sn_backward_kernel(PlanView P, const S
             continue;
         }
         const int J = T.front, nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
+        const int a0 = T.r0, na = T.rows;
+        const int rs = a0 & ~31;
+        const int* rows = P.rows + P.rows_off[J];
+        for (int i = rs + tid; i < nj; i += kNT) g[i] = P.ynew[c0 + i];   // from the forward launch
         if (tid == 0) {
             const int p = P.parent[J];
             if (p >= 0 && !wait_at_least(done + p, P.ntb[p], P.err)) atomicExch(P.err, 1);
         }
         __syncthreads();
-        const int a0 = T.r0, na = T.rows;
-        const int rs = a0 & ~31;
-        const int* rows = P.rows + P.rows_off[J];
-        for (int i = rs + tid; i < m; i += kNT) g[i] = (i < nj) ? P.ynew[c0 + i] : __ldcg(P.xnew + rows[i - nj]);
+        for (int i = max(rs, nj) + tid; i < m; i += kNT) g[i] = __ldcg(P.xnew + rows[i - nj]);
         __syncthreads();
         const size_t ld = (size_t)((m + 3) & ~3);
         const float* A = P.fw + P.fw_off[J];

@@ -3,6 +3,8 @@
 // reference's third-party solvers.
 #include "oracle_interface.h"
 
+#include <cstdlib>
+#include <chrono>
 #include <string>
 #include <algorithm>
 #include <climits>
@@ -1005,11 +1007,20 @@ void SigmaSolver<T>::initialize(const InterfaceSystem<T>& s, int smoothing_itera
     const double eps = 1e-5;  // Eigen_To_Pardiso default epsilon, SIGMA_SMOOTHER.cpp:176
     arr.resize(s.M);
     aii.assign(s.M, std::vector<Cholesky>(s.n_sub));
+    const bool verbose = std::getenv("HDDO_VERBOSE") != nullptr;
+    auto t0 = std::chrono::steady_clock::now();
+    auto stamp = [&](const char* what, int l) {
+        if (!verbose) return;
+        const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::fprintf(stderr, "[oracle setup]   level %d %s at %.2f s\n", l, what, sec);
+    };
     for (int l = 0; l < s.M; ++l) {
         arr[l].factor(s.Arr[l], eps, &s.iface_xyz[l]);
+        stamp("interface factor", l);
 #pragma omp parallel for schedule(dynamic)
         for (int sd = 0; sd < s.n_sub; ++sd)
             if (s.n_interior[l][sd] > 0) aii[l][sd].factor(s.Aii[l][sd], eps, &s.aii_xyz[l][sd]);
+        stamp("subdomain factors", l);
     }
     u.resize(s.M);
     r.resize(s.M);
