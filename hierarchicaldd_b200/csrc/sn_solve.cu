@@ -324,7 +324,27 @@ __global__ void __launch_bounds__(kNT, 8) sn_backward_kernel(PlanView P, const S
         const int a0 = T.r0, na = T.rows;
         const int rs = a0 & ~31;
         const int* rows = P.rows + P.rows_off[J];
+        const size_t ld = (size_t)((m + 3) & ~3);
+        const float* A = P.fw + P.fw_off[J];
+        float s4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        const int amin = a0 + w;
+        // Rows below nj (the L_JJ^{-T} y part) need only this front's forward
+        // result, so they are summed before waiting on the parent; each lane
+        // still adds its rows in ascending order.
         for (int i = rs + tid; i < nj; i += kNT) g[i] = P.ynew[c0 + i];   // from the forward launch
+        __syncthreads();
+        int r = (amin & ~31) + lane;
+        if (amin < a0 + na) {
+#pragma unroll 4
+            for (; r < nj; r += 32) {
+                const float gr = g[r];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int a = amin + 8 * j;
+                    if (a < a0 + na && r >= a) s4[j] = fmaf(__ldg(A + (size_t)a * ld + r), gr, s4[j]);
+                }
+            }
+        }
         if (tid == 0) {
             const int p = P.parent[J];
             if (p >= 0 && !wait_at_least(done + p, P.ntb[p], P.err)) atomicExch(P.err, 1);
@@ -332,18 +352,14 @@ __global__ void __launch_bounds__(kNT, 8) sn_backward_kernel(PlanView P, const S
         __syncthreads();
         for (int i = max(rs, nj) + tid; i < m; i += kNT) g[i] = __ldcg(P.xnew + rows[i - nj]);
         __syncthreads();
-        const size_t ld = (size_t)((m + 3) & ~3);
-        const float* A = P.fw + P.fw_off[J];
-        float s4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-        const int amin = a0 + w;
         if (amin < a0 + na) {
 #pragma unroll 4
-            for (int r = (amin & ~31) + lane; r < m; r += 32) {
+            for (; r < m; r += 32) {
                 const float gr = g[r];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const int a = amin + 8 * j;
-                    if (a < a0 + na && r >= a) s4[j] = fmaf(__ldg(A + (size_t)a * ld + r), gr, s4[j]);
+                    if (a < a0 + na) s4[j] = fmaf(__ldg(A + (size_t)a * ld + r), gr, s4[j]);
                 }
             }
         }
