@@ -111,10 +111,15 @@ hdd_status hdd_load_spgrid_dir(hdd_solver* s, const char* dir) {
             !read_file(d + "/data", fd))
             throw Error(HDD_ERR_IO, "cannot read SPGrid directory " + d);
         if (fs.size() != 12) throw Error(HDD_ERR_UNSUPPORTED, "only 3D SPGrid directories are supported");
+        // The writer stores the allocator's padded size (a multiple of the block
+        // size), so any size at least options.size is accepted; cells beyond
+        // options.size are ignored.
         int32_t size[3];
         std::memcpy(size, fs.data(), 12);
         for (int a = 0; a < 3; ++a)
-            if (size[a] != v.opts.size[a]) throw Error(HDD_ERR_INVALID_ARGUMENT, "SPGrid size differs from options.size");
+            if (size[a] < v.opts.size[a])
+                throw Error(HDD_ERR_INVALID_ARGUMENT, "SPGrid size is smaller than options.size");
+        for (int a = 0; a < 3; ++a) size[a] = v.opts.size[a];
         int32_t count = 0, alen = 0;
         if (fo.size() < 8) throw Error(HDD_ERR_IO, "truncated block_offset");
         std::memcpy(&count, fo.data(), 4);

@@ -490,6 +490,41 @@ struct SlabGeom {
     static constexpr int M2 = (SUB - 1) * (SUB - 1);
 };
 
+// The (y, z) x-line that thread t owns as its l-th line of a slab, or false.
+// Lines whose cells all lie within the Boundary band (3 cells) of the box's
+// y/z faces take boundary-sweep work on every cell; with 2 lines per thread
+// each thread gets at most one such line, so boundary sweeps are not paced by
+// threads holding two.  Any assignment gives the same results (Jacobi sweeps).
+template <int SUB, int NT, int LPT>
+__device__ __forceinline__ bool owned_line(int t, int l, int& y, int& z) {
+    constexpr int M1 = SUB - 1, D = 3, W = M1 - 2 * D;
+    constexpr int H = 2 * D * M1 + W * 2 * D;   // lines inside the band
+    constexpr int L = W * W;                    // the others
+    if constexpr (LPT == 2 && H <= NT && NT <= H + L && L <= 2 * NT - H) {
+        auto band = [](int i) { return i < D ? i + 1 : SUB - 2 * D + i; };  // 1..D, SUB-D..SUB-1
+        auto heavy = [&](int h) {
+            if (h < 2 * D * M1) { y = band(h / M1); z = h % M1 + 1; }
+            else { const int r = h - 2 * D * M1; y = D + 1 + r / (2 * D); z = band(r % (2 * D)); }
+        };
+        auto light = [&](int k) { y = D + 1 + k / W; z = D + 1 + k % W; };
+        if (t < H) {
+            if (l == 0) heavy(t);
+            else light(t);
+            return true;
+        }
+        const int j = t - H;
+        if (l == 0) { light(H + j); return true; }
+        if (NT + j < L) { light(NT + j); return true; }
+        return false;
+    } else {
+        const int q = t + l * NT;
+        if (q >= M1 * M1) return false;
+        y = q / M1 + 1;
+        z = q % M1 + 1;
+        return true;
+    }
+}
+
 template <int SUB, int C>
 size_t vcycle_cluster_smem_bytes(int levels) {
     using G = SlabGeom<SUB, C>;
@@ -612,11 +647,10 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
     };
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
-        const int q = threadIdx.x + l * NT;
         off[l] = -1;
         hlo[l] = hhi[l] = 0.0f;
-        if (q < M2) {
-            const int y = q / (SUB - 1) + 1, z = q % (SUB - 1) + 1;
+        int y = 0, z = 0;
+        if (owned_line<SUB, NT, LPT>(threadIdx.x, l, y, z)) {
             off[l] = y * E + z;
             hlo[l] = u0[off[l]];
             hhi[l] = u0[(np + 1) * PS + off[l]];

@@ -32,6 +32,7 @@ class SPGrid_Domain_Decomposition_Solver:
         self.flags = None
         self.rhs = None
         self.spgrid_dir = None
+        self.spgrid_size = None
         self.last_result = None
         self.options = None
 
@@ -41,7 +42,10 @@ class SPGrid_Domain_Decomposition_Solver:
         size = np.fromfile(os.path.join(base_dir, "size"), dtype=np.int32)
         if size.size != 3:
             raise HddError(5, "only 3D SPGrid directories are supported")
-        self.size = tuple(int(v) for v in size)
+        # The file holds the allocator's padded size; the grid size proper is
+        # the `size` given to Initialize_Preconditioner (at most this).
+        self.spgrid_size = tuple(int(v) for v in size)
+        self.size = None
         self.spgrid_dir = base_dir
         self.flags = self.rhs = None
 
@@ -61,7 +65,11 @@ class SPGrid_Domain_Decomposition_Solver:
         self.lib.hdd_options_default(C.byref(o))
         size = tuple(int(s) for s in (size if np.ndim(size) else (size,) * 3))
         sub = tuple(int(s) for s in (subdomain_size if np.ndim(subdomain_size) else (subdomain_size,) * 3))
-        if self.size is not None and tuple(size) != tuple(self.size):
+        if self.spgrid_dir is not None:
+            if any(a > b for a, b in zip(size, self.spgrid_size)):
+                raise HddError(1, f"size {size} exceeds the SPGrid directory's size {self.spgrid_size}")
+            self.size = tuple(size)
+        elif self.size is not None and tuple(size) != tuple(self.size):
             raise HddError(1, f"size {size} differs from the loaded domain {self.size}")
         for a in range(3):
             o.size[a] = size[a]

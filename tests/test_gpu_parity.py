@@ -213,3 +213,28 @@ def test_sigma_literal_bottom_smoothing(capfd, monkeypatch):
         assert rel_inf(s.Sigma_V_Cycle(b0), o.sigma_vcycle(b0)) < PRECOND_RTOL
     finally:
         s.close()
+
+
+def test_spgrid_directory_load_matches_dense(tmp_path):
+    """hdd_load_spgrid_dir reads the reference's on-disk format (padded size,
+    page offsets, per-block flags/data arrays) to the same domain as the dense
+    input: identical PCG iterations and solution."""
+    from hierarchicaldd_b200.solver import SPGrid_Domain_Decomposition_Solver
+    from spgrid_format import write_spgrid_dir
+    d = domains.small(32, 8, 6, seed=1)
+    write_spgrid_dir(str(tmp_path), d.flags, d.rhs)
+    m = d.meta
+    args = (m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"], m["interior_smoothing"],
+            m["boundary_smoothing"], m["sigma_smoothing"], m["sigma_mg"])
+    a = SPGrid_Domain_Decomposition_Solver()
+    a.Read_SPGrid(str(tmp_path))
+    a.Initialize_Preconditioner(*args)
+    ra, xa = a.Solve(), a.Solution()
+    a.close()
+    b = SPGrid_Domain_Decomposition_Solver()
+    b.Set_Domain(d.flags, d.rhs)
+    b.Initialize_Preconditioner(*args)
+    rb, xb = b.Solve(), b.Solution()
+    b.close()
+    assert ra["iterations"] == rb["iterations"]
+    assert np.array_equal(xa, xb)
