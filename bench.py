@@ -100,6 +100,21 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(x, dist, device):
+    """The maximum of a per-rank time over all ranks (the whole job's time)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, steps, seconds):
+    """Whole-job solves/s: every rank (replica) solves `steps` times."""
+    return world * steps / seconds
+
+
 def workload(cfg):
     from hierarchicaldd_b200 import domains
     return domains.CONFIGS[cfg]()
@@ -285,12 +300,8 @@ def main():
         t_wall = time.time() - t_wall
     launches = s.Kernel_Launches() - launches0
     dev_ms = np.array([r["solve_ms"] for r in res])
-    total_ms = float(dev_ms.sum())
-    if dist is not None:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * args.steps / (total_ms / 1000.0)
+    total_ms = max_over_ranks(float(dev_ms.sum()), dist, "cuda")
+    value = job_throughput(world, args.steps, total_ms / 1000.0)
 
     # End to end through the C ABI with pinned host buffers: H2D of b, solve, D2H of x.
     cells = int(np.prod(d.size))
@@ -300,20 +311,16 @@ def main():
     lib = _lib.load()
     fp = lambda t: C.cast(t.data_ptr(), C.POINTER(C.c_float))
     barrier()
-    t_e2e = time.time()
+    t_e2e = time.perf_counter()
     for _ in range(args.steps):
         st = lib.hdd_set_rhs_dense(s.h, fp(pin_b))
         assert st == 0, st
         s.Solve()
         st = lib.hdd_get_solution_dense(s.h, fp(pin_x))
         assert st == 0, st
-    barrier()
-    t_e2e = time.time() - t_e2e
-    e2e_val = world * args.steps / t_e2e
-    if dist is not None:
-        t = torch.tensor([t_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_val = world * args.steps / float(t.item())
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t_e2e     # host copies are part of this step, so host time
+    e2e_val = job_throughput(world, args.steps, max_over_ranks(t_e2e, dist, "cuda"))
 
     # Per-phase device timing (separate, instrumented solve): CUDA events on
     # the solver's stream around each phase's launches, with the phase's
