@@ -8,15 +8,16 @@
 //   products use an explicitly transposed CSR), so all sums are deterministic
 //   and follow the order of the host restatement.
 // * The PARDISO solves are supernodal triangular solves over nested-dissection
-//   fronts (sn_solve.cu): each front's explicit inverse blocks are cut into
-//   64-row tasks streamed through shared memory, one launch per tree level.
+//   fronts (sn_solve.cu): one persistent launch per solve direction walks the
+//   fronts in dependency order.
 // * The coarsest level's 200 smoothing steps (SIGMA_MULTIGRID_SOLVER.cpp:78)
 //   form a contraction whose fixed point is the Schur complement solve
 //   S^{-1} b with S = Arr+eps - sum_s Air_s^T (Aii_s+eps)^{-1} Air_s; setup
-//   estimates the contraction factor rho and checks rho^200 < 1e-7.  S^{-1} b
-//   is the interface block of the solution of K [x_i; x_G] = [0; b] with
-//   K = [Aii+eps, -Air; -Air^T, Arr+eps], so the coarsest level is one sparse
-//   supernodal solve of K instead of 200 dependent smoothing steps.
+//   estimates the contraction factor rho.  When rho^200 <= 1e-7 the steps
+//   have converged, and S^{-1} b is computed as the interface block of the
+//   solution of K [x_i; x_G] = [0; b] with K = [Aii+eps, -Air; -Air^T, Arr+eps]:
+//   one sparse supernodal solve of K instead of 200 dependent smoothing steps.
+//   Otherwise the 200 steps run as written.
 #include <cuda_runtime.h>
 
 #include <algorithm>
