@@ -1,0 +1,158 @@
+// Test shim: the product's host-side setup code (layout, interface assembly,
+// supernodal Cholesky) compiled without CUDA device code, so the CPU test suite
+// can check it against the oracle.  Built by tests/test_cpu_host.py with g++.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "host_setup.h"
+#include "sigma.h"
+
+using namespace hdd;
+
+namespace {
+struct Shim {
+    DomainLayout L;
+    InterfaceHost ih;
+    std::string err;
+};
+const CsrF* pick(Shim* s, int kind, int level, int sub) {
+    if (level < 0 || level >= s->ih.M) return nullptr;
+    switch (kind) {
+        case 0: return &s->ih.Arr[level];
+        case 1: return (sub >= 0 && sub < s->ih.n_sub) ? &s->ih.Aii[level][sub] : nullptr;
+        case 2: return (sub >= 0 && sub < s->ih.n_sub) ? &s->ih.Air[level][sub] : nullptr;
+        case 3: return level < (int)s->ih.Prr.size() ? &s->ih.Prr[level] : nullptr;
+        default: return nullptr;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+// Layout and interface system of a dense flag array; NULL on error (message in err).
+void* shim_build(const int size[3], const int sub[3], int vlevels, int sigma_levels, const uint32_t* flags,
+                 char* err, int errlen) {
+    Shim* s = new Shim();
+    try {
+        Options o;
+        for (int a = 0; a < 3; ++a) { o.size[a] = size[a]; o.sub[a] = sub[a]; }
+        o.vlevels = vlevels;
+        o.nvcycles = 1;
+        o.interior = o.boundary = 1;
+        o.sigma_levels = sigma_levels;
+        o.sigma_smoothing = 3;
+        o.sigma_mg = 1;
+        build_layout(o, flags, s->L);
+        build_interface(s->L, sigma_levels, s->ih);
+        return s;
+    } catch (const std::exception& e) {
+        if (err && errlen > 0) { std::strncpy(err, e.what(), errlen - 1); err[errlen - 1] = 0; }
+        delete s;
+        return nullptr;
+    }
+}
+
+void shim_free(void* h) { delete static_cast<Shim*>(h); }
+
+int shim_num_subdomains(void* h) { return static_cast<Shim*>(h)->ih.n_sub; }
+
+// kind: 0 Arr, 1 Aii, 2 Air, 3 Prr.  shape = {rows, cols, nnz}; returns 0 on success.
+int shim_matrix_shape(void* h, int kind, int level, int sub, int* shape) {
+    const CsrF* m = pick(static_cast<Shim*>(h), kind, level, sub);
+    if (!m) return 1;
+    shape[0] = m->rows;
+    shape[1] = m->cols;
+    shape[2] = (int)m->col.size();
+    return 0;
+}
+
+int shim_matrix_get(void* h, int kind, int level, int sub, int* ptr, int* col, double* val) {
+    const CsrF* m = pick(static_cast<Shim*>(h), kind, level, sub);
+    if (!m) return 1;
+    for (size_t i = 0; i < m->ptr.size(); ++i) ptr[i] = m->ptr[i];
+    for (size_t i = 0; i < m->col.size(); ++i) { col[i] = m->col[i]; val[i] = m->val[i]; }
+    return 0;
+}
+
+// Factor (A + 1e-5 I) of one matrix with the supernodal Cholesky (geometric
+// ordering when positions exist), solve for a random right-hand side on the
+// host and return ||(A + 1e-5 I) x - b|| / ||b||; also checks that the explicit
+// solve blocks reproduce the same solution (returned in *blocks_diff).
+double shim_factor_check(void* h, int kind, int level, int sub, double* blocks_diff) {
+    Shim* s = static_cast<Shim*>(h);
+    const CsrF* m = pick(s, kind, level, sub);
+    if (!m || (kind != 0 && kind != 1) || m->rows == 0) return -1.0;
+    const std::vector<std::array<int, 3>>* xyz = nullptr;
+    if (kind == 0 && level < (int)s->ih.iface_xyz.size() && (int)s->ih.iface_xyz[level].size() == m->rows)
+        xyz = &s->ih.iface_xyz[level];
+    if (kind == 1 && (int)s->ih.aii_xyz[level][sub].size() == m->rows) xyz = &s->ih.aii_xyz[level][sub];
+    const double eps = 1e-5;
+    SnFactor F;
+    F.analyze(*m, xyz);
+    F.factor(*m, eps);
+    F.build_solve_blocks();
+    const int n = m->rows;
+    std::mt19937 rng(7);
+    std::uniform_real_distribution<double> U(-1.0, 1.0);
+    std::vector<double> b(n), x(n);
+    for (int i = 0; i < n; ++i) b[i] = U(rng);
+    x = b;
+    F.solve(x.data());
+    double rn = 0, bn = 0;
+    for (int r = 0; r < n; ++r) {
+        double ax = eps * x[r];
+        for (int p = m->ptr[r]; p < m->ptr[r + 1]; ++p) ax += (double)m->val[p] * x[m->col[p]];
+        rn += (ax - b[r]) * (ax - b[r]);
+        bn += b[r] * b[r];
+    }
+    // Same solve through the explicit blocks Fw = [Linv; -W] the GPU uses:
+    // forward [y; v] = Fw f + [0; f_R], backward x_J = Fw^T [y; x_R].
+    std::vector<double> f(n), y(n, 0.0), xn(n, 0.0);
+    for (int i = 0; i < n; ++i) f[i] = b[F.perm[i]];
+    const int ns = (int)F.col0.size();
+    std::vector<std::vector<double>> upd(ns);
+    std::vector<std::vector<int>> kids(ns);
+    for (int j = 0; j < ns; ++j)
+        if (F.parent[j] >= 0) kids[F.parent[j]].push_back(j);
+    std::vector<int> pos(n, -1);
+    for (int j = 0; j < ns; ++j) {
+        const int nj = F.ncol[j], nr = (int)F.rows[j].size(), mm = nj + nr;
+        std::vector<double> v(mm, 0.0);
+        for (int a = 0; a < nj; ++a) { v[a] = f[F.col0[j] + a]; pos[F.col0[j] + a] = a; }
+        for (int k = 0; k < nr; ++k) pos[F.rows[j][k]] = nj + k;
+        for (int c : kids[j])
+            for (size_t k = 0; k < F.rows[c].size(); ++k) v[pos[F.rows[c][k]]] += upd[c][k];
+        const std::vector<double>& W = F.Fw[j];
+        for (int r = 0; r < mm; ++r) {
+            double acc = 0;
+            for (int c = 0; c < nj; ++c) acc += W[(size_t)c * mm + r] * v[c];
+            if (r < nj) y[F.col0[j] + r] = acc;
+            else upd[j].push_back(v[r] + acc);
+        }
+    }
+    for (int j = ns - 1; j >= 0; --j) {
+        const int nj = F.ncol[j], nr = (int)F.rows[j].size(), mm = nj + nr;
+        const std::vector<double>& W = F.Fw[j];
+        for (int a = 0; a < nj; ++a) {
+            double acc = 0;
+            for (int r = 0; r < mm; ++r) {
+                const double g = r < nj ? y[F.col0[j] + r] : xn[F.rows[j][r - nj]];
+                acc += W[(size_t)a * mm + r] * g;
+            }
+            xn[F.col0[j] + a] = acc;
+        }
+    }
+    double d = 0, xm = 0;
+    for (int i = 0; i < n; ++i) {
+        d = std::max(d, std::fabs(xn[i] - x[F.perm[i]]));
+        xm = std::max(xm, std::fabs(x[F.perm[i]]));
+    }
+    *blocks_diff = xm > 0 ? d / xm : d;
+    return std::sqrt(rn / bn);
+}
+}
