@@ -67,7 +67,8 @@ static Csr<T> csr_from_map(int rows, int cols, const std::unordered_map<uint64_t
 // Nested dissection by breadth-first level structures: the middle level of a
 // pseudo-peripheral BFS is the separator; the two sides are ordered first.
 static void nd_order(int n, const std::vector<int>& adjp, const std::vector<int>& adji,
-                     std::vector<int>& order) {
+                     std::vector<int>& order, std::vector<int>& starts) {
+    starts.clear();
     std::vector<int> part(n, 0), level(n, -1), queue(n);
     int next_part = 1;
     order.clear();
@@ -98,6 +99,7 @@ static void nd_order(int n, const std::vector<int>& adjp, const std::vector<int>
     };
     rec = [&](std::vector<int>& verts, int pid) {
         if (verts.size() <= 48) {
+            starts.push_back((int)order.size());
             for (int v : verts) order.push_back(v);
             return;
         }
@@ -122,6 +124,7 @@ static void nd_order(int n, const std::vector<int>& adjp, const std::vector<int>
         for (int v : comp) h = std::max(h, level[v]);
         if (h < 2) {
             for (int v : comp) level[v] = -1;
+            starts.push_back((int)order.size());
             for (int v : verts) order.push_back(v);
             return;
         }
@@ -145,6 +148,7 @@ static void nd_order(int n, const std::vector<int>& adjp, const std::vector<int>
         for (int v : S) part[v] = -1;
         rec(A, pa);
         rec(B, pb);
+        starts.push_back((int)order.size());
         for (int v : S) order.push_back(v);
     };
     std::vector<int> all(n);
@@ -157,13 +161,16 @@ static void nd_order(int n, const std::vector<int>& adjp, const std::vector<int>
 // one-sided boundary layer; the axis with the smallest separator wins.  Falls
 // back to the level-structure split when no axis separates.
 static void nd_order_xyz(int n, const std::vector<int>& adjp, const std::vector<int>& adji,
-                         const std::vector<std::array<int, 3>>& xyz, std::vector<int>& order) {
+                         const std::vector<std::array<int, 3>>& xyz, std::vector<int>& order,
+                         std::vector<int>& starts) {
+    starts.clear();
     std::vector<int> part(n, 0);
     int next_part = 1;
     order.clear();
     order.reserve(n);
     std::function<void(std::vector<int>&, int)> rec = [&](std::vector<int>& verts, int pid) {
         if (verts.size() <= 48) {
+            starts.push_back((int)order.size());
             for (int v : verts) order.push_back(v);
             return;
         }
@@ -193,6 +200,7 @@ static void nd_order_xyz(int n, const std::vector<int>& adjp, const std::vector<
             if (best_axis < 0 || sep < best_sep) { best_axis = ax; best_sep = sep; best_cut = cut; best_side = sl <= sr ? 0 : 1; }
         }
         if (best_axis < 0) {
+            starts.push_back((int)order.size());
             for (int v : verts) order.push_back(v);
             return;
         }
@@ -215,6 +223,7 @@ static void nd_order_xyz(int n, const std::vector<int>& adjp, const std::vector<
         for (int v : S) part[v] = -1;
         rec(A, pa);
         rec(B, pb);
+        starts.push_back((int)order.size());
         for (int v : S) order.push_back(v);
     };
     std::vector<int> all(n);
@@ -242,75 +251,107 @@ void Cholesky::factor(const Csr<T>& A, double eps, const std::vector<std::array<
     }
     adji.reserve(adjp[n]);
     for (int r = 0; r < n; ++r) adji.insert(adji.end(), nb[r].begin(), nb[r].end());
-    if (xyz && (int)xyz->size() == n) nd_order_xyz(n, adjp, adji, *xyz, perm);
-    else nd_order(n, adjp, adji, perm);
+    // Each group the dissection emits (a leaf block or a separator) is one
+    // supernode; the groups come children first.
+    std::vector<int> starts;
+    if (xyz && (int)xyz->size() == n) nd_order_xyz(n, adjp, adji, *xyz, perm, starts);
+    else nd_order(n, adjp, adji, perm, starts);
+    starts.push_back(n);
     std::vector<int> iperm(n);
     for (int i = 0; i < n; ++i) iperm[perm[i]] = i;
-    // Upper triangle of C = P (A + eps I) P^T by columns: entries (i <= k).
-    std::vector<std::vector<std::pair<int, double>>> up(n);
+    const int ns = (int)starts.size() - 1;
+    std::vector<int> sn_of(n);
+    for (int j = 0; j < ns; ++j)
+        for (int c = starts[j]; c < starts[j + 1]; ++c) sn_of[c] = j;
+    // Lower triangle of P (A + eps I) P^T by (new) columns.
+    std::vector<std::vector<std::pair<int, double>>> lowcol(n);
     for (int r = 0; r < n; ++r)
         for (int p = A.ptr[r]; p < A.ptr[r + 1]; ++p) {
-            int c = A.col[p];
-            int i = iperm[r], k = iperm[c];
-            if (i <= k) up[k].push_back({i, (double)A.val[p]});
+            const int i = iperm[r], k = iperm[A.col[p]];
+            if (i >= k) lowcol[k].push_back({i, (double)A.val[p]});
         }
-    for (int k = 0; k < n; ++k) up[k].push_back({k, eps});
-    // Elimination tree (row-wise path compression).
-    std::vector<int> parent(n, -1), anc(n, -1);
-    for (int k = 0; k < n; ++k)
-        for (auto& e : up[k]) {
-            int i = e.first;
-            while (i != -1 && i < k) {
-                int next = anc[i];
-                anc[i] = k;
-                if (next == -1) { parent[i] = k; break; }
-                i = next;
-            }
-        }
-    // Up-looking numeric factorisation.
-    std::vector<std::vector<int>> crow(n);
-    std::vector<std::vector<double>> cval(n);
-    std::vector<double> diag(n), x(n, 0.0);
-    std::vector<int> mark(n, -1), pattern;
-    for (int k = 0; k < n; ++k) {
-        pattern.clear();
-        mark[k] = k;
-        for (auto& e : up[k]) {
-            int i = e.first;
-            x[i] += e.second;
-            while (i != -1 && i < k && mark[i] != k) {
-                mark[i] = k;
-                pattern.push_back(i);
-                i = parent[i];
-            }
-        }
-        std::sort(pattern.begin(), pattern.end());
-        double d = x[k];
-        x[k] = 0;
-        for (int j : pattern) {
-            double lkj = x[j] / diag[j];
-            x[j] = 0;
-            const auto& rj = crow[j];
-            const auto& vj = cval[j];
-            for (size_t q = 0; q < rj.size(); ++q) x[rj[q]] -= vj[q] * lkj;
-            d -= lkj * lkj;
-            crow[j].push_back(k);
-            cval[j].push_back(lkj);
-        }
-        if (!(d > 0)) throw std::runtime_error("oracle Cholesky: matrix not positive definite");
-        diag[k] = std::sqrt(d);
+    for (int k = 0; k < n; ++k) lowcol[k].push_back({k, eps});
+    // Symbolic: rows below each supernode, and the assembly tree.
+    std::vector<std::vector<int>> rows(ns);
+    std::vector<std::vector<int>> kids(ns);
+    std::vector<int> mark(n, -1);
+    for (int j = 0; j < ns; ++j) {
+        const int last = starts[j + 1] - 1;
+        std::vector<int>& R = rows[j];
+        for (int c = starts[j]; c <= last; ++c)
+            for (auto& e : lowcol[c])
+                if (e.first > last && mark[e.first] != j) { mark[e.first] = j; R.push_back(e.first); }
+        for (int c : kids[j])
+            for (int i : rows[c])
+                if (i > last && mark[i] != j) { mark[i] = j; R.push_back(i); }
+        std::sort(R.begin(), R.end());
+        if (!R.empty()) kids[sn_of[R[0]]].push_back(j);
     }
+    // Numeric: multifrontal, dense fronts (column-major, lower triangle).
+    std::vector<std::vector<double>> upd(ns);
+    std::vector<std::vector<double>> Lcols(ns);     // nj x m panel of L^T rows: column a of L in block j
+    std::vector<int> pos(n, -1);
+    for (int j = 0; j < ns; ++j) {
+        const int c0 = starts[j], nj = starts[j + 1] - c0, nr = (int)rows[j].size(), m = nj + nr;
+        std::vector<double> F((size_t)m * m, 0.0);
+        for (int a = 0; a < nj; ++a) pos[c0 + a] = a;
+        for (int k = 0; k < nr; ++k) pos[rows[j][k]] = nj + k;
+        for (int a = 0; a < nj; ++a)
+            for (auto& e : lowcol[c0 + a]) F[(size_t)a * m + pos[e.first]] += e.second;
+        for (int c : kids[j]) {
+            const std::vector<int>& rc = rows[c];
+            const int mc = (int)rc.size();
+            const std::vector<double>& U = upd[c];
+            for (int b = 0; b < mc; ++b) {
+                const int pb = pos[rc[b]];
+                for (int a = b; a < mc; ++a) F[(size_t)pb * m + pos[rc[a]]] += U[(size_t)b * mc + a];
+            }
+            std::vector<double>().swap(upd[c]);
+        }
+        // Partial Cholesky of the first nj columns (right-looking within the front).
+        for (int a = 0; a < nj; ++a) {
+            double* col = &F[(size_t)a * m];
+            const double d = col[a];
+            if (!(d > 0)) throw std::runtime_error("oracle Cholesky: matrix not positive definite");
+            const double ld = std::sqrt(d);
+            col[a] = ld;
+            for (int i = a + 1; i < m; ++i) col[i] /= ld;
+#pragma omp parallel for schedule(static) if (m - a > 256)
+            for (int b = a + 1; b < m; ++b) {
+                const double lb = col[b];
+                if (lb == 0.0) continue;
+                double* cb = &F[(size_t)b * m];
+                for (int i = b; i < m; ++i) cb[i] -= col[i] * lb;
+            }
+        }
+        // Update matrix for the parent: the trailing nr x nr lower block.
+        if (nr > 0) {
+            std::vector<double>& U = upd[j];
+            U.assign((size_t)nr * nr, 0.0);
+            for (int b = 0; b < nr; ++b)
+                for (int a = b; a < nr; ++a) U[(size_t)b * nr + a] = F[(size_t)(nj + b) * m + nj + a];
+        }
+        std::vector<double>& Lc = Lcols[j];
+        Lc.assign((size_t)nj * m, 0.0);
+        for (int a = 0; a < nj; ++a)
+            for (int i = a; i < m; ++i) Lc[(size_t)a * m + i] = F[(size_t)a * m + i];
+    }
+    // CSC of L, diagonal first in each column.
     Lp.assign(n + 1, 0);
-    for (int j = 0; j < n; ++j) Lp[j + 1] = Lp[j] + 1 + (int)crow[j].size();
+    for (int j = 0; j < ns; ++j) {
+        const int c0 = starts[j], nj = starts[j + 1] - c0, nr = (int)rows[j].size();
+        for (int a = 0; a < nj; ++a) Lp[c0 + a + 1] = (nj - a) + nr;
+    }
+    for (int k = 0; k < n; ++k) Lp[k + 1] += Lp[k];
     Li.resize(Lp[n]);
     Lx.resize(Lp[n]);
-    for (int j = 0; j < n; ++j) {
-        int p = Lp[j];
-        Li[p] = j;
-        Lx[p] = diag[j];
-        for (size_t q = 0; q < crow[j].size(); ++q) {
-            Li[p + 1 + q] = crow[j][q];
-            Lx[p + 1 + q] = cval[j][q];
+    for (int j = 0; j < ns; ++j) {
+        const int c0 = starts[j], nj = starts[j + 1] - c0, nr = (int)rows[j].size(), m = nj + nr;
+        const std::vector<double>& Lc = Lcols[j];
+        for (int a = 0; a < nj; ++a) {
+            int p = Lp[c0 + a];
+            for (int i = a; i < nj; ++i) { Li[p] = c0 + i; Lx[p] = Lc[(size_t)a * m + i]; ++p; }
+            for (int k = 0; k < nr; ++k) { Li[p] = rows[j][k]; Lx[p] = Lc[(size_t)a * m + nj + k]; ++p; }
         }
     }
 }
