@@ -474,13 +474,16 @@ size_t vcycle_smem_bytes(int levels) {
 // Cluster variant: one subdomain per thread-block cluster of C CTAs.
 //
 // Level 0 is cut into C slabs along x; CTA `rank` owns interior planes
-// x0..x1 and keeps one halo plane on each side.  After every Jacobi update a
-// CTA stores its first/last owned planes straight into its neighbours'
-// shared memory (distributed shared memory), double-buffered by sweep parity,
-// and one cluster barrier per sweep orders the exchange.  The coarse levels
-// are small and live in rank 0; the restriction into rank 0 and the
-// prolongation out of it are spread over all ranks through DSMEM.  Every CTA
-// executes the same sequence of cluster barriers.
+// x0..x1.  Each thread owns x-lines of the slab and keeps their u in
+// registers (shared memory holds a copy for the y/z neighbours of other
+// threads).  After every Jacobi update a CTA stores its first/last owned
+// planes straight into its neighbours' shared memory (distributed shared
+// memory), double-buffered by sweep parity; one cluster barrier per sweep
+// orders the exchange and each thread reads its lines' new x-halos into
+// registers.  The coarse levels are small and live in rank 0; the
+// restriction into rank 0 and the prolongation out of it are spread over all
+// ranks through DSMEM.  Every CTA executes the same sequence of cluster
+// barriers.
 // ---------------------------------------------------------------------------
 template <int SUB, int C>
 struct SlabGeom {
@@ -558,7 +561,6 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
     const int x0 = 1 + rank * P;
     const int x1 = min(x0 + P - 1, SUB - 1);
     const int np = x1 - x0 + 1;
-    const int ncell = np * M2;
 
     float* u0 = reinterpret_cast<float*>(smem);            // (P+2) planes, plane lx <-> x = x0-1+lx
     float* b0 = u0 + (P + 2) * PS;                          // P planes, plane k <-> x = x0+k
