@@ -47,7 +47,7 @@ constexpr int kBC = 32;                  // columns per backward task (8 warps x
 constexpr long kSpinLimit = 1L << 22;    // polls (with ~128 ns sleeps) before a wait gives up
 constexpr int kWarps = kNT / 32;         // small fronts per bundle (one per warp)
 constexpr int kSmallM = 256;             // rows of a front solved by one warp
-constexpr int kSmallLoads = 64;          // ... when its row chunks x columns stay below this
+constexpr int kSmallLoads = 128;         // ... when its row chunks x columns stay below this
 
 constexpr int kBundleLevel = 2048;       // bundle only on levels with at least this many small fronts
 
