@@ -259,6 +259,9 @@ def main():
     if args.one_solve:
         one_solve(args)
         return
+    if world > 1 and "OMP_NUM_THREADS" not in os.environ:
+        # N replicas share the host for their (OpenMP) setup: split the cores.
+        os.environ["OMP_NUM_THREADS"] = str(max(1, (os.cpu_count() or 1) // world))
     import torch
     torch.cuda.set_device(local_rank)
     dist = None
