@@ -115,6 +115,12 @@ void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& L) {
     // Dirichlet layers (Create_3D_Domain/main.cpp:126-140); it keeps the
     // per-subdomain V-cycles of the GPU path decoupled at every coarse level.
     {
+        long long active = 0;
+#pragma omp parallel for schedule(static) reduction(+ : active)
+        for (long long x = 0; x < (long long)N; ++x) active += (L.flags0[x] & F_ACTIVE) ? 1 : 0;
+        if (active == 0) throw Error(HDD_ERR_INVALID_ARGUMENT, "domain has no Active cells");
+    }
+    {
         long long bad = 0;
 #pragma omp parallel for schedule(static) reduction(+ : bad)
         for (int i = 0; i < n[0]; ++i)

@@ -157,9 +157,13 @@ void Solver::initialize() {
     if (std::getenv("HDD_VERBOSE"))
         std::fprintf(stderr, "[hdd setup] interface assembly done at %.2f s\n",
                      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
-    sigma.setup(ih, opts.sigma_smoothing, stream);
     // Level-0 interface DOFs: cell slots and their Active face neighbours.
     const int n_if = ih.n_iface.empty() ? 0 : ih.n_iface[0];
+    // A domain inside one subdomain has no interface: the preconditioner is
+    // then the two subdomain V-cycle passes alone, and the coarser interface
+    // levels (which only feed level 0) are not built.
+    if (n_if > 0) sigma.setup(ih, opts.sigma_smoothing, stream);
+    else sigma.release();
     std::vector<long long> slot(n_if);
     std::vector<int> nbs(6 * (size_t)n_if, -1);
     const int* n = L.opt.size;
@@ -253,10 +257,10 @@ void Solver::apply_preconditioner(const float* rr, float* zz) {
         cuda_check(launch_interface_gather(g, iface_slot.p, iface_nb.p, n_if, rr, zz, sigma.b0(), stream), "gather");
         count();
     }
-    {
+    if (n_if > 0) {
         // u_G = 0 then sigma_mg V-cycles (Preconditioner.h:105,110-117).
         Tm tm(this, 4);
-        cuda_check(cudaMemsetAsync(sigma.u0(), 0, sizeof(float) * std::max(n_if, 1), stream), "memset u0");
+        cuda_check(cudaMemsetAsync(sigma.u0(), 0, sizeof(float) * n_if, stream), "memset u0");
         for (int i = 0; i < opts.sigma_mg; ++i) sigma.vcycle(stream, launches, &hook);
     }
     {
@@ -419,6 +423,7 @@ void Solver::multiply_dense(const float* xin, float* yout) {
 void Solver::sigma_vcycle_host(const float* b0, float* u0) {
     if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
     const int n_if = ih.n_iface.empty() ? 0 : ih.n_iface[0];
+    if (n_if == 0) return;
     cuda_check(cudaMemcpyAsync(sigma.b0(), b0, n_if * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
     cuda_check(cudaMemsetAsync(sigma.u0(), 0, n_if * sizeof(float), stream), "memset");
     sigma.vcycle(stream, launches);

@@ -144,17 +144,21 @@ def profile_case() -> Domain:
 
 
 def small(n_cells=32, sub=8, radius=6, seed=0, delta=None) -> Domain:
-    """A small test domain: n_cells^3 box, one centred Dirichlet sphere, random RHS."""
-    size = (n_cells + 1,) * 3
-    c = n_cells // 2
-    flags = box_with_spheres(size, [((c, c, c), radius)] if radius > 0 else [])
+    """A small test domain: an n_cells^3 box (or n_cells = (nx, ny, nz) for a
+    ragged one, whose last subdomains are partial), one centred Dirichlet sphere,
+    random RHS."""
+    cells = tuple(n_cells) if isinstance(n_cells, (tuple, list)) else (n_cells,) * 3
+    size = tuple(n + 1 for n in cells)
+    centre = tuple(n // 2 for n in cells)
+    flags = box_with_spheres(size, [(centre, radius)] if radius > 0 else [])
     rng = np.random.Generator(np.random.Philox(seed))
     rhs = rng.uniform(-1, 1, size).astype(np.float32)
     rhs[(flags & ACTIVE) == 0] = 0
     if delta is not None:
         rhs[:] = 0
         rhs[delta] = 1.0
-    return Domain(size, flags, rhs, (sub, sub, sub), f"small{n_cells}_sub{sub}",
+    tag = "x".join(str(n) for n in cells) if len(set(cells)) > 1 else str(cells[0])
+    return Domain(size, flags, rhs, (sub, sub, sub), f"small{tag}_sub{sub}",
                   dict(vlevels=3, nVcycles=1, interior_smoothing=3, boundary_smoothing=3,
                        sigma_levels=2, sigma_smoothing=3, sigma_mg=1))
 

@@ -68,7 +68,9 @@ def matrix(L, h, kind, level, sub=0):
     return sp.csr_matrix((val[:nnz], col[:nnz], ptr), shape=(rows, cols))
 
 
-@pytest.mark.parametrize("n,sub,radius", [(32, 8, 6), (32, 16, 5)])
+@pytest.mark.parametrize("n,sub,radius", [(32, 8, 6), (32, 16, 5),
+                                           # ragged: the last subdomains along y and z (and x) are partial
+                                           ((40, 36, 44), 8, 6), ((33, 40, 40), 8, 5), ((48, 40, 56), 16, 7)])
 def test_interface_matrices_match_oracle(shim, n, sub, radius):
     d = domains.small(n, sub, radius, seed=4)
     M = d.meta["sigma_levels"]
@@ -106,3 +108,29 @@ def test_supernodal_factorisation_solves(shim):
                 assert res < 1e-10 and diff.value < 1e-10, ("Aii", l, sd, res, diff.value)
     finally:
         shim.shim_free(h)
+
+
+def test_domain_without_active_cells_is_rejected(shim):
+    d = domains.small(16, 8, 0, seed=1)
+    d.flags[:] = 0
+    size = (C.c_int * 3)(*d.size)
+    sub = (C.c_int * 3)(*d.sub_size)
+    flags = np.ascontiguousarray(d.flags, np.uint32)
+    err = C.create_string_buffer(512)
+    h = shim.shim_build(size, sub, 3, 2, flags.ctypes.data_as(C.POINTER(C.c_uint32)), err, 512)
+    assert not h and b"no Active cells" in err.value
+
+
+def test_single_subdomain_has_no_level0_interface(shim):
+    """A domain inside one subdomain: no level-0 interface DOFs (the solver then
+    runs the subdomain V-cycles alone), same as the oracle."""
+    d = domains.small(16, 16, 3, seed=1)
+    h = build(shim, d, 2)
+    try:
+        assert shim.shim_num_subdomains(h) == 1
+        assert matrix(shim, h, 0, 0).shape == (0, 0)
+    finally:
+        shim.shim_free(h)
+    o = Oracle(d.size, d.sub_size, d.flags, vlevels=3, nVcycles=1, interior_smoothing=3, boundary_smoothing=3,
+               sigma_levels=2, sigma_smoothing=3, sigma_mg=1)
+    assert o.num_interface(0) == 0
