@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import hashlib
 import json
 import os
 import subprocess
@@ -37,7 +38,11 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--config", choices=["c1", "c2", "c3", "p128"], default="c2")
+    p.add_argument("--config", choices=["c1", "c2", "c3", "p128", "c4"], default="c2",
+                   help="c4 = serving: resident uneven domains, solve requests through hdd_server_*")
+    p.add_argument("--domains", type=int, default=4, help="c4: resident domains")
+    p.add_argument("--requests", type=int, default=32, help="c4: requests per timed run")
+    p.add_argument("--slots", type=int, default=4, help="c4: requests in flight")
     p.add_argument("--one-solve", action="store_true",
                    help="set up, run one solve with per-phase timing and print the phase table "
                         "(the command profiled under ncu; prints no JSON line)")
@@ -248,16 +253,147 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def percentiles(lat_ms):
+    a = np.asarray(lat_ms, np.float64)
+    return {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)), "max": float(a.max())}
+
+
+def run_serving(args):
+    """Serving workload: uneven resident domains (cube sides 64..192, random
+    Dirichlet spheres, mixed precision), solve requests with 1-3 delta sources
+    through the hdd_server_* C ABI with host buffers (rhs in, solution out).
+
+    * saturated: all requests queued at once; serving (``--slots`` in flight)
+      against the plain drop-in (one request in flight at a time, i.e. one
+      hdd_solve after another), solves/s = requests / makespan;
+    * open loop: Poisson arrivals at 0.8x the plain path's saturated rate;
+      latency = arrival to finish, for both.
+    """
+    from hierarchicaldd_b200 import domains
+    from hierarchicaldd_b200.server import SolveServer, make_options
+
+    ds = domains.serving_mix(args.domains)
+    rng = np.random.Generator(np.random.Philox(44))
+    K = args.requests
+    picks = [int(i) for i in rng.integers(0, len(ds), K)]
+    rhs = [domains.serving_rhs(ds[i], rng) for i in picks]
+    gaps = rng.exponential(1.0, K)
+    srv = SolveServer(slots=args.slots)
+    t0 = time.perf_counter()
+    ids = []
+    for d in ds:
+        m = dict(d.meta)
+        ids.append(srv.add_domain(d.flags, make_options(d.size, d.sub_size, tol=1e-6, max_iters=1000, **m)))
+    for dom in ids:
+        srv.wait_domain(dom)
+    setup_s = time.perf_counter() - t0
+    print(f"[bench] serving: {len(ds)} domains resident after {setup_s:.1f} s", file=sys.stderr, flush=True)
+    for i, dom in enumerate(ids):  # warm-up: one solve per domain
+        srv.poll(srv.submit(dom, ds[i].rhs), dom, want_x=False)
+
+    def digest(r):  # (status, result, solution digest, latency)
+        return r[0], r[1], hashlib.sha1(r[2].tobytes()).hexdigest(), r[3]
+
+    def saturated(in_flight):
+        out, t = [], time.perf_counter()
+        if in_flight == 1:
+            for k in range(K):
+                out.append(digest(srv.poll(srv.submit(ids[picks[k]], rhs[k]), ids[picks[k]])))
+        else:
+            reqs = [srv.submit(ids[picks[k]], rhs[k]) for k in range(K)]
+            out = [digest(srv.poll(r, ids[picks[k]])) for k, r in enumerate(reqs)]
+        return time.perf_counter() - t, out
+
+    def open_loop(rate, in_flight):
+        arrivals = np.cumsum(gaps / rate)
+        lat, results, t = [], [], time.perf_counter()
+        if in_flight == 1:
+            for k in range(K):
+                now = time.perf_counter() - t
+                if arrivals[k] > now:
+                    time.sleep(arrivals[k] - now)
+                results.append(srv.poll(srv.submit(ids[picks[k]], rhs[k]), ids[picks[k]], want_x=False))
+                lat.append((time.perf_counter() - t - arrivals[k]) * 1e3)
+        else:
+            reqs = []
+            done = {}
+
+            def collect():
+                for k in range(K):
+                    while len(reqs) <= k:
+                        time.sleep(1e-4)
+                    done[k] = srv.poll(reqs[k], ids[picks[k]], want_x=False)
+            th = threading.Thread(target=collect)
+            th.start()
+            for k in range(K):
+                now = time.perf_counter() - t
+                if arrivals[k] > now:
+                    time.sleep(arrivals[k] - now)
+                reqs.append(srv.submit(ids[picks[k]], rhs[k]))
+            th.join()
+            results = [done[k] for k in range(K)]
+            lat = [results[k][3] for k in range(K)]  # submit (= arrival) to finish
+        return lat, results
+
+    with ClockSampler(0) as clk:
+        t_plain, r_plain = saturated(1)
+        t_serve, r_serve = saturated(args.slots)
+    plain_rate, serve_rate = K / t_plain, K / t_serve
+    rate = 0.8 * plain_rate
+    lat_plain, _ = open_loop(rate, 1)
+    lat_serve, _ = open_loop(rate, args.slots)
+    srv_mem = srv.memory()
+    same = all(a[0] == b[0] and a[1]["iterations"] == b[1]["iterations"] and a[2] == b[2]
+               for a, b in zip(r_plain, r_serve))
+    statuses = [r[0] for r in r_serve]
+    its = [r[1]["iterations"] for r in r_serve]
+    cells = [int(np.prod(ds[i].size)) for i in picks]
+    for dom in ids:
+        srv.remove_domain(dom)
+    srv.close()
+    line = {
+        "metric": "Poisson solves/sec @1e-6 rel. residual (serving) + p50/p99 latency", "value": serve_rate,
+        "unit": "solves/s", "n_gpus": 1, "steps": K, "warmup": len(ds), "ms_per_step": 1e3 / serve_rate,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 dots, alpha/beta)",
+        "data": "synthetic",
+        "config": {"workload": "c4_serving_sample", "domains": [d.name for d in ds], "requests": K,
+                   "slots": args.slots, "precision": "mixed", "tol": 1e-6,
+                   "l2": "no flush: resident domains, per-request working sets from 1 MB to 30 MB per vector"},
+        "plain_one_in_flight": {"value": plain_rate, "unit": "solves/s",
+                                "saturated_latency_ms": percentiles([r[3] for r in r_plain]),
+                                "open_loop_latency_ms": percentiles(lat_plain)},
+        "latency_ms": {"saturated": percentiles([r[3] for r in r_serve]), "open_loop": percentiles(lat_serve),
+                       "open_loop_rate": rate},
+        "speedup_vs_plain": serve_rate / plain_rate,
+        "results_identical_to_plain": bool(same),
+        "statuses": {str(s_): statuses.count(s_) for s_ in set(statuses)},
+        "iterations": {"min": int(min(its)), "max": int(max(its))},
+        "setup_s": setup_s, "device_bytes_reserved": srv_mem[0],
+        "e2e": {"value": serve_rate, "unit": "solves/s", "h2d_bytes_per_step": 4 * float(np.mean(cells)),
+                "d2h_bytes_per_step": 4 * float(np.mean(cells))},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
+        if args.config == "c4":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving path: "
+                                  "its solver handles one domain per process"}), flush=True)
+            return
         run_reference(args, rank)
         return
     if args.one_solve:
         one_solve(args)
+        return
+    if args.config == "c4":
+        run_serving(args)
         return
     if world > 1 and "OMP_NUM_THREADS" not in os.environ:
         # N replicas share the host for their (OpenMP) setup: split the cores.

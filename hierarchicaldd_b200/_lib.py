@@ -46,6 +46,11 @@ class HddError(RuntimeError):
         self.status = status
 
 
+class hdd_server_options(C.Structure):
+    _fields_ = [("slots", C.c_int), ("hbm_budget_bytes", C.c_longlong), ("device", C.c_int),
+                ("setup_threads", C.c_int)]
+
+
 # Every symbol declared in include/hdd.h: name -> (restype, argtypes).
 _vp = C.c_void_p
 _fp = C.POINTER(C.c_float)
@@ -75,6 +80,18 @@ SIGNATURES = {
     "hdd_status_string": (C.c_char_p, [C.c_int]),
     "hdd_last_error": (C.c_char_p, [_vp]),
     "hdd_destroy": (None, [_vp]),
+    "hdd_server_options_default": (None, [C.POINTER(hdd_server_options)]),
+    "hdd_server_create": (C.c_int, [C.POINTER(hdd_server_options), C.POINTER(C.c_void_p)]),
+    "hdd_server_add_domain": (C.c_int, [_vp, C.POINTER(hdd_options), C.POINTER(C.c_uint32),
+                                        C.POINTER(C.c_longlong)]),
+    "hdd_server_domain_status": (C.c_int, [_vp, C.c_longlong, C.c_int]),
+    "hdd_server_domain_error": (C.c_int, [_vp, C.c_longlong, C.c_char_p, C.c_int]),
+    "hdd_server_submit": (C.c_int, [_vp, C.c_longlong, _fp, C.POINTER(C.c_longlong)]),
+    "hdd_server_poll": (C.c_int, [_vp, C.c_longlong, C.c_int, C.POINTER(hdd_result), _fp,
+                                  C.POINTER(C.c_double)]),
+    "hdd_server_remove_domain": (C.c_int, [_vp, C.c_longlong]),
+    "hdd_server_memory": (C.c_int, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "hdd_server_destroy": (None, [_vp]),
 }
 
 _lib = None

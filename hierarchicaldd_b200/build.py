@@ -19,6 +19,7 @@ SOURCES = [
     "host_interface.cpp",
     "host_cholesky.cpp",
     "capi.cpp",
+    "server.cpp",
     "kernels_vcycle.cu",
     "kernels_pcg.cu",
     "sigma.cu",

@@ -25,13 +25,15 @@ T* upload(const std::vector<T>& h, cudaStream_t s, size_t& bytes) {
     return p;
 }
 
+// Zeroed on the caller's stream: a legacy-stream memset would not be ordered
+// before work on the solver's non-blocking stream.
 template <class T>
-T* alloc_zero(size_t n, size_t& bytes) {
+T* alloc_zero(size_t n, size_t& bytes, cudaStream_t s) {
     if (n == 0) return nullptr;
     T* p = nullptr;
     cudaError_t e = cudaMalloc(&p, n * sizeof(T));
     if (e != cudaSuccess) throw Error(HDD_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    ck(cudaMemset(p, 0, n * sizeof(T)), "memset");
+    ck(cudaMemsetAsync(p, 0, n * sizeof(T), s), "memset");
     bytes += n * sizeof(T);
     return p;
 }

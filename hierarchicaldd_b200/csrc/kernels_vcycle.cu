@@ -19,6 +19,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "hdd_common.h"
 #include "kernels.h"
@@ -862,11 +865,30 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
     cluster.sync();  // no CTA leaves while a peer may still address its shared memory
 }
 
+// A kernel's dynamic shared-memory limit is process-wide state.  Solvers on
+// other host threads launch the same kernels with other level counts, so the
+// limit is only ever raised, under a lock: a concurrent launch can never find
+// it lowered between its own check and its launch.
+std::mutex g_smem_mu;
+std::map<std::pair<const void*, int>, size_t> g_smem_limit;
+
+cudaError_t ensure_smem_limit(const void* kern, size_t smem) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(g_smem_mu);
+    size_t& have = g_smem_limit[{kern, dev}];
+    if (have >= smem) return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) have = smem;
+    return e;
+}
+
 template <int SUB, int C, int NT>
 cudaError_t launch_cluster(const VcycleArgs& a, cudaStream_t stream) {
     const size_t smem = vcycle_cluster_smem_bytes<SUB, C>(a.levels);
     auto kern = vcycle_cluster_kernel<SUB, C, NT>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = ensure_smem_limit((const void*)kern, smem);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(a.nbox * C), 1, 1);
@@ -899,7 +921,7 @@ cudaError_t launch_vcycle(const VcycleArgs& a, cudaStream_t stream) {
             if (a.cluster == 2) return launch_cluster<16, 2, 256>(a, stream);
             constexpr int NT = 512;
             const size_t smem = vcycle_smem_bytes<16>(a.levels);
-            cudaError_t e = cudaFuncSetAttribute(vcycle_kernel<16, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaError_t e = ensure_smem_limit((const void*)vcycle_kernel<16, NT>, smem);
             if (e != cudaSuccess) return e;
             vcycle_kernel<16, NT><<<a.nbox, NT, smem, stream>>>(a);
             return cudaGetLastError();

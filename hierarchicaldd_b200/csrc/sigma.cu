@@ -183,12 +183,12 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
             L.prrT.upload(transpose(ih.Prr[l]), s);
         }
         size_t bytes = 0;
-        L.u = dev::alloc_zero<float>(std::max(L.n_iface, 1), bytes);
-        L.r = dev::alloc_zero<float>(std::max(L.n_iface, 1), bytes);
-        L.b = dev::alloc_zero<float>(std::max(L.n_iface, 1), bytes);
-        L.tmp = dev::alloc_zero<float>(std::max(L.n_iface, 1), bytes);
-        L.vb = dev::alloc_zero<float>(std::max(L.n_int, 1), bytes);
-        L.vx = dev::alloc_zero<float>(std::max(L.n_int, 1), bytes);
+        L.u = dev::alloc_zero<float>(std::max(L.n_iface, 1), bytes, s);
+        L.r = dev::alloc_zero<float>(std::max(L.n_iface, 1), bytes, s);
+        L.b = dev::alloc_zero<float>(std::max(L.n_iface, 1), bytes, s);
+        L.tmp = dev::alloc_zero<float>(std::max(L.n_iface, 1), bytes, s);
+        L.vb = dev::alloc_zero<float>(std::max(L.n_int, 1), bytes, s);
+        L.vx = dev::alloc_zero<float>(std::max(L.n_int, 1), bytes, s);
         device_bytes += bytes;
 
         // Factorisations.
@@ -324,8 +324,8 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
             n_bottom = nb;
             n_bottom_int = ni;
             size_t b2 = 0;
-            kb = dev::alloc_zero<float>(std::max(ni + nb, 1), b2);
-            kx = dev::alloc_zero<float>(std::max(ni + nb, 1), b2);
+            kb = dev::alloc_zero<float>(std::max(ni + nb, 1), b2, s);
+            kx = dev::alloc_zero<float>(std::max(ni + nb, 1), b2, s);
             device_bytes += b2 + bottom.bytes;
         }
     }

@@ -591,12 +591,12 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
     d_bfwd = dev::upload(bfwd.empty() ? std::vector<int>{0} : bfwd, s, bytes);
     d_bbwd = dev::upload(bbwd.empty() ? std::vector<int>{0} : bbwd, s, bytes);
     d_fw = dev::upload(fw, s, bytes);
-    d_part = dev::alloc_zero<float>(std::max<long long>(part_total, 1), bytes);
-    d_upd = dev::alloc_zero<float>(std::max<long long>(upd_total, 1), bytes);
-    d_ynew = dev::alloc_zero<float>(std::max(n, 1), bytes);
-    d_xnew = dev::alloc_zero<float>(std::max(n, 1), bytes);
-    d_ctr = dev::alloc_zero<int>(n_ctr, bytes);
-    d_err = dev::alloc_zero<int>(1, bytes);
+    d_part = dev::alloc_zero<float>(std::max<long long>(part_total, 1), bytes, s);
+    d_upd = dev::alloc_zero<float>(std::max<long long>(upd_total, 1), bytes, s);
+    d_ynew = dev::alloc_zero<float>(std::max(n, 1), bytes, s);
+    d_xnew = dev::alloc_zero<float>(std::max(n, 1), bytes, s);
+    d_ctr = dev::alloc_zero<int>(n_ctr, bytes, s);
+    d_err = dev::alloc_zero<int>(1, bytes, s);
     // Persistent grid: as many CTAs as fit on the device, but no more than tasks.
     int dev_id = 0, nsm = 0, bf = 0, bb = 0;
     dev::ck(cudaGetDevice(&dev_id), "cudaGetDevice");

@@ -148,6 +148,15 @@ struct Solver {
     void apply_preconditioner(const float* rr, float* zz);   // device tiled vectors
     void count(int n = 1) { launches += n; }
     void sync() { cuda_check(cudaStreamSynchronize(stream), "stream sync"); }
+    // Device memory held by this solver (vectors, tables, interface solver).
+    size_t device_bytes() const {
+        size_t t = 0;
+        for (const DevBuf<float>* v : {&x, &b, &r, &z, &s, &q, &dense, &partial_max, &scalars_f}) t += v->n * sizeof(float);
+        t += tflags.n * sizeof(uint16_t) + box_flags.n;
+        for (const DevBuf<int>* v : {&tile_nbr, &box_tile, &box_nb, &tile_xyz, &iface_nb}) t += v->n * sizeof(int);
+        t += (partial.n + sums.n) * sizeof(double) + iface_slot.n * sizeof(long long);
+        return t + sigma.device_bytes;
+    }
 };
 
 }  // namespace hdd

@@ -143,6 +143,46 @@ def profile_case() -> Domain:
     return Domain(d.size, d.flags, d.rhs, d.sub_size, "p128_128cube_sub32", d.meta)
 
 
+SERVING_SIDES = (64, 96, 128, 192)
+
+
+def serving_mix(n_domains=4, seed=4, sides=SERVING_SIDES) -> list:
+    """Uneven domains for the serving workload: cube side drawn from ``sides``
+    (cycled, so every side appears), 1-4 Dirichlet spheres with radii
+    U[0.05, 0.2] * side at uniform-random centres, subdomains 16^3 for sides
+    below 128 and 32^3 from 128 up, mixed precision with a true residual every
+    20 iterations.  The right-hand side is 1-3 unit deltas at random Active cells
+    (``serving_rhs`` draws more)."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    out = []
+    for n in range(n_domains):
+        side = int(sides[n % len(sides)])
+        size = (side + 1,) * 3
+        spheres = []
+        for _ in range(int(rng.integers(1, 5))):
+            c = tuple(int(v) for v in rng.integers(1, side, 3))
+            spheres.append((c, float(rng.uniform(0.05, 0.2)) * side))
+        flags = box_with_spheres(size, spheres)
+        sub = 16 if side < 128 else 32
+        meta = (dict(vlevels=3, nVcycles=1, interior_smoothing=3, boundary_smoothing=3, sigma_levels=3,
+                     sigma_smoothing=3, sigma_mg=1) if sub == 16 else
+                dict(vlevels=4, nVcycles=1, interior_smoothing=4, boundary_smoothing=4, sigma_levels=3,
+                     sigma_smoothing=3, sigma_mg=1))
+        meta.update(precision_mode=1, true_residual_every=20)
+        d = Domain(size, flags, np.zeros(size, np.float32), (sub,) * 3, f"serve{n}_{side}cube_sub{sub}", meta)
+        d.rhs = serving_rhs(d, rng)
+        out.append(d)
+    return out
+
+
+def serving_rhs(d: Domain, rng) -> np.ndarray:
+    """1-3 unit deltas at uniform-random Active cells of ``d``."""
+    act = np.flatnonzero((d.flags & ACTIVE) != 0)
+    rhs = np.zeros(d.size, np.float32)
+    rhs.reshape(-1)[act[rng.integers(0, len(act), int(rng.integers(1, 4)))]] = 1.0
+    return rhs
+
+
 def small(n_cells=32, sub=8, radius=6, seed=0, delta=None) -> Domain:
     """A small test domain: an n_cells^3 box (or n_cells = (nx, ny, nz) for a
     ragged one, whose last subdomains are partial), one centred Dirichlet sphere,

@@ -174,6 +174,66 @@ const char* hdd_status_string(hdd_status status);
 const char* hdd_last_error(const hdd_solver* s);
 void hdd_destroy(hdd_solver* s);
 
+/* ---- Serving: concurrent solves on resident domains ------------------------
+ * No counterpart in the reference, whose GPU demo solves one domain per
+ * process (GPU/Test_Bench_3D/main.cpp) through one worker thread per GPU
+ * (GPU/Nodes/Command.h:33-55).  A server owns `slots` worker threads.  A domain
+ * added with hdd_server_add_domain is admitted, in arrival order, once its
+ * estimated device footprint fits the HBM budget; a worker then runs its setup
+ * (as hdd_initialize_preconditioner) and the domain stays resident until
+ * removed.  Each solve request names a resident (or still setting-up) domain
+ * and a right-hand side; workers take the oldest request whose domain is idle,
+ * so requests on different domains run concurrently on separate CUDA streams
+ * and requests on one domain run in arrival order.  A request's result does not
+ * depend on what else is in flight.  All calls except hdd_server_destroy may be
+ * made from any thread at any time. */
+typedef struct hdd_server hdd_server;
+
+typedef struct {
+    int slots;                  /* worker threads = requests in flight (default 4, at most 64) */
+    long long hbm_budget_bytes; /* admission budget for resident domains; 0 = 90% of free device memory */
+    int device;                 /* CUDA device ordinal */
+    int setup_threads;          /* OpenMP threads per domain setup; 0 = host cores / slots */
+} hdd_server_options;
+
+void hdd_server_options_default(hdd_server_options* opts);
+hdd_status hdd_server_create(const hdd_server_options* opts, hdd_server** out);
+
+/* Queues a domain for setup (flags are copied; opts as for hdd_create, its
+ * device ignored).  Returns at once; HDD_ERR_OUT_OF_MEMORY when the domain's
+ * estimated footprint alone exceeds the budget. */
+hdd_status hdd_server_add_domain(hdd_server* srv, const hdd_options* opts, const uint32_t* flags,
+                                 long long* domain_id);
+
+/* HDD_OK once the domain is resident, HDD_ERR_BUSY while it waits for budget
+ * or sets up (after waiting up to wait_ms; -1 = until settled), otherwise the
+ * status its setup failed with (message via hdd_server_domain_error). */
+hdd_status hdd_server_domain_status(hdd_server* srv, long long domain_id, int wait_ms);
+hdd_status hdd_server_domain_error(hdd_server* srv, long long domain_id, char* message, int capacity);
+
+/* Queues one solve of the domain for the dense right-hand side rhs (copied). */
+hdd_status hdd_server_submit(hdd_server* srv, long long domain_id, const float* rhs, long long* request_id);
+
+/* Waits up to wait_ms (-1 = until done) for a request.  HDD_ERR_BUSY while it
+ * is pending.  Otherwise returns the request's own status (HDD_OK,
+ * HDD_ERR_NOT_CONVERGED, or its domain's setup failure), fills result, the
+ * dense solution x (if not NULL) and latency_ms = wall time from submit to
+ * finish (if not NULL), and forgets the request. */
+hdd_status hdd_server_poll(hdd_server* srv, long long request_id, int wait_ms, hdd_result* result, float* x,
+                           double* latency_ms);
+
+/* Waits for the domain's queued requests, then frees its device state and
+ * its budget. */
+hdd_status hdd_server_remove_domain(hdd_server* srv, long long domain_id);
+
+/* Device bytes held by admitted domains (estimates until set up, then what
+ * their solvers hold) and the budget. */
+hdd_status hdd_server_memory(hdd_server* srv, long long* reserved, long long* budget);
+
+/* Lets running setups and solves finish, stops the workers and frees every
+ * domain.  Requests still queued are dropped. */
+void hdd_server_destroy(hdd_server* srv);
+
 #ifdef __cplusplus
 }
 #endif

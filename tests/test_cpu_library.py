@@ -50,6 +50,23 @@ def test_status_strings(hdd_lib):
         assert s and isinstance(s, bytes)
 
 
+def test_server_options_default(hdd_lib):
+    o = _lib.hdd_server_options()
+    hdd_lib.hdd_server_options_default(C.byref(o))
+    assert o.slots == 4 and o.hbm_budget_bytes == 0 and o.device == 0 and o.setup_threads == 0
+    h = C.c_void_p()
+    o.slots = 0
+    assert hdd_lib.hdd_server_create(C.byref(o), C.byref(h)) == 1 and not h.value
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the GPU-less failure path")
+def test_server_create_fails_loudly_without_gpu(hdd_lib):
+    o = _lib.hdd_server_options()
+    hdd_lib.hdd_server_options_default(C.byref(o))
+    h = C.c_void_p()
+    assert hdd_lib.hdd_server_create(C.byref(o), C.byref(h)) == 2 and not h.value
+
+
 @pytest.mark.skipif(gpu_available(), reason="checks the GPU-less failure path")
 def test_create_fails_loudly_without_gpu(hdd_lib):
     o = _lib.hdd_options()

@@ -1,0 +1,126 @@
+"""The serving layer (hdd_server_*): concurrent solves of uneven domains.
+
+* every request's iterations and solution equal the plain one-handle solve of
+  the same domain and right-hand side, bit for bit, whether it ran alone or
+  among other requests in flight;
+* a budget that fits one domain at a time admits them in turn and all
+  requests still finish; the reserved bytes return to zero after removal;
+* a domain whose setup fails reports its status, and so do its requests.
+"""
+import numpy as np
+import pytest
+
+from hierarchicaldd_b200 import domains
+from hierarchicaldd_b200._lib import HddError
+from hierarchicaldd_b200.server import SolveServer, make_options
+
+pytestmark = pytest.mark.gpu
+
+
+def cases():
+    return [domains.small(32, 8, 6, seed=1), domains.small((40, 36, 44), 8, 6, seed=11),
+            domains.small(48, 16, 8, seed=7), domains.small(16, 16, 3, seed=1)]
+
+
+def options(d):
+    m = d.meta
+    return make_options(d.size, d.sub_size, m["vlevels"], m["nVcycles"], m["interior_smoothing"],
+                        m["boundary_smoothing"], m["sigma_levels"], m["sigma_smoothing"], m["sigma_mg"])
+
+
+def rhs_set(d, k):
+    rng = np.random.Generator(np.random.Philox(100 + k))
+    out = [d.rhs]
+    for _ in range(k):
+        r = rng.uniform(-1, 1, d.size).astype(np.float32)
+        r[(d.flags & domains.ACTIVE) == 0] = 0
+        out.append(r)
+    return out
+
+
+def solo(d, rhs_list):
+    from hierarchicaldd_b200.solver import SPGrid_Domain_Decomposition_Solver
+    m = d.meta
+    s = SPGrid_Domain_Decomposition_Solver()
+    s.Set_Domain(d.flags, d.rhs)
+    s.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"],
+                                m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"], m["sigma_mg"])
+    out = []
+    for r in rhs_list:
+        s.Set_RHS(r)
+        res = s.Solve()
+        out.append((res["iterations"], s.Solution()))
+    s.close()
+    return out
+
+
+def test_concurrent_requests_match_plain_solves():
+    ds = cases()
+    rhs = [rhs_set(d, 2) for d in ds]
+    ref = [solo(d, r) for d, r in zip(ds, rhs)]
+    srv = SolveServer(slots=3)
+    try:
+        ids = [srv.add_domain(d.flags, options(d)) for d in ds]
+        # Alone: one request at a time on the resident domains.
+        for i, dom in enumerate(ids):
+            assert srv.wait_domain(dom)
+            req = srv.submit(dom, rhs[i][0])
+            st, res, x, lat = srv.poll(req, dom)
+            assert st == 0 and res["converged"] == 1 and lat > 0
+            assert res["iterations"] == ref[i][0][0] and np.array_equal(x, ref[i][0][1])
+        # In the mix: every request submitted at once, interleaved over domains.
+        reqs = [(i, k, srv.submit(ids[i], rhs[i][k])) for k in range(3) for i in range(len(ds))]
+        for i, k, req in reqs:
+            st, res, x, _ = srv.poll(req, ids[i])
+            assert st == 0, (i, k, st)
+            assert res["iterations"] == ref[i][k][0], (i, k)
+            assert np.array_equal(x, ref[i][k][1]), (i, k, float(np.max(np.abs(x - ref[i][k][1]))))
+        for dom in ids:
+            srv.remove_domain(dom)
+        assert srv.memory()[0] == 0
+    finally:
+        srv.close()
+
+
+def test_budget_admits_domains_in_turn():
+    ds = cases()[:3]
+    probe = SolveServer(slots=1)
+    try:
+        sizes = []
+        for d in ds:
+            dom = probe.add_domain(d.flags, options(d))
+            sizes.append(probe.memory()[0])  # the estimate, or the actual if set up already
+            assert probe.wait_domain(dom)
+            sizes.append(probe.memory()[0])  # what the solver holds
+            probe.remove_domain(dom)
+    finally:
+        probe.close()
+    srv = SolveServer(slots=2, hbm_budget_bytes=int(max(sizes) * 1.05))
+    try:
+        ids = [srv.add_domain(d.flags, options(d)) for d in ds]
+        reqs = [(i, srv.submit(dom, d.rhs)) for i, (dom, d) in enumerate(zip(ids, ds))]
+        # Later domains wait for budget until earlier ones are removed.
+        for i, req in reqs:
+            st, res, _, _ = srv.poll(req, ids[i], want_x=False)
+            assert st == 0 and res["converged"] == 1
+            srv.remove_domain(ids[i])
+        assert srv.memory()[0] == 0
+    finally:
+        srv.close()
+
+
+def test_failed_domain_reports_its_status():
+    d = domains.small(16, 8, 0, seed=1)
+    d.flags[:] = 0
+    srv = SolveServer(slots=2)
+    try:
+        dom = srv.add_domain(d.flags, options(d))
+        req = srv.submit(dom, np.zeros(d.size, np.float32))
+        with pytest.raises(HddError) as e:
+            srv.wait_domain(dom)
+        assert e.value.status == 1 and "no Active cells" in str(e.value)
+        st, _, _, _ = srv.poll(req, dom, want_x=False)
+        assert st == 1
+        srv.remove_domain(dom)
+    finally:
+        srv.close()
