@@ -212,6 +212,9 @@ void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& L) {
                 L.boxes.push_back(bx);
             }
     L.box_flags.assign(L.boxes.size() * L.box_stride, 0);
+    // Set inside the parallel loop, thrown after it: an exception may not
+    // leave an OpenMP region.
+    int coupled = 0;
 #pragma omp parallel for schedule(dynamic)
     for (long long bi = 0; bi < (long long)L.boxes.size(); ++bi) {
         const Box& bx = L.boxes[bi];
@@ -253,8 +256,10 @@ void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& L) {
                 for (int y = 0; y < ce[1]; ++y)
                     for (int z = 0; z < ce[2]; ++z) {
                         bool halo = x == 0 || y == 0 || z == 0 || x == ce[0] - 1 || y == ce[1] - 1 || z == ce[2] - 1;
-                        if (halo && (coarse[at3(ce, x, y, z)] & F_ACTIVE))
-                            throw Error(HDD_ERR_UNSUPPORTED, "coarse level couples subdomains");
+                        if (halo && (coarse[at3(ce, x, y, z)] & F_ACTIVE)) {
+#pragma omp atomic write
+                            coupled = 1;
+                        }
                     }
             uint8_t* dst = rec + L.level_off[l];
             for (size_t x = 0; x < coarse.size(); ++x) dst[x] = compact8(coarse[x]);
@@ -262,6 +267,7 @@ void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& L) {
             for (int a = 0; a < 3; ++a) fe[a] = ce[a];
         }
     }
+    if (coupled) throw Error(HDD_ERR_UNSUPPORTED, "coarse level couples subdomains");
 }
 
 void dense_to_tiles(const DomainLayout& L, const float* dense, float* tiled) {

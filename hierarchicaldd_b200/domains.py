@@ -46,19 +46,62 @@ class Domain:
         return int(np.count_nonzero(self.flags & ACTIVE))
 
 
+def _neighbour(mask: np.ndarray, axis: int, step: int) -> np.ndarray:
+    """mask at cell + step along axis (False outside the grid)."""
+    pad = np.pad(mask, 1, constant_values=False)
+    sl = [slice(1, 1 + n) for n in mask.shape]
+    sl[axis] = slice(1 + step, 1 + step + mask.shape[axis])
+    return pad[tuple(sl)]
+
+
 def face_bits(flags: np.ndarray) -> np.ndarray:
-    """OR face bits into Active|Interface cells (SPGrid_Flag_Helper.h:74-106)."""
+    """OR face bits into Active|Interface cells (SPGrid_Flag_Helper.h:74-106):
+    bit FACE_MX << k for the faces -x, +x, -y, +y (, -z, +z) whose neighbour is
+    Active, Interface or Dirichlet.  2D or 3D."""
     f = flags.copy()
-    typ = f & (ACTIVE | INTERFACE | DIRICHLET)
-    nb_ok = typ != 0
+    nb_ok = (f & (ACTIVE | INTERFACE | DIRICHLET)) != 0
     solve = (f & (ACTIVE | INTERFACE)) != 0
-    pad = np.pad(nb_ok, 1, constant_values=False)
-    n0, n1, n2 = f.shape
-    shifts = [(-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1)]
-    for k, (a, b, c) in enumerate(shifts):
-        nb = pad[1 + a:1 + a + n0, 1 + b:1 + b + n1, 1 + c:1 + c + n2]
-        f[solve & nb] |= np.uint32(FACE_MX << k)
+    for k in range(2 * f.ndim):
+        f[solve & _neighbour(nb_ok, k // 2, 1 if k % 2 else -1)] |= np.uint32(FACE_MX << k)
     return f
+
+
+def reference_generator(size, delta) -> Domain:
+    """The reference's own test domain (Create_2D_Domain / Create_3D_Domain
+    main.cpp, Rasterizer::Consume at :100-149): a box whose outer cell layer is
+    Dirichlet and whose centre holds a Neumann bubble, with the right-hand side
+    4.0 at ``delta`` (main.cpp:282-287).  2D or 3D.
+
+    The rasterizer's grid is PhysBAM's GRID of size-2 nodes on the unit box,
+    so dx = 1/(size-3) and cell c has centre (c - 0.5) dx, in float; cells with
+    |centre - 0.5|^2 <= 0.09 are exterior (flag 0).  Dirichlet cells without an
+    Active face neighbour are exterior too, and face bits follow Flaging.  The
+    reference's shipped 2D output (256 x 256) decodes to exactly this.
+
+    The solver's GPU path rejects these inputs (exterior cells touch Active
+    ones); the oracle accepts them."""
+    n = tuple(int(v) for v in size)
+    grids = np.ogrid[tuple(slice(0, v) for v in n)]
+    d2 = np.float32(0)
+    interior = True
+    for a, g in enumerate(grids):
+        dx = np.float32(1) / np.float32(n[a] - 3)
+        x = (g.astype(np.float32) - np.float32(0.5)) * dx - np.float32(0.5)
+        d2 = d2 + x * x
+        interior = interior & (g >= 1) & (g <= n[a] - 2)
+    active = interior & ~(d2 <= np.float32(0.09))
+    touches = np.zeros(n, bool)
+    for a in range(len(n)):
+        touches |= _neighbour(active, a, -1) | _neighbour(active, a, 1)
+    flags = np.zeros(n, np.uint32)
+    flags[active] = ACTIVE
+    flags[~interior & touches] = DIRICHLET
+    flags = face_bits(flags)
+    rhs = np.zeros(n, np.float32)
+    if flags[tuple(delta)] == 0:
+        raise ValueError("the delta must sit on a non-exterior cell (main.cpp:286 asserts it)")
+    rhs[tuple(delta)] = 4.0
+    return Domain(n, flags, rhs, name="reference_bubble_" + "x".join(map(str, n)))
 
 
 def _finish(active: np.ndarray, dirichlet: np.ndarray) -> np.ndarray:

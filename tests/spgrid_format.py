@@ -96,3 +96,58 @@ def read_spgrid_dir(path, size):
                     if x < size[0] and y < size[1] and z < size[2]:
                         arr[x, y, z] = vals[e]
     return flags, data
+
+
+def axis_masks(dim, log2_struct=4, log2_field=2):
+    """Per-axis address masks of SPGrid_Mask<log2_struct, log2_field, dim>
+    (PB/Common_Libraries/SPGrid/Core/SPGrid_Mask.h: the 3D masks at :14-31 and
+    :56-60, the 2D ones at :308-358), and the block shape.  Inside the 4 KB page
+    the element bits sit above the field's byte bits, the last axis lowest; the
+    page bits above bit 12 interleave the axes.  The layout has to match the
+    reference's for the on-disk format to be read at all."""
+    full = (1 << 64) - 1
+    block_bits = 12 - log2_struct
+    if dim == 3:
+        bits = [block_bits // 3, block_bits // 3 + (block_bits % 3 > 1), block_bits // 3 + (block_bits % 3 > 0)]
+        sh = 3 - block_bits % 3
+        page = [0x4924924924924924, 0x2492492492492492, 0x9249249249249249]
+    elif dim == 2:
+        bits = [block_bits // 2, block_bits // 2 + (block_bits % 2 > 0)]
+        sh = 2 - block_bits % 2
+        page = [0xAAAAAAAAAAAAAAAA, 0x5555555555555555]
+    else:
+        raise ValueError("dim must be 2 or 3")
+    masks, shift = [0] * dim, log2_field
+    for a in reversed(range(dim)):
+        masks[a] = ((page[a] << sh) & full & 0xFFFFFFFFFFFFF000) | (((1 << bits[a]) - 1) << shift)
+        shift += bits[a]
+    return masks, tuple(1 << b for b in bits)
+
+
+def read_spgrid_dir_any(path):
+    """(size, flags, data, n_blocks) of a 2D or 3D directory; the dimension
+    comes from the length of the `size` file; arrays cover the padded size."""
+    with open(os.path.join(path, "size"), "rb") as fh:
+        raw = fh.read()
+    dim = len(raw) // 4
+    size = struct.unpack("<%di" % dim, raw)
+    masks, block = axis_masks(dim)
+    per_block = int(np.prod(block))
+    with open(os.path.join(path, "block_offset"), "rb") as fh:
+        count, alen = struct.unpack("<ii", fh.read(8))
+        assert alen == count
+        offs = struct.unpack("<%dQ" % count, fh.read(8 * count))
+    flags = np.zeros(size, np.uint32)
+    data = np.zeros(size, np.float32)
+    elem = np.arange(per_block, dtype=np.uint64) * 4
+    for name, arr, dt in (("flags", flags, "<u4"), ("data", data, "<f4")):
+        with open(os.path.join(path, name), "rb") as fh:
+            buf = fh.read()
+        rec = 4 + 4 * per_block
+        assert len(buf) == rec * count
+        for b, off in enumerate(offs):
+            assert struct.unpack_from("<i", buf, b * rec)[0] == per_block
+            vals = np.frombuffer(buf, dt, per_block, b * rec + 4)
+            idx = tuple(np.array([pext(int(off) + int(e), m) for e in elem]) for m in masks)
+            arr[idx] = vals
+    return size, flags, data, count
