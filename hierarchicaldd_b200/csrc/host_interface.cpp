@@ -593,14 +593,14 @@ void build_interface(const DomainLayout& L, int M, InterfaceHost& out) {
     out.iface_xyz.assign(M, {});
     out.aii_xyz.assign(M, std::vector<std::vector<std::array<int, 3>>>(nsub));
     std::vector<std::unordered_map<uint64_t, int>> gid(M);
-    std::vector<std::unordered_map<uint64_t, float>> arr(M);
-    std::vector<std::vector<std::pair<uint64_t, float>>> air_pairs(nsub);
     for (int m = 0; m < M; ++m) {
+        // Global numbers in first-encounter order (serial: the order is the result).
+        std::vector<std::vector<int>> to_g(nsub);
         for (int s = 0; s < nsub; ++s) {
-            BoxWork& W = work[s];
-            std::vector<int> to_g(W.iface_nodes[m].size());
-            for (size_t i = 0; i < W.iface_nodes[m].size(); ++i) {
-                const I3& nd = W.iface_nodes[m][i];
+            const std::vector<I3>& nodes = work[s].iface_nodes[m];
+            to_g[s].resize(nodes.size());
+            for (size_t i = 0; i < nodes.size(); ++i) {
+                const I3& nd = nodes[i];
                 const uint64_t key = ((uint64_t)nd[0] << 42) | ((uint64_t)nd[1] << 21) | (uint64_t)nd[2];
                 auto it = gid[m].find(key);
                 if (it == gid[m].end()) {
@@ -608,23 +608,68 @@ void build_interface(const DomainLayout& L, int M, InterfaceHost& out) {
                     if (m == 0) out.iface_map.push_back(nd);
                     out.iface_xyz[m].push_back({nd[0] << m, nd[1] << m, nd[2] << m});
                 }
-                to_g[i] = it->second;
+                to_g[s][i] = it->second;
             }
-            for (auto& tv : W.arr_terms[m])
-                arr[m][((uint64_t)(uint32_t)to_g[tv.first.first] << 32) | (uint32_t)to_g[tv.first.second]] += tv.second;
+        }
+        const int nif = out.n_iface[m];
+        // Arr: each entry is the float sum of its terms in (subdomain, term)
+        // order, starting from 0.  The terms are bucketed by row in that order
+        // (a serial fill), then every row sums its columns on its own.
+        std::vector<long long> row_ptr((size_t)nif + 1, 0);
+        for (int s = 0; s < nsub; ++s)
+            for (const auto& tv : work[s].arr_terms[m]) row_ptr[(size_t)to_g[s][tv.first.first] + 1]++;
+        for (int r = 0; r < nif; ++r) row_ptr[r + 1] += row_ptr[r];
+        std::vector<std::pair<int, float>> bucket((size_t)row_ptr[nif]);
+        {
+            std::vector<long long> fill(row_ptr.begin(), row_ptr.end() - 1);
+            for (int s = 0; s < nsub; ++s) {
+                for (const auto& tv : work[s].arr_terms[m])
+                    bucket[(size_t)fill[to_g[s][tv.first.first]]++] = {to_g[s][tv.first.second], tv.second};
+                std::vector<std::pair<std::pair<int, int>, float>>().swap(work[s].arr_terms[m]);
+            }
+        }
+        std::vector<int> row_nnz(nif, 0);
+#pragma omp parallel for schedule(dynamic, 256)
+        for (int r = 0; r < nif; ++r) {
+            auto* b = bucket.data() + row_ptr[r];
+            auto* e = bucket.data() + row_ptr[r + 1];
+            std::stable_sort(b, e, [](const auto& x, const auto& y) { return x.first < y.first; });
+            int w = 0;  // compacted (column, sum) pairs written from b
+            for (auto* p = b; p != e;) {
+                const int c = p->first;
+                float acc = 0.0f;
+                for (; p != e && p->first == c; ++p) acc += p->second;
+                if (acc != 0.0f) b[w++] = {c, acc};  // explicit zeros dropped, as csr_from_pairs does
+            }
+            row_nnz[r] = w;
+        }
+        CsrF& A = out.Arr[m];
+        A.rows = A.cols = nif;
+        A.ptr.assign((size_t)nif + 1, 0);
+        for (int r = 0; r < nif; ++r) A.ptr[r + 1] = A.ptr[r] + row_nnz[r];
+        A.col.resize((size_t)A.ptr[nif]);
+        A.val.resize((size_t)A.ptr[nif]);
+#pragma omp parallel for schedule(dynamic, 256)
+        for (int r = 0; r < nif; ++r) {
+            const auto* b = bucket.data() + row_ptr[r];
+            for (int i = 0; i < row_nnz[r]; ++i) {
+                A.col[(size_t)A.ptr[r] + i] = b[i].first;
+                A.val[(size_t)A.ptr[r] + i] = b[i].second;
+            }
+        }
+        std::vector<std::pair<int, float>>().swap(bucket);
+        // Air and Aii per subdomain (independent).
+#pragma omp parallel for schedule(dynamic)
+        for (int s = 0; s < nsub; ++s) {
+            BoxWork& W = work[s];
             std::vector<std::pair<uint64_t, float>> ap;
             ap.reserve(W.air_terms[m].size());
             for (auto& tv : W.air_terms[m])
-                ap.push_back({((uint64_t)(uint32_t)tv.first.first << 32) | (uint32_t)to_g[tv.first.second], tv.second});
-            air_pairs[s].swap(ap);
+                ap.push_back({((uint64_t)(uint32_t)tv.first.first << 32) | (uint32_t)to_g[s][tv.first.second], tv.second});
+            out.Air[m][s] = csr_from_pairs(W.n_int[m], nif, ap);
             out.Aii[m][s] = std::move(W.aii[m]);
             out.aii_xyz[m][s] = std::move(W.int_xyz[m]);
-            W.arr_terms[m].clear();
         }
-        for (int s = 0; s < nsub; ++s) out.Air[m][s] = csr_from_pairs(work[s].n_int[m], 0, air_pairs[s]);
-        std::vector<std::pair<uint64_t, float>> ae(arr[m].begin(), arr[m].end());
-        out.Arr[m] = csr_from_pairs(out.n_iface[m], out.n_iface[m], ae);
-        for (int s = 0; s < nsub; ++s) out.Air[m][s].cols = out.n_iface[m];
         if (m == 0)
             for (int r = 0; r < out.Arr[0].rows; ++r) {
                 bool diag = false;
