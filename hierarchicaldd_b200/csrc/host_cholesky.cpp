@@ -12,6 +12,9 @@
 #include <cmath>
 #include <functional>
 #include <numeric>
+#include <string>
+
+#include <omp.h>
 
 #include "sigma.h"
 
@@ -19,6 +22,63 @@ namespace hdd {
 
 namespace {
 constexpr int kLeaf = 32;
+
+// Trailing update of a front after a panel of kb columns starting at k0: for
+// the columns c in [c0, c0 + kColBlock) (clipped to f) and every row i >= c,
+//   F(i, c) -= sum_{kk < kb} F(i, k0 + kk) * F(c, k0 + kk),
+// F column-major with leading dimension f.  The panel rows t0..f-1 are read
+// from P, packed by pack_panel in blocks of kRowBlock rows so that each kk
+// step reads one contiguous run.  Each sum starts at 0 and adds its products
+// in kk order, whatever the blocking, so the result does not depend on the
+// instruction set or the thread that runs it (no FMA contraction: the library
+// is built with -ffp-contract=off).  kColBlock x kRowBlock independent
+// accumulators vectorise over the rows; the AVX-512 or AVX2 clone is picked at
+// load time where the CPU has it.  c0 - t0 is a multiple of kColBlock.
+constexpr int kColBlock = 4;
+constexpr int kRowBlock = 8;
+
+// P[(r * kb + kk) * kRowBlock + a] = F(t0 + r * kRowBlock + a, k0 + kk), zero
+// past row f - 1.
+void pack_panel(const double* F, int f, int k0, int kb, int t0, std::vector<double>& P) {
+    const int nrb = (f - t0 + kRowBlock - 1) / kRowBlock;
+    P.assign((size_t)nrb * kb * kRowBlock, 0.0);
+    for (int kk = 0; kk < kb; ++kk) {
+        const double* col = F + (size_t)(k0 + kk) * f;
+        for (int i = t0; i < f; ++i) {
+            const int r = (i - t0) / kRowBlock, a = (i - t0) % kRowBlock;
+            P[((size_t)r * kb + kk) * kRowBlock + a] = col[i];
+        }
+    }
+}
+
+__attribute__((target_clones("avx512f", "avx2", "default")))
+void trailing_update(double* F, int f, const double* P, int kb, int t0, int c0) {
+    const int cn = std::min(kColBlock, f - c0);
+    const int rc = (c0 - t0) / kRowBlock, ac = (c0 - t0) % kRowBlock;
+    const int nrb = (f - t0 + kRowBlock - 1) / kRowBlock;
+    const double* Pc = P + (size_t)rc * kb * kRowBlock + ac;
+    for (int r = rc; r < nrb; ++r) {
+        const double* Pr = P + (size_t)r * kb * kRowBlock;
+        double acc[kColBlock][kRowBlock];
+        for (int b = 0; b < kColBlock; ++b)
+            for (int a = 0; a < kRowBlock; ++a) acc[b][a] = 0.0;
+        for (int kk = 0; kk < kb; ++kk) {
+            double l[kColBlock];
+            for (int b = 0; b < kColBlock; ++b) l[b] = Pc[(size_t)kk * kRowBlock + b];
+            const double* pr = Pr + (size_t)kk * kRowBlock;
+            for (int b = 0; b < kColBlock; ++b)
+                for (int a = 0; a < kRowBlock; ++a) acc[b][a] += pr[a] * l[b];
+        }
+        const int i0 = t0 + r * kRowBlock;
+        for (int b = 0; b < cn; ++b) {
+            double* col = F + (size_t)(c0 + b) * f;
+            for (int a = 0; a < kRowBlock; ++a) {
+                const int i = i0 + a;
+                if (i >= c0 + b && i < f) col[i] -= acc[b][a];
+            }
+        }
+    }
+}
 }
 
 void SnFactor::analyze(const CsrF& A, const std::vector<std::array<int, 3>>* xyz) {
@@ -229,6 +289,38 @@ void SnFactor::analyze(const CsrF& A, const std::vector<std::array<int, 3>>* xyz
     }
 }
 
+namespace {
+// Column c of Fw = [L^{-1}; -L_RJ L^{-1}] for one front (x: nj + nr entries,
+// zero on entry): forward substitution of e_c through L (nj x nj, col-major),
+// then w = -R x with R = L_RJ (nr x nj, col-major).  Axpy loops only, so the
+// vectorised clones give the same values as the scalar one.
+__attribute__((target_clones("avx2", "default")))
+void solve_block_column(const double* L, const double* R, int nj, int nr, int c, double* x) {
+    x[c] = 1.0;
+    for (int jj = c; jj < nj; ++jj) {
+        const double* Lc = L + (size_t)jj * nj;
+        const double xj = x[jj] / Lc[jj];
+        x[jj] = xj;
+        if (xj == 0.0) continue;
+        for (int i = jj + 1; i < nj; ++i) x[i] -= Lc[i] * xj;
+    }
+    double* w = x + nj;
+    for (int a = c; a < nj; ++a) {
+        const double la = x[a];
+        if (la == 0.0) continue;
+        const double* Ra = R + (size_t)a * nr;
+        for (int k = 0; k < nr; ++k) w[k] -= Ra[k] * la;
+    }
+}
+}  // namespace
+
+namespace {
+struct FrontScratch {
+    std::vector<int> pos;
+    std::vector<double> front, panel;
+};
+}  // namespace
+
 void SnFactor::factor(const CsrF& A, double eps) {
     const int ns = (int)col0.size();
     std::vector<int> iperm(n);
@@ -239,10 +331,16 @@ void SnFactor::factor(const CsrF& A, double eps) {
     Ljj.assign(ns, {});
     Lrj.assign(ns, {});
     std::vector<std::vector<double>> upd(ns);
-    std::vector<int> pos(n, -1);
-    for (int j = 0; j < ns; ++j) {
+    // One front: assemble A's columns and the children's update matrices (in
+    // child order), partial dense Cholesky, keep L_JJ, L_RJ and the update
+    // matrix for the parent.  `scratch.pos` is an n-long map (all -1 on entry
+    // and on exit); the front and panel buffers are reused from front to front.  The arithmetic of a front does not depend on which thread
+    // runs it or on `inner_par`, so the factor is the same for any schedule.
+    auto factor_front = [&](int j, FrontScratch& scratch, bool inner_par) {
         const int nj = ncol[j], nr = (int)rows[j].size(), f = nj + nr;
-        std::vector<double> F((size_t)f * f, 0.0);  // col-major, lower triangle used
+        std::vector<int>& pos = scratch.pos;
+        std::vector<double>& F = scratch.front;
+        F.assign((size_t)f * f, 0.0);  // col-major, lower triangle used
         for (int a = 0; a < nj; ++a) pos[col0[j] + a] = a;
         for (int k = 0; k < nr; ++k) pos[rows[j][k]] = nj + k;
         for (int a = 0; a < nj; ++a) {
@@ -272,10 +370,9 @@ void SnFactor::factor(const CsrF& A, double eps) {
         }
         // Dense partial Cholesky of the front (first nj columns), blocked in
         // panels of kPanel columns: factor the panel, then update the trailing
-        // columns with row-major copies of the panel so every update is a
-        // contiguous dot product.
+        // columns (trailing_update).
         constexpr int kPanel = 48;
-        std::vector<double> Pn;
+        std::vector<double>& Pk = scratch.panel;
         for (int k0 = 0; k0 < nj; k0 += kPanel) {
             const int kb = std::min(kPanel, nj - k0);
             for (int k = k0; k < k0 + kb; ++k) {
@@ -294,22 +391,11 @@ void SnFactor::factor(const CsrF& A, double eps) {
             }
             const int t0 = k0 + kb;
             if (t0 >= f) continue;
-            Pn.assign((size_t)(f - t0) * kb, 0.0);
-            for (int kk = 0; kk < kb; ++kk) {
-                const double* colk = &F[(size_t)(k0 + kk) * f];
-                for (int i = t0; i < f; ++i) Pn[(size_t)(i - t0) * kb + kk] = colk[i];
-            }
-#pragma omp parallel for schedule(dynamic, 8) if ((size_t)(f - t0) * (f - t0) * kb > 4000000)
-            for (int c = t0; c < f; ++c) {
-                const double* lc = &Pn[(size_t)(c - t0) * kb];
-                double* colc = &F[(size_t)c * f];
-                for (int i = c; i < f; ++i) {
-                    const double* li = &Pn[(size_t)(i - t0) * kb];
-                    double acc = 0.0;
-                    for (int kk = 0; kk < kb; ++kk) acc += li[kk] * lc[kk];
-                    colc[i] -= acc;
-                }
-            }
+            pack_panel(F.data(), f, k0, kb, t0, Pk);
+            const int nblk = (f - t0 + kColBlock - 1) / kColBlock;
+            const double* P = Pk.data();
+#pragma omp parallel for schedule(dynamic, 2) if (inner_par && (size_t)(f - t0) * (f - t0) * kb > 4000000)
+            for (int cb = 0; cb < nblk; ++cb) trailing_update(F.data(), f, P, kb, t0, t0 + cb * kColBlock);
         }
         Ljj[j].assign((size_t)nj * nj, 0.0);
         Lrj[j].assign((size_t)nr * nj, 0.0);
@@ -324,7 +410,56 @@ void SnFactor::factor(const CsrF& A, double eps) {
         }
         for (int a = 0; a < nj; ++a) pos[col0[j] + a] = -1;
         for (int k = 0; k < nr; ++k) pos[rows[j][k]] = -1;
+    };
+
+    // Schedule over the elimination tree.  Fronts are in post-order, so the
+    // subtree of front j is the index range [first[j], j].  Subtrees whose work
+    // is at most 1/(8 * threads) of the total (and whose parent's is not) run
+    // in parallel, each in post-order on one thread; the remaining top fronts
+    // (the large separators near the root) then run in post-order with the
+    // trailing updates of big fronts split over the threads.
+    std::vector<double> work(ns, 0.0);
+    std::vector<int> first(ns);
+    for (int j = 0; j < ns; ++j) first[j] = j;
+    double total = 0;
+    for (int j = 0; j < ns; ++j) {
+        const double f = (double)ncol[j] + (double)rows[j].size();
+        work[j] += (double)ncol[j] * f * f + f;
+        total += (double)ncol[j] * f * f + f;
+        if (parent[j] >= 0) {
+            work[parent[j]] += work[j];
+            first[parent[j]] = std::min(first[parent[j]], first[j]);
+        }
     }
+    const int threads = std::max(1, omp_get_max_threads());
+    const double cut = total / (8.0 * threads);
+    std::vector<int> roots;
+    std::vector<char> in_subtree(ns, 0);
+    for (int j = 0; j < ns; ++j)
+        if (work[j] <= cut && (parent[j] < 0 || work[parent[j]] > cut)) roots.push_back(j);
+    for (int r : roots)
+        for (int j = first[r]; j <= r; ++j) in_subtree[j] = 1;
+    std::sort(roots.begin(), roots.end(), [&](int a, int b) { return work[a] > work[b]; });
+    std::string err;
+#pragma omp parallel if (roots.size() > 1 && !omp_in_parallel())
+    {
+        FrontScratch sc;
+        sc.pos.assign(n, -1);
+#pragma omp for schedule(dynamic, 1)
+        for (long t = 0; t < (long)roots.size(); ++t) {
+            try {
+                for (int j = first[roots[t]]; j <= roots[t]; ++j) factor_front(j, sc, false);
+            } catch (const std::exception& e) {
+#pragma omp critical(hdd_factor_err)
+                err = e.what();
+            }
+        }
+    }
+    if (!err.empty()) throw Error(HDD_ERR_INTERNAL, err);
+    FrontScratch sc;
+    sc.pos.assign(n, -1);
+    for (int j = 0; j < ns; ++j)
+        if (!in_subtree[j]) factor_front(j, sc, true);
 }
 
 void SnFactor::build_solve_blocks() {
@@ -342,24 +477,7 @@ void SnFactor::build_solve_blocks() {
         const std::vector<double>& L = Ljj[j];
         const std::vector<double>& R = Lrj[j];
 #pragma omp parallel for schedule(dynamic, 4) if (inner_par)
-        for (int c = 0; c < nj; ++c) {
-            double* x = &F[(size_t)c * m];
-            x[c] = 1.0;
-            for (int jj = c; jj < nj; ++jj) {
-                const double* Lc = &L[(size_t)jj * nj];
-                const double xj = x[jj] / Lc[jj];
-                x[jj] = xj;
-                if (xj == 0.0) continue;
-                for (int i = jj + 1; i < nj; ++i) x[i] -= Lc[i] * xj;
-            }
-            double* w = x + nj;
-            for (int a = c; a < nj; ++a) {
-                const double la = x[a];
-                if (la == 0.0) continue;
-                const double* Ra = &R[(size_t)a * nr];
-                for (int k = 0; k < nr; ++k) w[k] -= Ra[k] * la;
-            }
-        }
+        for (int c = 0; c < nj; ++c) solve_block_column(L.data(), R.data(), nj, nr, c, &F[(size_t)c * m]);
     };
     std::vector<int> small;
     for (int j = 0; j < ns; ++j)

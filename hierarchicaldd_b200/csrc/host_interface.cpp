@@ -183,6 +183,31 @@ struct LevelArrays {
     }
 };
 
+// m += P^T (G P) for one child (CELL_PROLONGATION_BAKER / GALERKIN_PROCESS):
+// t = G P, then m_ij += sum_k P_ki t_kj.  Every sum starts at 0 and adds its
+// eight products in k order; the loops run over j innermost so they vectorise
+// without changing that order (no FMA contraction: -ffp-contract=off).
+__attribute__((target_clones("avx2", "default")))
+void galerkin_add(const M8& g, const M8& p, M8& m) {
+    M8 t;
+    for (int i = 0; i < 8; ++i) {
+        float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int k = 0; k < 8; ++k) {
+            const float gik = g[i * 8 + k];
+            for (int j = 0; j < 8; ++j) acc[j] += gik * p[k * 8 + j];
+        }
+        for (int j = 0; j < 8; ++j) t[i * 8 + j] = acc[j];
+    }
+    for (int i = 0; i < 8; ++i) {
+        float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int k = 0; k < 8; ++k) {
+            const float pki = p[k * 8 + i];
+            for (int j = 0; j < 8; ++j) acc[j] += pki * t[k * 8 + j];
+        }
+        for (int j = 0; j < 8; ++j) m[i * 8 + j] += acc[j];
+    }
+}
+
 void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
     const I3 lo = W.lo, hi = W.hi;
     Stride qtop;
@@ -379,12 +404,41 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
         node_count[m] = count;
     }
 
-    // Galerkin-coarsened cell matrices, memoised per (level, cell).
+    // Galerkin-coarsened cell matrices, memoised per (level, cell): a dense
+    // box-local table per level (reused by the thread from box to box), with a
+    // hash table for any cell outside it.
+    struct MemoRange { int lo[3], e[3]; size_t base; };
+    std::vector<MemoRange> mr(levels + 1);
+    size_t memo_cells = 0;
+    for (int L = 1; L <= levels; ++L) {
+        size_t cnt = 1;
+        for (int a = 0; a < 3; ++a) {
+            mr[L].lo[a] = (lo[a] >> (L - 1)) - 1;
+            mr[L].e[a] = (hi[a] >> (L - 1)) + 2 - mr[L].lo[a];
+            cnt *= (size_t)mr[L].e[a];
+        }
+        mr[L].base = memo_cells;
+        memo_cells += cnt;
+    }
+    static thread_local std::vector<M8> memo_store;
+    static thread_local std::vector<uint8_t> memo_done;
+    if (memo_store.size() < memo_cells) memo_store.resize(memo_cells);
+    memo_done.assign(memo_cells, 0);
     std::vector<std::unordered_map<uint64_t, M8>> memo(levels + 1);
     std::function<const M8&(const I3&, int)> galerkin = [&](const I3& C, int level) -> const M8& {
+        const MemoRange& R = mr[level];
+        bool dense = true;
+        for (int a = 0; a < 3; ++a)
+            if (C[a] < R.lo[a] || C[a] >= R.lo[a] + R.e[a]) dense = false;
+        const size_t slot =
+            dense ? R.base + ((size_t)(C[0] - R.lo[0]) * R.e[1] + (C[1] - R.lo[1])) * R.e[2] + (C[2] - R.lo[2]) : 0;
         const uint64_t key = ((uint64_t)C[0] << 42) | ((uint64_t)C[1] << 21) | (uint64_t)C[2];
-        auto it = memo[level].find(key);
-        if (it != memo[level].end()) return it->second;
+        if (dense) {
+            if (memo_done[slot]) return memo_store[slot];
+        } else {
+            auto it = memo[level].find(key);
+            if (it != memo[level].end()) return it->second;
+        }
         M8 m;
         m.fill(0.0f);
         if (level == 1) {
@@ -413,30 +467,28 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
         } else {
             for (int o = 0; o < 8; ++o) {
                 const I3 child = {2 * C[0] - 1 + (o >> 2), 2 * C[1] - 1 + ((o >> 1) & 1), 2 * C[2] - 1 + (o & 1)};
-                const M8 g = galerkin(child, level - 1);
-                const M8& p = P[o];
-                M8 t;
-                for (int i = 0; i < 8; ++i)
-                    for (int j = 0; j < 8; ++j) {
-                        float acc = 0;
-                        for (int k = 0; k < 8; ++k) acc += g[i * 8 + k] * p[k * 8 + j];
-                        t[i * 8 + j] = acc;
-                    }
-                for (int i = 0; i < 8; ++i)
-                    for (int j = 0; j < 8; ++j) {
-                        float acc = 0;
-                        for (int k = 0; k < 8; ++k) acc += p[k * 8 + i] * t[k * 8 + j];
-                        m[i * 8 + j] += acc;
-                    }
+                galerkin_add(galerkin(child, level - 1), P[o], m);
             }
+        }
+        if (dense) {
+            memo_store[slot] = m;
+            memo_done[slot] = 1;
+            return memo_store[slot];
         }
         return memo[level].emplace(key, m).first->second;
     };
 
-    // Assembly (lines 554-655).
+    // Assembly (lines 554-655).  Each cell's node parents are resolved once;
+    // the entries are then summed in the reference's (cell, n1, n2, parent1,
+    // parent2) order, so every Aii / Air sum adds its terms in that order.
     for (int m = 1; m <= M; ++m) {
-        std::unordered_map<uint64_t, float> aii;
-        std::unordered_map<uint64_t, size_t> air_pos;
+        // Per interior row: its Aii entries (column, sum) and its Air entries
+        // (interface column, index into air_terms), in first-encounter order.
+        const int nrow = node_count[m];
+        std::vector<std::vector<std::pair<int, float>>> aii_rows(nrow);
+        std::vector<std::vector<std::pair<int, size_t>>> air_rows(nrow);
+        // Walks up the hierarchy to the level that owns node p; false when no
+        // level does (an error only if an entry with this parent is used).
         auto resolve = [&](int L, const I3& p, uint32_t& f, int& id) {
             I3 idx = p;
             int cur = L;
@@ -447,44 +499,64 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
                 id = A.index[pp];
             }
             while (!(f & N_DEGREE)) {
-                if (++cur > levels) throw Error(HDD_ERR_INTERNAL, "interface DOF lookup past the coarsest level");
+                if (++cur > levels) return false;
                 for (int a = 0; a < 3; ++a) idx[a] /= 2;
                 const LevelArrays& A = H[m][cur];
                 const size_t pp = A.at(idx);
                 f = A.flags[pp];
                 id = A.index[pp];
             }
+            return true;
         };
+        struct Resolved { uint32_t f; int id; float w; bool ok; };
+        std::vector<Resolved> res[8];
+        Parents par;
         for (int L = m; L <= levels; ++L)
             for (const I3& c : interior_cells(m, L)) {
                 const M8& cm = galerkin(c, L);
-                Parents par[8];
                 for (int li = 0; li < 8; ++li) {
                     const I3 N = {c[0] - 1 + (li >> 2), c[1] - 1 + ((li >> 1) & 1), c[2] - 1 + (li & 1)};
-                    embed(N, par[li], 1.0f, q[L]);
+                    par.clear();
+                    embed(N, par, 1.0f, q[L]);
+                    res[li].clear();
+                    for (auto& p : par) {
+                        Resolved r;
+                        r.ok = resolve(L, p.first, r.f, r.id);
+                        r.w = p.second;
+                        res[li].push_back(r);
+                    }
                 }
                 for (int n1 = 0; n1 < 8; ++n1)
                     for (int n2 = 0; n2 < 8; ++n2) {
                         const float e = cm[n1 * 8 + n2];
                         if (e == 0) continue;
-                        for (auto& p1 : par[n1])
-                            for (auto& p2 : par[n2]) {
-                                uint32_t f1, f2;
-                                int id1, id2;
-                                resolve(L, p1.first, f1, id1);
-                                resolve(L, p2.first, f2, id2);
-                                const float v = p1.second * p2.second * e;
+                        for (const Resolved& p1 : res[n1])
+                            for (const Resolved& p2 : res[n2]) {
+                                if (!p1.ok || !p2.ok)
+                                    throw Error(HDD_ERR_INTERNAL, "interface DOF lookup past the coarsest level");
+                                const uint32_t f1 = p1.f, f2 = p2.f;
+                                const int id1 = p1.id, id2 = p2.id;
+                                const float v = p1.w * p2.w * e;
                                 const bool a1 = f1 & (N_ACTIVE | N_COARSE_SHARED), a2 = f2 & (N_ACTIVE | N_COARSE_SHARED);
                                 if ((f1 & N_INTERFACE) && (f2 & N_INTERFACE))
                                     W.arr_terms[m - 1].push_back({{id1, id2}, v});
-                                if (a1 && a2) aii[((uint64_t)(uint32_t)id1 << 32) | (uint32_t)id2] += v;
+                                if (a1 && (id1 < 0 || id1 >= nrow))
+                                    throw Error(HDD_ERR_INTERNAL, "interior DOF number out of range");
+                                if (a1 && a2) {
+                                    auto& row = aii_rows[id1];
+                                    size_t k = 0;
+                                    while (k < row.size() && row[k].first != id2) ++k;
+                                    if (k == row.size()) row.push_back({id2, 0.0f});
+                                    row[k].second += v;
+                                }
                                 if (a1 && (f2 & N_INTERFACE)) {
-                                    const uint64_t key = ((uint64_t)(uint32_t)id1 << 32) | (uint32_t)id2;
-                                    auto it = air_pos.find(key);
-                                    if (it == air_pos.end()) {
-                                        air_pos.emplace(key, W.air_terms[m - 1].size());
+                                    auto& row = air_rows[id1];
+                                    size_t k = 0;
+                                    while (k < row.size() && row[k].first != id2) ++k;
+                                    if (k == row.size()) {
+                                        row.push_back({id2, W.air_terms[m - 1].size()});
                                         W.air_terms[m - 1].push_back({{id1, id2}, v});
-                                    } else W.air_terms[m - 1][it->second].second += v;
+                                    } else W.air_terms[m - 1][row[k].second].second += v;
                                 }
                             }
                     }
@@ -492,17 +564,18 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
         const int ni = node_count[m];
         W.n_int[m - 1] = ni;
         // Aii in CSR with explicit zeros dropped (Convert_To_Eigen, lines 687-705).
-        std::vector<std::pair<uint64_t, float>> e(aii.begin(), aii.end());
-        e.erase(std::remove_if(e.begin(), e.end(), [](const auto& t) { return t.second == 0.0f; }), e.end());
-        std::sort(e.begin(), e.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
         CsrF& A = W.aii[m - 1];
         A.rows = A.cols = ni;
         A.ptr.assign(ni + 1, 0);
-        for (auto& t : e) A.ptr[(int)(t.first >> 32) + 1]++;
-        for (int r = 0; r < ni; ++r) A.ptr[r + 1] += A.ptr[r];
-        A.col.resize(e.size());
-        A.val.resize(e.size());
-        for (size_t i = 0; i < e.size(); ++i) { A.col[i] = (int)(uint32_t)e[i].first; A.val[i] = e[i].second; }
+        A.col.clear();
+        A.val.clear();
+        for (int r = 0; r < ni; ++r) {
+            auto& row = aii_rows[r];
+            std::sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+            for (const auto& t : row)
+                if (t.second != 0.0f) { A.col.push_back(t.first); A.val.push_back(t.second); }
+            A.ptr[r + 1] = (int)A.col.size();
+        }
     }
 }
 
