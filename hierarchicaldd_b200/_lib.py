@@ -20,6 +20,8 @@ STATUS_NAMES = {
 }
 PRECISION_REFERENCE = 0
 PRECISION_MIXED = 1
+# Initialize_Preconditioner's iomode (reference Test_Bench -iomode).
+IOMODES = {"neither": 0, "output": 1, "input": 2}
 
 
 class hdd_options(C.Structure):
@@ -60,6 +62,7 @@ SIGNATURES = {
     "hdd_create": (C.c_int, [C.POINTER(hdd_options), C.POINTER(C.c_void_p)]),
     "hdd_set_domain_dense": (C.c_int, [_vp, C.POINTER(C.c_uint32), _fp]),
     "hdd_load_spgrid_dir": (C.c_int, [_vp, C.c_char_p]),
+    "hdd_set_iomode": (C.c_int, [_vp, C.c_int, C.c_char_p]),
     "hdd_initialize_preconditioner": (C.c_int, [_vp]),
     "hdd_set_rhs_dense": (C.c_int, [_vp, _fp]),
     "hdd_solve": (C.c_int, [_vp, C.POINTER(hdd_result)]),

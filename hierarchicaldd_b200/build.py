@@ -18,6 +18,7 @@ SOURCES = [
     "host_setup.cpp",
     "host_interface.cpp",
     "host_cholesky.cpp",
+    "host_interface_io.cpp",
     "capi.cpp",
     "server.cpp",
     "kernels_vcycle.cu",

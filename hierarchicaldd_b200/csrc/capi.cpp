@@ -184,6 +184,17 @@ hdd_status hdd_vcycle_dense(hdd_solver* s, float* u, const float* b, int n_vcycl
     return guard(s, [&](Solver& v) { v.vcycle_dense(u, b, n_vcycles); });
 }
 
+hdd_status hdd_set_iomode(hdd_solver* s, int iomode, const char* directory) {
+    return guard(s, [&](Solver& v) {
+        if (iomode < HDD_IOMODE_NEITHER || iomode > HDD_IOMODE_INPUT)
+            throw Error(HDD_ERR_INVALID_ARGUMENT, "iomode must be HDD_IOMODE_NEITHER, _OUTPUT or _INPUT");
+        if (iomode != HDD_IOMODE_NEITHER && (!directory || !*directory))
+            throw Error(HDD_ERR_INVALID_ARGUMENT, "iomode output/input needs a directory");
+        v.iomode = iomode;
+        v.io_dir = directory ? directory : "";
+    });
+}
+
 hdd_status hdd_multiply_dense(hdd_solver* s, const float* x, float* y) {
     if (!x || !y) return HDD_ERR_INVALID_ARGUMENT;
     return guard(s, [&](Solver& v) { v.multiply_dense(x, y); });

@@ -6,6 +6,7 @@
 
 #include <array>
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "hdd_common.h"
@@ -38,6 +39,16 @@ struct InterfaceHost {
 // Domain_Divider pass, as the reference splits first), in parallel over
 // subdomains.
 void build_interface(const DomainLayout& L, int sigma_levels, InterfaceHost& out);
+
+// Interface dump and reload, the reference's -iomode output / input
+// (CPU/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Decomposition_Solver.h:121-161);
+// host_interface_io.cpp.  read_interface_dir throws HDD_ERR_IO on a missing or
+// malformed file; check_interface throws HDD_ERR_INVALID_ARGUMENT when a
+// reloaded system does not fit the domain (levels, subdomain count, sizes,
+// interface cells).
+void write_interface_dir(const InterfaceHost& ih, const std::string& dir);
+void read_interface_dir(const std::string& dir, InterfaceHost& ih);
+void check_interface(const DomainLayout& L, int sigma_levels, const InterfaceHost& ih);
 
 // Supernodal Cholesky of (A + eps I) (zero rows get eps), the stand-in for
 // the reference's MKL PARDISO phases 11/22 (SIGMA_SMOOTHER.cpp:241-414).

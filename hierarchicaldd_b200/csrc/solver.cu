@@ -17,7 +17,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cerrno>
 #include <cstring>
+
+#include <sys/stat.h>
 
 #include "solver.h"
 
@@ -153,7 +156,17 @@ void Solver::initialize() {
         std::fprintf(stderr, "[hdd setup] layout %.2f s (%zu tiles, %zu boxes)\n",
                      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(), L.tiles.size(),
                      L.boxes.size());
-    build_interface(L, opts.sigma_levels, ih);
+    if (iomode == HDD_IOMODE_INPUT) {
+        read_interface_dir(io_dir, ih);
+        check_interface(L, opts.sigma_levels, ih);
+    } else {
+        build_interface(L, opts.sigma_levels, ih);
+    }
+    if (iomode == HDD_IOMODE_OUTPUT) {
+        if (::mkdir(io_dir.c_str(), 0777) != 0 && errno != EEXIST)
+            throw Error(HDD_ERR_IO, "cannot create " + io_dir + ": " + std::strerror(errno));
+        write_interface_dir(ih, io_dir);
+    }
     if (std::getenv("HDD_VERBOSE"))
         std::fprintf(stderr, "[hdd setup] interface assembly done at %.2f s\n",
                      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());

@@ -78,6 +78,8 @@ struct Solver {
     DevBuf<int> iface_nb;
     SigmaGpu sigma;
     InterfaceHost ih;
+    int iomode = HDD_IOMODE_NEITHER;  // interface dump / reload at initialize()
+    std::string io_dir;
     double setup_ms = 0;
 
     // Optional per-phase device timing with CUDA events on the solver stream

@@ -60,7 +60,14 @@ class SPGrid_Domain_Decomposition_Solver:
     def Initialize_Preconditioner(self, v_cycle_levels, size, subdomain_size, sigma_levels, nVcycles,
                                   interior_smoothing, boundary_smoothing, sigma_smoothing, n_sigma_mg,
                                   tol=1e-6, relative_tol=True, max_iters=5000, min_iters=0,
-                                  precision_mode=_lib.PRECISION_REFERENCE, true_residual_every=20):
+                                  precision_mode=_lib.PRECISION_REFERENCE, true_residual_every=20,
+                                  iomode="neither", dump_directory="matrices_dump"):
+        """Setup with the reference's arguments (SPGrid_Domain_Decomposition_Solver.h:121).
+        ``iomode`` "output" writes the interface matrices to ``dump_directory`` in the
+        reference's dump layout, "input" reads them from there instead of assembling
+        (the reference defaults to "output"; this mirror to "neither")."""
+        if iomode not in _lib.IOMODES:
+            raise HddError(1, f"iomode must be one of {sorted(_lib.IOMODES)}, not {iomode!r}")
         o = hdd_options()
         self.lib.hdd_options_default(C.byref(o))
         size = tuple(int(s) for s in (size if np.ndim(size) else (size,) * 3))
@@ -91,6 +98,7 @@ class SPGrid_Domain_Decomposition_Solver:
         else:
             self._check(self.lib.hdd_set_domain_dense(self.h, self.flags.ctypes.data_as(C.POINTER(C.c_uint32)),
                                                       _fp(self.rhs)))
+        self._check(self.lib.hdd_set_iomode(self.h, _lib.IOMODES[iomode], str(dump_directory).encode()))
         self._check(self.lib.hdd_initialize_preconditioner(self.h))
 
     # -- solve --------------------------------------------------------------------

@@ -95,6 +95,28 @@ hdd_status hdd_set_domain_dense(hdd_solver* s, const uint32_t* flags, const floa
  * (demos/SPGrid_Create_Simple_Domain/SPGRID_READ_WRITE.h:43-51). */
 hdd_status hdd_load_spgrid_dir(hdd_solver* s, const char* directory);
 
+/* Interface-matrix dump modes of Initialize_Preconditioner's iomode argument
+ * (demos/Domain_Decomposition_CPU_Only/SPGrid_Domain_Decomposition_Solver/
+ *  SPGrid_Domain_Decomposition_Solver.h:121-161, Test_Bench -iomode). */
+enum {
+    HDD_IOMODE_NEITHER = 0, /* assemble, write nothing (this library's default) */
+    HDD_IOMODE_OUTPUT = 1,  /* assemble, then write the matrices to the directory */
+    HDD_IOMODE_INPUT = 2    /* read the matrices from the directory instead of assembling */
+};
+
+/* Sets the iomode and dump directory used by the next
+ * hdd_initialize_preconditioner.  The directory holds the reference's dump
+ * layout (INTERFACE_SOLVER_DATA::Write_To_File, INTERFACE_SOLVER_DATA.h:177-212,
+ * and INTERFACE_MATRIX_GENERATOR::Write_Interface_Map, :66-72): files levels and
+ * number_of_subdomains, Matrix Market Aii_<l>_<s>, Air_<l>_<s>, Arr_<l>, Prr_<l>,
+ * and interface_map; this library adds positions_<l> for its fill-reducing
+ * ordering.  OUTPUT creates the directory if needed.  INPUT checks the dump
+ * against the domain (HDD_ERR_INVALID_ARGUMENT when its levels, subdomain count,
+ * sizes or interface cells differ) and reports unreadable files as HDD_ERR_IO.
+ * The reference defaults to iomode "output" into "matrices_dump"; this library
+ * defaults to HDD_IOMODE_NEITHER. */
+hdd_status hdd_set_iomode(hdd_solver* s, int iomode, const char* directory);
+
 /* Replaces Initialize_Preconditioner (SPGrid_Domain_Decomposition_Solver.h:121-161):
  * flags, subdomains, V-cycle topology, interface matrices and factorisations. */
 hdd_status hdd_initialize_preconditioner(hdd_solver* s);

@@ -59,6 +59,64 @@ void* shim_build(const int size[3], const int sub[3], int vlevels, int sigma_lev
 
 void shim_free(void* h) { delete static_cast<Shim*>(h); }
 
+// Interface dump / reload (the reference's -iomode): 0 on success, else the
+// hdd_status with its message in err.
+int shim_write_interface(void* h, const char* dir, char* err, int errlen) {
+    try {
+        write_interface_dir(static_cast<Shim*>(h)->ih, dir);
+        return 0;
+    } catch (const Error& e) {
+        if (err && errlen > 0) { std::strncpy(err, e.what(), errlen - 1); err[errlen - 1] = 0; }
+        return (int)e.status;
+    }
+}
+
+// A handle holding only a reloaded interface system (NULL on error).
+void* shim_read_interface(const char* dir, char* err, int errlen) {
+    Shim* s = new Shim();
+    try {
+        read_interface_dir(dir, s->ih);
+        return s;
+    } catch (const Error& e) {
+        if (err && errlen > 0) { std::strncpy(err, e.what(), errlen - 1); err[errlen - 1] = 0; }
+        delete s;
+        return nullptr;
+    }
+}
+
+// Checks the interface system of `sys` against the layout of `dom`.
+int shim_check_interface(void* dom, void* sys, int sigma_levels, char* err, int errlen) {
+    try {
+        check_interface(static_cast<Shim*>(dom)->L, sigma_levels, static_cast<Shim*>(sys)->ih);
+        return 0;
+    } catch (const Error& e) {
+        if (err && errlen > 0) { std::strncpy(err, e.what(), errlen - 1); err[errlen - 1] = 0; }
+        return (int)e.status;
+    }
+}
+
+// Interface DOF positions of level l: n entries (3 ints each) into out when
+// out != NULL; sub < 0 selects the interface, else that subdomain's interior.
+long long shim_positions(void* h, int l, int sub, int* out) {
+    const InterfaceHost& ih = static_cast<Shim*>(h)->ih;
+    if (l < 0 || l >= (int)ih.iface_xyz.size()) return -1;
+    const std::vector<std::array<int, 3>>& p =
+        sub < 0 ? ih.iface_xyz[l] : (sub < (int)ih.aii_xyz[l].size() ? ih.aii_xyz[l][sub] : ih.iface_xyz[l]);
+    if (out)
+        for (size_t i = 0; i < p.size(); ++i)
+            for (int a = 0; a < 3; ++a) out[3 * i + a] = p[i][a];
+    return (long long)p.size();
+}
+
+// Level-0 interface map: n cells into out (3 ints each) when out != NULL.
+long long shim_interface_map(void* h, int* out) {
+    const InterfaceHost& ih = static_cast<Shim*>(h)->ih;
+    if (out)
+        for (size_t i = 0; i < ih.iface_map.size(); ++i)
+            for (int a = 0; a < 3; ++a) out[3 * i + a] = ih.iface_map[i][a];
+    return (long long)ih.iface_map.size();
+}
+
 int shim_num_subdomains(void* h) { return static_cast<Shim*>(h)->ih.n_sub; }
 
 // kind: 0 Arr, 1 Aii, 2 Air, 3 Prr.  shape = {rows, cols, nnz}; returns 0 on success.

@@ -3,6 +3,9 @@ assembly and supernodal Cholesky sources of the CUDA library compiled on their
 own into a test shim (tests/host_shim.cpp).
 
 * the interface matrices (Arr, Aii, Air, Prr) equal the oracle's bit for bit;
+* the interface dump (the reference's -iomode output layout) reads back
+  unchanged, follows the reference's file layout, reads hand-written Matrix
+  Market files, and is checked against the domain on reload;
 * the supernodal factorisation solves (A + 1e-5 I) x = b to FP64 accuracy for
   every matrix kind, and its explicit solve blocks [L^-1; -L_RJ L^-1] (what the
   GPU kernels read) give the same solution.
@@ -28,7 +31,7 @@ SHIM = os.path.join(BUILD, "libhost_shim.so")
 def shim():
     os.makedirs(BUILD, exist_ok=True)
     srcs = [os.path.join(ROOT, "tests", "host_shim.cpp")] + [
-        os.path.join(CSRC, f) for f in ("host_setup.cpp", "host_interface.cpp", "host_cholesky.cpp")]
+        os.path.join(CSRC, f) for f in ("host_setup.cpp", "host_interface.cpp", "host_cholesky.cpp", "host_interface_io.cpp")]
     if not os.path.exists(SHIM) or any(os.path.getmtime(f) > os.path.getmtime(SHIM) for f in srcs):
         subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
                         "-I", CSRC, "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
@@ -41,6 +44,15 @@ def shim():
     L.shim_num_subdomains.argtypes = [C.c_void_p]
     L.shim_matrix_shape.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, ip]
     L.shim_matrix_get.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, ip, ip, C.POINTER(C.c_double)]
+    cp = C.c_char_p
+    L.shim_write_interface.argtypes = [C.c_void_p, cp, cp, C.c_int]
+    L.shim_read_interface.restype = C.c_void_p
+    L.shim_read_interface.argtypes = [cp, cp, C.c_int]
+    L.shim_check_interface.argtypes = [C.c_void_p, C.c_void_p, C.c_int, cp, C.c_int]
+    L.shim_positions.restype = C.c_longlong
+    L.shim_positions.argtypes = [C.c_void_p, C.c_int, C.c_int, ip]
+    L.shim_interface_map.restype = C.c_longlong
+    L.shim_interface_map.argtypes = [C.c_void_p, ip]
     L.shim_factor_check.restype = C.c_double
     L.shim_factor_check.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
     return L
@@ -134,3 +146,165 @@ def test_single_subdomain_has_no_level0_interface(shim):
     o = Oracle(d.size, d.sub_size, d.flags, vlevels=3, nVcycles=1, interior_smoothing=3, boundary_smoothing=3,
                sigma_levels=2, sigma_smoothing=3, sigma_mg=1)
     assert o.num_interface(0) == 0
+
+
+# ---- interface dump / reload (the reference's -iomode output / input) ---------------------
+
+
+def raw_matrix(L, h, kind, level, sub=0):
+    shape = (C.c_int * 3)()
+    if L.shim_matrix_shape(h, kind, level, sub, shape) != 0:
+        return None
+    rows, cols, nnz = shape
+    ptr = np.zeros(rows + 1, np.int32)
+    col = np.zeros(max(nnz, 1), np.int32)
+    val = np.zeros(max(nnz, 1), np.float64)
+    L.shim_matrix_get(h, kind, level, sub, ptr.ctypes.data_as(C.POINTER(C.c_int)),
+                      col.ctypes.data_as(C.POINTER(C.c_int)), val.ctypes.data_as(C.POINTER(C.c_double)))
+    return rows, cols, ptr, col[:nnz], val[:nnz]
+
+
+def points(L, h, level, sub):
+    n = L.shim_positions(h, level, sub, None)
+    out = np.zeros((max(n, 0), 3), np.int32)
+    if n > 0:
+        L.shim_positions(h, level, sub, out.ctypes.data_as(C.POINTER(C.c_int)))
+    return out
+
+
+def imap(L, h):
+    n = L.shim_interface_map(h, None)
+    out = np.zeros((n, 3), np.int32)
+    if n:
+        L.shim_interface_map(h, out.ctypes.data_as(C.POINTER(C.c_int)))
+    return out
+
+
+def read_dump(L, path):
+    err = C.create_string_buffer(512)
+    h = L.shim_read_interface(str(path).encode(), err, 512)
+    return h, err.value.decode()
+
+
+def test_interface_dump_reads_back_unchanged(shim, tmp_path):
+    d = domains.small((40, 36, 44), 8, 6, seed=4)
+    M = d.meta["sigma_levels"]
+    h = build(shim, d, M)
+    err = C.create_string_buffer(512)
+    try:
+        assert shim.shim_write_interface(h, str(tmp_path).encode(), err, 512) == 0, err.value
+        h2, msg = read_dump(shim, tmp_path)
+        assert h2, msg
+        try:
+            nsub = shim.shim_num_subdomains(h)
+            assert shim.shim_num_subdomains(h2) == nsub
+            for l in range(M):
+                mats = [(0, 0)] + ([(3, 0)] if l + 1 < M else []) + [(k, s) for s in range(nsub) for k in (1, 2)]
+                for kind, sub in mats:
+                    a, b = raw_matrix(shim, h, kind, l, sub), raw_matrix(shim, h2, kind, l, sub)
+                    assert a[:2] == b[:2], (kind, l, sub)
+                    for x, y in zip(a[2:], b[2:]):
+                        assert np.array_equal(x, y), (kind, l, sub)
+                assert np.array_equal(points(shim, h, l, -1), points(shim, h2, l, -1))
+                for s in range(nsub):
+                    assert np.array_equal(points(shim, h, l, s), points(shim, h2, l, s))
+            assert np.array_equal(imap(shim, h), imap(shim, h2))
+            assert shim.shim_check_interface(h, h2, M, err, 512) == 0, err.value
+        finally:
+            shim.shim_free(h2)
+    finally:
+        shim.shim_free(h)
+
+
+def _market(path):
+    lines = open(path).read().splitlines()
+    rows, cols, nnz = (int(v) for v in lines[1].split())
+    ent = np.array([ln.split() for ln in lines[2:]], dtype=object).reshape(-1, 3)
+    return lines[0], (rows, cols, nnz), ent[:, 0].astype(int), ent[:, 1].astype(int), ent[:, 2].astype(np.float32)
+
+
+def test_interface_dump_follows_the_reference_layout(shim, tmp_path):
+    """levels / number_of_subdomains (int32), Matrix Market Aii/Arr in column-major
+    and Air/Prr in row-major entry order with 1-based indices, interface_map as a
+    uint64 count and int32 triples (INTERFACE_SOLVER_DATA.h:177-212,
+    INTERFACE_MATRIX_GENERATOR.h:66-72)."""
+    d = domains.small(32, 8, 6, seed=4)
+    M = d.meta["sigma_levels"]
+    h = build(shim, d, M)
+    err = C.create_string_buffer(512)
+    try:
+        assert shim.shim_write_interface(h, str(tmp_path).encode(), err, 512) == 0, err.value
+        nsub = shim.shim_num_subdomains(h)
+        assert np.fromfile(tmp_path / "levels", np.int32).tolist() == [M]
+        assert np.fromfile(tmp_path / "number_of_subdomains", np.int32).tolist() == [nsub]
+        for name, kind, sub, col_major in (("Arr_0", 0, 0, True), ("Aii_0_3", 1, 3, True),
+                                           ("Air_0_3", 2, 3, False), ("Prr_0", 3, 0, False)):
+            head, shape, r, c, v = _market(tmp_path / name)
+            assert head == "%%MatrixMarket matrix coordinate real general"
+            ref = matrix(shim, h, kind, 0, sub).tocoo()
+            assert shape == (ref.shape[0], ref.shape[1], ref.nnz) and len(r) == ref.nnz
+            assert r.min() >= 1 and c.min() >= 1
+            outer = c if col_major else r
+            assert np.all(np.diff(outer) >= 0), name
+            got = sp.csr_matrix((v.astype(np.float64), (r - 1, c - 1)), shape=ref.shape)
+            assert (got != ref.tocsr()).nnz == 0, name
+        raw = (tmp_path / "interface_map").read_bytes()
+        n = int(np.frombuffer(raw[:8], np.uint64)[0])
+        assert len(raw) == 8 + 12 * n
+        assert np.array_equal(np.frombuffer(raw[8:], np.int32).reshape(n, 3), imap(shim, h))
+    finally:
+        shim.shim_free(h)
+
+
+def test_reload_reads_hand_written_market_files(shim, tmp_path):
+    """A one-subdomain dump written by hand the way Eigen's saveMarket writes it:
+    comment lines, a symmetric header storing one triangle, duplicate entries
+    summed."""
+    np.array([1], np.int32).tofile(tmp_path / "levels")
+    np.array([1], np.int32).tofile(tmp_path / "number_of_subdomains")
+    (tmp_path / "Arr_0").write_text("%%MatrixMarket matrix coordinate real symmetric\n% interface\n2 2 3\n"
+                                    "1 1 2.0\n2 1 -5.00000000e-01\n2 2 3.0\n")
+    (tmp_path / "Aii_0_0").write_text("%%MatrixMarket matrix coordinate real general\n1 1 2\n1 1 1.5\n1 1 0.25\n")
+    (tmp_path / "Air_0_0").write_text("%%MatrixMarket matrix coordinate real general\n1 2 1\n1 2 -0.125\n")
+    with open(tmp_path / "interface_map", "wb") as f:
+        np.array([2], np.uint64).tofile(f)
+        np.array([[0, 0, 4], [0, 0, 8]], np.int32).tofile(f)
+    h, msg = read_dump(shim, tmp_path)
+    assert h, msg
+    try:
+        assert np.array_equal(matrix(shim, h, 0, 0).toarray(), [[2.0, -0.5], [-0.5, 3.0]])
+        assert np.array_equal(matrix(shim, h, 1, 0, 0).toarray(), [[1.75]])
+        assert np.array_equal(matrix(shim, h, 2, 0, 0).toarray(), [[0.0, -0.125]])
+        assert imap(shim, h).tolist() == [[0, 0, 4], [0, 0, 8]]
+        # No positions file: the level-0 interface positions are the interface cells.
+        assert points(shim, h, 0, -1).tolist() == [[0, 0, 4], [0, 0, 8]]
+    finally:
+        shim.shim_free(h)
+
+
+def test_reload_errors(shim, tmp_path):
+    d = domains.small(32, 8, 6, seed=4)
+    M = d.meta["sigma_levels"]
+    h = build(shim, d, M)
+    err = C.create_string_buffer(512)
+    try:
+        h0, msg = read_dump(shim, tmp_path / "missing")
+        assert not h0 and "cannot open" in msg
+        assert shim.shim_write_interface(h, str(tmp_path).encode(), err, 512) == 0, err.value
+        h2, msg = read_dump(shim, tmp_path)
+        assert h2, msg
+        try:
+            # A dump of another sigma hierarchy depth, or of another domain, is refused.
+            assert shim.shim_check_interface(h, h2, M + 1, err, 512) == 1 and b"levels" in err.value
+            other = build(shim, domains.small(32, 16, 5, seed=4), M)
+            try:
+                assert shim.shim_check_interface(other, h2, M, err, 512) == 1 and b"subdomains" in err.value
+            finally:
+                shim.shim_free(other)
+        finally:
+            shim.shim_free(h2)
+        (tmp_path / "Arr_0").write_text("%%MatrixMarket matrix coordinate real general\n3 3 2\n1 1 1.0\n")
+        h3, msg = read_dump(shim, tmp_path)
+        assert not h3 and "fewer entries" in msg
+    finally:
+        shim.shim_free(h)
