@@ -1,4 +1,5 @@
-"""Builds the CUDA library libhdd_b200.so in-tree for sm_100a.
+"""Builds the CUDA library libhdd_b200.so in-tree for sm_100a, and the
+hdd_test_bench command line (the reference's Test_Bench_3D flags) linked to it.
 
 Usage: python -m hierarchicaldd_b200.build  (or build() from Python).
 """
@@ -12,6 +13,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libhdd_b200.so")
+# The reference's Test_Bench_3D command line over the C ABI.
+CLI = os.path.join(HERE, "hdd_test_bench")
 BUILD = os.path.join(HERE, "_build")
 
 SOURCES = [
@@ -70,6 +73,14 @@ def build(verbose: bool = False, force: bool = False) -> str:
         subprocess.run(cmd, check=True)
     if force or not os.path.exists(OUT) or any(os.path.getmtime(o) > os.path.getmtime(OUT) for o in objs):
         cmd = [nvcc] + ARCH + ["-shared", "-ccbin", cxx, "-o", OUT] + objs + ["-lgomp"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    cli_src = os.path.join(CSRC, "test_bench_main.cpp")
+    if force or not os.path.exists(CLI) or any(os.path.getmtime(f) > os.path.getmtime(CLI)
+                                               for f in (cli_src, OUT)):
+        cmd = [cxx, "-std=c++17", "-O2", "-fopenmp", "-I", os.path.join(os.path.dirname(HERE), "include"),
+               cli_src, "-o", CLI, "-L", HERE, "-l:libhdd_b200.so", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
