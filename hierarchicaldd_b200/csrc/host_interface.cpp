@@ -15,6 +15,7 @@
 // (subdomain, cell) order, so the assembled matrices follow the reference's
 // numbering and float summation order.
 #include <algorithm>
+#include <deque>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -404,8 +405,12 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
         node_count[m] = count;
     }
 
-    // Galerkin-coarsened cell matrices, memoised per (level, cell): a dense
-    // box-local table per level (reused by the thread from box to box), with a
+    // Galerkin-coarsened cell matrices.  A cell's matrix depends only on its
+    // type: at level 1 the kinds of its 8 nodes (Active/Interface, Dirichlet or
+    // neither), at coarser levels the types of its 8 children.  Each distinct
+    // type is computed once per subdomain, by the same operations in the same
+    // order as for any cell of that type; cells keep a type id, in a dense
+    // box-local table per level (reused by the thread from box to box) with a
     // hash table for any cell outside it.
     struct MemoRange { int lo[3], e[3]; size_t base; };
     std::vector<MemoRange> mr(levels + 1);
@@ -420,12 +425,20 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
         mr[L].base = memo_cells;
         memo_cells += cnt;
     }
-    static thread_local std::vector<M8> memo_store;
-    static thread_local std::vector<uint8_t> memo_done;
-    if (memo_store.size() < memo_cells) memo_store.resize(memo_cells);
-    memo_done.assign(memo_cells, 0);
-    std::vector<std::unordered_map<uint64_t, M8>> memo(levels + 1);
-    std::function<const M8&(const I3&, int)> galerkin = [&](const I3& C, int level) -> const M8& {
+    static thread_local std::vector<int> memo_type;
+    memo_type.assign(memo_cells, -1);
+    std::vector<std::unordered_map<uint64_t, int>> memo(levels + 1);
+    std::deque<M8> mats;                              // matrix of each type id
+    std::vector<int> node_types(6561, -1);            // level 1: 3^8 node-kind codes
+    struct ChildHash {
+        size_t operator()(const std::array<int, 8>& k) const {
+            uint64_t h = 1469598103934665603ull;
+            for (int v : k) h = (h ^ (uint32_t)v) * 1099511628211ull;
+            return (size_t)h;
+        }
+    };
+    std::vector<std::unordered_map<std::array<int, 8>, int, ChildHash>> child_types(levels + 1);
+    std::function<int(const I3&, int)> cell_type = [&](const I3& C, int level) -> int {
         const MemoRange& R = mr[level];
         bool dense = true;
         for (int a = 0; a < 3; ++a)
@@ -434,49 +447,68 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
             dense ? R.base + ((size_t)(C[0] - R.lo[0]) * R.e[1] + (C[1] - R.lo[1])) * R.e[2] + (C[2] - R.lo[2]) : 0;
         const uint64_t key = ((uint64_t)C[0] << 42) | ((uint64_t)C[1] << 21) | (uint64_t)C[2];
         if (dense) {
-            if (memo_done[slot]) return memo_store[slot];
+            if (memo_type[slot] >= 0) return memo_type[slot];
         } else {
             auto it = memo[level].find(key);
             if (it != memo[level].end()) return it->second;
         }
-        M8 m;
-        m.fill(0.0f);
+        int id;
         if (level == 1) {
-            const float w = (float)(1.0 / (1 << 2));
             uint32_t nf[8];
-            for (int li = 0; li < 8; ++li) {
+            int code = 0;
+            for (int li = 7; li >= 0; --li) {
                 const I3 node = {C[0] - 1 + (li >> 2), C[1] - 1 + ((li >> 1) & 1), C[2] - 1 + (li & 1)};
                 const uint32_t s = W.sf(node);
                 nf[li] = (s & (F_ACTIVE | F_INTERFACE)) ? 1u : ((s & F_DIRICHLET) ? 2u : 0u);
+                code = code * 3 + (int)nf[li];
             }
-            for (int v = 0; v < 3; ++v) {
-                const int a = (v == 0) ? 1 : 0, b = (v == 2) ? 1 : 2;
-                for (int e = 0; e < 4; ++e) {
-                    int lb[3], ub[3];
-                    lb[v] = 0; ub[v] = 1;
-                    lb[a] = ub[a] = e >> 1;
-                    lb[b] = ub[b] = e & 1;
-                    const int l = lb[0] * 4 + lb[1] * 2 + lb[2], u = ub[0] * 4 + ub[1] * 2 + ub[2];
-                    if (nf[l] == 1u && nf[u] == 1u) {
-                        m[l * 8 + u] -= w; m[l * 8 + l] += w; m[u * 8 + u] += w; m[u * 8 + l] -= w;
+            id = node_types[code];
+            if (id < 0) {
+                M8 m;
+                m.fill(0.0f);
+                const float w = (float)(1.0 / (1 << 2));
+                for (int v = 0; v < 3; ++v) {
+                    const int a = (v == 0) ? 1 : 0, b = (v == 2) ? 1 : 2;
+                    for (int e = 0; e < 4; ++e) {
+                        int lb[3], ub[3];
+                        lb[v] = 0; ub[v] = 1;
+                        lb[a] = ub[a] = e >> 1;
+                        lb[b] = ub[b] = e & 1;
+                        const int l = lb[0] * 4 + lb[1] * 2 + lb[2], u = ub[0] * 4 + ub[1] * 2 + ub[2];
+                        if (nf[l] == 1u && nf[u] == 1u) {
+                            m[l * 8 + u] -= w; m[l * 8 + l] += w; m[u * 8 + u] += w; m[u * 8 + l] -= w;
+                        }
+                        if (nf[l] == 1u && nf[u] == 2u) m[l * 8 + l] += w;
+                        if (nf[l] == 2u && nf[u] == 1u) m[u * 8 + u] += w;
                     }
-                    if (nf[l] == 1u && nf[u] == 2u) m[l * 8 + l] += w;
-                    if (nf[l] == 2u && nf[u] == 1u) m[u * 8 + u] += w;
                 }
+                id = (int)mats.size();
+                mats.push_back(m);
+                node_types[code] = id;
             }
         } else {
+            std::array<int, 8> ch;
             for (int o = 0; o < 8; ++o) {
                 const I3 child = {2 * C[0] - 1 + (o >> 2), 2 * C[1] - 1 + ((o >> 1) & 1), 2 * C[2] - 1 + (o & 1)};
-                galerkin_add(galerkin(child, level - 1), P[o], m);
+                ch[o] = cell_type(child, level - 1);
+            }
+            auto it = child_types[level].find(ch);
+            if (it != child_types[level].end()) {
+                id = it->second;
+            } else {
+                M8 m;
+                m.fill(0.0f);
+                for (int o = 0; o < 8; ++o) galerkin_add(mats[ch[o]], P[o], m);
+                id = (int)mats.size();
+                mats.push_back(m);
+                child_types[level].emplace(ch, id);
             }
         }
-        if (dense) {
-            memo_store[slot] = m;
-            memo_done[slot] = 1;
-            return memo_store[slot];
-        }
-        return memo[level].emplace(key, m).first->second;
+        if (dense) memo_type[slot] = id;
+        else memo[level].emplace(key, id);
+        return id;
     };
+    auto galerkin = [&](const I3& C, int level) -> const M8& { return mats[cell_type(C, level)]; };
 
     // Assembly (lines 554-655).  Each cell's node parents are resolved once;
     // the entries are then summed in the reference's (cell, n1, n2, parent1,
