@@ -62,6 +62,9 @@ SIGNATURES = {
     "hdd_create": (C.c_int, [C.POINTER(hdd_options), C.POINTER(C.c_void_p)]),
     "hdd_set_domain_dense": (C.c_int, [_vp, C.POINTER(C.c_uint32), _fp]),
     "hdd_load_spgrid_dir": (C.c_int, [_vp, C.c_char_p]),
+    "hdd_set_domain_pages": (C.c_int, [_vp, C.c_longlong, _ip, C.POINTER(C.c_uint32), _fp]),
+    "hdd_set_rhs_pages": (C.c_int, [_vp, C.c_longlong, _ip, _fp]),
+    "hdd_get_solution_pages": (C.c_int, [_vp, C.c_longlong, _ip, _fp]),
     "hdd_set_iomode": (C.c_int, [_vp, C.c_int, C.c_char_p]),
     "hdd_initialize_preconditioner": (C.c_int, [_vp]),
     "hdd_set_rhs_dense": (C.c_int, [_vp, _fp]),

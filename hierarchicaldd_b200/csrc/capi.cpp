@@ -102,6 +102,38 @@ hdd_status hdd_set_domain_dense(hdd_solver* s, const uint32_t* flags, const floa
     return guard(s, [&](Solver& v) { v.set_domain(flags, rhs); });
 }
 
+hdd_status hdd_set_domain_pages(hdd_solver* s, long long n_pages, const int32_t* page_origin,
+                                const uint32_t* flags, const float* rhs) {
+    if ((n_pages > 0 && (!page_origin || !flags || !rhs)) || n_pages < 0) return HDD_ERR_INVALID_ARGUMENT;
+    return guard(s, [&](Solver& v) {
+        const size_t N = (size_t)v.opts.size[0] * v.opts.size[1] * v.opts.size[2];
+        std::vector<uint32_t> f(N, 0u);
+        std::vector<float> b(N, 0.0f);
+        hdd::pages_to_dense(v.opts.size, n_pages, page_origin, flags, f.data());
+        hdd::pages_to_dense(v.opts.size, n_pages, page_origin, rhs, b.data());
+        v.set_domain(f.data(), b.data());
+    });
+}
+
+hdd_status hdd_set_rhs_pages(hdd_solver* s, long long n_pages, const int32_t* page_origin, const float* rhs) {
+    if ((n_pages > 0 && (!page_origin || !rhs)) || n_pages < 0) return HDD_ERR_INVALID_ARGUMENT;
+    return guard(s, [&](Solver& v) {
+        if (!v.initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+        std::vector<float> b((size_t)v.opts.size[0] * v.opts.size[1] * v.opts.size[2], 0.0f);
+        hdd::pages_to_dense(v.opts.size, n_pages, page_origin, rhs, b.data());
+        v.set_rhs(b.data());
+    });
+}
+
+hdd_status hdd_get_solution_pages(hdd_solver* s, long long n_pages, const int32_t* page_origin, float* x) {
+    if ((n_pages > 0 && (!page_origin || !x)) || n_pages < 0) return HDD_ERR_INVALID_ARGUMENT;
+    return guard(s, [&](Solver& v) {
+        std::vector<float> d((size_t)v.opts.size[0] * v.opts.size[1] * v.opts.size[2]);
+        v.get_solution(d.data());
+        hdd::dense_to_pages(v.opts.size, n_pages, page_origin, d.data(), x);
+    });
+}
+
 hdd_status hdd_load_spgrid_dir(hdd_solver* s, const char* dir) {
     if (!dir) return HDD_ERR_INVALID_ARGUMENT;
     return guard(s, [&](Solver& v) {

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <unordered_set>
 
 namespace hdd {
 
@@ -291,6 +292,62 @@ void tiles_to_dense(const DomainLayout& L, const float* tiled, float* dense) {
                 long long s = L.tile_slot(i, j, k);
                 dense[at3(n, i, j, k)] = s >= 0 ? tiled[s] : 0.0f;
             }
+}
+
+namespace {
+
+void check_pages(long long n, const int32_t* origin) {
+    if (n < 0 || (n > 0 && !origin)) throw Error(HDD_ERR_INVALID_ARGUMENT, "bad page count or origin array");
+    std::unordered_set<uint64_t> seen;
+    seen.reserve((size_t)n);
+    for (long long p = 0; p < n; ++p) {
+        uint64_t key = 0;
+        for (int a = 0; a < 3; ++a) {
+            const int32_t o = origin[3 * p + a];
+            if (o < 0 || o % kPageDims[a] != 0)
+                throw Error(HDD_ERR_INVALID_ARGUMENT, "page origin " + std::to_string(p) +
+                                                          " is negative or not a multiple of (4, 8, 8)");
+            if (o / kPageDims[a] >= (1 << 21))
+                throw Error(HDD_ERR_INVALID_ARGUMENT, "page origin " + std::to_string(p) + " is too large");
+            key = (key << 21) | (uint64_t)(o / kPageDims[a]);
+        }
+        if (!seen.insert(key).second)
+            throw Error(HDD_ERR_INVALID_ARGUMENT, "page " + std::to_string(p) + " is listed twice");
+    }
+}
+
+// Calls fn(page element, dense index) for every cell of the pages inside the grid.
+template <class Fn>
+void for_page_cells(const int size[3], long long n, const int32_t* origin, Fn fn) {
+    for (long long p = 0; p < n; ++p) {
+        const int32_t* o = origin + 3 * p;
+        for (int x = 0; x < kPageDims[0]; ++x)
+            for (int y = 0; y < kPageDims[1]; ++y)
+                for (int z = 0; z < kPageDims[2]; ++z) {
+                    const long long i = (long long)o[0] + x, j = (long long)o[1] + y, k = (long long)o[2] + z;
+                    if (i >= size[0] || j >= size[1] || k >= size[2]) continue;
+                    fn((size_t)p * kPageCells + (size_t)((x * 8 + y) * 8 + z),
+                       ((size_t)i * size[1] + (size_t)j) * size[2] + (size_t)k);
+                }
+    }
+}
+
+}  // namespace
+
+void pages_to_dense(const int size[3], long long n, const int32_t* origin, const uint32_t* values, uint32_t* dense) {
+    check_pages(n, origin);
+    for_page_cells(size, n, origin, [&](size_t e, size_t d) { dense[d] = values[e]; });
+}
+
+void pages_to_dense(const int size[3], long long n, const int32_t* origin, const float* values, float* dense) {
+    check_pages(n, origin);
+    for_page_cells(size, n, origin, [&](size_t e, size_t d) { dense[d] = values[e]; });
+}
+
+void dense_to_pages(const int size[3], long long n, const int32_t* origin, const float* dense, float* values) {
+    check_pages(n, origin);
+    std::fill(values, values + (size_t)n * kPageCells, 0.0f);
+    for_page_cells(size, n, origin, [&](size_t e, size_t d) { values[e] = dense[d]; });
 }
 
 }  // namespace hdd

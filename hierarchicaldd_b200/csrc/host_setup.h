@@ -70,6 +70,22 @@ void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& out);
 void dense_to_tiles(const DomainLayout& L, const float* dense, float* tiled);
 void tiles_to_dense(const DomainLayout& L, const float* tiled, float* dense);
 
+// SPGrid pages: 4 x 8 x 8 cells, the 4 KB page of a 16-byte cell struct with
+// 4-byte channels (SPGrid_Mask<4,2,3>, SPGrid_Mask.h:25-31); cell (x, y, z) of a
+// page is element (x * 8 + y) * 8 + z, and a page's origin (its cell (0,0,0))
+// is a multiple of (4, 8, 8).
+constexpr int kPageDims[3] = {4, 8, 8};
+constexpr int kPageCells = 256;
+
+// Scatters n pages (origin[3*p + a], values[256*p + e]) into a dense grid of
+// size[0..2] cells, z fastest; cells outside the grid are skipped, other dense
+// cells are left as they are.  Throws HDD_ERR_INVALID_ARGUMENT for a negative or
+// misaligned origin or a page listed twice.
+void pages_to_dense(const int size[3], long long n, const int32_t* origin, const uint32_t* values, uint32_t* dense);
+void pages_to_dense(const int size[3], long long n, const int32_t* origin, const float* values, float* dense);
+// Gathers the same pages from a dense grid (0 outside the grid).
+void dense_to_pages(const int size[3], long long n, const int32_t* origin, const float* dense, float* values);
+
 // Level-0 flag pipeline pieces (same semantics as the reference passes).
 void divide_domain(const int size[3], const int sub[3], uint32_t* f);
 void flag_faces(const int n[3], uint32_t* f);

@@ -246,4 +246,25 @@ def small(n_cells=32, sub=8, radius=6, seed=0, delta=None) -> Domain:
                        sigma_levels=2, sigma_smoothing=3, sigma_mg=1))
 
 
+def to_pages(flags: np.ndarray, *fields: np.ndarray):
+    """SPGrid pages (4 x 8 x 8 cells) of a dense domain, as hdd_set_domain_pages
+    takes them: the pages holding a non-zero flag, their origins (n, 3) and each
+    array as (n, 256) with cell (x, y, z) of a page at (x*8 + y)*8 + z."""
+    dims = (4, 8, 8)
+    size = flags.shape
+    padded = tuple(-(-n // d) * d for n, d in zip(size, dims))
+
+    def blocks(a):
+        p = np.zeros(padded, a.dtype)
+        p[:size[0], :size[1], :size[2]] = a
+        p = p.reshape(padded[0] // 4, 4, padded[1] // 8, 8, padded[2] // 8, 8)
+        return p.transpose(0, 2, 4, 1, 3, 5).reshape(-1, 256)
+
+    fb = blocks(flags)
+    keep = np.flatnonzero(fb.any(axis=1))
+    nb = (padded[0] // 4, padded[1] // 8, padded[2] // 8)
+    origin = (np.stack(np.unravel_index(keep, nb), axis=1) * np.array(dims)).astype(np.int32)
+    return (origin, fb[keep]) + tuple(blocks(f)[keep] for f in fields)
+
+
 CONFIGS = {"c1": config1, "c2": config2, "c3": config3, "p128": profile_case}

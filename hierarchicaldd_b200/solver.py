@@ -18,6 +18,10 @@ from . import _lib
 from ._lib import HddError, hdd_options, hdd_result
 
 
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
 def _fp(a):
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
@@ -33,6 +37,7 @@ class SPGrid_Domain_Decomposition_Solver:
         self.rhs = None
         self.spgrid_dir = None
         self.spgrid_size = None
+        self.pages = None
         self.last_result = None
         self.options = None
 
@@ -48,6 +53,20 @@ class SPGrid_Domain_Decomposition_Solver:
         self.size = None
         self.spgrid_dir = base_dir
         self.flags = self.rhs = None
+        self.pages = None
+
+    def Set_Domain_Pages(self, page_origin: np.ndarray, flags: np.ndarray, rhs: np.ndarray):
+        """SPGrid pages of 4x8x8 cells, as Convert/Copy read them from an SPGrid
+        allocator: page_origin (n, 3) cell index of each page's first cell,
+        flags / rhs (n, 256) with cell (x, y, z) of a page at (x*8 + y)*8 + z.
+        The grid size is the ``size`` given to Initialize_Preconditioner."""
+        origin = np.ascontiguousarray(page_origin, np.int32).reshape(-1, 3)
+        n = origin.shape[0]
+        self.pages = (origin, np.ascontiguousarray(flags, np.uint32).reshape(n, 256),
+                      np.ascontiguousarray(rhs, np.float32).reshape(n, 256))
+        self.size = None
+        self.spgrid_dir = None
+        self.flags = self.rhs = None
 
     def Set_Domain(self, flags: np.ndarray, rhs: np.ndarray):
         """Dense flags (uint32, reference bits) and right-hand side (float32)."""
@@ -55,6 +74,7 @@ class SPGrid_Domain_Decomposition_Solver:
         self.flags = np.ascontiguousarray(flags, np.uint32)
         self.rhs = np.ascontiguousarray(rhs, np.float32)
         self.spgrid_dir = None
+        self.pages = None
 
     # -- setup ------------------------------------------------------------------
     def Initialize_Preconditioner(self, v_cycle_levels, size, subdomain_size, sigma_levels, nVcycles,
@@ -76,6 +96,8 @@ class SPGrid_Domain_Decomposition_Solver:
             if any(a > b for a, b in zip(size, self.spgrid_size)):
                 raise HddError(1, f"size {size} exceeds the SPGrid directory's size {self.spgrid_size}")
             self.size = tuple(size)
+        elif self.pages is not None:
+            self.size = tuple(size)
         elif self.size is not None and tuple(size) != tuple(self.size):
             raise HddError(1, f"size {size} differs from the loaded domain {self.size}")
         for a in range(3):
@@ -95,6 +117,10 @@ class SPGrid_Domain_Decomposition_Solver:
         self.h = h
         if self.spgrid_dir is not None:
             self._check(self.lib.hdd_load_spgrid_dir(self.h, self.spgrid_dir.encode()))
+        elif self.pages is not None:
+            origin, flags, rhs = self.pages
+            self._check(self.lib.hdd_set_domain_pages(self.h, origin.shape[0], _ip(origin),
+                                                      flags.ctypes.data_as(C.POINTER(C.c_uint32)), _fp(rhs)))
         else:
             self._check(self.lib.hdd_set_domain_dense(self.h, self.flags.ctypes.data_as(C.POINTER(C.c_uint32)),
                                                       _fp(self.rhs)))
@@ -105,6 +131,11 @@ class SPGrid_Domain_Decomposition_Solver:
     def Set_RHS(self, rhs: np.ndarray):
         rhs = np.ascontiguousarray(rhs, np.float32)
         self._check(self.lib.hdd_set_rhs_dense(self.h, _fp(rhs)))
+
+    def Set_RHS_Pages(self, page_origin: np.ndarray, rhs: np.ndarray):
+        origin = np.ascontiguousarray(page_origin, np.int32).reshape(-1, 3)
+        rhs = np.ascontiguousarray(rhs, np.float32).reshape(origin.shape[0], 256)
+        self._check(self.lib.hdd_set_rhs_pages(self.h, origin.shape[0], _ip(origin), _fp(rhs)))
 
     def Solve(self, allow_not_converged: bool = False) -> dict:
         res = hdd_result()
@@ -118,6 +149,12 @@ class SPGrid_Domain_Decomposition_Solver:
     def Solution(self) -> np.ndarray:
         x = np.zeros(self.size, np.float32)
         self._check(self.lib.hdd_get_solution_dense(self.h, _fp(x)))
+        return x
+
+    def Solution_Pages(self, page_origin: np.ndarray) -> np.ndarray:
+        origin = np.ascontiguousarray(page_origin, np.int32).reshape(-1, 3)
+        x = np.zeros((origin.shape[0], 256), np.float32)
+        self._check(self.lib.hdd_get_solution_pages(self.h, origin.shape[0], _ip(origin), _fp(x)))
         return x
 
     # -- seams mirroring the reference's internal entry points ---------------------

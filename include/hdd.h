@@ -90,6 +90,23 @@ hdd_status hdd_create(const hdd_options* opts, hdd_solver** out);
  * loads cell flags and the right-hand side b. */
 hdd_status hdd_set_domain_dense(hdd_solver* s, const uint32_t* flags, const float* rhs);
 
+/* Sparse input in SPGrid pages, for callers holding an SPGrid allocator:
+ * replaces Convert / Copy (SPGrid_Domain_Decomposition_Solver.h:73-105 of the
+ * CPU demo), which read the flags and right-hand side channels page by page.
+ * A page is 4 x 8 x 8 cells (the 4 KB page of a 16-byte cell struct with
+ * 4-byte channels, SPGrid_Mask<4,2,3>); page_origin[3*p + a] is the cell
+ * index of page p's first cell (a multiple of 4, 8, 8 per axis), and cell
+ * (x, y, z) of page p is element 256*p + (x*8 + y)*8 + z of flags / rhs / x.
+ * Cells of pages outside options.size are ignored; cells in no page are
+ * exterior (flag 0).  A negative or misaligned origin, or a page listed twice,
+ * gives HDD_ERR_INVALID_ARGUMENT. */
+hdd_status hdd_set_domain_pages(hdd_solver* s, long long n_pages, const int32_t* page_origin,
+                                const uint32_t* flags, const float* rhs);
+/* Replaces the right-hand side only (zero outside the pages given). */
+hdd_status hdd_set_rhs_pages(hdd_solver* s, long long n_pages, const int32_t* page_origin, const float* rhs);
+/* Copies the solution of the last solve into the pages given (0 outside the grid). */
+hdd_status hdd_get_solution_pages(hdd_solver* s, long long n_pages, const int32_t* page_origin, float* x);
+
 /* Reads the reference's SPGrid directory format (size, block_offset, flags,
  * data) written by SPGRID_READ_WRITE::Write_SPGrid
  * (demos/SPGrid_Create_Simple_Domain/SPGRID_READ_WRITE.h:43-51). */

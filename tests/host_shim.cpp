@@ -59,6 +59,28 @@ void* shim_build(const int size[3], const int sub[3], int vlevels, int sigma_lev
 
 void shim_free(void* h) { delete static_cast<Shim*>(h); }
 
+// SPGrid page scatter / gather (hdd_set_domain_pages); 0 or the hdd_status.
+int shim_pages_to_dense(const int size[3], long long n, const int32_t* origin, const uint32_t* flags,
+                        const float* vals, uint32_t* dflags, float* dvals, char* err, int errlen) {
+    try {
+        pages_to_dense(size, n, origin, flags, dflags);
+        pages_to_dense(size, n, origin, vals, dvals);
+        return 0;
+    } catch (const Error& e) {
+        if (err && errlen > 0) { std::strncpy(err, e.what(), errlen - 1); err[errlen - 1] = 0; }
+        return (int)e.status;
+    }
+}
+
+int shim_dense_to_pages(const int size[3], long long n, const int32_t* origin, const float* dense, float* vals) {
+    try {
+        dense_to_pages(size, n, origin, dense, vals);
+        return 0;
+    } catch (const Error& e) {
+        return (int)e.status;
+    }
+}
+
 // Interface dump / reload (the reference's -iomode): 0 on success, else the
 // hdd_status with its message in err.
 int shim_write_interface(void* h, const char* dir, char* err, int errlen) {

@@ -6,6 +6,8 @@ own into a test shim (tests/host_shim.cpp).
 * the interface dump (the reference's -iomode output layout) reads back
   unchanged, follows the reference's file layout, reads hand-written Matrix
   Market files, and is checked against the domain on reload;
+* SPGrid pages (hdd_set_domain_pages) scatter to and gather from the dense grid
+  as the page layout says, and bad page lists are refused;
 * the supernodal factorisation solves (A + 1e-5 I) x = b to FP64 accuracy for
   every matrix kind, and its explicit solve blocks [L^-1; -L_RJ L^-1] (what the
   GPU kernels read) give the same solution.
@@ -53,6 +55,9 @@ def shim():
     L.shim_positions.argtypes = [C.c_void_p, C.c_int, C.c_int, ip]
     L.shim_interface_map.restype = C.c_longlong
     L.shim_interface_map.argtypes = [C.c_void_p, ip]
+    L.shim_pages_to_dense.argtypes = [ip, C.c_longlong, ip, C.POINTER(C.c_uint32), C.POINTER(C.c_float),
+                                      C.POINTER(C.c_uint32), C.POINTER(C.c_float), cp, C.c_int]
+    L.shim_dense_to_pages.argtypes = [ip, C.c_longlong, ip, C.POINTER(C.c_float), C.POINTER(C.c_float)]
     L.shim_factor_check.restype = C.c_double
     L.shim_factor_check.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
     return L
@@ -308,3 +313,60 @@ def test_reload_errors(shim, tmp_path):
         assert not h3 and "fewer entries" in msg
     finally:
         shim.shim_free(h)
+
+
+# ---- SPGrid pages (hdd_set_domain_pages / hdd_get_solution_pages) ------------------------
+
+
+def _u32(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def _f32(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _i32(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def test_pages_scatter_and_gather(shim):
+    d = domains.small((37, 30, 21), 8, 5, seed=2)   # ragged: the last pages reach past the grid
+    origin, fp, rp = domains.to_pages(d.flags, d.rhs)
+    rng = np.random.default_rng(0)
+    order = rng.permutation(len(origin))          # pages in any order
+    origin, fp, rp = (np.ascontiguousarray(a[order]) for a in (origin, fp, rp))
+    # A page wholly outside the grid is skipped.
+    origin = np.vstack([origin, [[40, 0, 0]]]).astype(np.int32)
+    fp = np.vstack([fp, np.full((1, 256), 0x10000, np.uint32)])
+    rp = np.vstack([rp, np.ones((1, 256), np.float32)])
+    size = (C.c_int * 3)(*d.size)
+    df = np.zeros(d.size, np.uint32)
+    dr = np.zeros(d.size, np.float32)
+    err = C.create_string_buffer(256)
+    assert shim.shim_pages_to_dense(size, len(origin), _i32(origin), _u32(fp), _f32(rp), _u32(df), _f32(dr),
+                                    err, 256) == 0, err.value
+    assert np.array_equal(df, d.flags) and np.array_equal(dr, d.rhs)
+    # Gather: cell (x, y, z) of page p at (x*8 + y)*8 + z; 0 outside the grid.
+    back = np.full((len(origin), 256), np.nan, np.float32)
+    assert shim.shim_dense_to_pages(size, len(origin), _i32(origin), _f32(dr), _f32(back)) == 0
+    for p in (0, len(origin) // 2, len(origin) - 1):
+        for x, y, z in ((0, 0, 0), (3, 7, 7), (1, 5, 2)):
+            i, j, k = origin[p] + (x, y, z)
+            want = dr[i, j, k] if i < d.size[0] and j < d.size[1] and k < d.size[2] else 0.0
+            assert back[p, (x * 8 + y) * 8 + z] == want
+
+
+@pytest.mark.parametrize("origin,msg", [([[4, 8, 8], [4, 8, 8]], b"twice"), ([[2, 0, 0]], b"multiple"),
+                                        ([[0, -8, 0]], b"negative")])
+def test_bad_page_lists_are_refused(shim, origin, msg):
+    origin = np.array(origin, np.int32)
+    size = (C.c_int * 3)(17, 17, 17)
+    v = np.zeros((len(origin), 256), np.uint32)
+    f = np.zeros((len(origin), 256), np.float32)
+    df = np.zeros((17, 17, 17), np.uint32)
+    dr = np.zeros((17, 17, 17), np.float32)
+    err = C.create_string_buffer(256)
+    assert shim.shim_pages_to_dense(size, len(origin), _i32(origin), _u32(v), _f32(f), _u32(df), _f32(dr),
+                                    err, 256) == 1
+    assert msg in err.value
