@@ -25,7 +25,7 @@ def test_pages_solve_like_the_dense_input():
     origin, fp, rp = origin[order], fp[order], rp[order]
     rhs2 = np.where((d.flags & domains.ACTIVE) != 0,
                     np.random.default_rng(2).uniform(-1, 1, d.size), 0).astype(np.float32)
-    _, r2p = domains.to_pages(d.flags, rhs2)
+    _, _, r2p = domains.to_pages(d.flags, rhs2)
     r2p = r2p[order]
     a = SPGrid_Domain_Decomposition_Solver()
     b = SPGrid_Domain_Decomposition_Solver()
@@ -38,7 +38,7 @@ def test_pages_solve_like_the_dense_input():
         xa = a.Solution()
         assert ra["iterations"] == rb["iterations"]
         assert np.array_equal(xa, b.Solution())
-        _, xa_pages = domains.to_pages(d.flags, xa)
+        _, _, xa_pages = domains.to_pages(d.flags, xa)
         assert np.array_equal(b.Solution_Pages(origin), xa_pages[order])
         a.Set_RHS(rhs2)
         b.Set_RHS_Pages(origin, r2p)
