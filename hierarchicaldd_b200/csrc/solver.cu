@@ -99,6 +99,7 @@ TileGeom Solver::geom() const {
 
 void Solver::initialize() {
     if (!have_domain) throw Error(HDD_ERR_NOT_INITIALIZED, "no domain set");
+    NvtxRange range("Initialize_Preconditioner");
     cuda_check(cudaSetDevice(opts.device), "cudaSetDevice");
     const auto t0 = std::chrono::steady_clock::now();
     build_layout(to_options(opts), flags_in.data(), L);
@@ -262,8 +263,12 @@ void Solver::run_vcycle(float* u, const float* bb, int halo_from_u, int zero_ini
 }
 
 void Solver::apply_preconditioner(const float* rr, float* zz) {
+    NvtxRange range("Apply_Preconditioner");
     const TileGeom g = geom();
-    run_vcycle(zz, rr, 0, 1, opts.nVcycles);
+    {
+        NvtxRange step("Step ONE");
+        run_vcycle(zz, rr, 0, 1, opts.nVcycles);
+    }
     const int n_if = ih.n_iface.empty() ? 0 : ih.n_iface[0];
     {
         Tm tm(this, 3);
@@ -272,6 +277,7 @@ void Solver::apply_preconditioner(const float* rr, float* zz) {
     }
     if (n_if > 0) {
         // u_G = 0 then sigma_mg V-cycles (Preconditioner.h:105,110-117).
+        NvtxRange sigma_range("Sigma_V_Cycle");
         Tm tm(this, 4);
         cuda_check(cudaMemsetAsync(sigma.u0(), 0, sizeof(float) * n_if, stream), "memset u0");
         for (int i = 0; i < opts.sigma_mg; ++i) sigma.vcycle(stream, launches, &hook);
@@ -281,11 +287,13 @@ void Solver::apply_preconditioner(const float* rr, float* zz) {
         cuda_check(launch_interface_scatter(iface_slot.p, n_if, sigma.u0(), zz, stream), "scatter");
         count();
     }
+    NvtxRange step("Step Two");
     run_vcycle(zz, rr, 1, 1, opts.nVcycles);
 }
 
 void Solver::solve(hdd_result* res) {
     if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+    NvtxRange range("solve");
     cuda_check(cudaSetDevice(opts.device), "cudaSetDevice");
     const TileGeom g = geom();
     const int nt = g.ntiles;

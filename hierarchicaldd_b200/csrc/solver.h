@@ -2,6 +2,7 @@
 // orchestration on one stream.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <memory>
 #include <string>
@@ -48,6 +49,17 @@ struct DevBuf {
     static void check(cudaError_t e) {
         if (e != cudaSuccess) throw Error(HDD_ERR_CUDA, cudaGetErrorString(e));
     }
+};
+
+// Host-side NVTX range named after the reference's LOG::SCOPE phases
+// (SPGrid_Domain_Decomposition_Preconditioner.h:119-152 of the GPU demo:
+// "Step ONE", "Sigma_V_Cycle", "Step Two"; Solver.h:193 "solve"), for Nsight
+// timelines; a no-op unless a profiler is attached.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
 };
 
 inline void cuda_check(cudaError_t e, const char* what) {
