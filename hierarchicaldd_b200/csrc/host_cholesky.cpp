@@ -140,15 +140,51 @@ void SnFactor::analyze(const CsrF& A, const std::vector<std::array<int, 3>>* xyz
         const int far = bfs(verts[0], pid, comp);
         for (int v : comp) level[v] = -1;
         if (comp.size() < verts.size()) {
-            const int pa = next_part++, pb = next_part++;
-            for (int v : verts) part[v] = pb;
-            for (int v : comp) part[v] = pa;
-            std::vector<int> rest;
-            for (int v : verts)
-                if (part[v] == pb) rest.push_back(v);
-            std::vector<int> ra = rec(comp, pa), rb = rec(rest, pb);
-            ra.insert(ra.end(), rb.begin(), rb.end());
-            return ra;
+            // Disconnected: order the components one after another.  All
+            // components are found in one pass over verts (each breadth-first
+            // from its first vertex in verts order), so a set of many small
+            // components costs linear time and no recursion depth.  Component
+            // i is ordered on its own (BFS order), except that once the
+            // remaining components hold at most kLeaf vertices they form one
+            // leaf, and the last component is ordered from its vertices in
+            // verts order: the ordering of peeling one component at a time.
+            std::vector<std::vector<int>> comps;
+            std::vector<int> ids;
+            ids.push_back(next_part++);
+            for (int v : comp) part[v] = ids.back();
+            comps.push_back(std::move(comp));
+            for (int v : verts) {
+                if (part[v] != pid) continue;
+                std::vector<int> c;
+                bfs(v, pid, c);
+                for (int w : c) level[w] = -1;
+                ids.push_back(next_part++);
+                for (int w : c) part[w] = ids.back();
+                comps.push_back(std::move(c));
+            }
+            std::vector<int> roots;
+            size_t remaining = verts.size();
+            for (size_t i = 0; i < comps.size(); ++i) {
+                if (i > 0 && remaining <= (size_t)kLeaf) {
+                    std::vector<int> rest;
+                    for (int v : verts)
+                        if (part[v] >= ids[i] && part[v] <= ids.back()) rest.push_back(v);
+                    roots.push_back(make_node(rest, {}));
+                    break;
+                }
+                std::vector<int> r;
+                if (i > 0 && i + 1 == comps.size()) {
+                    std::vector<int> last;
+                    for (int v : verts)
+                        if (part[v] == ids[i]) last.push_back(v);
+                    r = rec(last, ids[i]);
+                } else {
+                    r = rec(comps[i], ids[i]);
+                }
+                roots.insert(roots.end(), r.begin(), r.end());
+                remaining -= comps[i].size();
+            }
+            return roots;
         }
         if (xyz) {
             // Geometric split: for each axis, cut at the median position; the

@@ -177,6 +177,44 @@ def config3() -> Domain:
                        sigma_levels=4, sigma_smoothing=3, sigma_mg=1, true_residual_every=20))
 
 
+def config5(scale: int = 1) -> Domain:
+    """Sparse domain: a 1024^3-cell bounding box (size 1025) holding the union of
+    64 spheres, radii U[40, 120] cells, centres uniform in the box (Philox seed
+    5), about a tenth of the box.  Union cells with a face neighbour outside the
+    union are Dirichlet, the other union cells Active, everything else exterior
+    (flag 0), so SPGrid pages away from the spheres hold nothing.  Right-hand
+    side U[0, 1] on the Active cells minus its mean there.  Subdomains 32^3,
+    vlevels 5, mixed precision.  The workload asks for 5 sigma levels, but a
+    32^3 subdomain's adaptive interface hierarchy has 4, and the reference
+    refuses more (INTERFACE_MATRIX_GENERATOR.h:143), so sigma_levels is 4.
+    ``scale`` = 2, 4, ... divides the box and the radii (same seeds) for
+    smaller runs of the same shape."""
+    n = 1024 // scale
+    size = (n + 1,) * 3
+    rng = np.random.Generator(np.random.Philox(5))
+    union = np.zeros(size, bool)
+    for _ in range(64):
+        c = rng.uniform(0, n, 3)
+        r = rng.uniform(40, 120) / scale
+        lo = np.maximum(np.floor(c - r).astype(int), 0)
+        hi = np.minimum(np.ceil(c + r).astype(int) + 1, n + 1)
+        i, j, k = np.ogrid[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]]
+        union[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] |= (i - c[0]) ** 2 + (j - c[1]) ** 2 + (k - c[2]) ** 2 <= r * r
+    interior = union.copy()
+    for axis in range(3):
+        for step in (-1, 1):
+            interior &= _neighbour(union, axis, step)
+    flags = _finish(interior, union & ~interior)
+    act = (flags & ACTIVE) != 0
+    vals = rng.uniform(0, 1, int(act.sum()))
+    rhs = np.zeros(size, np.float32)
+    rhs[act] = (vals - vals.mean()).astype(np.float32)
+    tag = f"c5_{n}box_sparse_sub32" if scale > 1 else "c5_1024box_sparse_sub32"
+    return Domain(size, flags, rhs, (32, 32, 32), tag,
+                  dict(vlevels=5, nVcycles=1, interior_smoothing=3, boundary_smoothing=3, sigma_levels=4,
+                       sigma_smoothing=3, sigma_mg=1, precision_mode=1, true_residual_every=20))
+
+
 def profile_case() -> Domain:
     """128^3 cells (size 129), centred Dirichlet sphere r=24, 32^3 subdomains:
     the 256^3 workload's kernels (sub 32, vlevels 4, smoothing 4/4) on an eighth

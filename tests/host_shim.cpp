@@ -1,6 +1,7 @@
 // Test shim: the product's host-side setup code (layout, interface assembly,
 // supernodal Cholesky) compiled without CUDA device code, so the CPU test suite
 // can check it against the oracle.  Built by tests/test_cpu_host.py with g++.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -58,6 +59,50 @@ void* shim_build(const int size[3], const int sub[3], int vlevels, int sigma_lev
 }
 
 void shim_free(void* h) { delete static_cast<Shim*>(h); }
+
+// Factors a matrix of ncomp disconnected path graphs of csize vertices each
+// (diagonal 2.5, off-diagonal -1, interleaved so that every component's
+// vertices are spread through the numbering) and returns the relative
+// residual of one solve; -1 on an exception.  Interface systems of sparse
+// domains fall apart into many such pieces.
+double shim_factor_components(int ncomp, int csize) {
+    try {
+        const int n = ncomp * csize;
+        CsrF A;
+        A.rows = A.cols = n;
+        A.ptr.assign(1, 0);
+        auto id = [&](int c, int k) { return k * ncomp + c; };  // component c, position k
+        std::vector<int> comp_of(n), pos_of(n);
+        for (int c = 0; c < ncomp; ++c)
+            for (int k = 0; k < csize; ++k) { comp_of[id(c, k)] = c; pos_of[id(c, k)] = k; }
+        for (int r = 0; r < n; ++r) {
+            const int c = comp_of[r], k = pos_of[r];
+            std::vector<std::pair<int, float>> e = {{r, 2.5f}};
+            if (k > 0) e.push_back({id(c, k - 1), -1.0f});
+            if (k + 1 < csize) e.push_back({id(c, k + 1), -1.0f});
+            std::sort(e.begin(), e.end());
+            for (auto& t : e) { A.col.push_back(t.first); A.val.push_back(t.second); }
+            A.ptr.push_back((int)A.col.size());
+        }
+        SnFactor F;
+        F.analyze(A, nullptr);
+        F.factor(A, 1e-5);
+        std::vector<double> b(n), x(n);
+        for (int i = 0; i < n; ++i) b[i] = std::sin(0.37 * i);
+        x = b;
+        F.solve(x.data());
+        double rn = 0, bn = 0;
+        for (int r = 0; r < n; ++r) {
+            double ax = 1e-5 * x[r];
+            for (int p = A.ptr[r]; p < A.ptr[r + 1]; ++p) ax += (double)A.val[p] * x[A.col[p]];
+            rn += (ax - b[r]) * (ax - b[r]);
+            bn += b[r] * b[r];
+        }
+        return std::sqrt(rn / bn);
+    } catch (const std::exception&) {
+        return -1.0;
+    }
+}
 
 // SPGrid page scatter / gather (hdd_set_domain_pages); 0 or the hdd_status.
 int shim_pages_to_dense(const int size[3], long long n, const int32_t* origin, const uint32_t* flags,

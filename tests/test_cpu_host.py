@@ -58,6 +58,8 @@ def shim():
     L.shim_pages_to_dense.argtypes = [ip, C.c_longlong, ip, C.POINTER(C.c_uint32), C.POINTER(C.c_float),
                                       C.POINTER(C.c_uint32), C.POINTER(C.c_float), cp, C.c_int]
     L.shim_dense_to_pages.argtypes = [ip, C.c_longlong, ip, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    L.shim_factor_components.restype = C.c_double
+    L.shim_factor_components.argtypes = [C.c_int, C.c_int]
     L.shim_factor_check.restype = C.c_double
     L.shim_factor_check.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
     return L
@@ -125,6 +127,14 @@ def test_supernodal_factorisation_solves(shim):
                 assert res < 1e-10 and diff.value < 1e-10, ("Aii", l, sd, res, diff.value)
     finally:
         shim.shim_free(h)
+
+
+@pytest.mark.parametrize("ncomp,csize", [(300000, 3), (2000, 40), (37, 33)])
+def test_factorisation_of_many_disconnected_pieces(shim, ncomp, csize):
+    """The interface system of a sparse domain falls apart into many pieces; the
+    ordering visits them in one pass (300000 pieces once overflowed the stack
+    by recursing once per piece)."""
+    assert 0 <= shim.shim_factor_components(ncomp, csize) < 1e-12
 
 
 def test_domain_without_active_cells_is_rejected(shim):
