@@ -107,15 +107,44 @@ static void nd_order(int n, const std::vector<int>& adjp, const std::vector<int>
         int far = bfs(verts[0], pid, comp);
         for (int v : comp) level[v] = -1;
         if (comp.size() < verts.size()) {
-            // Disconnected: split into the reached component and the rest.
-            int pa = next_part++, pb = next_part++;
-            for (int v : verts) part[v] = pb;
-            for (int v : comp) part[v] = pa;
-            std::vector<int> rest;
-            for (int v : verts)
-                if (part[v] == pb) rest.push_back(v);
-            rec(comp, pa);
-            rec(rest, pb);
+            // Disconnected: the components one after another, as peeling off
+            // the reached component and recursing on the rest would order
+            // them, but found in one pass (linear time, no recursion per
+            // component): component i in BFS order from its first vertex,
+            // the remaining components as one block once they hold at most 48
+            // vertices, the last component from its vertices in verts order.
+            std::vector<std::vector<int>> comps;
+            std::vector<int> ids;
+            ids.push_back(next_part++);
+            for (int v : comp) part[v] = ids.back();
+            comps.push_back(std::move(comp));
+            for (int v : verts) {
+                if (part[v] != pid) continue;
+                std::vector<int> c;
+                bfs(v, pid, c);
+                for (int w : c) level[w] = -1;
+                ids.push_back(next_part++);
+                for (int w : c) part[w] = ids.back();
+                comps.push_back(std::move(c));
+            }
+            size_t remaining = verts.size();
+            for (size_t i = 0; i < comps.size(); ++i) {
+                if (i > 0 && remaining <= 48) {
+                    starts.push_back((int)order.size());
+                    for (int v : verts)
+                        if (part[v] >= ids[i] && part[v] <= ids.back()) order.push_back(v);
+                    return;
+                }
+                if (i > 0 && i + 1 == comps.size()) {
+                    std::vector<int> last;
+                    for (int v : verts)
+                        if (part[v] == ids[i]) last.push_back(v);
+                    rec(last, ids[i]);
+                } else {
+                    rec(comps[i], ids[i]);
+                }
+                remaining -= comps[i].size();
+            }
             return;
         }
         comp.clear();
