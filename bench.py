@@ -5,7 +5,8 @@ One step = one Poisson solve (PCG to 1e-6 relative residual, preconditioner
 already initialised) of the workload's domain.  The default workload is the
 256^3-cell domain with a Dirichlet sphere and 32^3 subdomains (sub_size 32,
 vlevels 4, interior/boundary smoothing 4, sigma_levels 4, sigma_mg 1);
-``--config c1`` selects the 64^3-cell, 16^3-subdomain case.
+``--config c1`` selects the 64^3-cell, 16^3-subdomain case; ``c5`` the sparse
+1024^3-cell sphere union (``c5_half`` the same shape at 512^3).
 
 ``--impl reference`` times the CPU restatement of the reference dd_pcg path
 (the oracle) on the host cores instead.
@@ -38,7 +39,7 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--config", choices=["c1", "c2", "c3", "p128", "c4"], default="c2",
+    p.add_argument("--config", choices=["c1", "c2", "c3", "p128", "c4", "c5", "c5_half"], default="c2",
                    help="c4 = serving: resident uneven domains, solve requests through hdd_server_*")
     p.add_argument("--domains", type=int, default=4, help="c4: resident domains")
     p.add_argument("--requests", type=int, default=32, help="c4: requests per timed run")

@@ -305,4 +305,5 @@ def to_pages(flags: np.ndarray, *fields: np.ndarray):
     return (origin, fb[keep]) + tuple(blocks(f)[keep] for f in fields)
 
 
-CONFIGS = {"c1": config1, "c2": config2, "c3": config3, "p128": profile_case}
+CONFIGS = {"c1": config1, "c2": config2, "c3": config3, "p128": profile_case, "c5": config5,
+           "c5_half": lambda: config5(2)}
