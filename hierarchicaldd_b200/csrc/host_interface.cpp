@@ -215,6 +215,22 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
     const int levels = adaptive_stride(lo, hi, qtop);
     if (M > levels) throw Error(HDD_ERR_INVALID_ARGUMENT, "sigma_levels exceeds the adaptive levels of a subdomain");
     W.levels = levels;
+    // A box without Active or Interface cells has no interface and no interior
+    // DOFs at any level (no cell is activated below), so its matrices are
+    // empty; sparse domains have many such boxes.
+    bool solvable = false;
+    for (uint32_t f : W.sub_flags)
+        if (f & (F_ACTIVE | F_INTERFACE)) { solvable = true; break; }
+    if (!solvable) {
+        W.iface_nodes.assign(M, {});
+        W.arr_terms.assign(M, {});
+        W.air_terms.assign(M, {});
+        W.aii.assign(M, CsrF());
+        for (CsrF& A : W.aii) A.ptr.assign(1, 0);
+        W.n_int.assign(M, 0);
+        W.int_xyz.assign(M, {});
+        return;
+    }
     std::vector<Stride> q(levels + 1);
     for (int L = 1; L <= levels; ++L) {
         I3 l2, h2;
