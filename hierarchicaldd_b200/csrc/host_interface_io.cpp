@@ -110,7 +110,8 @@ void read_market(const std::string& path, CsrF& A) {
         throw Error(HDD_ERR_IO, path + ": bad size line");
     struct T { int r, c; float v; };
     std::vector<T> t;
-    t.reserve((size_t)nnz * (symmetric ? 2 : 1));
+    // The size line is not trusted for the allocation: a short file fails below.
+    t.reserve((size_t)std::min<long long>(nnz, 1ll << 22) * (symmetric ? 2 : 1));
     for (long long k = 0; k < nnz; ++k) {
         if (!std::getline(in, line)) throw Error(HDD_ERR_IO, path + ": fewer entries than its size line says");
         char* p = const_cast<char*>(line.c_str());
