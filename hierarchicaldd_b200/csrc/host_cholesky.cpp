@@ -9,6 +9,7 @@
 // leaf block) is one dense front, so the factor is a tree of dense blocks that
 // the GPU solves level by level.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <functional>
 #include <numeric>
@@ -104,38 +105,62 @@ void SnFactor::analyze(const CsrF& A, const std::vector<std::array<int, 3>>* xyz
     perm.clear();
     perm.reserve(n);
     col0.clear(); ncol.clear(); parent.clear(); rows.clear();
-    std::vector<int> part(n, 0), level(n, -1), queue(n);
-    int next_part = 1;
+    // The recursion splits a vertex set into parts ordered first and a
+    // separator ordered after them.  Each call returns the supernodes of its
+    // set in post-order (its own list, so large parts run as OpenMP tasks);
+    // the caller appends the lists in the order the serial recursion creates
+    // them (first part, second part, separator), so the ordering is the same
+    // for any number of threads.  part[] marks which set a vertex belongs to
+    // (ids are unique; a task only writes the ids of its own vertices, and it
+    // only compares a neighbour's id with its own, so it reads them relaxed);
+    // level[] is only touched for vertices of the caller's own set.
+    struct Node { std::vector<int> cols, kids; };
+    struct Sub { std::vector<Node> nodes; std::vector<int> roots; };
+    auto append = [](Sub& to, Sub&& from) {
+        const int off = (int)to.nodes.size();
+        for (Node& nd : from.nodes) {
+            for (int& k : nd.kids) k += off;
+            to.nodes.push_back(std::move(nd));
+        }
+        for (int r : from.roots) to.roots.push_back(r + off);
+    };
+    auto leaf = [](std::vector<int> cols) {
+        Sub s;
+        s.nodes.push_back({std::move(cols), {}});
+        s.roots.push_back(0);
+        return s;
+    };
+    // Separator node over the roots of `s` (appended last).
+    auto close = [](Sub& s, std::vector<int> cols) {
+        Node nd{std::move(cols), s.roots};
+        s.nodes.push_back(std::move(nd));
+        s.roots.assign(1, (int)s.nodes.size() - 1);
+    };
+    std::vector<int> part(n, 0), level(n, -1);
+    std::atomic<int> next_part{1};
+    auto get_part = [&](int v) { return __atomic_load_n(&part[v], __ATOMIC_RELAXED); };
+    auto set_part = [&](int v, int id) { __atomic_store_n(&part[v], id, __ATOMIC_RELAXED); };
     auto bfs = [&](int src, int pid, std::vector<int>& seen) {
-        int qh = 0, qt = 0, last = src;
-        queue[qt++] = src;
+        // seen doubles as the queue: vertices are appended in visiting order.
+        size_t qh = seen.size();
+        int last = src;
         level[src] = 0;
         seen.push_back(src);
-        while (qh < qt) {
-            const int v = queue[qh++];
+        while (qh < seen.size()) {
+            const int v = seen[qh++];
             last = v;
             for (int p = adjp[v]; p < adjp[v + 1]; ++p) {
                 const int w = adj[p];
-                if (part[w] != pid || level[w] >= 0) continue;
+                if (get_part(w) != pid || level[w] >= 0) continue;
                 level[w] = level[v] + 1;
-                queue[qt++] = w;
                 seen.push_back(w);
             }
         }
         return last;
     };
-    auto make_node = [&](const std::vector<int>& cols, const std::vector<int>& children) {
-        const int id = (int)col0.size();
-        col0.push_back((int)perm.size());
-        ncol.push_back((int)cols.size());
-        parent.push_back(-1);
-        for (int c : children) parent[c] = id;
-        perm.insert(perm.end(), cols.begin(), cols.end());
-        return id;
-    };
-    // Returns the roots of the supernode forest covering `verts`.
-    std::function<std::vector<int>(std::vector<int>&, int)> rec = [&](std::vector<int>& verts, int pid) {
-        if ((int)verts.size() <= kLeaf) return std::vector<int>{make_node(verts, {})};
+    constexpr size_t kTaskMin = 16384;  // parts at least this large run as tasks
+    std::function<Sub(std::vector<int>&, int)> rec = [&](std::vector<int>& verts, int pid) -> Sub {
+        if ((int)verts.size() <= kLeaf) return leaf(verts);
         std::vector<int> comp;
         const int far = bfs(verts[0], pid, comp);
         for (int v : comp) level[v] = -1;
@@ -151,41 +176,62 @@ void SnFactor::analyze(const CsrF& A, const std::vector<std::array<int, 3>>* xyz
             std::vector<std::vector<int>> comps;
             std::vector<int> ids;
             ids.push_back(next_part++);
-            for (int v : comp) part[v] = ids.back();
+            for (int v : comp) set_part(v, ids.back());
             comps.push_back(std::move(comp));
             for (int v : verts) {
-                if (part[v] != pid) continue;
+                if (get_part(v) != pid) continue;
                 std::vector<int> c;
                 bfs(v, pid, c);
                 for (int w : c) level[w] = -1;
                 ids.push_back(next_part++);
-                for (int w : c) part[w] = ids.back();
+                for (int w : c) set_part(w, ids.back());
                 comps.push_back(std::move(c));
             }
-            std::vector<int> roots;
+            Sub out;
             size_t remaining = verts.size();
             for (size_t i = 0; i < comps.size(); ++i) {
                 if (i > 0 && remaining <= (size_t)kLeaf) {
                     std::vector<int> rest;
-                    for (int v : verts)
-                        if (part[v] >= ids[i] && part[v] <= ids.back()) rest.push_back(v);
-                    roots.push_back(make_node(rest, {}));
+                    for (int v : verts) {
+                        const int pv = get_part(v);
+                        if (pv >= ids[i] && pv <= ids.back()) rest.push_back(v);
+                    }
+                    append(out, leaf(std::move(rest)));
                     break;
                 }
-                std::vector<int> r;
                 if (i > 0 && i + 1 == comps.size()) {
                     std::vector<int> last;
                     for (int v : verts)
-                        if (part[v] == ids[i]) last.push_back(v);
-                    r = rec(last, ids[i]);
+                        if (get_part(v) == ids[i]) last.push_back(v);
+                    append(out, rec(last, ids[i]));
                 } else {
-                    r = rec(comps[i], ids[i]);
+                    append(out, rec(comps[i], ids[i]));
                 }
-                roots.insert(roots.end(), r.begin(), r.end());
                 remaining -= comps[i].size();
             }
-            return roots;
+            return out;
         }
+        // Orders the two parts (the first as a task when both are large) and
+        // closes them with the separator.
+        auto split = [&](std::vector<int>& Av, std::vector<int>& Sv, std::vector<int>& Bv) -> Sub {
+            const int pa = next_part++, pb = next_part++;
+            for (int v : Av) set_part(v, pa);
+            for (int v : Bv) set_part(v, pb);
+            for (int v : Sv) set_part(v, -1);
+            Sub ra, rb;
+            if (Av.size() >= kTaskMin && Bv.size() >= kTaskMin && omp_in_parallel()) {
+#pragma omp task shared(ra, Av)
+                ra = rec(Av, pa);
+                rb = rec(Bv, pb);
+#pragma omp taskwait
+            } else {
+                ra = rec(Av, pa);
+                rb = rec(Bv, pb);
+            }
+            append(ra, std::move(rb));
+            close(ra, std::move(Sv));
+            return ra;
+        };
         if (xyz) {
             // Geometric split: for each axis, cut at the median position; the
             // separator is the smaller of the two one-sided boundary layers.
@@ -213,7 +259,7 @@ void SnFactor::analyze(const CsrF& A, const std::vector<std::array<int, 3>>* xyz
                     const bool left = (*xyz)[v][ax] < cut;
                     for (int p = adjp[v]; p < adjp[v + 1]; ++p) {
                         const int w = adj[p];
-                        if (part[w] != pid) continue;
+                        if (get_part(w) != pid) continue;
                         if (((*xyz)[w][ax] < cut) != left) {
                             (left ? sl : sr)++;
                             break;
@@ -238,21 +284,13 @@ void SnFactor::analyze(const CsrF& A, const std::vector<std::array<int, 3>>* xyz
                     if (on_sep_side)
                         for (int p = adjp[v]; p < adjp[v + 1] && !boundary; ++p) {
                             const int w = adj[p];
-                            if (part[w] == pid && ((*xyz)[w][best_axis] < best_cut) != left) boundary = true;
+                            if (get_part(w) == pid && ((*xyz)[w][best_axis] < best_cut) != left) boundary = true;
                         }
                     if (boundary) Sv.push_back(v);
                     else if (left) Av.push_back(v);
                     else Bv.push_back(v);
                 }
-                if (!Av.empty() && !Bv.empty()) {
-                    const int pa = next_part++, pb = next_part++;
-                    for (int v : Av) part[v] = pa;
-                    for (int v : Bv) part[v] = pb;
-                    for (int v : Sv) part[v] = -1;
-                    std::vector<int> children = rec(Av, pa), rb = rec(Bv, pb);
-                    children.insert(children.end(), rb.begin(), rb.end());
-                    return std::vector<int>{make_node(Sv, children)};
-                }
+                if (!Av.empty() && !Bv.empty()) return split(Av, Sv, Bv);
             }
         }
         comp.clear();
@@ -261,7 +299,7 @@ void SnFactor::analyze(const CsrF& A, const std::vector<std::array<int, 3>>* xyz
         for (int v : comp) h = std::max(h, level[v]);
         if (h < 2) {
             for (int v : comp) level[v] = -1;
-            return std::vector<int>{make_node(verts, {})};
+            return leaf(verts);
         }
         std::vector<int> cnt(h + 1, 0);
         for (int v : comp) cnt[level[v]]++;
@@ -287,17 +325,24 @@ void SnFactor::analyze(const CsrF& A, const std::vector<std::array<int, 3>>* xyz
             else Bv.push_back(v);
             level[v] = -1;
         }
-        const int pa = next_part++, pb = next_part++;
-        for (int v : Av) part[v] = pa;
-        for (int v : Bv) part[v] = pb;
-        for (int v : Sv) part[v] = -1;
-        std::vector<int> children = rec(Av, pa), rb = rec(Bv, pb);
-        children.insert(children.end(), rb.begin(), rb.end());
-        return std::vector<int>{make_node(Sv, children)};
+        return split(Av, Sv, Bv);
     };
     std::vector<int> all(n);
     std::iota(all.begin(), all.end(), 0);
-    if (n > 0) rec(all, 0);
+    Sub top;
+    if (n > 0) {
+#pragma omp parallel if (n >= (int)(4 * kTaskMin) && !omp_in_parallel())
+#pragma omp single
+        top = rec(all, 0);
+    }
+    for (size_t k = 0; k < top.nodes.size(); ++k) {
+        col0.push_back((int)perm.size());
+        ncol.push_back((int)top.nodes[k].cols.size());
+        parent.push_back(-1);
+        perm.insert(perm.end(), top.nodes[k].cols.begin(), top.nodes[k].cols.end());
+    }
+    for (size_t k = 0; k < top.nodes.size(); ++k)
+        for (int c : top.nodes[k].kids) parent[c] = (int)k;
 
     // Row structure of every front (symbolic factorisation).
     std::vector<int> iperm(n);
