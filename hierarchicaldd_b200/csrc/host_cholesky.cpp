@@ -371,26 +371,41 @@ void SnFactor::analyze(const CsrF& A, const std::vector<std::array<int, 3>>* xyz
 }
 
 namespace {
-// Column c of Fw = [L^{-1}; -L_RJ L^{-1}] for one front (x: nj + nr entries,
-// zero on entry): forward substitution of e_c through L (nj x nj, col-major),
-// then w = -R x with R = L_RJ (nr x nj, col-major).  Axpy loops only, so the
-// vectorised clones give the same values as the scalar one.
-__attribute__((target_clones("avx2", "default")))
-void solve_block_column(const double* L, const double* R, int nj, int nr, int c, double* x) {
-    x[c] = 1.0;
-    for (int jj = c; jj < nj; ++jj) {
-        const double* Lc = L + (size_t)jj * nj;
-        const double xj = x[jj] / Lc[jj];
-        x[jj] = xj;
-        if (xj == 0.0) continue;
-        for (int i = jj + 1; i < nj; ++i) x[i] -= Lc[i] * xj;
+// Columns c0 .. c0+cn-1 (cn <= kSolveGroup) of Fw = [L^{-1}; -L_RJ L^{-1}] for
+// one front, column c at Fw + c*m with m = nj + nr (cleared here): forward
+// substitution of e_c through L (nj x nj, col-major), then w = -R x with
+// R = L_RJ (nr x nj, col-major).  The columns of a group share every column of
+// L and R they read (a front's L and R are read once per group, not once per
+// column), and each column receives its updates in the order of the
+// one-column algorithm (axpy loops only), so the grouping and the vectorised
+// clones give the same values.
+constexpr int kSolveGroup = 8;
+__attribute__((target_clones("avx512f", "avx2", "default")))
+void solve_block_columns(const double* L, const double* R, int nj, int nr, int c0, int cn, double* Fw, int m) {
+    double* x[kSolveGroup];
+    for (int g = 0; g < cn; ++g) {
+        x[g] = Fw + (size_t)(c0 + g) * m;
+        std::fill(x[g], x[g] + m, 0.0);
+        x[g][c0 + g] = 1.0;
     }
-    double* w = x + nj;
-    for (int a = c; a < nj; ++a) {
-        const double la = x[a];
-        if (la == 0.0) continue;
+    for (int jj = c0; jj < nj; ++jj) {
+        const double* Lc = L + (size_t)jj * nj;
+        for (int g = 0; g < cn && c0 + g <= jj; ++g) {
+            double* xg = x[g];
+            const double xj = xg[jj] / Lc[jj];
+            xg[jj] = xj;
+            if (xj == 0.0) continue;
+            for (int i = jj + 1; i < nj; ++i) xg[i] -= Lc[i] * xj;
+        }
+    }
+    for (int a = c0; a < nj; ++a) {
         const double* Ra = R + (size_t)a * nr;
-        for (int k = 0; k < nr; ++k) w[k] -= Ra[k] * la;
+        for (int g = 0; g < cn && c0 + g <= a; ++g) {
+            const double la = x[g][a];
+            if (la == 0.0) continue;
+            double* w = x[g] + nj;
+            for (int k = 0; k < nr; ++k) w[k] -= Ra[k] * la;
+        }
     }
 }
 }  // namespace
@@ -553,12 +568,16 @@ void SnFactor::build_solve_blocks() {
     Fw.assign(ns, {});
     auto work = [&](int j, bool inner_par) {
         const int nj = ncol[j], nr = (int)rows[j].size(), m = nj + nr;
-        std::vector<double>& F = Fw[j];
-        F.assign((size_t)m * nj, 0.0);
+        BlockVec& F = Fw[j];
+        F.resize((size_t)m * nj);  // every column is cleared and written by solve_block_columns
         const std::vector<double>& L = Ljj[j];
         const std::vector<double>& R = Lrj[j];
-#pragma omp parallel for schedule(dynamic, 4) if (inner_par)
-        for (int c = 0; c < nj; ++c) solve_block_column(L.data(), R.data(), nj, nr, c, &F[(size_t)c * m]);
+        const int ngroups = (nj + kSolveGroup - 1) / kSolveGroup;
+#pragma omp parallel for schedule(dynamic, 1) if (inner_par)
+        for (int gi = 0; gi < ngroups; ++gi) {
+            const int c0 = gi * kSolveGroup;
+            solve_block_columns(L.data(), R.data(), nj, nr, c0, std::min(kSolveGroup, nj - c0), F.data(), m);
+        }
     };
     std::vector<int> small;
     for (int j = 0; j < ns; ++j)

@@ -8,6 +8,9 @@
 #include <cstdint>
 #include <string>
 #include <vector>
+#include <utility>
+#include <type_traits>
+#include <memory>
 
 #include "hdd_common.h"
 
@@ -50,6 +53,27 @@ void write_interface_dir(const InterfaceHost& ih, const std::string& dir);
 void read_interface_dir(const std::string& dir, InterfaceHost& ih);
 void check_interface(const DomainLayout& L, int sigma_levels, const InterfaceHost& ih);
 
+// Allocator whose resize leaves new elements uninitialised, for blocks that are
+// written in full right after (by several threads, instead of one thread
+// zeroing them first).
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind { using other = NoInitAlloc<U>; };
+    NoInitAlloc() = default;
+    template <class U>
+    NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... Args>
+    void construct(U* p, Args&&... args) {
+        ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+    }
+};
+using BlockVec = std::vector<double, NoInitAlloc<double>>;
+
 // Supernodal Cholesky of (A + eps I) (zero rows get eps), the stand-in for
 // the reference's MKL PARDISO phases 11/22 (SIGMA_SMOOTHER.cpp:241-414).
 // Supernodes are the fronts of a nested-dissection separator tree.
@@ -59,7 +83,7 @@ struct SnFactor {
     std::vector<int> col0, ncol, parent;       // per supernode, post-order
     std::vector<std::vector<int>> rows;        // below-diagonal rows (new indices), sorted
     std::vector<std::vector<double>> Ljj, Lrj; // col-major dense blocks
-    std::vector<std::vector<double>> Fw;       // [Linv; -L_RJ Linv], (nj+nr) x nj col-major
+    std::vector<BlockVec> Fw;                  // [Linv; -L_RJ Linv], (nj+nr) x nj col-major
     // Nested-dissection ordering and symbolic factorisation.  With DOF
     // positions the separators are planes cut at the median along the axis
     // that gives the smallest separator; without them, breadth-first level sets.

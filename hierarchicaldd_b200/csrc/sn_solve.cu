@@ -536,7 +536,7 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
 #pragma omp parallel for schedule(dynamic)
     for (int g = 0; g < nsn; ++g) {
         const SnFactor& F = *factors[where[g].first];
-        const std::vector<double>& W = F.Fw[where[g].second];  // m x nj, col-major
+        const BlockVec& W = F.Fw[where[g].second];  // m x nj, col-major
         const int nj = ncol[g], m = nj + nrow[g], ld = (m + 3) & ~3;
         float* dst = &fw[(size_t)fw_off[g]];
         for (int c = 0; c < nj; ++c)

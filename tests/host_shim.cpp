@@ -252,7 +252,7 @@ double shim_factor_check(void* h, int kind, int level, int sub, double* blocks_d
         for (int k = 0; k < nr; ++k) pos[F.rows[j][k]] = nj + k;
         for (int c : kids[j])
             for (size_t k = 0; k < F.rows[c].size(); ++k) v[pos[F.rows[c][k]]] += upd[c][k];
-        const std::vector<double>& W = F.Fw[j];
+        const BlockVec& W = F.Fw[j];
         for (int r = 0; r < mm; ++r) {
             double acc = 0;
             for (int c = 0; c < nj; ++c) acc += W[(size_t)c * mm + r] * v[c];
@@ -262,7 +262,7 @@ double shim_factor_check(void* h, int kind, int level, int sub, double* blocks_d
     }
     for (int j = ns - 1; j >= 0; --j) {
         const int nj = F.ncol[j], nr = (int)F.rows[j].size(), mm = nj + nr;
-        const std::vector<double>& W = F.Fw[j];
+        const BlockVec& W = F.Fw[j];
         for (int a = 0; a < nj; ++a) {
             double acc = 0;
             for (int r = 0; r < mm; ++r) {
