@@ -434,9 +434,15 @@ void SnFactor::factor(const CsrF& A, double eps) {
     // runs it or on `inner_par`, so the factor is the same for any schedule.
     auto factor_front = [&](int j, FrontScratch& scratch, bool inner_par) {
         const int nj = ncol[j], nr = (int)rows[j].size(), f = nj + nr;
+        // Large fronts (the separators near the root) split their clearing,
+        // assembly, panel rows and copies over the threads too; every value is
+        // computed by the same operations in the same order either way.
+        const bool big = inner_par && (size_t)f * f > ((size_t)1 << 20);
         std::vector<int>& pos = scratch.pos;
-        std::vector<double>& F = scratch.front;
-        F.assign((size_t)f * f, 0.0);  // col-major, lower triangle used
+        std::vector<double>& F = scratch.front;  // col-major, lower triangle used
+        if (F.size() < (size_t)f * f) F.resize((size_t)f * f);
+#pragma omp parallel for schedule(dynamic, 64) if (big)
+        for (int a = 0; a < f; ++a) std::fill(F.begin() + (size_t)a * f + a, F.begin() + (size_t)(a + 1) * f, 0.0);
         for (int a = 0; a < nj; ++a) pos[col0[j] + a] = a;
         for (int k = 0; k < nr; ++k) pos[rows[j][k]] = nj + k;
         for (int a = 0; a < nj; ++a) {
@@ -452,6 +458,9 @@ void SnFactor::factor(const CsrF& A, double eps) {
             const std::vector<int>& rc = rows[c];
             const int m = (int)rc.size();
             const std::vector<double>& U = upd[c];
+            // Column b of the child's update goes to front column pos[rc[b]]:
+            // distinct columns, so the columns of one child run in parallel.
+#pragma omp parallel for schedule(dynamic, 16) if (big)
             for (int b = 0; b < m; ++b) {
                 const int pb = pos[rc[b]];
                 for (int a = b; a < m; ++a) {
@@ -465,28 +474,46 @@ void SnFactor::factor(const CsrF& A, double eps) {
             upd[c].shrink_to_fit();
         }
         // Dense partial Cholesky of the front (first nj columns), blocked in
-        // panels of kPanel columns: factor the panel, then update the trailing
-        // columns (trailing_update).
+        // panels of kPanel columns: factor the panel's diagonal block, then
+        // the panel rows below it (each row on its own), then update the
+        // trailing columns (trailing_update).
         constexpr int kPanel = 48;
         std::vector<double>& Pk = scratch.panel;
         for (int k0 = 0; k0 < nj; k0 += kPanel) {
             const int kb = std::min(kPanel, nj - k0);
-            for (int k = k0; k < k0 + kb; ++k) {
+            const int t0 = k0 + kb;
+            for (int k = k0; k < t0; ++k) {
                 double d = F[(size_t)k * f + k];
                 if (!(d > 0)) throw Error(HDD_ERR_INTERNAL, "interface matrix is not positive definite");
                 d = std::sqrt(d);
                 F[(size_t)k * f + k] = d;
-                for (int i = k + 1; i < f; ++i) F[(size_t)k * f + i] /= d;
-                for (int c = k + 1; c < k0 + kb; ++c) {
+                for (int i = k + 1; i < t0; ++i) F[(size_t)k * f + i] /= d;
+                for (int c = k + 1; c < t0; ++c) {
                     const double lck = F[(size_t)k * f + c];
                     if (lck == 0.0) continue;
                     double* colc = &F[(size_t)c * f];
                     const double* colk = &F[(size_t)k * f];
-                    for (int i = c; i < f; ++i) colc[i] -= colk[i] * lck;
+                    for (int i = c; i < t0; ++i) colc[i] -= colk[i] * lck;
                 }
             }
-            const int t0 = k0 + kb;
             if (t0 >= f) continue;
+            constexpr int kRows = 256;
+            const int nchunk = (f - t0 + kRows - 1) / kRows;
+#pragma omp parallel for schedule(dynamic, 1) if (big)
+            for (int q = 0; q < nchunk; ++q) {
+                const int r0 = t0 + q * kRows, r1 = std::min(f, r0 + kRows);
+                for (int k = k0; k < t0; ++k) {
+                    const double d = F[(size_t)k * f + k];
+                    double* colk = &F[(size_t)k * f];
+                    for (int i = r0; i < r1; ++i) colk[i] /= d;
+                    for (int c = k + 1; c < t0; ++c) {
+                        const double lck = F[(size_t)k * f + c];
+                        if (lck == 0.0) continue;
+                        double* colc = &F[(size_t)c * f];
+                        for (int i = r0; i < r1; ++i) colc[i] -= colk[i] * lck;
+                    }
+                }
+            }
             pack_panel(F.data(), f, k0, kb, t0, Pk);
             const int nblk = (f - t0 + kColBlock - 1) / kColBlock;
             const double* P = Pk.data();
@@ -495,14 +522,20 @@ void SnFactor::factor(const CsrF& A, double eps) {
         }
         Ljj[j].assign((size_t)nj * nj, 0.0);
         Lrj[j].assign((size_t)nr * nj, 0.0);
-        for (int a = 0; a < nj; ++a) {
-            for (int i = a; i < nj; ++i) Ljj[j][(size_t)a * nj + i] = F[(size_t)a * f + i];
-            for (int k = 0; k < nr; ++k) Lrj[j][(size_t)a * nr + k] = F[(size_t)a * f + nj + k];
-        }
-        if (nr > 0) {
-            upd[j].assign((size_t)nr * nr, 0.0);
+        if (nr > 0) upd[j].assign((size_t)nr * nr, 0.0);
+        std::vector<double>& Lj = Ljj[j];
+        std::vector<double>& Rj = Lrj[j];
+        std::vector<double>& Uj = upd[j];
+#pragma omp parallel if (big)
+        {
+#pragma omp for schedule(dynamic, 16) nowait
+            for (int a = 0; a < nj; ++a) {
+                for (int i = a; i < nj; ++i) Lj[(size_t)a * nj + i] = F[(size_t)a * f + i];
+                for (int k = 0; k < nr; ++k) Rj[(size_t)a * nr + k] = F[(size_t)a * f + nj + k];
+            }
+#pragma omp for schedule(dynamic, 16)
             for (int b = 0; b < nr; ++b)
-                for (int a = b; a < nr; ++a) upd[j][(size_t)b * nr + a] = F[(size_t)(nj + b) * f + nj + a];
+                for (int a = b; a < nr; ++a) Uj[(size_t)b * nr + a] = F[(size_t)(nj + b) * f + nj + a];
         }
         for (int a = 0; a < nj; ++a) pos[col0[j] + a] = -1;
         for (int k = 0; k < nr; ++k) pos[rows[j][k]] = -1;
