@@ -7,7 +7,8 @@
 * without a GPU, creating a solver fails loudly with HDD_ERR_CUDA: there is no
   CPU fallback;
 * the synthetic domain generator follows its rules (Dirichlet outer layer and
-  spheres, orphan Dirichlet cells dropped, face bits on Active cells).
+  spheres, orphan Dirichlet cells dropped, face bits on Active cells), and so
+  does the sparse sphere-union generator.
 """
 import ctypes as C
 import os
@@ -115,3 +116,24 @@ def test_config_shapes():
     assert d1.rhs[16, 16, 16] == 1.0 and np.count_nonzero(d1.rhs) == 1
     assert not (d1.flags[32, 32, 32] & ACTIVE) and (d1.flags[32, 32, 32 + 13] & ACTIVE)
     assert FACE_MX == 0x100000
+
+
+def test_sparse_sphere_union_rules():
+    """The sparse workload's generator (at 1/8 scale): Active cells are the union
+    cells whose six neighbours are all in the union, the union's edge is
+    Dirichlet, the rest exterior; so no exterior cell touches an Active cell (the
+    subdomain V-cycles need that), about a tenth of the box is Active, and the
+    right-hand side has zero mean on the Active cells."""
+    d = domains.config5(8)
+    f = d.flags
+    act = (f & ACTIVE) != 0
+    dirichlet = (f & DIRICHLET) != 0
+    ext = f == 0
+    assert not np.any(act & dirichlet)
+    pad = np.pad(ext, 1, constant_values=True)
+    n0, n1, n2 = f.shape
+    for a, b, c in [(-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1)]:
+        assert not np.any(act & pad[1 + a:1 + a + n0, 1 + b:1 + b + n1, 1 + c:1 + c + n2])
+    assert 0.05 < act.mean() < 0.15
+    assert np.all(d.rhs[~act] == 0) and abs(float(d.rhs[act].astype(np.float64).mean())) < 1e-6
+    assert d.sub_size == (32, 32, 32) and d.meta["sigma_levels"] == 4 and d.meta["vlevels"] == 5
