@@ -3,6 +3,7 @@
 #include <fstream>
 #include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "noalloc.h"
@@ -111,7 +112,7 @@ hdd_status hdd_set_domain_pages(hdd_solver* s, long long n_pages, const int32_t*
         std::vector<float> b(N, 0.0f);
         hdd::pages_to_dense(v.opts.size, n_pages, page_origin, flags, f.data());
         hdd::pages_to_dense(v.opts.size, n_pages, page_origin, rhs, b.data());
-        v.set_domain(f.data(), b.data());
+        v.set_domain(std::move(f), std::move(b));
     });
 }
 
@@ -181,7 +182,7 @@ hdd_status hdd_load_spgrid_dir(hdd_solver* s, const char* dir) {
                 }
             }
         }
-        v.set_domain(flags.data(), rhs.data());
+        v.set_domain(std::move(flags), std::move(rhs));
     });
 }
 

@@ -88,6 +88,16 @@ void Solver::set_domain(const uint32_t* flags, const float* rhs) {
     solved = false;
 }
 
+void Solver::set_domain(std::vector<uint32_t>&& flags, std::vector<float>&& rhs) {
+    const size_t n = (size_t)opts.size[0] * opts.size[1] * opts.size[2];
+    if (flags.size() != n || rhs.size() != n) throw Error(HDD_ERR_INTERNAL, "dense domain arrays of the wrong size");
+    flags_in = std::move(flags);
+    rhs_dense = std::move(rhs);
+    have_domain = true;
+    initialized = false;
+    solved = false;
+}
+
 TileGeom Solver::geom() const {
     TileGeom g;
     g.sub = L.opt.sub[0];

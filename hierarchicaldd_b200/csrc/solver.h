@@ -144,6 +144,8 @@ struct Solver {
     ~Solver();
 
     void set_domain(const uint32_t* flags, const float* rhs);
+    // Same, taking over dense arrays the caller built (no second copy).
+    void set_domain(std::vector<uint32_t>&& flags, std::vector<float>&& rhs);
     void set_rhs(const float* rhs);
     void initialize();
     void solve(hdd_result* res);
