@@ -306,7 +306,13 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
                 }
     }
 
-    auto interior_cells = [&](int m, int L) {
+    // Interior cells of (m, L) in SPGrid page order.  Their CELL_INTERIOR marks
+    // are final after the activation above (the DOF numbering only adds node
+    // bits), so each list is built once and reused.
+    std::vector<std::vector<std::vector<I3>>> cell_lists(M + 1, std::vector<std::vector<I3>>(levels + 1));
+    std::vector<std::vector<char>> cell_listed(M + 1, std::vector<char>(levels + 1, 0));
+    auto interior_cells = [&](int m, int L) -> const std::vector<I3>& {
+        if (cell_listed[m][L]) return cell_lists[m][L];
         const LevelArrays& A = H[m][L];
         std::vector<std::pair<uint64_t, I3>> cells;
         for (int x = 0; x < A.e[0]; ++x)
@@ -317,8 +323,10 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
                         cells.push_back({page_key(c), c});
                     }
         std::sort(cells.begin(), cells.end(), [](const auto& p, const auto& r) { return p.first < r.first; });
-        std::vector<I3> out(cells.size());
+        std::vector<I3>& out = cell_lists[m][L];
+        out.resize(cells.size());
         for (size_t i = 0; i < cells.size(); ++i) out[i] = cells[i].second;
+        cell_listed[m][L] = 1;
         return out;
     };
 
@@ -329,6 +337,7 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
     W.n_int.assign(M, 0);
     W.int_xyz.assign(M, {});
     std::vector<int> node_count(M + 1, 0);
+    Parents tj_par;  // parents of a T-junction node (reused)
 
     for (int m = 1; m <= M; ++m) {
         // Interface DOFs (lines 249-312), numbered locally in encounter order.
@@ -404,8 +413,9 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
                         }
                     } else {
                         A.flags[pn] |= N_TJUNCTION;
-                        Parents par;
-                        embed(N, par, 1.0f, q[L]);
+                        tj_par.clear();
+                        embed(N, tj_par, 1.0f, q[L]);
+                        const Parents& par = tj_par;
                         for (auto& p : par) {
                             const size_t pp = A.at(p.first);
                             if (!(A.flags[pp] & N_DEGREE)) {
