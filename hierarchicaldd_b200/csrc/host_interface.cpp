@@ -705,6 +705,7 @@ void build_interface(const DomainLayout& L, int M, InterfaceHost& out) {
                         W.sub_flags[lid(x, y, z)] = v;
                     }
             process_box(W, M, P);
+            std::vector<uint32_t>().swap(W.sub_flags);  // not needed by the merge below
         } catch (const std::exception& e) {
             errors[s] = e.what();
         }
