@@ -567,29 +567,45 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
             return true;
         };
         struct Resolved { uint32_t f; int id; float w; bool ok; };
-        std::vector<Resolved> res[8];
+        // Resolved parents of each node of level L, computed once per node
+        // (a node is shared by up to 8 cells): node_first[node] indexes pool.
+        std::vector<Resolved> pool;
+        std::vector<int> node_first, node_n;
+        int rb[8], rn[8];
         Parents par;
-        for (int L = m; L <= levels; ++L)
+        for (int L = m; L <= levels; ++L) {
+            const LevelArrays& AL = H[m][L];
+            node_first.assign(AL.flags.size(), -1);
+            node_n.assign(AL.flags.size(), 0);
+            pool.clear();
             for (const I3& c : interior_cells(m, L)) {
                 const M8& cm = galerkin(c, L);
                 for (int li = 0; li < 8; ++li) {
                     const I3 N = {c[0] - 1 + (li >> 2), c[1] - 1 + ((li >> 1) & 1), c[2] - 1 + (li & 1)};
-                    par.clear();
-                    embed(N, par, 1.0f, q[L]);
-                    res[li].clear();
-                    for (auto& p : par) {
-                        Resolved r;
-                        r.ok = resolve(L, p.first, r.f, r.id);
-                        r.w = p.second;
-                        res[li].push_back(r);
+                    const size_t nidx = AL.at(N);
+                    if (node_first[nidx] < 0) {
+                        par.clear();
+                        embed(N, par, 1.0f, q[L]);
+                        node_first[nidx] = (int)pool.size();
+                        node_n[nidx] = (int)par.size();
+                        for (auto& p : par) {
+                            Resolved r;
+                            r.ok = resolve(L, p.first, r.f, r.id);
+                            r.w = p.second;
+                            pool.push_back(r);
+                        }
                     }
+                    rb[li] = node_first[nidx];
+                    rn[li] = node_n[nidx];
                 }
                 for (int n1 = 0; n1 < 8; ++n1)
                     for (int n2 = 0; n2 < 8; ++n2) {
                         const float e = cm[n1 * 8 + n2];
                         if (e == 0) continue;
-                        for (const Resolved& p1 : res[n1])
-                            for (const Resolved& p2 : res[n2]) {
+                        for (int i1 = 0; i1 < rn[n1]; ++i1)
+                            for (int i2 = 0; i2 < rn[n2]; ++i2) {
+                                const Resolved& p1 = pool[(size_t)rb[n1] + i1];
+                                const Resolved& p2 = pool[(size_t)rb[n2] + i2];
                                 if (!p1.ok || !p2.ok)
                                     throw Error(HDD_ERR_INTERNAL, "interface DOF lookup past the coarsest level");
                                 const uint32_t f1 = p1.f, f2 = p2.f;
@@ -619,6 +635,7 @@ void process_box(BoxWork& W, int M, const std::array<M8, 8>& P) {
                             }
                     }
             }
+        }
         const int ni = node_count[m];
         W.n_int[m - 1] = ni;
         // Aii in CSR with explicit zeros dropped (Convert_To_Eigen, lines 687-705).
