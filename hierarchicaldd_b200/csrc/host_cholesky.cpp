@@ -426,7 +426,7 @@ void SnFactor::factor(const CsrF& A, double eps) {
         if (parent[j] >= 0) kids[parent[j]].push_back(j);
     Ljj.assign(ns, {});
     Lrj.assign(ns, {});
-    std::vector<std::vector<double>> upd(ns);
+    std::vector<BlockVec> upd(ns);
     // One front: assemble A's columns and the children's update matrices (in
     // child order), partial dense Cholesky, keep L_JJ, L_RJ and the update
     // matrix for the parent.  `scratch.pos` is an n-long map (all -1 on entry
@@ -457,7 +457,7 @@ void SnFactor::factor(const CsrF& A, double eps) {
         for (int c : kids[j]) {
             const std::vector<int>& rc = rows[c];
             const int m = (int)rc.size();
-            const std::vector<double>& U = upd[c];
+            const BlockVec& U = upd[c];
             // Column b of the child's update goes to front column pos[rc[b]]:
             // distinct columns, so the columns of one child run in parallel.
 #pragma omp parallel for schedule(dynamic, 16) if (big)
@@ -520,12 +520,14 @@ void SnFactor::factor(const CsrF& A, double eps) {
 #pragma omp parallel for schedule(dynamic, 2) if (inner_par && (size_t)(f - t0) * (f - t0) * kb > 4000000)
             for (int cb = 0; cb < nblk; ++cb) trailing_update(F.data(), f, P, kb, t0, t0 + cb * kColBlock);
         }
-        Ljj[j].assign((size_t)nj * nj, 0.0);
-        Lrj[j].assign((size_t)nr * nj, 0.0);
-        if (nr > 0) upd[j].assign((size_t)nr * nr, 0.0);
-        std::vector<double>& Lj = Ljj[j];
-        std::vector<double>& Rj = Lrj[j];
-        std::vector<double>& Uj = upd[j];
+        // Only the parts read later are written: the lower triangle of L_JJ and
+        // of the update matrix, all of L_RJ.
+        Ljj[j].resize((size_t)nj * nj);
+        Lrj[j].resize((size_t)nr * nj);
+        if (nr > 0) upd[j].resize((size_t)nr * nr);
+        BlockVec& Lj = Ljj[j];
+        BlockVec& Rj = Lrj[j];
+        BlockVec& Uj = upd[j];
 #pragma omp parallel if (big)
         {
 #pragma omp for schedule(dynamic, 16) nowait
@@ -603,8 +605,8 @@ void SnFactor::build_solve_blocks() {
         const int nj = ncol[j], nr = (int)rows[j].size(), m = nj + nr;
         BlockVec& F = Fw[j];
         F.resize((size_t)m * nj);  // every column is cleared and written by solve_block_columns
-        const std::vector<double>& L = Ljj[j];
-        const std::vector<double>& R = Lrj[j];
+        const BlockVec& L = Ljj[j];
+        const BlockVec& R = Lrj[j];
         const int ngroups = (nj + kSolveGroup - 1) / kSolveGroup;
 #pragma omp parallel for schedule(dynamic, 1) if (inner_par)
         for (int gi = 0; gi < ngroups; ++gi) {

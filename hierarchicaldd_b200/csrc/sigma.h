@@ -82,7 +82,7 @@ struct SnFactor {
     std::vector<int> perm;                     // new -> old
     std::vector<int> col0, ncol, parent;       // per supernode, post-order
     std::vector<std::vector<int>> rows;        // below-diagonal rows (new indices), sorted
-    std::vector<std::vector<double>> Ljj, Lrj; // col-major dense blocks
+    std::vector<BlockVec> Ljj, Lrj;            // col-major dense blocks (L_JJ: lower triangle only)
     std::vector<BlockVec> Fw;                  // [Linv; -L_RJ Linv], (nj+nr) x nj col-major
     // Nested-dissection ordering and symbolic factorisation.  With DOF
     // positions the separators are planes cut at the median along the axis
