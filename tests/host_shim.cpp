@@ -104,6 +104,43 @@ double shim_factor_components(int ncomp, int csize) {
     }
 }
 
+// FNV-1a digest of everything the GPU plans are built from: the interface
+// matrices of every level and subdomain, and the solve blocks and L_RJ of the
+// level-0 Arr factorisation and of every level-0 Aii factorisation.  Used to
+// check that the host setup gives the same bits for any number of threads.
+unsigned long long shim_setup_digest(void* h) {
+    Shim* s = static_cast<Shim*>(h);
+    unsigned long long d = 1469598103934665603ull;
+    auto mix = [&](const void* p, size_t n) {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        for (size_t i = 0; i < n; ++i) d = (d ^ b[i]) * 1099511628211ull;
+    };
+    auto csr = [&](const CsrF& A) {
+        mix(A.ptr.data(), A.ptr.size() * sizeof(int));
+        mix(A.col.data(), A.col.size() * sizeof(int));
+        mix(A.val.data(), A.val.size() * sizeof(float));
+    };
+    auto factor = [&](const CsrF& A, const std::vector<std::array<int, 3>>* xyz) {
+        if (A.rows == 0) return;
+        SnFactor F;
+        F.analyze(A, xyz);
+        F.factor(A, 1e-5);
+        F.build_solve_blocks();
+        mix(F.perm.data(), F.perm.size() * sizeof(int));
+        for (const auto& v : F.Fw) mix(v.data(), v.size() * sizeof(double));
+        for (const auto& v : F.Lrj) mix(v.data(), v.size() * sizeof(double));
+    };
+    const InterfaceHost& ih = s->ih;
+    for (int l = 0; l < ih.M; ++l) {
+        csr(ih.Arr[l]);
+        if (l < (int)ih.Prr.size()) csr(ih.Prr[l]);
+        for (int sd = 0; sd < ih.n_sub; ++sd) { csr(ih.Aii[l][sd]); csr(ih.Air[l][sd]); }
+    }
+    factor(ih.Arr[0], &ih.iface_xyz[0]);
+    for (int sd = 0; sd < ih.n_sub; ++sd) factor(ih.Aii[0][sd], &ih.aii_xyz[0][sd]);
+    return d;
+}
+
 // SPGrid page scatter / gather (hdd_set_domain_pages); 0 or the hdd_status.
 int shim_pages_to_dense(const int size[3], long long n, const int32_t* origin, const uint32_t* flags,
                         const float* vals, uint32_t* dflags, float* dvals, char* err, int errlen) {

@@ -6,6 +6,7 @@ own into a test shim (tests/host_shim.cpp).
 * the interface dump (the reference's -iomode output layout) reads back
   unchanged, follows the reference's file layout, reads hand-written Matrix
   Market files, and is checked against the domain on reload;
+* the host setup gives the same bits with 1, 3 and 8 threads;
 * SPGrid pages (hdd_set_domain_pages) scatter to and gather from the dense grid
   as the page layout says, and bad page lists are refused;
 * the supernodal factorisation solves (A + 1e-5 I) x = b to FP64 accuracy for
@@ -58,6 +59,8 @@ def shim():
     L.shim_pages_to_dense.argtypes = [ip, C.c_longlong, ip, C.POINTER(C.c_uint32), C.POINTER(C.c_float),
                                       C.POINTER(C.c_uint32), C.POINTER(C.c_float), cp, C.c_int]
     L.shim_dense_to_pages.argtypes = [ip, C.c_longlong, ip, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    L.shim_setup_digest.restype = C.c_ulonglong
+    L.shim_setup_digest.argtypes = [C.c_void_p]
     L.shim_factor_components.restype = C.c_double
     L.shim_factor_components.argtypes = [C.c_int, C.c_int]
     L.shim_factor_check.restype = C.c_double
@@ -380,3 +383,38 @@ def test_bad_page_lists_are_refused(shim, origin, msg):
     assert shim.shim_pages_to_dense(size, len(origin), _i32(origin), _u32(v), _f32(f), _u32(df), _f32(dr),
                                     err, 256) == 1
     assert msg in err.value
+
+
+
+
+def test_setup_bits_do_not_depend_on_thread_count(shim):
+    """Interface assembly, orderings, factorisations and solve blocks are split
+    over OpenMP threads; every value is computed in the same order whatever the
+    thread count, so the digest of all of them is the same for 1, 3 and 8
+    threads (each run in its own process, where OMP_NUM_THREADS takes effect)."""
+    import subprocess
+    import sys
+    code = (
+        "import ctypes as C, sys, numpy as np\n"
+        f"sys.path.insert(0, {os.path.join(ROOT)!r})\n"
+        "from hierarchicaldd_b200 import domains\n"
+        f"L = C.CDLL({SHIM!r})\n"
+        "ip = C.POINTER(C.c_int)\n"
+        "L.shim_build.restype = C.c_void_p\n"
+        "L.shim_build.argtypes = [ip, ip, C.c_int, C.c_int, C.POINTER(C.c_uint32), C.c_char_p, C.c_int]\n"
+        "L.shim_setup_digest.restype = C.c_ulonglong\n"
+        "L.shim_setup_digest.argtypes = [C.c_void_p]\n"
+        "d = domains.small(96, 16, 20, seed=6)\n"
+        "f = np.ascontiguousarray(d.flags, np.uint32)\n"
+        "err = C.create_string_buffer(256)\n"
+        "h = L.shim_build((C.c_int * 3)(*d.size), (C.c_int * 3)(*d.sub_size), 3, 2,"
+        " f.ctypes.data_as(C.POINTER(C.c_uint32)), err, 256)\n"
+        "assert h, err.value\n"
+        "print(L.shim_setup_digest(h))\n")
+    digests = set()
+    for threads in ("1", "3", "8"):
+        env = dict(os.environ, OMP_NUM_THREADS=threads)
+        p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=300)
+        assert p.returncode == 0, p.stderr
+        digests.add(p.stdout.strip())
+    assert len(digests) == 1, digests
