@@ -84,23 +84,52 @@ void trailing_update(double* F, int f, const double* P, int kb, int t0, int c0) 
 
 void SnFactor::analyze(const CsrF& A, const std::vector<std::array<int, 3>>* xyz) {
     n = A.rows;
-    std::vector<std::vector<int>> nb(n);
-    for (int r = 0; r < n; ++r)
-        for (int p = A.ptr[r]; p < A.ptr[r + 1]; ++p) {
-            const int c = A.col[p];
-            if (c == r) continue;
-            nb[r].push_back(c);
-            nb[c].push_back(r);
-        }
+    // Symmetric adjacency without self loops: every off-diagonal entry (r, c)
+    // gives c to r's list and r to c's; each list is then sorted and
+    // deduplicated, so the fill order (parallel, atomic slots) does not matter.
     std::vector<int> adjp(n + 1, 0), adj;
-    for (int r = 0; r < n; ++r) {
-        std::sort(nb[r].begin(), nb[r].end());
-        nb[r].erase(std::unique(nb[r].begin(), nb[r].end()), nb[r].end());
-        adjp[r + 1] = adjp[r] + (int)nb[r].size();
+    {
+        std::vector<int> deg(n, 0);
+#pragma omp parallel for schedule(static)
+        for (int r = 0; r < n; ++r)
+            for (int p = A.ptr[r]; p < A.ptr[r + 1]; ++p) {
+                const int c = A.col[p];
+                if (c == r) continue;
+#pragma omp atomic
+                deg[r]++;
+#pragma omp atomic
+                deg[c]++;
+            }
+        std::vector<long long> start((size_t)n + 1, 0);
+        for (int r = 0; r < n; ++r) start[(size_t)r + 1] = start[r] + deg[r];
+        std::vector<int> raw((size_t)start[n]);
+        std::vector<int> fill(n, 0);
+#pragma omp parallel for schedule(static)
+        for (int r = 0; r < n; ++r)
+            for (int p = A.ptr[r]; p < A.ptr[r + 1]; ++p) {
+                const int c = A.col[p];
+                if (c == r) continue;
+                int kr, kc;
+#pragma omp atomic capture
+                kr = fill[r]++;
+#pragma omp atomic capture
+                kc = fill[c]++;
+                raw[(size_t)start[r] + kr] = c;
+                raw[(size_t)start[c] + kc] = r;
+            }
+#pragma omp parallel for schedule(dynamic, 1024)
+        for (int r = 0; r < n; ++r) {
+            int* b = raw.data() + start[r];
+            int* e = raw.data() + start[(size_t)r + 1];
+            std::sort(b, e);
+            deg[r] = (int)(std::unique(b, e) - b);
+        }
+        for (int r = 0; r < n; ++r) adjp[r + 1] = adjp[r] + deg[r];
+        adj.resize((size_t)adjp[n]);
+#pragma omp parallel for schedule(static)
+        for (int r = 0; r < n; ++r)
+            std::copy(raw.data() + start[r], raw.data() + start[r] + deg[r], adj.data() + adjp[r]);
     }
-    adj.reserve(adjp[n]);
-    for (int r = 0; r < n; ++r) adj.insert(adj.end(), nb[r].begin(), nb[r].end());
-    nb.clear();
 
     perm.clear();
     perm.reserve(n);
