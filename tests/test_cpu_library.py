@@ -137,3 +137,17 @@ def test_sparse_sphere_union_rules():
     assert 0.05 < act.mean() < 0.15
     assert np.all(d.rhs[~act] == 0) and abs(float(d.rhs[act].astype(np.float64).mean())) < 1e-6
     assert d.sub_size == (32, 32, 32) and d.meta["sigma_levels"] == 4 and d.meta["vlevels"] == 5
+
+
+def test_header_is_plain_c():
+    """include/hdd.h is a C ABI: it compiles as C99 (for C, cgo or other FFI
+    callers) as well as C++."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    hdr = os.path.join(ROOT, "include", "hdd.h")
+    p = subprocess.run([gcc, "-fsyntax-only", "-x", "c", "-std=c99", "-Wall", "-Wextra", "-Werror", hdr],
+                       capture_output=True, text=True)
+    assert p.returncode == 0, p.stderr
