@@ -827,37 +827,49 @@ void build_interface(const DomainLayout& L, int M, InterfaceHost& out) {
                 if (!diag) throw Error(HDD_ERR_INTERNAL, "zero diagonal in the level-0 interface matrix");
             }
     }
-    // Interface prolongation Prr[m]: fine level m -> coarse level m+1.  Each
-    // fine DOF contributes its own (row, column) entries, so the DOFs are
-    // visited in parallel; csr_from_pairs sorts the (unique) keys.
+    // Interface prolongation Prr[m]: fine level m -> coarse level m+1.  Row id
+    // holds fine DOF id's (at most 8) coarse parents with positive trilinear
+    // weight, columns ascending: the fine DOFs are visited in parallel, each
+    // filling its own row.
     out.Prr.assign(M > 1 ? M - 1 : 0, CsrF());
     for (int m = 0; m + 1 < M; ++m) {
         const int nf = out.n_iface[m];
-        std::vector<std::pair<uint64_t, float>> pe;
-#pragma omp parallel
-        {
-            std::vector<std::pair<uint64_t, float>> mine;
-#pragma omp for schedule(static)
-            for (int id = 0; id < nf; ++id) {
-                const std::array<int, 3>& X = out.iface_xyz[m][id];
-                const I3 F = {X[0] >> m, X[1] >> m, X[2] >> m};
-                int base[3];
-                for (int v = 0; v < 3; ++v) base[v] = (int)std::floor(F[v] / 2.0);
-                for (int ci = 0; ci < 8; ++ci) {
-                    const I3 C = {base[0] + (ci >> 2), base[1] + ((ci >> 1) & 1), base[2] + (ci & 1)};
-                    float w = 1.0f;
-                    for (int v = 0; v < 3; ++v) w *= (2.0f - std::abs(C[v] * 2 - F[v])) / 2.0;
-                    if (!(w > 0)) continue;
-                    const uint64_t ck = ((uint64_t)C[0] << 42) | ((uint64_t)C[1] << 21) | (uint64_t)C[2];
-                    auto it = gid[m + 1].find(ck);
-                    if (it == gid[m + 1].end()) continue;
-                    mine.push_back({((uint64_t)(uint32_t)id << 32) | (uint32_t)it->second, w});
-                }
+        std::vector<std::array<std::pair<int, float>, 8>> ent(nf);
+        std::vector<int> cnt(nf, 0);
+#pragma omp parallel for schedule(static)
+        for (int id = 0; id < nf; ++id) {
+            const std::array<int, 3>& X = out.iface_xyz[m][id];
+            const I3 F = {X[0] >> m, X[1] >> m, X[2] >> m};
+            int base[3];
+            for (int v = 0; v < 3; ++v) base[v] = (int)std::floor(F[v] / 2.0);
+            int k = 0;
+            for (int ci = 0; ci < 8; ++ci) {
+                const I3 C = {base[0] + (ci >> 2), base[1] + ((ci >> 1) & 1), base[2] + (ci & 1)};
+                float w = 1.0f;
+                for (int v = 0; v < 3; ++v) w *= (2.0f - std::abs(C[v] * 2 - F[v])) / 2.0;
+                if (!(w > 0)) continue;
+                const uint64_t ck = ((uint64_t)C[0] << 42) | ((uint64_t)C[1] << 21) | (uint64_t)C[2];
+                auto it = gid[m + 1].find(ck);
+                if (it == gid[m + 1].end()) continue;
+                ent[id][k++] = {it->second, w};
             }
-#pragma omp critical(hdd_prr_merge)
-            pe.insert(pe.end(), mine.begin(), mine.end());
+            std::sort(ent[id].begin(), ent[id].begin() + k,
+                      [](const auto& x, const auto& y) { return x.first < y.first; });
+            cnt[id] = k;
         }
-        out.Prr[m] = csr_from_pairs(out.n_iface[m], out.n_iface[m + 1], pe);
+        CsrF& P = out.Prr[m];
+        P.rows = nf;
+        P.cols = out.n_iface[m + 1];
+        P.ptr.assign((size_t)nf + 1, 0);
+        for (int id = 0; id < nf; ++id) P.ptr[id + 1] = P.ptr[id] + cnt[id];
+        P.col.resize((size_t)P.ptr[nf]);
+        P.val.resize((size_t)P.ptr[nf]);
+#pragma omp parallel for schedule(static)
+        for (int id = 0; id < nf; ++id)
+            for (int k = 0; k < cnt[id]; ++k) {
+                P.col[(size_t)P.ptr[id] + k] = ent[id][k].first;
+                P.val[(size_t)P.ptr[id] + k] = ent[id][k].second;
+            }
     }
 }
 
