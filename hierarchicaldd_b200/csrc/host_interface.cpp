@@ -15,6 +15,7 @@
 // (subdomain, cell) order, so the assembled matrices follow the reference's
 // numbering and float summation order.
 #include <algorithm>
+#include <parallel/algorithm>
 #include <deque>
 #include <climits>
 #include <cmath>
@@ -741,23 +742,58 @@ void build_interface(const DomainLayout& L, int M, InterfaceHost& out) {
     out.Air.assign(M, std::vector<CsrF>(nsub));
     out.iface_xyz.assign(M, {});
     out.aii_xyz.assign(M, std::vector<std::vector<std::array<int, 3>>>(nsub));
-    std::vector<std::unordered_map<uint64_t, int>> gid(M);
+    // Per level: (node key, global number) of every interface DOF, sorted by key
+    // (the prolongation below looks coarse DOFs up in it).
+    std::vector<std::vector<std::pair<uint64_t, int>>> gkeys(M);
+    auto node_key = [](const I3& nd) {
+        return ((uint64_t)nd[0] << 42) | ((uint64_t)nd[1] << 21) | (uint64_t)nd[2];
+    };
     for (int m = 0; m < M; ++m) {
-        // Global numbers in first-encounter order (serial: the order is the result).
-        std::vector<std::vector<int>> to_g(nsub);
+        // Global numbers in first-encounter order over (subdomain, local
+        // index): the entries sorted by (key, position) give each key's first
+        // encounter, and numbering the first encounters in position order gives
+        // the reference's order.
+        std::vector<long long> off((size_t)nsub + 1, 0);
+        for (int s = 0; s < nsub; ++s) off[(size_t)s + 1] = off[s] + (long long)work[s].iface_nodes[m].size();
+        const long long T = off[nsub];
+        std::vector<std::pair<uint64_t, long long>> ent((size_t)T);
+#pragma omp parallel for schedule(dynamic, 16)
         for (int s = 0; s < nsub; ++s) {
             const std::vector<I3>& nodes = work[s].iface_nodes[m];
-            to_g[s].resize(nodes.size());
+            for (size_t i = 0; i < nodes.size(); ++i) ent[(size_t)off[s] + i] = {node_key(nodes[i]), off[s] + (long long)i};
+        }
+        __gnu_parallel::sort(ent.begin(), ent.end());
+        std::vector<char> first((size_t)T, 0);
+        for (long long k = 0; k < T; ++k)
+            if (k == 0 || ent[k].first != ent[k - 1].first) first[(size_t)ent[k].second] = 1;
+        std::vector<int> number((size_t)T, -1);  // the DOF number at its first encounter
+        int nfirst = 0;
+        for (long long e = 0; e < T; ++e)
+            if (first[(size_t)e]) number[(size_t)e] = nfirst++;
+        out.n_iface[m] = nfirst;
+        std::vector<int> flat((size_t)T);
+        gkeys[m].reserve((size_t)nfirst);
+        for (long long k = 0, cur = -1; k < T; ++k) {
+            if (k == 0 || ent[k].first != ent[k - 1].first) {
+                cur = number[(size_t)ent[k].second];
+                gkeys[m].push_back({ent[k].first, (int)cur});
+            }
+            flat[(size_t)ent[k].second] = (int)cur;
+        }
+        std::vector<std::pair<uint64_t, long long>>().swap(ent);
+        if (m == 0) out.iface_map.resize((size_t)nfirst);
+        out.iface_xyz[m].resize((size_t)nfirst);
+        std::vector<std::vector<int>> to_g(nsub);
+#pragma omp parallel for schedule(dynamic, 16)
+        for (int s = 0; s < nsub; ++s) {
+            const std::vector<I3>& nodes = work[s].iface_nodes[m];
+            to_g[s].assign(flat.begin() + off[s], flat.begin() + off[(size_t)s + 1]);
             for (size_t i = 0; i < nodes.size(); ++i) {
+                const long long e = off[s] + (long long)i;
+                if (!first[(size_t)e]) continue;
                 const I3& nd = nodes[i];
-                const uint64_t key = ((uint64_t)nd[0] << 42) | ((uint64_t)nd[1] << 21) | (uint64_t)nd[2];
-                auto it = gid[m].find(key);
-                if (it == gid[m].end()) {
-                    it = gid[m].emplace(key, out.n_iface[m]++).first;
-                    if (m == 0) out.iface_map.push_back(nd);
-                    out.iface_xyz[m].push_back({nd[0] << m, nd[1] << m, nd[2] << m});
-                }
-                to_g[s][i] = it->second;
+                if (m == 0) out.iface_map[(size_t)number[(size_t)e]] = nd;
+                out.iface_xyz[m][(size_t)number[(size_t)e]] = {nd[0] << m, nd[1] << m, nd[2] << m};
             }
         }
         const int nif = out.n_iface[m];
@@ -849,8 +885,9 @@ void build_interface(const DomainLayout& L, int M, InterfaceHost& out) {
                 for (int v = 0; v < 3; ++v) w *= (2.0f - std::abs(C[v] * 2 - F[v])) / 2.0;
                 if (!(w > 0)) continue;
                 const uint64_t ck = ((uint64_t)C[0] << 42) | ((uint64_t)C[1] << 21) | (uint64_t)C[2];
-                auto it = gid[m + 1].find(ck);
-                if (it == gid[m + 1].end()) continue;
+                const auto& keys = gkeys[m + 1];
+                auto it = std::lower_bound(keys.begin(), keys.end(), std::make_pair(ck, INT_MIN));
+                if (it == keys.end() || it->first != ck) continue;
                 ent[id][k++] = {it->second, w};
             }
             std::sort(ent[id].begin(), ent[id].begin() + k,
