@@ -8,16 +8,16 @@
 //
 // Data structures differ from the reference: every subdomain works on dense
 // box-local arrays per hierarchy level instead of SPGrid allocators and hash
-// tables, Galerkin-coarsened element matrices are memoised per (level, cell),
+// tables, Galerkin-coarsened element matrices are computed once per cell type,
 // and subdomains are processed concurrently.  Global interface DOF numbers are
-// then assigned in a serial pass in the reference's first-encounter order, and
-// interface-interface contributions are summed per key in the reference's
-// (subdomain, cell) order, so the assembled matrices follow the reference's
-// numbering and float summation order.
+// then assigned in the reference's first-encounter order over (subdomain, local
+// index), and interface-interface contributions are summed per key in the
+// reference's (subdomain, cell) order, so the assembled matrices follow the
+// reference's numbering and float summation order.
 #include <algorithm>
-#include <parallel/algorithm>
-#include <deque>
 #include <climits>
+#include <deque>
+#include <parallel/algorithm>
 #include <cmath>
 #include <cstring>
 #include <functional>
