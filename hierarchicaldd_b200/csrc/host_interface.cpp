@@ -16,11 +16,11 @@
 // reference's numbering and float summation order.
 #include <algorithm>
 #include <climits>
-#include <deque>
-#include <parallel/algorithm>
 #include <cmath>
 #include <cstring>
+#include <deque>
 #include <functional>
+#include <parallel/algorithm>
 #include <string>
 #include <unordered_map>
 
