@@ -589,7 +589,7 @@ def main():
         "iterations": its[0] if its else None,
         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
         "true_residual_inf": res[-1]["true_residual_inf"] if res else None,
-        "setup_s": setup_s,
+        "setup_s": setup_s, "setup_host_threads": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
         "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": 4 * cells, "d2h_bytes_per_step": 4 * cells},
         "gpu_launches": int(launches),
         "phase_ms_per_solve": phase_ms, "phase_launches_per_solve": phase_n,
