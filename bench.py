@@ -498,7 +498,11 @@ def main():
                                 m["sigma_mg"], tol=1e-6,
                                 precision_mode=1 if args.precision == "mixed" else 0)
     setup_s = time.time() - t0
-    print(f"[bench] {d.name}: setup {setup_s:.1f} s", file=sys.stderr, flush=True)
+    try:
+        setup_phases = s.Setup_Timing()
+    except Exception as e:  # a diagnostic only
+        setup_phases = {"error": str(e)}
+    print(f"[bench] {d.name}: setup {setup_s:.1f} s {setup_phases}", file=sys.stderr, flush=True)
 
     def barrier():
         if dist is not None:
@@ -589,7 +593,8 @@ def main():
         "iterations": its[0] if its else None,
         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
         "true_residual_inf": res[-1]["true_residual_inf"] if res else None,
-        "setup_s": setup_s, "setup_host_threads": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+        "setup_s": setup_s, "setup_phases_s": setup_phases,
+        "setup_host_threads": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
         "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": 4 * cells, "d2h_bytes_per_step": 4 * cells},
         "gpu_launches": int(launches),
         "phase_ms_per_solve": phase_ms, "phase_launches_per_solve": phase_n,

@@ -80,6 +80,7 @@ SIGNATURES = {
     "hdd_interface_matrix": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _ip, _ip, _ip, _ip, _ip,
                                        C.POINTER(C.c_double)]),
     "hdd_kernel_launch_count": (C.c_int, [_vp, C.POINTER(C.c_longlong)]),
+    "hdd_get_setup_timing": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "hdd_set_kernel_timing": (C.c_int, [_vp, C.c_int]),
     "hdd_get_kernel_timing": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
     "hdd_get_kernel_bytes": (C.c_int, [_vp, C.POINTER(C.c_double)]),

@@ -217,6 +217,14 @@ hdd_status hdd_vcycle_dense(hdd_solver* s, float* u, const float* b, int n_vcycl
     return guard(s, [&](Solver& v) { v.vcycle_dense(u, b, n_vcycles); });
 }
 
+hdd_status hdd_get_setup_timing(hdd_solver* s, double* ms) {
+    if (!ms) return HDD_ERR_INVALID_ARGUMENT;
+    return guard(s, [&](Solver& v) {
+        if (!v.initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+        for (int k = 0; k < 4; ++k) ms[k] = v.setup_phase_ms[k];
+    });
+}
+
 hdd_status hdd_set_iomode(hdd_solver* s, int iomode, const char* directory) {
     return guard(s, [&](Solver& v) {
         if (iomode < HDD_IOMODE_NEITHER || iomode > HDD_IOMODE_INPUT)

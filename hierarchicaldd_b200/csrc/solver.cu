@@ -163,6 +163,11 @@ void Solver::initialize() {
     (void)S;
 
     // Interface system (host assembly + factorisations) and its device solver.
+    auto since_ms = [&](std::chrono::steady_clock::time_point a) {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
+    };
+    setup_phase_ms[0] = since_ms(t0);
+    const auto t_iface = std::chrono::steady_clock::now();
     if (std::getenv("HDD_VERBOSE"))
         std::fprintf(stderr, "[hdd setup] layout %.2f s (%zu tiles, %zu boxes)\n",
                      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(), L.tiles.size(),
@@ -183,11 +188,14 @@ void Solver::initialize() {
                      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
     // Level-0 interface DOFs: cell slots and their Active face neighbours.
     const int n_if = ih.n_iface.empty() ? 0 : ih.n_iface[0];
+    setup_phase_ms[1] = since_ms(t_iface);
+    const auto t_sigma = std::chrono::steady_clock::now();
     // A domain inside one subdomain has no interface: the preconditioner is
     // then the two subdomain V-cycle passes alone, and the coarser interface
     // levels (which only feed level 0) are not built.
     if (n_if > 0) sigma.setup(ih, opts.sigma_smoothing, stream);
     else sigma.release();
+    setup_phase_ms[2] = since_ms(t_sigma);
     std::vector<long long> slot(n_if);
     std::vector<int> nbs(6 * (size_t)n_if, -1);
     const int* n = L.opt.size;
@@ -213,6 +221,7 @@ void Solver::initialize() {
     sync();
     initialized = true;
     setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    setup_phase_ms[3] = setup_ms;
 }
 
 void Solver::set_rhs(const float* rhs) {

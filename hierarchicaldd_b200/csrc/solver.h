@@ -93,6 +93,10 @@ struct Solver {
     int iomode = HDD_IOMODE_NEITHER;  // interface dump / reload at initialize()
     std::string io_dir;
     double setup_ms = 0;
+    // Host wall time of the setup phases: layout and vector uploads, interface
+    // system (assembly or reload, and dump), interface solver (factorisations
+    // and solve plans), total.
+    double setup_phase_ms[4] = {0, 0, 0, 0};
 
     // Optional per-phase device timing with CUDA events on the solver stream
     // (categories: 0 V-cycle kernel, 1 Laplacian kernel, 2 PCG vector kernels,

@@ -202,6 +202,10 @@ int main(int argc, char** argv) {
                                                                                     : HDD_IOMODE_NEITHER;
     if ((st = hdd_set_iomode(h, io, a.out.c_str())) != HDD_OK) return fail("iomode", st);
     if ((st = hdd_initialize_preconditioner(h)) != HDD_OK) return fail("Initialize_Preconditioner", st);
+    double phase_ms[4];
+    if (hdd_get_setup_timing(h, phase_ms) == HDD_OK)
+        std::printf("setup ms: layout %.1f, interface system %.1f, interface solver %.1f, total %.1f\n",
+                    phase_ms[0], phase_ms[1], phase_ms[2], phase_ms[3]);
     hdd_result r;
     st = hdd_solve(h, &r);
     if (st != HDD_OK && st != HDD_ERR_NOT_CONVERGED) return fail("Solve", st);

@@ -137,6 +137,13 @@ class SPGrid_Domain_Decomposition_Solver:
         rhs = np.ascontiguousarray(rhs, np.float32).reshape(origin.shape[0], 256)
         self._check(self.lib.hdd_set_rhs_pages(self.h, origin.shape[0], _ip(origin), _fp(rhs)))
 
+    def Setup_Timing(self) -> dict:
+        """Host wall seconds of the last Initialize_Preconditioner by phase."""
+        ms = (C.c_double * 4)()
+        self._check(self.lib.hdd_get_setup_timing(self.h, ms))
+        return {"layout": ms[0] / 1e3, "interface_system": ms[1] / 1e3, "interface_solver": ms[2] / 1e3,
+                "total": ms[3] / 1e3}
+
     def Solve(self, allow_not_converged: bool = False) -> dict:
         res = hdd_result()
         st = self.lib.hdd_solve(self.h, C.byref(res))

@@ -206,6 +206,13 @@ hdd_status hdd_set_kernel_timing(hdd_solver* s, int enable);
 hdd_status hdd_get_kernel_timing(hdd_solver* s, double* ms, long long* launches);
 hdd_status hdd_get_kernel_bytes(hdd_solver* s, double* bytes);
 
+/* Host wall time (ms) of the last hdd_initialize_preconditioner, by phase:
+ * ms[0] layout and vector uploads, ms[1] interface system (assembly, or reload
+ * and dump under hdd_set_iomode), ms[2] interface solver (factorisations and
+ * solve plans), ms[3] total.  No reference counterpart (the reference logs its
+ * setup scopes with LOG::SCOPE). */
+hdd_status hdd_get_setup_timing(hdd_solver* s, double* ms);
+
 /* Number of our CUDA kernel launches issued since the handle was created. */
 hdd_status hdd_kernel_launch_count(hdd_solver* s, long long* count);
 
