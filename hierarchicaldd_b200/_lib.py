@@ -70,6 +70,7 @@ SIGNATURES = {
     "hdd_set_rhs_dense": (C.c_int, [_vp, _fp]),
     "hdd_solve": (C.c_int, [_vp, C.POINTER(hdd_result)]),
     "hdd_get_solution_dense": (C.c_int, [_vp, _fp]),
+    "hdd_get_residual_history": (C.c_int, [_vp, C.POINTER(C.c_double), C.c_int, _ip]),
     "hdd_apply_preconditioner_dense": (C.c_int, [_vp, _fp, _fp]),
     "hdd_vcycle_dense": (C.c_int, [_vp, _fp, _fp, C.c_int]),
     "hdd_multiply_dense": (C.c_int, [_vp, _fp, _fp]),
@@ -80,6 +81,8 @@ SIGNATURES = {
     "hdd_interface_matrix": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _ip, _ip, _ip, _ip, _ip,
                                        C.POINTER(C.c_double)]),
     "hdd_kernel_launch_count": (C.c_int, [_vp, C.POINTER(C.c_longlong)]),
+    "hdd_set_wait_limit": (C.c_int, [_vp, C.c_longlong]),
+    "hdd_test_stall_dependency": (C.c_int, [_vp, C.c_int]),
     "hdd_get_setup_timing": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "hdd_set_kernel_timing": (C.c_int, [_vp, C.c_int]),
     "hdd_get_kernel_timing": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),

@@ -207,6 +207,15 @@ hdd_status hdd_get_solution_dense(hdd_solver* s, float* x) {
     return guard(s, [&](Solver& v) { v.get_solution(x); });
 }
 
+hdd_status hdd_get_residual_history(hdd_solver* s, double* out, int capacity, int* n) {
+    if (!n || capacity < 0 || (capacity > 0 && !out)) return HDD_ERR_INVALID_ARGUMENT;
+    return guard(s, [&](Solver& v) {
+        if (!v.solved) throw Error(HDD_ERR_NOT_INITIALIZED, "no solve has run");
+        *n = (int)v.history.size();
+        for (int i = 0; i < capacity && i < *n; ++i) out[i] = v.history[i];
+    });
+}
+
 hdd_status hdd_apply_preconditioner_dense(hdd_solver* s, const float* r, float* z) {
     if (!r || !z) return HDD_ERR_INVALID_ARGUMENT;
     return guard(s, [&](Solver& v) { v.apply_preconditioner_dense(r, z); });
@@ -322,6 +331,22 @@ hdd_status hdd_get_kernel_bytes(hdd_solver* s, double* bytes) {
     return guard(s, [&](Solver& v) {
         v.collect_timing();
         for (int c = 0; c < Solver::kCats; ++c) bytes[c] = v.cat_bytes[c];
+    });
+}
+
+hdd_status hdd_set_wait_limit(hdd_solver* s, long long polls) {
+    if (polls < 1) return HDD_ERR_INVALID_ARGUMENT;
+    return guard(s, [&](Solver& v) {
+        if (!v.initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+        v.sigma.set_wait_limit(polls);
+    });
+}
+
+hdd_status hdd_test_stall_dependency(hdd_solver* s, int on) {
+    return guard(s, [&](Solver& v) {
+        if (!v.initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+        hdd::cuda_check(cudaSetDevice(v.opts.device), "cudaSetDevice");
+        v.sigma.stall_dependency(on != 0, v.stream);
     });
 }
 

@@ -141,6 +141,7 @@ void SigmaGpu::release() {
     bottom.release();
     dev::release(kb);
     dev::release(kx);
+    dev::release(d_err);
     device_bytes = 0;
 }
 
@@ -155,6 +156,11 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
     };
     M = ih.M;
     smoothing = smoothing_iterations;
+    {
+        size_t b0 = 0;
+        d_err = dev::alloc_zero<int>(1, b0, s);
+        device_bytes += b0;
+    }
     const double eps = 1e-5;  // SIGMA_SMOOTHER.cpp:176 default epsilon
     lv.resize(M);
     for (int l = 0; l < M; ++l) {
@@ -218,8 +224,8 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
             std::vector<int> offs;
             for (int sd = 0; sd < ih.n_sub; ++sd)
                 if (aii[sd].n > 0) { fs.push_back(&aii[sd]); offs.push_back(off[sd]); }
-            L.aii.build(fs, offs, s);
-            L.arr_solve.build({&arrf}, {0}, s);
+            L.aii.build(fs, offs, s, d_err);
+            L.arr_solve.build({&arrf}, {0}, s, d_err);
             device_bytes += L.aii.bytes + L.arr_solve.bytes;
             stamp("device plans", l);
         } else {
@@ -276,8 +282,8 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
                 std::vector<int> offs;
                 for (int sd = 0; sd < ih.n_sub; ++sd)
                     if (aii[sd].n > 0) { fs.push_back(&aii[sd]); offs.push_back(off[sd]); }
-                L.aii.build(fs, offs, s);
-                L.arr_solve.build({&arrf}, {0}, s);
+                L.aii.build(fs, offs, s, d_err);
+                L.arr_solve.build({&arrf}, {0}, s, d_err);
                 device_bytes += L.aii.bytes + L.arr_solve.bytes;
                 stamp("device plans (coarsest level, literal smoothing)", l);
                 continue;
@@ -320,7 +326,7 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
             kf.analyze(K, have_xyz ? &kxyz : nullptr);
             kf.factor(K, eps);
             kf.build_solve_blocks();
-            bottom.build({&kf}, {0}, s);
+            bottom.build({&kf}, {0}, s, d_err);
             n_bottom = nb;
             n_bottom_int = ni;
             size_t b2 = 0;
@@ -372,9 +378,26 @@ void SigmaGpu::vcycle(cudaStream_t s, long long& launches, PhaseHook* hook) {
 }
 
 int SigmaGpu::error_flag(cudaStream_t s) const {
-    int e = bottom.error_flag(s);
-    for (const SigmaLevel& L : lv) e |= L.aii.error_flag(s) | L.arr_solve.error_flag(s);
-    return e;
+    if (!d_err) return 0;
+    int h = 0;
+    ck(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, s), "read error word");
+    ck(cudaStreamSynchronize(s), "read error word");
+    return h;
+}
+
+void SigmaGpu::clear_error(cudaStream_t s) {
+    if (d_err) ck(cudaMemsetAsync(d_err, 0, sizeof(int), s), "clear error word");
+}
+
+void SigmaGpu::set_wait_limit(long long polls) {
+    for (SigmaLevel& L : lv) { L.aii.spin_limit = polls; L.arr_solve.spin_limit = polls; }
+    bottom.spin_limit = polls;
+}
+
+void SigmaGpu::stall_dependency(bool on, cudaStream_t s) {
+    if (lv.empty()) return;
+    SolvePlan& p = lv[0].arr_solve.nsn > 0 ? lv[0].arr_solve : bottom;
+    p.stall_dependency(on, s);
 }
 
 }  // namespace hdd

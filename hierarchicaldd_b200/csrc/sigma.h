@@ -145,13 +145,23 @@ struct SolvePlan {
     float* d_xnew = nullptr;         // backward result in new order
     int* d_ctr = nullptr;            // tickets, completion and chunk counters
     int* d_err = nullptr;            // set when a bounded wait gives up
+    bool own_err = false;            // d_err allocated by this plan (else shared)
+    long long spin_limit = 1LL << 22;  // polls of a bounded wait before it gives up
+    int stall_front = -1, stall_ntf = 0;  // front used by stall_dependency and its task count
     size_t bytes = 0;
-    void build(const std::vector<const SnFactor*>& factors, const std::vector<int>& offsets, cudaStream_t s);
+    // shared_err: an error word shared with other plans (owned by the caller),
+    // or null for a word of the plan's own.
+    void build(const std::vector<const SnFactor*>& factors, const std::vector<int>& offsets, cudaStream_t s,
+               int* shared_err = nullptr);
     void release();
     // x_old = (A+eps I)^{-1} b_old (both in the concatenated original order).
     void solve(const float* b_old, float* x_old, cudaStream_t s, long long& launches,
                PhaseHook* hook = nullptr) const;
     int error_flag(cudaStream_t s) const;
+    // Test seam: on = raise the forward task count that one front's parent
+    // waits for by one, so that wait can never be satisfied and runs into its
+    // poll limit; off = restore it.
+    void stall_dependency(bool on, cudaStream_t s);
     ~SolvePlan() { release(); }
 };
 
@@ -189,12 +199,20 @@ struct SigmaGpu {
     bool bottom_exact = true;
     static constexpr int kBottomSmoothing = 200;  // SIGMA_MULTIGRID_SOLVER.cpp:78
     size_t device_bytes = 0;
+    // Error word shared by every solve plan of this solver: nonzero once a
+    // bounded wait gave up (then later waits return at once).
+    int* d_err = nullptr;
     void setup(const InterfaceHost& ih, int smoothing_iterations, cudaStream_t s);
     void release();
     // u[0] = sigma V-cycle(b[0]) (SIGMA_MULTIGRID_SOLVER.cpp:70-82), u[0] starting at 0.
     void vcycle(cudaStream_t s, long long& launches, PhaseHook* hook = nullptr);
     // Nonzero when a bounded wait inside a supernodal solve gave up.
     int error_flag(cudaStream_t s) const;
+    void clear_error(cudaStream_t s);
+    // Poll limit of every bounded wait (default 1 << 22).
+    void set_wait_limit(long long polls);
+    // Test seam (SolvePlan::stall_dependency) on the level-0 interface plan.
+    void stall_dependency(bool on, cudaStream_t s);
     float* b0() const { return lv.empty() ? nullptr : lv[0].b; }
     float* u0() const { return lv.empty() ? nullptr : lv[0].u; }
     ~SigmaGpu() { release(); }

@@ -44,7 +44,6 @@ constexpr int kNT = 256;                 // threads per CTA
 constexpr int kRB = 128;                 // rows per forward row block
 constexpr int kCC = 128;                 // columns per forward column block
 constexpr int kBC = 32;                  // columns per backward task (8 warps x 4)
-constexpr long kSpinLimit = 1L << 22;    // polls (with ~128 ns sleeps) before a wait gives up
 constexpr int kWarps = kNT / 32;         // small fronts per bundle (one per warp)
 constexpr int kSmallM = 256;             // rows of a front solved by one warp
 constexpr int kSmallLoads = 128;         // ... when its row chunks x columns stay below this
@@ -73,6 +72,7 @@ struct PlanView {
     float* xnew;
     int* ctr;
     int* err;
+    long long spin_limit;  // polls (with ~128 ns sleeps) before a wait gives up
 };
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
@@ -84,8 +84,8 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
 // Waits until *p >= target; false when the wait gave up, or at once when an
 // earlier wait of this launch already gave up (so one failure cannot turn
 // into a long chain of timeouts).
-__device__ bool wait_at_least(const int* p, int target, const int* err) {
-    for (long i = 0; i < kSpinLimit; ++i) {
+__device__ bool wait_at_least(const int* p, int target, const int* err, long long limit) {
+    for (long long i = 0; i < limit; ++i) {
         if (ld_acquire(p) >= target) return true;
         if (ld_acquire(err) != 0) return false;
         __nanosleep(128);
@@ -132,7 +132,7 @@ __device__ void warp_forward(const PlanView& P, int J, float* f, int lane, const
     for (int i = lane; i < m; i += 32) f[i] = (i < nj) ? b_old[P.perm[c0 + i]] : 0.0f;
     if (lane == 0) {
         bool ok = true;
-        for (int c = cb; c < ce; ++c) ok &= wait_at_least(done + P.child[c], P.ntf[P.child[c]], P.err);
+        for (int c = cb; c < ce; ++c) ok &= wait_at_least(done + P.child[c], P.ntf[P.child[c]], P.err, P.spin_limit);
         if (!ok) atomicExch(P.err, 1);
     }
     __syncwarp();
@@ -159,7 +159,7 @@ __device__ void warp_backward(const PlanView& P, int J, float* g, int lane, floa
     for (int i = lane; i < nj; i += 32) g[i] = P.ynew[c0 + i];   // from the forward launch
     if (lane == 0) {
         const int p = P.parent[J];
-        if (p >= 0 && !wait_at_least(done + p, P.ntb[p], P.err)) atomicExch(P.err, 1);
+        if (p >= 0 && !wait_at_least(done + p, P.ntb[p], P.err, P.spin_limit)) atomicExch(P.err, 1);
     }
     __syncwarp();
     for (int i = nj + lane; i < m; i += 32) g[i] = __ldcg(P.xnew + rows[i - nj]);
@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(kNT, 8) sn_forward_kernel(PlanView P, const Sn
         for (int i = tid; i < m; i += kNT) f[i] = (i < nj) ? b_old[P.perm[c0 + i]] : 0.0f;
         if (tid == 0) {
             bool ok = true;
-            for (int c = cb; c < ce; ++c) ok &= wait_at_least(done + P.child[c], P.ntf[P.child[c]], P.err);
+            for (int c = cb; c < ce; ++c) ok &= wait_at_least(done + P.child[c], P.ntf[P.child[c]], P.err, P.spin_limit);
             if (!ok) atomicExch(P.err, 1);
         }
         __syncthreads();
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(kNT, 8) sn_backward_kernel(PlanView P, const S
         }
         if (tid == 0) {
             const int p = P.parent[J];
-            if (p >= 0 && !wait_at_least(done + p, P.ntb[p], P.err)) atomicExch(P.err, 1);
+            if (p >= 0 && !wait_at_least(done + p, P.ntb[p], P.err, P.spin_limit)) atomicExch(P.err, 1);
         }
         __syncthreads();
         for (int i = max(rs, nj) + tid; i < m; i += kNT) g[i] = __ldcg(P.xnew + rows[i - nj]);
@@ -402,7 +402,8 @@ void raise_smem_limit(int device, int bytes) {
 
 }  // namespace
 
-void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::vector<int>& offsets, cudaStream_t s) {
+void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::vector<int>& offsets, cudaStream_t s,
+                      int* shared_err) {
     release();
     std::vector<int> col0, ncol, nrow, rows, child_ptr{0}, child, relmap, perm, height, depth, parent_g;
     std::vector<long long> rows_off, relmap_off, upd_off, fw_off;
@@ -596,7 +597,19 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
     d_ynew = dev::alloc_zero<float>(std::max(n, 1), bytes, s);
     d_xnew = dev::alloc_zero<float>(std::max(n, 1), bytes, s);
     d_ctr = dev::alloc_zero<int>(n_ctr, bytes, s);
-    d_err = dev::alloc_zero<int>(1, bytes, s);
+    if (shared_err) {
+        d_err = shared_err;
+        own_err = false;
+    } else {
+        d_err = dev::alloc_zero<int>(1, bytes, s);
+        own_err = true;
+    }
+    // A front with a parent, for stall_dependency (the wait of its parent's
+    // forward task on it can be made unsatisfiable).
+    stall_front = -1;
+    stall_ntf = 0;
+    for (int g = 0; g < nsn; ++g)
+        if (parent_g[g] >= 0) { stall_front = g; stall_ntf = ntf[g]; break; }
     // Persistent grid: as many CTAs as fit on the device, but no more than tasks.
     int dev_id = 0, nsm = 0, bf = 0, bb = 0;
     dev::ck(cudaGetDevice(&dev_id), "cudaGetDevice");
@@ -615,7 +628,10 @@ void SolvePlan::release() {
     dev::release(d_relmap_off); dev::release(d_relmap); dev::release(d_upd_off); dev::release(d_fw_off);
     dev::release(d_ntf); dev::release(d_ntb); dev::release(d_perm);
     dev::release(d_fwd); dev::release(d_bwd); dev::release(d_bfwd); dev::release(d_bbwd); dev::release(d_fw); dev::release(d_part); dev::release(d_upd);
-    dev::release(d_ynew); dev::release(d_xnew); dev::release(d_ctr); dev::release(d_err);
+    dev::release(d_ynew); dev::release(d_xnew); dev::release(d_ctr);
+    if (own_err) dev::release(d_err);
+    d_err = nullptr;
+    own_err = false;
     nsn = 0;
     n = 0;
     n_fwd = n_bwd = n_ctr = 0;
@@ -626,7 +642,7 @@ void SolvePlan::solve(const float* b_old, float* x_old, cudaStream_t s, long lon
     PlanView P{nsn, max_front, d_col0, d_ncol, d_nrow, d_parent, d_rows, d_rows_off, d_child_ptr, d_child,
                d_relmap_off, d_relmap, d_upd_off, d_fw_off, d_ntf, d_ntb, d_perm, d_bfwd, d_bbwd, d_fw, d_part, d_upd,
                d_ynew,
-               d_xnew, d_ctr, d_err};
+               d_xnew, d_ctr, d_err, spin_limit};
     dev::ck(cudaMemsetAsync(d_ctr, 0, sizeof(int) * n_ctr, s), "reset counters");
     if (hook) hook->begin(kPhaseSnForward);
     sn_forward_kernel<<<std::min(grid, n_fwd), kNT, forward_smem(max_front), s>>>(P, d_fwd, n_fwd, b_old);
@@ -637,6 +653,13 @@ void SolvePlan::solve(const float* b_old, float* x_old, cudaStream_t s, long lon
     dev::ck(cudaGetLastError(), "sn backward");
     if (hook) hook->end(kPhaseSnBackward, bwd_bytes);
     launches += 2;
+}
+
+void SolvePlan::stall_dependency(bool on, cudaStream_t s) {
+    if (stall_front < 0) return;
+    const int v = on ? stall_ntf + 1 : stall_ntf;
+    dev::ck(cudaMemcpyAsync(d_ntf + stall_front, &v, sizeof(int), cudaMemcpyHostToDevice, s), "stall dependency");
+    dev::ck(cudaStreamSynchronize(s), "stall dependency");
 }
 
 int SolvePlan::error_flag(cudaStream_t s) const {

@@ -323,6 +323,7 @@ void Solver::solve(hdd_result* res) {
     init.rho_old_d = 3.402823466e+38;
     cuda_check(cudaMemcpyAsync(scal.p, &init, sizeof(init), cudaMemcpyHostToDevice, stream), "init scalars");
     x.zero(stream);
+    sigma.clear_error(stream);
     cudaEvent_t e0, e1;
     cuda_check(cudaEventCreate(&e0), "event");
     cuda_check(cudaEventCreate(&e1), "event");
@@ -335,6 +336,7 @@ void Solver::solve(hdd_result* res) {
     cuda_check(cudaMemcpyAsync(&rmax, scalars_f.p, sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
     sync();
     const double b_inf = rmax;
+    history.assign(1, (double)rmax);
     const float threshold = opts.relative_tol ? (float)(opts.tol * b_inf) : (float)opts.tol;
     const float small_number = 1.1920929e-07f;
     int it = 0;
@@ -366,7 +368,14 @@ void Solver::solve(hdd_result* res) {
         cuda_check(launch_reduce_max(partial_max.p, nt, scalars_f.p, stream), "reduce"); count();
         cuda_check(cudaMemcpyAsync(&rmax, scalars_f.p, sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
         cuda_check(cudaMemcpyAsync(&hs, scal.p, sizeof(hs), cudaMemcpyDeviceToHost, stream), "D2H");
+        int herr = 0;
+        if (sigma.d_err)
+            cuda_check(cudaMemcpyAsync(&herr, sigma.d_err, sizeof(int), cudaMemcpyDeviceToHost, stream), "D2H");
         sync();
+        history.push_back((double)rmax);
+        // A bounded wait that gave up leaves this iteration's preconditioner
+        // invalid: stop here (check_waits below reports HDD_ERR_TIMEOUT).
+        if (herr != 0) { ++it; break; }
         if (hs.status != 0 || !std::isfinite(rmax)) { breakdown = true; ++it; break; }
     }
     cuda_check(cudaEventRecord(e1, stream), "event record");
@@ -420,6 +429,7 @@ void Solver::apply_preconditioner_dense(const float* rin, float* zout) {
     dense_to_tiles(L, rin, t.data());
     cuda_check(cudaMemcpyAsync(r.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
     z.zero(stream);
+    sigma.clear_error(stream);
     apply_preconditioner(r.p, z.p);
     cuda_check(launch_project(geom(), z.p, stream), "project"); count();
     cuda_check(cudaMemcpyAsync(t.data(), z.p, t.size() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
@@ -466,6 +476,7 @@ void Solver::sigma_vcycle_host(const float* b0, float* u0) {
     if (n_if == 0) return;
     cuda_check(cudaMemcpyAsync(sigma.b0(), b0, n_if * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
     cuda_check(cudaMemsetAsync(sigma.u0(), 0, n_if * sizeof(float), stream), "memset");
+    sigma.clear_error(stream);
     sigma.vcycle(stream, launches);
     cuda_check(cudaMemcpyAsync(u0, sigma.u0(), n_if * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
     sync();

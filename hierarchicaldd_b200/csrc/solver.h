@@ -93,6 +93,10 @@ struct Solver {
     int iomode = HDD_IOMODE_NEITHER;  // interface dump / reload at initialize()
     std::string io_dir;
     double setup_ms = 0;
+    // max|r| of the recursively updated residual at the start of each PCG
+    // iteration of the last solve (entry 0: r = b), for parity checks against
+    // the oracle's history.
+    std::vector<double> history;
     // Host wall time of the setup phases: layout and vector uploads, interface
     // system (assembly or reload, and dump), interface solver (factorisations
     // and solve plans), total.

@@ -153,6 +153,15 @@ class SPGrid_Domain_Decomposition_Solver:
         self.last_result["status"] = st
         return self.last_result
 
+    def Residual_History(self) -> np.ndarray:
+        """max|r| at the start of every PCG iteration of the last solve (entry 0: r = b)."""
+        n = C.c_int()
+        self._check(self.lib.hdd_get_residual_history(self.h, None, 0, C.byref(n)))
+        out = np.zeros(n.value, np.float64)
+        self._check(self.lib.hdd_get_residual_history(self.h, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                                      n.value, C.byref(n)))
+        return out
+
     def Solution(self) -> np.ndarray:
         x = np.zeros(self.size, np.float32)
         self._check(self.lib.hdd_get_solution_dense(self.h, _fp(x)))

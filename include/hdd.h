@@ -147,6 +147,13 @@ hdd_status hdd_solve(hdd_solver* s, hdd_result* result);
 /* Copies the solution x of the last solve. */
 hdd_status hdd_get_solution_dense(hdd_solver* s, float* x);
 
+/* The convergence norm max|r| of the last solve at the start of every PCG
+ * iteration, entry 0 being that of r = b: the values CONJUGATE_GRADIENT::Solve
+ * logs with print_residuals
+ * (PB/Public_Library/PhysBAM_Tools/Krylov_Solvers/CONJUGATE_GRADIENT.cpp:38-41).
+ * Writes min(capacity, *n) entries of out; *n gets iterations + 1. */
+hdd_status hdd_get_residual_history(hdd_solver* s, double* out, int capacity, int* n);
+
 /* Test seam: z = Project(Apply_Preconditioner(r)), replacing
  * SPGrid_Domain_Decomposition_Preconditioner::Apply_Preconditioner
  * (SPGrid_Domain_Decomposition_Preconditioner.h:88-128) followed by
@@ -212,6 +219,22 @@ hdd_status hdd_get_kernel_bytes(hdd_solver* s, double* bytes);
  * solve plans), ms[3] total.  No reference counterpart (the reference logs its
  * setup scopes with LOG::SCOPE). */
 hdd_status hdd_get_setup_timing(hdd_solver* s, double* ms);
+
+/* Poll budget of the bounded device waits inside the interface solves (a
+ * task of a persistent supernodal solve waiting for the fronts it depends
+ * on; about 0.2-0.5 us per poll).  A wait that runs out raises an error word:
+ * the solve stops after that PCG iteration and returns HDD_ERR_TIMEOUT, and
+ * the next call starts with the word cleared.  Default 1 << 22 polls; takes
+ * effect for solves after hdd_initialize_preconditioner.  No reference
+ * counterpart (the reference's host threads wait without bound,
+ * GPU/Nodes/Communicator.cpp:30-33). */
+hdd_status hdd_set_wait_limit(hdd_solver* s, long long polls);
+
+/* Test seam for the bounded waits: on != 0 makes one dependency of the level-0
+ * interface solve unsatisfiable (a parent front then waits for one task more
+ * than its child runs), so every solve reports HDD_ERR_TIMEOUT once the wait
+ * limit runs out; on == 0 restores the dependency.  No reference counterpart. */
+hdd_status hdd_test_stall_dependency(hdd_solver* s, int on);
 
 /* Number of our CUDA kernel launches issued since the handle was created. */
 hdd_status hdd_kernel_launch_count(hdd_solver* s, long long* count);
