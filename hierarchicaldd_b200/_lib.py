@@ -76,6 +76,7 @@ SIGNATURES = {
     "hdd_multiply_dense": (C.c_int, [_vp, _fp, _fp]),
     "hdd_multiply_dot_dense_device_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "hdd_sigma_vcycle": (C.c_int, [_vp, _fp, _fp]),
+    "hdd_interface_solve": (C.c_int, [_vp, C.c_int, C.c_int, _fp, _fp, _ip]),
     "hdd_interface_size": (C.c_int, [_vp, C.c_int, _ip]),
     "hdd_interface_map": (C.c_int, [_vp, _ip]),
     "hdd_interface_matrix": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _ip, _ip, _ip, _ip, _ip,

@@ -27,6 +27,7 @@ SOURCES = [
     "kernels_vcycle.cu",
     "kernels_pcg.cu",
     "sigma.cu",
+    "sn_plan.cpp",
     "sn_solve.cu",
     "solver.cu",
     "noalloc.cu",

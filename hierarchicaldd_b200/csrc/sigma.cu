@@ -40,13 +40,6 @@ constexpr int kNT = 256;
 
 using dev::ck;
 
-// DOF positions of one subdomain's interior block, when assembly recorded them.
-const std::vector<std::array<int, 3>>* positions(const std::vector<std::vector<std::vector<std::array<int, 3>>>>& xyz,
-                                                int l, int sd, int rows) {
-    if (l >= (int)xyz.size() || sd >= (int)xyz[l].size() || (int)xyz[l][sd].size() != rows) return nullptr;
-    return &xyz[l][sd];
-}
-
 // ---------------------------------------------------------------------------
 // Kernels
 // ---------------------------------------------------------------------------
@@ -204,7 +197,7 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
         for (int sd = 0; sd < ih.n_sub; ++sd) {
             try {
                 if (ih.Aii[l][sd].rows == 0) continue;
-                aii[sd].analyze(ih.Aii[l][sd], positions(ih.aii_xyz, l, sd, ih.Aii[l][sd].rows));
+                aii[sd].analyze(ih.Aii[l][sd], interior_positions(ih, l, sd));
                 aii[sd].factor(ih.Aii[l][sd], eps);
                 if (l + 1 < M) aii[sd].build_solve_blocks();
             } catch (const std::exception& e) { err[sd] = e.what(); }
@@ -213,8 +206,7 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
             if (!e.empty()) throw Error(HDD_ERR_INTERNAL, "subdomain factorisation: " + e);
         stamp("subdomain factors", l);
         SnFactor arrf;
-        const std::vector<std::array<int, 3>>* ixyz =
-            (l < (int)ih.iface_xyz.size() && (int)ih.iface_xyz[l].size() == ih.Arr[l].rows) ? &ih.iface_xyz[l] : nullptr;
+        const std::vector<std::array<int, 3>>* ixyz = interface_positions(ih, l);
         arrf.analyze(ih.Arr[l], ixyz);
         arrf.factor(ih.Arr[l], eps);
         if (l + 1 < M) arrf.build_solve_blocks();
@@ -317,7 +309,7 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
             std::vector<std::array<int, 3>> kxyz;
             bool have_xyz = ixyz != nullptr;
             for (int sd = 0; sd < ih.n_sub && have_xyz; ++sd) {
-                const auto* px = positions(ih.aii_xyz, l, sd, ih.Aii[l][sd].rows);
+                const auto* px = interior_positions(ih, l, sd);
                 if (!px) have_xyz = false;
                 else kxyz.insert(kxyz.end(), px->begin(), px->end());
             }

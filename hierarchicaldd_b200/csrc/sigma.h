@@ -107,6 +107,35 @@ protected:
 constexpr int kPhaseSnForward = 6;
 constexpr int kPhaseSnBackward = 7;
 
+// Host reference of a solve plan (sn_plan.cpp): the fronts of a batch of
+// independent factorisations with concatenated unknowns and the FP32
+// coefficient blocks Fw the device plan stores, solved front by front in
+// post-order with FP64 accumulation and FP64 vectors between fronts (the
+// device kernels' arithmetic, up to the order of FP64 sums).  Test
+// infrastructure for the device plan: CPU tests check it against the FP64
+// factorisation, GPU tests check the device solve against it.
+struct PlanHost {
+    int n = 0, nsn = 0;
+    std::vector<int> perm;                        // new -> old (concatenated)
+    std::vector<int> col0, ncol, nrow, parent, rows;
+    std::vector<long long> rows_off, fw_off;
+    std::vector<float> fw;                        // Fw blocks, m x nj col-major, ld round4(m)
+    void build(const std::vector<const SnFactor*>& factors, const std::vector<int>& offsets);
+    void emulate(const float* b_old, float* x_old) const;
+};
+
+// DOF positions (for the fill-reducing ordering) of level l's interface
+// system and of subdomain sd's interior system, or null when assembly did not
+// record them.
+const std::vector<std::array<int, 3>>* interface_positions(const InterfaceHost& ih, int l);
+const std::vector<std::array<int, 3>>* interior_positions(const InterfaceHost& ih, int l, int sd);
+
+// Factorisations of one interface solve as the sigma solver builds them
+// (A + 1e-5 I, ordering from the positions, explicit solve blocks) and the
+// plan over them: kind 0 = Arr of level l, kind 1 = Aii of every subdomain of
+// level l with the unknowns concatenated in subdomain order.
+void interface_solve_plan(const InterfaceHost& ih, int kind, int l, std::vector<SnFactor>& factors, PlanHost& plan);
+
 // One unit of device work of a supernodal solve, taken by a CTA of the
 // persistent solve kernels (sn_solve.cu).  With front >= 0, forward: rows
 // [r0, r0+rows) of front `front` times its columns [c0, c0+ncols); when a row
@@ -127,6 +156,7 @@ struct SolvePlan {
     int n_fwd = 0, n_bwd = 0;        // task counts
     int n_ctr = 0;                   // ints in the counter block
     int grid = 0;                    // persistent CTAs per launch
+    int ntasks_f = 0, ntasks_b = 0;  // tasks, forward / backward
     double fwd_bytes = 0, bwd_bytes = 0;  // algorithmic bytes of one forward / backward launch
     int *d_col0 = nullptr, *d_ncol = nullptr, *d_nrow = nullptr, *d_parent = nullptr;
     int *d_rows = nullptr; long long *d_rows_off = nullptr;
@@ -139,10 +169,10 @@ struct SolvePlan {
     SnTask *d_fwd = nullptr, *d_bwd = nullptr;
     int *d_bfwd = nullptr, *d_bbwd = nullptr;  // fronts of the forward / backward bundles
     float* d_fw = nullptr;           // Fw blocks of all fronts
-    float* d_part = nullptr;         // partial sums of split row blocks
-    float* d_upd = nullptr;          // update vectors
-    float* d_ynew = nullptr;         // forward result in new order
-    float* d_xnew = nullptr;         // backward result in new order
+    double* d_part = nullptr;        // partial sums of split row blocks
+    double* d_upd = nullptr;         // update vectors
+    double* d_ynew = nullptr;        // forward result in new order
+    double* d_xnew = nullptr;        // backward result in new order
     int* d_ctr = nullptr;            // tickets, completion and chunk counters
     int* d_err = nullptr;            // set when a bounded wait gives up
     bool own_err = false;            // d_err allocated by this plan (else shared)

@@ -1,12 +1,18 @@
 // Supernodal triangular solves on the GPU (the device half of the PARDISO
-// stand-in, SIGMA_SMOOTHER.cpp:433-449 phase 33).
+// stand-in; the reference's phase-33 solves are in
+// CPU/Interface_Solver/SIGMA_SMOOTHER.cpp:293-324).
 //
 // Every front J of the nested-dissection forest carries
 // Fw = [L_JJ^{-1}; -L_RJ L_JJ^{-1}] (m = nj + nr rows, nj columns), stored once,
 // column-major with leading dimension round4(m), so
 //   forward   [y_J; v_J] = Fw f_J + [0; f_R]   (f assembled from b and the children's v)
 //   backward  x_J        = Fw^T [y_J; x_R]
-// are dense products over the same coefficients.
+// are dense products over the same coefficients.  The coefficients are FP32
+// (what the HBM stream carries); products are accumulated in FP64 (every
+// FP32 x FP32 product is exact in FP64) and the vectors passed between fronts
+// (the assembled f, y, x and the update vectors) are FP64, so a solve rounds
+// to FP32 once, at its output, like the FP64 substitution it replaces up to
+// the rounding of the stored coefficients.
 //
 // Each direction is ONE persistent launch.  Its work is a list of tasks in
 // topological order (forward: children before parents; backward: parents
@@ -66,10 +72,10 @@ struct PlanView {
     const int* perm;
     const int *bfwd, *bbwd;
     const float* fw;
-    float* part;
-    float* upd;
-    float* ynew;
-    float* xnew;
+    double* part;
+    double* upd;
+    double* ynew;
+    double* xnew;
     int* ctr;
     int* err;
     long long spin_limit;  // polls (with ~128 ns sleeps) before a wait gives up
@@ -95,23 +101,23 @@ __device__ bool wait_at_least(const int* p, int target, const int* err, long lon
 
 // Forward solve of one small front by one warp (MQ row chunks of 32 rows).
 template <int MQ>
-__device__ __forceinline__ void warp_forward_rows(const PlanView& P, int J, int m, int nj, const float* f, int lane) {
+__device__ __forceinline__ void warp_forward_rows(const PlanView& P, int J, int m, int nj, const double* f, int lane) {
     const size_t ld = (size_t)((m + 3) & ~3);
     const float* A = P.fw + P.fw_off[J];
-    float acc[MQ];
+    double acc[MQ];
 #pragma unroll
-    for (int q = 0; q < MQ; ++q) acc[q] = 0.0f;
+    for (int q = 0; q < MQ; ++q) acc[q] = 0.0;
 #pragma unroll 2
     for (int c = 0; c < nj; c += 4) {
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
             if (c + t >= nj) break;
-            const float fc = f[c + t];
+            const double fc = f[c + t];
             const float* col = A + (size_t)(c + t) * ld;
 #pragma unroll
             for (int q = 0; q < MQ; ++q) {
                 const int r = q * 32 + lane;
-                if (r < m && r >= c + t) acc[q] = fmaf(__ldg(col + r), fc, acc[q]);
+                if (r < m && r >= c + t) acc[q] = fma((double)__ldg(col + r), fc, acc[q]);
             }
         }
     }
@@ -126,10 +132,10 @@ __device__ __forceinline__ void warp_forward_rows(const PlanView& P, int J, int 
     }
 }
 
-__device__ void warp_forward(const PlanView& P, int J, float* f, int lane, const float* b_old, int* done) {
+__device__ void warp_forward(const PlanView& P, int J, double* f, int lane, const float* b_old, int* done) {
     const int nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
     const int cb = P.child_ptr[J], ce = P.child_ptr[J + 1];
-    for (int i = lane; i < m; i += 32) f[i] = (i < nj) ? b_old[P.perm[c0 + i]] : 0.0f;
+    for (int i = lane; i < m; i += 32) f[i] = (i < nj) ? (double)b_old[P.perm[c0 + i]] : 0.0;
     if (lane == 0) {
         bool ok = true;
         for (int c = cb; c < ce; ++c) ok &= wait_at_least(done + P.child[c], P.ntf[P.child[c]], P.err, P.spin_limit);
@@ -139,7 +145,7 @@ __device__ void warp_forward(const PlanView& P, int J, float* f, int lane, const
     for (int c = cb; c < ce; ++c) {
         const int C = P.child[c];
         const int mc = P.nrow[C];
-        const float* uc = P.upd + P.upd_off[C];
+        const double* uc = P.upd + P.upd_off[C];
         const int* rm = P.relmap + P.relmap_off[C];
         for (int k = lane; k < mc; k += 32) f[rm[k]] += __ldcg(uc + k);
         __syncwarp();
@@ -153,7 +159,7 @@ __device__ void warp_forward(const PlanView& P, int J, float* f, int lane, const
 }
 
 // Backward solve of one small front by one warp: x_a = sum_{r >= a} Fw(r, a) g_r.
-__device__ void warp_backward(const PlanView& P, int J, float* g, int lane, float* x_old, int* done) {
+__device__ void warp_backward(const PlanView& P, int J, double* g, int lane, float* x_old, int* done) {
     const int nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
     const int* rows = P.rows + P.rows_off[J];
     for (int i = lane; i < nj; i += 32) g[i] = P.ynew[c0 + i];   // from the forward launch
@@ -167,13 +173,13 @@ __device__ void warp_backward(const PlanView& P, int J, float* g, int lane, floa
     const size_t ld = (size_t)((m + 3) & ~3);
     const float* A = P.fw + P.fw_off[J];
     for (int a = 0; a < nj; a += 4) {
-        float s4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        double s4[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll 4
         for (int r = (a & ~31) + lane; r < m; r += 32) {
-            const float gr = g[r];
+            const double gr = g[r];
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-                if (a + j < nj && r >= a + j) s4[j] = fmaf(__ldg(A + (size_t)(a + j) * ld + r), gr, s4[j]);
+                if (a + j < nj && r >= a + j) s4[j] = fma((double)__ldg(A + (size_t)(a + j) * ld + r), gr, s4[j]);
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j)
@@ -184,7 +190,7 @@ __device__ void warp_backward(const PlanView& P, int J, float* g, int lane, floa
             for (int j = 0; j < 4; ++j)
                 if (a + j < nj) {
                     P.xnew[c0 + a + j] = s4[j];
-                    x_old[P.perm[c0 + a + j]] = s4[j];
+                    x_old[P.perm[c0 + a + j]] = (float)s4[j];
                 }
         }
     }
@@ -193,11 +199,11 @@ __device__ void warp_backward(const PlanView& P, int J, float* g, int lane, floa
     if (lane == 0) atomicAdd(done + J, 1);
 }
 
-__global__ void __launch_bounds__(kNT, 8) sn_forward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks,
+__global__ void __launch_bounds__(kNT, 5) sn_forward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks,
                                                          const float* __restrict__ b_old) {
-    extern __shared__ float sh[];
-    float* f = sh;                 // the front's input vector, m entries
-    float* red = sh + P.max_m;     // column-slice partial sums, kNT entries
+    extern __shared__ double sh[];
+    double* f = sh;                // the front's input vector, m entries
+    double* red = sh + P.max_m;    // column-slice partial sums, kNT entries
     __shared__ int s_ticket, s_last;
     int* done = P.ctr + 2;
     int* chunk_ctr = P.ctr + 2 + 2 * P.nsn;
@@ -236,7 +242,7 @@ __global__ void __launch_bounds__(kNT, 8) sn_forward_kernel(PlanView P, const Sn
 #pragma unroll
         for (int u = 0; u < 8; ++u) v0[u] = (cbeg + u < cend) ? __ldg(A + (size_t)(cbeg + u) * ld) : 0.0f;
         // b's part of the input vector does not depend on other fronts.
-        for (int i = tid; i < m; i += kNT) f[i] = (i < nj) ? b_old[P.perm[c0 + i]] : 0.0f;
+        for (int i = tid; i < m; i += kNT) f[i] = (i < nj) ? (double)b_old[P.perm[c0 + i]] : 0.0;
         if (tid == 0) {
             bool ok = true;
             for (int c = cb; c < ce; ++c) ok &= wait_at_least(done + P.child[c], P.ntf[P.child[c]], P.err, P.spin_limit);
@@ -246,31 +252,31 @@ __global__ void __launch_bounds__(kNT, 8) sn_forward_kernel(PlanView P, const Sn
         for (int c = cb; c < ce; ++c) {
             const int C = P.child[c];
             const int mc = P.nrow[C];
-            const float* uc = P.upd + P.upd_off[C];
+            const double* uc = P.upd + P.upd_off[C];
             const int* rm = P.relmap + P.relmap_off[C];
             for (int k = tid; k < mc; k += kNT) f[rm[k]] += __ldcg(uc + k);
             __syncthreads();
         }
-        float acc = 0.0f;
+        double acc = 0.0;
         if (active) {
 #pragma unroll
             for (int u = 0; u < 8; ++u)
-                if (cbeg + u < cend) acc = fmaf(v0[u], f[cbeg + u], acc);
+                if (cbeg + u < cend) acc = fma((double)v0[u], f[cbeg + u], acc);
             int c = cbeg + 8;
             for (; c + 8 <= cend; c += 8) {
                 float v[8];
 #pragma unroll
                 for (int u = 0; u < 8; ++u) v[u] = __ldg(A + (size_t)(c + u) * ld);
 #pragma unroll
-                for (int u = 0; u < 8; ++u) acc = fmaf(v[u], f[c + u], acc);
+                for (int u = 0; u < 8; ++u) acc = fma((double)v[u], f[c + u], acc);
             }
-            for (; c < cend; ++c) acc = fmaf(__ldg(A + (size_t)c * ld), f[c], acc);
+            for (; c < cend; ++c) acc = fma((double)__ldg(A + (size_t)c * ld), f[c], acc);
         }
         if (ks > 1) {
             if (sl < ks) red[tid] = acc;
             __syncthreads();
             if (sl == 0 && lr < T.rows) {
-                float s2 = red[lr];
+                double s2 = red[lr];
                 for (int q = 1; q < ks; ++q) s2 += red[q * mr + lr];
                 acc = s2;
             }
@@ -290,7 +296,7 @@ __global__ void __launch_bounds__(kNT, 8) sn_forward_kernel(PlanView P, const Sn
             if (s_last) {
                 __threadfence();
                 if (mine) {
-                    float s2 = 0.0f;
+                    double s2 = 0.0;
                     for (int k = 0; k < T.nk; ++k) s2 += __ldcg(P.part + T.part + (size_t)k * kRB + lr);
                     if (row < nj) P.ynew[c0 + row] = s2;
                     else P.upd[P.upd_off[J] + (row - nj)] = f[row] + s2;
@@ -303,9 +309,9 @@ __global__ void __launch_bounds__(kNT, 8) sn_forward_kernel(PlanView P, const Sn
     }
 }
 
-__global__ void __launch_bounds__(kNT, 8) sn_backward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks,
+__global__ void __launch_bounds__(kNT, 5) sn_backward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks,
                                                           float* __restrict__ x_old) {
-    extern __shared__ float g[];   // [y_J; x_R], m entries
+    extern __shared__ double g[];  // [y_J; x_R], m entries
     __shared__ int s_ticket;
     int* done = P.ctr + 2 + P.nsn;
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
@@ -326,7 +332,7 @@ __global__ void __launch_bounds__(kNT, 8) sn_backward_kernel(PlanView P, const S
         const int* rows = P.rows + P.rows_off[J];
         const size_t ld = (size_t)((m + 3) & ~3);
         const float* A = P.fw + P.fw_off[J];
-        float s4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        double s4[4] = {0.0, 0.0, 0.0, 0.0};
         const int amin = a0 + w;
         // Rows below nj (the L_JJ^{-T} y part) need only this front's forward
         // result, so they are summed before waiting on the parent; each lane
@@ -337,11 +343,11 @@ __global__ void __launch_bounds__(kNT, 8) sn_backward_kernel(PlanView P, const S
         if (amin < a0 + na) {
 #pragma unroll 4
             for (; r < nj; r += 32) {
-                const float gr = g[r];
+                const double gr = g[r];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const int a = amin + 8 * j;
-                    if (a < a0 + na && r >= a) s4[j] = fmaf(__ldg(A + (size_t)a * ld + r), gr, s4[j]);
+                    if (a < a0 + na && r >= a) s4[j] = fma((double)__ldg(A + (size_t)a * ld + r), gr, s4[j]);
                 }
             }
         }
@@ -355,11 +361,11 @@ __global__ void __launch_bounds__(kNT, 8) sn_backward_kernel(PlanView P, const S
         if (amin < a0 + na) {
 #pragma unroll 4
             for (; r < m; r += 32) {
-                const float gr = g[r];
+                const double gr = g[r];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const int a = amin + 8 * j;
-                    if (a < a0 + na) s4[j] = fmaf(__ldg(A + (size_t)a * ld + r), gr, s4[j]);
+                    if (a < a0 + na) s4[j] = fma((double)__ldg(A + (size_t)a * ld + r), gr, s4[j]);
                 }
             }
         }
@@ -373,7 +379,7 @@ __global__ void __launch_bounds__(kNT, 8) sn_backward_kernel(PlanView P, const S
                 const int a = amin + 8 * j;
                 if (a < a0 + na) {
                     P.xnew[c0 + a] = s4[j];
-                    x_old[P.perm[c0 + a]] = s4[j];
+                    x_old[P.perm[c0 + a]] = (float)s4[j];
                 }
             }
         }
@@ -383,8 +389,8 @@ __global__ void __launch_bounds__(kNT, 8) sn_backward_kernel(PlanView P, const S
     }
 }
 
-size_t forward_smem(int max_m) { return (size_t)std::max(max_m + kNT, kWarps * kSmallM) * sizeof(float); }
-size_t backward_smem(int max_m) { return (size_t)std::max(max_m, kWarps * kSmallM) * sizeof(float); }
+size_t forward_smem(int max_m) { return (size_t)std::max(max_m + kNT, kWarps * kSmallM) * sizeof(double); }
+size_t backward_smem(int max_m) { return (size_t)std::max(max_m, kWarps * kSmallM) * sizeof(double); }
 
 // The dynamic shared-memory limit of the two kernels only ever grows, so a
 // plan built later with smaller fronts cannot invalidate an earlier plan's
@@ -592,10 +598,10 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
     d_bfwd = dev::upload(bfwd.empty() ? std::vector<int>{0} : bfwd, s, bytes);
     d_bbwd = dev::upload(bbwd.empty() ? std::vector<int>{0} : bbwd, s, bytes);
     d_fw = dev::upload(fw, s, bytes);
-    d_part = dev::alloc_zero<float>(std::max<long long>(part_total, 1), bytes, s);
-    d_upd = dev::alloc_zero<float>(std::max<long long>(upd_total, 1), bytes, s);
-    d_ynew = dev::alloc_zero<float>(std::max(n, 1), bytes, s);
-    d_xnew = dev::alloc_zero<float>(std::max(n, 1), bytes, s);
+    d_part = dev::alloc_zero<double>(std::max<long long>(part_total, 1), bytes, s);
+    d_upd = dev::alloc_zero<double>(std::max<long long>(upd_total, 1), bytes, s);
+    d_ynew = dev::alloc_zero<double>(std::max(n, 1), bytes, s);
+    d_xnew = dev::alloc_zero<double>(std::max(n, 1), bytes, s);
     d_ctr = dev::alloc_zero<int>(n_ctr, bytes, s);
     if (shared_err) {
         d_err = shared_err;
@@ -605,11 +611,13 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
         own_err = true;
     }
     // A front with a parent, for stall_dependency (the wait of its parent's
-    // forward task on it can be made unsatisfiable).
+    // forward tasks on it can be made unsatisfiable).
     stall_front = -1;
     stall_ntf = 0;
     for (int g = 0; g < nsn; ++g)
         if (parent_g[g] >= 0) { stall_front = g; stall_ntf = ntf[g]; break; }
+    ntasks_f = n_fwd;
+    ntasks_b = n_bwd;
     // Persistent grid: as many CTAs as fit on the device, but no more than tasks.
     int dev_id = 0, nsm = 0, bf = 0, bb = 0;
     dev::ck(cudaGetDevice(&dev_id), "cudaGetDevice");

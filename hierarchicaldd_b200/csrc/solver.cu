@@ -483,6 +483,29 @@ void Solver::sigma_vcycle_host(const float* b0, float* u0) {
     check_waits();
 }
 
+void Solver::interface_solve(int kind, int level, const float* bh, float* xh, int* n) {
+    if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+    if (level < 0 || level >= (int)sigma.lv.size()) throw Error(HDD_ERR_INVALID_ARGUMENT, "level out of range");
+    SigmaLevel& Lv = sigma.lv[level];
+    const SolvePlan& plan = kind == 0 ? Lv.arr_solve : Lv.aii;
+    const int rows = kind == 0 ? Lv.n_iface : Lv.n_int;
+    *n = rows;
+    if (!bh || !xh) return;
+    if (plan.nsn == 0 && rows > 0)
+        throw Error(HDD_ERR_UNSUPPORTED, "no separate solve plan at this level (coarsest level solved as a whole)");
+    if (rows == 0) return;
+    float* db = kind == 0 ? Lv.tmp : Lv.vb;
+    float* dx = kind == 0 ? Lv.u : Lv.vx;
+    cuda_check(cudaSetDevice(opts.device), "cudaSetDevice");
+    cuda_check(cudaMemcpyAsync(db, bh, rows * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
+    cuda_check(cudaMemsetAsync(dx, 0, rows * sizeof(float), stream), "memset");
+    sigma.clear_error(stream);
+    plan.solve(db, dx, stream, launches, &hook);
+    cuda_check(cudaMemcpyAsync(xh, dx, rows * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    check_waits();
+}
+
 void Solver::check_waits() {
     if (sigma.error_flag(stream))
         throw Error(HDD_ERR_TIMEOUT, "a bounded device wait in the sigma solve gave up; results are invalid");

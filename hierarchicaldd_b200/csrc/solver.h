@@ -162,6 +162,8 @@ struct Solver {
     void vcycle_dense(float* u, const float* bb, int nv);
     void multiply_dense(const float* xin, float* yout);
     void sigma_vcycle_host(const float* b0, float* u0);
+    // One Arr (kind 0) or concatenated Aii (kind 1) supernodal solve of a sigma level.
+    void interface_solve(int kind, int level, const float* bh, float* xh, int* n);
     // Throws HDD_ERR_TIMEOUT when a device-side bounded wait gave up.
     void check_waits();
 

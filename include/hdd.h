@@ -191,6 +191,16 @@ hdd_status hdd_multiply_dot_dense_device_noalloc(hdd_solver* s, const float* x, 
  * on the level-0 interface right-hand side b0 (interface DOF order). */
 hdd_status hdd_sigma_vcycle(hdd_solver* s, const float* b0, float* u0);
 
+/* Test seam: one supernodal solve x = (A + 1e-5 I)^{-1} b on the GPU, the
+ * stand-in for a PARDISO phase-33 solve of SIGMA_SMOOTHER::Smooth
+ * (CPU/Interface_Solver/SIGMA_SMOOTHER.cpp:293-324): kind 0 = Arr of sigma
+ * level `level`, kind 1 = Aii of every subdomain of that level with the
+ * unknowns concatenated in subdomain order.  *n gets the number of unknowns;
+ * with b or x NULL nothing else happens.  HDD_ERR_UNSUPPORTED for the
+ * coarsest level when its smoothing steps are replaced by one solve of the
+ * whole level (no separate Arr / Aii plans exist there). */
+hdd_status hdd_interface_solve(hdd_solver* s, int kind, int level, const float* b, float* x, int* n);
+
 /* Interface DOF count at a sigma level and the level-0 DOF -> cell map
  * (INTERFACE_MATRIX_GENERATOR::interface_map). */
 hdd_status hdd_interface_size(hdd_solver* s, int level, int* n);

@@ -317,4 +317,56 @@ double shim_factor_check(void* h, int kind, int level, int sub, double* blocks_d
     *blocks_diff = xm > 0 ? d / xm : d;
     return std::sqrt(rn / bn);
 }
+
+// The supernodal solve plan of one interface solve (kind 0: Arr of level l;
+// 1: Aii of all subdomains, concatenated), built as the sigma solver builds
+// it and solved on the host front by front with the device kernels'
+// arithmetic (PlanHost::emulate): x = plan solve of b.  Returns 0, or 1 on an
+// exception.
+int shim_plan_emulate(void* h, int kind, int level, const float* b, float* x) {
+    Shim* s = static_cast<Shim*>(h);
+    try {
+        if (level < 0 || level >= s->ih.M || (kind != 0 && kind != 1)) return 1;
+        std::vector<SnFactor> fs;
+        PlanHost plan;
+        interface_solve_plan(s->ih, kind, level, fs, plan);
+        plan.emulate(b, x);
+        return 0;
+    } catch (const std::exception&) {
+        return 1;
+    }
+}
+
+// Same plan: relative max-norm difference between its host solve (FP32
+// coefficients) and the factorisations' own FP64 solve, for a random
+// right-hand side; -1 on error.  *n gets the number of unknowns.
+double shim_plan_check(void* h, int kind, int level, int* n) {
+    Shim* s = static_cast<Shim*>(h);
+    try {
+        if (level < 0 || level >= s->ih.M || (kind != 0 && kind != 1)) return -1.0;
+        std::vector<SnFactor> fs;
+        PlanHost plan;
+        interface_solve_plan(s->ih, kind, level, fs, plan);
+        *n = plan.n;
+        std::mt19937 rng(11);
+        std::uniform_real_distribution<float> U(-1.0f, 1.0f);
+        std::vector<float> b(plan.n), x(plan.n, 0.0f);
+        for (float& v : b) v = U(rng);
+        plan.emulate(b.data(), x.data());
+        std::vector<double> ref(b.begin(), b.end());
+        int off = 0;  // unknowns are concatenated in factor order (empty factors add none)
+        for (const SnFactor& F : fs) {
+            F.solve(ref.data() + off);
+            off += F.n;
+        }
+        double dmax = 0, rmax = 0;
+        for (int i = 0; i < plan.n; ++i) {
+            dmax = std::max(dmax, std::fabs((double)x[i] - ref[i]));
+            rmax = std::max(rmax, std::fabs(ref[i]));
+        }
+        return rmax > 0 ? dmax / rmax : dmax;
+    } catch (const std::exception&) {
+        return -1.0;
+    }
+}
 }

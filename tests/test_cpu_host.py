@@ -24,48 +24,11 @@ import scipy.sparse as sp
 from conftest import ROOT
 from hierarchicaldd_b200 import domains
 from oracle_ffi import Oracle
-
-CSRC = os.path.join(ROOT, "hierarchicaldd_b200", "csrc")
-BUILD = os.path.join(ROOT, "hierarchicaldd_b200", "_build")
-SHIM = os.path.join(BUILD, "libhost_shim.so")
-
+from shim_ffi import BUILD, SHIM, load_shim  # noqa: F401
 
 @pytest.fixture(scope="module")
 def shim():
-    os.makedirs(BUILD, exist_ok=True)
-    srcs = [os.path.join(ROOT, "tests", "host_shim.cpp")] + [
-        os.path.join(CSRC, f) for f in ("host_setup.cpp", "host_interface.cpp", "host_cholesky.cpp", "host_interface_io.cpp")]
-    if not os.path.exists(SHIM) or any(os.path.getmtime(f) > os.path.getmtime(SHIM) for f in srcs):
-        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
-                        "-I", CSRC, "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
-                        "-o", SHIM] + srcs, check=True)
-    L = C.CDLL(SHIM)
-    ip = C.POINTER(C.c_int)
-    L.shim_build.restype = C.c_void_p
-    L.shim_build.argtypes = [ip, ip, C.c_int, C.c_int, C.POINTER(C.c_uint32), C.c_char_p, C.c_int]
-    L.shim_free.argtypes = [C.c_void_p]
-    L.shim_num_subdomains.argtypes = [C.c_void_p]
-    L.shim_matrix_shape.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, ip]
-    L.shim_matrix_get.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, ip, ip, C.POINTER(C.c_double)]
-    cp = C.c_char_p
-    L.shim_write_interface.argtypes = [C.c_void_p, cp, cp, C.c_int]
-    L.shim_read_interface.restype = C.c_void_p
-    L.shim_read_interface.argtypes = [cp, cp, C.c_int]
-    L.shim_check_interface.argtypes = [C.c_void_p, C.c_void_p, C.c_int, cp, C.c_int]
-    L.shim_positions.restype = C.c_longlong
-    L.shim_positions.argtypes = [C.c_void_p, C.c_int, C.c_int, ip]
-    L.shim_interface_map.restype = C.c_longlong
-    L.shim_interface_map.argtypes = [C.c_void_p, ip]
-    L.shim_pages_to_dense.argtypes = [ip, C.c_longlong, ip, C.POINTER(C.c_uint32), C.POINTER(C.c_float),
-                                      C.POINTER(C.c_uint32), C.POINTER(C.c_float), cp, C.c_int]
-    L.shim_dense_to_pages.argtypes = [ip, C.c_longlong, ip, C.POINTER(C.c_float), C.POINTER(C.c_float)]
-    L.shim_setup_digest.restype = C.c_ulonglong
-    L.shim_setup_digest.argtypes = [C.c_void_p]
-    L.shim_factor_components.restype = C.c_double
-    L.shim_factor_components.argtypes = [C.c_int, C.c_int]
-    L.shim_factor_check.restype = C.c_double
-    L.shim_factor_check.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
-    return L
+    return load_shim()
 
 
 def build(L, d, M):
@@ -128,6 +91,26 @@ def test_supernodal_factorisation_solves(shim):
                 if res < 0:
                     continue  # no interior DOFs
                 assert res < 1e-10 and diff.value < 1e-10, ("Aii", l, sd, res, diff.value)
+    finally:
+        shim.shim_free(h)
+
+
+@pytest.mark.parametrize("n,sub,radius", [(32, 8, 6), (64, 16, 12), ((40, 36, 44), 8, 6)])
+def test_solve_plan_walk_matches_the_factorisation(shim, n, sub, radius):
+    """The device solve plans' FP32 blocks Fw = [L_JJ^{-1}; -L_RJ L_JJ^{-1}],
+    solved on the host front by front with the kernels' arithmetic (FP64
+    accumulation, FP64 vectors between fronts), solve (A + 1e-5 I) x = b like
+    the FP64 factorisation itself, up to the FP32 rounding of the stored
+    coefficients and of x."""
+    d = domains.small(n, sub, radius, seed=4)
+    M = d.meta["sigma_levels"]
+    h = build(shim, d, M)
+    try:
+        nn = C.c_int()
+        for l in range(M):
+            for kind in (0, 1):
+                err = shim.shim_plan_check(h, kind, l, C.byref(nn))
+                assert 0 <= err < 2e-6, (kind, l, nn.value, err)
     finally:
         shim.shim_free(h)
 
