@@ -99,37 +99,53 @@ __device__ bool wait_at_least(const int* p, int target, const int* err, long lon
     return false;
 }
 
-// Forward solve of one small front by one warp (MQ row chunks of 32 rows).
+__device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+// Four FP64 fused multiply-adds acc[e] += v.e * x.
+__device__ __forceinline__ void fma4(double (&acc)[4], const float4 v, double x) {
+    acc[0] = fma((double)v.x, x, acc[0]);
+    acc[1] = fma((double)v.y, x, acc[1]);
+    acc[2] = fma((double)v.z, x, acc[2]);
+    acc[3] = fma((double)v.w, x, acc[3]);
+}
+
+// Fw is stored column-major with a leading dimension of round4(m) and
+// columns starting on 16-byte boundaries, so four consecutive rows of a column
+// are one 16-byte load.  Entries above the diagonal of L_JJ^{-1} and the
+// padding rows m .. round4(m) are stored zeros: a load may cover them.
+
+// Forward solve of one small front by one warp: the lane owns the row quads
+// 4 * (lane + 32 q), q < MQ.
 template <int MQ>
 __device__ __forceinline__ void warp_forward_rows(const PlanView& P, int J, int m, int nj, const double* f, int lane) {
     const size_t ld = (size_t)((m + 3) & ~3);
     const float* A = P.fw + P.fw_off[J];
-    double acc[MQ];
+    double acc[MQ][4];
 #pragma unroll
-    for (int q = 0; q < MQ; ++q) acc[q] = 0.0;
-#pragma unroll 2
-    for (int c = 0; c < nj; c += 4) {
+    for (int q = 0; q < MQ; ++q)
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-            if (c + t >= nj) break;
-            const double fc = f[c + t];
-            const float* col = A + (size_t)(c + t) * ld;
+        for (int e = 0; e < 4; ++e) acc[q][e] = 0.0;
+#pragma unroll 4
+    for (int c = 0; c < nj; ++c) {
+        const double fc = f[c];
+        const float* col = A + (size_t)c * ld;
 #pragma unroll
-            for (int q = 0; q < MQ; ++q) {
-                const int r = q * 32 + lane;
-                if (r < m && r >= c + t) acc[q] = fma((double)__ldg(col + r), fc, acc[q]);
-            }
+        for (int q = 0; q < MQ; ++q) {
+            const int r = 4 * (lane + 32 * q);
+            if (r < m && r + 3 >= c) fma4(acc[q], ldg4(col + r), fc);
         }
     }
     const int c0 = P.col0[J];
     const long long uo = P.upd_off[J];
 #pragma unroll
-    for (int q = 0; q < MQ; ++q) {
-        const int r = q * 32 + lane;
-        if (r >= m) continue;
-        if (r < nj) P.ynew[c0 + r] = acc[q];
-        else P.upd[uo + (r - nj)] = f[r] + acc[q];
-    }
+    for (int q = 0; q < MQ; ++q)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int r = 4 * (lane + 32 * q) + e;
+            if (r >= m) continue;
+            if (r < nj) P.ynew[c0 + r] = acc[q][e];
+            else P.upd[uo + (r - nj)] = f[r] + acc[q][e];
+        }
 }
 
 __device__ void warp_forward(const PlanView& P, int J, double* f, int lane, const float* b_old, int* done) {
@@ -150,19 +166,21 @@ __device__ void warp_forward(const PlanView& P, int J, double* f, int lane, cons
         for (int k = lane; k < mc; k += 32) f[rm[k]] += __ldcg(uc + k);
         __syncwarp();
     }
-    if (m <= 64) warp_forward_rows<2>(P, J, m, nj, f, lane);
-    else if (m <= 128) warp_forward_rows<4>(P, J, m, nj, f, lane);
-    else warp_forward_rows<8>(P, J, m, nj, f, lane);
+    if (m <= 128) warp_forward_rows<1>(P, J, m, nj, f, lane);
+    else warp_forward_rows<2>(P, J, m, nj, f, lane);
     __threadfence();
     __syncwarp();
     if (lane == 0) atomicAdd(done + J, 1);
 }
 
-// Backward solve of one small front by one warp: x_a = sum_{r >= a} Fw(r, a) g_r.
+// Backward solve of one small front by one warp: x_a = sum_{r >= a} Fw(r, a) g_r,
+// four columns at a time, the lane summing the row quads a + 4 lane + 128 k.
 __device__ void warp_backward(const PlanView& P, int J, double* g, int lane, float* x_old, int* done) {
     const int nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
+    const int m4 = (m + 3) & ~3;
     const int* rows = P.rows + P.rows_off[J];
     for (int i = lane; i < nj; i += 32) g[i] = P.ynew[c0 + i];   // from the forward launch
+    for (int i = m + lane; i < m4; i += 32) g[i] = 0.0;          // padding rows
     if (lane == 0) {
         const int p = P.parent[J];
         if (p >= 0 && !wait_at_least(done + p, P.ntb[p], P.err, P.spin_limit)) atomicExch(P.err, 1);
@@ -170,16 +188,22 @@ __device__ void warp_backward(const PlanView& P, int J, double* g, int lane, flo
     __syncwarp();
     for (int i = nj + lane; i < m; i += 32) g[i] = __ldcg(P.xnew + rows[i - nj]);
     __syncwarp();
-    const size_t ld = (size_t)((m + 3) & ~3);
+    const size_t ld = (size_t)m4;
     const float* A = P.fw + P.fw_off[J];
     for (int a = 0; a < nj; a += 4) {
         double s4[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 4
-        for (int r = (a & ~31) + lane; r < m; r += 32) {
-            const double gr = g[r];
+#pragma unroll 2
+        for (int r = a + 4 * lane; r < m; r += 128) {
+            const double g0 = g[r], g1 = g[r + 1], g2 = g[r + 2], g3 = g[r + 3];
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-                if (a + j < nj && r >= a + j) s4[j] = fma((double)__ldg(A + (size_t)(a + j) * ld + r), gr, s4[j]);
+                if (a + j < nj) {
+                    const float4 v = ldg4(A + (size_t)(a + j) * ld + r);
+                    s4[j] = fma((double)v.x, g0, s4[j]);
+                    s4[j] = fma((double)v.y, g1, s4[j]);
+                    s4[j] = fma((double)v.z, g2, s4[j]);
+                    s4[j] = fma((double)v.w, g3, s4[j]);
+                }
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j)
@@ -203,7 +227,7 @@ __global__ void __launch_bounds__(kNT, 5) sn_forward_kernel(PlanView P, const Sn
                                                          const float* __restrict__ b_old) {
     extern __shared__ double sh[];
     double* f = sh;                // the front's input vector, m entries
-    double* red = sh + P.max_m;    // column-slice partial sums, kNT entries
+    double* red = sh + P.max_m;    // column-slice partial sums, 4 kNT entries
     __shared__ int s_ticket, s_last;
     int* done = P.ctr + 2;
     int* chunk_ctr = P.ctr + 2 + 2 * P.nsn;
@@ -222,25 +246,29 @@ __global__ void __launch_bounds__(kNT, 5) sn_forward_kernel(PlanView P, const Sn
         }
         const int J = T.front, nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
         const int cb = P.child_ptr[J], ce = P.child_ptr[J + 1];
-        // Row lanes x column slices; each thread's first eight coefficients
-        // are requested before the dependency wait and the assembly.
-        const int mr = (T.rows + 31) & ~31;
-        const int ks = kNT / mr;
-        const int sl = tid / mr, lr = tid - sl * mr;
-        const int row = T.r0 + lr;
-        const bool active = sl < ks && lr < T.rows;
+        // Row quads x column slices: the block's rows in quads of four (one
+        // 16-byte load per column), mq quad lanes per slice, ks slices.  Each
+        // thread's first four coefficient loads are issued before the
+        // dependency wait and the assembly.
+        const int nq = (T.rows + 3) >> 2;
+        const int mq = nq <= 8 ? 8 : (nq <= 16 ? 16 : 32);
+        const int ks = kNT / mq;
+        const int sl = tid / mq, lq = tid - sl * mq;
+        const int row = T.r0 + 4 * lq;
+        const bool active = lq < nq;
         int cbeg = 0, cend = 0;
         const size_t ld = (size_t)((m + 3) & ~3);
         const float* A = P.fw + P.fw_off[J] + row;
-        float v0[8];
         if (active) {
             const int cs = (T.ncols + ks - 1) / ks;
             cbeg = T.c0 + sl * cs;
             cend = min(T.c0 + T.ncols, cbeg + cs);
-            if (row < nj) cend = min(cend, row + 1);  // L_JJ^{-1} is lower triangular
+            if (row < nj) cend = min(cend, row + 4);  // L_JJ^{-1} is lower triangular
         }
+        float4 v0[4];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) v0[u] = (cbeg + u < cend) ? __ldg(A + (size_t)(cbeg + u) * ld) : 0.0f;
+        for (int u = 0; u < 4; ++u)
+            v0[u] = (cbeg + u < cend) ? ldg4(A + (size_t)(cbeg + u) * ld) : make_float4(0.f, 0.f, 0.f, 0.f);
         // b's part of the input vector does not depend on other fronts.
         for (int i = tid; i < m; i += kNT) f[i] = (i < nj) ? (double)b_old[P.perm[c0 + i]] : 0.0;
         if (tid == 0) {
@@ -257,38 +285,51 @@ __global__ void __launch_bounds__(kNT, 5) sn_forward_kernel(PlanView P, const Sn
             for (int k = tid; k < mc; k += kNT) f[rm[k]] += __ldcg(uc + k);
             __syncthreads();
         }
-        double acc = 0.0;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
         if (active) {
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
-                if (cbeg + u < cend) acc = fma((double)v0[u], f[cbeg + u], acc);
-            int c = cbeg + 8;
-            for (; c + 8 <= cend; c += 8) {
-                float v[8];
+            for (int u = 0; u < 4; ++u)
+                if (cbeg + u < cend) fma4(acc, v0[u], f[cbeg + u]);
+            int c = cbeg + 4;
+            for (; c + 4 <= cend; c += 4) {
 #pragma unroll
-                for (int u = 0; u < 8; ++u) v[u] = __ldg(A + (size_t)(c + u) * ld);
+                for (int u = 0; u < 4; ++u) v0[u] = ldg4(A + (size_t)(c + u) * ld);
 #pragma unroll
-                for (int u = 0; u < 8; ++u) acc = fma((double)v[u], f[c + u], acc);
+                for (int u = 0; u < 4; ++u) fma4(acc, v0[u], f[c + u]);
             }
-            for (; c < cend; ++c) acc = fma((double)__ldg(A + (size_t)c * ld), f[c], acc);
+            for (; c < cend; ++c) fma4(acc, ldg4(A + (size_t)c * ld), f[c]);
         }
         if (ks > 1) {
-            if (sl < ks) red[tid] = acc;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) red[(size_t)e * kNT + tid] = acc[e];
             __syncthreads();
-            if (sl == 0 && lr < T.rows) {
-                double s2 = red[lr];
-                for (int q = 1; q < ks; ++q) s2 += red[q * mr + lr];
-                acc = s2;
+            if (sl == 0 && active) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    double s2 = red[(size_t)e * kNT + lq];
+                    for (int q = 1; q < ks; ++q) s2 += red[(size_t)e * kNT + q * mq + lq];
+                    acc[e] = s2;
+                }
             }
         }
-        const bool mine = sl == 0 && lr < T.rows;
+        const bool mine = sl == 0 && active;
+        const int rend = T.r0 + T.rows;
         if (T.nk == 1) {
             if (mine) {
-                if (row < nj) P.ynew[c0 + row] = acc;
-                else P.upd[P.upd_off[J] + (row - nj)] = f[row] + acc;
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int r = row + e;
+                    if (r >= rend) break;
+                    if (r < nj) P.ynew[c0 + r] = acc[e];
+                    else P.upd[P.upd_off[J] + (r - nj)] = f[r] + acc[e];
+                }
             }
         } else {
-            if (mine) P.part[T.part + (size_t)T.k * kRB + lr] = acc;
+            if (mine) {
+                double* pp = P.part + T.part + (size_t)T.k * kRB + 4 * lq;
+#pragma unroll
+                for (int e = 0; e < 4; ++e) pp[e] = acc[e];
+            }
             __threadfence();
             __syncthreads();
             if (tid == 0) s_last = (atomicAdd(chunk_ctr + T.chunk, 1) == T.nk - 1);
@@ -296,10 +337,15 @@ __global__ void __launch_bounds__(kNT, 5) sn_forward_kernel(PlanView P, const Sn
             if (s_last) {
                 __threadfence();
                 if (mine) {
-                    double s2 = 0.0;
-                    for (int k = 0; k < T.nk; ++k) s2 += __ldcg(P.part + T.part + (size_t)k * kRB + lr);
-                    if (row < nj) P.ynew[c0 + row] = s2;
-                    else P.upd[P.upd_off[J] + (row - nj)] = f[row] + s2;
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const int r = row + e;
+                        if (r >= rend) break;
+                        double s2 = 0.0;
+                        for (int k = 0; k < T.nk; ++k) s2 += __ldcg(P.part + T.part + (size_t)k * kRB + 4 * lq + e);
+                        if (r < nj) P.ynew[c0 + r] = s2;
+                        else P.upd[P.upd_off[J] + (r - nj)] = f[r] + s2;
+                    }
                 }
             }
         }
@@ -311,7 +357,7 @@ __global__ void __launch_bounds__(kNT, 5) sn_forward_kernel(PlanView P, const Sn
 
 __global__ void __launch_bounds__(kNT, 5) sn_backward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks,
                                                           float* __restrict__ x_old) {
-    extern __shared__ double g[];  // [y_J; x_R], m entries
+    extern __shared__ double g[];  // [y_J; x_R], m entries (+ zero padding to round4(m))
     __shared__ int s_ticket;
     int* done = P.ctr + 2 + P.nsn;
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
@@ -327,29 +373,38 @@ __global__ void __launch_bounds__(kNT, 5) sn_backward_kernel(PlanView P, const S
             continue;
         }
         const int J = T.front, nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
+        const int m4 = (m + 3) & ~3;
         const int a0 = T.r0, na = T.rows;
-        const int rs = a0 & ~31;
+        const int rs = a0;  // a multiple of kBC: the first row any column of the block needs
         const int* rows = P.rows + P.rows_off[J];
-        const size_t ld = (size_t)((m + 3) & ~3);
+        const size_t ld = (size_t)m4;
         const float* A = P.fw + P.fw_off[J];
         double s4[4] = {0.0, 0.0, 0.0, 0.0};
         const int amin = a0 + w;
-        // Rows below nj (the L_JJ^{-T} y part) need only this front's forward
-        // result, so they are summed before waiting on the parent; each lane
-        // still adds its rows in ascending order.
+        // Row quads wholly below nj (the L_JJ^{-T} y part) need only this
+        // front's forward result, so they are summed before waiting on the
+        // parent; each lane adds its quads in ascending order.
         for (int i = rs + tid; i < nj; i += kNT) g[i] = P.ynew[c0 + i];   // from the forward launch
+        for (int i = m + tid; i < m4; i += kNT) g[i] = 0.0;               // padding rows
         __syncthreads();
-        int r = (amin & ~31) + lane;
-        if (amin < a0 + na) {
-#pragma unroll 4
-            for (; r < nj; r += 32) {
-                const double gr = g[r];
+        int r = rs + 4 * lane;
+        auto quad = [&](int rr) {
+            const double g0 = g[rr], g1 = g[rr + 1], g2 = g[rr + 2], g3 = g[rr + 3];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int a = amin + 8 * j;
-                    if (a < a0 + na && r >= a) s4[j] = fma((double)__ldg(A + (size_t)a * ld + r), gr, s4[j]);
+            for (int j = 0; j < 4; ++j) {
+                const int a = amin + 8 * j;
+                if (a < a0 + na) {
+                    const float4 v = ldg4(A + (size_t)a * ld + rr);
+                    s4[j] = fma((double)v.x, g0, s4[j]);
+                    s4[j] = fma((double)v.y, g1, s4[j]);
+                    s4[j] = fma((double)v.z, g2, s4[j]);
+                    s4[j] = fma((double)v.w, g3, s4[j]);
                 }
             }
+        };
+        if (amin < a0 + na) {
+#pragma unroll 2
+            for (; r + 4 <= nj; r += 128) quad(r);
         }
         if (tid == 0) {
             const int p = P.parent[J];
@@ -359,15 +414,8 @@ __global__ void __launch_bounds__(kNT, 5) sn_backward_kernel(PlanView P, const S
         for (int i = max(rs, nj) + tid; i < m; i += kNT) g[i] = __ldcg(P.xnew + rows[i - nj]);
         __syncthreads();
         if (amin < a0 + na) {
-#pragma unroll 4
-            for (; r < m; r += 32) {
-                const double gr = g[r];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int a = amin + 8 * j;
-                    if (a < a0 + na) s4[j] = fma((double)__ldg(A + (size_t)a * ld + r), gr, s4[j]);
-                }
-            }
+#pragma unroll 2
+            for (; r < m; r += 128) quad(r);
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j)
@@ -389,8 +437,8 @@ __global__ void __launch_bounds__(kNT, 5) sn_backward_kernel(PlanView P, const S
     }
 }
 
-size_t forward_smem(int max_m) { return (size_t)std::max(max_m + kNT, kWarps * kSmallM) * sizeof(double); }
-size_t backward_smem(int max_m) { return (size_t)std::max(max_m, kWarps * kSmallM) * sizeof(double); }
+size_t forward_smem(int max_m) { return (size_t)std::max(max_m + 4 * kNT, kWarps * kSmallM) * sizeof(double); }
+size_t backward_smem(int max_m) { return (size_t)std::max((max_m + 3) & ~3, kWarps * kSmallM) * sizeof(double); }
 
 // The dynamic shared-memory limit of the two kernels only ever grows, so a
 // plan built later with smaller fronts cannot invalidate an earlier plan's
