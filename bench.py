@@ -184,12 +184,21 @@ def measured_traffic(kernel, workload):
     return None
 
 
-# PCG iterations one full solve of each workload takes in the oracle (the CPU
-# restatement of the reference dd_pcg path) at 1e-6 relative residual, from a
-# full oracle run of each workload.  A CPU sample of a few iterations is scaled
-# to one solve with it; c1 is timed as whole solves.
-ORACLE_ITERATIONS = {"c1": 12, "c2": 34, "p128": 23}
-SAMPLE_ITERATIONS = {"c1": 12, "c2": 1, "p128": 4}
+def oracle_iterations(cfg):
+    """PCG iterations of the oracle's full solve of a workload at 1e-6 relative
+    residual, with where the count comes from: the committed fixture made by
+    tests/golden/make_c2_fixture.py (a full FP32 oracle run) for c2, None for
+    workloads whose oracle samples are whole solves."""
+    if cfg == "c2":
+        path = os.path.join(ROOT, "tests", "golden", "c2_oracle.npz")
+        if os.path.exists(path):
+            return int(np.load(path)["iterations_fp32"]), "tests/golden/c2_oracle.npz (full FP32 oracle solve)"
+    return None, None
+
+
+# PCG iterations of the bounded CPU sample in the GPU arm's line: whole solves
+# where one takes seconds, else a few iterations scaled by the oracle's count.
+SAMPLE_ITERATIONS = {"c1": None, "c2": 2, "p128": 4}
 
 
 def make_oracle(d):
@@ -201,11 +210,25 @@ def make_oracle(d):
                   sigma_levels=m["sigma_levels"], sigma_smoothing=m["sigma_smoothing"], sigma_mg=m["sigma_mg"])
 
 
-def oracle_sample(o, d, iters):
-    """Seconds for `iters` PCG iterations of the oracle from x = 0."""
-    t0 = time.time()
-    o.solve(d.rhs, tol=0.0, max_it=iters, min_it=iters)
-    return time.time() - t0
+def config_dict(d, args, world=1):
+    """The workload description shared by both arms' lines."""
+    m = d.meta
+    return {"workload": d.name, "size": list(d.size), "sub_size": list(d.sub_size), "vlevels": m["vlevels"],
+            "nVcycles": m["nVcycles"], "interior_smoothing": m["interior_smoothing"],
+            "boundary_smoothing": m["boundary_smoothing"], "sigma_levels": m["sigma_levels"],
+            "sigma_smoothing": m["sigma_smoothing"], "sigma_mg": m["sigma_mg"], "tol": 1e-6,
+            "precision": args.precision, "l2": "working set > L2 (no flush)", "parallelism": f"replicas{world}"}
+
+
+def level0_updates_per_iteration(d):
+    """Level-0 stencil evaluations per PCG iteration per Active|Interface cell:
+    the Laplacian of q = A s, plus per V-cycle 2 x (boundary + interior +
+    boundary) smoothing sweeps (each computes the residual over every active
+    cell) and the residual before restriction, for the 2 x nVcycles V-cycles
+    of one preconditioner application.  Coarse levels are not counted."""
+    m = d.meta
+    per_vcycle = 2 * (2 * m["boundary_smoothing"] + m["interior_smoothing"]) + 1
+    return 1 + 2 * m["nVcycles"] * per_vcycle
 
 
 def cpu_baseline(args, d):
@@ -215,22 +238,42 @@ def cpu_baseline(args, d):
     o = make_oracle(d)
     setup_s = time.time() - t0
     iters = SAMPLE_ITERATIONS[args.config]
-    dt = oracle_sample(o, d, iters)
-    per_solve = dt / iters * ORACLE_ITERATIONS[args.config]
-    return {"value": 1.0 / per_solve, "unit": "solves/s", "cores": cores, "kind": "port",
-            "sample": (f"{iters} PCG iteration(s) of {d.name} on the oracle ({dt:.2f} s, OpenMP over "
-                       f"{cores} threads), scaled to a {ORACLE_ITERATIONS[args.config]}-iteration solve; "
-                       f"oracle setup {setup_s:.1f} s untimed")}
+    if iters is None:
+        t0 = time.time()
+        _, it, _ = o.solve(d.rhs, tol=1e-6)
+        dt = time.time() - t0
+        return {"value": 1.0 / dt, "unit": "solves/s", "cores": cores, "kind": "port",
+                "sample": (f"one whole oracle solve of {d.name} ({it} PCG iterations, {dt:.2f} s, OpenMP over "
+                           f"{cores} threads); oracle setup {setup_s:.1f} s untimed")}
+    full, src = oracle_iterations(args.config)
+    _, _, _, times = o.solve_timed(d.rhs, tol=0.0, max_it=iters, min_it=iters)
+    per_it = float(times[-1]) / iters
+    line = {"unit": "solves/s", "cores": cores, "kind": "port", "ms_per_pcg_iteration": per_it * 1e3}
+    if full is None:
+        line.update(value=None, sample=f"{iters} oracle PCG iterations of {d.name}, {per_it:.2f} s each; "
+                                       f"no full-solve count for this workload")
+        return line
+    line.update(value=1.0 / (per_it * full),
+                sample=(f"{iters} PCG iterations of {d.name} on the oracle ({per_it:.2f} s each, OpenMP over "
+                        f"{cores} threads) times the oracle's {full}-iteration solve ({src}); "
+                        f"oracle setup {setup_s:.1f} s untimed"))
+    return line
 
 
 def run_reference(args, rank):
     """The reference's CPU path (its restatement in oracle/, since the reference
-    itself cannot be built here) on this workload: each step is a bounded sample
-    of PCG iterations, scaled to solves/s by the full-solve iteration count."""
+    itself cannot be built here) on this workload, on the host cores.
+
+    One full oracle solve runs to 1e-6 relative residual, so its PCG iteration
+    count and its wall time are measured in this run; value = 1 / that solve's
+    wall time.  A step is one PCG iteration of that solve: the first `warmup`
+    iterations are warm-up, the next `steps` are the timed steps
+    (ms_per_step), and the solve then runs on, untimed, to convergence.  For
+    the 64^3 workload, whose solves take seconds, a step is a whole solve."""
     if rank != 0:
         return
-    if args.config not in ORACLE_ITERATIONS:
-        print(json.dumps({"impl": "reference", "unavailable": f"no bounded oracle sample is defined for "
+    if args.config not in ("c1", "c2", "p128"):
+        print(json.dumps({"impl": "reference", "unavailable": f"no bounded oracle run is defined for "
                           f"{args.config}: its oracle setup alone takes from tens of minutes to hours"}),
               flush=True)
         return
@@ -238,25 +281,32 @@ def run_reference(args, rank):
     cores = os.cpu_count() or 1
     t0 = time.time()
     o = make_oracle(d)
-    print(f"[bench reference] {d.name}: oracle setup {time.time() - t0:.1f} s", file=sys.stderr, flush=True)
-    iters = SAMPLE_ITERATIONS[args.config]
-    for _ in range(args.warmup):
-        oracle_sample(o, d, iters)
-    times = [oracle_sample(o, d, iters) for _ in range(args.steps)]
-    per_solve = [t / iters * ORACLE_ITERATIONS[args.config] for t in times]
-    v = len(per_solve) / sum(per_solve)
-    lat = np.sort(np.array(per_solve) * 1000.0)
+    setup_s = time.time() - t0
+    print(f"[bench reference] {d.name}: oracle setup {setup_s:.1f} s", file=sys.stderr, flush=True)
+    whole_solves = args.config == "c1"
+    durations, solves = [], []
+    while len(durations) < args.warmup + args.steps:
+        t1 = time.time()
+        _, it, info, times = o.solve_timed(d.rhs, tol=1e-6, max_it=2000)
+        solves.append((time.time() - t1, it, info))
+        durations.extend([solves[-1][0]] if whole_solves else list(np.diff(np.concatenate([[0.0], times]))))
+    timed = np.array(durations[args.warmup:args.warmup + args.steps])
+    solve_s, its, info = solves[0]
+    v = 1.0 / solve_s
+    step = "one whole oracle solve" if whole_solves else (
+        f"one PCG iteration of a full oracle solve: iterations {args.warmup + 1}..{args.warmup + args.steps} of "
+        f"the solve are the timed steps, the first {args.warmup} warm-up")
     line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": 0, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": float(np.mean(per_solve)) * 1000.0, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": d.name, "size": list(d.size), "sub_size": list(d.sub_size),
-                       "vlevels": d.meta["vlevels"], "sigma_levels": d.meta["sigma_levels"], "tol": 1e-6},
-            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "warmup": args.warmup, "ms_per_step": float(timed.mean()) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": config_dict(d, args),
+            "step": step, "iterations": int(its), "iterations_measured_in_run": True,
+            "solve_s": solve_s, "ms_per_pcg_iteration": solve_s / max(its, 1) * 1e3,
+            "true_residual_inf": float(info["true_res_inf"] / info["b_inf"]),
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
-                             "sample": (f"each step: {iters} PCG iteration(s) of {d.name} on the oracle "
-                                        f"(OpenMP, {cores} threads), scaled to a "
-                                        f"{ORACLE_ITERATIONS[args.config]}-iteration solve")},
+                             "sample": (f"one full oracle solve of {d.name} ({its} PCG iterations measured in this "
+                                        f"run, {solve_s:.1f} s, OpenMP over {cores} threads); oracle setup "
+                                        f"{setup_s:.1f} s untimed")},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -486,6 +536,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from hierarchicaldd_b200 import _lib
+    from hierarchicaldd_b200.domains import ACTIVE
     from hierarchicaldd_b200.solver import SPGrid_Domain_Decomposition_Solver
 
     d = workload(args.config)
@@ -580,17 +631,23 @@ def main():
 
     its = [r["iterations"] for r in res]
     lat = np.sort(dev_ms)
+    # Active|Interface cells after the divider = the caller's Active cells.
+    n_solve = int(np.count_nonzero(d.flags & ACTIVE))
+    it0 = its[0] if its else 0
+    updates = n_solve * level0_updates_per_iteration(d) * it0
+    o_its, o_src = oracle_iterations(args.config)
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": d.name, "size": list(d.size), "sub_size": list(d.sub_size),
-                   "vlevels": m["vlevels"], "interior_smoothing": m["interior_smoothing"],
-                   "boundary_smoothing": m["boundary_smoothing"], "sigma_levels": m["sigma_levels"],
-                   "sigma_smoothing": m["sigma_smoothing"], "sigma_mg": m["sigma_mg"],
-                   "tol": 1e-6, "precision": args.precision, "l2": "working set > L2 (no flush)",
-                   "parallelism": f"replicas{world}"},
-        "iterations": its[0] if its else None,
+        "config": config_dict(d, args, world),
+        "iterations": it0, "oracle_iterations": o_its, "oracle_iterations_source": o_src,
+        "ms_per_pcg_iteration": total_ms / args.steps / max(it0, 1),
+        "cell_updates_per_s": world * updates / (total_ms / args.steps * 1e-3),
+        "cell_updates_definition": (f"level-0 stencil evaluations: {n_solve} Active|Interface cells x "
+                                    f"{level0_updates_per_iteration(d)} per PCG iteration (1 Laplacian + "
+                                    f"2 x nVcycles x (2 x (2 boundary + interior) sweeps + 1 residual)) x "
+                                    f"{it0} iterations per solve; coarse levels not counted"),
         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
         "true_residual_inf": res[-1]["true_residual_inf"] if res else None,
         "setup_s": setup_s, "setup_phases_s": setup_phases,
@@ -605,7 +662,7 @@ def main():
         "kernels": per_kernel,
         "clocks": clk.summary(),
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.config in ORACLE_ITERATIONS:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.config in SAMPLE_ITERATIONS:
         try:
             line["cpu_baseline"] = cpu_baseline(args, d)
         except Exception as e:  # reported, not fatal

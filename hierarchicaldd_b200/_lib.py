@@ -20,6 +20,8 @@ STATUS_NAMES = {
 }
 PRECISION_REFERENCE = 0
 PRECISION_MIXED = 1
+COARSE_REFERENCE = 0
+COARSE_EXACT = 1
 # Initialize_Preconditioner's iomode (reference Test_Bench -iomode).
 IOMODES = {"neither": 0, "output": 1, "input": 2}
 
@@ -30,7 +32,7 @@ class hdd_options(C.Structure):
         ("interior_smoothing", C.c_int), ("boundary_smoothing", C.c_int), ("sigma_levels", C.c_int),
         ("sigma_smoothing", C.c_int), ("sigma_mg", C.c_int), ("tol", C.c_double), ("relative_tol", C.c_int),
         ("max_iters", C.c_int), ("min_iters", C.c_int), ("precision_mode", C.c_int),
-        ("true_residual_every", C.c_int), ("device", C.c_int),
+        ("true_residual_every", C.c_int), ("device", C.c_int), ("coarse_solve", C.c_int),
     ]
 
 
@@ -70,6 +72,7 @@ SIGNATURES = {
     "hdd_set_rhs_dense": (C.c_int, [_vp, _fp]),
     "hdd_solve": (C.c_int, [_vp, C.POINTER(hdd_result)]),
     "hdd_get_solution_dense": (C.c_int, [_vp, _fp]),
+    "hdd_get_solution_dense_f64": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "hdd_get_residual_history": (C.c_int, [_vp, C.POINTER(C.c_double), C.c_int, _ip]),
     "hdd_apply_preconditioner_dense": (C.c_int, [_vp, _fp, _fp]),
     "hdd_vcycle_dense": (C.c_int, [_vp, _fp, _fp, C.c_int]),
@@ -82,6 +85,7 @@ SIGNATURES = {
     "hdd_interface_matrix": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _ip, _ip, _ip, _ip, _ip,
                                        C.POINTER(C.c_double)]),
     "hdd_kernel_launch_count": (C.c_int, [_vp, C.POINTER(C.c_longlong)]),
+    "hdd_get_pcg_coefficients": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, _ip]),
     "hdd_set_wait_limit": (C.c_int, [_vp, C.c_longlong]),
     "hdd_test_stall_dependency": (C.c_int, [_vp, C.c_int]),
     "hdd_get_setup_timing": (C.c_int, [_vp, C.POINTER(C.c_double)]),

@@ -37,6 +37,22 @@ hdd_status guard(hdd_solver* s, F&& f) {
     }
 }
 
+// Makes `device` current for its lifetime and restores the calling thread's
+// previous device afterwards (also when an exception leaves the scope).
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int device) {
+        hdd::cuda_check(cudaGetDevice(&prev), "cudaGetDevice");
+        if (prev != device) hdd::cuda_check(cudaSetDevice(device), "cudaSetDevice");
+        else prev = -1;
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 // Reads the reference SPGrid directory format (SPGRID_READ_WRITE.h:31-106):
 // `size` = d ints, `block_offset` = int count + PhysBAM array (int length +
 // uint64 page offsets), `flags`/`data` = per block a PhysBAM array of 256
@@ -78,6 +94,7 @@ void hdd_options_default(hdd_options* o) {
     o->precision_mode = HDD_PRECISION_REFERENCE;
     o->true_residual_every = 20;
     o->device = 0;
+    o->coarse_solve = HDD_COARSE_REFERENCE;
 }
 
 hdd_status hdd_create(const hdd_options* opts, hdd_solver** out) {
@@ -207,6 +224,11 @@ hdd_status hdd_get_solution_dense(hdd_solver* s, float* x) {
     return guard(s, [&](Solver& v) { v.get_solution(x); });
 }
 
+hdd_status hdd_get_solution_dense_f64(hdd_solver* s, double* x) {
+    if (!x) return HDD_ERR_INVALID_ARGUMENT;
+    return guard(s, [&](Solver& v) { v.get_solution_f64(x); });
+}
+
 hdd_status hdd_get_residual_history(hdd_solver* s, double* out, int capacity, int* n) {
     if (!n || capacity < 0 || (capacity > 0 && !out)) return HDD_ERR_INVALID_ARGUMENT;
     return guard(s, [&](Solver& v) {
@@ -255,7 +277,9 @@ hdd_status hdd_multiply_dot_dense_device_noalloc(hdd_solver* s, const float* x, 
     if (!x || !y || !dot) return HDD_ERR_INVALID_ARGUMENT;
     return guard(s, [&](Solver& v) {
         if (!v.initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
-        hdd::cuda_check(cudaSetDevice(v.opts.device), "cudaSetDevice");
+        // The caller's thread may be working on another device: switch for
+        // the launch and switch back on every exit path.
+        DeviceGuard dg(v.opts.device);
         hdd::multiply_dot_dense_device_noalloc(v.geom(), v.tile_xyz.p, v.L.opt.size, v.opts.device, x, y, dot,
                                                static_cast<cudaStream_t>(stream));
         v.count(2);
@@ -352,6 +376,15 @@ hdd_status hdd_test_stall_dependency(hdd_solver* s, int on) {
         if (!v.initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
         hdd::cuda_check(cudaSetDevice(v.opts.device), "cudaSetDevice");
         v.sigma.stall_dependency(on != 0, v.stream);
+    });
+}
+
+hdd_status hdd_get_pcg_coefficients(hdd_solver* s, double* alpha, double* beta, int capacity, int* n) {
+    if (!n || capacity < 0 || (capacity > 0 && (!alpha || !beta))) return HDD_ERR_INVALID_ARGUMENT;
+    return guard(s, [&](Solver& v) {
+        if (!v.solved) throw Error(HDD_ERR_NOT_INITIALIZED, "no solve has run");
+        *n = (int)v.alphas.size();
+        for (int i = 0; i < capacity && i < *n; ++i) { alpha[i] = v.alphas[i]; beta[i] = v.betas[i]; }
     });
 }
 

@@ -1,10 +1,10 @@
 // Interface system assembly (host, parallel over subdomains).
 //
 // Restates CPU/Interface_Solver/INTERFACE_MATRIX_GENERATOR.h:130-735 with its
-// helpers STRIDE_GENERATOR.h:70-101, CELL_PROLONGATION_BAKER.h:125-152,
-// GALERKIN_PROCESS.h:183-224 and PROLONGATION_MATRIX_HELPER.cpp:268-294, and
+// helpers STRIDE_GENERATOR.h:23-54, CELL_PROLONGATION_BAKER.h:22-50,
+// GALERKIN_PROCESS.h:27-69 and PROLONGATION_MATRIX_HELPER.cpp:13-40, and
 // the subdomain flag extraction of SPGrid_Subdomain_Splitter.h:123-154 /
-// SPGrid_Subdomain_Rasterizer.h:253-300.
+// SPGrid_Subdomain_Rasterizer.h:59-136.
 //
 // Data structures differ from the reference: every subdomain works on dense
 // box-local arrays per hierarchy level instead of SPGrid allocators and hash

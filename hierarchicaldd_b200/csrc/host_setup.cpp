@@ -16,12 +16,12 @@ static inline bool in3(const int n[3], int i, int j, int k) {
 }
 
 void number_of_subdomains(const int size[3], const int sub[3], int out[3]) {
-    // SPGrid_Domain_Divider_Helper.h:192-196 (origin 0).
+    // SPGrid_Domain_Divider_Helper.h:31-35 (origin 0).
     for (int a = 0; a < 3; ++a) out[a] = (size[a] - 1) / sub[a] + (((size[a] - 1) % sub[a]) ? 1 : 0);
 }
 
 void divide_domain(const int size[3], const int sub[3], uint32_t* f) {
-    // SPGrid_Domain_Divider_Helper.h:210-241: Active cells on planes index % sub == 0
+    // SPGrid_Domain_Divider_Helper.h:49-74: Active cells on planes index % sub == 0
     // become Interface; the others carry the 1-based partition id.
     int ns[3];
     number_of_subdomains(size, sub, ns);
@@ -53,7 +53,7 @@ void flag_faces(const int n[3], uint32_t* f) {
 }
 
 void flag_boundary(const int n[3], uint32_t* f) {
-    // SPGrid_Flag_Boundary_Helper.h:238-307: Active cells within Manhattan
+    // SPGrid_Flag_Boundary_Helper.h:40-109: Active cells within Manhattan
     // distance 3 of an exterior (flag 0, or outside the grid), Interface or
     // Dirichlet cell are Boundary.  Computed as a separable distance transform.
     const size_t N = (size_t)n[0] * n[1] * n[2];
@@ -102,7 +102,14 @@ void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& L) {
     for (int a = 0; a < 3; ++a) {
         if (opt.size[a] < 3) throw Error(HDD_ERR_INVALID_ARGUMENT, "size must be >= 3 on every axis");
         int s = opt.sub[a];
-        if (s < 4 || (s & (s - 1))) throw Error(HDD_ERR_UNSUPPORTED, "sub_size must be a power of two >= 4");
+        // The resident V-cycle keeps a subdomain's levels on chip: one CTA for
+        // 8^3 and 16^3 boxes, a 4-CTA cluster for 32^3.  A 64^3 box (the
+        // reference Test_Bench default, CPU/Test_Bench_3D/main.cpp:247) needs
+        // 64^3 x 8 B of level-0 state, more than a 16-CTA cluster's shared
+        // memory, and 4^3 boxes have no coarse level worth a launch; both are
+        // refused here, before any setup work.
+        if (s != 8 && s != 16 && s != 32)
+            throw Error(HDD_ERR_UNSUPPORTED, "sub_size must be 8, 16 or 32 (got " + std::to_string(s) + ")");
         if ((s >> (opt.vlevels - 1)) < 2)
             throw Error(HDD_ERR_INVALID_ARGUMENT, "vlevels too deep for sub_size (needs sub_size >> (vlevels-1) >= 2)");
     }

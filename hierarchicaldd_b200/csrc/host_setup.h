@@ -4,7 +4,7 @@
 // Layout.  The grid is cut into tiles of sub_size cells per axis; tile t holds
 // cells [t*sub, (t+1)*sub) per axis, z fastest inside a tile.  Tile k coincides
 // with the reference's subdomain box k ([k*sub, (k+1)*sub], inclusive,
-// SPGrid_Domain_Divider_Helper.h:197-201) minus its upper interface planes,
+// SPGrid_Domain_Divider_Helper.h:36-40) minus its upper interface planes,
 // which are the lower planes of tiles k+1.  Only tiles holding Active or
 // Interface cells are stored; absent tiles read as zero.
 #pragma once

@@ -66,15 +66,21 @@ cudaError_t launch_project_dot(const TileGeom& g, float* a, const float* b, doub
 // s = beta*s + z (first: s = z); beta from scalars (mode 0 float, 1 double).
 cudaError_t launch_update_s(const TileGeom& g, float* s, const float* z, const PcgScalars* sc, int first,
                             int mode, cudaStream_t stream);
-// x += alpha s; r -= alpha q; partial max|r| per tile.
+// x += alpha s; r -= alpha q; partial max|r| per tile.  With xd (mode 1) the
+// iterate is kept in FP64 (xd += alpha s) and x is its FP32 rounding.
 cudaError_t launch_update_xr(const TileGeom& g, float* x, float* r, const float* s, const float* q,
-                             const PcgScalars* sc, int mode, float* partial_max, cudaStream_t stream);
+                             const PcgScalars* sc, int mode, float* partial_max, cudaStream_t stream,
+                             double* xd = nullptr);
+// r = Project((float)(b - A x)) for an FP64 iterate x, in FP64; partial max|r|.
+cudaError_t launch_residual_f64(const TileGeom& g, const float* b, const double* x, float* r, float* partial_max,
+                                cudaStream_t stream);
 // Scalar steps (single thread).
 cudaError_t launch_scalar_rho(PcgScalars* sc, const double* rho_sum, int first, cudaStream_t stream);
 cudaError_t launch_scalar_alpha(PcgScalars* sc, const double* sdq_sum, cudaStream_t stream);
-// r = Project(b - A x); partial max|r|.
+// r = Project(b - A x); partial max|r|.  precise = 1 subtracts A x in FP64
+// before rounding r (else A x is rounded to FP32 first, as the reference).
 cudaError_t launch_residual(const TileGeom& g, const float* b, const float* x, float* r, float* partial_max,
-                            cudaStream_t stream);
+                            cudaStream_t stream, int precise = 0);
 // v = Project(v).
 cudaError_t launch_project(const TileGeom& g, float* v, cudaStream_t stream);
 // Dense (x-slowest grid of size[0..2]) <-> tiled copies on the device;
@@ -83,6 +89,8 @@ cudaError_t launch_dense_to_tiles(const TileGeom& g, const int* tile_xyz, int sx
                                   float* tiled, cudaStream_t stream);
 cudaError_t launch_tiles_to_dense(const TileGeom& g, const int* tile_xyz, int sx, int sy, int sz, const float* tiled,
                                   float* dense, cudaStream_t stream);
+cudaError_t launch_tiles_to_dense_f64(const TileGeom& g, const int* tile_xyz, int sx, int sy, int sz,
+                                      const double* tiled, double* dense, cudaStream_t stream);
 
 // ---------------------------------------------------------------------------
 // Interface coupling (Laplace_ri gather and the interface scatter)

@@ -22,8 +22,8 @@ namespace {
 constexpr int kNT = 256;
 
 // Value of the face neighbour `face` of local cell (x,y,z) of tile t.
-__device__ __forceinline__ float nb_value(const TileGeom& g, const float* v, int t, int x, int y, int z,
-                                          int face) {
+template <class V>
+__device__ __forceinline__ V nb_value(const TileGeom& g, const V* v, int t, int x, int y, int z, int face) {
     const int S = g.sub;
     int nx = x, ny = y, nz = z, tt = t;
     switch (face) {
@@ -34,12 +34,13 @@ __device__ __forceinline__ float nb_value(const TileGeom& g, const float* v, int
         case 4: if (z > 0) nz = z - 1; else { tt = g.nbr[6 * t + 4]; nz = S - 1; } break;
         default: if (z < S - 1) nz = z + 1; else { tt = g.nbr[6 * t + 5]; nz = 0; } break;
     }
-    if (tt < 0) return 0.0f;
+    if (tt < 0) return V(0);
     return v[(size_t)tt * S * S * S + (nx * S + ny) * S + nz];
 }
 
-__device__ __forceinline__ double laplace_cell(const TileGeom& g, const float* v, int t, int x, int y, int z,
-                                               uint32_t fl, float c) {
+template <class V>
+__device__ __forceinline__ double laplace_cell(const TileGeom& g, const V* v, int t, int x, int y, int z,
+                                               uint32_t fl, V c) {
     const double cd = (double)c;
     double result = 0.0;
 #pragma unroll
@@ -96,9 +97,12 @@ __global__ void __launch_bounds__(kNT) laplace_dot_kernel(TileGeom g, const floa
     if (threadIdx.x == 0) partial[t] = acc;
 }
 
+// precise = 0: r = b - (float)(A x), the reference's float subtraction;
+// precise = 1: r = (float)(b - A x) with A x kept in FP64 (the FP64 true
+// residual of the precision form).
 __global__ void __launch_bounds__(kNT) residual_kernel(TileGeom g, const float* __restrict__ b,
                                                        const float* __restrict__ x, float* __restrict__ r,
-                                                       float* partial_max) {
+                                                       float* partial_max, int precise) {
     const int t = blockIdx.x;
     const int S = g.sub, TC = S * S * S;
     const size_t base = (size_t)t * TC;
@@ -108,8 +112,31 @@ __global__ void __launch_bounds__(kNT) residual_kernel(TileGeom g, const float* 
         float out = 0.0f;
         if (fl & (C_ACTIVE | C_INTERFACE)) {
             const int z = c % S, tmp = c / S, y = tmp % S, xx = tmp / S;
-            const float ax = (float)laplace_cell(g, x, t, xx, y, z, fl, x[base + c]);
-            out = __fsub_rn(b[base + c], ax);
+            const double axd = laplace_cell(g, x, t, xx, y, z, fl, x[base + c]);
+            out = precise ? (float)((double)b[base + c] - axd) : __fsub_rn(b[base + c], (float)axd);
+        }
+        r[base + c] = out;
+        m = fmaxf(m, fabsf(out));
+    }
+    m = block_max(m);
+    if (threadIdx.x == 0) partial_max[t] = m;
+}
+
+// r = (float)(b - A x) for an FP64 iterate x (the precision form's true
+// residual), FP64 throughout; partial max|r|.
+__global__ void __launch_bounds__(kNT) residual_f64_kernel(TileGeom g, const float* __restrict__ b,
+                                                           const double* __restrict__ x, float* __restrict__ r,
+                                                           float* partial_max) {
+    const int t = blockIdx.x;
+    const int S = g.sub, TC = S * S * S;
+    const size_t base = (size_t)t * TC;
+    float m = 0.0f;
+    for (int c = threadIdx.x; c < TC; c += kNT) {
+        const uint32_t fl = g.flags[base + c];
+        float out = 0.0f;
+        if (fl & (C_ACTIVE | C_INTERFACE)) {
+            const int z = c % S, tmp = c / S, y = tmp % S, xx = tmp / S;
+            out = (float)((double)b[base + c] - laplace_cell(g, x, t, xx, y, z, fl, x[base + c]));
         }
         r[base + c] = out;
         m = fmaxf(m, fabsf(out));
@@ -154,9 +181,12 @@ __global__ void __launch_bounds__(kNT) update_s_kernel(size_t n, float* __restri
     }
 }
 
+// xd (mode 1, optional): the FP64 iterate, updated as xd += alpha s with x
+// its FP32 rounding.
 __global__ void __launch_bounds__(kNT) update_xr_kernel(int TC, float* __restrict__ x, float* __restrict__ r,
                                                         const float* __restrict__ s, const float* __restrict__ q,
-                                                        const PcgScalars* sc, int mode, float* partial_max) {
+                                                        const PcgScalars* sc, int mode, float* partial_max,
+                                                        double* __restrict__ xd) {
     const int t = blockIdx.x;
     const size_t base = (size_t)t * TC;
     const float alpha = sc->alpha;
@@ -168,6 +198,11 @@ __global__ void __launch_bounds__(kNT) update_xr_kernel(int TC, float* __restric
         if (mode == 0) {
             xv = __fadd_rn(__fmul_rn(s[i], alpha), x[i]);
             rv = __fadd_rn(__fmul_rn(q[i], -alpha), r[i]);
+        } else if (xd) {
+            const double xn = xd[i] + alpha_d * (double)s[i];
+            xd[i] = xn;
+            xv = (float)xn;
+            rv = (float)((double)r[i] - alpha_d * (double)q[i]);
         } else {
             xv = (float)((double)x[i] + alpha_d * (double)s[i]);
             rv = (float)((double)r[i] - alpha_d * (double)q[i]);
@@ -237,8 +272,9 @@ __global__ void __launch_bounds__(kNT) interface_scatter_kernel(const long long*
     if (i < n) z[slot[i]] = u0[i];
 }
 
+template <class V>
 __global__ void __launch_bounds__(kNT) dense_tiles_kernel(int S, const int* tile_xyz, int sx, int sy, int sz,
-                                                          const float* __restrict__ src, float* __restrict__ dst,
+                                                          const V* __restrict__ src, V* __restrict__ dst,
                                                           int to_tiles) {
     const int t = blockIdx.x, TC = S * S * S;
     const int ox = tile_xyz[3 * t] * S, oy = tile_xyz[3 * t + 1] * S, oz = tile_xyz[3 * t + 2] * S;
@@ -247,7 +283,7 @@ __global__ void __launch_bounds__(kNT) dense_tiles_kernel(int S, const int* tile
         const int gx = ox + x, gy = oy + y, gz = oz + z;
         const bool in = gx < sx && gy < sy && gz < sz;
         const size_t di = ((size_t)gx * sy + gy) * sz + gz, ti = (size_t)t * TC + c;
-        if (to_tiles) dst[ti] = in ? src[di] : 0.0f;
+        if (to_tiles) dst[ti] = in ? src[di] : V(0);
         else if (in) dst[di] = src[ti];
     }
 }
@@ -267,14 +303,28 @@ cudaError_t launch_tiles_to_dense(const TileGeom& g, const int* txyz, int sx, in
     return cudaGetLastError();
 }
 
+cudaError_t launch_tiles_to_dense_f64(const TileGeom& g, const int* txyz, int sx, int sy, int sz, const double* tiled,
+                                      double* dense, cudaStream_t st) {
+    if (g.ntiles == 0) return cudaSuccess;
+    dense_tiles_kernel<<<g.ntiles, kNT, 0, st>>>(g.sub, txyz, sx, sy, sz, tiled, dense, 0);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_laplace_dot(const TileGeom& g, const float* s, float* q, double* partial, cudaStream_t st) {
     if (g.ntiles == 0) return cudaSuccess;
     laplace_dot_kernel<<<g.ntiles, kNT, 0, st>>>(g, s, q, partial);
     return cudaGetLastError();
 }
-cudaError_t launch_residual(const TileGeom& g, const float* b, const float* x, float* r, float* pm, cudaStream_t st) {
+cudaError_t launch_residual(const TileGeom& g, const float* b, const float* x, float* r, float* pm, cudaStream_t st,
+                            int precise) {
     if (g.ntiles == 0) return cudaSuccess;
-    residual_kernel<<<g.ntiles, kNT, 0, st>>>(g, b, x, r, pm);
+    residual_kernel<<<g.ntiles, kNT, 0, st>>>(g, b, x, r, pm, precise);
+    return cudaGetLastError();
+}
+cudaError_t launch_residual_f64(const TileGeom& g, const float* b, const double* x, float* r, float* pm,
+                                cudaStream_t st) {
+    if (g.ntiles == 0) return cudaSuccess;
+    residual_f64_kernel<<<g.ntiles, kNT, 0, st>>>(g, b, x, r, pm);
     return cudaGetLastError();
 }
 cudaError_t launch_project_dot(const TileGeom& g, float* a, const float* b, double* partial, cudaStream_t st) {
@@ -297,9 +347,9 @@ cudaError_t launch_update_s(const TileGeom& g, float* s, const float* z, const P
     return cudaGetLastError();
 }
 cudaError_t launch_update_xr(const TileGeom& g, float* x, float* r, const float* s, const float* q,
-                             const PcgScalars* sc, int mode, float* pm, cudaStream_t st) {
+                             const PcgScalars* sc, int mode, float* pm, cudaStream_t st, double* xd) {
     if (g.ntiles == 0) return cudaSuccess;
-    update_xr_kernel<<<g.ntiles, kNT, 0, st>>>(g.sub * g.sub * g.sub, x, r, s, q, sc, mode, pm);
+    update_xr_kernel<<<g.ntiles, kNT, 0, st>>>(g.sub * g.sub * g.sub, x, r, s, q, sc, mode, pm, xd);
     return cudaGetLastError();
 }
 cudaError_t launch_reduce_sum(const double* partial, int n, double* out, cudaStream_t st) {

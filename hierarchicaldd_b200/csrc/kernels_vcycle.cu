@@ -10,7 +10,7 @@
 // Arithmetic follows the reference's float operation order with explicit
 // round-to-nearest intrinsics, so no multiply-add is contracted:
 //   residual   r = b - sum_faces (u_n - u_c)      (SPGrid_Residual_Legacy.h:52-61)
-//   correction u += (omega/face_count) * r        (SPGrid_Correction_Legacy.h:161-191)
+//   correction u += (omega/face_count) * r        (SPGrid_Correction_Legacy.h:47-80)
 //   restriction, prolongation weights and order  (SPGrid_Restriction_Legacy.h:47-186,
 //                                                 SPGrid_Prolongation_Legacy.h:46-128)
 // Smoothing is Jacobi: every residual of a sweep is computed from the old u

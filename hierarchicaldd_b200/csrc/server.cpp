@@ -62,9 +62,10 @@ struct Request {
 
 // Device footprint estimate made before the setup: the dense staging buffer
 // (4 B per grid cell), six PCG vectors plus flags over the stored tiles
-// (26 B per tile cell), the V-cycle level flags (about 1.2 B per tile cell)
-// and the interface solver's factors and vectors (48 B per Active cell, an
-// upper estimate from the 64^3..256^3 sphere domains).
+// (26 B per tile cell, 8 B more for the FP64 iterate of the precision form),
+// the V-cycle level flags (about 1.2 B per tile cell) and the interface
+// solver's factors and FP64 vectors (56 B per Active cell, an upper estimate
+// from the 64^3..256^3 sphere domains).
 long long estimate_bytes(const hdd_options& o, const uint32_t* flags) {
     const long long n0 = o.size[0], n1 = o.size[1], n2 = o.size[2];
     const int s = std::max(1, o.sub_size[0]);
@@ -81,7 +82,8 @@ long long estimate_bytes(const hdd_options& o, const uint32_t* flags) {
     long long tiles = 0;
     for (uint8_t u : used) tiles += u;
     const long long tile_cells = tiles * s * s * s;
-    return 4 * n0 * n1 * n2 + 28 * tile_cells + 48 * active + (16ll << 20);
+    const long long per_tile_cell = o.precision_mode == HDD_PRECISION_MIXED ? 36 : 28;
+    return 4 * n0 * n1 * n2 + per_tile_cell * tile_cells + 56 * active + (16ll << 20);
 }
 
 }  // namespace

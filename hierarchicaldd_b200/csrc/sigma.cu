@@ -1,7 +1,7 @@
 // Device-side sigma (interface Schur complement) V-cycle, sm_100a.
 //
-// Restates CPU/Interface_Solver/SIGMA_MULTIGRID_SOLVER.cpp:70-82 and
-// SIGMA_SMOOTHER.cpp:418-478 on the GPU:
+// Restates CPU/Interface_Solver/SIGMA_MULTIGRID_SOLVER.cpp:35-47 and
+// SIGMA_SMOOTHER.cpp:290-352 on the GPU:
 //   Smooth:   u <- (Arr+eps)^{-1} (b + sum_s Air_s^T (Aii_s+eps)^{-1} Air_s u)
 //   Residual: r <- b + sum_s Air_s^T (Aii_s+eps)^{-1} Air_s u - Arr u
 // * Every SpMV is a row-per-thread CSR walk in a fixed order (the transposed
@@ -10,7 +10,7 @@
 // * The PARDISO solves are supernodal triangular solves over nested-dissection
 //   fronts (sn_solve.cu): one persistent launch per solve direction walks the
 //   fronts in dependency order.
-// * The coarsest level's 200 smoothing steps (SIGMA_MULTIGRID_SOLVER.cpp:78)
+// * The coarsest level's 200 smoothing steps (SIGMA_MULTIGRID_SOLVER.cpp:43)
 //   form a contraction whose fixed point is the Schur complement solve
 //   S^{-1} b with S = Arr+eps - sum_s Air_s^T (Aii_s+eps)^{-1} Air_s; setup
 //   estimates the contraction factor rho.  When rho^200 <= 1e-7 the steps
@@ -138,7 +138,7 @@ void SigmaGpu::release() {
     device_bytes = 0;
 }
 
-void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStream_t s) {
+void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStream_t s, bool force_exact) {
     release();
     const bool verbose = std::getenv("HDD_VERBOSE") != nullptr;
     auto t_start = std::chrono::steady_clock::now();
@@ -221,7 +221,7 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
             device_bytes += L.aii.bytes + L.arr_solve.bytes;
             stamp("device plans", l);
         } else {
-            // Coarsest level.  The 200 smoothing steps (SIGMA_MULTIGRID_SOLVER.cpp:78)
+            // Coarsest level.  The 200 smoothing steps (SIGMA_MULTIGRID_SOLVER.cpp:43)
             // contract towards u = S^{-1} b, S = (Arr+eps) - sum_s Air_s^T (Aii_s+eps)^{-1} Air_s;
             // estimate the contraction factor on the host first.
             const int nb = L.n_iface;
@@ -252,10 +252,11 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
                     xv.swap(yv);
                 }
                 bottom_contraction = rho;
-                bottom_exact = std::pow(rho, 200.0) <= 1e-7;
+                bottom_exact = force_exact || std::pow(rho, 200.0) <= 1e-7;
                 if (verbose)
                     std::fprintf(stderr, "[hdd setup] coarsest sigma smoother: rho %.4f, %s\n", rho,
-                                 bottom_exact ? "exact Schur solve" : "200 literal smoothing steps");
+                                 bottom_exact ? (force_exact ? "exact Schur solve (requested)" : "exact Schur solve")
+                                              : "200 literal smoothing steps");
             }
             if (!bottom_exact) {
                 // The 200 steps have not converged to S^{-1} b: run them as the

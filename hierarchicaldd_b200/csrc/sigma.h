@@ -75,7 +75,7 @@ struct NoInitAlloc : std::allocator<T> {
 using BlockVec = std::vector<double, NoInitAlloc<double>>;
 
 // Supernodal Cholesky of (A + eps I) (zero rows get eps), the stand-in for
-// the reference's MKL PARDISO phases 11/22 (SIGMA_SMOOTHER.cpp:241-414).
+// the reference's MKL PARDISO phases 11/22 (SIGMA_SMOOTHER.cpp:115-288).
 // Supernodes are the fronts of a nested-dissection separator tree.
 struct SnFactor {
     int n = 0;
@@ -227,14 +227,16 @@ struct SigmaGpu {
     // True when 200 bottom smoothing steps have converged to S^{-1} b (rho^200 <=
     // 1e-7), so the coarsest level is one solve of K; false runs the 200 steps.
     bool bottom_exact = true;
-    static constexpr int kBottomSmoothing = 200;  // SIGMA_MULTIGRID_SOLVER.cpp:78
+    static constexpr int kBottomSmoothing = 200;  // SIGMA_MULTIGRID_SOLVER.cpp:43
     size_t device_bytes = 0;
     // Error word shared by every solve plan of this solver: nonzero once a
     // bounded wait gave up (then later waits return at once).
     int* d_err = nullptr;
-    void setup(const InterfaceHost& ih, int smoothing_iterations, cudaStream_t s);
+    // force_exact: solve the coarsest level exactly even where the 200
+    // smoothing steps have not converged (HDD_COARSE_EXACT).
+    void setup(const InterfaceHost& ih, int smoothing_iterations, cudaStream_t s, bool force_exact = false);
     void release();
-    // u[0] = sigma V-cycle(b[0]) (SIGMA_MULTIGRID_SOLVER.cpp:70-82), u[0] starting at 0.
+    // u[0] = sigma V-cycle(b[0]) (SIGMA_MULTIGRID_SOLVER.cpp:35-47), u[0] starting at 0.
     void vcycle(cudaStream_t s, long long& launches, PhaseHook* hook = nullptr);
     // Nonzero when a bounded wait inside a supernodal solve gave up.
     int error_flag(cudaStream_t s) const;

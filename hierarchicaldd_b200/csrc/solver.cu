@@ -46,6 +46,8 @@ Solver::Solver(const hdd_options& o) : opts(o) {
     if (o.sub_size[0] != o.sub_size[1] || o.sub_size[0] != o.sub_size[2])
         throw Error(HDD_ERR_UNSUPPORTED, "sub_size must be equal on all axes");
     if (o.vlevels < 1 || o.vlevels > kMaxLevels) throw Error(HDD_ERR_INVALID_ARGUMENT, "vlevels out of range");
+    if (o.coarse_solve != HDD_COARSE_REFERENCE && o.coarse_solve != HDD_COARSE_EXACT)
+        throw Error(HDD_ERR_INVALID_ARGUMENT, "coarse_solve must be HDD_COARSE_REFERENCE or HDD_COARSE_EXACT");
     if (o.sigma_levels < 1 || o.nVcycles < 0 || o.sigma_mg < 0 || o.interior_smoothing < 0 ||
         o.boundary_smoothing < 0 || o.sigma_smoothing < 0)
         throw Error(HDD_ERR_INVALID_ARGUMENT, "negative iteration counts");
@@ -155,6 +157,8 @@ void Solver::initialize() {
     box_nb.upload(bnb.data(), bnb.size(), stream);
     box_flags.upload(L.box_flags.data(), L.box_flags.size(), stream);
     for (DevBuf<float>* v : {&x, &b, &r, &z, &s, &q}) { v->alloc(std::max<size_t>(N, 1)); v->zero(stream); }
+    if (opts.precision_mode == HDD_PRECISION_MIXED) xd.alloc(std::max<size_t>(N, 1));
+    else xd.release();
     partial.alloc(std::max<size_t>(nt, 1));
     partial_max.alloc(std::max<size_t>(nt, 1));
     sums.alloc(8);
@@ -193,7 +197,7 @@ void Solver::initialize() {
     // A domain inside one subdomain has no interface: the preconditioner is
     // then the two subdomain V-cycle passes alone, and the coarser interface
     // levels (which only feed level 0) are not built.
-    if (n_if > 0) sigma.setup(ih, opts.sigma_smoothing, stream);
+    if (n_if > 0) sigma.setup(ih, opts.sigma_smoothing, stream, opts.coarse_solve == HDD_COARSE_EXACT);
     else sigma.release();
     setup_phase_ms[2] = since_ms(t_sigma);
     std::vector<long long> slot(n_if);
@@ -257,7 +261,7 @@ VcycleArgs Solver::vcycle_args(float* u, const float* bb, int halo_from_u, int z
     a.cluster = 1;
     if (const char* e = std::getenv("HDD_VCYCLE_CLUSTER")) a.cluster = std::atoi(e);
     // Correction weights omega/face_count with omega = (float)(2/3)
-    // (SPGrid_Correction_Legacy.h:149,190), divided in float on the host.
+    // (SPGrid_Correction_Legacy.h:35,76), divided in float on the host.
     const float omega = (float)(2. / 3.);
     a.inv_diag[0] = 0.0f;
     for (int k = 1; k < 8; ++k) a.inv_diag[k] = omega / (float)k;
@@ -323,6 +327,8 @@ void Solver::solve(hdd_result* res) {
     init.rho_old_d = 3.402823466e+38;
     cuda_check(cudaMemcpyAsync(scal.p, &init, sizeof(init), cudaMemcpyHostToDevice, stream), "init scalars");
     x.zero(stream);
+    xd.zero(stream);
+    double* xdp = mode == 1 ? xd.p : nullptr;
     sigma.clear_error(stream);
     cudaEvent_t e0, e1;
     cuda_check(cudaEventCreate(&e0), "event");
@@ -337,6 +343,8 @@ void Solver::solve(hdd_result* res) {
     sync();
     const double b_inf = rmax;
     history.assign(1, (double)rmax);
+    alphas.clear();
+    betas.clear();
     const float threshold = opts.relative_tol ? (float)(opts.tol * b_inf) : (float)opts.tol;
     const float small_number = 1.1920929e-07f;
     int it = 0;
@@ -360,10 +368,11 @@ void Solver::solve(hdd_result* res) {
             Tm tm(this, 2);
             cuda_check(launch_reduce_sum(partial.p, nt, sums.p + 1, stream), "reduce"); count();
             cuda_check(launch_scalar_alpha(scal.p, sums.p + 1, stream), "alpha"); count();
-            cuda_check(launch_update_xr(g, x.p, r.p, s.p, q.p, scal.p, mode, partial_max.p, stream), "update_xr"); count();
+            cuda_check(launch_update_xr(g, x.p, r.p, s.p, q.p, scal.p, mode, partial_max.p, stream, xdp), "update_xr");
+            count();
         }
         if (mode == 1 && opts.true_residual_every > 0 && (it + 1) % opts.true_residual_every == 0) {
-            cuda_check(launch_residual(g, b.p, x.p, r.p, partial_max.p, stream), "true residual"); count();
+            cuda_check(launch_residual_f64(g, b.p, xdp, r.p, partial_max.p, stream), "true residual"); count();
         }
         cuda_check(launch_reduce_max(partial_max.p, nt, scalars_f.p, stream), "reduce"); count();
         cuda_check(cudaMemcpyAsync(&rmax, scalars_f.p, sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
@@ -373,6 +382,8 @@ void Solver::solve(hdd_result* res) {
             cuda_check(cudaMemcpyAsync(&herr, sigma.d_err, sizeof(int), cudaMemcpyDeviceToHost, stream), "D2H");
         sync();
         history.push_back((double)rmax);
+        alphas.push_back(mode == 1 ? hs.alpha_d : (double)hs.alpha);
+        betas.push_back(it == 0 ? 0.0 : (mode == 1 ? hs.beta_d : (double)hs.beta));
         // A bounded wait that gave up leaves this iteration's preconditioner
         // invalid: stop here (check_waits below reports HDD_ERR_TIMEOUT).
         if (herr != 0) { ++it; break; }
@@ -384,8 +395,11 @@ void Solver::solve(hdd_result* res) {
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    // True residual of the returned x (reported, not used for stopping).
-    cuda_check(launch_residual(g, b.p, x.p, q.p, partial_max.p, stream), "true residual"); count();
+    // True residual of the returned iterate (reported, not used for stopping):
+    // the FP64 iterate in the precision form, else x.
+    if (xdp) cuda_check(launch_residual_f64(g, b.p, xdp, q.p, partial_max.p, stream), "true residual");
+    else cuda_check(launch_residual(g, b.p, x.p, q.p, partial_max.p, stream), "true residual");
+    count();
     cuda_check(launch_reduce_max(partial_max.p, nt, scalars_f.p + 1, stream), "reduce"); count();
     cuda_check(launch_project_dot(g, q.p, q.p, partial.p, stream), "dot"); count();
     cuda_check(launch_reduce_sum(partial.p, nt, sums.p + 2, stream), "reduce"); count();
@@ -420,6 +434,27 @@ void Solver::get_solution(float* out) {
                                      stream), "tiles_to_dense");
     count();
     cuda_check(cudaMemcpyAsync(out, dense.p, L.cell_count() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H x");
+    sync();
+}
+
+void Solver::get_solution_f64(double* out) {
+    if (!solved) throw Error(HDD_ERR_NOT_INITIALIZED, "no solution available");
+    const size_t n = L.cell_count();
+    DevBuf<double> tmp_tiles, tmp_dense;
+    const double* src = xd.p;
+    if (!src) {
+        // Reference precision: the FP32 iterate, widened.
+        std::vector<float> xf(n);
+        get_solution(xf.data());
+        for (size_t i = 0; i < n; ++i) out[i] = xf[i];
+        return;
+    }
+    tmp_dense.alloc(std::max<size_t>(n, 1));
+    cuda_check(cudaMemsetAsync(tmp_dense.p, 0, n * sizeof(double), stream), "memset");
+    cuda_check(launch_tiles_to_dense_f64(geom(), tile_xyz.p, L.opt.size[0], L.opt.size[1], L.opt.size[2], src,
+                                         tmp_dense.p, stream), "tiles_to_dense_f64");
+    count();
+    cuda_check(cudaMemcpyAsync(out, tmp_dense.p, n * sizeof(double), cudaMemcpyDeviceToHost, stream), "D2H x");
     sync();
 }
 

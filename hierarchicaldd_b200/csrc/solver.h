@@ -78,6 +78,7 @@ struct Solver {
 
     cudaStream_t stream = nullptr;
     DevBuf<float> x, b, r, z, s, q;
+    DevBuf<double> xd;      // precision form: the FP64 iterate (x is its FP32 rounding)
     DevBuf<uint16_t> tflags;
     DevBuf<int> tile_nbr, box_tile, box_nb, tile_xyz;
     DevBuf<float> dense;   // staging buffer in the caller's dense layout
@@ -97,6 +98,8 @@ struct Solver {
     // iteration of the last solve (entry 0: r = b), for parity checks against
     // the oracle's history.
     std::vector<double> history;
+    // Step lengths alpha and beta of every PCG iteration of the last solve.
+    std::vector<double> alphas, betas;
     // Host wall time of the setup phases: layout and vector uploads, interface
     // system (assembly or reload, and dump), interface solver (factorisations
     // and solve plans), total.
@@ -158,6 +161,7 @@ struct Solver {
     void initialize();
     void solve(hdd_result* res);
     void get_solution(float* out);
+    void get_solution_f64(double* out);
     void apply_preconditioner_dense(const float* r, float* zout);
     void vcycle_dense(float* u, const float* bb, int nv);
     void multiply_dense(const float* xin, float* yout);
@@ -180,7 +184,7 @@ struct Solver {
         for (const DevBuf<float>* v : {&x, &b, &r, &z, &s, &q, &dense, &partial_max, &scalars_f}) t += v->n * sizeof(float);
         t += tflags.n * sizeof(uint16_t) + box_flags.n;
         for (const DevBuf<int>* v : {&tile_nbr, &box_tile, &box_nb, &tile_xyz, &iface_nb}) t += v->n * sizeof(int);
-        t += (partial.n + sums.n) * sizeof(double) + iface_slot.n * sizeof(long long);
+        t += (partial.n + sums.n + xd.n) * sizeof(double) + iface_slot.n * sizeof(long long);
         return t + sigma.device_bytes;
     }
 };

@@ -81,7 +81,8 @@ class SPGrid_Domain_Decomposition_Solver:
                                   interior_smoothing, boundary_smoothing, sigma_smoothing, n_sigma_mg,
                                   tol=1e-6, relative_tol=True, max_iters=5000, min_iters=0,
                                   precision_mode=_lib.PRECISION_REFERENCE, true_residual_every=20,
-                                  iomode="neither", dump_directory="matrices_dump"):
+                                  iomode="neither", dump_directory="matrices_dump",
+                                  coarse_solve=_lib.COARSE_REFERENCE):
         """Setup with the reference's arguments (SPGrid_Domain_Decomposition_Solver.h:121).
         ``iomode`` "output" writes the interface matrices to ``dump_directory`` in the
         reference's dump layout, "input" reads them from there instead of assembling
@@ -109,6 +110,7 @@ class SPGrid_Domain_Decomposition_Solver:
         o.tol, o.relative_tol = float(tol), 1 if relative_tol else 0
         o.max_iters, o.min_iters = int(max_iters), int(min_iters)
         o.precision_mode, o.true_residual_every = int(precision_mode), int(true_residual_every)
+        o.coarse_solve = int(coarse_solve)
         o.device = self.device
         self.options = o
         self.close()
@@ -153,6 +155,12 @@ class SPGrid_Domain_Decomposition_Solver:
         self.last_result["status"] = st
         return self.last_result
 
+    def Solution_F64(self) -> np.ndarray:
+        """The FP64 iterate of the precision form (the FP32 solution widened otherwise)."""
+        x = np.zeros(self.size, np.float64)
+        self._check(self.lib.hdd_get_solution_dense_f64(self.h, x.ctypes.data_as(C.POINTER(C.c_double))))
+        return x
+
     def Residual_History(self) -> np.ndarray:
         """max|r| at the start of every PCG iteration of the last solve (entry 0: r = b)."""
         n = C.c_int()
@@ -161,6 +169,17 @@ class SPGrid_Domain_Decomposition_Solver:
         self._check(self.lib.hdd_get_residual_history(self.h, out.ctypes.data_as(C.POINTER(C.c_double)),
                                                       n.value, C.byref(n)))
         return out
+
+    def PCG_Coefficients(self):
+        """(alpha, beta) of every PCG iteration of the last solve (beta[0] = 0)."""
+        n = C.c_int()
+        dp = C.POINTER(C.c_double)
+        self._check(self.lib.hdd_get_pcg_coefficients(self.h, dp(), dp(), 0, C.byref(n)))
+        a = np.zeros(n.value, np.float64)
+        b = np.zeros(n.value, np.float64)
+        self._check(self.lib.hdd_get_pcg_coefficients(self.h, a.ctypes.data_as(dp), b.ctypes.data_as(dp), n.value,
+                                                      C.byref(n)))
+        return a, b
 
     def Solution(self) -> np.ndarray:
         x = np.zeros(self.size, np.float32)

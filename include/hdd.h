@@ -41,7 +41,8 @@ typedef enum {
 /* Precision modes of the PCG outer loop (the preconditioner is FP32 in all). */
 enum {
     HDD_PRECISION_REFERENCE = 0, /* FP32 vectors, FP64 dot accumulation, FP32 alpha/beta (as the reference) */
-    HDD_PRECISION_MIXED = 1      /* FP32 vectors, FP64 dots and alpha/beta, periodic FP64 true residual */
+    HDD_PRECISION_MIXED = 1      /* FP32 preconditioner and search vectors; FP64 iterate x, dots,
+                                    alpha/beta and periodic true residual r = b - A x */
 };
 
 typedef struct {
@@ -61,15 +62,27 @@ typedef struct {
     int precision_mode;     /* HDD_PRECISION_* */
     int true_residual_every;/* mixed mode: recompute r = b - A x every N iterations (0 = never) */
     int device;             /* CUDA device ordinal */
+    int coarse_solve;       /* HDD_COARSE_* : how the coarsest interface level is solved */
 } hdd_options;
+
+/* Coarsest interface (sigma) level.  The reference runs 200 smoothing steps
+ * there (CPU/Interface_Solver/SIGMA_MULTIGRID_SOLVER.cpp:43), a contraction
+ * towards the Schur complement solve S^{-1} b. */
+enum {
+    HDD_COARSE_REFERENCE = 0, /* the 200 steps; replaced by one exact solve of S when they have
+                                 converged (setup's estimate rho^200 <= 1e-7): same result */
+    HDD_COARSE_EXACT = 1      /* always one exact solve of S: a deviation from the reference where
+                                 the 200 steps have not converged (slowly contracting coarse levels) */
+};
 
 typedef struct {
     int iterations;
     int converged;
     double final_norm;        /* max|r| of the recursively updated residual */
     double b_inf;             /* max|b| over Active|Interface cells */
-    double true_residual_inf; /* max|b - A x| / max|b| of the returned x */
-    double true_residual_l2;  /* ||b - A x||_2 / ||b||_2 of the returned x */
+    double true_residual_inf; /* max|b - A x| / max|b| of the returned iterate (FP64 under
+                                 HDD_PRECISION_MIXED, see hdd_get_solution_dense_f64) */
+    double true_residual_l2;  /* ||b - A x||_2 / ||b||_2 of the same */
     double solve_ms;          /* device time of the PCG loop */
     double setup_ms;          /* host+device time of hdd_initialize_preconditioner */
 } hdd_result;
@@ -147,6 +160,14 @@ hdd_status hdd_solve(hdd_solver* s, hdd_result* result);
 /* Copies the solution x of the last solve. */
 hdd_status hdd_get_solution_dense(hdd_solver* s, float* x);
 
+/* The same in FP64.  Under HDD_PRECISION_MIXED the iterate is accumulated in
+ * FP64 (the preconditioner stays FP32) and this returns it unrounded: a
+ * solution of magnitude |x| carries an FP32 rounding error of about
+ * 6e-8 |x|, which bounds the relative residual an FP32 x can show at about
+ * 6e-8 ||A|| |x| / |b|; the FP64 iterate has no such floor.  Under
+ * HDD_PRECISION_REFERENCE it is the FP32 solution widened. */
+hdd_status hdd_get_solution_dense_f64(hdd_solver* s, double* x);
+
 /* The convergence norm max|r| of the last solve at the start of every PCG
  * iteration, entry 0 being that of r = b: the values CONJUGATE_GRADIENT::Solve
  * logs with print_residuals
@@ -183,11 +204,13 @@ hdd_status hdd_multiply_dense(hdd_solver* s, const float* x, float* y);
  * (256 KiB, held by every GPU that loads the library); domains with more
  * stored tiles get HDD_ERR_INVALID_ARGUMENT.  The first call on a device looks
  * up that array's device address, so make it before any stream capture.
- * Calls that overlap on the GPU share the array and race. */
+ * Calls that overlap on the GPU share the array and race.  The call runs on
+ * the solver's device and leaves the calling thread's current device as it
+ * found it. */
 hdd_status hdd_multiply_dot_dense_device_noalloc(hdd_solver* s, const float* x, float* y, double* dot,
                                                  void* stream);
 
-/* Test seam: one sigma V-cycle (SIGMA_MULTIGRID_SOLVER.cpp:70-82) from u = 0
+/* Test seam: one sigma V-cycle (SIGMA_MULTIGRID_SOLVER.cpp:35-47) from u = 0
  * on the level-0 interface right-hand side b0 (interface DOF order). */
 hdd_status hdd_sigma_vcycle(hdd_solver* s, const float* b0, float* u0);
 
@@ -245,6 +268,12 @@ hdd_status hdd_set_wait_limit(hdd_solver* s, long long polls);
  * than its child runs), so every solve reports HDD_ERR_TIMEOUT once the wait
  * limit runs out; on == 0 restores the dependency.  No reference counterpart. */
 hdd_status hdd_test_stall_dependency(hdd_solver* s, int on);
+
+/* The PCG step lengths of the last solve, alpha[i] and beta[i] of iteration i
+ * (beta[0] = 0), in the precision the solve used: the Lanczos coefficients of
+ * the preconditioned operator (its extreme eigenvalues follow from them).
+ * Writes min(capacity, *n) entries of each; *n gets the iteration count. */
+hdd_status hdd_get_pcg_coefficients(hdd_solver* s, double* alpha, double* beta, int capacity, int* n);
 
 /* Number of our CUDA kernel launches issued since the handle was created. */
 hdd_status hdd_kernel_launch_count(hdd_solver* s, long long* count);

@@ -132,8 +132,11 @@ struct Solver : SolverBase {
     // CONJUGATE_GRADIENT.cpp:22-67 with KRYLOV_SYSTEM_BASE::Precondition.  The
     // stop test is max|r| <= tol (relative=0, the reference's test) or
     // max|r| <= tol * max|b| over Active|Interface cells (relative=1).
+    // times (optional, history_len entries): wall seconds from the start of
+    // the solve to the end of each PCG iteration.
     int solve(const T* b_in, T* x, double tol, bool relative, int min_it, int max_it, double* norms,
-              double* history, int history_len) {
+              double* history, int history_len, double* times = nullptr) {
+        const auto t_start = std::chrono::steady_clock::now();
         const size_t n = d0.count();
         std::vector<T> b(b_in, b_in + n), q(n, T(0)), s(n, T(0)), r(n, T(0)), z(n, T(0));
         project(b.data());
@@ -169,6 +172,8 @@ struct Solver : SolverBase {
             for (size_t i = 0; i < n; ++i) x[i] = s[i] * alpha + x[i];
             for (size_t i = 0; i < n; ++i) r[i] = q[i] * (-alpha) + r[i];
             rho_old = rho;
+            if (times && it < history_len)
+                times[it] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
         }
         if (norms) {
             norms[0] = (double)convergence_norm;
@@ -345,6 +350,17 @@ int hddo_solve(void* hp, const void* b, void* x, double tol, int relative, int m
     return DISPATCH(h, ([&] {
         using T = typename std::remove_reference<decltype(s.lv[0].u[0])>::type;
         return s.solve((const T*)b, (T*)x, tol, relative != 0, min_it, max_it, norms, history, history_len);
+    })());
+}
+
+// hddo_solve with the wall time at the end of every PCG iteration (seconds
+// from the start of the solve) in times[0 .. history_len).
+int hddo_solve_timed(void* hp, const void* b, void* x, double tol, int relative, int min_it, int max_it,
+                     double* norms, double* history, int history_len, double* times) {
+    Handle* h = static_cast<Handle*>(hp);
+    return DISPATCH(h, ([&] {
+        using T = typename std::remove_reference<decltype(s.lv[0].u[0])>::type;
+        return s.solve((const T*)b, (T*)x, tol, relative != 0, min_it, max_it, norms, history, history_len, times);
     })());
 }
 

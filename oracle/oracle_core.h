@@ -96,7 +96,7 @@ void downsample_topology(const Dims& fd, const uint32_t* ff, const Dims& cd, uin
 template <class T>
 void residual(const Dims& d, const uint32_t* f, const T* u, T* r, const T* b);
 
-// CPU/SPGrid_Library/SPGrid_Correction_Legacy.h:161-191.  Damped Jacobi update
+// CPU/SPGrid_Library/SPGrid_Correction_Legacy.h:47-80.  Damped Jacobi update
 // u += (omega/face_count) r on Active cells, split by the Boundary bit.
 template <class T>
 void correction(const Dims& d, const uint32_t* f, T* u, const T* r, bool write_interior,
@@ -127,7 +127,7 @@ void v_cycle(std::vector<MGLevel<T>>& lv, T* u0, T* r0, const T* b0, int interio
 template <class T>
 void laplace_ai(const Dims& d, const uint32_t* f, const T* u, T* lu);
 
-// CPU/SPGrid_Library/SPGrid_Laplace_Legacy.h:310-335 (Laplace_ri): at Interface
+// CPU/SPGrid_Library/SPGrid_Laplace_Legacy.h:70-117 (Laplace_ri): at Interface
 // cells, Lu -= (T)(-sum over active-face Active neighbours of u_n).
 template <class T>
 void laplace_ri(const Dims& d, const uint32_t* f, const T* u, T* lu);

@@ -475,7 +475,7 @@ struct Stride1D {
 };
 typedef std::array<Stride1D, 3> Stride3;
 
-// CPU/Interface_Solver/STRIDE_GENERATOR.h:70-101.
+// CPU/Interface_Solver/STRIDE_GENERATOR.h:23-54.
 static int generate_adaptive_stride(const I3& lo, const I3& hi, Stride3& q) {
     int level = INT_MAX;
     for (int a = 0; a < 3; ++a) {
@@ -546,7 +546,7 @@ static void embed(const I3& idx, Parents<T>& parents, T w, const Stride3& q) {
 template <class T>
 using M8 = std::array<T, 64>;
 
-// CPU/Interface_Solver/CELL_PROLONGATION_BAKER.h:125-152.
+// CPU/Interface_Solver/CELL_PROLONGATION_BAKER.h:22-50.
 template <class T>
 static std::array<M8<T>, 8> bake_cell_prolongation() {
     std::array<M8<T>, 8> P;
@@ -582,7 +582,7 @@ struct SubsetFlags {
     }
 };
 
-// CPU/Interface_Solver/GALERKIN_PROCESS.h:183-224.
+// CPU/Interface_Solver/GALERKIN_PROCESS.h:27-69.
 template <class T>
 using GalerkinMemo = std::vector<std::unordered_map<uint64_t, M8<T>>>;
 
@@ -929,7 +929,7 @@ static void create_subdomain_hierarchy(const SubsetFlags& sf, LocalIface<T>& li,
 }
 
 // Subdomain node flags, CPU/SPGrid_Domain_Decomposition_Solver/SPGrid_Subdomain_Splitter.h:123-143
-// with SPGrid_Subdomain_Rasterizer.h:253-300 and the Domain_Divider pass on the box.
+// with SPGrid_Subdomain_Rasterizer.h:59-136 and the Domain_Divider pass on the box.
 static SubsetFlags extract_subset(const Dims& gd, const uint32_t* gf, const I3& lo, const I3& hi,
                                   const int sub[3]) {
     SubsetFlags s;
@@ -1061,7 +1061,7 @@ void build_interface_system(const Dims& gd, const uint32_t* gflags_in, const int
         }
         for (int sd = 0; sd < out.n_sub; ++sd) out.Air[m][sd].cols = out.n_iface[m];
     }
-    // Prr (CPU/Interface_Solver/PROLONGATION_MATRIX_HELPER.cpp:268-294).
+    // Prr (CPU/Interface_Solver/PROLONGATION_MATRIX_HELPER.cpp:13-40).
     out.Prr.resize(M > 1 ? M - 1 : 0);
     for (int m = 0; m + 1 < M; ++m) {
         std::unordered_map<uint64_t, T> P;

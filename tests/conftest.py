@@ -15,7 +15,7 @@ def pytest_configure(config):
 # Run order: the CPU tests, then the GPU parity, edge-case and serving suites,
 # then the other GPU tests, and the allocation-free entry point's test last, so
 # that a run stopping at its first failure (-x) has already run the main suites.
-_CORE_GPU = ("test_gpu_parity.py", "test_gpu_edge_cases.py", "test_gpu_server.py")
+_CORE_GPU = ("test_gpu_parity.py", "test_gpu_c2_parity.py", "test_gpu_edge_cases.py", "test_gpu_server.py")
 
 
 def pytest_collection_modifyitems(session, config, items):

@@ -6,7 +6,7 @@ decodes to.  The reference tree is only read by this script; the tests compare
 the restated generator against these digests everywhere, and against the
 directory itself where it exists.
 
-Usage: python tests/golden/make_spgrid2d_golden.py [reference_root]
+Usage: python tests/golden/make_spgrid2d_golden.py <reference_root>  (or HDD_REFERENCE_ROOT)
 """
 import hashlib
 import json
@@ -23,7 +23,9 @@ REL = os.path.join("demos", "SPGrid_Create_Simple_Domain", "Create_2D_Domain", "
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2 and not os.environ.get("HDD_REFERENCE_ROOT"):
+        sys.exit("usage: make_spgrid2d_golden.py <reference checkout> (or set HDD_REFERENCE_ROOT)")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ["HDD_REFERENCE_ROOT"]
     size, flags, data, count = read_spgrid_dir_any(os.path.join(root, REL))
     delta = [int(v) for v in np.argwhere(data != 0)[0]]
     out = {

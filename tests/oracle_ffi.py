@@ -48,6 +48,11 @@ def lib():
         L.hddo_sigma_smooth.argtypes = [vp, C.c_int, vp, vp]
         L.hddo_solve.restype = C.c_int
         L.hddo_solve.argtypes = [vp, vp, vp, C.c_double, C.c_int, C.c_int, C.c_int, dp, dp, C.c_int]
+        try:
+            L.hddo_solve_timed.restype = C.c_int
+            L.hddo_solve_timed.argtypes = [vp, vp, vp, C.c_double, C.c_int, C.c_int, C.c_int, dp, dp, C.c_int, dp]
+        except AttributeError:  # a library built before it existed: solve_timed() raises
+            pass
         _lib = L
     return _lib
 
@@ -162,3 +167,18 @@ class Oracle:
         info = dict(final_norm=norms[0], b_inf=norms[1], true_res_inf=norms[2], true_res_l2=norms[3],
                     b_l2=norms[4], history=hist[:it + 1].copy())
         return x, it, info
+
+    def solve_timed(self, rhs, tol=1e-6, relative=True, max_it=500, min_it=0):
+        """solve() that also returns the wall seconds (from the start of the
+        solve) at the end of every PCG iteration: (x, iterations, info, times)."""
+        b = self._vec(rhs)
+        x = self._vec()
+        norms = np.zeros(5, np.float64)
+        hist = np.zeros(max_it + 1, np.float64)
+        times = np.zeros(max_it + 1, np.float64)
+        it = lib().hddo_solve_timed(self.h, b.ctypes.data, x.ctypes.data, tol, 1 if relative else 0, min_it, max_it,
+                                    _p(norms, C.c_double), _p(hist, C.c_double), max_it + 1,
+                                    _p(times, C.c_double))
+        info = dict(final_norm=norms[0], b_inf=norms[1], true_res_inf=norms[2], true_res_l2=norms[3],
+                    b_l2=norms[4], history=hist[:it + 1].copy())
+        return x, it, info, times[:it].copy()

@@ -401,3 +401,18 @@ def test_setup_bits_do_not_depend_on_thread_count(shim):
         assert p.returncode == 0, p.stderr
         digests.add(p.stdout.strip())
     assert len(digests) == 1, digests
+
+
+@pytest.mark.parametrize("sub", [4, 64])
+def test_unsupported_sub_sizes_are_refused_before_setup(shim, sub):
+    """The resident V-cycle handles 8^3, 16^3 and 32^3 subdomains; 4 and the
+    reference Test_Bench default 64 are refused by the layout, before any
+    interface assembly or factorisation."""
+    d = domains.small(64, 16, 12, seed=4)
+    size = (C.c_int * 3)(*d.size)
+    sb = (C.c_int * 3)(sub, sub, sub)
+    flags = np.ascontiguousarray(d.flags, np.uint32)
+    err = C.create_string_buffer(512)
+    h = shim.shim_build(size, sb, 2, 2, flags.ctypes.data_as(C.POINTER(C.c_uint32)), err, 512)
+    assert not h
+    assert b"sub_size must be 8, 16 or 32" in err.value, err.value

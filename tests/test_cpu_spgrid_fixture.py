@@ -26,7 +26,10 @@ from oracle_ffi import Oracle
 from spgrid_format import XM, YM, ZM, axis_masks, read_spgrid_dir_any
 
 GOLDEN = json.load(open(os.path.join(ROOT, "tests", "golden", "spgrid2d_fixture.json")))
-REFERENCE_DIR = os.path.join("/root/reference", GOLDEN["source"])
+# The reference checkout, when one is at hand (HDD_REFERENCE_ROOT); the digests
+# above were made from it by tests/golden/make_spgrid2d_golden.py.
+REFERENCE_DIR = (os.path.join(os.environ["HDD_REFERENCE_ROOT"], GOLDEN["source"])
+                 if os.environ.get("HDD_REFERENCE_ROOT") else None)
 
 
 def digest(a, dt):
@@ -50,7 +53,8 @@ def test_generator_matches_the_reference_2d_output():
     assert int(np.sum((d.flags & domains.DIRICHLET) != 0)) == cells["dirichlet"]
 
 
-@pytest.mark.skipif(not os.path.isdir(REFERENCE_DIR), reason="reference tree not present")
+@pytest.mark.skipif(not REFERENCE_DIR or not os.path.isdir(REFERENCE_DIR),
+                    reason="reference tree not given (HDD_REFERENCE_ROOT)")
 def test_reference_2d_directory_decodes_to_the_generator():
     size, flags, data, blocks = read_spgrid_dir_any(REFERENCE_DIR)
     assert list(size) == GOLDEN["size"] and blocks == GOLDEN["blocks"]
