@@ -210,6 +210,12 @@ def make_oracle(d):
                   sigma_levels=m["sigma_levels"], sigma_smoothing=m["sigma_smoothing"], sigma_mg=m["sigma_mg"])
 
 
+def precision_mode(args, d):
+    """PCG precision: the workload's own (the sparse workload asks for the
+    precision form) unless --precision mixed asks for the precision form."""
+    return 1 if args.precision == "mixed" or d.meta.get("precision_mode", 0) == 1 else 0
+
+
 def config_dict(d, args, world=1):
     """The workload description shared by both arms' lines."""
     m = d.meta
@@ -217,7 +223,8 @@ def config_dict(d, args, world=1):
             "nVcycles": m["nVcycles"], "interior_smoothing": m["interior_smoothing"],
             "boundary_smoothing": m["boundary_smoothing"], "sigma_levels": m["sigma_levels"],
             "sigma_smoothing": m["sigma_smoothing"], "sigma_mg": m["sigma_mg"], "tol": 1e-6,
-            "precision": args.precision, "l2": "working set > L2 (no flush)", "parallelism": f"replicas{world}"}
+            "precision": "mixed" if precision_mode(args, d) == 1 else "reference",
+            "l2": "working set > L2 (no flush)", "parallelism": f"replicas{world}"}
 
 
 def level0_updates_per_iteration(d):
@@ -546,8 +553,8 @@ def main():
     t0 = time.time()
     s.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"],
                                 m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"],
-                                m["sigma_mg"], tol=1e-6,
-                                precision_mode=1 if args.precision == "mixed" else 0)
+                                m["sigma_mg"], tol=1e-6, precision_mode=precision_mode(args, d),
+                                true_residual_every=int(m.get("true_residual_every", 20)))
     setup_s = time.time() - t0
     try:
         setup_phases = s.Setup_Timing()

@@ -95,6 +95,7 @@ void hdd_options_default(hdd_options* o) {
     o->true_residual_every = 20;
     o->device = 0;
     o->coarse_solve = HDD_COARSE_REFERENCE;
+    o->solve_share = 0;
 }
 
 hdd_status hdd_create(const hdd_options* opts, hdd_solver** out) {
@@ -232,9 +233,9 @@ hdd_status hdd_get_solution_dense_f64(hdd_solver* s, double* x) {
 hdd_status hdd_get_residual_history(hdd_solver* s, double* out, int capacity, int* n) {
     if (!n || capacity < 0 || (capacity > 0 && !out)) return HDD_ERR_INVALID_ARGUMENT;
     return guard(s, [&](Solver& v) {
-        if (!v.solved) throw Error(HDD_ERR_NOT_INITIALIZED, "no solve has run");
-        *n = (int)v.history.size();
-        for (int i = 0; i < capacity && i < *n; ++i) out[i] = v.history[i];
+        if (!v.w0.solved) throw Error(HDD_ERR_NOT_INITIALIZED, "no solve has run");
+        *n = (int)v.w0.history.size();
+        for (int i = 0; i < capacity && i < *n; ++i) out[i] = v.w0.history[i];
     });
 }
 
@@ -282,7 +283,7 @@ hdd_status hdd_multiply_dot_dense_device_noalloc(hdd_solver* s, const float* x, 
         DeviceGuard dg(v.opts.device);
         hdd::multiply_dot_dense_device_noalloc(v.geom(), v.tile_xyz.p, v.L.opt.size, v.opts.device, x, y, dot,
                                                static_cast<cudaStream_t>(stream));
-        v.count(2);
+        v.count(v.w0, 2);
     });
 }
 
@@ -367,6 +368,8 @@ hdd_status hdd_set_wait_limit(hdd_solver* s, long long polls) {
     if (polls < 1) return HDD_ERR_INVALID_ARGUMENT;
     return guard(s, [&](Solver& v) {
         if (!v.initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+        v.sync();
+        v.release_graphs();  // the limit is a launch parameter of the captured solves
         v.sigma.set_wait_limit(polls);
     });
 }
@@ -382,15 +385,15 @@ hdd_status hdd_test_stall_dependency(hdd_solver* s, int on) {
 hdd_status hdd_get_pcg_coefficients(hdd_solver* s, double* alpha, double* beta, int capacity, int* n) {
     if (!n || capacity < 0 || (capacity > 0 && (!alpha || !beta))) return HDD_ERR_INVALID_ARGUMENT;
     return guard(s, [&](Solver& v) {
-        if (!v.solved) throw Error(HDD_ERR_NOT_INITIALIZED, "no solve has run");
-        *n = (int)v.alphas.size();
-        for (int i = 0; i < capacity && i < *n; ++i) { alpha[i] = v.alphas[i]; beta[i] = v.betas[i]; }
+        if (!v.w0.solved) throw Error(HDD_ERR_NOT_INITIALIZED, "no solve has run");
+        *n = (int)v.w0.alphas.size();
+        for (int i = 0; i < capacity && i < *n; ++i) { alpha[i] = v.w0.alphas[i]; beta[i] = v.w0.betas[i]; }
     });
 }
 
 hdd_status hdd_kernel_launch_count(hdd_solver* s, long long* count) {
     if (!count) return HDD_ERR_INVALID_ARGUMENT;
-    return guard(s, [&](Solver& v) { *count = v.launches; });
+    return guard(s, [&](Solver& v) { *count = v.w0.launches; });
 }
 
 const char* hdd_status_string(hdd_status st) {

@@ -42,9 +42,11 @@ struct TileGeom {
 };
 
 // q = Project(A s) (double accumulation, CG_SYSTEM::Multiply + Project);
-// partial[tile] = sum over the tile of (double)(s*q) (float products).
+// partial[0 .. laplace_partials(g)) = sums of (double)(s*q) (float products)
+// over fixed parts of the tiles, to be reduced with launch_reduce_sum.
 cudaError_t launch_laplace_dot(const TileGeom& g, const float* s, float* q, double* partial,
                                cudaStream_t stream);
+int laplace_partials(const TileGeom& g);
 
 // Deterministic final sums of per-tile partials into out[slot] (double).
 cudaError_t launch_reduce_sum(const double* partial, int n, double* out, cudaStream_t stream);

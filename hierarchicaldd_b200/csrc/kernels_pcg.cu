@@ -97,6 +97,147 @@ __global__ void __launch_bounds__(kNT) laplace_dot_kernel(TileGeom g, const floa
     if (threadIdx.x == 0) partial[t] = acc;
 }
 
+// q = Project(A s) and per-work-unit partial sums of s*q, marching x-planes.
+//
+// A group of S*S/4 threads covers one x-plane of a tile, one float4 of four
+// z-consecutive cells per thread (thread i: row y = i / (S/4), quad zq =
+// i % (S/4)); a CTA of 256 threads holds G = 1024 / (S*S) groups, each
+// marching over the planes [x0, x0 + S/SLABS) of its own (tile, slab) unit.
+// Every cell value is read from HBM once per launch: the x neighbours stay in
+// registers (previous / current / prefetched next plane), the y neighbours
+// come from the current plane staged in shared memory (double-buffered, one
+// barrier per plane), the z neighbours from the adjacent lanes of the row
+// (shuffles); only the tile-face halos are read from the neighbouring tiles.
+// The arithmetic per cell is laplace_cell's (FP64 face sums, faces -x,+x,-y,
+// +y,-z,+z), so q is bit-identical to it; the dot sums the same FP32 products
+// in FP64 in a fixed order per unit.
+template <int S, int SLABS>
+struct MarchShape {
+    static constexpr int P = S / 4;           // quads per row
+    static constexpr int GT = S * S / 4;      // threads per group (one plane)
+    static constexpr int G = kNT / GT;        // groups per CTA
+    static constexpr int NP = S / SLABS;      // planes per unit
+};
+
+template <int S, int SLABS>
+__global__ void __launch_bounds__(kNT, 4) laplace_dot_march_kernel(TileGeom g, const float* __restrict__ s,
+                                                                float* __restrict__ q, double* partial) {
+    using M = MarchShape<S, SLABS>;
+    constexpr int P = M::P, GT = M::GT, NP = M::NP, S2 = S * S, S3 = S * S * S;
+    __shared__ float4 plane[2][kNT];
+    __shared__ double red[kNT / 32];
+    const int i = threadIdx.x % GT, grp = threadIdx.x / GT;
+    const long long unit = (long long)blockIdx.x * M::G + grp;
+    const bool valid = unit < (long long)g.ntiles * SLABS;
+    const int t = valid ? (int)(unit / SLABS) : 0;
+    const int x0 = valid ? (int)(unit % SLABS) * NP : 0;
+    const int y = i / P, zq = i % P;
+    const size_t tb = (size_t)t * S3;
+    const int nb[6] = {g.nbr[6 * t + 0], g.nbr[6 * t + 1], g.nbr[6 * t + 2],
+                       g.nbr[6 * t + 3], g.nbr[6 * t + 4], g.nbr[6 * t + 5]};
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    // float4 of this thread's cells in plane xx of tile tt (zero if absent).
+    auto load4 = [&](int tt, int xx) -> float4 {
+        if (!valid || tt < 0) return zero4;
+        return __ldg(reinterpret_cast<const float4*>(s + (size_t)tt * S3 + (size_t)xx * S2) + i);
+    };
+    auto flags4 = [&](int xx) -> uint2 {
+        if (!valid) return make_uint2(0u, 0u);
+        return __ldg(reinterpret_cast<const uint2*>(g.flags + tb + (size_t)xx * S2) + i);
+    };
+    // Plane x (0 <= x < S) of this tile, or the neighbouring tile's face
+    // plane for x = -1 and x = S.
+    auto plane4 = [&](int xx) -> float4 {
+        if (xx < 0) return load4(nb[0], S - 1);
+        if (xx >= S) return load4(nb[1], 0);
+        return load4(t, xx);
+    };
+    // Two planes are in flight ahead of the one being computed.
+    float4 prev = plane4(x0 - 1);
+    float4 cur = plane4(x0);
+    float4 nxt = plane4(x0 + 1);
+    uint2 fcur = flags4(x0);
+    uint2 fnxt = NP > 1 ? flags4(x0 + 1) : make_uint2(0u, 0u);
+    double acc = 0.0;
+#pragma unroll 1
+    for (int k = 0; k < NP; ++k) {
+        const int x = x0 + k;
+        const float4 nxt2 = k + 2 <= NP ? plane4(x + 2) : zero4;
+        const uint2 fnxt2 = k + 2 < NP ? flags4(x + 2) : make_uint2(0u, 0u);
+        // Tile-face halos of this plane (y rows and z ends).
+        float4 ym = zero4, yp = zero4;
+        float zm = 0.f, zp = 0.f;
+        if (valid) {
+            if (y == 0 && nb[2] >= 0)
+                ym = __ldg(reinterpret_cast<const float4*>(s + (size_t)nb[2] * S3 + (size_t)x * S2 + (S - 1) * S) + zq);
+            if (y == S - 1 && nb[3] >= 0)
+                yp = __ldg(reinterpret_cast<const float4*>(s + (size_t)nb[3] * S3 + (size_t)x * S2) + zq);
+            if (zq == 0 && nb[4] >= 0) zm = __ldg(s + (size_t)nb[4] * S3 + (size_t)x * S2 + y * S + (S - 1));
+            if (zq == P - 1 && nb[5] >= 0) zp = __ldg(s + (size_t)nb[5] * S3 + (size_t)x * S2 + y * S);
+        }
+        float4* buf = plane[k & 1];
+        buf[threadIdx.x] = cur;
+        __syncthreads();
+        if (y > 0) ym = buf[threadIdx.x - P];
+        if (y < S - 1) yp = buf[threadIdx.x + P];
+        const float zl = __shfl_up_sync(0xffffffffu, cur.w, 1);
+        const float zr = __shfl_down_sync(0xffffffffu, cur.x, 1);
+        if (zq > 0) zm = zl;
+        if (zq < P - 1) zp = zr;
+        const float cv[4] = {cur.x, cur.y, cur.z, cur.w};
+        const float xm[4] = {prev.x, prev.y, prev.z, prev.w};
+        const float xp[4] = {nxt.x, nxt.y, nxt.z, nxt.w};
+        const float ymv[4] = {ym.x, ym.y, ym.z, ym.w};
+        const float ypv[4] = {yp.x, yp.y, yp.z, yp.w};
+        const uint32_t fw[4] = {fcur.x & 0xffffu, fcur.x >> 16, fcur.y & 0xffffu, fcur.y >> 16};
+        float out[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const uint32_t fl = fw[e];
+            out[e] = 0.0f;
+            if (fl & (C_ACTIVE | C_INTERFACE)) {
+                const double cd = (double)cv[e];
+                const float zmv = e == 0 ? zm : cv[e > 0 ? e - 1 : 0];
+                const float zpv = e == 3 ? zp : cv[e < 3 ? e + 1 : 3];
+                double r = 0.0;
+                if (fl & 1u) r -= ((double)xm[e] - cd);
+                if (fl & 2u) r -= ((double)xp[e] - cd);
+                if (fl & 4u) r -= ((double)ymv[e] - cd);
+                if (fl & 8u) r -= ((double)ypv[e] - cd);
+                if (fl & 16u) r -= ((double)zmv - cd);
+                if (fl & 32u) r -= ((double)zpv - cd);
+                out[e] = (float)r;
+            }
+            acc += (double)(cv[e] * out[e]);
+        }
+        if (valid)
+            reinterpret_cast<float4*>(q + tb + (size_t)x * S2)[i] = make_float4(out[0], out[1], out[2], out[3]);
+        prev = cur;
+        cur = nxt;
+        nxt = nxt2;
+        fcur = fnxt;
+        fnxt = fnxt2;
+    }
+    // Per-unit sums: warps never straddle groups (GT is a multiple of 32 or
+    // the group is a half or quarter warp, summed by masked shuffles below).
+    if (GT >= 32) {
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        const int w = threadIdx.x >> 5;
+        if ((threadIdx.x & 31) == 0) red[w] = acc;
+        __syncthreads();
+        constexpr int WPG = GT / 32;  // warps per group
+        if (threadIdx.x < M::G) {
+            const long long u = (long long)blockIdx.x * M::G + threadIdx.x;
+            double v = 0.0;
+            for (int j = 0; j < WPG; ++j) v += red[threadIdx.x * WPG + j];
+            if (u < (long long)g.ntiles * SLABS) partial[u] = v;
+        }
+    } else {
+        for (int o = GT / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, GT);
+        if (i == 0 && valid) partial[unit] = acc;
+    }
+}
+
 // precise = 0: r = b - (float)(A x), the reference's float subtraction;
 // precise = 1: r = (float)(b - A x) with A x kept in FP64 (the FP64 true
 // residual of the precision form).
@@ -310,9 +451,31 @@ cudaError_t launch_tiles_to_dense_f64(const TileGeom& g, const int* txyz, int sx
     return cudaGetLastError();
 }
 
+// Work units of the marching Laplacian: (tile, slab) pairs, two slabs of 16
+// planes per 32^3 tile so that a 256^3 domain gives 1024 CTAs.
+static int laplace_slabs(int sub) { return sub == 32 ? 2 : 1; }
+
+int laplace_partials(const TileGeom& g) {
+    if (g.sub == 8 || g.sub == 16 || g.sub == 32) return g.ntiles * laplace_slabs(g.sub);
+    return g.ntiles;
+}
+
+template <int S, int SLABS>
+static void launch_march(const TileGeom& g, const float* s, float* q, double* partial, cudaStream_t st) {
+    using M = MarchShape<S, SLABS>;
+    const long long units = (long long)g.ntiles * SLABS;
+    const int grid = (int)((units + M::G - 1) / M::G);
+    laplace_dot_march_kernel<S, SLABS><<<grid, kNT, 0, st>>>(g, s, q, partial);
+}
+
 cudaError_t launch_laplace_dot(const TileGeom& g, const float* s, float* q, double* partial, cudaStream_t st) {
     if (g.ntiles == 0) return cudaSuccess;
-    laplace_dot_kernel<<<g.ntiles, kNT, 0, st>>>(g, s, q, partial);
+    switch (g.sub) {
+        case 32: launch_march<32, 2>(g, s, q, partial, st); break;
+        case 16: launch_march<16, 1>(g, s, q, partial, st); break;
+        case 8: launch_march<8, 1>(g, s, q, partial, st); break;
+        default: laplace_dot_kernel<<<g.ntiles, kNT, 0, st>>>(g, s, q, partial); break;
+    }
     return cudaGetLastError();
 }
 cudaError_t launch_residual(const TileGeom& g, const float* b, const float* x, float* r, float* pm, cudaStream_t st,

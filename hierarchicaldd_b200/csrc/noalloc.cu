@@ -7,11 +7,12 @@
 // y = Project(A x) and read sum(x*y) with nothing allocated per call: the
 // per-tile partial sums live in one fixed, file-scope device array.
 //
-// The kernel is the dense-addressed twin of laplace_dot_kernel: the same
-// per-tile CTA, the same cell-to-thread mapping, the same FP64 face sums in
-// the same face order and the same block reduction, so y and the dot are
-// bit-identical to the tiled path on the same data.  Cells outside the stored
-// tiles read as zero (as they do in the tiled vectors) and are not written.
+// The kernel applies the tiled path's per-cell arithmetic on dense addresses:
+// the same FP64 face sums in the same face order, so y is bit-identical to
+// the tiled Laplacian on the same data; the dot sums the same FP32 products
+// in FP64, per tile and then over tiles, in an order of its own.  Cells
+// outside the stored tiles read as zero (as they do in the tiled vectors) and
+// are not written.
 //
 // The scratch array is shared by every call in the process: two calls whose
 // kernels overlap on the GPU race on it.  Every slot a call reads is written
@@ -77,7 +78,7 @@ __global__ void __launch_bounds__(kNT) laplace_dot_dense_kernel(TileGeom g, cons
         if (gx < sx && gy < sy && gz < sz) yv[((size_t)gx * sy + gy) * sz + gz] = out;
         acc += (double)(sv * out);
     }
-    // Block reduction in the same shape as the tiled kernel's.
+    // Block reduction.
     __shared__ double red[32];
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;

@@ -4,14 +4,19 @@
 // The reference has no counterpart: its GPU demo solves one domain per process
 // (GPU/Test_Bench_3D/main.cpp), with one worker thread per GPU draining a
 // command queue (GPU/Nodes/Command.h:33-55).  Here a server owns `slots`
-// worker threads.  Each resident domain is one Solver (its own CUDA stream and
-// device state); a worker takes the oldest queued request whose domain is
-// resident and idle, so requests on different domains overlap on the device
-// while requests on one domain keep their arrival order.  Domains are admitted
-// in arrival order once their estimated device footprint fits the HBM budget;
-// their host setup (layout, interface assembly, factorisation) runs on a
-// worker with setup_threads OpenMP threads, so setups overlap with solves of
-// other domains.
+// worker threads.  Each resident domain is one Solver: read-only device data
+// (layout tables, interface matrices, factors and solve plans) plus a pool of
+// solve contexts (PCG vectors, sigma V-cycle buffers and a captured CUDA graph
+// of the preconditioner, each on its own stream).  A worker takes the oldest
+// queued request whose domain is resident and has an idle context, or room in
+// the HBM budget for a new one (at most `slots` per domain), so requests on
+// one domain overlap on the device as well as requests on different domains.
+// Every context runs the same kernels in the same order, so a request's
+// result does not depend on which context or how many others ran beside it.
+// Domains are admitted in arrival order once their estimated device footprint
+// fits the HBM budget; their host setup (layout, interface assembly,
+// factorisation) runs on a worker with setup_threads OpenMP threads, so
+// setups overlap with solves of other domains.
 #include <omp.h>
 
 #include <algorithm>
@@ -31,6 +36,7 @@
 
 using hdd::Error;
 using hdd::Solver;
+using hdd::Work;
 using Clock = std::chrono::steady_clock;
 
 namespace {
@@ -44,8 +50,12 @@ struct Domain {
     hdd_status status = HDD_OK;      // setup failure status
     std::string error;
     std::unique_ptr<Solver> solver;
+    std::vector<std::unique_ptr<Work>> extra;  // contexts beyond the solver's first
+    std::vector<Work*> idle;         // contexts free for a request
+    int contexts = 0;                // contexts made (the first included)
+    long long work_bytes = 0;        // device bytes of one further context
     long long reserved = 0;          // bytes counted against the budget
-    bool busy = false;               // a worker is solving on it
+    int running = 0;                 // requests being solved on it
     bool removing = false;
     int queued = 0;                  // requests not yet finished
 };
@@ -173,6 +183,9 @@ struct hdd_server {
             reserved += actual - dd.reserved;
             dd.reserved = actual;
             dd.solver = std::move(s);
+            dd.idle.assign(1, &dd.solver->w0);
+            dd.contexts = 1;
+            dd.work_bytes = (long long)dd.solver->work_bytes();
             dd.state = DomainState::Resident;
         } else {
             reserved -= dd.reserved;
@@ -188,24 +201,41 @@ struct hdd_server {
     void run_solve(long long rid, std::unique_lock<std::mutex>& lk) {
         Request& r = requests.at(rid);
         Domain& d = domains.at(r.domain);
-        d.busy = true;
+        ++d.running;
         Solver* s = d.solver.get();
+        Work* w = nullptr;
+        bool fresh = false;  // a new context, its bytes already reserved
+        if (!d.idle.empty()) {
+            w = d.idle.back();
+            d.idle.pop_back();
+        } else {
+            fresh = true;
+            ++d.contexts;
+            d.reserved += d.work_bytes;
+            reserved += d.work_bytes;
+        }
+        const long long wb = d.work_bytes;
         std::vector<float> rhs;
         rhs.swap(r.rhs);
         lk.unlock();
         hdd_status st = HDD_OK;
         hdd_result res{};
         std::vector<float> x;
+        std::unique_ptr<Work> made;
         try {
-            s->set_rhs(rhs.data());
+            if (fresh) {
+                made = s->make_work();
+                w = made.get();
+            }
+            s->set_rhs(*w, rhs.data());
             try {
-                s->solve(&res);
+                s->solve(*w, &res);
             } catch (const Error& e) {
                 if (e.status != HDD_ERR_NOT_CONVERGED) throw;
                 st = e.status;
             }
             x.resize(rhs.size());
-            s->get_solution(x.data());
+            s->get_solution(*w, x.data());
         } catch (const Error& e) {
             st = e.status;
         } catch (const std::bad_alloc&) {
@@ -219,15 +249,33 @@ struct hdd_server {
         rr.x.swap(x);
         finish(rr, st);
         Domain& dd = domains.at(rr.domain);
-        dd.busy = false;
+        if (made) {
+            dd.extra.push_back(std::move(made));
+        } else if (fresh) {
+            // The context could not be made: give its reservation back.
+            --dd.contexts;
+            dd.reserved -= wb;
+            reserved -= wb;
+            w = nullptr;
+        }
+        if (w) dd.idle.push_back(w);
+        --dd.running;
         --dd.queued;
+    }
+
+    // Whether a queued request of `d` can start now: an idle context, or
+    // room for one more (at most `slots` per domain, within the budget).
+    bool can_run(const Domain& d) const {
+        if (d.state != DomainState::Resident) return false;
+        if (!d.idle.empty()) return true;
+        return d.contexts < opt.slots && reserved + d.work_bytes <= budget;
     }
 
     // Index in `queue` of the oldest request whose domain can run now, or -1.
     long long runnable() {
         for (size_t i = 0; i < queue.size(); ++i) {
             const Domain& d = domains.at(requests.at(queue[i]).domain);
-            if (d.state == DomainState::Resident && !d.busy) return (long long)i;
+            if (can_run(d)) return (long long)i;
         }
         return -1;
     }
@@ -329,6 +377,9 @@ hdd_status hdd_server_add_domain(hdd_server* srv, const hdd_options* opts, const
         Domain d;
         d.opts = *opts;
         d.opts.device = srv->opt.device;
+        // Each request's persistent interface solves take a share of the
+        // device, so that `slots` of them run side by side.
+        if (d.opts.solve_share == 0) d.opts.solve_share = srv->opt.slots;
         const size_t n = (size_t)opts->size[0] * opts->size[1] * opts->size[2];
         d.flags.assign(flags, flags + n);
         d.reserved = estimate_bytes(d.opts, flags);
@@ -421,6 +472,7 @@ hdd_status hdd_server_poll(hdd_server* srv, long long request_id, int wait_ms, h
 hdd_status hdd_server_remove_domain(hdd_server* srv, long long domain_id) {
     return guarded(srv, [&] {
         std::unique_ptr<Solver> s;
+        std::vector<std::unique_ptr<Work>> extra;
         {
             std::unique_lock<std::mutex> lk(srv->mu);
             auto it = srv->domains.find(domain_id);
@@ -428,7 +480,7 @@ hdd_status hdd_server_remove_domain(hdd_server* srv, long long domain_id) {
             it->second.removing = true;
             srv->cv.wait(lk, [&] {
                 const Domain& d = srv->domains.at(domain_id);
-                return srv->stop || (d.queued == 0 && !d.busy && d.state != DomainState::SettingUp &&
+                return srv->stop || (d.queued == 0 && d.running == 0 && d.state != DomainState::SettingUp &&
                                      d.state != DomainState::Admitted);
             });
             if (srv->stop) return HDD_ERR_BUSY;
@@ -440,11 +492,13 @@ hdd_status hdd_server_remove_domain(hdd_server* srv, long long domain_id) {
                 srv->reserved -= d.reserved;
             }
             s = std::move(d.solver);
+            extra.swap(d.extra);
             srv->domains.erase(domain_id);
             srv->admit();
             srv->cv.notify_all();
         }
-        s.reset();  // device memory freed outside the lock
+        extra.clear();  // device memory freed outside the lock, contexts before the solver they read
+        s.reset();
         return HDD_OK;
     });
 }

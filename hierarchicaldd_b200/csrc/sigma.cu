@@ -331,43 +331,129 @@ void SigmaGpu::setup(const InterfaceHost& ih, int smoothing_iterations, cudaStre
     ck(cudaStreamSynchronize(s), "sigma setup");
 }
 
-void SigmaGpu::vcycle(cudaStream_t s, long long& launches, PhaseHook* hook) {
+SigmaScratch SigmaGpu::primary() const {
+    SigmaScratch sc;
+    sc.lv.resize(lv.size());
+    for (size_t l = 0; l < lv.size(); ++l) {
+        const SigmaLevel& L = lv[l];
+        SigmaScratch::Level& S = sc.lv[l];
+        S.u = L.u; S.r = L.r; S.b = L.b; S.tmp = L.tmp; S.vb = L.vb; S.vx = L.vx;
+        S.aii = L.aii.primary();
+        S.arr = L.arr_solve.primary();
+    }
+    sc.bottom = bottom.primary();
+    sc.kb = kb;
+    sc.kx = kx;
+    sc.err = d_err;
+    return sc;
+}
+
+void SigmaGpu::alloc_scratch(SigmaScratch& sc, cudaStream_t s) const {
+    free_scratch(sc);
+    size_t& b = sc.bytes;
+    sc.err = dev::alloc_zero<int>(1, b, s);
+    sc.lv.resize(lv.size());
+    for (size_t l = 0; l < lv.size(); ++l) {
+        const SigmaLevel& L = lv[l];
+        SigmaScratch::Level& S = sc.lv[l];
+        S.u = dev::alloc_zero<float>(std::max(L.n_iface, 1), b, s);
+        S.r = dev::alloc_zero<float>(std::max(L.n_iface, 1), b, s);
+        S.b = dev::alloc_zero<float>(std::max(L.n_iface, 1), b, s);
+        S.tmp = dev::alloc_zero<float>(std::max(L.n_iface, 1), b, s);
+        S.vb = dev::alloc_zero<float>(std::max(L.n_int, 1), b, s);
+        S.vx = dev::alloc_zero<float>(std::max(L.n_int, 1), b, s);
+        if (L.aii.nsn > 0) L.aii.alloc_scratch(S.aii, sc.err, s, b);
+        if (L.arr_solve.nsn > 0) L.arr_solve.alloc_scratch(S.arr, sc.err, s, b);
+    }
+    if (bottom.nsn > 0) bottom.alloc_scratch(sc.bottom, sc.err, s, b);
+    if (kb) {
+        sc.kb = dev::alloc_zero<float>(std::max(n_bottom_int + n_bottom, 1), b, s);
+        sc.kx = dev::alloc_zero<float>(std::max(n_bottom_int + n_bottom, 1), b, s);
+    }
+}
+
+size_t SigmaGpu::scratch_bytes() const {
+    size_t t = 4;
+    for (const SigmaLevel& L : lv) {
+        t += 16 * (size_t)std::max(L.n_iface, 1) + 8 * (size_t)std::max(L.n_int, 1);
+        t += L.aii.scratch_bytes() + L.arr_solve.scratch_bytes();
+    }
+    t += bottom.scratch_bytes();
+    if (kb) t += 8 * (size_t)std::max(n_bottom_int + n_bottom, 1);
+    return t;
+}
+
+void SigmaGpu::free_scratch(SigmaScratch& sc) {
+    for (SigmaScratch::Level& S : sc.lv) {
+        dev::release(S.u); dev::release(S.r); dev::release(S.b); dev::release(S.tmp); dev::release(S.vb);
+        dev::release(S.vx);
+        SolvePlan::free_scratch(S.aii);
+        SolvePlan::free_scratch(S.arr);
+    }
+    sc.lv.clear();
+    SolvePlan::free_scratch(sc.bottom);
+    dev::release(sc.kb);
+    dev::release(sc.kx);
+    dev::release(sc.err);
+    sc.bytes = 0;
+}
+
+void SigmaGpu::vcycle(cudaStream_t s, long long& launches, PhaseHook* hook) { vcycle(primary(), s, launches, hook); }
+
+void SigmaGpu::vcycle(const SigmaScratch& sc, cudaStream_t s, long long& launches, PhaseHook* hook) {
     auto schur_apply = [&](int l, const float* u, float* out_tmp) {
-        SigmaLevel& L = lv[l];
-        launch_csr(L.air, u, nullptr, L.vb, 0, s, launches);
-        L.aii.solve(L.vb, L.vx, s, launches, hook);
-        launch_csr(L.airT, L.vx, L.b, out_tmp, 1, s, launches);  // tmp = b + Air^T vx
+        const SigmaLevel& L = lv[l];
+        const SigmaScratch::Level& S = sc.lv[l];
+        launch_csr(L.air, u, nullptr, S.vb, 0, s, launches);
+        L.aii.solve(S.aii, S.vb, S.vx, s, launches, hook);
+        launch_csr(L.airT, S.vx, S.b, out_tmp, 1, s, launches);  // tmp = b + Air^T vx
     };
     auto smooth = [&](int l) {
-        SigmaLevel& L = lv[l];
-        schur_apply(l, L.u, L.tmp);
-        L.arr_solve.solve(L.tmp, L.u, s, launches, hook);
+        const SigmaScratch::Level& S = sc.lv[l];
+        schur_apply(l, S.u, S.tmp);
+        lv[l].arr_solve.solve(S.arr, S.tmp, S.u, s, launches, hook);
     };
     for (int l = 0; l + 1 < M; ++l) {
-        SigmaLevel& L = lv[l];
+        const SigmaLevel& L = lv[l];
+        const SigmaScratch::Level& S = sc.lv[l];
         for (int i = 0; i < smoothing; ++i) smooth(l);
-        schur_apply(l, L.u, L.tmp);
-        launch_csr(L.arr, L.u, L.tmp, L.r, 2, s, launches);           // r = tmp - Arr u
-        launch_fill(lv[l + 1].u, lv[l + 1].n_iface, 0.0f, s, launches);
-        launch_csr(L.prrT, L.r, nullptr, lv[l + 1].b, 0, s, launches); // b_{l+1} = Prr^T r
+        schur_apply(l, S.u, S.tmp);
+        launch_csr(L.arr, S.u, S.tmp, S.r, 2, s, launches);                 // r = tmp - Arr u
+        launch_fill(sc.lv[l + 1].u, lv[l + 1].n_iface, 0.0f, s, launches);
+        launch_csr(L.prrT, S.r, nullptr, sc.lv[l + 1].b, 0, s, launches);  // b_{l+1} = Prr^T r
     }
     if (!bottom_exact) {
         for (int i = 0; i < kBottomSmoothing; ++i) smooth(M - 1);
     } else {
-        SigmaLevel& B = lv[M - 1];
+        const SigmaScratch::Level& B = sc.lv[M - 1];
         if (n_bottom > 0) {
             // Right-hand side [0; b], solution's interface block -> u.
-            if (n_bottom_int > 0) ck(cudaMemsetAsync(kb, 0, sizeof(float) * n_bottom_int, s), "memset kb");
-            ck(cudaMemcpyAsync(kb + n_bottom_int, B.b, sizeof(float) * n_bottom, cudaMemcpyDeviceToDevice, s), "copy b");
-            bottom.solve(kb, kx, s, launches, hook);
-            ck(cudaMemcpyAsync(B.u, kx + n_bottom_int, sizeof(float) * n_bottom, cudaMemcpyDeviceToDevice, s), "copy u");
+            if (n_bottom_int > 0) ck(cudaMemsetAsync(sc.kb, 0, sizeof(float) * n_bottom_int, s), "memset kb");
+            ck(cudaMemcpyAsync(sc.kb + n_bottom_int, B.b, sizeof(float) * n_bottom, cudaMemcpyDeviceToDevice, s),
+               "copy b");
+            bottom.solve(sc.bottom, sc.kb, sc.kx, s, launches, hook);
+            ck(cudaMemcpyAsync(B.u, sc.kx + n_bottom_int, sizeof(float) * n_bottom, cudaMemcpyDeviceToDevice, s),
+               "copy u");
         }
     }
     for (int l = M - 2; l >= 0; --l) {
-        SigmaLevel& L = lv[l];
-        launch_csr(L.prr, lv[l + 1].u, nullptr, L.u, 3, s, launches);  // u += Prr u_{l+1}
+        const SigmaLevel& L = lv[l];
+        const SigmaScratch::Level& S = sc.lv[l];
+        launch_csr(L.prr, sc.lv[l + 1].u, nullptr, S.u, 3, s, launches);  // u += Prr u_{l+1}
         for (int i = 0; i < smoothing; ++i) smooth(l);
     }
+}
+
+int SigmaGpu::error_flag(const SigmaScratch& sc, cudaStream_t s) {
+    if (!sc.err) return 0;
+    int h = 0;
+    ck(cudaMemcpyAsync(&h, sc.err, sizeof(int), cudaMemcpyDeviceToHost, s), "read error word");
+    ck(cudaStreamSynchronize(s), "read error word");
+    return h;
+}
+
+void SigmaGpu::clear_error(const SigmaScratch& sc, cudaStream_t s) {
+    if (sc.err) ck(cudaMemsetAsync(sc.err, 0, sizeof(int), s), "clear error word");
 }
 
 int SigmaGpu::error_flag(cudaStream_t s) const {

@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <array>
 #include <cstdint>
 #include <string>
@@ -148,6 +149,21 @@ struct SnTask {
     long long part;
 };
 
+// The device buffers one supernodal solve writes (split-block partial sums,
+// update vectors, forward and backward results, task counters, error word):
+// every solve context of a plan has its own, so solves of one plan on
+// different streams can run at the same time.
+struct PlanScratch {
+    double *part = nullptr, *upd = nullptr, *ynew = nullptr, *xnew = nullptr;
+    int* ctr = nullptr;
+    int* err = nullptr;
+    bool own_err = false;
+    // The persistent launches use 1/grid_div of the plan's CTAs (rounded up),
+    // leaving room on the device for concurrent solves; the results do not
+    // depend on it.
+    int grid_div = 1;
+};
+
 // Device plan for a batch of independent supernodal triangular solves.
 struct SolvePlan {
     int n = 0;                       // total unknowns (concatenated)
@@ -184,9 +200,22 @@ struct SolvePlan {
     void build(const std::vector<const SnFactor*>& factors, const std::vector<int>& offsets, cudaStream_t s,
                int* shared_err = nullptr);
     void release();
-    // x_old = (A+eps I)^{-1} b_old (both in the concatenated original order).
+    long long part_len = 0, upd_len = 0;  // doubles in a scratch's partial-sum and update buffers
+    // x_old = (A+eps I)^{-1} b_old (both in the concatenated original order),
+    // with the plan's own scratch or a context's.
     void solve(const float* b_old, float* x_old, cudaStream_t s, long long& launches,
                PhaseHook* hook = nullptr) const;
+    void solve(const PlanScratch& sc, const float* b_old, float* x_old, cudaStream_t s, long long& launches,
+               PhaseHook* hook = nullptr) const;
+    // Scratch for another solve context (error word shared_err, or its own).
+    void alloc_scratch(PlanScratch& sc, int* shared_err, cudaStream_t s, size_t& bytes) const;
+    static void free_scratch(PlanScratch& sc);
+    PlanScratch primary() const;
+    // Device bytes alloc_scratch takes (without a shared error word).
+    size_t scratch_bytes() const {
+        if (nsn == 0) return 0;
+        return 8 * (size_t)(part_len + upd_len) + 16 * (size_t)std::max(n, 1) + 4 * (size_t)std::max(n_ctr, 1) + 4;
+    }
     int error_flag(cudaStream_t s) const;
     // Test seam: on = raise the forward task count that one front's parent
     // waits for by one, so that wait can never be satisfied and runs into its
@@ -214,6 +243,28 @@ struct SigmaLevel {
     float *u = nullptr, *r = nullptr, *b = nullptr, *tmp = nullptr, *vb = nullptr, *vx = nullptr;
 };
 
+// The device buffers one sigma V-cycle writes: every level's vectors, the
+// scratch of its solve plans, the coarsest level's [0; b] / solution pair and
+// the error word.  The solver's first solve context uses the SigmaGpu's own;
+// further contexts (concurrent solves of one resident domain) allocate theirs.
+struct SigmaScratch {
+    struct Level {
+        float *u = nullptr, *r = nullptr, *b = nullptr, *tmp = nullptr, *vb = nullptr, *vx = nullptr;
+        PlanScratch aii, arr;
+    };
+    std::vector<Level> lv;
+    PlanScratch bottom;
+    void set_grid_div(int div) {
+        for (Level& L : lv) L.aii.grid_div = L.arr.grid_div = div;
+        bottom.grid_div = div;
+    }
+    float *kb = nullptr, *kx = nullptr;
+    int* err = nullptr;
+    size_t bytes = 0;
+    float* b0() const { return lv.empty() ? nullptr : lv[0].b; }
+    float* u0() const { return lv.empty() ? nullptr : lv[0].u; }
+};
+
 struct SigmaGpu {
     int M = 0, smoothing = 3;
     std::vector<SigmaLevel> lv;
@@ -236,11 +287,19 @@ struct SigmaGpu {
     // smoothing steps have not converged (HDD_COARSE_EXACT).
     void setup(const InterfaceHost& ih, int smoothing_iterations, cudaStream_t s, bool force_exact = false);
     void release();
-    // u[0] = sigma V-cycle(b[0]) (SIGMA_MULTIGRID_SOLVER.cpp:35-47), u[0] starting at 0.
+    // u[0] = sigma V-cycle(b[0]) (SIGMA_MULTIGRID_SOLVER.cpp:35-47), u[0] starting at 0,
+    // in the given scratch (default: the SigmaGpu's own).
     void vcycle(cudaStream_t s, long long& launches, PhaseHook* hook = nullptr);
+    void vcycle(const SigmaScratch& sc, cudaStream_t s, long long& launches, PhaseHook* hook = nullptr);
+    SigmaScratch primary() const;
+    void alloc_scratch(SigmaScratch& sc, cudaStream_t s) const;
+    size_t scratch_bytes() const;
+    static void free_scratch(SigmaScratch& sc);
     // Nonzero when a bounded wait inside a supernodal solve gave up.
     int error_flag(cudaStream_t s) const;
     void clear_error(cudaStream_t s);
+    static int error_flag(const SigmaScratch& sc, cudaStream_t s);
+    static void clear_error(const SigmaScratch& sc, cudaStream_t s);
     // Poll limit of every bounded wait (default 1 << 22).
     void set_wait_limit(long long polls);
     // Test seam (SolvePlan::stall_dependency) on the level-0 interface plan.

@@ -646,17 +646,14 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
     d_bfwd = dev::upload(bfwd.empty() ? std::vector<int>{0} : bfwd, s, bytes);
     d_bbwd = dev::upload(bbwd.empty() ? std::vector<int>{0} : bbwd, s, bytes);
     d_fw = dev::upload(fw, s, bytes);
-    d_part = dev::alloc_zero<double>(std::max<long long>(part_total, 1), bytes, s);
-    d_upd = dev::alloc_zero<double>(std::max<long long>(upd_total, 1), bytes, s);
-    d_ynew = dev::alloc_zero<double>(std::max(n, 1), bytes, s);
-    d_xnew = dev::alloc_zero<double>(std::max(n, 1), bytes, s);
-    d_ctr = dev::alloc_zero<int>(n_ctr, bytes, s);
-    if (shared_err) {
-        d_err = shared_err;
-        own_err = false;
-    } else {
-        d_err = dev::alloc_zero<int>(1, bytes, s);
-        own_err = true;
+    part_len = std::max<long long>(part_total, 1);
+    upd_len = std::max<long long>(upd_total, 1);
+    {
+        PlanScratch sc;
+        alloc_scratch(sc, shared_err, s, bytes);
+        d_part = sc.part; d_upd = sc.upd; d_ynew = sc.ynew; d_xnew = sc.xnew; d_ctr = sc.ctr;
+        d_err = sc.err;
+        own_err = sc.own_err;
     }
     // A front with a parent, for stall_dependency (the wait of its parent's
     // forward tasks on it can be made unsatisfiable).
@@ -693,19 +690,53 @@ void SolvePlan::release() {
     n_fwd = n_bwd = n_ctr = 0;
 }
 
+void SolvePlan::alloc_scratch(PlanScratch& sc, int* shared_err, cudaStream_t s, size_t& b) const {
+    sc.part = dev::alloc_zero<double>(part_len, b, s);
+    sc.upd = dev::alloc_zero<double>(upd_len, b, s);
+    sc.ynew = dev::alloc_zero<double>(std::max(n, 1), b, s);
+    sc.xnew = dev::alloc_zero<double>(std::max(n, 1), b, s);
+    sc.ctr = dev::alloc_zero<int>(std::max(n_ctr, 1), b, s);
+    if (shared_err) {
+        sc.err = shared_err;
+        sc.own_err = false;
+    } else {
+        sc.err = dev::alloc_zero<int>(1, b, s);
+        sc.own_err = true;
+    }
+}
+
+void SolvePlan::free_scratch(PlanScratch& sc) {
+    dev::release(sc.part); dev::release(sc.upd); dev::release(sc.ynew); dev::release(sc.xnew); dev::release(sc.ctr);
+    if (sc.own_err) dev::release(sc.err);
+    sc.err = nullptr;
+    sc.own_err = false;
+}
+
+PlanScratch SolvePlan::primary() const {
+    PlanScratch sc;
+    sc.part = d_part; sc.upd = d_upd; sc.ynew = d_ynew; sc.xnew = d_xnew; sc.ctr = d_ctr; sc.err = d_err;
+    sc.own_err = false;
+    return sc;
+}
+
 void SolvePlan::solve(const float* b_old, float* x_old, cudaStream_t s, long long& launches, PhaseHook* hook) const {
+    solve(primary(), b_old, x_old, s, launches, hook);
+}
+
+void SolvePlan::solve(const PlanScratch& sc, const float* b_old, float* x_old, cudaStream_t s, long long& launches,
+                      PhaseHook* hook) const {
     if (nsn == 0) return;
     PlanView P{nsn, max_front, d_col0, d_ncol, d_nrow, d_parent, d_rows, d_rows_off, d_child_ptr, d_child,
-               d_relmap_off, d_relmap, d_upd_off, d_fw_off, d_ntf, d_ntb, d_perm, d_bfwd, d_bbwd, d_fw, d_part, d_upd,
-               d_ynew,
-               d_xnew, d_ctr, d_err, spin_limit};
-    dev::ck(cudaMemsetAsync(d_ctr, 0, sizeof(int) * n_ctr, s), "reset counters");
+               d_relmap_off, d_relmap, d_upd_off, d_fw_off, d_ntf, d_ntb, d_perm, d_bfwd, d_bbwd, d_fw, sc.part, sc.upd,
+               sc.ynew, sc.xnew, sc.ctr, sc.err, spin_limit};
+    dev::ck(cudaMemsetAsync(sc.ctr, 0, sizeof(int) * n_ctr, s), "reset counters");
+    const int g = sc.grid_div > 1 ? std::max(1, (grid + sc.grid_div - 1) / sc.grid_div) : grid;
     if (hook) hook->begin(kPhaseSnForward);
-    sn_forward_kernel<<<std::min(grid, n_fwd), kNT, forward_smem(max_front), s>>>(P, d_fwd, n_fwd, b_old);
+    sn_forward_kernel<<<std::min(g, n_fwd), kNT, forward_smem(max_front), s>>>(P, d_fwd, n_fwd, b_old);
     dev::ck(cudaGetLastError(), "sn forward");
     if (hook) hook->end(kPhaseSnForward, fwd_bytes);
     if (hook) hook->begin(kPhaseSnBackward);
-    sn_backward_kernel<<<std::min(grid, n_bwd), kNT, backward_smem(max_front), s>>>(P, d_bwd, n_bwd, x_old);
+    sn_backward_kernel<<<std::min(g, n_bwd), kNT, backward_smem(max_front), s>>>(P, d_bwd, n_bwd, x_old);
     dev::ck(cudaGetLastError(), "sn backward");
     if (hook) hook->end(kPhaseSnBackward, bwd_bytes);
     launches += 2;

@@ -46,6 +46,7 @@ Solver::Solver(const hdd_options& o) : opts(o) {
     if (o.sub_size[0] != o.sub_size[1] || o.sub_size[0] != o.sub_size[2])
         throw Error(HDD_ERR_UNSUPPORTED, "sub_size must be equal on all axes");
     if (o.vlevels < 1 || o.vlevels > kMaxLevels) throw Error(HDD_ERR_INVALID_ARGUMENT, "vlevels out of range");
+    if (o.solve_share < 0 || o.solve_share > 64) throw Error(HDD_ERR_INVALID_ARGUMENT, "solve_share out of range");
     if (o.coarse_solve != HDD_COARSE_REFERENCE && o.coarse_solve != HDD_COARSE_EXACT)
         throw Error(HDD_ERR_INVALID_ARGUMENT, "coarse_solve must be HDD_COARSE_REFERENCE or HDD_COARSE_EXACT");
     if (o.sigma_levels < 1 || o.nVcycles < 0 || o.sigma_mg < 0 || o.interior_smoothing < 0 ||
@@ -55,15 +56,33 @@ Solver::Solver(const hdd_options& o) : opts(o) {
     cuda_check(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
     if (o.device < 0 || o.device >= ndev) throw Error(HDD_ERR_INVALID_ARGUMENT, "device ordinal out of range");
     cuda_check(cudaSetDevice(o.device), "cudaSetDevice");
-    cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    cuda_check(cudaStreamCreateWithFlags(&w0.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    w0.own_stream = true;
 }
 
 Solver::~Solver() {
     if (stream) {
         cudaStreamSynchronize(stream);
+        release_graphs();
         sigma.release();
-        cudaStreamDestroy(stream);
     }
+}
+
+Work::~Work() {
+    if (!stream) return;
+    cudaStreamSynchronize(stream);
+    release_graphs();
+    if (own_sig) SigmaGpu::free_scratch(sig);
+    if (own_stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+}
+
+void Work::release_graphs() {
+    if (pc_exec) cudaGraphExecDestroy(pc_exec);
+    pc_exec = nullptr;
+    pc_r = nullptr;
+    pc_z = nullptr;
+    pc_launches = 0;
 }
 
 void Solver::collect_timing() {
@@ -87,7 +106,7 @@ void Solver::set_domain(const uint32_t* flags, const float* rhs) {
     rhs_dense.assign(rhs, rhs + n);
     have_domain = true;
     initialized = false;
-    solved = false;
+    w0.solved = false;
 }
 
 void Solver::set_domain(std::vector<uint32_t>&& flags, std::vector<float>&& rhs) {
@@ -97,7 +116,7 @@ void Solver::set_domain(std::vector<uint32_t>&& flags, std::vector<float>&& rhs)
     rhs_dense = std::move(rhs);
     have_domain = true;
     initialized = false;
-    solved = false;
+    w0.solved = false;
 }
 
 TileGeom Solver::geom() const {
@@ -111,6 +130,7 @@ TileGeom Solver::geom() const {
 
 void Solver::initialize() {
     if (!have_domain) throw Error(HDD_ERR_NOT_INITIALIZED, "no domain set");
+    release_graphs();
     NvtxRange range("Initialize_Preconditioner");
     cuda_check(cudaSetDevice(opts.device), "cudaSetDevice");
     const auto t0 = std::chrono::steady_clock::now();
@@ -135,17 +155,14 @@ void Solver::initialize() {
             for (int a = 0; a < 3; ++a) txyz[3 * t + a] = L.tiles[t][a];
         tile_xyz.upload(txyz.data(), txyz.size(), stream);
     }
-    dense.alloc(std::max<size_t>(L.cell_count(), 1));
     tflags.upload(L.tile_flags.data(), L.tile_flags.size(), stream);
     {
-        // Algorithmic HBM bytes of one launch: the Laplacian reads s and the
-        // flags and writes q at each Active|Interface cell (4 + 2 + 4 + the
-        // per-tile partial, rounded to 12 B per cell); the V-cycle reads u, b
-        // and the level-0 flags and writes u once per box cell (13 B).
-        size_t nsolve = 0;
-        for (uint16_t f : L.tile_flags) nsolve += (f & (C_ACTIVE | C_INTERFACE)) ? 1 : 0;
+        // Algorithmic HBM bytes of one launch: the Laplacian reads s (4 B)
+        // and the flags (2 B) and writes q (4 B) once per stored tile cell,
+        // the storage unit of the tiled vectors (10 B); the V-cycle reads u,
+        // b and the level-0 flags and writes u once per box cell (13 B).
         const double sub3 = (double)L.opt.sub[0] * L.opt.sub[0] * L.opt.sub[0];
-        laplace_bytes = 12.0 * (double)nsolve;
+        laplace_bytes = 10.0 * sub3 * (double)L.tiles.size();
         vcycle_bytes = 13.0 * sub3 * (double)L.boxes.size();
     }
     std::vector<int> btile(L.boxes.size()), bnb(3 * L.boxes.size());
@@ -156,15 +173,9 @@ void Solver::initialize() {
     box_tile.upload(btile.data(), btile.size(), stream);
     box_nb.upload(bnb.data(), bnb.size(), stream);
     box_flags.upload(L.box_flags.data(), L.box_flags.size(), stream);
-    for (DevBuf<float>* v : {&x, &b, &r, &z, &s, &q}) { v->alloc(std::max<size_t>(N, 1)); v->zero(stream); }
-    if (opts.precision_mode == HDD_PRECISION_MIXED) xd.alloc(std::max<size_t>(N, 1));
-    else xd.release();
-    partial.alloc(std::max<size_t>(nt, 1));
-    partial_max.alloc(std::max<size_t>(nt, 1));
-    sums.alloc(8);
-    scalars_f.alloc(8);
-    scal.alloc(1);
+    alloc_vectors(w0);
     (void)S;
+    (void)N;
 
     // Interface system (host assembly + factorisations) and its device solver.
     auto since_ms = [&](std::chrono::steady_clock::time_point a) {
@@ -221,6 +232,9 @@ void Solver::initialize() {
     }
     iface_slot.upload(slot.data(), slot.size(), stream);
     iface_nb.upload(nbs.data(), nbs.size(), stream);
+    w0.sig = sigma.primary();
+    w0.sig.set_grid_div(std::max(1, opts.solve_share));
+    w0.own_sig = false;
     set_rhs(rhs_dense.data());
     sync();
     initialized = true;
@@ -228,15 +242,54 @@ void Solver::initialize() {
     setup_phase_ms[3] = setup_ms;
 }
 
-void Solver::set_rhs(const float* rhs) {
+void Solver::alloc_vectors(Work& w) {
+    const size_t nt = L.tiles.size(), N = nt * (size_t)L.tile_cells;
+    w.dense.alloc(std::max<size_t>(L.cell_count(), 1));
+    for (DevBuf<float>* v : {&w.x, &w.b, &w.r, &w.z, &w.s, &w.q}) { v->alloc(std::max<size_t>(N, 1)); v->zero(w.stream); }
+    if (opts.precision_mode == HDD_PRECISION_MIXED) w.xd.alloc(std::max<size_t>(N, 1));
+    else w.xd.release();
+    w.partial.alloc(std::max<size_t>({nt, (size_t)laplace_partials(geom()), (size_t)1}));
+    w.partial_max.alloc(std::max<size_t>(nt, 1));
+    w.sums.alloc(8);
+    w.scalars_f.alloc(8);
+    w.scal.alloc(1);
+}
+
+std::unique_ptr<Work> Solver::make_work() {
+    if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+    std::unique_ptr<Work> w(new Work());
+    cuda_check(cudaSetDevice(opts.device), "cudaSetDevice");
+    cuda_check(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    w->own_stream = true;
+    alloc_vectors(*w);
+    if (!sigma.lv.empty()) {
+        sigma.alloc_scratch(w->sig, w->stream);
+        w->sig.set_grid_div(std::max(1, opts.solve_share));
+        w->own_sig = true;
+    }
+    sync(*w);
+    return w;
+}
+
+size_t Solver::work_bytes() const {
+    const size_t nt = L.tiles.size(), N = nt * (size_t)L.tile_cells;
+    size_t t = std::max<size_t>(L.cell_count(), 1) * 4 + 6 * std::max<size_t>(N, 1) * 4;
+    if (opts.precision_mode == HDD_PRECISION_MIXED) t += std::max<size_t>(N, 1) * 8;
+    t += std::max<size_t>({nt, (size_t)laplace_partials(geom()), (size_t)1}) * 8 + std::max<size_t>(nt, 1) * 4 + 128 +
+         sizeof(PcgScalars);
+    return t + sigma.scratch_bytes();
+}
+
+void Solver::set_rhs(Work& w, const float* rhs) {
     // H2D of the dense right-hand side, then a device gather into the tiles.
-    if (rhs != rhs_dense.data()) rhs_dense.clear();
-    Tm tm(this, 5);
-    cuda_check(cudaMemcpyAsync(dense.p, rhs, L.cell_count() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D rhs");
-    cuda_check(launch_dense_to_tiles(geom(), tile_xyz.p, L.opt.size[0], L.opt.size[1], L.opt.size[2], dense.p, b.p,
-                                     stream), "dense_to_tiles");
-    count();
-    sync();
+    if (&w == &w0 && rhs != rhs_dense.data()) rhs_dense.clear();
+    Tm tm(this, w, 5);
+    cuda_check(cudaMemcpyAsync(w.dense.p, rhs, L.cell_count() * sizeof(float), cudaMemcpyHostToDevice, w.stream),
+               "H2D rhs");
+    cuda_check(launch_dense_to_tiles(geom(), tile_xyz.p, L.opt.size[0], L.opt.size[1], L.opt.size[2], w.dense.p,
+                                     w.b.p, w.stream), "dense_to_tiles");
+    count(w);
+    sync(w);
 }
 
 VcycleArgs Solver::vcycle_args(float* u, const float* bb, int halo_from_u, int zero_init, int nv) const {
@@ -278,43 +331,88 @@ VcycleArgs Solver::vcycle_args(float* u, const float* bb, int halo_from_u, int z
     return a;
 }
 
-void Solver::run_vcycle(float* u, const float* bb, int halo_from_u, int zero_init, int nv) {
+void Solver::run_vcycle(Work& w, float* u, const float* bb, int halo_from_u, int zero_init, int nv) {
     VcycleArgs a = vcycle_args(u, bb, halo_from_u, zero_init, nv);
-    Tm tm(this, 0, vcycle_bytes);
-    cuda_check(launch_vcycle(a, stream), "vcycle kernel");
-    count();
+    Tm tm(this, w, 0, vcycle_bytes);
+    cuda_check(launch_vcycle(a, w.stream), "vcycle kernel");
+    count(w);
 }
 
-void Solver::apply_preconditioner(const float* rr, float* zz) {
+void Solver::apply_preconditioner(Work& w, const float* rr, float* zz) {
+    // One application is a fixed sequence of launches on fixed buffers (for a
+    // 32^3-subdomain domain whose coarsest interface level runs the 200
+    // smoothing steps, well over a thousand): it is captured once as a CUDA
+    // graph and replayed, so the host issues one launch per application.
+    // Per-phase timing needs events between the launches and runs them
+    // directly; a failed capture falls back to direct launches for good.
+    if (w.use_graphs && !timing) {
+        if (w.pc_exec && w.pc_r == rr && w.pc_z == zz) {
+            cuda_check(cudaGraphLaunch(w.pc_exec, w.stream), "cudaGraphLaunch");
+            w.launches += w.pc_launches;
+            return;
+        }
+        w.release_graphs();
+        cudaGraph_t graph = nullptr;
+        const long long before = w.launches;
+        if (cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            bool ok = true;
+            try {
+                apply_preconditioner_launches(w, rr, zz);
+            } catch (const Error&) {
+                ok = false;
+            }
+            const cudaError_t e = cudaStreamEndCapture(w.stream, &graph);
+            if (ok && e == cudaSuccess && graph &&
+                cudaGraphInstantiate(&w.pc_exec, graph, 0) == cudaSuccess) {
+                cudaGraphDestroy(graph);
+                w.pc_r = rr;
+                w.pc_z = zz;
+                w.pc_launches = w.launches - before;
+                w.launches = before;
+                cuda_check(cudaGraphLaunch(w.pc_exec, w.stream), "cudaGraphLaunch");
+                w.launches += w.pc_launches;
+                return;
+            }
+            if (graph) cudaGraphDestroy(graph);
+            w.pc_exec = nullptr;
+            cudaGetLastError();  // clear a capture error; run the launches directly from now on
+        }
+        w.launches = before;
+        w.use_graphs = false;
+    }
+    apply_preconditioner_launches(w, rr, zz);
+}
+
+void Solver::apply_preconditioner_launches(Work& w, const float* rr, float* zz) {
     NvtxRange range("Apply_Preconditioner");
     const TileGeom g = geom();
     {
         NvtxRange step("Step ONE");
-        run_vcycle(zz, rr, 0, 1, opts.nVcycles);
+        run_vcycle(w, zz, rr, 0, 1, opts.nVcycles);
     }
     const int n_if = ih.n_iface.empty() ? 0 : ih.n_iface[0];
     {
-        Tm tm(this, 3);
-        cuda_check(launch_interface_gather(g, iface_slot.p, iface_nb.p, n_if, rr, zz, sigma.b0(), stream), "gather");
-        count();
+        Tm tm(this, w, 3);
+        cuda_check(launch_interface_gather(g, iface_slot.p, iface_nb.p, n_if, rr, zz, w.sig.b0(), w.stream), "gather");
+        count(w);
     }
     if (n_if > 0) {
         // u_G = 0 then sigma_mg V-cycles (Preconditioner.h:105,110-117).
         NvtxRange sigma_range("Sigma_V_Cycle");
-        Tm tm(this, 4);
-        cuda_check(cudaMemsetAsync(sigma.u0(), 0, sizeof(float) * n_if, stream), "memset u0");
-        for (int i = 0; i < opts.sigma_mg; ++i) sigma.vcycle(stream, launches, &hook);
+        Tm tm(this, w, 4);
+        cuda_check(cudaMemsetAsync(w.sig.u0(), 0, sizeof(float) * n_if, w.stream), "memset u0");
+        for (int i = 0; i < opts.sigma_mg; ++i) sigma.vcycle(w.sig, w.stream, w.launches, &w == &w0 ? &hook : nullptr);
     }
     {
-        Tm tm(this, 3);
-        cuda_check(launch_interface_scatter(iface_slot.p, n_if, sigma.u0(), zz, stream), "scatter");
-        count();
+        Tm tm(this, w, 3);
+        cuda_check(launch_interface_scatter(iface_slot.p, n_if, w.sig.u0(), zz, w.stream), "scatter");
+        count(w);
     }
     NvtxRange step("Step Two");
-    run_vcycle(zz, rr, 1, 1, opts.nVcycles);
+    run_vcycle(w, zz, rr, 1, 1, opts.nVcycles);
 }
 
-void Solver::solve(hdd_result* res) {
+void Solver::solve(Work& w, hdd_result* res) {
     if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
     NvtxRange range("solve");
     cuda_check(cudaSetDevice(opts.device), "cudaSetDevice");
@@ -325,71 +423,97 @@ void Solver::solve(hdd_result* res) {
     std::memset(&init, 0, sizeof(init));
     init.rho_old = 3.402823466e+38f;
     init.rho_old_d = 3.402823466e+38;
-    cuda_check(cudaMemcpyAsync(scal.p, &init, sizeof(init), cudaMemcpyHostToDevice, stream), "init scalars");
-    x.zero(stream);
-    xd.zero(stream);
-    double* xdp = mode == 1 ? xd.p : nullptr;
-    sigma.clear_error(stream);
+    cuda_check(cudaMemcpyAsync(w.scal.p, &init, sizeof(init), cudaMemcpyHostToDevice, w.stream), "init scalars");
+    w.x.zero(w.stream);
+    w.xd.zero(w.stream);
+    double* xdp = mode == 1 ? w.xd.p : nullptr;
+    SigmaGpu::clear_error(w.sig, w.stream);
     cudaEvent_t e0, e1;
     cuda_check(cudaEventCreate(&e0), "event");
     cuda_check(cudaEventCreate(&e1), "event");
-    cuda_check(cudaEventRecord(e0, stream), "event record");
+    cuda_check(cudaEventRecord(e0, w.stream), "event record");
     // r = Project(b - A x) with x = 0 (restart branch, CONJUGATE_GRADIENT.cpp:36).
-    cuda_check(launch_residual(g, b.p, x.p, r.p, partial_max.p, stream), "residual"); count();
-    cuda_check(launch_reduce_max(partial_max.p, nt, scalars_f.p, stream), "reduce"); count();
+    cuda_check(launch_residual(g, w.b.p, w.x.p, w.r.p, w.partial_max.p, w.stream), "residual"); count(w);
+    cuda_check(launch_reduce_max(w.partial_max.p, nt, w.scalars_f.p, w.stream), "reduce"); count(w);
     float rmax = 0;
     PcgScalars hs;
-    cuda_check(cudaMemcpyAsync(&rmax, scalars_f.p, sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
-    sync();
+    cuda_check(cudaMemcpyAsync(&rmax, w.scalars_f.p, sizeof(float), cudaMemcpyDeviceToHost, w.stream), "D2H");
+    sync(w);
     const double b_inf = rmax;
-    history.assign(1, (double)rmax);
-    alphas.clear();
-    betas.clear();
+    w.history.assign(1, (double)rmax);
+    w.alphas.clear();
+    w.betas.clear();
     const float threshold = opts.relative_tol ? (float)(opts.tol * b_inf) : (float)opts.tol;
     const float small_number = 1.1920929e-07f;
     int it = 0;
     bool converged = false, breakdown = false;
+    // The precision form stops on its FP64 true residual: when the recursively
+    // updated (FP32) residual reaches the tolerance, r is recomputed from the
+    // FP64 iterate (residual replacement) and the loop goes on if the true
+    // residual is still above it.  An FP32 recursive residual drifts from the
+    // true one by about the FP32 rounding of the updates.
+    // When that recomputed residual is still above the tolerance, it differs
+    // from the recursive one by far more than the recursive one itself, and
+    // the search directions built on the recursive residual no longer fit:
+    // PCG restarts from x (s = z, the restart branch of
+    // PB/Public_Library/PhysBAM_Tools/Krylov_Solvers/CONJUGATE_GRADIENT.cpp:30-36,47).
+    bool replaced = false;  // r was recomputed from x in this iteration
+    bool restart = false;   // the next iteration starts a new search direction
     for (;; ++it) {
-        if (rmax <= threshold && (it >= opts.min_iters || rmax < small_number)) { converged = true; break; }
+        if (rmax <= threshold && (it >= opts.min_iters || rmax < small_number)) {
+            if (mode != 1 || replaced) { converged = true; break; }
+            cuda_check(launch_residual_f64(g, w.b.p, xdp, w.r.p, w.partial_max.p, w.stream), "true residual"); count(w);
+            cuda_check(launch_reduce_max(w.partial_max.p, nt, w.scalars_f.p, w.stream), "reduce"); count(w);
+            cuda_check(cudaMemcpyAsync(&rmax, w.scalars_f.p, sizeof(float), cudaMemcpyDeviceToHost, w.stream), "D2H");
+            sync(w);
+            w.history.back() = (double)rmax;
+            replaced = true;
+            if (rmax <= threshold) { converged = true; break; }
+            restart = true;
+        }
         if (it >= opts.max_iters) break;
-        apply_preconditioner(r.p, z.p);
+        replaced = false;
+        const int first = (it == 0 || restart) ? 1 : 0;
+        restart = false;
+        apply_preconditioner(w, w.r.p, w.z.p);
         {
-            Tm tm(this, 2);
-            cuda_check(launch_project_dot(g, z.p, r.p, partial.p, stream), "project_dot"); count();
-            cuda_check(launch_reduce_sum(partial.p, nt, sums.p + 0, stream), "reduce"); count();
-            cuda_check(launch_scalar_rho(scal.p, sums.p + 0, it == 0, stream), "rho"); count();
-            cuda_check(launch_update_s(g, s.p, z.p, scal.p, it == 0, mode, stream), "update_s"); count();
+            Tm tm(this, w, 2);
+            cuda_check(launch_project_dot(g, w.z.p, w.r.p, w.partial.p, w.stream), "project_dot"); count(w);
+            cuda_check(launch_reduce_sum(w.partial.p, nt, w.sums.p + 0, w.stream), "reduce"); count(w);
+            cuda_check(launch_scalar_rho(w.scal.p, w.sums.p + 0, first, w.stream), "rho"); count(w);
+            cuda_check(launch_update_s(g, w.s.p, w.z.p, w.scal.p, first, mode, w.stream), "update_s"); count(w);
         }
         {
-            Tm tm(this, 1, laplace_bytes);
-            cuda_check(launch_laplace_dot(g, s.p, q.p, partial.p, stream), "laplace"); count();
+            Tm tm(this, w, 1, laplace_bytes);
+            cuda_check(launch_laplace_dot(g, w.s.p, w.q.p, w.partial.p, w.stream), "laplace"); count(w);
         }
         {
-            Tm tm(this, 2);
-            cuda_check(launch_reduce_sum(partial.p, nt, sums.p + 1, stream), "reduce"); count();
-            cuda_check(launch_scalar_alpha(scal.p, sums.p + 1, stream), "alpha"); count();
-            cuda_check(launch_update_xr(g, x.p, r.p, s.p, q.p, scal.p, mode, partial_max.p, stream, xdp), "update_xr");
-            count();
+            Tm tm(this, w, 2);
+            cuda_check(launch_reduce_sum(w.partial.p, laplace_partials(g), w.sums.p + 1, w.stream), "reduce"); count(w);
+            cuda_check(launch_scalar_alpha(w.scal.p, w.sums.p + 1, w.stream), "alpha"); count(w);
+            cuda_check(launch_update_xr(g, w.x.p, w.r.p, w.s.p, w.q.p, w.scal.p, mode, w.partial_max.p, w.stream, xdp), "update_xr");
+            count(w);
         }
         if (mode == 1 && opts.true_residual_every > 0 && (it + 1) % opts.true_residual_every == 0) {
-            cuda_check(launch_residual_f64(g, b.p, xdp, r.p, partial_max.p, stream), "true residual"); count();
+            cuda_check(launch_residual_f64(g, w.b.p, xdp, w.r.p, w.partial_max.p, w.stream), "true residual"); count(w);
+            replaced = true;
         }
-        cuda_check(launch_reduce_max(partial_max.p, nt, scalars_f.p, stream), "reduce"); count();
-        cuda_check(cudaMemcpyAsync(&rmax, scalars_f.p, sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
-        cuda_check(cudaMemcpyAsync(&hs, scal.p, sizeof(hs), cudaMemcpyDeviceToHost, stream), "D2H");
+        cuda_check(launch_reduce_max(w.partial_max.p, nt, w.scalars_f.p, w.stream), "reduce"); count(w);
+        cuda_check(cudaMemcpyAsync(&rmax, w.scalars_f.p, sizeof(float), cudaMemcpyDeviceToHost, w.stream), "D2H");
+        cuda_check(cudaMemcpyAsync(&hs, w.scal.p, sizeof(hs), cudaMemcpyDeviceToHost, w.stream), "D2H");
         int herr = 0;
-        if (sigma.d_err)
-            cuda_check(cudaMemcpyAsync(&herr, sigma.d_err, sizeof(int), cudaMemcpyDeviceToHost, stream), "D2H");
-        sync();
-        history.push_back((double)rmax);
-        alphas.push_back(mode == 1 ? hs.alpha_d : (double)hs.alpha);
-        betas.push_back(it == 0 ? 0.0 : (mode == 1 ? hs.beta_d : (double)hs.beta));
+        if (w.sig.err)
+            cuda_check(cudaMemcpyAsync(&herr, w.sig.err, sizeof(int), cudaMemcpyDeviceToHost, w.stream), "D2H");
+        sync(w);
+        w.history.push_back((double)rmax);
+        w.alphas.push_back(mode == 1 ? hs.alpha_d : (double)hs.alpha);
+        w.betas.push_back(first ? 0.0 : (mode == 1 ? hs.beta_d : (double)hs.beta));
         // A bounded wait that gave up leaves this iteration's preconditioner
         // invalid: stop here (check_waits below reports HDD_ERR_TIMEOUT).
         if (herr != 0) { ++it; break; }
         if (hs.status != 0 || !std::isfinite(rmax)) { breakdown = true; ++it; break; }
     }
-    cuda_check(cudaEventRecord(e1, stream), "event record");
+    cuda_check(cudaEventRecord(e1, w.stream), "event record");
     cuda_check(cudaEventSynchronize(e1), "event sync");
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
@@ -397,21 +521,21 @@ void Solver::solve(hdd_result* res) {
     cudaEventDestroy(e1);
     // True residual of the returned iterate (reported, not used for stopping):
     // the FP64 iterate in the precision form, else x.
-    if (xdp) cuda_check(launch_residual_f64(g, b.p, xdp, q.p, partial_max.p, stream), "true residual");
-    else cuda_check(launch_residual(g, b.p, x.p, q.p, partial_max.p, stream), "true residual");
-    count();
-    cuda_check(launch_reduce_max(partial_max.p, nt, scalars_f.p + 1, stream), "reduce"); count();
-    cuda_check(launch_project_dot(g, q.p, q.p, partial.p, stream), "dot"); count();
-    cuda_check(launch_reduce_sum(partial.p, nt, sums.p + 2, stream), "reduce"); count();
-    cuda_check(launch_project_dot(g, b.p, b.p, partial.p, stream), "dot"); count();
-    cuda_check(launch_reduce_sum(partial.p, nt, sums.p + 3, stream), "reduce"); count();
+    if (xdp) cuda_check(launch_residual_f64(g, w.b.p, xdp, w.q.p, w.partial_max.p, w.stream), "true residual");
+    else cuda_check(launch_residual(g, w.b.p, w.x.p, w.q.p, w.partial_max.p, w.stream), "true residual");
+    count(w);
+    cuda_check(launch_reduce_max(w.partial_max.p, nt, w.scalars_f.p + 1, w.stream), "reduce"); count(w);
+    cuda_check(launch_project_dot(g, w.q.p, w.q.p, w.partial.p, w.stream), "dot"); count(w);
+    cuda_check(launch_reduce_sum(w.partial.p, nt, w.sums.p + 2, w.stream), "reduce"); count(w);
+    cuda_check(launch_project_dot(g, w.b.p, w.b.p, w.partial.p, w.stream), "dot"); count(w);
+    cuda_check(launch_reduce_sum(w.partial.p, nt, w.sums.p + 3, w.stream), "reduce"); count(w);
     float tmax = 0;
     double d2[2] = {0, 0};
-    cuda_check(cudaMemcpyAsync(&tmax, scalars_f.p + 1, sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
-    cuda_check(cudaMemcpyAsync(d2, sums.p + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream), "D2H");
-    sync();
-    solved = true;
-    check_waits();
+    cuda_check(cudaMemcpyAsync(&tmax, w.scalars_f.p + 1, sizeof(float), cudaMemcpyDeviceToHost, w.stream), "D2H");
+    cuda_check(cudaMemcpyAsync(d2, w.sums.p + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, w.stream), "D2H");
+    sync(w);
+    w.solved = true;
+    check_waits(w);
     if (res) {
         res->iterations = it;
         res->converged = converged ? 1 : 0;
@@ -426,22 +550,23 @@ void Solver::solve(hdd_result* res) {
     if (!converged) throw Error(HDD_ERR_NOT_CONVERGED, "PCG did not converge within max_iters");
 }
 
-void Solver::get_solution(float* out) {
-    if (!solved) throw Error(HDD_ERR_NOT_INITIALIZED, "no solution available");
-    Tm tm(this, 5);
-    cuda_check(cudaMemsetAsync(dense.p, 0, L.cell_count() * sizeof(float), stream), "memset");
-    cuda_check(launch_tiles_to_dense(geom(), tile_xyz.p, L.opt.size[0], L.opt.size[1], L.opt.size[2], x.p, dense.p,
-                                     stream), "tiles_to_dense");
-    count();
-    cuda_check(cudaMemcpyAsync(out, dense.p, L.cell_count() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H x");
-    sync();
+void Solver::get_solution(Work& w, float* out) {
+    if (!w.solved) throw Error(HDD_ERR_NOT_INITIALIZED, "no solution available");
+    Tm tm(this, w, 5);
+    cuda_check(cudaMemsetAsync(w.dense.p, 0, L.cell_count() * sizeof(float), w.stream), "memset");
+    cuda_check(launch_tiles_to_dense(geom(), tile_xyz.p, L.opt.size[0], L.opt.size[1], L.opt.size[2], w.x.p,
+                                     w.dense.p, w.stream), "tiles_to_dense");
+    count(w);
+    cuda_check(cudaMemcpyAsync(out, w.dense.p, L.cell_count() * sizeof(float), cudaMemcpyDeviceToHost, w.stream),
+               "D2H x");
+    sync(w);
 }
 
 void Solver::get_solution_f64(double* out) {
-    if (!solved) throw Error(HDD_ERR_NOT_INITIALIZED, "no solution available");
+    if (!w0.solved) throw Error(HDD_ERR_NOT_INITIALIZED, "no solution available");
     const size_t n = L.cell_count();
-    DevBuf<double> tmp_tiles, tmp_dense;
-    const double* src = xd.p;
+    DevBuf<double> tmp_dense;
+    const double* src = w0.xd.p;
     if (!src) {
         // Reference precision: the FP32 iterate, widened.
         std::vector<float> xf(n);
@@ -453,7 +578,7 @@ void Solver::get_solution_f64(double* out) {
     cuda_check(cudaMemsetAsync(tmp_dense.p, 0, n * sizeof(double), stream), "memset");
     cuda_check(launch_tiles_to_dense_f64(geom(), tile_xyz.p, L.opt.size[0], L.opt.size[1], L.opt.size[2], src,
                                          tmp_dense.p, stream), "tiles_to_dense_f64");
-    count();
+    count(w0);
     cuda_check(cudaMemcpyAsync(out, tmp_dense.p, n * sizeof(double), cudaMemcpyDeviceToHost, stream), "D2H x");
     sync();
 }
@@ -462,12 +587,12 @@ void Solver::apply_preconditioner_dense(const float* rin, float* zout) {
     if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
     std::vector<float> t(L.tiled_count());
     dense_to_tiles(L, rin, t.data());
-    cuda_check(cudaMemcpyAsync(r.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
-    z.zero(stream);
+    cuda_check(cudaMemcpyAsync(w0.r.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
+    w0.z.zero(stream);
     sigma.clear_error(stream);
-    apply_preconditioner(r.p, z.p);
-    cuda_check(launch_project(geom(), z.p, stream), "project"); count();
-    cuda_check(cudaMemcpyAsync(t.data(), z.p, t.size() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
+    apply_preconditioner(w0, w0.r.p, w0.z.p);
+    cuda_check(launch_project(geom(), w0.z.p, stream), "project"); count(w0);
+    cuda_check(cudaMemcpyAsync(t.data(), w0.z.p, t.size() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
     sync();
     check_waits();
     tiles_to_dense(L, t.data(), zout);
@@ -477,12 +602,12 @@ void Solver::vcycle_dense(float* u, const float* bb, int nv) {
     if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
     std::vector<float> t(L.tiled_count());
     dense_to_tiles(L, u, t.data());
-    cuda_check(cudaMemcpyAsync(z.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
+    cuda_check(cudaMemcpyAsync(w0.z.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
     std::vector<float> tb(L.tiled_count());
     dense_to_tiles(L, bb, tb.data());
-    cuda_check(cudaMemcpyAsync(q.p, tb.data(), tb.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
-    run_vcycle(z.p, q.p, 1, 0, nv);
-    cuda_check(cudaMemcpyAsync(t.data(), z.p, t.size() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
+    cuda_check(cudaMemcpyAsync(w0.q.p, tb.data(), tb.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
+    run_vcycle(w0, w0.z.p, w0.q.p, 1, 0, nv);
+    cuda_check(cudaMemcpyAsync(t.data(), w0.z.p, t.size() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
     sync();
     // Cells outside stored tiles keep the caller's values.
     std::vector<float> dense(L.cell_count());
@@ -498,9 +623,9 @@ void Solver::multiply_dense(const float* xin, float* yout) {
     if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
     std::vector<float> t(L.tiled_count());
     dense_to_tiles(L, xin, t.data());
-    cuda_check(cudaMemcpyAsync(s.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
-    cuda_check(launch_laplace_dot(geom(), s.p, q.p, partial.p, stream), "laplace"); count();
-    cuda_check(cudaMemcpyAsync(t.data(), q.p, t.size() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
+    cuda_check(cudaMemcpyAsync(w0.s.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
+    cuda_check(launch_laplace_dot(geom(), w0.s.p, w0.q.p, w0.partial.p, stream), "laplace"); count(w0);
+    cuda_check(cudaMemcpyAsync(t.data(), w0.q.p, t.size() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
     sync();
     tiles_to_dense(L, t.data(), yout);
 }
@@ -512,7 +637,7 @@ void Solver::sigma_vcycle_host(const float* b0, float* u0) {
     cuda_check(cudaMemcpyAsync(sigma.b0(), b0, n_if * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
     cuda_check(cudaMemsetAsync(sigma.u0(), 0, n_if * sizeof(float), stream), "memset");
     sigma.clear_error(stream);
-    sigma.vcycle(stream, launches);
+    sigma.vcycle(stream, w0.launches);
     cuda_check(cudaMemcpyAsync(u0, sigma.u0(), n_if * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
     sync();
     check_waits();
@@ -535,14 +660,14 @@ void Solver::interface_solve(int kind, int level, const float* bh, float* xh, in
     cuda_check(cudaMemcpyAsync(db, bh, rows * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
     cuda_check(cudaMemsetAsync(dx, 0, rows * sizeof(float), stream), "memset");
     sigma.clear_error(stream);
-    plan.solve(db, dx, stream, launches, &hook);
+    plan.solve(db, dx, stream, w0.launches, &hook);
     cuda_check(cudaMemcpyAsync(xh, dx, rows * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
     sync();
     check_waits();
 }
 
-void Solver::check_waits() {
-    if (sigma.error_flag(stream))
+void Solver::check_waits(Work& w) {
+    if (SigmaGpu::error_flag(w.sig, w.stream))
         throw Error(HDD_ERR_TIMEOUT, "a bounded device wait in the sigma solve gave up; results are invalid");
 }
 

@@ -66,26 +66,64 @@ inline void cuda_check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw Error(HDD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// The device state one PCG solve writes, on its own stream: the tiled
+// vectors, reduction partials and scalars, the sigma V-cycle's buffers, the
+// CUDA graph of one preconditioner application on them, and the last solve's
+// record.  A Solver's first context (`w0`) serves the C ABI's single-solve
+// calls; a server adds contexts to run several solves of one resident domain
+// at once, all reading the domain's factors, matrices and layout tables.
+struct Work {
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    DevBuf<float> x, b, r, z, s, q;
+    DevBuf<double> xd;      // precision form: the FP64 iterate (x is its FP32 rounding)
+    DevBuf<float> dense;    // staging buffer in the caller's dense layout
+    DevBuf<double> partial, sums;
+    DevBuf<float> partial_max, scalars_f;
+    DevBuf<PcgScalars> scal;
+    SigmaScratch sig;
+    bool own_sig = false;
+    // CUDA graph of one preconditioner application (on buffers pc_r -> pc_z)
+    // and the kernel launches it holds; dropped when a launch parameter
+    // changes (re-initialisation, the wait limit).
+    bool use_graphs = true;
+    cudaGraphExec_t pc_exec = nullptr;
+    const float* pc_r = nullptr;
+    float* pc_z = nullptr;
+    long long pc_launches = 0;
+    long long launches = 0;  // kernel launches issued on this context
+    bool solved = false;
+    // max|r| of the recursively updated residual at the start of each PCG
+    // iteration of the last solve (entry 0: r = b), for parity checks against
+    // the oracle's history; step lengths alpha and beta of every iteration.
+    std::vector<double> history, alphas, betas;
+
+    Work() = default;
+    Work(const Work&) = delete;
+    Work& operator=(const Work&) = delete;
+    ~Work();
+    void release_graphs();
+    size_t bytes() const {
+        size_t t = 0;
+        for (const DevBuf<float>* v : {&x, &b, &r, &z, &s, &q, &dense, &partial_max, &scalars_f}) t += v->n * sizeof(float);
+        t += (partial.n + sums.n + xd.n) * sizeof(double) + scal.n * sizeof(PcgScalars);
+        return t + (own_sig ? sig.bytes : 0);
+    }
+};
+
 struct Solver {
     hdd_options opts;
     std::string last_error;
-    long long launches = 0;
 
-    bool have_domain = false, initialized = false, solved = false;
+    bool have_domain = false, initialized = false;
     DomainLayout L;
     std::vector<uint32_t> flags_in;
     std::vector<float> rhs_dense;
 
-    cudaStream_t stream = nullptr;
-    DevBuf<float> x, b, r, z, s, q;
-    DevBuf<double> xd;      // precision form: the FP64 iterate (x is its FP32 rounding)
+    // Read-only device data of the domain, shared by every solve context.
     DevBuf<uint16_t> tflags;
     DevBuf<int> tile_nbr, box_tile, box_nb, tile_xyz;
-    DevBuf<float> dense;   // staging buffer in the caller's dense layout
     DevBuf<uint8_t> box_flags;
-    DevBuf<double> partial, sums;
-    DevBuf<float> partial_max, scalars_f;
-    DevBuf<PcgScalars> scal;
     // Level-0 interface DOFs (sigma level 0 order).
     DevBuf<long long> iface_slot;
     DevBuf<int> iface_nb;
@@ -94,12 +132,8 @@ struct Solver {
     int iomode = HDD_IOMODE_NEITHER;  // interface dump / reload at initialize()
     std::string io_dir;
     double setup_ms = 0;
-    // max|r| of the recursively updated residual at the start of each PCG
-    // iteration of the last solve (entry 0: r = b), for parity checks against
-    // the oracle's history.
-    std::vector<double> history;
-    // Step lengths alpha and beta of every PCG iteration of the last solve.
-    std::vector<double> alphas, betas;
+    Work w0;                    // the first solve context (owns the solver's stream)
+    cudaStream_t& stream = w0.stream;
     // Host wall time of the setup phases: layout and vector uploads, interface
     // system (assembly or reload, and dump), interface solver (factorisations
     // and solve plans), total.
@@ -118,16 +152,17 @@ struct Solver {
     double vcycle_bytes = 0, laplace_bytes = 0;  // algorithmic bytes of one launch
     struct Pending { int cat; cudaEvent_t a, b; double bytes; };
     std::vector<Pending> pending;
+    // Timed phases are recorded on the first context only.
     struct Tm {
-        Solver* s; int cat; double bytes; cudaEvent_t a = nullptr, b = nullptr;
-        Tm(Solver* sv, int c, double by = 0) : s(sv), cat(c), bytes(by) {
-            if (!s->timing) return;
+        Solver* s; cudaStream_t st; int cat; double bytes; cudaEvent_t a = nullptr, b = nullptr;
+        Tm(Solver* sv, const Work& w, int c, double by = 0) : s(sv), st(w.stream), cat(c), bytes(by) {
+            if (!s->timing || &w != &s->w0) return;
             cudaEventCreate(&a); cudaEventCreate(&b);
-            cudaEventRecord(a, s->stream);
+            cudaEventRecord(a, st);
         }
         ~Tm() {
             if (!a) return;
-            cudaEventRecord(b, s->stream);
+            cudaEventRecord(b, st);
             s->pending.push_back({cat, a, b, bytes});
         }
     };
@@ -157,11 +192,19 @@ struct Solver {
     void set_domain(const uint32_t* flags, const float* rhs);
     // Same, taking over dense arrays the caller built (no second copy).
     void set_domain(std::vector<uint32_t>&& flags, std::vector<float>&& rhs);
-    void set_rhs(const float* rhs);
+    void set_rhs(const float* rhs) { set_rhs(w0, rhs); }
     void initialize();
-    void solve(hdd_result* res);
-    void get_solution(float* out);
+    void solve(hdd_result* res) { solve(w0, res); }
+    void get_solution(float* out) { get_solution(w0, out); }
     void get_solution_f64(double* out);
+    // A further solve context of this domain on a stream of its own (device
+    // buffers for the vectors and the sigma V-cycle; bytes() tells how much).
+    // Contexts run solves concurrently from different host threads; the
+    // domain's own setup state is only read.
+    std::unique_ptr<Work> make_work();
+    void set_rhs(Work& w, const float* rhs);
+    void solve(Work& w, hdd_result* res);
+    void get_solution(Work& w, float* out);
     void apply_preconditioner_dense(const float* r, float* zout);
     void vcycle_dense(float* u, const float* bb, int nv);
     void multiply_dense(const float* xin, float* yout);
@@ -169,24 +212,30 @@ struct Solver {
     // One Arr (kind 0) or concatenated Aii (kind 1) supernodal solve of a sigma level.
     void interface_solve(int kind, int level, const float* bh, float* xh, int* n);
     // Throws HDD_ERR_TIMEOUT when a device-side bounded wait gave up.
-    void check_waits();
+    void check_waits() { check_waits(w0); }
+    void check_waits(Work& w);
 
     // Device pieces.
     TileGeom geom() const;
     VcycleArgs vcycle_args(float* u, const float* bb, int halo_from_u, int zero_init, int nv) const;
-    void run_vcycle(float* u, const float* bb, int halo_from_u, int zero_init, int nv);
-    void apply_preconditioner(const float* rr, float* zz);   // device tiled vectors
-    void count(int n = 1) { launches += n; }
+    void run_vcycle(Work& w, float* u, const float* bb, int halo_from_u, int zero_init, int nv);
+    void apply_preconditioner(Work& w, const float* rr, float* zz);   // device tiled vectors (graph replay)
+    void apply_preconditioner_launches(Work& w, const float* rr, float* zz);
+    void release_graphs() { w0.release_graphs(); }
+    void alloc_vectors(Work& w);
+    static void count(Work& w, int n = 1) { w.launches += n; }
     void sync() { cuda_check(cudaStreamSynchronize(stream), "stream sync"); }
-    // Device memory held by this solver (vectors, tables, interface solver).
+    static void sync(Work& w) { cuda_check(cudaStreamSynchronize(w.stream), "stream sync"); }
+    // Device memory held by this solver (tables, interface solver and the
+    // first context).
     size_t device_bytes() const {
-        size_t t = 0;
-        for (const DevBuf<float>* v : {&x, &b, &r, &z, &s, &q, &dense, &partial_max, &scalars_f}) t += v->n * sizeof(float);
-        t += tflags.n * sizeof(uint16_t) + box_flags.n;
+        size_t t = tflags.n * sizeof(uint16_t) + box_flags.n;
         for (const DevBuf<int>* v : {&tile_nbr, &box_tile, &box_nb, &tile_xyz, &iface_nb}) t += v->n * sizeof(int);
-        t += (partial.n + sums.n + xd.n) * sizeof(double) + iface_slot.n * sizeof(long long);
-        return t + sigma.device_bytes;
+        t += iface_slot.n * sizeof(long long);
+        return t + sigma.device_bytes + w0.bytes();
     }
+    // Device bytes a further context of this domain allocates.
+    size_t work_bytes() const;
 };
 
 }  // namespace hdd

@@ -2,9 +2,9 @@
 requests from any thread, per-request latency.
 
 The reference has no serving layer (its GPU demo solves one domain per
-process); this mirrors the C interface one to one.  Solves on different
-domains run concurrently on the GPU; a request's result does not depend on
-what else is in flight.
+process); this mirrors the C interface one to one.  Solves on one domain and
+on different domains run concurrently on the GPU; a request's result does not
+depend on what else is in flight.
 """
 from __future__ import annotations
 

@@ -82,7 +82,7 @@ class SPGrid_Domain_Decomposition_Solver:
                                   tol=1e-6, relative_tol=True, max_iters=5000, min_iters=0,
                                   precision_mode=_lib.PRECISION_REFERENCE, true_residual_every=20,
                                   iomode="neither", dump_directory="matrices_dump",
-                                  coarse_solve=_lib.COARSE_REFERENCE):
+                                  coarse_solve=_lib.COARSE_REFERENCE, solve_share=0):
         """Setup with the reference's arguments (SPGrid_Domain_Decomposition_Solver.h:121).
         ``iomode`` "output" writes the interface matrices to ``dump_directory`` in the
         reference's dump layout, "input" reads them from there instead of assembling
@@ -111,6 +111,7 @@ class SPGrid_Domain_Decomposition_Solver:
         o.max_iters, o.min_iters = int(max_iters), int(min_iters)
         o.precision_mode, o.true_residual_every = int(precision_mode), int(true_residual_every)
         o.coarse_solve = int(coarse_solve)
+        o.solve_share = int(solve_share)
         o.device = self.device
         self.options = o
         self.close()

@@ -42,7 +42,9 @@ typedef enum {
 enum {
     HDD_PRECISION_REFERENCE = 0, /* FP32 vectors, FP64 dot accumulation, FP32 alpha/beta (as the reference) */
     HDD_PRECISION_MIXED = 1      /* FP32 preconditioner and search vectors; FP64 iterate x, dots,
-                                    alpha/beta and periodic true residual r = b - A x */
+                                    alpha/beta and true residual r = b - A x, recomputed every
+                                    true_residual_every iterations and before stopping, so the
+                                    stop test holds for the true residual */
 };
 
 typedef struct {
@@ -63,6 +65,9 @@ typedef struct {
     int true_residual_every;/* mixed mode: recompute r = b - A x every N iterations (0 = never) */
     int device;             /* CUDA device ordinal */
     int coarse_solve;       /* HDD_COARSE_* : how the coarsest interface level is solved */
+    int solve_share;        /* persistent interface solves use 1/solve_share of the device's
+                               resident CTAs (0 or 1 = all), leaving room for concurrent solves
+                               (the server sets it to its slot count); results do not depend on it */
 } hdd_options;
 
 /* Coarsest interface (sigma) level.  The reference runs 200 smoothing steps
@@ -290,11 +295,14 @@ void hdd_destroy(hdd_solver* s);
  * estimated device footprint fits the HBM budget; a worker then runs its setup
  * (as hdd_initialize_preconditioner) and the domain stays resident until
  * removed.  Each solve request names a resident (or still setting-up) domain
- * and a right-hand side; workers take the oldest request whose domain is idle,
- * so requests on different domains run concurrently on separate CUDA streams
- * and requests on one domain run in arrival order.  A request's result does not
- * depend on what else is in flight.  All calls except hdd_server_destroy may be
- * made from any thread at any time. */
+ * and a right-hand side.  A resident domain keeps a pool of solve contexts (the
+ * PCG and interface-solve vectors on a CUDA stream of their own, sharing the
+ * domain's factors and tables), growing on demand up to `slots` while the HBM
+ * budget allows; workers take the oldest request whose domain has a context
+ * free, so requests on one domain and on different domains run concurrently.
+ * A request's result does not depend on what else is in flight (bit-identical
+ * to a solve alone).  All calls except hdd_server_destroy may be made from any
+ * thread at any time. */
 typedef struct hdd_server hdd_server;
 
 typedef struct {
@@ -335,7 +343,7 @@ hdd_status hdd_server_poll(hdd_server* srv, long long request_id, int wait_ms, h
 hdd_status hdd_server_remove_domain(hdd_server* srv, long long domain_id);
 
 /* Device bytes held by admitted domains (estimates until set up, then what
- * their solvers hold) and the budget. */
+ * their solvers and solve contexts hold) and the budget. */
 hdd_status hdd_server_memory(hdd_server* srv, long long* reserved, long long* budget);
 
 /* Lets running setups and solves finish, stops the workers and frees every

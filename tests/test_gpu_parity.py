@@ -60,6 +60,23 @@ def test_multiply_bitexact(small_pair):
     assert np.array_equal(y, yo)
 
 
+@pytest.mark.parametrize("n,sub", [((40, 36, 44), 8), (48, 16), ((50, 40, 33), 16), (64, 32), ((70, 64, 40), 32)])
+def test_multiply_bitexact_sub_sizes(n, sub):
+    # The marching-plane Laplacian at every supported tile edge, on ragged
+    # grids (partial last tiles, absent neighbour tiles); unmasked values in
+    # Dirichlet and exterior cells must not leak into the result.
+    d = domains.small(n, sub, 6 if sub < 32 else 10, seed=2)
+    s, o = make_pair(d)
+    try:
+        rng = np.random.default_rng(5)
+        x = rng.standard_normal(d.size).astype(np.float32)
+        f0 = o.level_flags(0)
+        x[(f0 & (ACTIVE | INTERFACE)) == 0] = 0
+        assert np.array_equal(s.Multiply(x), o.multiply(x))
+    finally:
+        s.close()
+
+
 def test_vcycle_bitexact(small_pair):
     d, s, o = small_pair
     rng = np.random.default_rng(4)

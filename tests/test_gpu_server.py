@@ -2,7 +2,8 @@
 
 * every request's iterations and solution equal the plain one-handle solve of
   the same domain and right-hand side, bit for bit, whether it ran alone or
-  among other requests in flight;
+  among other requests in flight, on the same domain (several solve contexts
+  of one resident domain at once) or on others;
 * a budget that fits one domain at a time admits them in turn and all
   requests still finish; the reserved bytes return to zero after removal;
 * a domain whose setup fails reports its status, and so do its requests.
@@ -22,10 +23,10 @@ def cases():
             domains.small(48, 16, 8, seed=7), domains.small(16, 16, 3, seed=1)]
 
 
-def options(d):
+def options(d, **extra):
     m = d.meta
     return make_options(d.size, d.sub_size, m["vlevels"], m["nVcycles"], m["interior_smoothing"],
-                        m["boundary_smoothing"], m["sigma_levels"], m["sigma_smoothing"], m["sigma_mg"])
+                        m["boundary_smoothing"], m["sigma_levels"], m["sigma_smoothing"], m["sigma_mg"], **extra)
 
 
 def rhs_set(d, k):
@@ -80,6 +81,64 @@ def test_concurrent_requests_match_plain_solves():
         assert srv.memory()[0] == 0
     finally:
         srv.close()
+
+
+def test_one_domain_many_requests_in_flight():
+    # Six requests on one domain with four slots: up to four solve contexts of
+    # the domain run at once (precision form, exact coarsest interface level).
+    d = domains.small(48, 16, 8, seed=7)
+    m = d.meta
+    rhs = rhs_set(d, 5)
+    from hierarchicaldd_b200.solver import SPGrid_Domain_Decomposition_Solver
+    s = SPGrid_Domain_Decomposition_Solver()
+    s.Set_Domain(d.flags, d.rhs)
+    s.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"],
+                                m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"], m["sigma_mg"],
+                                precision_mode=1, true_residual_every=20)
+    ref = []
+    for r in rhs:
+        s.Set_RHS(r)
+        res = s.Solve()
+        ref.append((res["iterations"], s.Solution()))
+    s.close()
+    srv = SolveServer(slots=4)
+    try:
+        dom = srv.add_domain(d.flags, options(d, precision_mode=1, true_residual_every=20))
+        assert srv.wait_domain(dom)
+        one = srv.memory()[0]
+        for rnd in range(2):
+            reqs = [srv.submit(dom, r) for r in rhs]
+            for k, req in enumerate(reqs):
+                st, res, x, _ = srv.poll(req, dom)
+                assert st == 0, (rnd, k, st)
+                assert res["iterations"] == ref[k][0], (rnd, k)
+                assert np.array_equal(x, ref[k][1]), (rnd, k, float(np.max(np.abs(x - ref[k][1]))))
+        # Contexts beyond the first are counted against the budget.
+        assert srv.memory()[0] >= one
+        srv.remove_domain(dom)
+        assert srv.memory()[0] == 0
+    finally:
+        srv.close()
+
+
+def test_solve_share_does_not_change_results():
+    # The persistent interface solves on a fraction of the device: the same
+    # tasks in the same order on fewer CTAs, so the same bits.
+    from hierarchicaldd_b200.solver import SPGrid_Domain_Decomposition_Solver
+    d = domains.small(64, 16, 10, seed=3)
+    m = d.meta
+    out = []
+    for share in (0, 2, 7):
+        s = SPGrid_Domain_Decomposition_Solver()
+        s.Set_Domain(d.flags, d.rhs)
+        s.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"],
+                                    m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"],
+                                    m["sigma_mg"], solve_share=share)
+        res = s.Solve()
+        out.append((res["iterations"], s.Solution()))
+        s.close()
+    for its, x in out[1:]:
+        assert its == out[0][0] and np.array_equal(x, out[0][1])
 
 
 def test_budget_admits_domains_in_turn():
