@@ -148,9 +148,9 @@ def one_solve(args):
     lib = _lib.load()
     lib.hdd_set_kernel_timing(s.h, 1)
     r = s.Solve()
-    ms = (C.c_double * 8)()
-    cnt = (C.c_longlong * 8)()
-    nbytes = (C.c_double * 8)()
+    ms = (C.c_double * len(PHASES))()
+    cnt = (C.c_longlong * len(PHASES))()
+    nbytes = (C.c_double * len(PHASES))()
     lib.hdd_get_kernel_timing(s.h, ms, cnt)
     lib.hdd_get_kernel_bytes(s.h, nbytes)
     print(f"solve: {r['iterations']} iterations, {r['solve_ms']:.2f} ms, true residual {r['true_residual_inf']:.3e}")
@@ -325,17 +325,26 @@ def percentiles(lat_ms):
 
 def run_serving(args):
     """Serving workload: uneven resident domains (cube sides 64..192, random
-    Dirichlet spheres, mixed precision), solve requests with 1-3 delta sources
-    through the hdd_server_* C ABI with host buffers (rhs in, solution out).
+    Dirichlet spheres), solve requests with 1-3 delta sources, rhs in and
+    solution out through host buffers.
 
-    * saturated: all requests queued at once; serving (``--slots`` in flight)
-      against the plain drop-in (one request in flight at a time, i.e. one
-      hdd_solve after another), solves/s = requests / makespan;
-    * open loop: Poisson arrivals at 0.8x the plain path's saturated rate;
-      latency = arrival to finish, for both.
+    * serving form: mixed precision (FP32 operators, FP64 PCG scalars and
+      iterate) with the coarsest interface level solved exactly
+      (HDD_COARSE_EXACT), up to ``--slots`` requests in flight through the
+      hdd_server_* C ABI (a pool of solve contexts per resident domain);
+    * plain drop-in: the reference's settings (reference precision, 200
+      coarsest smoothing steps) through hdd_set_rhs_dense / hdd_solve /
+      hdd_get_solution_dense, one request at a time;
+    * the serving form with one request in flight, for the gain of
+      concurrency alone and for the check that every result is bit-identical
+      alone and in the mix.
+    Saturated: all requests queued at once, solves/s = requests / makespan.
+    Open loop: Poisson arrivals at 0.8x the plain path's saturated rate;
+    latency = arrival to finish.
     """
-    from hierarchicaldd_b200 import domains
+    from hierarchicaldd_b200 import _lib, domains
     from hierarchicaldd_b200.server import SolveServer, make_options
+    from hierarchicaldd_b200.solver import SPGrid_Domain_Decomposition_Solver
 
     ds = domains.serving_mix(args.domains)
     rng = np.random.Generator(np.random.Philox(44))
@@ -343,25 +352,53 @@ def run_serving(args):
     picks = [int(i) for i in rng.integers(0, len(ds), K)]
     rhs = [domains.serving_rhs(ds[i], rng) for i in picks]
     gaps = rng.exponential(1.0, K)
+
+    def serving_meta(d):
+        m = dict(d.meta)
+        m.update(precision_mode=_lib.PRECISION_MIXED, coarse_solve=_lib.COARSE_EXACT)
+        return m
+
     srv = SolveServer(slots=args.slots)
     t0 = time.perf_counter()
-    ids = []
-    for d in ds:
-        m = dict(d.meta)
-        ids.append(srv.add_domain(d.flags, make_options(d.size, d.sub_size, tol=1e-6, max_iters=1000, **m)))
+    ids = [srv.add_domain(d.flags, make_options(d.size, d.sub_size, tol=1e-6, max_iters=1000, **serving_meta(d)))
+           for d in ds]
     for dom in ids:
         srv.wait_domain(dom)
     setup_s = time.perf_counter() - t0
     print(f"[bench] serving: {len(ds)} domains resident after {setup_s:.1f} s", file=sys.stderr, flush=True)
-    for i, dom in enumerate(ids):  # warm-up: one solve per domain
+    # The plain drop-in: one handle per domain, reference settings.
+    plain = []
+    for d in ds:
+        m = dict(d.meta)
+        m.pop("precision_mode", None)
+        m.pop("true_residual_every", None)
+        h = SPGrid_Domain_Decomposition_Solver()
+        h.Set_Domain(d.flags, d.rhs)
+        h.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"],
+                                    m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"],
+                                    m["sigma_mg"], tol=1e-6, max_iters=1000)
+        plain.append(h)
+    for i, dom in enumerate(ids):  # warm-up: one solve per domain on each path
         srv.poll(srv.submit(dom, ds[i].rhs), dom, want_x=False)
+        plain[i].Set_RHS(ds[i].rhs)
+        plain[i].Solve(allow_not_converged=True)
 
     def digest(r):  # (status, result, solution digest, latency)
         return r[0], r[1], hashlib.sha1(r[2].tobytes()).hexdigest(), r[3]
 
+    def plain_solve(k):
+        t = time.perf_counter()
+        h = plain[picks[k]]
+        h.Set_RHS(rhs[k])
+        res = h.Solve(allow_not_converged=True)
+        x = h.Solution()
+        return 0 if res["converged"] else 3, res, x, (time.perf_counter() - t) * 1e3
+
     def saturated(in_flight):
         out, t = [], time.perf_counter()
-        if in_flight == 1:
+        if in_flight == 0:
+            out = [digest(plain_solve(k)) for k in range(K)]
+        elif in_flight == 1:
             for k in range(K):
                 out.append(digest(srv.poll(srv.submit(ids[picks[k]], rhs[k]), ids[picks[k]])))
         else:
@@ -369,70 +406,79 @@ def run_serving(args):
             out = [digest(srv.poll(r, ids[picks[k]])) for k, r in enumerate(reqs)]
         return time.perf_counter() - t, out
 
-    def open_loop(rate, in_flight):
+    def open_loop(rate, serving):
         arrivals = np.cumsum(gaps / rate)
-        lat, results, t = [], [], time.perf_counter()
-        if in_flight == 1:
+        lat, t = [], time.perf_counter()
+        if not serving:
             for k in range(K):
                 now = time.perf_counter() - t
                 if arrivals[k] > now:
                     time.sleep(arrivals[k] - now)
-                results.append(srv.poll(srv.submit(ids[picks[k]], rhs[k]), ids[picks[k]], want_x=False))
+                plain_solve(k)
                 lat.append((time.perf_counter() - t - arrivals[k]) * 1e3)
-        else:
-            reqs = []
-            done = {}
+            return lat
+        reqs, done = [], {}
 
-            def collect():
-                for k in range(K):
-                    while len(reqs) <= k:
-                        time.sleep(1e-4)
-                    done[k] = srv.poll(reqs[k], ids[picks[k]], want_x=False)
-            th = threading.Thread(target=collect)
-            th.start()
+        def collect():
             for k in range(K):
-                now = time.perf_counter() - t
-                if arrivals[k] > now:
-                    time.sleep(arrivals[k] - now)
-                reqs.append(srv.submit(ids[picks[k]], rhs[k]))
-            th.join()
-            results = [done[k] for k in range(K)]
-            lat = [results[k][3] for k in range(K)]  # submit (= arrival) to finish
-        return lat, results
+                while len(reqs) <= k:
+                    time.sleep(1e-4)
+                done[k] = srv.poll(reqs[k], ids[picks[k]], want_x=False)
+        th = threading.Thread(target=collect)
+        th.start()
+        for k in range(K):
+            now = time.perf_counter() - t
+            if arrivals[k] > now:
+                time.sleep(arrivals[k] - now)
+            reqs.append(srv.submit(ids[picks[k]], rhs[k]))
+        th.join()
+        return [done[k][3] for k in range(K)]  # submit (= arrival) to finish
 
     with ClockSampler(0) as clk:
-        t_plain, r_plain = saturated(1)
+        t_plain, r_plain = saturated(0)
+        t_alone, r_alone = saturated(1)
         t_serve, r_serve = saturated(args.slots)
-    plain_rate, serve_rate = K / t_plain, K / t_serve
+    plain_rate, alone_rate, serve_rate = K / t_plain, K / t_alone, K / t_serve
     rate = 0.8 * plain_rate
-    lat_plain, _ = open_loop(rate, 1)
-    lat_serve, _ = open_loop(rate, args.slots)
+    lat_plain = open_loop(rate, False)
+    lat_serve = open_loop(rate, True)
     srv_mem = srv.memory()
     same = all(a[0] == b[0] and a[1]["iterations"] == b[1]["iterations"] and a[2] == b[2]
-               for a, b in zip(r_plain, r_serve))
+               for a, b in zip(r_alone, r_serve))
     statuses = [r[0] for r in r_serve]
     its = [r[1]["iterations"] for r in r_serve]
+    its_plain = [r[1]["iterations"] for r in r_plain]
+    tres = max(r[1]["true_residual_inf"] for r in r_serve)
+    tres_plain = max(r[1]["true_residual_inf"] for r in r_plain)
     cells = [int(np.prod(ds[i].size)) for i in picks]
     for dom in ids:
         srv.remove_domain(dom)
     srv.close()
+    for h in plain:
+        h.close()
     line = {
         "metric": "Poisson solves/sec @1e-6 rel. residual (serving) + p50/p99 latency", "value": serve_rate,
         "unit": "solves/s", "n_gpus": 1, "steps": K, "warmup": len(ds), "ms_per_step": 1e3 / serve_rate,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 dots, alpha/beta)",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 dots, alpha/beta, iterate)",
         "data": "synthetic",
         "config": {"workload": "c4_serving_sample", "domains": [d.name for d in ds], "requests": K,
-                   "slots": args.slots, "precision": "mixed", "tol": 1e-6,
+                   "slots": args.slots, "precision": "mixed", "coarse_solve": "exact", "tol": 1e-6,
                    "l2": "no flush: resident domains, per-request working sets from 1 MB to 30 MB per vector"},
         "plain_one_in_flight": {"value": plain_rate, "unit": "solves/s",
+                                "settings": "reference precision, 200 coarsest smoothing steps (hdd_solve)",
                                 "saturated_latency_ms": percentiles([r[3] for r in r_plain]),
-                                "open_loop_latency_ms": percentiles(lat_plain)},
+                                "open_loop_latency_ms": percentiles(lat_plain),
+                                "iterations": {"min": int(min(its_plain)), "max": int(max(its_plain))},
+                                "max_true_residual": tres_plain},
+        "serving_form_one_in_flight": {"value": alone_rate, "unit": "solves/s",
+                                       "speedup_from_concurrency": serve_rate / alone_rate},
         "latency_ms": {"saturated": percentiles([r[3] for r in r_serve]), "open_loop": percentiles(lat_serve),
                        "open_loop_rate": rate},
         "speedup_vs_plain": serve_rate / plain_rate,
-        "results_identical_to_plain": bool(same),
+        "results_identical_alone_and_in_mix": bool(same),
         "statuses": {str(s_): statuses.count(s_) for s_ in set(statuses)},
         "iterations": {"min": int(min(its)), "max": int(max(its))},
+        "max_true_residual": tres,
         "setup_s": setup_s, "device_bytes_reserved": srv_mem[0],
         "e2e": {"value": serve_rate, "unit": "solves/s", "h2d_bytes_per_step": 4 * float(np.mean(cells)),
                 "d2h_bytes_per_step": 4 * float(np.mean(cells))},
@@ -444,35 +490,59 @@ def run_serving(args):
 def run_serving_fresh(args):
     """Serving with a new domain per request, as the serving workload states it:
     each request is a domain (cube side cycling through 64..192, 1-4 random
-    Dirichlet spheres, mixed precision) and a right-hand side, so its setup
-    (interface assembly, factorisations, uploads) is part of its latency.
+    Dirichlet spheres) and a right-hand side, so its setup (interface
+    assembly, factorisations, uploads) is part of its latency.
 
-    * plain: one request at a time (add the domain, solve, remove it);
-    * serving: all requests queued at once; the server admits domains by HBM
-      footprint, sets up to slots - 1 of them while others solve, and each
-      domain is removed once its result is collected.
+    * plain drop-in: one request at a time with the reference's settings
+      (hdd_create, hdd_initialize_preconditioner, hdd_solve, hdd_destroy);
+    * serving form (mixed precision, exact coarsest interface solve): the
+      same one at a time through the server, then all requests queued at
+      once; the server admits domains by HBM footprint, sets up to slots - 1
+      of them while others solve, and each domain is removed once its result
+      is collected.
     solves/s = requests / makespan; latency = domain added to result ready.
     """
-    from hierarchicaldd_b200 import domains
+    from hierarchicaldd_b200 import _lib, domains
     from hierarchicaldd_b200.server import SolveServer, make_options
+    from hierarchicaldd_b200.solver import SPGrid_Domain_Decomposition_Solver
 
     K = args.requests
     ds = domains.serving_mix(K, seed=45)
     srv = SolveServer(slots=args.slots)
-    opts = [make_options(d.size, d.sub_size, tol=1e-6, max_iters=1000, **dict(d.meta)) for d in ds]
+
+    def serving_meta(d):
+        m = dict(d.meta)
+        m.update(precision_mode=_lib.PRECISION_MIXED, coarse_solve=_lib.COARSE_EXACT)
+        return m
+
+    opts = [make_options(d.size, d.sub_size, tol=1e-6, max_iters=1000, **serving_meta(d)) for d in ds]
 
     def digest(x):
         return hashlib.sha1(x.tobytes()).hexdigest()
 
     with ClockSampler(0) as clk:
         plain, t = [], time.perf_counter()
+        for d in ds:
+            ta = time.perf_counter()
+            m = d.meta
+            h = SPGrid_Domain_Decomposition_Solver()
+            h.Set_Domain(d.flags, d.rhs)
+            h.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"],
+                                        m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"],
+                                        m["sigma_mg"], tol=1e-6, max_iters=1000)
+            res = h.Solve(allow_not_converged=True)
+            h.Solution()
+            h.close()
+            plain.append((0 if res["converged"] else 3, res["iterations"], (time.perf_counter() - ta) * 1e3))
+        t_plain = time.perf_counter() - t
+        alone, t = [], time.perf_counter()
         for k, d in enumerate(ds):
             ta = time.perf_counter()
             dom = srv.add_domain(d.flags, opts[k])
             st, res, x, _ = srv.poll(srv.submit(dom, d.rhs), dom)
-            plain.append((st, res["iterations"], digest(x), (time.perf_counter() - ta) * 1e3))
+            alone.append((st, res["iterations"], digest(x), (time.perf_counter() - ta) * 1e3))
             srv.remove_domain(dom)
-        t_plain = time.perf_counter() - t
+        t_alone = time.perf_counter() - t
         serve, t = [], time.perf_counter()
         doms, reqs = [], []
         for k, d in enumerate(ds):
@@ -485,23 +555,28 @@ def run_serving_fresh(args):
             srv.remove_domain(doms[k])
         t_serve = time.perf_counter() - t
     srv.close()
-    same = all(a[:3] == b[:3] for a, b in zip(plain, serve))
+    same = all(a[:3] == b[:3] for a, b in zip(alone, serve))
     statuses = [r[0] for r in serve]
     cells = [int(np.prod(d.size)) for d in ds]
-    serve_rate, plain_rate = K / t_serve, K / t_plain
+    serve_rate, plain_rate, alone_rate = K / t_serve, K / t_plain, K / t_alone
     line = {
         "metric": "Poisson solves/sec @1e-6 rel. residual (serving, a new domain per request) + p50/p99 latency",
         "value": serve_rate, "unit": "solves/s", "n_gpus": 1, "steps": K, "warmup": 0,
         "ms_per_step": 1e3 / serve_rate, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 (f64 dots, alpha/beta)", "data": "synthetic",
+        "dtype": "f32 (f64 dots, alpha/beta, iterate)", "data": "synthetic",
         "config": {"workload": "c4_serving_fresh_domains", "requests": K, "slots": args.slots,
-                   "sides": sorted({d.size[0] - 1 for d in ds}), "precision": "mixed", "tol": 1e-6,
-                   "l2": "no flush: every request is a new domain"},
+                   "sides": sorted({d.size[0] - 1 for d in ds}), "precision": "mixed", "coarse_solve": "exact",
+                   "tol": 1e-6, "l2": "no flush: every request is a new domain"},
         "plain_one_in_flight": {"value": plain_rate, "unit": "solves/s",
-                                "latency_ms": percentiles([r[3] for r in plain])},
+                                "settings": "reference precision, 200 coarsest smoothing steps",
+                                "latency_ms": percentiles([r[2] for r in plain]),
+                                "statuses": {str(s_): [r[0] for r in plain].count(s_) for s_ in {r[0] for r in plain}}},
+        "serving_form_one_in_flight": {"value": alone_rate, "unit": "solves/s",
+                                       "latency_ms": percentiles([r[3] for r in alone]),
+                                       "speedup_from_concurrency": serve_rate / alone_rate},
         "latency_ms": percentiles([r[3] for r in serve]),
         "speedup_vs_plain": serve_rate / plain_rate,
-        "results_identical_to_plain": bool(same),
+        "results_identical_alone_and_in_mix": bool(same),
         "statuses": {str(s_): statuses.count(s_) for s_ in set(statuses)},
         "e2e": {"value": serve_rate, "unit": "solves/s", "h2d_bytes_per_step": 8 * float(np.mean(cells)),
                 "d2h_bytes_per_step": 4 * float(np.mean(cells))},
@@ -606,9 +681,9 @@ def main():
     # Per-phase device timing (separate, instrumented solve): CUDA events on
     # the solver's stream around each phase's launches, with the phase's
     # algorithmic bytes accounted by the library.
-    ms = (C.c_double * 8)()
-    cnt = (C.c_longlong * 8)()
-    nbytes = (C.c_double * 8)()
+    ms = (C.c_double * len(PHASES))()
+    cnt = (C.c_longlong * len(PHASES))()
+    nbytes = (C.c_double * len(PHASES))()
     lib.hdd_set_kernel_timing(s.h, 1)
     prof = s.Solve()
     lib.hdd_get_kernel_timing(s.h, ms, cnt)
@@ -621,7 +696,8 @@ def main():
     # Roofline (HBM-bound kernels) of every timed kernel; the dominant one by
     # device time is the headline.
     hbm, peak_kind = peaks()
-    kernels = {0: "vcycle_cluster_kernel" if d.sub_size[0] == 32 else "vcycle_kernel", 1: "laplace_dot_kernel",
+    kernels = {0: "vcycle_cluster_kernel" if d.sub_size[0] == 32 else "vcycle_kernel",
+               1: "laplace_dot_march_kernel" if d.sub_size[0] in (8, 16, 32) else "laplace_dot_kernel",
                6: "sn_forward_kernel", 7: "sn_backward_kernel"}
     per_kernel = {}
     for i, kname in kernels.items():

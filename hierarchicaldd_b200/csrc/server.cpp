@@ -377,9 +377,6 @@ hdd_status hdd_server_add_domain(hdd_server* srv, const hdd_options* opts, const
         Domain d;
         d.opts = *opts;
         d.opts.device = srv->opt.device;
-        // Each request's persistent interface solves take a share of the
-        // device, so that `slots` of them run side by side.
-        if (d.opts.solve_share == 0) d.opts.solve_share = srv->opt.slots;
         const size_t n = (size_t)opts->size[0] * opts->size[1] * opts->size[2];
         d.flags.assign(flags, flags + n);
         d.reserved = estimate_bytes(d.opts, flags);

@@ -66,8 +66,8 @@ typedef struct {
     int device;             /* CUDA device ordinal */
     int coarse_solve;       /* HDD_COARSE_* : how the coarsest interface level is solved */
     int solve_share;        /* persistent interface solves use 1/solve_share of the device's
-                               resident CTAs (0 or 1 = all), leaving room for concurrent solves
-                               (the server sets it to its slot count); results do not depend on it */
+                               resident CTAs (0 or 1 = all), leaving room for concurrent solves;
+                               results do not depend on it */
 } hdd_options;
 
 /* Coarsest interface (sigma) level.  The reference runs 200 smoothing steps
