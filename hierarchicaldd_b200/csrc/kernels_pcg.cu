@@ -11,6 +11,7 @@
 
 #include <cfloat>
 #include <cstdint>
+#include <cstdlib>
 
 #include "hdd_common.h"
 #include "kernels.h"
@@ -453,7 +454,12 @@ cudaError_t launch_tiles_to_dense_f64(const TileGeom& g, const int* txyz, int sx
 
 // Work units of the marching Laplacian: (tile, slab) pairs, two slabs of 16
 // planes per 32^3 tile so that a 256^3 domain gives 1024 CTAs.
-static int laplace_slabs(int sub) { return sub == 32 ? 2 : 1; }
+static int laplace_slabs(int sub) {
+    if (sub != 32) return 1;
+    const char* e = std::getenv("HDD_LAPLACE_SLABS");
+    const int v = e ? std::atoi(e) : 2;
+    return (v == 1 || v == 4) ? v : 2;
+}
 
 int laplace_partials(const TileGeom& g) {
     if (g.sub == 8 || g.sub == 16 || g.sub == 32) return g.ntiles * laplace_slabs(g.sub);
@@ -471,7 +477,11 @@ static void launch_march(const TileGeom& g, const float* s, float* q, double* pa
 cudaError_t launch_laplace_dot(const TileGeom& g, const float* s, float* q, double* partial, cudaStream_t st) {
     if (g.ntiles == 0) return cudaSuccess;
     switch (g.sub) {
-        case 32: launch_march<32, 2>(g, s, q, partial, st); break;
+        case 32:
+            if (laplace_slabs(32) == 1) launch_march<32, 1>(g, s, q, partial, st);
+            else if (laplace_slabs(32) == 4) launch_march<32, 4>(g, s, q, partial, st);
+            else launch_march<32, 2>(g, s, q, partial, st);
+            break;
         case 16: launch_march<16, 1>(g, s, q, partial, st); break;
         case 8: launch_march<8, 1>(g, s, q, partial, st); break;
         default: laplace_dot_kernel<<<g.ntiles, kNT, 0, st>>>(g, s, q, partial); break;
