@@ -44,6 +44,8 @@ def parse():
     p.add_argument("--domains", type=int, default=4, help="c4: resident domains")
     p.add_argument("--requests", type=int, default=32, help="c4: requests per timed run")
     p.add_argument("--slots", type=int, default=4, help="c4: requests in flight")
+    p.add_argument("--batch", type=int, default=4, choices=[0, 2, 4],
+                   help="c4: requests of one domain solved together in shared launches (0 = off)")
     p.add_argument("--fresh-domains", action="store_true",
                    help="c4: every request brings its own new domain (setup counted in its latency)")
     p.add_argument("--one-solve", action="store_true",
@@ -330,8 +332,9 @@ def run_serving(args):
 
     * serving form: mixed precision (FP32 operators, FP64 PCG scalars and
       iterate) with the coarsest interface level solved exactly
-      (HDD_COARSE_EXACT), up to ``--slots`` requests in flight through the
-      hdd_server_* C ABI (a pool of solve contexts per resident domain);
+      (HDD_COARSE_EXACT), through the hdd_server_* C ABI with ``--slots``
+      workers and continuous batching (``--batch`` requests of one domain
+      solved together in shared launches, joining as systems free up);
     * plain drop-in: the reference's settings (reference precision, 200
       coarsest smoothing steps) through hdd_set_rhs_dense / hdd_solve /
       hdd_get_solution_dense, one request at a time;
@@ -358,7 +361,7 @@ def run_serving(args):
         m.update(precision_mode=_lib.PRECISION_MIXED, coarse_solve=_lib.COARSE_EXACT)
         return m
 
-    srv = SolveServer(slots=args.slots)
+    srv = SolveServer(slots=args.slots, batch=args.batch)
     t0 = time.perf_counter()
     ids = [srv.add_domain(d.flags, make_options(d.size, d.sub_size, tol=1e-6, max_iters=1000, **serving_meta(d)))
            for d in ds]
@@ -462,7 +465,8 @@ def run_serving(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 dots, alpha/beta, iterate)",
         "data": "synthetic",
         "config": {"workload": "c4_serving_sample", "domains": [d.name for d in ds], "requests": K,
-                   "slots": args.slots, "precision": "mixed", "coarse_solve": "exact", "tol": 1e-6,
+                   "slots": args.slots, "batch": args.batch, "precision": "mixed", "coarse_solve": "exact",
+                   "tol": 1e-6,
                    "l2": "no flush: resident domains, per-request working sets from 1 MB to 30 MB per vector"},
         "plain_one_in_flight": {"value": plain_rate, "unit": "solves/s",
                                 "settings": "reference precision, 200 coarsest smoothing steps (hdd_solve)",
@@ -508,7 +512,7 @@ def run_serving_fresh(args):
 
     K = args.requests
     ds = domains.serving_mix(K, seed=45)
-    srv = SolveServer(slots=args.slots)
+    srv = SolveServer(slots=args.slots, batch=args.batch)
 
     def serving_meta(d):
         m = dict(d.meta)

@@ -53,7 +53,7 @@ class HddError(RuntimeError):
 
 class hdd_server_options(C.Structure):
     _fields_ = [("slots", C.c_int), ("hbm_budget_bytes", C.c_longlong), ("device", C.c_int),
-                ("setup_threads", C.c_int)]
+                ("setup_threads", C.c_int), ("batch", C.c_int)]
 
 
 # Every symbol declared in include/hdd.h: name -> (restype, argtypes).
@@ -81,6 +81,7 @@ SIGNATURES = {
     "hdd_multiply_dot_dense_device_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "hdd_sigma_vcycle": (C.c_int, [_vp, _fp, _fp]),
     "hdd_interface_solve": (C.c_int, [_vp, C.c_int, C.c_int, _fp, _fp, _ip]),
+    "hdd_interface_solve_batch": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _fp, _fp, _ip]),
     "hdd_interface_size": (C.c_int, [_vp, C.c_int, _ip]),
     "hdd_interface_map": (C.c_int, [_vp, _ip]),
     "hdd_interface_matrix": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _ip, _ip, _ip, _ip, _ip,

@@ -292,6 +292,11 @@ hdd_status hdd_sigma_vcycle(hdd_solver* s, const float* b0, float* u0) {
     return guard(s, [&](Solver& v) { v.sigma_vcycle_host(b0, u0); });
 }
 
+hdd_status hdd_interface_solve_batch(hdd_solver* s, int kind, int level, int nrhs, const float* b, float* x, int* n) {
+    if (!n || (kind != 0 && kind != 1)) return HDD_ERR_INVALID_ARGUMENT;
+    return guard(s, [&](Solver& v) { v.interface_solve_batch(kind, level, nrhs, b, x, n); });
+}
+
 hdd_status hdd_interface_solve(hdd_solver* s, int kind, int level, const float* b, float* x, int* n) {
     if (!n || (kind != 0 && kind != 1)) return HDD_ERR_INVALID_ARGUMENT;
     return guard(s, [&](Solver& v) { v.interface_solve(kind, level, b, x, n); });

@@ -9,6 +9,19 @@ namespace hdd {
 
 constexpr int kMaxLevels = 8;
 
+// k independent systems on one domain solved side by side: system j's
+// vectors start j * vstride elements after system 0's, its per-tile partial
+// sums j * pstride after, its scalars at PcgScalars + j.  active[j] == 0
+// leaves system j's state untouched (its slot is free); first[j] != 0 starts
+// its search direction afresh.  k = 1 with null arrays is a single system.
+struct Batch {
+    int k = 1;
+    size_t vstride = 0;
+    int pstride = 0;
+    const int* active = nullptr;
+    const int* first = nullptr;
+};
+
 struct VcycleArgs {
     float* u;                  // tiled level-0 solution (read halos, write interiors)
     const float* b;            // tiled level-0 right-hand side
@@ -27,6 +40,11 @@ struct VcycleArgs {
     float inv_diag[8];         // omega / face_count (float division on the host)
     float restrict_w[64];      // (1/8,3/8,3/8,1/8)^3 tensor weights
     float prolong_w[8];        // 4 * (3/4,1/4)^3 tensor weights
+    // Systems side by side (blockIdx.y): u and b of system j at + j * slot_stride;
+    // a system whose active entry is 0 is skipped.
+    int nslots;
+    size_t slot_stride;
+    const int* active;
 };
 
 cudaError_t launch_vcycle(const VcycleArgs& a, cudaStream_t stream);
@@ -45,12 +63,15 @@ struct TileGeom {
 // partial[0 .. laplace_partials(g)) = sums of (double)(s*q) (float products)
 // over fixed parts of the tiles, to be reduced with launch_reduce_sum.
 cudaError_t launch_laplace_dot(const TileGeom& g, const float* s, float* q, double* partial,
-                               cudaStream_t stream);
+                               cudaStream_t stream, const Batch& B = Batch());
 int laplace_partials(const TileGeom& g);
 
-// Deterministic final sums of per-tile partials into out[slot] (double).
-cudaError_t launch_reduce_sum(const double* partial, int n, double* out, cudaStream_t stream);
-cudaError_t launch_reduce_max(const float* partial, int n, float* out, cudaStream_t stream);
+// Deterministic final sums of per-tile partials into out[slot] (double);
+// batched: system j's n partials at partial + j * pstride into out[j * ostride].
+cudaError_t launch_reduce_sum(const double* partial, int n, double* out, cudaStream_t stream,
+                              const Batch& B = Batch(), int ostride = 0);
+cudaError_t launch_reduce_max(const float* partial, int n, float* out, cudaStream_t stream,
+                              const Batch& B = Batch(), int ostride = 0);
 
 // Scalar state of the PCG loop on the device.
 struct PcgScalars {
@@ -64,21 +85,24 @@ struct PcgScalars {
 
 // partial[tile] = sum (double)(a*b) with project(a) applied in place.
 cudaError_t launch_project_dot(const TileGeom& g, float* a, const float* b, double* partial,
-                               cudaStream_t stream);
+                               cudaStream_t stream, const Batch& B = Batch());
 // s = beta*s + z (first: s = z); beta from scalars (mode 0 float, 1 double).
 cudaError_t launch_update_s(const TileGeom& g, float* s, const float* z, const PcgScalars* sc, int first,
-                            int mode, cudaStream_t stream);
+                            int mode, cudaStream_t stream, const Batch& B = Batch());
 // x += alpha s; r -= alpha q; partial max|r| per tile.  With xd (mode 1) the
 // iterate is kept in FP64 (xd += alpha s) and x is its FP32 rounding.
 cudaError_t launch_update_xr(const TileGeom& g, float* x, float* r, const float* s, const float* q,
                              const PcgScalars* sc, int mode, float* partial_max, cudaStream_t stream,
-                             double* xd = nullptr);
-// r = Project((float)(b - A x)) for an FP64 iterate x, in FP64; partial max|r|.
+                             double* xd = nullptr, const Batch& B = Batch());
+// r = Project((float)(b - A x)) for an FP64 iterate x, in FP64; partial max|r|
+// (batched: only the systems whose active entry is set).
 cudaError_t launch_residual_f64(const TileGeom& g, const float* b, const double* x, float* r, float* partial_max,
-                                cudaStream_t stream);
-// Scalar steps (single thread).
-cudaError_t launch_scalar_rho(PcgScalars* sc, const double* rho_sum, int first, cudaStream_t stream);
-cudaError_t launch_scalar_alpha(PcgScalars* sc, const double* sdq_sum, cudaStream_t stream);
+                                cudaStream_t stream, const Batch& B = Batch());
+// Scalar steps (one thread per system); batched sums at sum + j * sstride.
+cudaError_t launch_scalar_rho(PcgScalars* sc, const double* rho_sum, int first, cudaStream_t stream,
+                              const Batch& B = Batch(), int sstride = 0);
+cudaError_t launch_scalar_alpha(PcgScalars* sc, const double* sdq_sum, cudaStream_t stream, const Batch& B = Batch(),
+                                int sstride = 0);
 // r = Project(b - A x); partial max|r|.  precise = 1 subtracts A x in FP64
 // before rounding r (else A x is rounded to FP32 first, as the reference).
 cudaError_t launch_residual(const TileGeom& g, const float* b, const float* x, float* r, float* partial_max,
@@ -98,11 +122,12 @@ cudaError_t launch_tiles_to_dense_f64(const TileGeom& g, const int* tile_xyz, in
 // Interface coupling (Laplace_ri gather and the interface scatter)
 // ---------------------------------------------------------------------------
 // b0[i] = r[c_i] - (float)(-sum over active-face Active neighbours of z)  at Interface cells.
+// Batched: system j's r and z at + j * B.vstride, its b0 at + j * istride.
 cudaError_t launch_interface_gather(const TileGeom& g, const long long* iface_slot, const int* iface_nb_slots,
                                     int n_iface, const float* r, const float* z, float* b0,
-                                    cudaStream_t stream);
+                                    cudaStream_t stream, const Batch& B = Batch(), size_t istride = 0);
 // z[c_i] = u0[i].
 cudaError_t launch_interface_scatter(const long long* iface_slot, int n_iface, const float* u0, float* z,
-                                     cudaStream_t stream);
+                                     cudaStream_t stream, const Batch& B = Batch(), size_t istride = 0);
 
 }  // namespace hdd

@@ -78,7 +78,11 @@ __device__ __forceinline__ float block_max(float v) {
 }
 
 __global__ void __launch_bounds__(kNT) laplace_dot_kernel(TileGeom g, const float* __restrict__ s,
-                                                          float* __restrict__ q, double* partial) {
+                                                          float* __restrict__ q, double* partial, size_t vstride,
+                                                          int pstride) {
+    s += (size_t)blockIdx.y * vstride;
+    q += (size_t)blockIdx.y * vstride;
+    partial += (size_t)blockIdx.y * pstride;
     const int t = blockIdx.x;
     const int S = g.sub, TC = S * S * S;
     const size_t base = (size_t)t * TC;
@@ -122,8 +126,12 @@ struct MarchShape {
 
 template <int S, int SLABS>
 __global__ void __launch_bounds__(kNT, 4) laplace_dot_march_kernel(TileGeom g, const float* __restrict__ s,
-                                                                float* __restrict__ q, double* partial) {
+                                                                float* __restrict__ q, double* partial,
+                                                                size_t vstride, int pstride) {
     using M = MarchShape<S, SLABS>;
+    s += (size_t)blockIdx.y * vstride;
+    q += (size_t)blockIdx.y * vstride;
+    partial += (size_t)blockIdx.y * pstride;
     constexpr int P = M::P, GT = M::GT, NP = M::NP, S2 = S * S, S3 = S * S * S;
     __shared__ float4 plane[2][kNT];
     __shared__ double red[kNT / 32];
@@ -268,7 +276,12 @@ __global__ void __launch_bounds__(kNT) residual_kernel(TileGeom g, const float* 
 // residual), FP64 throughout; partial max|r|.
 __global__ void __launch_bounds__(kNT) residual_f64_kernel(TileGeom g, const float* __restrict__ b,
                                                            const double* __restrict__ x, float* __restrict__ r,
-                                                           float* partial_max) {
+                                                           float* partial_max, Batch B) {
+    if (B.active && !B.active[blockIdx.y]) return;
+    b += (size_t)blockIdx.y * B.vstride;
+    x += (size_t)blockIdx.y * B.vstride;
+    r += (size_t)blockIdx.y * B.vstride;
+    partial_max += (size_t)blockIdx.y * B.pstride;
     const int t = blockIdx.x;
     const int S = g.sub, TC = S * S * S;
     const size_t base = (size_t)t * TC;
@@ -288,7 +301,11 @@ __global__ void __launch_bounds__(kNT) residual_f64_kernel(TileGeom g, const flo
 }
 
 __global__ void __launch_bounds__(kNT) project_dot_kernel(TileGeom g, float* __restrict__ a,
-                                                          const float* __restrict__ bv, double* partial) {
+                                                          const float* __restrict__ bv, double* partial,
+                                                          size_t vstride, int pstride) {
+    a += (size_t)blockIdx.y * vstride;
+    bv += (size_t)blockIdx.y * vstride;
+    partial += (size_t)blockIdx.y * pstride;
     const int t = blockIdx.x;
     const int TC = g.sub * g.sub * g.sub;
     const size_t base = (size_t)t * TC;
@@ -313,7 +330,13 @@ __global__ void __launch_bounds__(kNT) project_kernel(TileGeom g, float* __restr
 
 __global__ void __launch_bounds__(kNT) update_s_kernel(size_t n, float* __restrict__ s,
                                                        const float* __restrict__ z, const PcgScalars* sc,
-                                                       int first, int mode) {
+                                                       int first, int mode, Batch B) {
+    const int j = blockIdx.y;
+    if (B.active && !B.active[j]) return;
+    if (B.first) first = B.first[j];
+    s += (size_t)j * B.vstride;
+    z += (size_t)j * B.vstride;
+    sc += j;
     const float beta = sc->beta;
     const double beta_d = sc->beta_d;
     for (size_t i = blockIdx.x * (size_t)kNT + threadIdx.x; i < n; i += (size_t)gridDim.x * kNT) {
@@ -328,7 +351,14 @@ __global__ void __launch_bounds__(kNT) update_s_kernel(size_t n, float* __restri
 __global__ void __launch_bounds__(kNT) update_xr_kernel(int TC, float* __restrict__ x, float* __restrict__ r,
                                                         const float* __restrict__ s, const float* __restrict__ q,
                                                         const PcgScalars* sc, int mode, float* partial_max,
-                                                        double* __restrict__ xd) {
+                                                        double* __restrict__ xd, Batch B) {
+    const int j = blockIdx.y;
+    if (B.active && !B.active[j]) return;
+    const size_t so = (size_t)j * B.vstride;
+    x += so; r += so; s += so; q += so;
+    if (xd) xd += so;
+    partial_max += (size_t)j * B.pstride;
+    sc += j;
     const int t = blockIdx.x;
     const size_t base = (size_t)t * TC;
     const float alpha = sc->alpha;
@@ -357,21 +387,30 @@ __global__ void __launch_bounds__(kNT) update_xr_kernel(int TC, float* __restric
     if (threadIdx.x == 0) partial_max[t] = m;
 }
 
-__global__ void reduce_sum_kernel(const double* partial, int n, double* out) {
+__global__ void reduce_sum_kernel(const double* partial, int n, double* out, int pstride, int ostride) {
+    partial += (size_t)blockIdx.x * pstride;
+    out += (size_t)blockIdx.x * ostride;
     double acc = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
     acc = block_sum(acc);
     if (threadIdx.x == 0) *out = acc;
 }
 
-__global__ void reduce_max_kernel(const float* partial, int n, float* out) {
+__global__ void reduce_max_kernel(const float* partial, int n, float* out, int pstride, int ostride) {
+    partial += (size_t)blockIdx.x * pstride;
+    out += (size_t)blockIdx.x * ostride;
     float m = 0.0f;
     for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, partial[i]);
     m = block_max(m);
     if (threadIdx.x == 0) *out = m;
 }
 
-__global__ void scalar_rho_kernel(PcgScalars* sc, const double* rho_sum, int first) {
+__global__ void scalar_rho_kernel(PcgScalars* sc, const double* rho_sum, int first, Batch B, int sstride) {
+    const int j = threadIdx.x;
+    if (j >= B.k || (B.active && !B.active[j])) return;
+    if (B.first) first = B.first[j];
+    sc += j;
+    rho_sum += (size_t)j * sstride;
     const double rd = *rho_sum;
     sc->rho_d = rd;
     sc->rho = (float)rd;
@@ -383,7 +422,11 @@ __global__ void scalar_rho_kernel(PcgScalars* sc, const double* rho_sum, int fir
     if (!isfinite(rd)) sc->status = 1;
 }
 
-__global__ void scalar_alpha_kernel(PcgScalars* sc, const double* sdq_sum) {
+__global__ void scalar_alpha_kernel(PcgScalars* sc, const double* sdq_sum, Batch B, int sstride) {
+    const int j = threadIdx.x;
+    if (j >= B.k || (B.active && !B.active[j])) return;
+    sc += j;
+    sdq_sum += (size_t)j * sstride;
     const double sd = *sdq_sum;
     sc->sdq_d = sd;
     const float sdq = (float)sd;
@@ -396,7 +439,11 @@ __global__ void scalar_alpha_kernel(PcgScalars* sc, const double* sdq_sum) {
 }
 
 __global__ void __launch_bounds__(kNT) interface_gather_kernel(const long long* slot, const int* nbs, int n,
-                                                               const float* r, const float* z, float* b0) {
+                                                               const float* r, const float* z, float* b0,
+                                                               size_t vstride, size_t istride) {
+    r += (size_t)blockIdx.y * vstride;
+    z += (size_t)blockIdx.y * vstride;
+    b0 += (size_t)blockIdx.y * istride;
     const int i = blockIdx.x * kNT + threadIdx.x;
     if (i >= n) return;
     double result = 0.0;
@@ -409,7 +456,9 @@ __global__ void __launch_bounds__(kNT) interface_gather_kernel(const long long* 
 }
 
 __global__ void __launch_bounds__(kNT) interface_scatter_kernel(const long long* slot, int n, const float* u0,
-                                                                float* z) {
+                                                                float* z, size_t vstride, size_t istride) {
+    u0 += (size_t)blockIdx.y * istride;
+    z += (size_t)blockIdx.y * vstride;
     const int i = blockIdx.x * kNT + threadIdx.x;
     if (i < n) z[slot[i]] = u0[i];
 }
@@ -467,24 +516,28 @@ int laplace_partials(const TileGeom& g) {
 }
 
 template <int S, int SLABS>
-static void launch_march(const TileGeom& g, const float* s, float* q, double* partial, cudaStream_t st) {
+static void launch_march(const TileGeom& g, const float* s, float* q, double* partial, cudaStream_t st,
+                         const Batch& B) {
     using M = MarchShape<S, SLABS>;
     const long long units = (long long)g.ntiles * SLABS;
     const int grid = (int)((units + M::G - 1) / M::G);
-    laplace_dot_march_kernel<S, SLABS><<<grid, kNT, 0, st>>>(g, s, q, partial);
+    laplace_dot_march_kernel<S, SLABS><<<dim3(grid, B.k), kNT, 0, st>>>(g, s, q, partial, B.vstride, B.pstride);
 }
 
-cudaError_t launch_laplace_dot(const TileGeom& g, const float* s, float* q, double* partial, cudaStream_t st) {
+cudaError_t launch_laplace_dot(const TileGeom& g, const float* s, float* q, double* partial, cudaStream_t st,
+                               const Batch& B) {
     if (g.ntiles == 0) return cudaSuccess;
     switch (g.sub) {
         case 32:
-            if (laplace_slabs(32) == 1) launch_march<32, 1>(g, s, q, partial, st);
-            else if (laplace_slabs(32) == 4) launch_march<32, 4>(g, s, q, partial, st);
-            else launch_march<32, 2>(g, s, q, partial, st);
+            if (laplace_slabs(32) == 1) launch_march<32, 1>(g, s, q, partial, st, B);
+            else if (laplace_slabs(32) == 4) launch_march<32, 4>(g, s, q, partial, st, B);
+            else launch_march<32, 2>(g, s, q, partial, st, B);
             break;
-        case 16: launch_march<16, 1>(g, s, q, partial, st); break;
-        case 8: launch_march<8, 1>(g, s, q, partial, st); break;
-        default: laplace_dot_kernel<<<g.ntiles, kNT, 0, st>>>(g, s, q, partial); break;
+        case 16: launch_march<16, 1>(g, s, q, partial, st, B); break;
+        case 8: launch_march<8, 1>(g, s, q, partial, st, B); break;
+        default:
+            laplace_dot_kernel<<<dim3(g.ntiles, B.k), kNT, 0, st>>>(g, s, q, partial, B.vstride, B.pstride);
+            break;
     }
     return cudaGetLastError();
 }
@@ -495,14 +548,15 @@ cudaError_t launch_residual(const TileGeom& g, const float* b, const float* x, f
     return cudaGetLastError();
 }
 cudaError_t launch_residual_f64(const TileGeom& g, const float* b, const double* x, float* r, float* pm,
-                                cudaStream_t st) {
+                                cudaStream_t st, const Batch& B) {
     if (g.ntiles == 0) return cudaSuccess;
-    residual_f64_kernel<<<g.ntiles, kNT, 0, st>>>(g, b, x, r, pm);
+    residual_f64_kernel<<<dim3(g.ntiles, B.k), kNT, 0, st>>>(g, b, x, r, pm, B);
     return cudaGetLastError();
 }
-cudaError_t launch_project_dot(const TileGeom& g, float* a, const float* b, double* partial, cudaStream_t st) {
+cudaError_t launch_project_dot(const TileGeom& g, float* a, const float* b, double* partial, cudaStream_t st,
+                               const Batch& B) {
     if (g.ntiles == 0) return cudaSuccess;
-    project_dot_kernel<<<g.ntiles, kNT, 0, st>>>(g, a, b, partial);
+    project_dot_kernel<<<dim3(g.ntiles, B.k), kNT, 0, st>>>(g, a, b, partial, B.vstride, B.pstride);
     return cudaGetLastError();
 }
 cudaError_t launch_project(const TileGeom& g, float* v, cudaStream_t st) {
@@ -511,45 +565,50 @@ cudaError_t launch_project(const TileGeom& g, float* v, cudaStream_t st) {
     return cudaGetLastError();
 }
 cudaError_t launch_update_s(const TileGeom& g, float* s, const float* z, const PcgScalars* sc, int first, int mode,
-                            cudaStream_t st) {
+                            cudaStream_t st, const Batch& B) {
     const size_t n = (size_t)g.ntiles * g.sub * g.sub * g.sub;
     if (n == 0) return cudaSuccess;
     int blocks = (int)((n + kNT - 1) / kNT);
     if (blocks > 148 * 16) blocks = 148 * 16;
-    update_s_kernel<<<blocks, kNT, 0, st>>>(n, s, z, sc, first, mode);
+    update_s_kernel<<<dim3(blocks, B.k), kNT, 0, st>>>(n, s, z, sc, first, mode, B);
     return cudaGetLastError();
 }
 cudaError_t launch_update_xr(const TileGeom& g, float* x, float* r, const float* s, const float* q,
-                             const PcgScalars* sc, int mode, float* pm, cudaStream_t st, double* xd) {
+                             const PcgScalars* sc, int mode, float* pm, cudaStream_t st, double* xd, const Batch& B) {
     if (g.ntiles == 0) return cudaSuccess;
-    update_xr_kernel<<<g.ntiles, kNT, 0, st>>>(g.sub * g.sub * g.sub, x, r, s, q, sc, mode, pm, xd);
+    update_xr_kernel<<<dim3(g.ntiles, B.k), kNT, 0, st>>>(g.sub * g.sub * g.sub, x, r, s, q, sc, mode, pm, xd, B);
     return cudaGetLastError();
 }
-cudaError_t launch_reduce_sum(const double* partial, int n, double* out, cudaStream_t st) {
-    reduce_sum_kernel<<<1, 1024, 0, st>>>(partial, n, out);
+cudaError_t launch_reduce_sum(const double* partial, int n, double* out, cudaStream_t st, const Batch& B,
+                              int ostride) {
+    reduce_sum_kernel<<<B.k, 1024, 0, st>>>(partial, n, out, B.pstride, ostride);
     return cudaGetLastError();
 }
-cudaError_t launch_reduce_max(const float* partial, int n, float* out, cudaStream_t st) {
-    reduce_max_kernel<<<1, 1024, 0, st>>>(partial, n, out);
+cudaError_t launch_reduce_max(const float* partial, int n, float* out, cudaStream_t st, const Batch& B, int ostride) {
+    reduce_max_kernel<<<B.k, 1024, 0, st>>>(partial, n, out, B.pstride, ostride);
     return cudaGetLastError();
 }
-cudaError_t launch_scalar_rho(PcgScalars* sc, const double* rho_sum, int first, cudaStream_t st) {
-    scalar_rho_kernel<<<1, 1, 0, st>>>(sc, rho_sum, first);
+cudaError_t launch_scalar_rho(PcgScalars* sc, const double* rho_sum, int first, cudaStream_t st, const Batch& B,
+                              int sstride) {
+    scalar_rho_kernel<<<1, 32, 0, st>>>(sc, rho_sum, first, B, sstride);
     return cudaGetLastError();
 }
-cudaError_t launch_scalar_alpha(PcgScalars* sc, const double* sdq_sum, cudaStream_t st) {
-    scalar_alpha_kernel<<<1, 1, 0, st>>>(sc, sdq_sum);
+cudaError_t launch_scalar_alpha(PcgScalars* sc, const double* sdq_sum, cudaStream_t st, const Batch& B,
+                                int sstride) {
+    scalar_alpha_kernel<<<1, 32, 0, st>>>(sc, sdq_sum, B, sstride);
     return cudaGetLastError();
 }
 cudaError_t launch_interface_gather(const TileGeom&, const long long* slot, const int* nbs, int n, const float* r,
-                                    const float* z, float* b0, cudaStream_t st) {
+                                    const float* z, float* b0, cudaStream_t st, const Batch& B, size_t istride) {
     if (n == 0) return cudaSuccess;
-    interface_gather_kernel<<<(n + kNT - 1) / kNT, kNT, 0, st>>>(slot, nbs, n, r, z, b0);
+    interface_gather_kernel<<<dim3((n + kNT - 1) / kNT, B.k), kNT, 0, st>>>(slot, nbs, n, r, z, b0, B.vstride,
+                                                                            istride);
     return cudaGetLastError();
 }
-cudaError_t launch_interface_scatter(const long long* slot, int n, const float* u0, float* z, cudaStream_t st) {
+cudaError_t launch_interface_scatter(const long long* slot, int n, const float* u0, float* z, cudaStream_t st,
+                                     const Batch& B, size_t istride) {
     if (n == 0) return cudaSuccess;
-    interface_scatter_kernel<<<(n + kNT - 1) / kNT, kNT, 0, st>>>(slot, n, u0, z);
+    interface_scatter_kernel<<<dim3((n + kNT - 1) / kNT, B.k), kNT, 0, st>>>(slot, n, u0, z, B.vstride, istride);
     return cudaGetLastError();
 }
 

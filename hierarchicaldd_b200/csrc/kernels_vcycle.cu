@@ -18,6 +18,7 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -365,6 +366,10 @@ __global__ void __launch_bounds__(NT, 1) vcycle_kernel(VcycleArgs a) {
 
     const int box = blockIdx.x;
     if (box >= a.nbox) return;
+    if (a.active && !a.active[blockIdx.y]) return;
+    // System blockIdx.y of a batch: its u and b.
+    float* const au = a.u + (size_t)blockIdx.y * a.slot_stride;
+    const float* const ab = a.b + (size_t)blockIdx.y * a.slot_stride;
     if (threadIdx.x < 8) s_inv[threadIdx.x] = a.inv_diag[threadIdx.x];
     if (threadIdx.x < 64) s_sc64[threadIdx.x] = a.restrict_w[threadIdx.x];
     if (threadIdx.x < 8) s_sc8[threadIdx.x] = a.prolong_w[threadIdx.x];
@@ -386,8 +391,8 @@ __global__ void __launch_bounds__(NT, 1) vcycle_kernel(VcycleArgs a) {
     }
     const uint8_t* rec = a.box_flags + (size_t)box * a.box_stride;
     const int tile = a.box_tile[box];
-    const float* gu = a.u + (size_t)tile * (SUB * SUB * SUB);
-    const float* gb = a.b + (size_t)tile * (SUB * SUB * SUB);
+    const float* gu = au + (size_t)tile * (SUB * SUB * SUB);
+    const float* gb = ab + (size_t)tile * (SUB * SUB * SUB);
 
     // Zero every level (halo cells, r and coarse values start at zero).
     for (int l = 0; l < a.levels; ++l) {
@@ -416,7 +421,7 @@ __global__ void __launch_bounds__(NT, 1) vcycle_kernel(VcycleArgs a) {
         for (int axis = 0; axis < 3; ++axis) {
             const int nt = a.box_nb[3 * box + axis];
             if (nt < 0) continue;
-            const float* gn = a.u + (size_t)nt * (SUB * SUB * SUB);
+            const float* gn = au + (size_t)nt * (SUB * SUB * SUB);
             for (int q = threadIdx.x; q < (SUB - 1) * (SUB - 1); q += NT) {
                 const int p1 = q % (SUB - 1) + 1, p0 = q / (SUB - 1) + 1;
                 int lx, ly, lz, bx, by, bz;
@@ -453,7 +458,7 @@ __global__ void __launch_bounds__(NT, 1) vcycle_kernel(VcycleArgs a) {
     }
 
     // Store the interior cells (1..SUB-1 per axis) of level 0.
-    float* gw = a.u + (size_t)tile * (SUB * SUB * SUB);
+    float* gw = au + (size_t)tile * (SUB * SUB * SUB);
     for (int q = threadIdx.x; q < SUB * SUB * SUB; q += NT) {
         const int z = q % SUB, t = q / SUB;
         const int y = t % SUB, x = t / SUB;
@@ -557,6 +562,10 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
     const int rank = (int)cluster.block_rank();
     const int box = blockIdx.x / C;
     if (box >= a.nbox) return;  // uniform across the cluster
+    if (a.active && !a.active[blockIdx.y]) return;  // a cluster shares its blockIdx.y
+    // System blockIdx.y of a batch: its u and b.
+    float* const au = a.u + (size_t)blockIdx.y * a.slot_stride;
+    const float* const ab = a.b + (size_t)blockIdx.y * a.slot_stride;
     if (threadIdx.x < 8) s_inv[threadIdx.x] = a.inv_diag[threadIdx.x];
     if (threadIdx.x < 64) s_sc64[threadIdx.x] = a.restrict_w[threadIdx.x];
     if (threadIdx.x < 8) s_sc8[threadIdx.x] = a.prolong_w[threadIdx.x];
@@ -586,8 +595,8 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
     const uint8_t* rec = a.box_flags + (size_t)box * a.box_stride;
     const int tile = a.box_tile[box];
     constexpr int TC = SUB * SUB * SUB;
-    const float* gu = a.u + (size_t)tile * TC;
-    const float* gb = a.b + (size_t)tile * TC;
+    const float* gu = au + (size_t)tile * TC;
+    const float* gb = ab + (size_t)tile * TC;
 
     // Load level 0: halo planes / rows from u (interface values) or zero.
     auto load_u = [&](int x, int y, int z) -> float {
@@ -601,7 +610,7 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
         const int nt = a.box_nb[3 * box + axis];
         if (nt < 0) return 0.0f;
         const int lx = (axis == 0) ? 0 : x, ly = (axis == 1) ? 0 : y, lz = (axis == 2) ? 0 : z;
-        return a.u[(size_t)nt * TC + (lx * SUB + ly) * SUB + lz];
+        return au[(size_t)nt * TC + (lx * SUB + ly) * SUB + lz];
     };
     for (int q = threadIdx.x; q < (np + 2) * PS; q += NT) {
         const int lx = q / PS, rem = q % PS, y = rem / E, z = rem % E;
@@ -853,7 +862,7 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
         for (int i = 0; i < a.boundary_itr; ++i) slab_sweep(1);
     }
 
-    float* gw = a.u + (size_t)tile * TC;
+    float* gw = au + (size_t)tile * TC;
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
         if (off[l] < 0) continue;
@@ -891,7 +900,7 @@ cudaError_t launch_cluster(const VcycleArgs& a, cudaStream_t stream) {
     cudaError_t e = ensure_smem_limit((const void*)kern, smem);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(a.nbox * C), 1, 1);
+    cfg.gridDim = dim3((unsigned)(a.nbox * C), (unsigned)std::max(1, a.nslots), 1);
     cfg.blockDim = dim3(NT, 1, 1);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
@@ -914,7 +923,7 @@ cudaError_t launch_vcycle(const VcycleArgs& a, cudaStream_t stream) {
         case 8: {
             constexpr int NT = 128;
             const size_t smem = vcycle_smem_bytes<8>(a.levels);
-            vcycle_kernel<8, NT><<<a.nbox, NT, smem, stream>>>(a);
+            vcycle_kernel<8, NT><<<dim3(a.nbox, std::max(1, a.nslots)), NT, smem, stream>>>(a);
             return cudaGetLastError();
         }
         case 16: {
@@ -923,7 +932,7 @@ cudaError_t launch_vcycle(const VcycleArgs& a, cudaStream_t stream) {
             const size_t smem = vcycle_smem_bytes<16>(a.levels);
             cudaError_t e = ensure_smem_limit((const void*)vcycle_kernel<16, NT>, smem);
             if (e != cudaSuccess) return e;
-            vcycle_kernel<16, NT><<<a.nbox, NT, smem, stream>>>(a);
+            vcycle_kernel<16, NT><<<dim3(a.nbox, std::max(1, a.nslots)), NT, smem, stream>>>(a);
             return cudaGetLastError();
         }
         case 32:

@@ -56,6 +56,12 @@ struct Domain {
     long long work_bytes = 0;        // device bytes of one further context
     long long reserved = 0;          // bytes counted against the budget
     int running = 0;                 // requests being solved on it
+    // Continuous batching: one batch context (k systems) whose driver pulls
+    // this domain's queued requests into free systems as they arrive.
+    std::unique_ptr<Work> batch;
+    int batch_k = 0;                 // systems per batch (0: batching off for this domain)
+    long long batch_bytes = 0;
+    bool batch_running = false;
     bool removing = false;
     int queued = 0;                  // requests not yet finished
 };
@@ -186,6 +192,11 @@ struct hdd_server {
             dd.idle.assign(1, &dd.solver->w0);
             dd.contexts = 1;
             dd.work_bytes = (long long)dd.solver->work_bytes();
+            if (opt.batch >= 2) {
+                const int kmax = dd.solver->max_batch();
+                dd.batch_k = opt.batch >= 4 && kmax >= 4 ? 4 : (kmax >= 2 ? 2 : 0);
+                if (dd.batch_k) dd.batch_bytes = (long long)dd.solver->work_bytes(dd.batch_k);
+            }
             dd.state = DomainState::Resident;
         } else {
             reserved -= dd.reserved;
@@ -263,12 +274,113 @@ struct hdd_server {
         --dd.queued;
     }
 
-    // Whether a queued request of `d` can start now: an idle context, or
-    // room for one more (at most `slots` per domain, within the budget).
+    // Whether a queued request of `d` can start now: its batch driver is
+    // idle (a running driver takes the domain's requests itself), or an idle
+    // context, or room for one more (at most `slots` per domain, within the
+    // budget).
     bool can_run(const Domain& d) const {
         if (d.state != DomainState::Resident) return false;
+        if (d.batch_k) return !d.batch_running && (d.batch || reserved + d.batch_bytes <= budget);
         if (!d.idle.empty()) return true;
         return d.contexts < opt.slots && reserved + d.work_bytes <= budget;
+    }
+
+    // The batch driver of request rid's domain: solves it and every request
+    // of the domain queued while the batch runs, k at a time.
+    struct Feeder : hdd::BatchFeeder {
+        hdd_server* srv;
+        long long dom;
+        long long first_id;
+        std::vector<float> first_rhs;
+        bool first_taken = false;
+        std::map<long long, std::vector<float>> rhs;  // kept until the request ends
+        bool next(const float** out, long long* id) override {
+            if (!first_taken) {
+                first_taken = true;
+                rhs[first_id] = std::move(first_rhs);
+                *out = rhs[first_id].data();
+                *id = first_id;
+                return true;
+            }
+            std::lock_guard<std::mutex> lk(srv->mu);
+            if (srv->stop) return false;
+            for (auto it = srv->queue.begin(); it != srv->queue.end(); ++it) {
+                Request& r = srv->requests.at(*it);
+                if (r.domain != dom) continue;
+                const long long rid = *it;
+                srv->queue.erase(it);
+                std::vector<float>& v = rhs[rid];
+                v.swap(r.rhs);
+                *out = v.data();
+                *id = rid;
+                return true;
+            }
+            return false;
+        }
+        void done(long long id, hdd_status st, const hdd_result& res, std::vector<float>&& x) override {
+            rhs.erase(id);
+            std::lock_guard<std::mutex> lk(srv->mu);
+            Request& r = srv->requests.at(id);
+            r.result = res;
+            r.x = std::move(x);
+            srv->finish(r, st);
+            --srv->domains.at(dom).queued;
+            srv->cv.notify_all();
+        }
+    };
+
+    void run_batch(long long rid, std::unique_lock<std::mutex>& lk) {
+        Request& r = requests.at(rid);
+        const long long dom = r.domain;
+        Domain& d = domains.at(dom);
+        d.batch_running = true;
+        Solver* s = d.solver.get();
+        const int k = d.batch_k;
+        bool make = !d.batch;
+        if (make) {
+            d.reserved += d.batch_bytes;
+            reserved += d.batch_bytes;
+        }
+        Feeder feed;
+        feed.srv = this;
+        feed.dom = dom;
+        feed.first_id = rid;
+        feed.first_rhs.swap(r.rhs);
+        Work* w = d.batch.get();
+        lk.unlock();
+        std::unique_ptr<Work> made;
+        hdd_status st = HDD_OK;
+        try {
+            if (make) {
+                made = s->make_work(k);
+                w = made.get();
+            }
+            s->solve_batch(*w, feed);
+        } catch (const Error& e) {
+            st = e.status;
+        } catch (const std::bad_alloc&) {
+            st = HDD_ERR_OUT_OF_MEMORY;
+        } catch (const std::exception&) {
+            st = HDD_ERR_INTERNAL;
+        }
+        lk.lock();
+        Domain& dd = domains.at(dom);
+        if (made) dd.batch = std::move(made);
+        else if (make) {
+            // The batch context could not be made: give its reservation back
+            // and run this domain's requests on single contexts from now on.
+            dd.reserved -= dd.batch_bytes;
+            reserved -= dd.batch_bytes;
+            dd.batch_k = 0;
+        }
+        // A request not yet handed to the batch when it failed (the first
+        // one, if the context could not be made) fails with it.
+        if (!feed.first_taken) {
+            Request& rr = requests.at(rid);
+            finish(rr, st == HDD_OK ? HDD_ERR_INTERNAL : st);
+            --dd.queued;
+        }
+        dd.batch_running = false;
     }
 
     // Index in `queue` of the oldest request whose domain can run now, or -1.
@@ -300,7 +412,8 @@ struct hdd_server {
             if (qi >= 0) {
                 const long long rid = queue[(size_t)qi];
                 queue.erase(queue.begin() + qi);
-                run_solve(rid, lk);
+                if (domains.at(requests.at(rid).domain).batch_k) run_batch(rid, lk);
+                else run_solve(rid, lk);
             } else {
                 const long long id = setups.front();
                 setups.pop_front();
@@ -334,10 +447,12 @@ void hdd_server_options_default(hdd_server_options* o) {
     o->hbm_budget_bytes = 0;
     o->device = 0;
     o->setup_threads = 0;
+    o->batch = 0;
 }
 
 hdd_status hdd_server_create(const hdd_server_options* o, hdd_server** out) {
-    if (!o || !out || o->slots < 1 || o->slots > 64 || o->hbm_budget_bytes < 0 || o->setup_threads < 0)
+    if (!o || !out || o->slots < 1 || o->slots > 64 || o->hbm_budget_bytes < 0 || o->setup_threads < 0 ||
+        o->batch < 0 || o->batch > 4)
         return HDD_ERR_INVALID_ARGUMENT;
     *out = nullptr;
     int ndev = 0;
@@ -477,7 +592,8 @@ hdd_status hdd_server_remove_domain(hdd_server* srv, long long domain_id) {
             it->second.removing = true;
             srv->cv.wait(lk, [&] {
                 const Domain& d = srv->domains.at(domain_id);
-                return srv->stop || (d.queued == 0 && d.running == 0 && d.state != DomainState::SettingUp &&
+                return srv->stop || (d.queued == 0 && d.running == 0 && !d.batch_running &&
+                                     d.state != DomainState::SettingUp &&
                                      d.state != DomainState::Admitted);
             });
             if (srv->stop) return HDD_ERR_BUSY;
@@ -490,6 +606,7 @@ hdd_status hdd_server_remove_domain(hdd_server* srv, long long domain_id) {
             }
             s = std::move(d.solver);
             extra.swap(d.extra);
+            if (d.batch) extra.push_back(std::move(d.batch));
             srv->domains.erase(domain_id);
             srv->admit();
             srv->cv.notify_all();

@@ -48,9 +48,14 @@ using dev::ck;
 // y = b + A x        (mode 1)
 // y = b - A x        (mode 2)
 // y = y + A x        (mode 3)
+// for system blockIdx.y: x, b, y at + blockIdx.y * (xs, bs, ys).
 __global__ void __launch_bounds__(kNT) csr_kernel(int rows, const int* __restrict__ ptr, const int* __restrict__ col,
                                                   const float* __restrict__ val, const float* __restrict__ x,
-                                                  const float* __restrict__ b, float* __restrict__ y, int mode) {
+                                                  const float* __restrict__ b, float* __restrict__ y, int mode,
+                                                  size_t xs, size_t bs, size_t ys) {
+    x += (size_t)blockIdx.y * xs;
+    if (b) b += (size_t)blockIdx.y * bs;
+    y += (size_t)blockIdx.y * ys;
     const int r = blockIdx.x * kNT + threadIdx.x;
     if (r >= rows) return;
     float acc = (mode == 1) ? b[r] : 0.0f;
@@ -65,9 +70,10 @@ __global__ void fill_kernel(float* p, size_t n, float v) {
 }
 
 void launch_csr(const DeviceCsr& A, const float* x, const float* b, float* y, int mode, cudaStream_t s,
-                long long& launches) {
+                long long& launches, int k = 1, size_t xs = 0, size_t bs = 0, size_t ys = 0) {
     if (A.rows == 0) return;
-    csr_kernel<<<(A.rows + kNT - 1) / kNT, kNT, 0, s>>>(A.rows, A.ptr, A.col, A.val, x, b, y, mode);
+    csr_kernel<<<dim3((A.rows + kNT - 1) / kNT, k), kNT, 0, s>>>(A.rows, A.ptr, A.col, A.val, x, b, y, mode, xs, bs,
+                                                                 ys);
     ck(cudaGetLastError(), "csr_kernel");
     ++launches;
 }
@@ -338,48 +344,69 @@ SigmaScratch SigmaGpu::primary() const {
         const SigmaLevel& L = lv[l];
         SigmaScratch::Level& S = sc.lv[l];
         S.u = L.u; S.r = L.r; S.b = L.b; S.tmp = L.tmp; S.vb = L.vb; S.vx = L.vx;
+        S.si = (size_t)std::max(L.n_iface, 1);
+        S.sn = (size_t)std::max(L.n_int, 1);
         S.aii = L.aii.primary();
         S.arr = L.arr_solve.primary();
     }
     sc.bottom = bottom.primary();
     sc.kb = kb;
     sc.kx = kx;
+    sc.kbs = (size_t)std::max(n_bottom_int + n_bottom, 1);
     sc.err = d_err;
+    sc.nrhs = 1;
     return sc;
 }
 
-void SigmaGpu::alloc_scratch(SigmaScratch& sc, cudaStream_t s) const {
+int SigmaGpu::max_rhs() const {
+    int k = 4;
+    for (const SigmaLevel& L : lv) {
+        if (L.aii.nsn > 0) k = std::min(k, L.aii.kmax);
+        if (L.arr_solve.nsn > 0) k = std::min(k, L.arr_solve.kmax);
+    }
+    if (bottom.nsn > 0) k = std::min(k, bottom.kmax);
+    return k;
+}
+
+void SigmaGpu::alloc_scratch(SigmaScratch& sc, cudaStream_t s, int nrhs) const {
     free_scratch(sc);
+    if (nrhs != 1 && nrhs != 2 && nrhs != 4) throw Error(HDD_ERR_INVALID_ARGUMENT, "systems per batch: 1, 2 or 4");
+    if (nrhs > max_rhs())
+        throw Error(HDD_ERR_UNSUPPORTED, "the interface solver's largest fronts leave no room for that many systems");
     size_t& b = sc.bytes;
+    sc.nrhs = nrhs;
     sc.err = dev::alloc_zero<int>(1, b, s);
     sc.lv.resize(lv.size());
     for (size_t l = 0; l < lv.size(); ++l) {
         const SigmaLevel& L = lv[l];
         SigmaScratch::Level& S = sc.lv[l];
-        S.u = dev::alloc_zero<float>(std::max(L.n_iface, 1), b, s);
-        S.r = dev::alloc_zero<float>(std::max(L.n_iface, 1), b, s);
-        S.b = dev::alloc_zero<float>(std::max(L.n_iface, 1), b, s);
-        S.tmp = dev::alloc_zero<float>(std::max(L.n_iface, 1), b, s);
-        S.vb = dev::alloc_zero<float>(std::max(L.n_int, 1), b, s);
-        S.vx = dev::alloc_zero<float>(std::max(L.n_int, 1), b, s);
-        if (L.aii.nsn > 0) L.aii.alloc_scratch(S.aii, sc.err, s, b);
-        if (L.arr_solve.nsn > 0) L.arr_solve.alloc_scratch(S.arr, sc.err, s, b);
+        S.si = (size_t)std::max(L.n_iface, 1);
+        S.sn = (size_t)std::max(L.n_int, 1);
+        S.u = dev::alloc_zero<float>(S.si * nrhs, b, s);
+        S.r = dev::alloc_zero<float>(S.si * nrhs, b, s);
+        S.b = dev::alloc_zero<float>(S.si * nrhs, b, s);
+        S.tmp = dev::alloc_zero<float>(S.si * nrhs, b, s);
+        S.vb = dev::alloc_zero<float>(S.sn * nrhs, b, s);
+        S.vx = dev::alloc_zero<float>(S.sn * nrhs, b, s);
+        if (L.aii.nsn > 0) L.aii.alloc_scratch(S.aii, sc.err, s, b, nrhs);
+        if (L.arr_solve.nsn > 0) L.arr_solve.alloc_scratch(S.arr, sc.err, s, b, nrhs);
     }
-    if (bottom.nsn > 0) bottom.alloc_scratch(sc.bottom, sc.err, s, b);
+    if (bottom.nsn > 0) bottom.alloc_scratch(sc.bottom, sc.err, s, b, nrhs);
+    sc.kbs = (size_t)std::max(n_bottom_int + n_bottom, 1);
     if (kb) {
-        sc.kb = dev::alloc_zero<float>(std::max(n_bottom_int + n_bottom, 1), b, s);
-        sc.kx = dev::alloc_zero<float>(std::max(n_bottom_int + n_bottom, 1), b, s);
+        sc.kb = dev::alloc_zero<float>(sc.kbs * nrhs, b, s);
+        sc.kx = dev::alloc_zero<float>(sc.kbs * nrhs, b, s);
     }
 }
 
-size_t SigmaGpu::scratch_bytes() const {
+size_t SigmaGpu::scratch_bytes(int nrhs) const {
     size_t t = 4;
     for (const SigmaLevel& L : lv) {
-        t += 16 * (size_t)std::max(L.n_iface, 1) + 8 * (size_t)std::max(L.n_int, 1);
-        t += L.aii.scratch_bytes() + L.arr_solve.scratch_bytes();
+        t += nrhs * (16 * (size_t)std::max(L.n_iface, 1) + 8 * (size_t)std::max(L.n_int, 1));
+        t += L.aii.scratch_bytes(nrhs) + L.arr_solve.scratch_bytes(nrhs);
     }
-    t += bottom.scratch_bytes();
-    if (kb) t += 8 * (size_t)std::max(n_bottom_int + n_bottom, 1);
+    t += bottom.scratch_bytes(nrhs);
+    if (kb) t += 8 * (size_t)std::max(n_bottom_int + n_bottom, 1) * nrhs;
     return t;
 }
 
@@ -401,45 +428,52 @@ void SigmaGpu::free_scratch(SigmaScratch& sc) {
 void SigmaGpu::vcycle(cudaStream_t s, long long& launches, PhaseHook* hook) { vcycle(primary(), s, launches, hook); }
 
 void SigmaGpu::vcycle(const SigmaScratch& sc, cudaStream_t s, long long& launches, PhaseHook* hook) {
+    const int k = sc.nrhs;
     auto schur_apply = [&](int l, const float* u, float* out_tmp) {
         const SigmaLevel& L = lv[l];
         const SigmaScratch::Level& S = sc.lv[l];
-        launch_csr(L.air, u, nullptr, S.vb, 0, s, launches);
-        L.aii.solve(S.aii, S.vb, S.vx, s, launches, hook);
-        launch_csr(L.airT, S.vx, S.b, out_tmp, 1, s, launches);  // tmp = b + Air^T vx
+        launch_csr(L.air, u, nullptr, S.vb, 0, s, launches, k, S.si, 0, S.sn);
+        L.aii.solve(S.aii, S.vb, S.vx, s, launches, hook, k, (long long)S.sn, (long long)S.sn);
+        launch_csr(L.airT, S.vx, S.b, out_tmp, 1, s, launches, k, S.sn, S.si, S.si);  // tmp = b + Air^T vx
     };
     auto smooth = [&](int l) {
         const SigmaScratch::Level& S = sc.lv[l];
         schur_apply(l, S.u, S.tmp);
-        lv[l].arr_solve.solve(S.arr, S.tmp, S.u, s, launches, hook);
+        lv[l].arr_solve.solve(S.arr, S.tmp, S.u, s, launches, hook, k, (long long)S.si, (long long)S.si);
     };
     for (int l = 0; l + 1 < M; ++l) {
         const SigmaLevel& L = lv[l];
         const SigmaScratch::Level& S = sc.lv[l];
+        const SigmaScratch::Level& N = sc.lv[l + 1];
         for (int i = 0; i < smoothing; ++i) smooth(l);
         schur_apply(l, S.u, S.tmp);
-        launch_csr(L.arr, S.u, S.tmp, S.r, 2, s, launches);                 // r = tmp - Arr u
-        launch_fill(sc.lv[l + 1].u, lv[l + 1].n_iface, 0.0f, s, launches);
-        launch_csr(L.prrT, S.r, nullptr, sc.lv[l + 1].b, 0, s, launches);  // b_{l+1} = Prr^T r
+        launch_csr(L.arr, S.u, S.tmp, S.r, 2, s, launches, k, S.si, S.si, S.si);  // r = tmp - Arr u
+        launch_fill(N.u, N.si * k, 0.0f, s, launches);
+        launch_csr(L.prrT, S.r, nullptr, N.b, 0, s, launches, k, S.si, 0, N.si);  // b_{l+1} = Prr^T r
     }
     if (!bottom_exact) {
         for (int i = 0; i < kBottomSmoothing; ++i) smooth(M - 1);
     } else {
         const SigmaScratch::Level& B = sc.lv[M - 1];
         if (n_bottom > 0) {
-            // Right-hand side [0; b], solution's interface block -> u.
-            if (n_bottom_int > 0) ck(cudaMemsetAsync(sc.kb, 0, sizeof(float) * n_bottom_int, s), "memset kb");
-            ck(cudaMemcpyAsync(sc.kb + n_bottom_int, B.b, sizeof(float) * n_bottom, cudaMemcpyDeviceToDevice, s),
+            // Right-hand sides [0; b], solutions' interface blocks -> u.
+            const size_t p = sc.kbs * sizeof(float);
+            if (n_bottom_int > 0)
+                ck(cudaMemset2DAsync(sc.kb, p, 0, sizeof(float) * n_bottom_int, k, s), "memset kb");
+            ck(cudaMemcpy2DAsync(sc.kb + n_bottom_int, p, B.b, B.si * sizeof(float), sizeof(float) * n_bottom, k,
+                                 cudaMemcpyDeviceToDevice, s),
                "copy b");
-            bottom.solve(sc.bottom, sc.kb, sc.kx, s, launches, hook);
-            ck(cudaMemcpyAsync(B.u, sc.kx + n_bottom_int, sizeof(float) * n_bottom, cudaMemcpyDeviceToDevice, s),
+            bottom.solve(sc.bottom, sc.kb, sc.kx, s, launches, hook, k, (long long)sc.kbs, (long long)sc.kbs);
+            ck(cudaMemcpy2DAsync(B.u, B.si * sizeof(float), sc.kx + n_bottom_int, p, sizeof(float) * n_bottom, k,
+                                 cudaMemcpyDeviceToDevice, s),
                "copy u");
         }
     }
     for (int l = M - 2; l >= 0; --l) {
         const SigmaLevel& L = lv[l];
         const SigmaScratch::Level& S = sc.lv[l];
-        launch_csr(L.prr, sc.lv[l + 1].u, nullptr, S.u, 3, s, launches);  // u += Prr u_{l+1}
+        const SigmaScratch::Level& N = sc.lv[l + 1];
+        launch_csr(L.prr, N.u, nullptr, S.u, 3, s, launches, k, N.si, 0, S.si);  // u += Prr u_{l+1}
         for (int i = 0; i < smoothing; ++i) smooth(l);
     }
 }

@@ -162,6 +162,7 @@ struct PlanScratch {
     // leaving room on the device for concurrent solves; the results do not
     // depend on it.
     int grid_div = 1;
+    int nrhs = 1;  // right-hand sides the buffers hold (1, 2 or 4)
 };
 
 // Device plan for a batch of independent supernodal triangular solves.
@@ -171,7 +172,9 @@ struct SolvePlan {
     int max_front = 0;
     int n_fwd = 0, n_bwd = 0;        // task counts
     int n_ctr = 0;                   // ints in the counter block
-    int grid = 0;                    // persistent CTAs per launch
+    int grid = 0;                    // persistent CTAs per launch (one right-hand side)
+    int grids[3] = {0, 0, 0};        // ... for 1, 2 and 4 right-hand sides (0: shared memory too small)
+    int kmax = 1;                    // most right-hand sides one launch takes
     int ntasks_f = 0, ntasks_b = 0;  // tasks, forward / backward
     double fwd_bytes = 0, bwd_bytes = 0;  // algorithmic bytes of one forward / backward launch
     int *d_col0 = nullptr, *d_ncol = nullptr, *d_nrow = nullptr, *d_parent = nullptr;
@@ -205,16 +208,25 @@ struct SolvePlan {
     // with the plan's own scratch or a context's.
     void solve(const float* b_old, float* x_old, cudaStream_t s, long long& launches,
                PhaseHook* hook = nullptr) const;
+    // With nrhs = 2 or 4 it solves that many systems at once: right-hand side
+    // j at b_old + j ld_b, solution at x_old + j ld_x, each coefficient read
+    // once for all of them; each solution is bit-identical to its solve alone.
     void solve(const PlanScratch& sc, const float* b_old, float* x_old, cudaStream_t s, long long& launches,
-               PhaseHook* hook = nullptr) const;
-    // Scratch for another solve context (error word shared_err, or its own).
-    void alloc_scratch(PlanScratch& sc, int* shared_err, cudaStream_t s, size_t& bytes) const;
+               PhaseHook* hook = nullptr, int nrhs = 1, long long ld_b = 0, long long ld_x = 0) const;
+    // Scratch for another solve context (error word shared_err, or its own),
+    // for up to nrhs right-hand sides per solve.
+    void alloc_scratch(PlanScratch& sc, int* shared_err, cudaStream_t s, size_t& bytes, int nrhs = 1) const;
     static void free_scratch(PlanScratch& sc);
     PlanScratch primary() const;
     // Device bytes alloc_scratch takes (without a shared error word).
     size_t scratch_bytes() const {
         if (nsn == 0) return 0;
         return 8 * (size_t)(part_len + upd_len) + 16 * (size_t)std::max(n, 1) + 4 * (size_t)std::max(n_ctr, 1) + 4;
+    }
+    size_t scratch_bytes(int nrhs) const {
+        if (nsn == 0) return 0;
+        return nrhs * (8 * (size_t)(part_len + upd_len) + 16 * (size_t)std::max(n, 1)) +
+               4 * (size_t)std::max(n_ctr, 1) + 4;
     }
     int error_flag(cudaStream_t s) const;
     // Test seam: on = raise the forward task count that one front's parent
@@ -248,10 +260,15 @@ struct SigmaLevel {
 // the error word.  The solver's first solve context uses the SigmaGpu's own;
 // further contexts (concurrent solves of one resident domain) allocate theirs.
 struct SigmaScratch {
+    // Level vectors for nrhs systems: system j's interface vectors (u, r, b,
+    // tmp) at + j * si, its interior vectors (vb, vx) at + j * sn.
     struct Level {
         float *u = nullptr, *r = nullptr, *b = nullptr, *tmp = nullptr, *vb = nullptr, *vx = nullptr;
+        size_t si = 0, sn = 0;
         PlanScratch aii, arr;
     };
+    int nrhs = 1;
+    size_t kbs = 0;  // stride of the coarsest level's [0; b] / solution pair
     std::vector<Level> lv;
     PlanScratch bottom;
     void set_grid_div(int div) {
@@ -290,10 +307,15 @@ struct SigmaGpu {
     // u[0] = sigma V-cycle(b[0]) (SIGMA_MULTIGRID_SOLVER.cpp:35-47), u[0] starting at 0,
     // in the given scratch (default: the SigmaGpu's own).
     void vcycle(cudaStream_t s, long long& launches, PhaseHook* hook = nullptr);
+    // With sc.nrhs = 2 or 4 it runs that many V-cycles at once (each
+    // bit-identical to its V-cycle alone), every supernodal solve taking all
+    // right-hand sides in one launch pair.
     void vcycle(const SigmaScratch& sc, cudaStream_t s, long long& launches, PhaseHook* hook = nullptr);
     SigmaScratch primary() const;
-    void alloc_scratch(SigmaScratch& sc, cudaStream_t s) const;
-    size_t scratch_bytes() const;
+    void alloc_scratch(SigmaScratch& sc, cudaStream_t s, int nrhs = 1) const;
+    // Most right-hand sides every plan of this hierarchy takes in one launch.
+    int max_rhs() const;
+    size_t scratch_bytes(int nrhs = 1) const;
     static void free_scratch(SigmaScratch& sc);
     // Nonzero when a bounded wait inside a supernodal solve gave up.
     int error_flag(cudaStream_t s) const;

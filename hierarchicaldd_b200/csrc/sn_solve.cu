@@ -79,6 +79,9 @@ struct PlanView {
     int* ctr;
     int* err;
     long long spin_limit;  // polls (with ~128 ns sleeps) before a wait gives up
+    // Right-hand side j (of K solved together) uses part + j ld_part,
+    // upd + j ld_upd, ynew / xnew + j ld_n, b_old + j ld_b, x_old + j ld_x.
+    long long ld_part, ld_upd, ld_n, ld_b, ld_x;
 };
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
@@ -113,26 +116,40 @@ __device__ __forceinline__ void fma4(double (&acc)[4], const float4 v, double x)
 // columns starting on 16-byte boundaries, so four consecutive rows of a column
 // are one 16-byte load.  Entries above the diagonal of L_JJ^{-1} and the
 // padding rows m .. round4(m) are stored zeros: a load may cover them.
+//
+// K right-hand sides are solved together: each coefficient load feeds K
+// products.  A front's vectors in shared memory hold entry i of right-hand
+// side j at i * K + j.  Every right-hand side's arithmetic (which products,
+// summed in which order) is the same for every K, so a solve's result does not
+// depend on what it was batched with.
 
 // Forward solve of one small front by one warp: the lane owns the row quads
 // 4 * (lane + 32 q), q < MQ.
-template <int MQ>
+template <int MQ, int K>
 __device__ __forceinline__ void warp_forward_rows(const PlanView& P, int J, int m, int nj, const double* f, int lane) {
     const size_t ld = (size_t)((m + 3) & ~3);
     const float* A = P.fw + P.fw_off[J];
-    double acc[MQ][4];
+    double acc[MQ][K][4];
 #pragma unroll
     for (int q = 0; q < MQ; ++q)
 #pragma unroll
-        for (int e = 0; e < 4; ++e) acc[q][e] = 0.0;
+        for (int j = 0; j < K; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[q][j][e] = 0.0;
 #pragma unroll 4
     for (int c = 0; c < nj; ++c) {
-        const double fc = f[c];
+        double fc[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) fc[j] = f[(size_t)c * K + j];
         const float* col = A + (size_t)c * ld;
 #pragma unroll
         for (int q = 0; q < MQ; ++q) {
             const int r = 4 * (lane + 32 * q);
-            if (r < m && r + 3 >= c) fma4(acc[q], ldg4(col + r), fc);
+            if (r < m && r + 3 >= c) {
+                const float4 v = ldg4(col + r);
+#pragma unroll
+                for (int j = 0; j < K; ++j) fma4(acc[q][j], v, fc[j]);
+            }
         }
     }
     const int c0 = P.col0[J];
@@ -143,15 +160,23 @@ __device__ __forceinline__ void warp_forward_rows(const PlanView& P, int J, int 
         for (int e = 0; e < 4; ++e) {
             const int r = 4 * (lane + 32 * q) + e;
             if (r >= m) continue;
-            if (r < nj) P.ynew[c0 + r] = acc[q][e];
-            else P.upd[uo + (r - nj)] = f[r] + acc[q][e];
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                if (r < nj) P.ynew[j * P.ld_n + c0 + r] = acc[q][j][e];
+                else P.upd[j * P.ld_upd + uo + (r - nj)] = f[(size_t)r * K + j] + acc[q][j][e];
+            }
         }
 }
 
+template <int K>
 __device__ void warp_forward(const PlanView& P, int J, double* f, int lane, const float* b_old, int* done) {
     const int nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
     const int cb = P.child_ptr[J], ce = P.child_ptr[J + 1];
-    for (int i = lane; i < m; i += 32) f[i] = (i < nj) ? (double)b_old[P.perm[c0 + i]] : 0.0;
+    for (int i = lane; i < m; i += 32) {
+        const int po = i < nj ? P.perm[c0 + i] : 0;
+#pragma unroll
+        for (int j = 0; j < K; ++j) f[(size_t)i * K + j] = (i < nj) ? (double)b_old[j * P.ld_b + po] : 0.0;
+    }
     if (lane == 0) {
         bool ok = true;
         for (int c = cb; c < ce; ++c) ok &= wait_at_least(done + P.child[c], P.ntf[P.child[c]], P.err, P.spin_limit);
@@ -163,11 +188,15 @@ __device__ void warp_forward(const PlanView& P, int J, double* f, int lane, cons
         const int mc = P.nrow[C];
         const double* uc = P.upd + P.upd_off[C];
         const int* rm = P.relmap + P.relmap_off[C];
-        for (int k = lane; k < mc; k += 32) f[rm[k]] += __ldcg(uc + k);
+        for (int k = lane; k < mc; k += 32) {
+            const int t = rm[k];
+#pragma unroll
+            for (int j = 0; j < K; ++j) f[(size_t)t * K + j] += __ldcg(uc + j * P.ld_upd + k);
+        }
         __syncwarp();
     }
-    if (m <= 128) warp_forward_rows<1>(P, J, m, nj, f, lane);
-    else warp_forward_rows<2>(P, J, m, nj, f, lane);
+    if (m <= 128) warp_forward_rows<1, K>(P, J, m, nj, f, lane);
+    else warp_forward_rows<2, K>(P, J, m, nj, f, lane);
     __threadfence();
     __syncwarp();
     if (lane == 0) atomicAdd(done + J, 1);
@@ -175,46 +204,72 @@ __device__ void warp_forward(const PlanView& P, int J, double* f, int lane, cons
 
 // Backward solve of one small front by one warp: x_a = sum_{r >= a} Fw(r, a) g_r,
 // four columns at a time, the lane summing the row quads a + 4 lane + 128 k.
+template <int K>
 __device__ void warp_backward(const PlanView& P, int J, double* g, int lane, float* x_old, int* done) {
     const int nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
     const int m4 = (m + 3) & ~3;
     const int* rows = P.rows + P.rows_off[J];
-    for (int i = lane; i < nj; i += 32) g[i] = P.ynew[c0 + i];   // from the forward launch
-    for (int i = m + lane; i < m4; i += 32) g[i] = 0.0;          // padding rows
+    for (int i = lane; i < nj; i += 32)  // from the forward launch
+#pragma unroll
+        for (int j = 0; j < K; ++j) g[(size_t)i * K + j] = P.ynew[j * P.ld_n + c0 + i];
+    for (int i = m + lane; i < m4; i += 32)  // padding rows
+#pragma unroll
+        for (int j = 0; j < K; ++j) g[(size_t)i * K + j] = 0.0;
     if (lane == 0) {
         const int p = P.parent[J];
         if (p >= 0 && !wait_at_least(done + p, P.ntb[p], P.err, P.spin_limit)) atomicExch(P.err, 1);
     }
     __syncwarp();
-    for (int i = nj + lane; i < m; i += 32) g[i] = __ldcg(P.xnew + rows[i - nj]);
+    for (int i = nj + lane; i < m; i += 32) {
+        const int t = rows[i - nj];
+#pragma unroll
+        for (int j = 0; j < K; ++j) g[(size_t)i * K + j] = __ldcg(P.xnew + j * P.ld_n + t);
+    }
     __syncwarp();
     const size_t ld = (size_t)m4;
     const float* A = P.fw + P.fw_off[J];
     for (int a = 0; a < nj; a += 4) {
-        double s4[4] = {0.0, 0.0, 0.0, 0.0};
+        double s4[K][4];
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) s4[j][jj] = 0.0;
 #pragma unroll 2
         for (int r = a + 4 * lane; r < m; r += 128) {
-            const double g0 = g[r], g1 = g[r + 1], g2 = g[r + 2], g3 = g[r + 3];
+            double gg[K][4];
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if (a + j < nj) {
-                    const float4 v = ldg4(A + (size_t)(a + j) * ld + r);
-                    s4[j] = fma((double)v.x, g0, s4[j]);
-                    s4[j] = fma((double)v.y, g1, s4[j]);
-                    s4[j] = fma((double)v.z, g2, s4[j]);
-                    s4[j] = fma((double)v.w, g3, s4[j]);
+            for (int j = 0; j < K; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) gg[j][e] = g[(size_t)(r + e) * K + j];
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj)
+                if (a + jj < nj) {
+                    const float4 v = ldg4(A + (size_t)(a + jj) * ld + r);
+#pragma unroll
+                    for (int j = 0; j < K; ++j) {
+                        s4[j][jj] = fma((double)v.x, gg[j][0], s4[j][jj]);
+                        s4[j][jj] = fma((double)v.y, gg[j][1], s4[j][jj]);
+                        s4[j][jj] = fma((double)v.z, gg[j][2], s4[j][jj]);
+                        s4[j][jj] = fma((double)v.w, gg[j][3], s4[j][jj]);
+                    }
                 }
         }
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < K; ++j)
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s4[j] += __shfl_xor_sync(0xffffffffu, s4[j], o);
+            for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) s4[j][jj] += __shfl_xor_sync(0xffffffffu, s4[j][jj], o);
         if (lane == 0) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if (a + j < nj) {
-                    P.xnew[c0 + a + j] = s4[j];
-                    x_old[P.perm[c0 + a + j]] = (float)s4[j];
+            for (int jj = 0; jj < 4; ++jj)
+                if (a + jj < nj) {
+                    const int po = P.perm[c0 + a + jj];
+#pragma unroll
+                    for (int j = 0; j < K; ++j) {
+                        P.xnew[j * P.ld_n + c0 + a + jj] = s4[j][jj];
+                        x_old[j * P.ld_x + po] = (float)s4[j][jj];
+                    }
                 }
         }
     }
@@ -223,11 +278,12 @@ __device__ void warp_backward(const PlanView& P, int J, double* g, int lane, flo
     if (lane == 0) atomicAdd(done + J, 1);
 }
 
-__global__ void __launch_bounds__(kNT, 5) sn_forward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks,
-                                                         const float* __restrict__ b_old) {
+template <int K>
+__global__ void __launch_bounds__(kNT, K == 1 ? 5 : (K == 2 ? 3 : 2))
+    sn_forward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks, const float* __restrict__ b_old) {
     extern __shared__ double sh[];
-    double* f = sh;                // the front's input vector, m entries
-    double* red = sh + P.max_m;    // column-slice partial sums, 4 kNT entries
+    double* f = sh;                    // the front's input vectors, m x K entries
+    double* red = sh + P.max_m * K;    // column-slice partial sums, 4 K kNT entries
     __shared__ int s_ticket, s_last;
     int* done = P.ctr + 2;
     int* chunk_ctr = P.ctr + 2 + 2 * P.nsn;
@@ -240,7 +296,7 @@ __global__ void __launch_bounds__(kNT, 5) sn_forward_kernel(PlanView P, const Sn
         const SnTask T = tasks[t];
         if (T.front < 0) {
             const int w = tid >> 5;
-            if (w < T.rows) warp_forward(P, P.bfwd[T.r0 + w], sh + w * kSmallM, tid & 31, b_old, done);
+            if (w < T.rows) warp_forward<K>(P, P.bfwd[T.r0 + w], sh + (size_t)w * kSmallM * K, tid & 31, b_old, done);
             __syncthreads();
             continue;
         }
@@ -269,8 +325,12 @@ __global__ void __launch_bounds__(kNT, 5) sn_forward_kernel(PlanView P, const Sn
 #pragma unroll
         for (int u = 0; u < 4; ++u)
             v0[u] = (cbeg + u < cend) ? ldg4(A + (size_t)(cbeg + u) * ld) : make_float4(0.f, 0.f, 0.f, 0.f);
-        // b's part of the input vector does not depend on other fronts.
-        for (int i = tid; i < m; i += kNT) f[i] = (i < nj) ? (double)b_old[P.perm[c0 + i]] : 0.0;
+        // b's part of the input vectors does not depend on other fronts.
+        for (int i = tid; i < m; i += kNT) {
+            const int po = i < nj ? P.perm[c0 + i] : 0;
+#pragma unroll
+            for (int j = 0; j < K; ++j) f[(size_t)i * K + j] = (i < nj) ? (double)b_old[j * P.ld_b + po] : 0.0;
+        }
         if (tid == 0) {
             bool ok = true;
             for (int c = cb; c < ce; ++c) ok &= wait_at_least(done + P.child[c], P.ntf[P.child[c]], P.err, P.spin_limit);
@@ -282,34 +342,54 @@ __global__ void __launch_bounds__(kNT, 5) sn_forward_kernel(PlanView P, const Sn
             const int mc = P.nrow[C];
             const double* uc = P.upd + P.upd_off[C];
             const int* rm = P.relmap + P.relmap_off[C];
-            for (int k = tid; k < mc; k += kNT) f[rm[k]] += __ldcg(uc + k);
+            for (int k = tid; k < mc; k += kNT) {
+                const int tr = rm[k];
+#pragma unroll
+                for (int j = 0; j < K; ++j) f[(size_t)tr * K + j] += __ldcg(uc + j * P.ld_upd + k);
+            }
             __syncthreads();
         }
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        double acc[K][4];
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[j][e] = 0.0;
         if (active) {
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (cbeg + u < cend) fma4(acc, v0[u], f[cbeg + u]);
+                if (cbeg + u < cend)
+#pragma unroll
+                    for (int j = 0; j < K; ++j) fma4(acc[j], v0[u], f[(size_t)(cbeg + u) * K + j]);
             int c = cbeg + 4;
             for (; c + 4 <= cend; c += 4) {
 #pragma unroll
                 for (int u = 0; u < 4; ++u) v0[u] = ldg4(A + (size_t)(c + u) * ld);
 #pragma unroll
-                for (int u = 0; u < 4; ++u) fma4(acc, v0[u], f[c + u]);
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int j = 0; j < K; ++j) fma4(acc[j], v0[u], f[(size_t)(c + u) * K + j]);
             }
-            for (; c < cend; ++c) fma4(acc, ldg4(A + (size_t)c * ld), f[c]);
+            for (; c < cend; ++c) {
+                const float4 v = ldg4(A + (size_t)c * ld);
+#pragma unroll
+                for (int j = 0; j < K; ++j) fma4(acc[j], v, f[(size_t)c * K + j]);
+            }
         }
         if (ks > 1) {
 #pragma unroll
-            for (int e = 0; e < 4; ++e) red[(size_t)e * kNT + tid] = acc[e];
+            for (int j = 0; j < K; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) red[(size_t)(j * 4 + e) * kNT + tid] = acc[j][e];
             __syncthreads();
             if (sl == 0 && active) {
 #pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    double s2 = red[(size_t)e * kNT + lq];
-                    for (int q = 1; q < ks; ++q) s2 += red[(size_t)e * kNT + q * mq + lq];
-                    acc[e] = s2;
-                }
+                for (int j = 0; j < K; ++j)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        double s2 = red[(size_t)(j * 4 + e) * kNT + lq];
+                        for (int q = 1; q < ks; ++q) s2 += red[(size_t)(j * 4 + e) * kNT + q * mq + lq];
+                        acc[j][e] = s2;
+                    }
             }
         }
         const bool mine = sl == 0 && active;
@@ -320,15 +400,21 @@ __global__ void __launch_bounds__(kNT, 5) sn_forward_kernel(PlanView P, const Sn
                 for (int e = 0; e < 4; ++e) {
                     const int r = row + e;
                     if (r >= rend) break;
-                    if (r < nj) P.ynew[c0 + r] = acc[e];
-                    else P.upd[P.upd_off[J] + (r - nj)] = f[r] + acc[e];
+#pragma unroll
+                    for (int j = 0; j < K; ++j) {
+                        if (r < nj) P.ynew[j * P.ld_n + c0 + r] = acc[j][e];
+                        else P.upd[j * P.ld_upd + P.upd_off[J] + (r - nj)] = f[(size_t)r * K + j] + acc[j][e];
+                    }
                 }
             }
         } else {
             if (mine) {
-                double* pp = P.part + T.part + (size_t)T.k * kRB + 4 * lq;
 #pragma unroll
-                for (int e = 0; e < 4; ++e) pp[e] = acc[e];
+                for (int j = 0; j < K; ++j) {
+                    double* pp = P.part + j * P.ld_part + T.part + (size_t)T.k * kRB + 4 * lq;
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) pp[e] = acc[j][e];
+                }
             }
             __threadfence();
             __syncthreads();
@@ -341,10 +427,14 @@ __global__ void __launch_bounds__(kNT, 5) sn_forward_kernel(PlanView P, const Sn
                     for (int e = 0; e < 4; ++e) {
                         const int r = row + e;
                         if (r >= rend) break;
-                        double s2 = 0.0;
-                        for (int k = 0; k < T.nk; ++k) s2 += __ldcg(P.part + T.part + (size_t)k * kRB + 4 * lq + e);
-                        if (r < nj) P.ynew[c0 + r] = s2;
-                        else P.upd[P.upd_off[J] + (r - nj)] = f[r] + s2;
+#pragma unroll
+                        for (int j = 0; j < K; ++j) {
+                            const double* pj = P.part + j * P.ld_part + T.part + 4 * lq + e;
+                            double s2 = 0.0;
+                            for (int k = 0; k < T.nk; ++k) s2 += __ldcg(pj + (size_t)k * kRB);
+                            if (r < nj) P.ynew[j * P.ld_n + c0 + r] = s2;
+                            else P.upd[j * P.ld_upd + P.upd_off[J] + (r - nj)] = f[(size_t)r * K + j] + s2;
+                        }
                     }
                 }
             }
@@ -355,9 +445,10 @@ __global__ void __launch_bounds__(kNT, 5) sn_forward_kernel(PlanView P, const Sn
     }
 }
 
-__global__ void __launch_bounds__(kNT, 5) sn_backward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks,
-                                                          float* __restrict__ x_old) {
-    extern __shared__ double g[];  // [y_J; x_R], m entries (+ zero padding to round4(m))
+template <int K>
+__global__ void __launch_bounds__(kNT, K == 1 ? 5 : (K == 2 ? 3 : 2))
+    sn_backward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks, float* __restrict__ x_old) {
+    extern __shared__ double g[];  // [y_J; x_R] x K, m4 x K entries (zero padding rows)
     __shared__ int s_ticket;
     int* done = P.ctr + 2 + P.nsn;
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
@@ -368,7 +459,7 @@ __global__ void __launch_bounds__(kNT, 5) sn_backward_kernel(PlanView P, const S
         if (t >= ntasks) break;
         const SnTask T = tasks[t];
         if (T.front < 0) {
-            if (w < T.rows) warp_backward(P, P.bbwd[T.r0 + w], g + w * kSmallM, lane, x_old, done);
+            if (w < T.rows) warp_backward<K>(P, P.bbwd[T.r0 + w], g + (size_t)w * kSmallM * K, lane, x_old, done);
             __syncthreads();
             continue;
         }
@@ -379,26 +470,41 @@ __global__ void __launch_bounds__(kNT, 5) sn_backward_kernel(PlanView P, const S
         const int* rows = P.rows + P.rows_off[J];
         const size_t ld = (size_t)m4;
         const float* A = P.fw + P.fw_off[J];
-        double s4[4] = {0.0, 0.0, 0.0, 0.0};
+        double s4[K][4];
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) s4[j][jj] = 0.0;
         const int amin = a0 + w;
         // Row quads wholly below nj (the L_JJ^{-T} y part) need only this
         // front's forward result, so they are summed before waiting on the
         // parent; each lane adds its quads in ascending order.
-        for (int i = rs + tid; i < nj; i += kNT) g[i] = P.ynew[c0 + i];   // from the forward launch
-        for (int i = m + tid; i < m4; i += kNT) g[i] = 0.0;               // padding rows
+        for (int i = rs + tid; i < nj; i += kNT)  // from the forward launch
+#pragma unroll
+            for (int j = 0; j < K; ++j) g[(size_t)i * K + j] = P.ynew[j * P.ld_n + c0 + i];
+        for (int i = m + tid; i < m4; i += kNT)  // padding rows
+#pragma unroll
+            for (int j = 0; j < K; ++j) g[(size_t)i * K + j] = 0.0;
         __syncthreads();
         int r = rs + 4 * lane;
         auto quad = [&](int rr) {
-            const double g0 = g[rr], g1 = g[rr + 1], g2 = g[rr + 2], g3 = g[rr + 3];
+            double gg[K][4];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int a = amin + 8 * j;
+            for (int j = 0; j < K; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) gg[j][e] = g[(size_t)(rr + e) * K + j];
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) {
+                const int a = amin + 8 * jj;
                 if (a < a0 + na) {
                     const float4 v = ldg4(A + (size_t)a * ld + rr);
-                    s4[j] = fma((double)v.x, g0, s4[j]);
-                    s4[j] = fma((double)v.y, g1, s4[j]);
-                    s4[j] = fma((double)v.z, g2, s4[j]);
-                    s4[j] = fma((double)v.w, g3, s4[j]);
+#pragma unroll
+                    for (int j = 0; j < K; ++j) {
+                        s4[j][jj] = fma((double)v.x, gg[j][0], s4[j][jj]);
+                        s4[j][jj] = fma((double)v.y, gg[j][1], s4[j][jj]);
+                        s4[j][jj] = fma((double)v.z, gg[j][2], s4[j][jj]);
+                        s4[j][jj] = fma((double)v.w, gg[j][3], s4[j][jj]);
+                    }
                 }
             }
         };
@@ -411,23 +517,33 @@ __global__ void __launch_bounds__(kNT, 5) sn_backward_kernel(PlanView P, const S
             if (p >= 0 && !wait_at_least(done + p, P.ntb[p], P.err, P.spin_limit)) atomicExch(P.err, 1);
         }
         __syncthreads();
-        for (int i = max(rs, nj) + tid; i < m; i += kNT) g[i] = __ldcg(P.xnew + rows[i - nj]);
+        for (int i = max(rs, nj) + tid; i < m; i += kNT) {
+            const int tr = rows[i - nj];
+#pragma unroll
+            for (int j = 0; j < K; ++j) g[(size_t)i * K + j] = __ldcg(P.xnew + j * P.ld_n + tr);
+        }
         __syncthreads();
         if (amin < a0 + na) {
 #pragma unroll 2
             for (; r < m; r += 128) quad(r);
         }
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < K; ++j)
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s4[j] += __shfl_xor_sync(0xffffffffu, s4[j], o);
+            for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) s4[j][jj] += __shfl_xor_sync(0xffffffffu, s4[j][jj], o);
         if (lane == 0) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int a = amin + 8 * j;
+            for (int jj = 0; jj < 4; ++jj) {
+                const int a = amin + 8 * jj;
                 if (a < a0 + na) {
-                    P.xnew[c0 + a] = s4[j];
-                    x_old[P.perm[c0 + a]] = (float)s4[j];
+                    const int po = P.perm[c0 + a];
+#pragma unroll
+                    for (int j = 0; j < K; ++j) {
+                        P.xnew[j * P.ld_n + c0 + a] = s4[j][jj];
+                        x_old[j * P.ld_x + po] = (float)s4[j][jj];
+                    }
                 }
             }
         }
@@ -437,21 +553,46 @@ __global__ void __launch_bounds__(kNT, 5) sn_backward_kernel(PlanView P, const S
     }
 }
 
-size_t forward_smem(int max_m) { return (size_t)std::max(max_m + 4 * kNT, kWarps * kSmallM) * sizeof(double); }
-size_t backward_smem(int max_m) { return (size_t)std::max((max_m + 3) & ~3, kWarps * kSmallM) * sizeof(double); }
+size_t forward_smem(int max_m, int k) {
+    return (size_t)std::max((max_m + 4 * kNT) * k, kWarps * kSmallM * k) * sizeof(double);
+}
+size_t backward_smem(int max_m, int k) {
+    return (size_t)std::max(((max_m + 3) & ~3) * k, kWarps * kSmallM * k) * sizeof(double);
+}
 
-// The dynamic shared-memory limit of the two kernels only ever grows, so a
-// plan built later with smaller fronts cannot invalidate an earlier plan's
-// launches.
+// Right-hand-side counts a launch can take (template instances), and the
+// shared memory any of them may use.
+constexpr int kBatches[3] = {1, 2, 4};
+constexpr size_t kSmemMax = 227 * 1024;
+
+// The dynamic shared-memory limit of each kernel instance only ever grows,
+// so a plan built later with smaller fronts cannot invalidate an earlier
+// plan's launches.
 std::mutex g_smem_mu;
-int g_smem_limit[64] = {0};
-void raise_smem_limit(int device, int bytes) {
+int g_smem_limit[64][3] = {};
+template <int K>
+void raise_limit_k(int device, int bytes, int slot) {
+    if (bytes <= g_smem_limit[device][slot]) return;
+    dev::ck(cudaFuncSetAttribute(sn_forward_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+            "smem attr");
+    dev::ck(cudaFuncSetAttribute(sn_backward_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+            "smem attr");
+    g_smem_limit[device][slot] = bytes;
+}
+void raise_smem_limit(int device, int k, int bytes) {
     std::lock_guard<std::mutex> lock(g_smem_mu);
     if (device < 0 || device >= 64) throw Error(HDD_ERR_INVALID_ARGUMENT, "device ordinal out of range");
-    if (bytes <= g_smem_limit[device]) return;
-    dev::ck(cudaFuncSetAttribute(sn_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "smem attr");
-    dev::ck(cudaFuncSetAttribute(sn_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "smem attr");
-    g_smem_limit[device] = bytes;
+    if (k == 1) raise_limit_k<1>(device, bytes, 0);
+    else if (k == 2) raise_limit_k<2>(device, bytes, 1);
+    else raise_limit_k<4>(device, bytes, 2);
+}
+
+template <int K>
+int occupancy_k(size_t smf, size_t smb) {
+    int bf = 0, bb = 0;
+    dev::ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, sn_forward_kernel<K>, kNT, smf), "occupancy");
+    dev::ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, sn_backward_kernel<K>, kNT, smb), "occupancy");
+    return std::max(1, std::min(bf, bb));
 }
 
 }  // namespace
@@ -623,7 +764,7 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
             relmap.push_back(posn);
         }
     }
-    if (forward_smem(max_front) > 200 * 1024)
+    if (forward_smem(max_front, 1) > 200 * 1024)
         throw Error(HDD_ERR_UNSUPPORTED, "supernodal front too large for shared memory: " + std::to_string(max_front));
     bytes = 0;
     d_col0 = dev::upload(col0, s, bytes);
@@ -663,15 +804,23 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
         if (parent_g[g] >= 0) { stall_front = g; stall_ntf = ntf[g]; break; }
     ntasks_f = n_fwd;
     ntasks_b = n_bwd;
-    // Persistent grid: as many CTAs as fit on the device, but no more than tasks.
-    int dev_id = 0, nsm = 0, bf = 0, bb = 0;
+    // Persistent grid: as many CTAs as fit on the device, per right-hand-side
+    // count whose shared memory fits; no more than tasks at launch.
+    int dev_id = 0, nsm = 0;
     dev::ck(cudaGetDevice(&dev_id), "cudaGetDevice");
     dev::ck(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev_id), "SM count");
-    const size_t smf = forward_smem(max_front), smb = backward_smem(max_front);
-    raise_smem_limit(dev_id, (int)smf);
-    dev::ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, sn_forward_kernel, kNT, smf), "occupancy");
-    dev::ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, sn_backward_kernel, kNT, smb), "occupancy");
-    grid = std::max(1, nsm * std::max(1, std::min(bf, bb)));
+    kmax = 1;
+    for (int i = 0; i < 3; ++i) {
+        const int k = kBatches[i];
+        const size_t smf = forward_smem(max_front, k), smb = backward_smem(max_front, k);
+        grids[i] = 0;
+        if (std::max(smf, smb) > kSmemMax) break;
+        raise_smem_limit(dev_id, k, (int)std::max(smf, smb));
+        const int occ = k == 1 ? occupancy_k<1>(smf, smb) : (k == 2 ? occupancy_k<2>(smf, smb) : occupancy_k<4>(smf, smb));
+        grids[i] = std::max(1, nsm * occ);
+        kmax = k;
+    }
+    grid = grids[0];
     dev::ck(cudaStreamSynchronize(s), "plan upload");
 }
 
@@ -690,11 +839,13 @@ void SolvePlan::release() {
     n_fwd = n_bwd = n_ctr = 0;
 }
 
-void SolvePlan::alloc_scratch(PlanScratch& sc, int* shared_err, cudaStream_t s, size_t& b) const {
-    sc.part = dev::alloc_zero<double>(part_len, b, s);
-    sc.upd = dev::alloc_zero<double>(upd_len, b, s);
-    sc.ynew = dev::alloc_zero<double>(std::max(n, 1), b, s);
-    sc.xnew = dev::alloc_zero<double>(std::max(n, 1), b, s);
+void SolvePlan::alloc_scratch(PlanScratch& sc, int* shared_err, cudaStream_t s, size_t& b, int nrhs) const {
+    if (nrhs != 1 && nrhs != 2 && nrhs != 4) throw Error(HDD_ERR_INVALID_ARGUMENT, "right-hand sides per solve: 1, 2 or 4");
+    sc.nrhs = nrhs;
+    sc.part = dev::alloc_zero<double>(part_len * nrhs, b, s);
+    sc.upd = dev::alloc_zero<double>(upd_len * nrhs, b, s);
+    sc.ynew = dev::alloc_zero<double>((long long)std::max(n, 1) * nrhs, b, s);
+    sc.xnew = dev::alloc_zero<double>((long long)std::max(n, 1) * nrhs, b, s);
     sc.ctr = dev::alloc_zero<int>(std::max(n_ctr, 1), b, s);
     if (shared_err) {
         sc.err = shared_err;
@@ -716,6 +867,7 @@ PlanScratch SolvePlan::primary() const {
     PlanScratch sc;
     sc.part = d_part; sc.upd = d_upd; sc.ynew = d_ynew; sc.xnew = d_xnew; sc.ctr = d_ctr; sc.err = d_err;
     sc.own_err = false;
+    sc.nrhs = 1;
     return sc;
 }
 
@@ -723,22 +875,37 @@ void SolvePlan::solve(const float* b_old, float* x_old, cudaStream_t s, long lon
     solve(primary(), b_old, x_old, s, launches, hook);
 }
 
-void SolvePlan::solve(const PlanScratch& sc, const float* b_old, float* x_old, cudaStream_t s, long long& launches,
-                      PhaseHook* hook) const {
-    if (nsn == 0) return;
-    PlanView P{nsn, max_front, d_col0, d_ncol, d_nrow, d_parent, d_rows, d_rows_off, d_child_ptr, d_child,
-               d_relmap_off, d_relmap, d_upd_off, d_fw_off, d_ntf, d_ntb, d_perm, d_bfwd, d_bbwd, d_fw, sc.part, sc.upd,
-               sc.ynew, sc.xnew, sc.ctr, sc.err, spin_limit};
-    dev::ck(cudaMemsetAsync(sc.ctr, 0, sizeof(int) * n_ctr, s), "reset counters");
-    const int g = sc.grid_div > 1 ? std::max(1, (grid + sc.grid_div - 1) / sc.grid_div) : grid;
+template <int K>
+static void launch_pair(const PlanView& P, int g, int n_fwd, int n_bwd, int max_front, const SnTask* fwd,
+                        const SnTask* bwd, const float* b_old, float* x_old, cudaStream_t s, PhaseHook* hook,
+                        double fwd_bytes, double bwd_bytes) {
     if (hook) hook->begin(kPhaseSnForward);
-    sn_forward_kernel<<<std::min(g, n_fwd), kNT, forward_smem(max_front), s>>>(P, d_fwd, n_fwd, b_old);
+    sn_forward_kernel<K><<<std::min(g, n_fwd), kNT, forward_smem(max_front, K), s>>>(P, fwd, n_fwd, b_old);
     dev::ck(cudaGetLastError(), "sn forward");
     if (hook) hook->end(kPhaseSnForward, fwd_bytes);
     if (hook) hook->begin(kPhaseSnBackward);
-    sn_backward_kernel<<<std::min(g, n_bwd), kNT, backward_smem(max_front), s>>>(P, d_bwd, n_bwd, x_old);
+    sn_backward_kernel<K><<<std::min(g, n_bwd), kNT, backward_smem(max_front, K), s>>>(P, bwd, n_bwd, x_old);
     dev::ck(cudaGetLastError(), "sn backward");
     if (hook) hook->end(kPhaseSnBackward, bwd_bytes);
+}
+
+void SolvePlan::solve(const PlanScratch& sc, const float* b_old, float* x_old, cudaStream_t s, long long& launches,
+                      PhaseHook* hook, int nrhs, long long ld_b, long long ld_x) const {
+    if (nsn == 0) return;
+    if ((nrhs != 1 && nrhs != 2 && nrhs != 4) || nrhs > sc.nrhs || nrhs > kmax)
+        throw Error(HDD_ERR_INVALID_ARGUMENT, "right-hand sides per solve: 1, 2 or 4, within the scratch and the plan");
+    PlanView P{nsn, max_front, d_col0, d_ncol, d_nrow, d_parent, d_rows, d_rows_off, d_child_ptr, d_child,
+               d_relmap_off, d_relmap, d_upd_off, d_fw_off, d_ntf, d_ntb, d_perm, d_bfwd, d_bbwd, d_fw, sc.part, sc.upd,
+               sc.ynew, sc.xnew, sc.ctr, sc.err, spin_limit,
+               part_len, upd_len, (long long)std::max(n, 1), ld_b, ld_x};
+    dev::ck(cudaMemsetAsync(sc.ctr, 0, sizeof(int) * n_ctr, s), "reset counters");
+    const int slot = nrhs == 1 ? 0 : (nrhs == 2 ? 1 : 2);
+    const int full = grids[slot];
+    const int g = sc.grid_div > 1 ? std::max(1, (full + sc.grid_div - 1) / sc.grid_div) : full;
+    const double fb = fwd_bytes + 8.0 * n * (nrhs - 1), bb = bwd_bytes + 8.0 * n * (nrhs - 1);
+    if (nrhs == 1) launch_pair<1>(P, g, n_fwd, n_bwd, max_front, d_fwd, d_bwd, b_old, x_old, s, hook, fb, bb);
+    else if (nrhs == 2) launch_pair<2>(P, g, n_fwd, n_bwd, max_front, d_fwd, d_bwd, b_old, x_old, s, hook, fb, bb);
+    else launch_pair<4>(P, g, n_fwd, n_bwd, max_front, d_fwd, d_bwd, b_old, x_old, s, hook, fb, bb);
     launches += 2;
 }
 

@@ -243,27 +243,42 @@ void Solver::initialize() {
 }
 
 void Solver::alloc_vectors(Work& w) {
-    const size_t nt = L.tiles.size(), N = nt * (size_t)L.tile_cells;
+    const size_t nt = L.tiles.size(), N = std::max<size_t>(nt * (size_t)L.tile_cells, 1);
+    const size_t P = std::max<size_t>({nt, (size_t)laplace_partials(geom()), (size_t)1});
+    const size_t k = (size_t)w.k;
+    w.vstride = N;
+    w.pstride = (int)P;
     w.dense.alloc(std::max<size_t>(L.cell_count(), 1));
-    for (DevBuf<float>* v : {&w.x, &w.b, &w.r, &w.z, &w.s, &w.q}) { v->alloc(std::max<size_t>(N, 1)); v->zero(w.stream); }
-    if (opts.precision_mode == HDD_PRECISION_MIXED) w.xd.alloc(std::max<size_t>(N, 1));
+    for (DevBuf<float>* v : {&w.x, &w.b, &w.r, &w.z, &w.s, &w.q}) { v->alloc(N * k); v->zero(w.stream); }
+    if (opts.precision_mode == HDD_PRECISION_MIXED) w.xd.alloc(N * k);
     else w.xd.release();
-    w.partial.alloc(std::max<size_t>({nt, (size_t)laplace_partials(geom()), (size_t)1}));
-    w.partial_max.alloc(std::max<size_t>(nt, 1));
-    w.sums.alloc(8);
-    w.scalars_f.alloc(8);
-    w.scal.alloc(1);
+    w.partial.alloc(P * k);
+    w.partial_max.alloc(P * k);
+    w.sums.alloc(8 * k);
+    w.scalars_f.alloc(8 * k);
+    w.scal.alloc(k);
+    if (w.k > 1) {
+        for (DevBuf<int>* v : {&w.active, &w.first, &w.replace}) { v->alloc(k); v->zero(w.stream); }
+    }
 }
 
-std::unique_ptr<Work> Solver::make_work() {
+int Solver::max_batch() const {
+    if (!initialized) return 1;
+    return sigma.lv.empty() ? 4 : sigma.max_rhs();
+}
+
+std::unique_ptr<Work> Solver::make_work(int k) {
     if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+    if (k != 1 && k != 2 && k != 4) throw Error(HDD_ERR_INVALID_ARGUMENT, "systems per context: 1, 2 or 4");
+    if (k > max_batch()) throw Error(HDD_ERR_UNSUPPORTED, "the interface solver's fronts leave no room for that batch");
     std::unique_ptr<Work> w(new Work());
+    w->k = k;
     cuda_check(cudaSetDevice(opts.device), "cudaSetDevice");
     cuda_check(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     w->own_stream = true;
     alloc_vectors(*w);
     if (!sigma.lv.empty()) {
-        sigma.alloc_scratch(w->sig, w->stream);
+        sigma.alloc_scratch(w->sig, w->stream, k);
         w->sig.set_grid_div(std::max(1, opts.solve_share));
         w->own_sig = true;
     }
@@ -271,13 +286,13 @@ std::unique_ptr<Work> Solver::make_work() {
     return w;
 }
 
-size_t Solver::work_bytes() const {
+size_t Solver::work_bytes(int k) const {
     const size_t nt = L.tiles.size(), N = nt * (size_t)L.tile_cells;
-    size_t t = std::max<size_t>(L.cell_count(), 1) * 4 + 6 * std::max<size_t>(N, 1) * 4;
-    if (opts.precision_mode == HDD_PRECISION_MIXED) t += std::max<size_t>(N, 1) * 8;
-    t += std::max<size_t>({nt, (size_t)laplace_partials(geom()), (size_t)1}) * 8 + std::max<size_t>(nt, 1) * 4 + 128 +
-         sizeof(PcgScalars);
-    return t + sigma.scratch_bytes();
+    const size_t P = std::max<size_t>({nt, (size_t)laplace_partials(geom()), (size_t)1});
+    size_t t = std::max<size_t>(L.cell_count(), 1) * 4 + 6 * std::max<size_t>(N, 1) * 4 * k;
+    if (opts.precision_mode == HDD_PRECISION_MIXED) t += std::max<size_t>(N, 1) * 8 * k;
+    t += (P * 12 + 128 + sizeof(PcgScalars) + 12) * k;
+    return t + sigma.scratch_bytes(k);
 }
 
 void Solver::set_rhs(Work& w, const float* rhs) {
@@ -312,6 +327,9 @@ VcycleArgs Solver::vcycle_args(float* u, const float* bb, int halo_from_u, int z
     a.halo_from_u = halo_from_u;
     a.zero_init = zero_init;
     a.cluster = 1;
+    a.nslots = 1;
+    a.slot_stride = 0;
+    a.active = nullptr;
     if (const char* e = std::getenv("HDD_VCYCLE_CLUSTER")) a.cluster = std::atoi(e);
     // Correction weights omega/face_count with omega = (float)(2/3)
     // (SPGrid_Correction_Legacy.h:35,76), divided in float on the host.
@@ -333,6 +351,11 @@ VcycleArgs Solver::vcycle_args(float* u, const float* bb, int halo_from_u, int z
 
 void Solver::run_vcycle(Work& w, float* u, const float* bb, int halo_from_u, int zero_init, int nv) {
     VcycleArgs a = vcycle_args(u, bb, halo_from_u, zero_init, nv);
+    if (w.k > 1) {
+        a.nslots = w.k;
+        a.slot_stride = w.vstride;
+        a.active = w.active.p;
+    }
     Tm tm(this, w, 0, vcycle_bytes);
     cuda_check(launch_vcycle(a, w.stream), "vcycle kernel");
     count(w);
@@ -393,19 +416,23 @@ void Solver::apply_preconditioner_launches(Work& w, const float* rr, float* zz) 
     const int n_if = ih.n_iface.empty() ? 0 : ih.n_iface[0];
     {
         Tm tm(this, w, 3);
-        cuda_check(launch_interface_gather(g, iface_slot.p, iface_nb.p, n_if, rr, zz, w.sig.b0(), w.stream), "gather");
+        const size_t is = w.sig.lv.empty() ? 0 : w.sig.lv[0].si;
+        cuda_check(launch_interface_gather(g, iface_slot.p, iface_nb.p, n_if, rr, zz, w.sig.b0(), w.stream, w.batch(),
+                                           is),
+                   "gather");
         count(w);
     }
     if (n_if > 0) {
         // u_G = 0 then sigma_mg V-cycles (Preconditioner.h:105,110-117).
         NvtxRange sigma_range("Sigma_V_Cycle");
         Tm tm(this, w, 4);
-        cuda_check(cudaMemsetAsync(w.sig.u0(), 0, sizeof(float) * n_if, w.stream), "memset u0");
+        cuda_check(cudaMemsetAsync(w.sig.u0(), 0, sizeof(float) * w.sig.lv[0].si * w.k, w.stream), "memset u0");
         for (int i = 0; i < opts.sigma_mg; ++i) sigma.vcycle(w.sig, w.stream, w.launches, &w == &w0 ? &hook : nullptr);
     }
     {
         Tm tm(this, w, 3);
-        cuda_check(launch_interface_scatter(iface_slot.p, n_if, w.sig.u0(), zz, w.stream), "scatter");
+        const size_t is = w.sig.lv.empty() ? 0 : w.sig.lv[0].si;
+        cuda_check(launch_interface_scatter(iface_slot.p, n_if, w.sig.u0(), zz, w.stream, w.batch(), is), "scatter");
         count(w);
     }
     NvtxRange step("Step Two");
@@ -550,6 +577,228 @@ void Solver::solve(Work& w, hdd_result* res) {
     if (!converged) throw Error(HDD_ERR_NOT_CONVERGED, "PCG did not converge within max_iters");
 }
 
+void Solver::solve_batch(Work& w, BatchFeeder& feed) {
+    if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+    NvtxRange range("solve_batch");
+    cuda_check(cudaSetDevice(opts.device), "cudaSetDevice");
+    const TileGeom g = geom();
+    const int nt = g.ntiles, K = w.k;
+    const int mode = opts.precision_mode == HDD_PRECISION_MIXED ? 1 : 0;
+    const int np = laplace_partials(g);
+    const size_t N = w.vstride;
+    const float small_number = 1.1920929e-07f;
+    // Per-system state, the host side of what Solver::solve keeps in locals.
+    struct Sys {
+        bool busy = false, replaced = false, restart = false;
+        long long id = -1;
+        int it = 0;
+        double b_inf = 0;
+        float threshold = 0, rmax = 0;
+        std::chrono::steady_clock::time_point t0;
+    };
+    std::vector<Sys> sys(K);
+    std::vector<int> h_active(K, 0), h_first(K, 0), h_rep(K, 0);
+    std::vector<float> h_rmax(K, 0.0f);
+    std::vector<PcgScalars> h_scal(K);
+    PcgScalars init;
+    std::memset(&init, 0, sizeof(init));
+    init.rho_old = 3.402823466e+38f;
+    init.rho_old_d = 3.402823466e+38;
+    auto xs = [&](int j) { return w.x.p + j * N; };
+    auto rs = [&](int j) { return w.r.p + j * N; };
+    auto bs = [&](int j) { return w.b.p + j * N; };
+    auto qs = [&](int j) { return w.q.p + j * N; };
+    auto xds = [&](int j) { return mode == 1 ? w.xd.p + j * N : nullptr; };
+    auto pms = [&](int j) { return w.partial_max.p + (size_t)j * w.pstride; };
+    auto pds = [&](int j) { return w.partial.p + (size_t)j * w.pstride; };
+    auto read_max = [&](int j, float* slot_out) {
+        float v = 0;
+        cuda_check(launch_reduce_max(pms(j), nt, slot_out, w.stream), "reduce");
+        count(w);
+        cuda_check(cudaMemcpyAsync(&v, slot_out, sizeof(float), cudaMemcpyDeviceToHost, w.stream), "D2H");
+        sync(w);
+        return v;
+    };
+    // Ends system j: the true residual of its iterate (reported), its
+    // solution in the caller's layout, the feeder told.
+    auto finish = [&](int j, hdd_status st) {
+        Sys& S = sys[j];
+        float* sf = w.scalars_f.p + 8 * j;
+        if (mode == 1) cuda_check(launch_residual_f64(g, bs(j), xds(j), qs(j), pms(j), w.stream), "true residual");
+        else cuda_check(launch_residual(g, bs(j), xs(j), qs(j), pms(j), w.stream), "true residual");
+        count(w);
+        cuda_check(launch_reduce_max(pms(j), nt, sf + 1, w.stream), "reduce"); count(w);
+        cuda_check(launch_project_dot(g, qs(j), qs(j), pds(j), w.stream), "dot"); count(w);
+        cuda_check(launch_reduce_sum(pds(j), nt, w.sums.p + 8 * j + 2, w.stream), "reduce"); count(w);
+        cuda_check(launch_project_dot(g, bs(j), bs(j), pds(j), w.stream), "dot"); count(w);
+        cuda_check(launch_reduce_sum(pds(j), nt, w.sums.p + 8 * j + 3, w.stream), "reduce"); count(w);
+        float tmax = 0;
+        double d2[2] = {0, 0};
+        cuda_check(cudaMemcpyAsync(&tmax, sf + 1, sizeof(float), cudaMemcpyDeviceToHost, w.stream), "D2H");
+        cuda_check(cudaMemcpyAsync(d2, w.sums.p + 8 * j + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, w.stream),
+                   "D2H");
+        cuda_check(cudaMemsetAsync(w.dense.p, 0, L.cell_count() * sizeof(float), w.stream), "memset");
+        cuda_check(launch_tiles_to_dense(g, tile_xyz.p, L.opt.size[0], L.opt.size[1], L.opt.size[2], xs(j), w.dense.p,
+                                         w.stream),
+                   "tiles_to_dense");
+        count(w);
+        std::vector<float> x(L.cell_count());
+        cuda_check(cudaMemcpyAsync(x.data(), w.dense.p, x.size() * sizeof(float), cudaMemcpyDeviceToHost, w.stream),
+                   "D2H x");
+        sync(w);
+        hdd_result res{};
+        res.iterations = S.it;
+        res.converged = st == HDD_OK ? 1 : 0;
+        res.final_norm = S.rmax;
+        res.b_inf = S.b_inf;
+        res.true_residual_inf = S.b_inf > 0 ? tmax / S.b_inf : tmax;
+        res.true_residual_l2 = d2[1] > 0 ? std::sqrt(d2[0] / d2[1]) : std::sqrt(d2[0]);
+        res.solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - S.t0).count();
+        res.setup_ms = setup_ms;
+        const long long id = S.id;
+        S = Sys();
+        h_active[j] = 0;
+        feed.done(id, st, res, std::move(x));
+    };
+    // The stop test of Solver::solve for system j (its rmax just read):
+    // true when the system is finished (converged, or its true residual
+    // check asked for a restart and it goes on).
+    auto stop_test = [&](int j) -> bool {
+        Sys& S = sys[j];
+        if (S.rmax <= S.threshold && (S.it >= opts.min_iters || S.rmax < small_number)) {
+            if (mode != 1 || S.replaced) { finish(j, HDD_OK); return true; }
+            float* sf = w.scalars_f.p + 8 * j;
+            cuda_check(launch_residual_f64(g, bs(j), xds(j), rs(j), pms(j), w.stream), "true residual"); count(w);
+            S.rmax = read_max(j, sf);
+            S.replaced = true;
+            if (S.rmax <= S.threshold) { finish(j, HDD_OK); return true; }
+            S.restart = true;
+        }
+        if (S.it >= opts.max_iters) { finish(j, HDD_ERR_NOT_CONVERGED); return true; }
+        return false;
+    };
+    // Starts a request on free system j: b from its right-hand side, x = 0,
+    // r = Project(b) (the restart branch of CONJUGATE_GRADIENT.cpp:36).
+    auto start = [&](int j, const float* rhs, long long id) {
+        Sys& S = sys[j];
+        S = Sys();
+        S.busy = true;
+        S.id = id;
+        S.t0 = std::chrono::steady_clock::now();
+        cuda_check(cudaMemcpyAsync(w.dense.p, rhs, L.cell_count() * sizeof(float), cudaMemcpyHostToDevice, w.stream),
+                   "H2D rhs");
+        cuda_check(launch_dense_to_tiles(g, tile_xyz.p, L.opt.size[0], L.opt.size[1], L.opt.size[2], w.dense.p, bs(j),
+                                         w.stream),
+                   "dense_to_tiles");
+        count(w);
+        cuda_check(cudaMemcpyAsync(w.scal.p + j, &init, sizeof(init), cudaMemcpyHostToDevice, w.stream), "scalars");
+        cuda_check(cudaMemsetAsync(xs(j), 0, N * sizeof(float), w.stream), "memset x");
+        if (mode == 1) cuda_check(cudaMemsetAsync(xds(j), 0, N * sizeof(double), w.stream), "memset xd");
+        cuda_check(launch_residual(g, bs(j), xs(j), rs(j), pms(j), w.stream), "residual"); count(w);
+        S.rmax = read_max(j, w.scalars_f.p + 8 * j);
+        S.b_inf = S.rmax;
+        S.threshold = opts.relative_tol ? (float)(opts.tol * S.b_inf) : (float)opts.tol;
+        h_active[j] = 1;
+        if (stop_test(j)) return;
+    };
+    SigmaGpu::clear_error(w.sig, w.stream);
+    // A failure of a device call ends every request the batch holds with its
+    // status, then propagates.
+    auto fail_all = [&](hdd_status st) {
+        for (int j = 0; j < K; ++j) {
+            if (!sys[j].busy) continue;
+            const long long id = sys[j].id;
+            sys[j] = Sys();
+            feed.done(id, st, hdd_result{}, std::vector<float>());
+        }
+    };
+    try {
+    for (;;) {
+        // Free systems take waiting requests.
+        for (int j = 0; j < K; ++j) {
+            while (!sys[j].busy) {
+                const float* rhs = nullptr;
+                long long id = -1;
+                if (!feed.next(&rhs, &id)) break;
+                start(j, rhs, id);
+            }
+        }
+        bool any = false;
+        for (int j = 0; j < K; ++j) any |= sys[j].busy;
+        if (!any) break;
+        for (int j = 0; j < K; ++j) {
+            h_first[j] = sys[j].busy && (sys[j].it == 0 || sys[j].restart) ? 1 : 0;
+            if (sys[j].busy) { sys[j].replaced = false; sys[j].restart = false; }
+        }
+        cuda_check(cudaMemcpyAsync(w.active.p, h_active.data(), K * sizeof(int), cudaMemcpyHostToDevice, w.stream),
+                   "H2D active");
+        cuda_check(cudaMemcpyAsync(w.first.p, h_first.data(), K * sizeof(int), cudaMemcpyHostToDevice, w.stream),
+                   "H2D first");
+        const Batch B = w.batch();
+        apply_preconditioner(w, w.r.p, w.z.p);
+        cuda_check(launch_project_dot(g, w.z.p, w.r.p, w.partial.p, w.stream, B), "project_dot"); count(w);
+        cuda_check(launch_reduce_sum(w.partial.p, nt, w.sums.p + 0, w.stream, B, 8), "reduce"); count(w);
+        cuda_check(launch_scalar_rho(w.scal.p, w.sums.p + 0, 0, w.stream, B, 8), "rho"); count(w);
+        cuda_check(launch_update_s(g, w.s.p, w.z.p, w.scal.p, 0, mode, w.stream, B), "update_s"); count(w);
+        cuda_check(launch_laplace_dot(g, w.s.p, w.q.p, w.partial.p, w.stream, B), "laplace"); count(w);
+        cuda_check(launch_reduce_sum(w.partial.p, np, w.sums.p + 1, w.stream, B, 8), "reduce"); count(w);
+        cuda_check(launch_scalar_alpha(w.scal.p, w.sums.p + 1, w.stream, B, 8), "alpha"); count(w);
+        cuda_check(launch_update_xr(g, w.x.p, w.r.p, w.s.p, w.q.p, w.scal.p, mode, w.partial_max.p, w.stream,
+                                    mode == 1 ? w.xd.p : nullptr, B),
+                   "update_xr");
+        count(w);
+        bool rep = false;
+        for (int j = 0; j < K; ++j) {
+            h_rep[j] = sys[j].busy && mode == 1 && opts.true_residual_every > 0 &&
+                       (sys[j].it + 1) % opts.true_residual_every == 0;
+            rep |= h_rep[j] != 0;
+        }
+        if (rep) {
+            cuda_check(cudaMemcpyAsync(w.replace.p, h_rep.data(), K * sizeof(int), cudaMemcpyHostToDevice, w.stream),
+                       "H2D replace");
+            Batch R = B;
+            R.active = w.replace.p;
+            cuda_check(launch_residual_f64(g, w.b.p, w.xd.p, w.r.p, w.partial_max.p, w.stream, R), "true residual");
+            count(w);
+        }
+        cuda_check(launch_reduce_max(w.partial_max.p, nt, w.scalars_f.p, w.stream, B, 8), "reduce"); count(w);
+        for (int j = 0; j < K; ++j) {
+            if (!sys[j].busy) continue;
+            cuda_check(cudaMemcpyAsync(&h_rmax[j], w.scalars_f.p + 8 * j, sizeof(float), cudaMemcpyDeviceToHost,
+                                       w.stream),
+                       "D2H");
+        }
+        cuda_check(cudaMemcpyAsync(h_scal.data(), w.scal.p, K * sizeof(PcgScalars), cudaMemcpyDeviceToHost, w.stream),
+                   "D2H");
+        int herr = 0;
+        if (w.sig.err)
+            cuda_check(cudaMemcpyAsync(&herr, w.sig.err, sizeof(int), cudaMemcpyDeviceToHost, w.stream), "D2H");
+        sync(w);
+        for (int j = 0; j < K; ++j) {
+            Sys& S = sys[j];
+            if (!S.busy) continue;
+            ++S.it;
+            S.rmax = h_rmax[j];
+            if (h_rep[j]) S.replaced = true;
+            // A bounded wait that gave up leaves this iteration's
+            // preconditioner invalid for every system of the batch.
+            if (herr != 0) { finish(j, HDD_ERR_TIMEOUT); continue; }
+            if (h_scal[j].status != 0 || !std::isfinite(S.rmax)) { finish(j, HDD_ERR_BREAKDOWN); continue; }
+            stop_test(j);
+        }
+        if (herr != 0) SigmaGpu::clear_error(w.sig, w.stream);
+    }
+    } catch (const Error& e) {
+        cudaStreamSynchronize(w.stream);
+        fail_all(e.status);
+        throw;
+    } catch (...) {
+        cudaStreamSynchronize(w.stream);
+        fail_all(HDD_ERR_INTERNAL);
+        throw;
+    }
+}
+
 void Solver::get_solution(Work& w, float* out) {
     if (!w.solved) throw Error(HDD_ERR_NOT_INITIALIZED, "no solution available");
     Tm tm(this, w, 5);
@@ -664,6 +913,43 @@ void Solver::interface_solve(int kind, int level, const float* bh, float* xh, in
     cuda_check(cudaMemcpyAsync(xh, dx, rows * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
     sync();
     check_waits();
+}
+
+void Solver::interface_solve_batch(int kind, int level, int nrhs, const float* bh, float* xh, int* n) {
+    if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
+    if (level < 0 || level >= (int)sigma.lv.size()) throw Error(HDD_ERR_INVALID_ARGUMENT, "level out of range");
+    if (nrhs != 1 && nrhs != 2 && nrhs != 4) throw Error(HDD_ERR_INVALID_ARGUMENT, "nrhs must be 1, 2 or 4");
+    const SigmaLevel& Lv = sigma.lv[level];
+    const SolvePlan& plan = kind == 0 ? Lv.arr_solve : Lv.aii;
+    const int rows = kind == 0 ? Lv.n_iface : Lv.n_int;
+    *n = rows;
+    if (!bh || !xh) return;
+    if (plan.nsn == 0 && rows > 0)
+        throw Error(HDD_ERR_UNSUPPORTED, "no separate solve plan at this level (coarsest level solved as a whole)");
+    if (rows == 0) return;
+    if (nrhs > plan.kmax) throw Error(HDD_ERR_UNSUPPORTED, "this plan's fronts leave no shared memory for that many right-hand sides");
+    cuda_check(cudaSetDevice(opts.device), "cudaSetDevice");
+    DevBuf<float> db, dx;
+    db.upload(bh, (size_t)rows * nrhs, stream);
+    dx.alloc((size_t)rows * nrhs);
+    dx.zero(stream);
+    PlanScratch sc;
+    size_t bytes = 0;
+    plan.alloc_scratch(sc, nullptr, stream, bytes, nrhs);
+    try {
+        plan.solve(sc, db.p, dx.p, stream, w0.launches, nullptr, nrhs, rows, rows);
+        cuda_check(cudaMemcpyAsync(xh, dx.p, (size_t)rows * nrhs * sizeof(float), cudaMemcpyDeviceToHost, stream),
+                   "D2H");
+        sync();
+    } catch (...) {
+        cudaStreamSynchronize(stream);
+        SolvePlan::free_scratch(sc);
+        throw;
+    }
+    int herr = 0;
+    cuda_check(cudaMemcpy(&herr, sc.err, sizeof(int), cudaMemcpyDeviceToHost), "D2H");
+    SolvePlan::free_scratch(sc);
+    if (herr) throw Error(HDD_ERR_TIMEOUT, "a bounded device wait in the batched solve gave up");
 }
 
 void Solver::check_waits(Work& w) {

@@ -75,6 +75,13 @@ inline void cuda_check(cudaError_t e, const char* what) {
 struct Work {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // Systems held side by side (1, 2 or 4): system j's tiled vectors at
+    // + j * vstride, its per-tile partial sums at + j * pstride, its scalars at
+    // scal + j; active / first / replace are per-system flags on the device.
+    int k = 1;
+    size_t vstride = 0;
+    int pstride = 0;
+    DevBuf<int> active, first, replace;
     DevBuf<float> x, b, r, z, s, q;
     DevBuf<double> xd;      // precision form: the FP64 iterate (x is its FP32 rounding)
     DevBuf<float> dense;    // staging buffer in the caller's dense layout
@@ -107,8 +114,32 @@ struct Work {
         size_t t = 0;
         for (const DevBuf<float>* v : {&x, &b, &r, &z, &s, &q, &dense, &partial_max, &scalars_f}) t += v->n * sizeof(float);
         t += (partial.n + sums.n + xd.n) * sizeof(double) + scal.n * sizeof(PcgScalars);
+        t += (active.n + first.n + replace.n) * sizeof(int);
         return t + (own_sig ? sig.bytes : 0);
     }
+    // The launch description of all k systems (a plain single system for k = 1).
+    Batch batch() const {
+        Batch B;
+        if (k == 1) return B;
+        B.k = k;
+        B.vstride = vstride;
+        B.pstride = pstride;
+        B.active = active.p;
+        B.first = first.p;
+        return B;
+    }
+};
+
+// Supplies a batched solve with requests and takes their results: next()
+// fills a free system's right-hand side (dense, in the caller's layout) and
+// returns false when nothing is waiting; done() hands back a finished
+// request's status, result and dense solution.
+struct BatchFeeder {
+    virtual bool next(const float** rhs, long long* id) = 0;
+    virtual void done(long long id, hdd_status st, const hdd_result& res, std::vector<float>&& x) = 0;
+
+protected:
+    ~BatchFeeder() = default;
 };
 
 struct Solver {
@@ -201,7 +232,15 @@ struct Solver {
     // buffers for the vectors and the sigma V-cycle; bytes() tells how much).
     // Contexts run solves concurrently from different host threads; the
     // domain's own setup state is only read.
-    std::unique_ptr<Work> make_work();
+    std::unique_ptr<Work> make_work(int k = 1);
+    // Most systems a batch of this domain can hold (the interface solver's
+    // largest fronts bound it).
+    int max_batch() const;
+    // Continuous batching: solves requests from the feeder on w's k systems
+    // side by side until no system is busy and none is waiting.  A request
+    // joins in the first iteration in which a system is free; each one's
+    // result is bit-identical to its solve alone.
+    void solve_batch(Work& w, BatchFeeder& feed);
     void set_rhs(Work& w, const float* rhs);
     void solve(Work& w, hdd_result* res);
     void get_solution(Work& w, float* out);
@@ -211,6 +250,8 @@ struct Solver {
     void sigma_vcycle_host(const float* b0, float* u0);
     // One Arr (kind 0) or concatenated Aii (kind 1) supernodal solve of a sigma level.
     void interface_solve(int kind, int level, const float* bh, float* xh, int* n);
+    // The same for nrhs (1, 2 or 4) right-hand sides solved in one launch pair.
+    void interface_solve_batch(int kind, int level, int nrhs, const float* bh, float* xh, int* n);
     // Throws HDD_ERR_TIMEOUT when a device-side bounded wait gave up.
     void check_waits() { check_waits(w0); }
     void check_waits(Work& w);
@@ -235,7 +276,7 @@ struct Solver {
         return t + sigma.device_bytes + w0.bytes();
     }
     // Device bytes a further context of this domain allocates.
-    size_t work_bytes() const;
+    size_t work_bytes(int k = 1) const;
 };
 
 }  // namespace hdd

@@ -34,11 +34,13 @@ def make_options(size, sub_size, vlevels=3, nVcycles=1, interior_smoothing=1, bo
 
 
 class SolveServer:
-    def __init__(self, slots: int = 4, hbm_budget_bytes: int = 0, device: int = 0, setup_threads: int = 0):
+    def __init__(self, slots: int = 4, hbm_budget_bytes: int = 0, device: int = 0, setup_threads: int = 0,
+                 batch: int = 0):
         self.lib = _lib.load()
         o = hdd_server_options()
         self.lib.hdd_server_options_default(C.byref(o))
         o.slots, o.hbm_budget_bytes, o.device, o.setup_threads = slots, hbm_budget_bytes, device, setup_threads
+        o.batch = batch
         h = C.c_void_p()
         self._check(self.lib.hdd_server_create(C.byref(o), C.byref(h)))
         self.h = h

@@ -229,6 +229,13 @@ hdd_status hdd_sigma_vcycle(hdd_solver* s, const float* b0, float* u0);
  * whole level (no separate Arr / Aii plans exist there). */
 hdd_status hdd_interface_solve(hdd_solver* s, int kind, int level, const float* b, float* x, int* n);
 
+/* Test seam: the same for nrhs (1, 2 or 4) right-hand sides at once, b and x
+ * holding nrhs vectors of *n entries one after another.  One launch pair
+ * reads each coefficient once for all of them; each solution is bit-identical
+ * to hdd_interface_solve of its right-hand side.  HDD_ERR_UNSUPPORTED when the
+ * plan's largest front leaves no shared memory for nrhs vectors. */
+hdd_status hdd_interface_solve_batch(hdd_solver* s, int kind, int level, int nrhs, const float* b, float* x, int* n);
+
 /* Interface DOF count at a sigma level and the level-0 DOF -> cell map
  * (INTERFACE_MATRIX_GENERATOR::interface_map). */
 hdd_status hdd_interface_size(hdd_solver* s, int level, int* n);
@@ -310,6 +317,8 @@ typedef struct {
     long long hbm_budget_bytes; /* admission budget for resident domains; 0 = 90% of free device memory */
     int device;                 /* CUDA device ordinal */
     int setup_threads;          /* OpenMP threads per domain setup; 0 = host cores / slots */
+    int batch;                  /* continuous batching: requests of one domain solved together, up to this
+                                   many (2 or 4) per batch; 0 or 1 = each request on its own context */
 } hdd_server_options;
 
 void hdd_server_options_default(hdd_server_options* opts);

@@ -183,3 +183,48 @@ def test_failed_domain_reports_its_status():
         srv.remove_domain(dom)
     finally:
         srv.close()
+
+
+@pytest.mark.parametrize("batch,precision", [(4, 0), (2, 1), (4, 1)])
+def test_batched_requests_equal_solo_solves(batch, precision):
+    # Continuous batching: a domain's requests solved k at a time in shared
+    # launches (multi-right-hand-side interface solves, V-cycles over all
+    # systems), requests joining as systems free up.  Every result equals the
+    # request's solve alone, bit for bit.
+    ds = [domains.small(48, 16, 8, seed=7), domains.small((40, 36, 44), 8, 6, seed=11)]
+    rhs = [rhs_set(d, 6) for d in ds]
+    from hierarchicaldd_b200.solver import SPGrid_Domain_Decomposition_Solver
+    ref = []
+    for d, rl in zip(ds, rhs):
+        m = d.meta
+        s = SPGrid_Domain_Decomposition_Solver()
+        s.Set_Domain(d.flags, d.rhs)
+        s.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"],
+                                    m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"],
+                                    m["sigma_mg"], precision_mode=precision, true_residual_every=5)
+        out = []
+        for r in rl:
+            s.Set_RHS(r)
+            res = s.Solve()
+            out.append((res["iterations"], s.Solution()))
+        s.close()
+        ref.append(out)
+    srv = SolveServer(slots=2, batch=batch)
+    try:
+        ids = [srv.add_domain(d.flags, options(d, precision_mode=precision, true_residual_every=5)) for d in ds]
+        for dom in ids:
+            assert srv.wait_domain(dom)
+        # All at once, interleaved over the two domains; then a second wave
+        # submitted while the first is still being solved.
+        reqs = [(i, k, srv.submit(ids[i], rhs[i][k])) for k in range(4) for i in range(len(ds))]
+        reqs += [(i, k, srv.submit(ids[i], rhs[i][k])) for k in range(4, 7) for i in range(len(ds))]
+        for i, k, req in reqs:
+            st, res, x, _ = srv.poll(req, ids[i])
+            assert st == 0, (i, k, st)
+            assert res["iterations"] == ref[i][k][0], (i, k, res["iterations"], ref[i][k][0])
+            assert np.array_equal(x, ref[i][k][1]), (i, k, float(np.max(np.abs(x - ref[i][k][1]))))
+        for dom in ids:
+            srv.remove_domain(dom)
+        assert srv.memory()[0] == 0
+    finally:
+        srv.close()

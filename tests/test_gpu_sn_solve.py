@@ -69,3 +69,48 @@ def test_gpu_plan_solves_match_the_host_reference(n, sub, radius, levels):
     finally:
         s.close()
         shim.shim_free(h)
+
+
+@pytest.mark.parametrize("n,sub,radius,levels", [(64, 16, 12, 3), (96, 32, 20, 3)])
+def test_batched_plan_solves_equal_single_solves(n, sub, radius, levels):
+    # 2 and 4 right-hand sides in one launch pair: every solution bit for bit
+    # the solve of its right-hand side alone.
+    from hierarchicaldd_b200 import _lib
+    from hierarchicaldd_b200.solver import SPGrid_Domain_Decomposition_Solver
+    d = domains.small(n, sub, radius, seed=6)
+    m = dict(d.meta)
+    s = SPGrid_Domain_Decomposition_Solver()
+    lib = _lib.load()
+    rng = np.random.default_rng(7)
+    try:
+        s.Set_Domain(d.flags, d.rhs)
+        s.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, levels, m["nVcycles"],
+                                    m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"],
+                                    m["sigma_mg"])
+        checked = 0
+        for level in range(levels):
+            for kind in (0, 1):
+                nn = C.c_int()
+                assert lib.hdd_interface_solve(s.h, kind, level, None, None, C.byref(nn)) == 0
+                if nn.value == 0:
+                    continue
+                bs = rng.uniform(-1, 1, (4, nn.value)).astype(np.float32)
+                singles = []
+                for k in range(4):
+                    x = np.zeros(nn.value, np.float32)
+                    st = lib.hdd_interface_solve(s.h, kind, level, _fp(bs[k]), _fp(x), C.byref(nn))
+                    singles.append((st, x))
+                if singles[0][0] == 5:
+                    continue  # coarsest level solved as a whole
+                assert all(st == 0 for st, _ in singles)
+                for nrhs in (1, 2, 4):
+                    xb = np.zeros((nrhs, nn.value), np.float32)
+                    bb = np.ascontiguousarray(bs[:nrhs])
+                    st = lib.hdd_interface_solve_batch(s.h, kind, level, nrhs, _fp(bb), _fp(xb), C.byref(nn))
+                    assert st == 0, (level, kind, nrhs, st)
+                    for k in range(nrhs):
+                        assert np.array_equal(xb[k], singles[k][1]), (level, kind, nrhs, k)
+                checked += 1
+        assert checked >= 2
+    finally:
+        s.close()
