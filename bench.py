@@ -44,8 +44,9 @@ def parse():
     p.add_argument("--domains", type=int, default=4, help="c4: resident domains")
     p.add_argument("--requests", type=int, default=32, help="c4: requests per timed run")
     p.add_argument("--slots", type=int, default=4, help="c4: requests in flight")
-    p.add_argument("--batch", type=int, default=4, choices=[0, 2, 4],
-                   help="c4: requests of one domain solved together in shared launches (0 = off)")
+    p.add_argument("--batch", type=int, default=0, choices=[0, 2, 4],
+                   help="c4: requests of one domain solved together in shared launches (0 = off: each "
+                        "request on a context of one system; measured faster on this mix)")
     p.add_argument("--fresh-domains", action="store_true",
                    help="c4: every request brings its own new domain (setup counted in its latency)")
     p.add_argument("--one-solve", action="store_true",
@@ -333,8 +334,9 @@ def run_serving(args):
     * serving form: mixed precision (FP32 operators, FP64 PCG scalars and
       iterate) with the coarsest interface level solved exactly
       (HDD_COARSE_EXACT), through the hdd_server_* C ABI with ``--slots``
-      workers and continuous batching (``--batch`` requests of one domain
-      solved together in shared launches, joining as systems free up);
+      workers, each a driver that solves its domain's queued requests as
+      its contexts free up (``--batch`` 2 or 4: several requests of one
+      domain solved together in shared launches);
     * plain drop-in: the reference's settings (reference precision, 200
       coarsest smoothing steps) through hdd_set_rhs_dense / hdd_solve /
       hdd_get_solution_dense, one request at a time;

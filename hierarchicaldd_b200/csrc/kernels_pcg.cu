@@ -501,14 +501,12 @@ cudaError_t launch_tiles_to_dense_f64(const TileGeom& g, const int* txyz, int sx
     return cudaGetLastError();
 }
 
-// Work units of the marching Laplacian: (tile, slab) pairs, two slabs of 16
-// planes per 32^3 tile so that a 256^3 domain gives 1024 CTAs.
-static int laplace_slabs(int sub) {
-    if (sub != 32) return 1;
-    const char* e = std::getenv("HDD_LAPLACE_SLABS");
-    const int v = e ? std::atoi(e) : 2;
-    return (v == 1 || v == 4) ? v : 2;
-}
+// Work units of the marching Laplacian: (tile, slab) pairs, four slabs of 8
+// planes per 32^3 tile, so that a 256^3 domain gives 2048 CTAs, 3.5 waves of
+// 4 per SM (measured at 256^3: 1, 2 and 4 slabs give 2326, 2442 and 2543
+// GB/s; the halo planes a slab reads twice cost less than the tail of fewer,
+// longer units).
+static int laplace_slabs(int sub) { return sub == 32 ? 4 : 1; }
 
 int laplace_partials(const TileGeom& g) {
     if (g.sub == 8 || g.sub == 16 || g.sub == 32) return g.ntiles * laplace_slabs(g.sub);
@@ -528,11 +526,7 @@ cudaError_t launch_laplace_dot(const TileGeom& g, const float* s, float* q, doub
                                const Batch& B) {
     if (g.ntiles == 0) return cudaSuccess;
     switch (g.sub) {
-        case 32:
-            if (laplace_slabs(32) == 1) launch_march<32, 1>(g, s, q, partial, st, B);
-            else if (laplace_slabs(32) == 4) launch_march<32, 4>(g, s, q, partial, st, B);
-            else launch_march<32, 2>(g, s, q, partial, st, B);
-            break;
+        case 32: launch_march<32, 4>(g, s, q, partial, st, B); break;
         case 16: launch_march<16, 1>(g, s, q, partial, st, B); break;
         case 8: launch_march<8, 1>(g, s, q, partial, st, B); break;
         default:

@@ -7,12 +7,17 @@
 // worker threads.  Each resident domain is one Solver: read-only device data
 // (layout tables, interface matrices, factors and solve plans) plus a pool of
 // solve contexts (PCG vectors, sigma V-cycle buffers and a captured CUDA graph
-// of the preconditioner, each on its own stream).  A worker takes the oldest
-// queued request whose domain is resident and has an idle context, or room in
-// the HBM budget for a new one (at most `slots` per domain), so requests on
-// one domain overlap on the device as well as requests on different domains.
-// Every context runs the same kernels in the same order, so a request's
-// result does not depend on which context or how many others ran beside it.
+// of the preconditioner, each on its own stream) holding 1, 2 or 4 systems.
+// A worker takes the oldest queued request whose domain is resident and has
+// an idle context, or room in the HBM budget for a new one (at most `slots`
+// drivers per domain), and becomes a driver: with batching on and more of the
+// domain's requests waiting it takes a context of several systems, otherwise
+// one of one, and solves requests of that domain continuously, each new one
+// joining as soon as a system is free (continuous batching), until none is
+// waiting.  Requests on one domain overlap on the device as well as requests
+// on different domains.  Every system of every context runs the same kernels
+// in the same order, so a request's result does not depend on which context,
+// which batch or how many others ran beside it.
 // Domains are admitted in arrival order once their estimated device footprint
 // fits the HBM budget; their host setup (layout, interface assembly,
 // factorisation) runs on a worker with setup_threads OpenMP threads, so
@@ -50,18 +55,18 @@ struct Domain {
     hdd_status status = HDD_OK;      // setup failure status
     std::string error;
     std::unique_ptr<Solver> solver;
-    std::vector<std::unique_ptr<Work>> extra;  // contexts beyond the solver's first
-    std::vector<Work*> idle;         // contexts free for a request
-    int contexts = 0;                // contexts made (the first included)
-    long long work_bytes = 0;        // device bytes of one further context
+    struct Ctx {
+        Work* w;
+        bool busy;
+    };
+    std::vector<Ctx> pool;           // solve contexts (the solver's first included)
+    std::vector<std::unique_ptr<Work>> owned;  // contexts beyond the solver's first
+    long long ctx_bytes[3] = {0, 0, 0};  // device bytes of a further context of 1, 2, 4 systems
+    int batch_k = 1;                 // most systems per context (1: batching off)
     long long reserved = 0;          // bytes counted against the budget
-    int running = 0;                 // requests being solved on it
-    // Continuous batching: one batch context (k systems) whose driver pulls
-    // this domain's queued requests into free systems as they arrive.
-    std::unique_ptr<Work> batch;
-    int batch_k = 0;                 // systems per batch (0: batching off for this domain)
-    long long batch_bytes = 0;
-    bool batch_running = false;
+    int running = 0;                 // drivers solving its requests
+    int capacity = 0;                // systems of the running drivers' contexts
+    int held = 0;                    // requests those systems hold
     bool removing = false;
     int queued = 0;                  // requests not yet finished
 };
@@ -189,14 +194,13 @@ struct hdd_server {
             reserved += actual - dd.reserved;
             dd.reserved = actual;
             dd.solver = std::move(s);
-            dd.idle.assign(1, &dd.solver->w0);
-            dd.contexts = 1;
-            dd.work_bytes = (long long)dd.solver->work_bytes();
+            dd.pool.assign(1, Domain::Ctx{&dd.solver->w0, false});
+            dd.batch_k = 1;
             if (opt.batch >= 2) {
                 const int kmax = dd.solver->max_batch();
-                dd.batch_k = opt.batch >= 4 && kmax >= 4 ? 4 : (kmax >= 2 ? 2 : 0);
-                if (dd.batch_k) dd.batch_bytes = (long long)dd.solver->work_bytes(dd.batch_k);
+                dd.batch_k = opt.batch >= 4 && kmax >= 4 ? 4 : (kmax >= 2 ? 2 : 1);
             }
+            for (int i = 0; i < 3; ++i) dd.ctx_bytes[i] = (long long)dd.solver->work_bytes(1 << i);
             dd.state = DomainState::Resident;
         } else {
             reserved -= dd.reserved;
@@ -209,88 +213,33 @@ struct hdd_server {
         }
     }
 
-    void run_solve(long long rid, std::unique_lock<std::mutex>& lk) {
-        Request& r = requests.at(rid);
-        Domain& d = domains.at(r.domain);
-        ++d.running;
-        Solver* s = d.solver.get();
-        Work* w = nullptr;
-        bool fresh = false;  // a new context, its bytes already reserved
-        if (!d.idle.empty()) {
-            w = d.idle.back();
-            d.idle.pop_back();
-        } else {
-            fresh = true;
-            ++d.contexts;
-            d.reserved += d.work_bytes;
-            reserved += d.work_bytes;
-        }
-        const long long wb = d.work_bytes;
-        std::vector<float> rhs;
-        rhs.swap(r.rhs);
-        lk.unlock();
-        hdd_status st = HDD_OK;
-        hdd_result res{};
-        std::vector<float> x;
-        std::unique_ptr<Work> made;
-        try {
-            if (fresh) {
-                made = s->make_work();
-                w = made.get();
-            }
-            s->set_rhs(*w, rhs.data());
-            try {
-                s->solve(*w, &res);
-            } catch (const Error& e) {
-                if (e.status != HDD_ERR_NOT_CONVERGED) throw;
-                st = e.status;
-            }
-            x.resize(rhs.size());
-            s->get_solution(*w, x.data());
-        } catch (const Error& e) {
-            st = e.status;
-        } catch (const std::bad_alloc&) {
-            st = HDD_ERR_OUT_OF_MEMORY;
-        } catch (const std::exception&) {
-            st = HDD_ERR_INTERNAL;
-        }
-        lk.lock();
-        Request& rr = requests.at(rid);
-        rr.result = res;
-        rr.x.swap(x);
-        finish(rr, st);
-        Domain& dd = domains.at(rr.domain);
-        if (made) {
-            dd.extra.push_back(std::move(made));
-        } else if (fresh) {
-            // The context could not be made: give its reservation back.
-            --dd.contexts;
-            dd.reserved -= wb;
-            reserved -= wb;
-            w = nullptr;
-        }
-        if (w) dd.idle.push_back(w);
-        --dd.running;
-        --dd.queued;
+    // Requests of domain `dom` in the queue.
+    int waiting_for(long long dom) const {
+        int n = 0;
+        for (long long q : queue)
+            if (requests.at(q).domain == dom) ++n;
+        return n;
     }
 
-    // Whether a queued request of `d` can start now: its batch driver is
-    // idle (a running driver takes the domain's requests itself), or an idle
-    // context, or room for one more (at most `slots` per domain, within the
-    // budget).
-    bool can_run(const Domain& d) const {
-        if (d.state != DomainState::Resident) return false;
-        if (d.batch_k) return !d.batch_running && (d.batch || reserved + d.batch_bytes <= budget);
-        if (!d.idle.empty()) return true;
-        return d.contexts < opt.slots && reserved + d.work_bytes <= budget;
+    // Whether a queued request of `d` can start a driver now: more of its
+    // requests wait than its running drivers have free systems (those take
+    // them at their next iteration), fewer than `slots` drivers on the
+    // domain, and an idle context or room in the budget for a new one of one
+    // system.
+    bool can_run(const Domain& d, long long dom) const {
+        if (d.state != DomainState::Resident || d.running >= opt.slots) return false;
+        if (d.running > 0 && waiting_for(dom) <= d.capacity - d.held) return false;
+        for (const Domain::Ctx& c : d.pool)
+            if (!c.busy) return true;
+        return reserved + d.ctx_bytes[0] <= budget;
     }
 
-    // The batch driver of request rid's domain: solves it and every request
-    // of the domain queued while the batch runs, k at a time.
+    // Feeds a driver: the request it started with, then every request of its
+    // domain that is queued when one of its systems is free.
     struct Feeder : hdd::BatchFeeder {
-        hdd_server* srv;
-        long long dom;
-        long long first_id;
+        hdd_server* srv = nullptr;
+        long long dom = 0;
+        long long first_id = 0;
         std::vector<float> first_rhs;
         bool first_taken = false;
         std::map<long long, std::vector<float>> rhs;  // kept until the request ends
@@ -309,6 +258,7 @@ struct hdd_server {
                 if (r.domain != dom) continue;
                 const long long rid = *it;
                 srv->queue.erase(it);
+                ++srv->domains.at(dom).held;
                 std::vector<float>& v = rhs[rid];
                 v.swap(r.rhs);
                 *out = v.data();
@@ -324,35 +274,62 @@ struct hdd_server {
             r.result = res;
             r.x = std::move(x);
             srv->finish(r, st);
-            --srv->domains.at(dom).queued;
+            Domain& d = srv->domains.at(dom);
+            --d.queued;
+            --d.held;
             srv->cv.notify_all();
         }
     };
 
-    void run_batch(long long rid, std::unique_lock<std::mutex>& lk) {
+    // A driver for request rid's domain: a context sized by how many of the
+    // domain's requests wait (several systems when batching is on and more
+    // than one waits, else one), then requests solved continuously on it.
+    void run_driver(long long rid, std::unique_lock<std::mutex>& lk) {
         Request& r = requests.at(rid);
         const long long dom = r.domain;
         Domain& d = domains.at(dom);
-        d.batch_running = true;
-        Solver* s = d.solver.get();
-        const int k = d.batch_k;
-        bool make = !d.batch;
-        if (make) {
-            d.reserved += d.batch_bytes;
-            reserved += d.batch_bytes;
+        // Requests this driver is for: this one and those that the running
+        // drivers' free systems will not take.
+        const int need = 1 + std::max(0, waiting_for(dom) - (d.capacity - d.held));
+        int want = 1;
+        if (d.batch_k >= 2 && need >= 2) want = (d.batch_k >= 4 && need >= 3) ? 4 : 2;
+        auto slot_of = [](int k) { return k == 1 ? 0 : (k == 2 ? 1 : 2); };
+        // An idle context of the wanted size, else a new one if the budget
+        // allows, else any idle context, else a new one of one system (which
+        // can_run guaranteed).
+        int pick = -1, make_k = 0;
+        for (size_t i = 0; i < d.pool.size() && pick < 0; ++i)
+            if (!d.pool[i].busy && d.pool[i].w->k == want) pick = (int)i;
+        if (pick < 0 && reserved + d.ctx_bytes[slot_of(want)] <= budget) make_k = want;
+        for (size_t i = 0; i < d.pool.size() && pick < 0 && !make_k; ++i)
+            if (!d.pool[i].busy) pick = (int)i;
+        if (pick < 0 && !make_k) make_k = 1;
+        Work* w = nullptr;
+        long long mb = 0;
+        if (pick >= 0) {
+            d.pool[pick].busy = true;
+            w = d.pool[pick].w;
+        } else {
+            mb = d.ctx_bytes[slot_of(make_k)];
+            d.reserved += mb;
+            reserved += mb;
         }
+        ++d.running;
+        const int cap = pick >= 0 ? w->k : make_k;
+        d.capacity += cap;
+        ++d.held;  // the request it starts with
+        Solver* s = d.solver.get();
         Feeder feed;
         feed.srv = this;
         feed.dom = dom;
         feed.first_id = rid;
         feed.first_rhs.swap(r.rhs);
-        Work* w = d.batch.get();
         lk.unlock();
         std::unique_ptr<Work> made;
         hdd_status st = HDD_OK;
         try {
-            if (make) {
-                made = s->make_work(k);
+            if (!w) {
+                made = s->make_work(make_k);
                 w = made.get();
             }
             s->solve_batch(*w, feed);
@@ -365,29 +342,31 @@ struct hdd_server {
         }
         lk.lock();
         Domain& dd = domains.at(dom);
-        if (made) dd.batch = std::move(made);
-        else if (make) {
-            // The batch context could not be made: give its reservation back
-            // and run this domain's requests on single contexts from now on.
-            dd.reserved -= dd.batch_bytes;
-            reserved -= dd.batch_bytes;
-            dd.batch_k = 0;
+        if (made) {
+            dd.pool.push_back(Domain::Ctx{made.get(), false});
+            dd.owned.push_back(std::move(made));
+        } else if (pick >= 0) {
+            dd.pool[pick].busy = false;
+        } else {
+            // The context could not be made: give its reservation back.
+            dd.reserved -= mb;
+            reserved -= mb;
         }
-        // A request not yet handed to the batch when it failed (the first
-        // one, if the context could not be made) fails with it.
+        // The first request fails with the driver if it never reached a system.
         if (!feed.first_taken) {
-            Request& rr = requests.at(rid);
-            finish(rr, st == HDD_OK ? HDD_ERR_INTERNAL : st);
+            finish(requests.at(rid), st == HDD_OK ? HDD_ERR_INTERNAL : st);
             --dd.queued;
+            --dd.held;
         }
-        dd.batch_running = false;
+        dd.capacity -= cap;
+        --dd.running;
     }
 
     // Index in `queue` of the oldest request whose domain can run now, or -1.
     long long runnable() {
         for (size_t i = 0; i < queue.size(); ++i) {
-            const Domain& d = domains.at(requests.at(queue[i]).domain);
-            if (can_run(d)) return (long long)i;
+            const long long dom = requests.at(queue[i]).domain;
+            if (can_run(domains.at(dom), dom)) return (long long)i;
         }
         return -1;
     }
@@ -412,8 +391,7 @@ struct hdd_server {
             if (qi >= 0) {
                 const long long rid = queue[(size_t)qi];
                 queue.erase(queue.begin() + qi);
-                if (domains.at(requests.at(rid).domain).batch_k) run_batch(rid, lk);
-                else run_solve(rid, lk);
+                run_driver(rid, lk);
             } else {
                 const long long id = setups.front();
                 setups.pop_front();
@@ -592,8 +570,7 @@ hdd_status hdd_server_remove_domain(hdd_server* srv, long long domain_id) {
             it->second.removing = true;
             srv->cv.wait(lk, [&] {
                 const Domain& d = srv->domains.at(domain_id);
-                return srv->stop || (d.queued == 0 && d.running == 0 && !d.batch_running &&
-                                     d.state != DomainState::SettingUp &&
+                return srv->stop || (d.queued == 0 && d.running == 0 && d.state != DomainState::SettingUp &&
                                      d.state != DomainState::Admitted);
             });
             if (srv->stop) return HDD_ERR_BUSY;
@@ -605,8 +582,7 @@ hdd_status hdd_server_remove_domain(hdd_server* srv, long long domain_id) {
                 srv->reserved -= d.reserved;
             }
             s = std::move(d.solver);
-            extra.swap(d.extra);
-            if (d.batch) extra.push_back(std::move(d.batch));
+            extra.swap(d.owned);
             srv->domains.erase(domain_id);
             srv->admit();
             srv->cv.notify_all();

@@ -730,16 +730,21 @@ void Solver::solve_batch(Work& w, BatchFeeder& feed) {
             h_first[j] = sys[j].busy && (sys[j].it == 0 || sys[j].restart) ? 1 : 0;
             if (sys[j].busy) { sys[j].replaced = false; sys[j].restart = false; }
         }
-        cuda_check(cudaMemcpyAsync(w.active.p, h_active.data(), K * sizeof(int), cudaMemcpyHostToDevice, w.stream),
-                   "H2D active");
-        cuda_check(cudaMemcpyAsync(w.first.p, h_first.data(), K * sizeof(int), cudaMemcpyHostToDevice, w.stream),
-                   "H2D first");
+        // One system runs as a plain solve (first passed by value below).
+        if (K > 1) {
+            cuda_check(cudaMemcpyAsync(w.active.p, h_active.data(), K * sizeof(int), cudaMemcpyHostToDevice,
+                                       w.stream),
+                       "H2D active");
+            cuda_check(cudaMemcpyAsync(w.first.p, h_first.data(), K * sizeof(int), cudaMemcpyHostToDevice, w.stream),
+                       "H2D first");
+        }
         const Batch B = w.batch();
+        const int first1 = K == 1 ? h_first[0] : 0;
         apply_preconditioner(w, w.r.p, w.z.p);
         cuda_check(launch_project_dot(g, w.z.p, w.r.p, w.partial.p, w.stream, B), "project_dot"); count(w);
         cuda_check(launch_reduce_sum(w.partial.p, nt, w.sums.p + 0, w.stream, B, 8), "reduce"); count(w);
-        cuda_check(launch_scalar_rho(w.scal.p, w.sums.p + 0, 0, w.stream, B, 8), "rho"); count(w);
-        cuda_check(launch_update_s(g, w.s.p, w.z.p, w.scal.p, 0, mode, w.stream, B), "update_s"); count(w);
+        cuda_check(launch_scalar_rho(w.scal.p, w.sums.p + 0, first1, w.stream, B, 8), "rho"); count(w);
+        cuda_check(launch_update_s(g, w.s.p, w.z.p, w.scal.p, first1, mode, w.stream, B), "update_s"); count(w);
         cuda_check(launch_laplace_dot(g, w.s.p, w.q.p, w.partial.p, w.stream, B), "laplace"); count(w);
         cuda_check(launch_reduce_sum(w.partial.p, np, w.sums.p + 1, w.stream, B, 8), "reduce"); count(w);
         cuda_check(launch_scalar_alpha(w.scal.p, w.sums.p + 1, w.stream, B, 8), "alpha"); count(w);
@@ -754,10 +759,13 @@ void Solver::solve_batch(Work& w, BatchFeeder& feed) {
             rep |= h_rep[j] != 0;
         }
         if (rep) {
-            cuda_check(cudaMemcpyAsync(w.replace.p, h_rep.data(), K * sizeof(int), cudaMemcpyHostToDevice, w.stream),
-                       "H2D replace");
             Batch R = B;
-            R.active = w.replace.p;
+            if (K > 1) {
+                cuda_check(cudaMemcpyAsync(w.replace.p, h_rep.data(), K * sizeof(int), cudaMemcpyHostToDevice,
+                                           w.stream),
+                           "H2D replace");
+                R.active = w.replace.p;
+            }
             cuda_check(launch_residual_f64(g, w.b.p, w.xd.p, w.r.p, w.partial_max.p, w.stream, R), "true residual");
             count(w);
         }
