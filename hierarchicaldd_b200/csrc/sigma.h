@@ -175,6 +175,7 @@ struct SolvePlan {
     int grid = 0;                    // persistent CTAs per launch (one right-hand side)
     int grids[3] = {0, 0, 0};        // ... for 1, 2 and 4 right-hand sides (0: shared memory too small)
     int kmax = 1;                    // most right-hand sides one launch takes
+    int nt = 256;                    // threads per CTA (128 for plans of many factors)
     int ntasks_f = 0, ntasks_b = 0;  // tasks, forward / backward
     double fwd_bytes = 0, bwd_bytes = 0;  // algorithmic bytes of one forward / backward launch
     int *d_col0 = nullptr, *d_ncol = nullptr, *d_nrow = nullptr, *d_parent = nullptr;

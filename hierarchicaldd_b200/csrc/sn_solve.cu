@@ -23,8 +23,8 @@
 // plan's error word when it gives up.  Data produced by other CTAs in the same
 // launch is read with L2-coherent loads after an acquire of the counter.
 //
-// Small fronts (a few row chunks times few columns) go in bundles of eight,
-// one warp per front, so eight short dependency chains run per CTA.  Other
+// Small fronts (a few row chunks times few columns) go in bundles of one per
+// warp, so that many short dependency chains run per CTA.  Other
 // forward tasks are row blocks of up to kRB rows; a CTA splits its threads
 // into row lanes x column slices and adds the slices in a fixed order.  Tall
 // fronts whose row block needs more than kCC columns are split into column
@@ -46,11 +46,20 @@
 namespace hdd {
 namespace {
 
-constexpr int kNT = 256;                 // threads per CTA
+// Threads per CTA: a plan of many independent factors (the subdomain
+// interiors) runs 128-thread CTAs, more of them per SM for its many short
+// tasks; a plan of one factor (the interface) runs 256-thread CTAs, which do
+// its tall fronts in fewer tasks.  Measured at 256^3: 128 threads make the
+// interior plans 10-20 % faster and the interface plans 20-30 % slower.
+constexpr int kNTInterior = 128, kNTInterface = 256;
 constexpr int kRB = 128;                 // rows per forward row block
 constexpr int kCC = 128;                 // columns per forward column block
-constexpr int kBC = 32;                  // columns per backward task (8 warps x 4)
-constexpr int kWarps = kNT / 32;         // small fronts per bundle (one per warp)
+// Small fronts per bundle (one per warp) and columns per backward task (4 per
+// warp), for NT threads.
+__host__ __device__ constexpr int warps_of(int nt) { return nt / 32; }
+__host__ __device__ constexpr int bc_of(int nt) { return 4 * (nt / 32); }
+// CTAs per SM the register budget is sized for (K right-hand sides, NT threads).
+__host__ __device__ constexpr int min_blocks(int k, int nt) { return (k == 1 ? 1280 : (k == 2 ? 768 : 512)) / nt; }
 constexpr int kSmallM = 256;             // rows of a front solved by one warp
 constexpr int kSmallLoads = 128;         // ... when its row chunks x columns stay below this
 
@@ -278,12 +287,12 @@ __device__ void warp_backward(const PlanView& P, int J, double* g, int lane, flo
     if (lane == 0) atomicAdd(done + J, 1);
 }
 
-template <int K>
-__global__ void __launch_bounds__(kNT, K == 1 ? 5 : (K == 2 ? 3 : 2))
+template <int K, int NT>
+__global__ void __launch_bounds__(NT, min_blocks(K, NT))
     sn_forward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks, const float* __restrict__ b_old) {
     extern __shared__ double sh[];
     double* f = sh;                    // the front's input vectors, m x K entries
-    double* red = sh + P.max_m * K;    // column-slice partial sums, 4 K kNT entries
+    double* red = sh + P.max_m * K;    // column-slice partial sums, 4 K NT entries
     __shared__ int s_ticket, s_last;
     int* done = P.ctr + 2;
     int* chunk_ctr = P.ctr + 2 + 2 * P.nsn;
@@ -308,7 +317,7 @@ __global__ void __launch_bounds__(kNT, K == 1 ? 5 : (K == 2 ? 3 : 2))
         // dependency wait and the assembly.
         const int nq = (T.rows + 3) >> 2;
         const int mq = nq <= 8 ? 8 : (nq <= 16 ? 16 : 32);
-        const int ks = kNT / mq;
+        const int ks = NT / mq;
         const int sl = tid / mq, lq = tid - sl * mq;
         const int row = T.r0 + 4 * lq;
         const bool active = lq < nq;
@@ -326,7 +335,7 @@ __global__ void __launch_bounds__(kNT, K == 1 ? 5 : (K == 2 ? 3 : 2))
         for (int u = 0; u < 4; ++u)
             v0[u] = (cbeg + u < cend) ? ldg4(A + (size_t)(cbeg + u) * ld) : make_float4(0.f, 0.f, 0.f, 0.f);
         // b's part of the input vectors does not depend on other fronts.
-        for (int i = tid; i < m; i += kNT) {
+        for (int i = tid; i < m; i += NT) {
             const int po = i < nj ? P.perm[c0 + i] : 0;
 #pragma unroll
             for (int j = 0; j < K; ++j) f[(size_t)i * K + j] = (i < nj) ? (double)b_old[j * P.ld_b + po] : 0.0;
@@ -342,7 +351,7 @@ __global__ void __launch_bounds__(kNT, K == 1 ? 5 : (K == 2 ? 3 : 2))
             const int mc = P.nrow[C];
             const double* uc = P.upd + P.upd_off[C];
             const int* rm = P.relmap + P.relmap_off[C];
-            for (int k = tid; k < mc; k += kNT) {
+            for (int k = tid; k < mc; k += NT) {
                 const int tr = rm[k];
 #pragma unroll
                 for (int j = 0; j < K; ++j) f[(size_t)tr * K + j] += __ldcg(uc + j * P.ld_upd + k);
@@ -379,15 +388,15 @@ __global__ void __launch_bounds__(kNT, K == 1 ? 5 : (K == 2 ? 3 : 2))
 #pragma unroll
             for (int j = 0; j < K; ++j)
 #pragma unroll
-                for (int e = 0; e < 4; ++e) red[(size_t)(j * 4 + e) * kNT + tid] = acc[j][e];
+                for (int e = 0; e < 4; ++e) red[(size_t)(j * 4 + e) * NT + tid] = acc[j][e];
             __syncthreads();
             if (sl == 0 && active) {
 #pragma unroll
                 for (int j = 0; j < K; ++j)
 #pragma unroll
                     for (int e = 0; e < 4; ++e) {
-                        double s2 = red[(size_t)(j * 4 + e) * kNT + lq];
-                        for (int q = 1; q < ks; ++q) s2 += red[(size_t)(j * 4 + e) * kNT + q * mq + lq];
+                        double s2 = red[(size_t)(j * 4 + e) * NT + lq];
+                        for (int q = 1; q < ks; ++q) s2 += red[(size_t)(j * 4 + e) * NT + q * mq + lq];
                         acc[j][e] = s2;
                     }
             }
@@ -445,8 +454,8 @@ __global__ void __launch_bounds__(kNT, K == 1 ? 5 : (K == 2 ? 3 : 2))
     }
 }
 
-template <int K>
-__global__ void __launch_bounds__(kNT, K == 1 ? 5 : (K == 2 ? 3 : 2))
+template <int K, int NT>
+__global__ void __launch_bounds__(NT, min_blocks(K, NT))
     sn_backward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks, float* __restrict__ x_old) {
     extern __shared__ double g[];  // [y_J; x_R] x K, m4 x K entries (zero padding rows)
     __shared__ int s_ticket;
@@ -479,10 +488,10 @@ __global__ void __launch_bounds__(kNT, K == 1 ? 5 : (K == 2 ? 3 : 2))
         // Row quads wholly below nj (the L_JJ^{-T} y part) need only this
         // front's forward result, so they are summed before waiting on the
         // parent; each lane adds its quads in ascending order.
-        for (int i = rs + tid; i < nj; i += kNT)  // from the forward launch
+        for (int i = rs + tid; i < nj; i += NT)  // from the forward launch
 #pragma unroll
             for (int j = 0; j < K; ++j) g[(size_t)i * K + j] = P.ynew[j * P.ld_n + c0 + i];
-        for (int i = m + tid; i < m4; i += kNT)  // padding rows
+        for (int i = m + tid; i < m4; i += NT)  // padding rows
 #pragma unroll
             for (int j = 0; j < K; ++j) g[(size_t)i * K + j] = 0.0;
         __syncthreads();
@@ -495,7 +504,7 @@ __global__ void __launch_bounds__(kNT, K == 1 ? 5 : (K == 2 ? 3 : 2))
                 for (int e = 0; e < 4; ++e) gg[j][e] = g[(size_t)(rr + e) * K + j];
 #pragma unroll
             for (int jj = 0; jj < 4; ++jj) {
-                const int a = amin + 8 * jj;
+                const int a = amin + warps_of(NT) * jj;
                 if (a < a0 + na) {
                     const float4 v = ldg4(A + (size_t)a * ld + rr);
 #pragma unroll
@@ -517,7 +526,7 @@ __global__ void __launch_bounds__(kNT, K == 1 ? 5 : (K == 2 ? 3 : 2))
             if (p >= 0 && !wait_at_least(done + p, P.ntb[p], P.err, P.spin_limit)) atomicExch(P.err, 1);
         }
         __syncthreads();
-        for (int i = max(rs, nj) + tid; i < m; i += kNT) {
+        for (int i = max(rs, nj) + tid; i < m; i += NT) {
             const int tr = rows[i - nj];
 #pragma unroll
             for (int j = 0; j < K; ++j) g[(size_t)i * K + j] = __ldcg(P.xnew + j * P.ld_n + tr);
@@ -536,7 +545,7 @@ __global__ void __launch_bounds__(kNT, K == 1 ? 5 : (K == 2 ? 3 : 2))
         if (lane == 0) {
 #pragma unroll
             for (int jj = 0; jj < 4; ++jj) {
-                const int a = amin + 8 * jj;
+                const int a = amin + warps_of(NT) * jj;
                 if (a < a0 + na) {
                     const int po = P.perm[c0 + a];
 #pragma unroll
@@ -553,11 +562,11 @@ __global__ void __launch_bounds__(kNT, K == 1 ? 5 : (K == 2 ? 3 : 2))
     }
 }
 
-size_t forward_smem(int max_m, int k) {
-    return (size_t)std::max((max_m + 4 * kNT) * k, kWarps * kSmallM * k) * sizeof(double);
+size_t forward_smem(int max_m, int k, int nt) {
+    return (size_t)std::max((max_m + 4 * nt) * k, warps_of(nt) * kSmallM * k) * sizeof(double);
 }
-size_t backward_smem(int max_m, int k) {
-    return (size_t)std::max(((max_m + 3) & ~3) * k, kWarps * kSmallM * k) * sizeof(double);
+size_t backward_smem(int max_m, int k, int nt) {
+    return (size_t)std::max(((max_m + 3) & ~3) * k, warps_of(nt) * kSmallM * k) * sizeof(double);
 }
 
 // Right-hand-side counts a launch can take (template instances), and the
@@ -569,30 +578,39 @@ constexpr size_t kSmemMax = 227 * 1024;
 // so a plan built later with smaller fronts cannot invalidate an earlier
 // plan's launches.
 std::mutex g_smem_mu;
-int g_smem_limit[64][3] = {};
-template <int K>
+int g_smem_limit[64][6] = {};
+template <int K, int NT>
 void raise_limit_k(int device, int bytes, int slot) {
     if (bytes <= g_smem_limit[device][slot]) return;
-    dev::ck(cudaFuncSetAttribute(sn_forward_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+    dev::ck(cudaFuncSetAttribute(sn_forward_kernel<K, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
             "smem attr");
-    dev::ck(cudaFuncSetAttribute(sn_backward_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+    dev::ck(cudaFuncSetAttribute(sn_backward_kernel<K, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
             "smem attr");
     g_smem_limit[device][slot] = bytes;
 }
-void raise_smem_limit(int device, int k, int bytes) {
+template <int NT>
+void raise_limit_nt(int device, int k, int bytes, int base) {
+    if (k == 1) raise_limit_k<1, NT>(device, bytes, base);
+    else if (k == 2) raise_limit_k<2, NT>(device, bytes, base + 1);
+    else raise_limit_k<4, NT>(device, bytes, base + 2);
+}
+void raise_smem_limit(int device, int k, int nt, int bytes) {
     std::lock_guard<std::mutex> lock(g_smem_mu);
     if (device < 0 || device >= 64) throw Error(HDD_ERR_INVALID_ARGUMENT, "device ordinal out of range");
-    if (k == 1) raise_limit_k<1>(device, bytes, 0);
-    else if (k == 2) raise_limit_k<2>(device, bytes, 1);
-    else raise_limit_k<4>(device, bytes, 2);
+    if (nt == kNTInterior) raise_limit_nt<kNTInterior>(device, k, bytes, 0);
+    else raise_limit_nt<kNTInterface>(device, k, bytes, 3);
 }
 
-template <int K>
+template <int K, int NT>
 int occupancy_k(size_t smf, size_t smb) {
     int bf = 0, bb = 0;
-    dev::ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, sn_forward_kernel<K>, kNT, smf), "occupancy");
-    dev::ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, sn_backward_kernel<K>, kNT, smb), "occupancy");
+    dev::ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, sn_forward_kernel<K, NT>, NT, smf), "occupancy");
+    dev::ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, sn_backward_kernel<K, NT>, NT, smb), "occupancy");
     return std::max(1, std::min(bf, bb));
+}
+template <int NT>
+int occupancy_nt(int k, size_t smf, size_t smb) {
+    return k == 1 ? occupancy_k<1, NT>(smf, smb) : (k == 2 ? occupancy_k<2, NT>(smf, smb) : occupancy_k<4, NT>(smf, smb));
 }
 
 }  // namespace
@@ -626,6 +644,8 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
         }
     }
     if (nsn == 0) return;
+    nt = factors.size() >= 2 ? kNTInterior : kNTInterface;
+    const int kWarps = warps_of(nt), kBC = bc_of(nt);
     height.assign(nsn, 0);
     depth.assign(nsn, 0);
     for (int g = 0; g < nsn; ++g)
@@ -764,7 +784,7 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
             relmap.push_back(posn);
         }
     }
-    if (forward_smem(max_front, 1) > 200 * 1024)
+    if (forward_smem(max_front, 1, nt) > 200 * 1024)
         throw Error(HDD_ERR_UNSUPPORTED, "supernodal front too large for shared memory: " + std::to_string(max_front));
     bytes = 0;
     d_col0 = dev::upload(col0, s, bytes);
@@ -812,11 +832,11 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
     kmax = 1;
     for (int i = 0; i < 3; ++i) {
         const int k = kBatches[i];
-        const size_t smf = forward_smem(max_front, k), smb = backward_smem(max_front, k);
+        const size_t smf = forward_smem(max_front, k, nt), smb = backward_smem(max_front, k, nt);
         grids[i] = 0;
         if (std::max(smf, smb) > kSmemMax) break;
-        raise_smem_limit(dev_id, k, (int)std::max(smf, smb));
-        const int occ = k == 1 ? occupancy_k<1>(smf, smb) : (k == 2 ? occupancy_k<2>(smf, smb) : occupancy_k<4>(smf, smb));
+        raise_smem_limit(dev_id, k, nt, (int)std::max(smf, smb));
+        const int occ = nt == kNTInterior ? occupancy_nt<kNTInterior>(k, smf, smb) : occupancy_nt<kNTInterface>(k, smf, smb);
         grids[i] = std::max(1, nsm * occ);
         kmax = k;
     }
@@ -875,16 +895,17 @@ void SolvePlan::solve(const float* b_old, float* x_old, cudaStream_t s, long lon
     solve(primary(), b_old, x_old, s, launches, hook);
 }
 
-template <int K>
+template <int K, int NT>
 static void launch_pair(const PlanView& P, int g, int n_fwd, int n_bwd, int max_front, const SnTask* fwd,
                         const SnTask* bwd, const float* b_old, float* x_old, cudaStream_t s, PhaseHook* hook,
                         double fwd_bytes, double bwd_bytes) {
     if (hook) hook->begin(kPhaseSnForward);
-    sn_forward_kernel<K><<<std::min(g, n_fwd), kNT, forward_smem(max_front, K), s>>>(P, fwd, n_fwd, b_old);
+    sn_forward_kernel<K, NT><<<std::min(g, n_fwd), NT, forward_smem(max_front, K, NT), s>>>(P, fwd, n_fwd, b_old);
     dev::ck(cudaGetLastError(), "sn forward");
     if (hook) hook->end(kPhaseSnForward, fwd_bytes);
     if (hook) hook->begin(kPhaseSnBackward);
-    sn_backward_kernel<K><<<std::min(g, n_bwd), kNT, backward_smem(max_front, K), s>>>(P, bwd, n_bwd, x_old);
+    sn_backward_kernel<K, NT><<<std::min(g, n_bwd), NT, backward_smem(max_front, K, NT), s>>>(P, bwd, n_bwd,
+                                                                                          x_old);
     dev::ck(cudaGetLastError(), "sn backward");
     if (hook) hook->end(kPhaseSnBackward, bwd_bytes);
 }
@@ -903,9 +924,15 @@ void SolvePlan::solve(const PlanScratch& sc, const float* b_old, float* x_old, c
     const int full = grids[slot];
     const int g = sc.grid_div > 1 ? std::max(1, (full + sc.grid_div - 1) / sc.grid_div) : full;
     const double fb = fwd_bytes + 8.0 * n * (nrhs - 1), bb = bwd_bytes + 8.0 * n * (nrhs - 1);
-    if (nrhs == 1) launch_pair<1>(P, g, n_fwd, n_bwd, max_front, d_fwd, d_bwd, b_old, x_old, s, hook, fb, bb);
-    else if (nrhs == 2) launch_pair<2>(P, g, n_fwd, n_bwd, max_front, d_fwd, d_bwd, b_old, x_old, s, hook, fb, bb);
-    else launch_pair<4>(P, g, n_fwd, n_bwd, max_front, d_fwd, d_bwd, b_old, x_old, s, hook, fb, bb);
+    if (nt == kNTInterior) {
+        if (nrhs == 1) launch_pair<1, kNTInterior>(P, g, n_fwd, n_bwd, max_front, d_fwd, d_bwd, b_old, x_old, s, hook, fb, bb);
+        else if (nrhs == 2) launch_pair<2, kNTInterior>(P, g, n_fwd, n_bwd, max_front, d_fwd, d_bwd, b_old, x_old, s, hook, fb, bb);
+        else launch_pair<4, kNTInterior>(P, g, n_fwd, n_bwd, max_front, d_fwd, d_bwd, b_old, x_old, s, hook, fb, bb);
+    } else {
+        if (nrhs == 1) launch_pair<1, kNTInterface>(P, g, n_fwd, n_bwd, max_front, d_fwd, d_bwd, b_old, x_old, s, hook, fb, bb);
+        else if (nrhs == 2) launch_pair<2, kNTInterface>(P, g, n_fwd, n_bwd, max_front, d_fwd, d_bwd, b_old, x_old, s, hook, fb, bb);
+        else launch_pair<4, kNTInterface>(P, g, n_fwd, n_bwd, max_front, d_fwd, d_bwd, b_old, x_old, s, hook, fb, bb);
+    }
     launches += 2;
 }
 
