@@ -47,11 +47,13 @@ namespace hdd {
 namespace {
 
 // Threads per CTA: a plan of many independent factors (the subdomain
-// interiors) runs 128-thread CTAs, more of them per SM for its many short
+// interiors) runs 64-thread CTAs, many of them per SM for its many short
 // tasks; a plan of one factor (the interface) runs 256-thread CTAs, which do
-// its tall fronts in fewer tasks.  Measured at 256^3: 128 threads make the
-// interior plans 10-20 % faster and the interface plans 20-30 % slower.
-constexpr int kNTInterior = 128, kNTInterface = 256;
+// its tall fronts in fewer tasks.  Measured at 256^3, level-0 interior plan
+// forward / backward: 801 / 836 us with 256 threads, 650 / 760 with 128,
+// 577 / 711 with 64; level-0 interface plan: 480 / 596 us with 256 threads,
+// 662 / 731 with 128, 703 / 565 with 512.
+constexpr int kNTInterior = 64, kNTInterface = 256;
 constexpr int kRB = 128;                 // rows per forward row block
 constexpr int kCC = 128;                 // columns per forward column block
 // Small fronts per bundle (one per warp) and columns per backward task (4 per
