@@ -182,6 +182,8 @@ struct SolvePlan {
     int *d_rows = nullptr; long long *d_rows_off = nullptr;
     int *d_child_ptr = nullptr, *d_child = nullptr;
     long long* d_relmap_off = nullptr; int* d_relmap = nullptr;
+    long long *d_gp_off = nullptr, *d_ge_off = nullptr;  // per front: gather-list offsets
+    int *d_gptr = nullptr, *d_gent = nullptr;           // gather lists (see sn_solve.cu)
     long long* d_upd_off = nullptr;
     long long* d_fw_off = nullptr;   // per front: float offset of Fw (leading dimension round4(m))
     int *d_ntf = nullptr, *d_ntb = nullptr;  // tasks per front, forward / backward

@@ -77,6 +77,11 @@ struct PlanView {
     const int *child_ptr, *child;
     const long long* relmap_off;
     const int* relmap;
+    // Gather lists: position p of front J's input vector receives the update
+    // entries gent[ge_off[J] + gptr[gp_off[J] + p] .. gptr[gp_off[J] + p + 1])
+    // (indices into upd), in child order.
+    const long long *gp_off, *ge_off;
+    const int *gptr, *gent;
     const long long* upd_off;
     const long long* fw_off;
     const int *ntf, *ntb;
@@ -336,29 +341,74 @@ __global__ void __launch_bounds__(NT, min_blocks(K, NT))
 #pragma unroll
         for (int u = 0; u < 4; ++u)
             v0[u] = (cbeg + u < cend) ? ldg4(A + (size_t)(cbeg + u) * ld) : make_float4(0.f, 0.f, 0.f, 0.f);
-        // b's part of the input vectors does not depend on other fronts.
-        for (int i = tid; i < m; i += NT) {
-            const int po = i < nj ? P.perm[c0 + i] : 0;
+        if constexpr (NT < 128) {
+            // Small fronts (the interior plans' 64-thread CTAs): the whole
+            // input vectors, b's part before the wait, then each child's
+            // update scattered in, child by child.
+            for (int i = tid; i < m; i += NT) {
+                const int po = i < nj ? P.perm[c0 + i] : 0;
 #pragma unroll
-            for (int j = 0; j < K; ++j) f[(size_t)i * K + j] = (i < nj) ? (double)b_old[j * P.ld_b + po] : 0.0;
-        }
-        if (tid == 0) {
-            bool ok = true;
-            for (int c = cb; c < ce; ++c) ok &= wait_at_least(done + P.child[c], P.ntf[P.child[c]], P.err, P.spin_limit);
-            if (!ok) atomicExch(P.err, 1);
-        }
-        __syncthreads();
-        for (int c = cb; c < ce; ++c) {
-            const int C = P.child[c];
-            const int mc = P.nrow[C];
-            const double* uc = P.upd + P.upd_off[C];
-            const int* rm = P.relmap + P.relmap_off[C];
-            for (int k = tid; k < mc; k += NT) {
-                const int tr = rm[k];
-#pragma unroll
-                for (int j = 0; j < K; ++j) f[(size_t)tr * K + j] += __ldcg(uc + j * P.ld_upd + k);
+                for (int j = 0; j < K; ++j) f[(size_t)i * K + j] = (i < nj) ? (double)b_old[j * P.ld_b + po] : 0.0;
+            }
+            if (tid == 0) {
+                bool ok = true;
+                for (int c = cb; c < ce; ++c)
+                    ok &= wait_at_least(done + P.child[c], P.ntf[P.child[c]], P.err, P.spin_limit);
+                if (!ok) atomicExch(P.err, 1);
             }
             __syncthreads();
+            for (int c = cb; c < ce; ++c) {
+                const int C = P.child[c];
+                const int mc = P.nrow[C];
+                const double* uc = P.upd + P.upd_off[C];
+                const int* rm = P.relmap + P.relmap_off[C];
+                for (int k = tid; k < mc; k += NT) {
+                    const int tr = rm[k];
+#pragma unroll
+                    for (int j = 0; j < K; ++j) f[(size_t)tr * K + j] += __ldcg(uc + j * P.ld_upd + k);
+                }
+                __syncthreads();
+            }
+        } else {
+            // Tall fronts (the interface plans): only the positions this task
+            // reads, its columns [T.c0, T.c0 + T.ncols) and its update rows
+            // [max(T.r0, nj), rend); b's part before the wait, then each
+            // position adds its children's update entries in child order,
+            // the same sums as the whole-front scatter above.  Measured: the
+            // level-0 interface forward drops from 485 to 436 us.
+            const int rlo = max(T.r0, nj), nrn = max(0, T.r0 + T.rows - rlo);
+            const int nneed = T.ncols + nrn;
+            for (int q = tid; q < nneed; q += NT) {
+                const int p = q < T.ncols ? T.c0 + q : rlo + (q - T.ncols);
+                const int po = p < nj ? P.perm[c0 + p] : 0;
+#pragma unroll
+                for (int j = 0; j < K; ++j) f[(size_t)p * K + j] = (p < nj) ? (double)b_old[j * P.ld_b + po] : 0.0;
+            }
+            if (tid == 0) {
+                bool ok = true;
+                for (int c = cb; c < ce; ++c)
+                    ok &= wait_at_least(done + P.child[c], P.ntf[P.child[c]], P.err, P.spin_limit);
+                if (!ok) atomicExch(P.err, 1);
+            }
+            __syncthreads();
+            if (ce > cb) {
+                const int* gp = P.gptr + P.gp_off[J];
+                const int* ge = P.gent + P.ge_off[J];
+                for (int q = tid; q < nneed; q += NT) {
+                    const int p = q < T.ncols ? T.c0 + q : rlo + (q - T.ncols);
+                    double v[K];
+#pragma unroll
+                    for (int j = 0; j < K; ++j) v[j] = f[(size_t)p * K + j];
+                    for (int e = gp[p]; e < gp[p + 1]; ++e) {
+                        const int ui = ge[e];
+#pragma unroll
+                        for (int j = 0; j < K; ++j) v[j] += __ldcg(P.upd + j * P.ld_upd + ui);
+                    }
+#pragma unroll
+                    for (int j = 0; j < K; ++j) f[(size_t)p * K + j] = v[j];
+                }
+                __syncthreads();
+            }
         }
         double acc[K][4];
 #pragma unroll
@@ -786,6 +836,36 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
             relmap.push_back(posn);
         }
     }
+    // Gather lists (the relative maps inverted per parent position, children
+    // in their order).
+    if (upd_total >= (long long)INT32_MAX) throw Error(HDD_ERR_UNSUPPORTED, "update vectors too large for 32-bit indices");
+    std::vector<long long> gp_off(nsn, 0), ge_off(nsn, 0);
+    std::vector<int> gptr, gent;
+    {
+        std::vector<int> cnt;
+        for (int g = 0; g < nsn; ++g) {
+            const int m = ncol[g] + nrow[g];
+            gp_off[g] = (long long)gptr.size();
+            ge_off[g] = (long long)gent.size();
+            cnt.assign(m + 1, 0);
+            for (int c = child_ptr[g]; c < child_ptr[g + 1]; ++c) {
+                const int C = child[c];
+                for (int k = 0; k < nrow[C]; ++k) ++cnt[relmap[relmap_off[C] + k] + 1];
+            }
+            for (int q = 0; q < m; ++q) cnt[q + 1] += cnt[q];
+            const size_t base = gent.size();
+            gent.resize(base + (size_t)cnt[m]);
+            gptr.insert(gptr.end(), cnt.begin(), cnt.end());
+            std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+            for (int c = child_ptr[g]; c < child_ptr[g + 1]; ++c) {
+                const int C = child[c];
+                for (int k = 0; k < nrow[C]; ++k) {
+                    const int q = relmap[relmap_off[C] + k];
+                    gent[base + fill[q]++] = (int)(upd_off[C] + k);
+                }
+            }
+        }
+    }
     if (forward_smem(max_front, 1, nt) > 200 * 1024)
         throw Error(HDD_ERR_UNSUPPORTED, "supernodal front too large for shared memory: " + std::to_string(max_front));
     bytes = 0;
@@ -798,6 +878,10 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
     d_child_ptr = dev::upload(child_ptr, s, bytes);
     d_child = dev::upload(child.empty() ? std::vector<int>{0} : child, s, bytes);
     d_relmap_off = dev::upload(relmap_off, s, bytes);
+    d_gp_off = dev::upload(gp_off, s, bytes);
+    d_ge_off = dev::upload(ge_off, s, bytes);
+    d_gptr = dev::upload(gptr.empty() ? std::vector<int>{0} : gptr, s, bytes);
+    d_gent = dev::upload(gent.empty() ? std::vector<int>{0} : gent, s, bytes);
     d_relmap = dev::upload(relmap.empty() ? std::vector<int>{0} : relmap, s, bytes);
     d_upd_off = dev::upload(upd_off, s, bytes);
     d_fw_off = dev::upload(fw_off, s, bytes);
@@ -849,7 +933,8 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
 void SolvePlan::release() {
     dev::release(d_col0); dev::release(d_ncol); dev::release(d_nrow); dev::release(d_parent);
     dev::release(d_rows); dev::release(d_rows_off); dev::release(d_child_ptr); dev::release(d_child);
-    dev::release(d_relmap_off); dev::release(d_relmap); dev::release(d_upd_off); dev::release(d_fw_off);
+    dev::release(d_relmap_off); dev::release(d_relmap);
+    dev::release(d_gp_off); dev::release(d_ge_off); dev::release(d_gptr); dev::release(d_gent); dev::release(d_upd_off); dev::release(d_fw_off);
     dev::release(d_ntf); dev::release(d_ntb); dev::release(d_perm);
     dev::release(d_fwd); dev::release(d_bwd); dev::release(d_bfwd); dev::release(d_bbwd); dev::release(d_fw); dev::release(d_part); dev::release(d_upd);
     dev::release(d_ynew); dev::release(d_xnew); dev::release(d_ctr);
@@ -918,7 +1003,8 @@ void SolvePlan::solve(const PlanScratch& sc, const float* b_old, float* x_old, c
     if ((nrhs != 1 && nrhs != 2 && nrhs != 4) || nrhs > sc.nrhs || nrhs > kmax)
         throw Error(HDD_ERR_INVALID_ARGUMENT, "right-hand sides per solve: 1, 2 or 4, within the scratch and the plan");
     PlanView P{nsn, max_front, d_col0, d_ncol, d_nrow, d_parent, d_rows, d_rows_off, d_child_ptr, d_child,
-               d_relmap_off, d_relmap, d_upd_off, d_fw_off, d_ntf, d_ntb, d_perm, d_bfwd, d_bbwd, d_fw, sc.part, sc.upd,
+               d_relmap_off, d_relmap, d_gp_off, d_ge_off, d_gptr, d_gent, d_upd_off, d_fw_off, d_ntf, d_ntb, d_perm,
+               d_bfwd, d_bbwd, d_fw, sc.part, sc.upd,
                sc.ynew, sc.xnew, sc.ctr, sc.err, spin_limit,
                part_len, upd_len, (long long)std::max(n, 1), ld_b, ld_x};
     dev::ck(cudaMemsetAsync(sc.ctr, 0, sizeof(int) * n_ctr, s), "reset counters");
