@@ -6,7 +6,10 @@ already initialised) of the workload's domain.  The default workload is the
 256^3-cell domain with a Dirichlet sphere and 32^3 subdomains (sub_size 32,
 vlevels 4, interior/boundary smoothing 4, sigma_levels 4, sigma_mg 1);
 ``--config c1`` selects the 64^3-cell, 16^3-subdomain case; ``c5`` the sparse
-1024^3-cell sphere union (``c5_half`` the same shape at 512^3).
+1024^3-cell sphere union (``c5_half`` the same shape at 512^3); ``c2ml`` the
+256^3 domain under two-level DD (the reference's -multilevel yes) at the
+two-level demo's defaults (64^3 subdomains split into 32^3 boxes, vlevels 3,
+smoothing 1/3, sigma_levels 3), ``tl128`` the same settings at 128^3.
 
 ``--impl reference`` times the CPU restatement of the reference dd_pcg path
 (the oracle) on the host cores instead.
@@ -39,7 +42,8 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--config", choices=["c1", "c2", "c3", "p128", "c4", "c5", "c5_half"], default="c2",
+    p.add_argument("--config", choices=["c1", "c2", "c3", "p128", "c4", "c5", "c5_half", "c2ml", "tl128"],
+                   default="c2",
                    help="c4 = serving: resident uneven domains, solve requests through hdd_server_*")
     p.add_argument("--domains", type=int, default=4, help="c4: resident domains")
     p.add_argument("--requests", type=int, default=32, help="c4: requests per timed run")
@@ -146,7 +150,7 @@ def one_solve(args):
     t0 = time.time()
     s.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"],
                                 m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"],
-                                m["sigma_mg"], tol=1e-6)
+                                m["sigma_mg"], tol=1e-6, multilevel=m.get("multilevel", False))
     print(f"{d.name}: setup {time.time() - t0:.1f} s", flush=True)
     lib = _lib.load()
     lib.hdd_set_kernel_timing(s.h, 1)
@@ -190,18 +194,24 @@ def measured_traffic(kernel, workload):
 def oracle_iterations(cfg):
     """PCG iterations of the oracle's full solve of a workload at 1e-6 relative
     residual, with where the count comes from: the committed fixture made by
-    tests/golden/make_c2_fixture.py (a full FP32 oracle run) for c2, None for
+    tests/golden/make_c2_fixture.py (a full FP32 oracle run) for c2, by
+    tests/golden/make_two_level_fixture.py for c2ml and tl128, None for
     workloads whose oracle samples are whole solves."""
     if cfg == "c2":
         path = os.path.join(ROOT, "tests", "golden", "c2_oracle.npz")
         if os.path.exists(path):
             return int(np.load(path)["iterations_fp32"]), "tests/golden/c2_oracle.npz (full FP32 oracle solve)"
+    if cfg in ("c2ml", "tl128"):
+        path = os.path.join(ROOT, "tests", "golden", "two_level_oracle.npz")
+        if os.path.exists(path):
+            return (int(np.load(path)[f"{cfg}_iterations_fp32"]),
+                    "tests/golden/two_level_oracle.npz (full FP32 oracle solve)")
     return None, None
 
 
 # PCG iterations of the bounded CPU sample in the GPU arm's line: whole solves
 # where one takes seconds, else a few iterations scaled by the oracle's count.
-SAMPLE_ITERATIONS = {"c1": None, "c2": 2, "p128": 4}
+SAMPLE_ITERATIONS = {"c1": None, "c2": 2, "p128": 4, "c2ml": 1, "tl128": 4}
 
 
 def make_oracle(d):
@@ -210,7 +220,8 @@ def make_oracle(d):
     m = d.meta
     return Oracle(d.size, d.sub_size, d.flags, vlevels=m["vlevels"], nVcycles=m["nVcycles"],
                   interior_smoothing=m["interior_smoothing"], boundary_smoothing=m["boundary_smoothing"],
-                  sigma_levels=m["sigma_levels"], sigma_smoothing=m["sigma_smoothing"], sigma_mg=m["sigma_mg"])
+                  sigma_levels=m["sigma_levels"], sigma_smoothing=m["sigma_smoothing"], sigma_mg=m["sigma_mg"],
+                  multilevel=m.get("multilevel", False))
 
 
 def precision_mode(args, d):
@@ -227,6 +238,7 @@ def config_dict(d, args, world=1):
             "boundary_smoothing": m["boundary_smoothing"], "sigma_levels": m["sigma_levels"],
             "sigma_smoothing": m["sigma_smoothing"], "sigma_mg": m["sigma_mg"], "tol": 1e-6,
             "precision": "mixed" if precision_mode(args, d) == 1 else "reference",
+            "multilevel": bool(m.get("multilevel", False)),
             "l2": "working set > L2 (no flush)", "parallelism": f"replicas{world}"}
 
 
@@ -235,10 +247,12 @@ def level0_updates_per_iteration(d):
     the Laplacian of q = A s, plus per V-cycle 2 x (boundary + interior +
     boundary) smoothing sweeps (each computes the residual over every active
     cell) and the residual before restriction, for the 2 x nVcycles V-cycles
-    of one preconditioner application.  Coarse levels are not counted."""
+    of one preconditioner application (4 x nVcycles under two-level DD, whose
+    subdomain solves run V-cycles twice each).  Coarse levels are not counted."""
     m = d.meta
     per_vcycle = 2 * (2 * m["boundary_smoothing"] + m["interior_smoothing"]) + 1
-    return 1 + 2 * m["nVcycles"] * per_vcycle
+    passes = 4 if m.get("multilevel") else 2
+    return 1 + passes * m["nVcycles"] * per_vcycle
 
 
 def cpu_baseline(args, d):
@@ -635,7 +649,8 @@ def main():
     s.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"],
                                 m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"],
                                 m["sigma_mg"], tol=1e-6, precision_mode=precision_mode(args, d),
-                                true_residual_every=int(m.get("true_residual_every", 20)))
+                                true_residual_every=int(m.get("true_residual_every", 20)),
+                                multilevel=m.get("multilevel", False))
     setup_s = time.time() - t0
     try:
         setup_phases = s.Setup_Timing()
@@ -702,8 +717,9 @@ def main():
     # Roofline (HBM-bound kernels) of every timed kernel; the dominant one by
     # device time is the headline.
     hbm, peak_kind = peaks()
-    kernels = {0: "vcycle_cluster_kernel" if d.sub_size[0] == 32 else "vcycle_kernel",
-               1: "laplace_dot_march_kernel" if d.sub_size[0] in (8, 16, 32) else "laplace_dot_kernel",
+    vbox = d.sub_size[0] // 2 if m.get("multilevel") else d.sub_size[0]  # V-cycle box and tile edge
+    kernels = {0: "vcycle_cluster_kernel" if vbox == 32 else "vcycle_kernel",
+               1: "laplace_dot_march_kernel" if vbox in (8, 16, 32) else "laplace_dot_kernel",
                6: "sn_forward_kernel", 7: "sn_backward_kernel"}
     per_kernel = {}
     for i, kname in kernels.items():

@@ -33,7 +33,7 @@ class hdd_options(C.Structure):
         ("sigma_smoothing", C.c_int), ("sigma_mg", C.c_int), ("tol", C.c_double), ("relative_tol", C.c_int),
         ("max_iters", C.c_int), ("min_iters", C.c_int), ("precision_mode", C.c_int),
         ("true_residual_every", C.c_int), ("device", C.c_int), ("coarse_solve", C.c_int),
-        ("solve_share", C.c_int),
+        ("solve_share", C.c_int), ("multilevel", C.c_int),
     ]
 
 

@@ -25,6 +25,7 @@ SOURCES = [
     "capi.cpp",
     "server.cpp",
     "kernels_vcycle.cu",
+    "kernels_vcycle_global.cu",
     "kernels_pcg.cu",
     "sigma.cu",
     "sn_plan.cpp",

@@ -96,6 +96,7 @@ void hdd_options_default(hdd_options* o) {
     o->device = 0;
     o->coarse_solve = HDD_COARSE_REFERENCE;
     o->solve_share = 0;
+    o->multilevel = 0;
 }
 
 hdd_status hdd_create(const hdd_options* opts, hdd_solver** out) {
@@ -376,6 +377,7 @@ hdd_status hdd_set_wait_limit(hdd_solver* s, long long polls) {
         v.sync();
         v.release_graphs();  // the limit is a launch parameter of the captured solves
         v.sigma.set_wait_limit(polls);
+        v.sigma2.set_wait_limit(polls);
     });
 }
 

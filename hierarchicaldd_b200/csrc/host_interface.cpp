@@ -910,4 +910,108 @@ void build_interface(const DomainLayout& L, int M, InterfaceHost& out) {
     }
 }
 
+void build_second_level(const DomainLayout& L, const int sub[3], int M, InterfaceHost& out) {
+    // Two-level DD (TWO/SPGrid_Domain_Decomposition_Solver/SPGrid_Subdomain_Splitter.h:168-193):
+    // every first-level subdomain box [lo, lo + sub] gets its own interface
+    // system, from the caller's flags with the Active cells on the
+    // first-level planes made Dirichlet (Domain_Divider with clear_flag),
+    // split at sub/2.  Each box is assembled as a grid of its own (origin lo,
+    // a multiple of sub, so the plane tests are the global ones); the
+    // systems with a level-0 interface are then stacked in box order (x
+    // slowest) into one block-diagonal system.  They are not assembled as
+    // one grid: coarse interface nodes on a first-level plane would then be
+    // shared by the boxes on either side.
+    const int* size = L.opt.size;
+    int ns[3], sub2[3];
+    number_of_subdomains(size, sub, ns);
+    for (int a = 0; a < 3; ++a) sub2[a] = sub[a] / 2;
+    const int nbox = ns[0] * ns[1] * ns[2];
+    std::vector<InterfaceHost> part(nbox);
+    std::vector<std::array<int, 3>> lo(nbox);
+    std::vector<std::string> errors(nbox);
+#pragma omp parallel for schedule(dynamic)
+    for (int s = 0; s < nbox; ++s) {
+        try {
+            const int b[3] = {s / (ns[1] * ns[2]), (s / ns[2]) % ns[1], s % ns[2]};
+            DomainLayout Ls;
+            Ls.opt = L.opt;
+            for (int a = 0; a < 3; ++a) {
+                lo[s][a] = b[a] * sub[a];
+                Ls.opt.size[a] = std::min(sub[a] + 1, size[a] - lo[s][a]);
+                Ls.opt.sub[a] = sub2[a];
+            }
+            const int* ld = Ls.opt.size;
+            Ls.flags_in.assign((size_t)ld[0] * ld[1] * ld[2], 0u);
+            for (int x = 0; x < ld[0]; ++x)
+                for (int y = 0; y < ld[1]; ++y)
+                    for (int z = 0; z < ld[2]; ++z)
+                        Ls.flags_in[((size_t)x * ld[1] + y) * ld[2] + z] =
+                            L.flags_in[L.dense_index(lo[s][0] + x, lo[s][1] + y, lo[s][2] + z)];
+            clear_planes(ld, sub, Ls.flags_in.data());
+            build_interface(Ls, M, part[s]);
+        } catch (const std::exception& e) {
+            errors[s] = e.what();
+        }
+    }
+    for (auto& e : errors)
+        if (!e.empty()) throw Error(HDD_ERR_UNSUPPORTED, "second-level interface assembly: " + e);
+    out = InterfaceHost();
+    out.M = M;
+    out.n_iface.assign(M, 0);
+    out.Arr.assign(M, CsrF());
+    out.Aii.assign(M, {});
+    out.Air.assign(M, {});
+    out.iface_xyz.assign(M, {});
+    out.aii_xyz.assign(M, {});
+    out.Prr.assign(M > 1 ? M - 1 : 0, CsrF());
+    auto append = [](CsrF& A, const CsrF& B, int col0) {
+        // B's rows appended to A's, its columns shifted by col0.
+        if (A.ptr.empty()) A.ptr.assign(1, 0);
+        for (int r = 0; r < B.rows; ++r) {
+            for (int p = B.ptr[r]; p < B.ptr[r + 1]; ++p) {
+                A.col.push_back(B.col[p] + col0);
+                A.val.push_back(B.val[p]);
+            }
+            A.ptr.push_back((int)A.col.size());
+        }
+    };
+    for (int s = 0; s < nbox; ++s) {
+        const InterfaceHost& P = part[s];
+        if (P.n_iface.empty() || P.n_iface[0] == 0) continue;
+        if (P.M != M) throw Error(HDD_ERR_INTERNAL, "second-level system with another level count");
+        const std::array<int, 3>& o = lo[s];
+        std::vector<int> off(M);
+        for (int m = 0; m < M; ++m) off[m] = out.n_iface[m];
+        for (const auto& c : P.iface_map) out.iface_map.push_back({c[0] + o[0], c[1] + o[1], c[2] + o[2]});
+        for (int m = 0; m < M; ++m) {
+            append(out.Arr[m], P.Arr[m], off[m]);
+            if (m + 1 < M) append(out.Prr[m], P.Prr[m], off[m + 1]);
+            for (const auto& x : P.iface_xyz[m]) out.iface_xyz[m].push_back({x[0] + o[0], x[1] + o[1], x[2] + o[2]});
+            for (int b = 0; b < P.n_sub; ++b) {
+                out.Aii[m].push_back(P.Aii[m][b]);
+                CsrF air;
+                air.rows = P.Air[m][b].rows;
+                append(air, P.Air[m][b], off[m]);
+                out.Air[m].push_back(std::move(air));
+                std::vector<std::array<int, 3>> xyz;
+                for (const auto& x : P.aii_xyz[m][b]) xyz.push_back({x[0] + o[0], x[1] + o[1], x[2] + o[2]});
+                out.aii_xyz[m].push_back(std::move(xyz));
+            }
+            out.n_iface[m] += P.n_iface[m];
+        }
+        out.n_sub += P.n_sub;
+    }
+    for (int m = 0; m < M; ++m) {
+        out.Arr[m].rows = out.Arr[m].cols = out.n_iface[m];
+        if (out.Arr[m].ptr.empty()) out.Arr[m].ptr.assign(1, 0);
+        for (auto& A : out.Air[m]) A.cols = out.n_iface[m];
+        if (m + 1 < M) {
+            CsrF& Pm = out.Prr[m];
+            Pm.rows = out.n_iface[m];
+            Pm.cols = out.n_iface[m + 1];
+            if (Pm.ptr.empty()) Pm.ptr.assign(1, 0);
+        }
+    }
+}
+
 }  // namespace hdd

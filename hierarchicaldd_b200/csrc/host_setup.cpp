@@ -36,6 +36,19 @@ void divide_domain(const int size[3], const int sub[3], uint32_t* f) {
             }
 }
 
+void clear_planes(const int size[3], const int sub[3], uint32_t* f) {
+    // Domain_Divider with clear_flag (two-level demo,
+    // TWO/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Divider_Helper.h:61-72):
+    // Active cells on planes index % sub == 0 become Dirichlet, nothing else.
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < size[0]; ++i)
+        for (int j = 0; j < size[1]; ++j)
+            for (int k = 0; k < size[2]; ++k) {
+                uint32_t& v = f[at3(size, i, j, k)];
+                if ((v & F_ACTIVE) && (i % sub[0] == 0 || j % sub[1] == 0 || k % sub[2] == 0)) v = F_DIRICHLET;
+            }
+}
+
 void flag_faces(const int n[3], uint32_t* f) {
     // SPGrid_Flag_Helper.h:74-106.
 #pragma omp parallel for schedule(static)
@@ -118,10 +131,6 @@ void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& L) {
     L.flags_in.assign(flags, flags + N);
     L.flags0 = L.flags_in;
     const int* n = opt.size;
-    // Input check: an exterior cell (no type bit) may not touch an Active cell
-    // across a face.  This is the rule the reference generator enforces for
-    // Dirichlet layers (Create_3D_Domain/main.cpp:126-140); it keeps the
-    // per-subdomain V-cycles of the GPU path decoupled at every coarse level.
     {
         long long active = 0;
 #pragma omp parallel for schedule(static) reduction(+ : active)
@@ -134,18 +143,12 @@ void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& L) {
         for (int i = 0; i < n[0]; ++i)
             for (int j = 0; j < n[1]; ++j)
                 for (int k = 0; k < n[2]; ++k) {
-                    uint32_t v = L.flags0[at3(n, i, j, k)];
-                    if (v & (F_INTERFACE | F_BOUNDARY)) { ++bad; continue; }
-                    if (v & (F_ACTIVE | F_DIRICHLET)) continue;
-                    for (int q = 0; q < 6; ++q) {
-                        int a = i + kFace[q][0], b = j + kFace[q][1], c = k + kFace[q][2];
-                        if (in3(n, a, b, c) && (L.flags0[at3(n, a, b, c)] & F_ACTIVE)) { ++bad; break; }
-                    }
+                    if (L.flags0[at3(n, i, j, k)] & (F_INTERFACE | F_BOUNDARY)) ++bad;
                 }
         if (bad)
-            throw Error(HDD_ERR_UNSUPPORTED,
-                        "domain has exterior cells face-adjacent to Active cells (or pre-set Interface/"
-                        "Boundary bits): " + std::to_string(bad) + " cells");
+            throw Error(HDD_ERR_INVALID_ARGUMENT,
+                        "input flags carry Interface or Boundary bits (set by the solver): " + std::to_string(bad) +
+                            " cells");
     }
     // Reference order: global Domain_Divider, Flaging, then the topology's
     // Flaging (faces again) and Flaging_Boundary on level 0.
@@ -183,8 +186,40 @@ void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& L) {
                 if (s >= 0) L.tile_flags[s] = compact16(L.flags0[at3(n, i, j, k)]);
             }
 
-    // Per-box V-cycle levels.
+    // Whole-grid levels (CPU/SPGrid_Domain_Decomposition_Solver/SPGrid_V_Cycle_Topology.h:35-178):
+    // level l+1 has n/2+1 cells per axis; a coarse cell is Dirichlet if a
+    // child (2c-1, 2c) is Dirichlet or Interface, else Active if a child is
+    // Active; then Flaging and Flaging_Boundary.
     const int V = opt.vlevels;
+    L.g_dims.assign(V, {0, 0, 0});
+    L.g_flags.assign(V, {});
+    {
+        std::vector<uint32_t> fine = L.flags0, coarse;
+        std::array<int, 3> fd = {n[0], n[1], n[2]};
+        for (int l = 0; l < V; ++l) {
+            if (l > 0) {
+                const std::array<int, 3> cd = {fd[0] / 2 + 1, fd[1] / 2 + 1, fd[2] / 2 + 1};
+                coarse.assign((size_t)cd[0] * cd[1] * cd[2], 0u);
+                for (int i = 0; i < fd[0]; ++i)
+                    for (int j = 0; j < fd[1]; ++j)
+                        for (int k = 0; k < fd[2]; ++k) {
+                            const uint32_t v = fine[at3(fd.data(), i, j, k)];
+                            uint32_t& c = coarse[at3(cd.data(), (i + 1) / 2, (j + 1) / 2, (k + 1) / 2)];
+                            if (v & (F_DIRICHLET | F_INTERFACE)) c = F_DIRICHLET;
+                            else if ((v & F_ACTIVE) && c != F_DIRICHLET) c = F_ACTIVE;
+                        }
+                flag_faces(cd.data(), coarse.data());
+                flag_boundary(cd.data(), coarse.data());
+                fine.swap(coarse);
+                fd = cd;
+            }
+            L.g_dims[l] = fd;
+            L.g_flags[l].resize(fine.size());
+            for (size_t x = 0; x < fine.size(); ++x) L.g_flags[l][x] = compact8(fine[x]);
+        }
+    }
+
+    // Per-box V-cycle levels.
     L.level_e.assign(3 * V, 0);
     L.level_off.assign(V + 1, 0);
     for (int l = 0; l < V; ++l) {
@@ -220,8 +255,7 @@ void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& L) {
                 L.boxes.push_back(bx);
             }
     L.box_flags.assign(L.boxes.size() * L.box_stride, 0);
-    // Set inside the parallel loop, thrown after it: an exception may not
-    // leave an OpenMP region.
+    // Set inside the parallel loop: a box level that is not the whole grid's.
     int coupled = 0;
 #pragma omp parallel for schedule(dynamic)
     for (long long bi = 0; bi < (long long)L.boxes.size(); ++bi) {
@@ -258,13 +292,21 @@ void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& L) {
                     }
             flag_faces(ce, coarse.data());
             flag_boundary(ce, coarse.data());
-            // Halo planes of a coarse box are never Active under the input check;
-            // verify, since the per-box V-cycle relies on it.
+            // The box's level must be the whole grid's inside the box (flags,
+            // faces, Boundary band), and its box-face cells, which the
+            // per-box V-cycle keeps at zero, must not be Active there.
+            const std::array<int, 3>& gd = L.g_dims[l];
+            const std::vector<uint8_t>& gf = L.g_flags[l];
+            const int o[3] = {bx.k[0] * (opt.sub[0] >> l), bx.k[1] * (opt.sub[1] >> l), bx.k[2] * (opt.sub[2] >> l)};
             for (int x = 0; x < ce[0]; ++x)
                 for (int y = 0; y < ce[1]; ++y)
                     for (int z = 0; z < ce[2]; ++z) {
-                        bool halo = x == 0 || y == 0 || z == 0 || x == ce[0] - 1 || y == ce[1] - 1 || z == ce[2] - 1;
-                        if (halo && (coarse[at3(ce, x, y, z)] & F_ACTIVE)) {
+                        const int gx = o[0] + x, gy = o[1] + y, gz = o[2] + z;
+                        const bool halo = x == 0 || y == 0 || z == 0 || x == ce[0] - 1 || y == ce[1] - 1 || z == ce[2] - 1;
+                        const bool inside = gx < gd[0] && gy < gd[1] && gz < gd[2];
+                        const uint8_t g = inside ? gf[at3(gd.data(), gx, gy, gz)] : 0;
+                        const bool bad = halo ? (g & C_ACTIVE) != 0 : g != compact8(coarse[at3(ce, x, y, z)]);
+                        if (bad) {
 #pragma omp atomic write
                             coupled = 1;
                         }
@@ -275,7 +317,11 @@ void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& L) {
             for (int a = 0; a < 3; ++a) fe[a] = ce[a];
         }
     }
-    if (coupled) throw Error(HDD_ERR_UNSUPPORTED, "coarse level couples subdomains");
+    L.global_vcycle = coupled != 0;
+    if (!L.global_vcycle) {
+        L.g_dims.clear();
+        L.g_flags.clear();
+    }
 }
 
 void dense_to_tiles(const DomainLayout& L, const float* dense, float* tiled) {

@@ -47,6 +47,16 @@ struct DomainLayout {
     std::vector<size_t> level_off;            // offset of level l inside a box record
     size_t box_stride = 0;
     std::vector<uint8_t> box_flags;           // boxes.size() * box_stride
+    // Whole-grid levels (V_Cycle_Topology on the whole grid): dims and
+    // compact8 flags.  global_vcycle is set when a box's levels differ from
+    // the whole grid's inside the box, or a box-face cell of a coarse level
+    // is Active there: the boxes' V-cycles would then not be the reference's
+    // (an exterior region touching Active cells, as the reference
+    // generator's Neumann bubble, couples boxes at coarse levels), and the
+    // whole-grid V-cycle runs instead.
+    bool global_vcycle = false;
+    std::vector<std::array<int, 3>> g_dims;
+    std::vector<std::vector<uint8_t>> g_flags;
 
     size_t cell_count() const { return (size_t)opt.size[0] * opt.size[1] * opt.size[2]; }
     size_t dense_index(int i, int j, int k) const {
@@ -88,6 +98,9 @@ void dense_to_pages(const int size[3], long long n, const int32_t* origin, const
 
 // Level-0 flag pipeline pieces (same semantics as the reference passes).
 void divide_domain(const int size[3], const int sub[3], uint32_t* f);
+// Two-level DD: Active cells on the first-level planes (index % sub == 0)
+// become Dirichlet, the flags of a first-level subdomain's own DD.
+void clear_planes(const int size[3], const int sub[3], uint32_t* f);
 void flag_faces(const int n[3], uint32_t* f);
 void flag_boundary(const int n[3], uint32_t* f);
 void number_of_subdomains(const int size[3], const int sub[3], int out[3]);

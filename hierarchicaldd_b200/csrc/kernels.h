@@ -28,6 +28,13 @@ struct VcycleArgs {
     const uint8_t* box_flags;  // per-box flag records (all levels)
     const int* box_tile;       // [nbox]
     const int* box_nb;         // [nbox*3] +x/+y/+z neighbour tiles (-1 absent)
+    // Optional (null = zero): the level-0 residual at the box's lower-face
+    // cells (x, y or z = 0), which the V-cycle never computes there but the
+    // first restriction reads (its stencil reaches box cells 0 .. sub-1).
+    // The reference's V-cycle reads its residual channel there, and two-level
+    // DD leaves Laplace_ir_Subdomain values in it
+    // (TWO/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Decomposition_Preconditioner.h:131-137).
+    const float* r_halo;
     int nbox;
     int sub;                   // cubic subdomain edge
     int levels;
@@ -48,6 +55,38 @@ struct VcycleArgs {
 };
 
 cudaError_t launch_vcycle(const VcycleArgs& a, cudaStream_t stream);
+
+// The V-cycle's float constants (as in VcycleArgs).
+struct VcycleWeights {
+    float inv_diag[8];
+    float restrict_w[64];
+    float prolong_w[8];
+};
+
+struct TileGeom;
+
+// Whole-grid V-cycle (kernels_vcycle_global.cu), for domains whose coarse
+// levels couple subdomain boxes: level l is a dense x-slowest grid of
+// dims[l] cells with compact8 flags f[l]; u, b, r are its vectors (level 0
+// staged from and back to the tiled vectors).  Coarse r must be zero where a
+// level is not Active (allocated zeroed; never written there).
+struct GlobalVcycleArgs {
+    int levels;
+    int dims[kMaxLevels][3];
+    const uint8_t* f[kMaxLevels];
+    float* u[kMaxLevels];
+    float* b[kMaxLevels];
+    float* r[kMaxLevels];
+    int n_vcycles, interior_itr, boundary_itr, bottom_itr;
+    int halo_from_u, zero_init;   // as in VcycleArgs
+    VcycleWeights w;
+};
+// Runs the V-cycles on the tiled u (read as VcycleArgs says, Active and other
+// non-Interface cells written back) and b; r_halo (nullable) gives the
+// level-0 residual where none is computed (as VcycleArgs::r_halo).  Returns
+// the launches issued; throws hdd::Error on a launch error.
+long long launch_vcycle_global(const GlobalVcycleArgs& a, const TileGeom& g, const int* tile_xyz, float* u,
+                               const float* b, const float* r_halo, cudaStream_t stream);
 
 // ---------------------------------------------------------------------------
 // PCG kernels over tiled vectors
@@ -121,11 +160,19 @@ cudaError_t launch_tiles_to_dense_f64(const TileGeom& g, const int* tile_xyz, in
 // ---------------------------------------------------------------------------
 // Interface coupling (Laplace_ri gather and the interface scatter)
 // ---------------------------------------------------------------------------
-// b0[i] = r[c_i] - (float)(-sum over active-face Active neighbours of z)  at Interface cells.
+// With s_i = (float)(-sum of z over the cell's listed neighbour slots, in
+// FP64, face order -x,+x,-y,+y,-z,+z), at the listed cells c_i:
+//   kGatherRi    b0[i] = r[c_i] - s_i        (Laplace_ri / Laplace_ri_Subdomain, then the copy)
+//   kGatherIr    b0[i] = -s_i                (Laplace_ir_Subdomain, then the copy)
+//   kGatherRiAdd b0[i] = b0[i] + (r[c_i] - s_i)  (Laplace_ri, then Accumulate_To_Eigen_Array)
+//   kGatherIrTiled b0[c_i] = -s_i            (Laplace_ir_Subdomain into a tiled vector b0)
+// The neighbour lists choose which neighbours count (-1 = none).
 // Batched: system j's r and z at + j * B.vstride, its b0 at + j * istride.
+enum { kGatherRi = 0, kGatherIr = 1, kGatherRiAdd = 2, kGatherIrTiled = 3 };
 cudaError_t launch_interface_gather(const TileGeom& g, const long long* iface_slot, const int* iface_nb_slots,
                                     int n_iface, const float* r, const float* z, float* b0,
-                                    cudaStream_t stream, const Batch& B = Batch(), size_t istride = 0);
+                                    cudaStream_t stream, const Batch& B = Batch(), size_t istride = 0,
+                                    int mode = kGatherRi);
 // z[c_i] = u0[i].
 cudaError_t launch_interface_scatter(const long long* iface_slot, int n_iface, const float* u0, float* z,
                                      cudaStream_t stream, const Batch& B = Batch(), size_t istride = 0);

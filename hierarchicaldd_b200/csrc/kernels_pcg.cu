@@ -438,6 +438,7 @@ __global__ void scalar_alpha_kernel(PcgScalars* sc, const double* sdq_sum, Batch
     if (!isfinite(sd) || !isfinite(sc->alpha)) sc->status = 1;
 }
 
+template <int MODE>
 __global__ void __launch_bounds__(kNT) interface_gather_kernel(const long long* slot, const int* nbs, int n,
                                                                const float* r, const float* z, float* b0,
                                                                size_t vstride, size_t istride) {
@@ -452,7 +453,10 @@ __global__ void __launch_bounds__(kNT) interface_gather_kernel(const long long* 
         const int s = nbs[6 * i + q];
         if (s >= 0) result -= (double)z[s];
     }
-    b0[i] = __fsub_rn(r[slot[i]], (float)result);
+    if (MODE == kGatherIr) b0[i] = -(float)result;
+    else if (MODE == kGatherIrTiled) b0[slot[i]] = -(float)result;
+    else if (MODE == kGatherRiAdd) b0[i] = __fadd_rn(b0[i], __fsub_rn(r[slot[i]], (float)result));
+    else b0[i] = __fsub_rn(r[slot[i]], (float)result);
 }
 
 __global__ void __launch_bounds__(kNT) interface_scatter_kernel(const long long* slot, int n, const float* u0,
@@ -593,10 +597,18 @@ cudaError_t launch_scalar_alpha(PcgScalars* sc, const double* sdq_sum, cudaStrea
     return cudaGetLastError();
 }
 cudaError_t launch_interface_gather(const TileGeom&, const long long* slot, const int* nbs, int n, const float* r,
-                                    const float* z, float* b0, cudaStream_t st, const Batch& B, size_t istride) {
+                                    const float* z, float* b0, cudaStream_t st, const Batch& B, size_t istride,
+                                    int mode) {
     if (n == 0) return cudaSuccess;
-    interface_gather_kernel<<<dim3((n + kNT - 1) / kNT, B.k), kNT, 0, st>>>(slot, nbs, n, r, z, b0, B.vstride,
-                                                                            istride);
+    const dim3 grid((n + kNT - 1) / kNT, B.k);
+    if (mode == kGatherIr)
+        interface_gather_kernel<kGatherIr><<<grid, kNT, 0, st>>>(slot, nbs, n, r, z, b0, B.vstride, istride);
+    else if (mode == kGatherRiAdd)
+        interface_gather_kernel<kGatherRiAdd><<<grid, kNT, 0, st>>>(slot, nbs, n, r, z, b0, B.vstride, istride);
+    else if (mode == kGatherIrTiled)
+        interface_gather_kernel<kGatherIrTiled><<<grid, kNT, 0, st>>>(slot, nbs, n, r, z, b0, B.vstride, istride);
+    else
+        interface_gather_kernel<kGatherRi><<<grid, kNT, 0, st>>>(slot, nbs, n, r, z, b0, B.vstride, istride);
     return cudaGetLastError();
 }
 cudaError_t launch_interface_scatter(const long long* slot, int n, const float* u0, float* z, cudaStream_t st,

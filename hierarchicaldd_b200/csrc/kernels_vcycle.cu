@@ -58,6 +58,13 @@ __device__ __forceinline__ float cell_residual(const LevelSmem& L, int i, uint32
     return __fsub_rn(L.b[i], res);
 }
 
+// Value of a tiled level-0 vector at box cell (x, y, z), 0 <= x, y, z < SUB
+// (the box's own tile).
+template <int SUB>
+__device__ __forceinline__ float own_tile_value(const float* v, int tile, int x, int y, int z) {
+    return v[(size_t)tile * (SUB * SUB * SUB) + (x * SUB + y) * SUB + z];
+}
+
 // Interior cell q (0 .. (e-2)^3-1) -> box index.
 __device__ __forceinline__ int interior_cell(int e, int q) {
     const int m = e - 2;
@@ -432,6 +439,14 @@ __global__ void __launch_bounds__(NT, 1) vcycle_kernel(VcycleArgs a) {
             }
         }
     }
+    // Residual at the lower-face cells, when given (else it stays zero).
+    if (a.r_halo) {
+        const float* rh = a.r_halo + (size_t)blockIdx.y * a.slot_stride;
+        for (int q = threadIdx.x; q < SUB * SUB * SUB; q += NT) {
+            const int z = q % SUB, t = q / SUB, y = t % SUB, x = t / SUB;
+            if (x == 0 || y == 0 || z == 0) lv[0].r[box_index(E0, x, y, z)] = own_tile_value<SUB>(rh, tile, x, y, z);
+        }
+    }
     __syncthreads();
 
     const int Lm = a.levels;
@@ -626,7 +641,11 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
             fv = rec[box_index(E, x, y, z)];
         }
         b0[q] = bv;
-        r0[q] = 0.0f;
+        // Residual: zero, or the given values at the lower y/z box faces.
+        float rv = 0.0f;
+        if (a.r_halo && k < np && (y == 0 || z == 0) && y < SUB && z < SUB)
+            rv = own_tile_value<SUB>(a.r_halo + (size_t)blockIdx.y * a.slot_stride, tile, x, y, z);
+        r0[q] = rv;
         f0[q] = fv;
     }
     if (rank == 0) {
@@ -786,13 +805,18 @@ __global__ void __launch_bounds__(NT, 1) vcycle_cluster_kernel(VcycleArgs a) {
 #pragma unroll
                 for (int i2 = 0; i2 < 4; ++i2) {
                     const int x = 2 * cx - 2 + i2;
+                    // x = 0 is no slab's plane; x <= SUB - 1 here (cx <= SUB/2 - 1).
                     const int owner = (x - 1) / P;           // x >= 1 when owner is used
                     const float* rp = (x == 0) ? nullptr : r0r[owner] + (x - 1 - owner * P) * PS;
 #pragma unroll
                     for (int j2 = 0; j2 < 4; ++j2)
 #pragma unroll
                         for (int k2 = 0; k2 < 4; ++k2) {
-                            const float v = rp ? rp[(2 * cy - 2 + j2) * E + (2 * cz - 2 + k2)] : 0.0f;
+                            const int y = 2 * cy - 2 + j2, z = 2 * cz - 2 + k2;
+                            float v = 0.0f;
+                            if (rp) v = rp[y * E + z];
+                            else if (a.r_halo)
+                                v = own_tile_value<SUB>(a.r_halo + (size_t)blockIdx.y * a.slot_stride, tile, 0, y, z);
                             acc = __fadd_rn(acc, __fmul_rn(s_sc64[(i2 * 4 + j2) * 4 + k2], v));
                         }
                 }

@@ -44,6 +44,11 @@ struct InterfaceHost {
 // subdomains.
 void build_interface(const DomainLayout& L, int sigma_levels, InterfaceHost& out);
 
+// Two-level DD: the second-level interface systems of every first-level
+// subdomain of sub cells (L.opt.size and L.flags_in are read), stacked into
+// one block-diagonal system on boxes of sub/2.
+void build_second_level(const DomainLayout& L, const int sub[3], int sigma_levels, InterfaceHost& out);
+
 // Interface dump and reload, the reference's -iomode output / input
 // (CPU/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Decomposition_Solver.h:121-161);
 // host_interface_io.cpp.  read_interface_dir throws HDD_ERR_IO on a missing or

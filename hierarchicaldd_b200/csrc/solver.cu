@@ -28,7 +28,9 @@ namespace hdd {
 
 static Options to_options(const hdd_options& o) {
     Options p;
-    for (int a = 0; a < 3; ++a) { p.size[a] = o.size[a]; p.sub[a] = o.sub_size[a]; }
+    // Two-level DD runs its V-cycles on boxes of sub_size/2
+    // (TWO/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Decomposition_Solver.h:129-145).
+    for (int a = 0; a < 3; ++a) { p.size[a] = o.size[a]; p.sub[a] = o.multilevel ? o.sub_size[a] / 2 : o.sub_size[a]; }
     p.vlevels = o.vlevels;
     p.nvcycles = o.nVcycles;
     p.interior = o.interior_smoothing;
@@ -49,6 +51,12 @@ Solver::Solver(const hdd_options& o) : opts(o) {
     if (o.solve_share < 0 || o.solve_share > 64) throw Error(HDD_ERR_INVALID_ARGUMENT, "solve_share out of range");
     if (o.coarse_solve != HDD_COARSE_REFERENCE && o.coarse_solve != HDD_COARSE_EXACT)
         throw Error(HDD_ERR_INVALID_ARGUMENT, "coarse_solve must be HDD_COARSE_REFERENCE or HDD_COARSE_EXACT");
+    if (o.multilevel != 0 && o.multilevel != 1) throw Error(HDD_ERR_INVALID_ARGUMENT, "multilevel must be 0 or 1");
+    if (o.multilevel && o.sub_size[0] % 2 != 0)
+        throw Error(HDD_ERR_INVALID_ARGUMENT, "two-level DD needs an even sub_size");  // the demo's PHYSBAM_ASSERT
+    if (o.multilevel && o.sub_size[0] != 16 && o.sub_size[0] != 32 && o.sub_size[0] != 64)
+        throw Error(HDD_ERR_UNSUPPORTED, "two-level DD runs its V-cycles on boxes of sub_size/2: sub_size must be "
+                                         "16, 32 or 64 (got " + std::to_string(o.sub_size[0]) + ")");
     if (o.sigma_levels < 1 || o.nVcycles < 0 || o.sigma_mg < 0 || o.interior_smoothing < 0 ||
         o.boundary_smoothing < 0 || o.sigma_smoothing < 0)
         throw Error(HDD_ERR_INVALID_ARGUMENT, "negative iteration counts");
@@ -65,6 +73,7 @@ Solver::~Solver() {
         cudaStreamSynchronize(stream);
         release_graphs();
         sigma.release();
+        sigma2.release();
     }
 }
 
@@ -73,6 +82,7 @@ Work::~Work() {
     cudaStreamSynchronize(stream);
     release_graphs();
     if (own_sig) SigmaGpu::free_scratch(sig);
+    if (own_sig2) SigmaGpu::free_scratch(sig2);
     if (own_stream) cudaStreamDestroy(stream);
     stream = nullptr;
 }
@@ -173,6 +183,10 @@ void Solver::initialize() {
     box_tile.upload(btile.data(), btile.size(), stream);
     box_nb.upload(bnb.data(), bnb.size(), stream);
     box_flags.upload(L.box_flags.data(), L.box_flags.size(), stream);
+    for (int l = 0; l < kMaxLevels; ++l) {
+        if (L.global_vcycle && l < L.opt.vlevels) gflags[l].upload(L.g_flags[l].data(), L.g_flags[l].size(), stream);
+        else gflags[l].release();
+    }
     alloc_vectors(w0);
     (void)S;
     (void)N;
@@ -187,7 +201,11 @@ void Solver::initialize() {
         std::fprintf(stderr, "[hdd setup] layout %.2f s (%zu tiles, %zu boxes)\n",
                      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(), L.tiles.size(),
                      L.boxes.size());
-    if (iomode == HDD_IOMODE_INPUT) {
+    if (opts.multilevel) {
+        if (iomode != HDD_IOMODE_NEITHER)
+            throw Error(HDD_ERR_UNSUPPORTED, "interface dump and reload are not implemented for two-level DD");
+        build_two_level_interfaces();
+    } else if (iomode == HDD_IOMODE_INPUT) {
         read_interface_dir(io_dir, ih);
         check_interface(L, opts.sigma_levels, ih);
     } else {
@@ -211,24 +229,92 @@ void Solver::initialize() {
     if (n_if > 0) sigma.setup(ih, opts.sigma_smoothing, stream, opts.coarse_solve == HDD_COARSE_EXACT);
     else sigma.release();
     setup_phase_ms[2] = since_ms(t_sigma);
-    std::vector<long long> slot(n_if);
-    std::vector<int> nbs(6 * (size_t)n_if, -1);
+    // Interface cells' slots and, per cell, the slots of the face neighbours
+    // that one gather reads (-1 for the others).  A neighbour counts when the
+    // cell's face bit is set and keep(neighbour flags, neighbour on a
+    // first-level plane) holds.  Single level: Laplace_ri's Active neighbours
+    // (SPGrid_Laplace_Legacy.h:70-117).
     const int* n = L.opt.size;
-    const int d6[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
-    for (int i = 0; i < n_if; ++i) {
-        const auto& c = ih.iface_map[i];
-        slot[i] = L.tile_slot(c[0], c[1], c[2]);
-        const uint32_t f = L.flags0[L.dense_index(c[0], c[1], c[2])];
-        if (slot[i] < 0 || !(f & F_INTERFACE)) throw Error(HDD_ERR_INTERNAL, "interface DOF outside the tile layout");
-        for (int qf = 0; qf < 6; ++qf) {
-            if (!(f & (F_FACE_MX << qf))) continue;
-            const int a = c[0] + d6[qf][0], bb = c[1] + d6[qf][1], e = c[2] + d6[qf][2];
-            if (a < 0 || bb < 0 || e < 0 || a >= n[0] || bb >= n[1] || e >= n[2]) continue;
-            if (!(L.flags0[L.dense_index(a, bb, e)] & F_ACTIVE)) continue;
-            const long long sl = L.tile_slot(a, bb, e);
-            if (sl > INT32_MAX) throw Error(HDD_ERR_UNSUPPORTED, "domain too large for 32-bit neighbour slots");
-            nbs[6 * (size_t)i + qf] = (int)sl;
+    const int* s1 = opts.sub_size;
+    auto on_plane1 = [&](int a, int b, int c) { return a % s1[0] == 0 || b % s1[1] == 0 || c % s1[2] == 0; };
+    auto tables = [&](const InterfaceHost& h, std::vector<long long>& slot, std::vector<int>& nbs, auto keep) {
+        const int m = h.n_iface.empty() ? 0 : h.n_iface[0];
+        const int d6[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+        slot.assign(m, 0);
+        nbs.assign(6 * (size_t)m, -1);
+        for (int i = 0; i < m; ++i) {
+            const auto& c = h.iface_map[i];
+            slot[i] = L.tile_slot(c[0], c[1], c[2]);
+            const uint32_t f = L.flags0[L.dense_index(c[0], c[1], c[2])];
+            if (slot[i] < 0 || !(f & F_INTERFACE)) throw Error(HDD_ERR_INTERNAL, "interface DOF outside the tile layout");
+            for (int qf = 0; qf < 6; ++qf) {
+                if (!(f & (F_FACE_MX << qf))) continue;
+                const int a = c[0] + d6[qf][0], bb = c[1] + d6[qf][1], e = c[2] + d6[qf][2];
+                if (a < 0 || bb < 0 || e < 0 || a >= n[0] || bb >= n[1] || e >= n[2]) continue;
+                if (!keep(L.flags0[L.dense_index(a, bb, e)], on_plane1(a, bb, e))) continue;
+                const long long sl = L.tile_slot(a, bb, e);
+                if (sl < 0) throw Error(HDD_ERR_INTERNAL, "interface neighbour outside the tile layout");
+                if (sl > INT32_MAX) throw Error(HDD_ERR_UNSUPPORTED, "domain too large for 32-bit neighbour slots");
+                nbs[6 * (size_t)i + qf] = (int)sl;
+            }
         }
+    };
+    std::vector<long long> slot;
+    std::vector<int> nbs;
+    if (!opts.multilevel) {
+        tables(ih, slot, nbs, [](uint32_t f, bool) { return (f & F_ACTIVE) != 0; });
+    } else {
+        // First level: Laplace_ri_Subdomain, the Active|Interface neighbours
+        // off the first-level planes (TWO/SPGrid_Library/SPGrid_Laplace_Legacy.h:120-178).
+        tables(ih, slot, nbs, [](uint32_t f, bool p1) { return (f & (F_ACTIVE | F_INTERFACE)) && !p1; });
+        // Second level: Laplace_ir_Subdomain's neighbours on the first-level
+        // planes (:232-290) and Laplace_ri's Active neighbours (:70-117).
+        std::vector<long long> slot2, slot2b;
+        std::vector<int> nb_ir, nb_ri;
+        tables(ih2, slot2, nb_ir, [](uint32_t f, bool p1) { return (f & (F_ACTIVE | F_INTERFACE)) && p1; });
+        tables(ih2, slot2b, nb_ri, [](uint32_t f, bool) { return (f & F_ACTIVE) != 0; });
+        // Laplace_ir_Subdomain's box-face cells (the V-cycle's face residual):
+        // Interface cells off the first-level planes with an open face to an
+        // Active|Interface cell on them.
+        std::vector<long long> fslot;
+        std::vector<int> fnb;
+        const int d6[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+        for (int i = 0; i < n[0]; ++i)
+            for (int j = 0; j < n[1]; ++j)
+                for (int k = 0; k < n[2]; ++k) {
+                    const uint32_t f = L.flags0[L.dense_index(i, j, k)];
+                    if (!(f & F_INTERFACE) || on_plane1(i, j, k)) continue;
+                    int nb6[6] = {-1, -1, -1, -1, -1, -1};
+                    bool any = false;
+                    for (int qf = 0; qf < 6; ++qf) {
+                        if (!(f & (F_FACE_MX << qf))) continue;
+                        const int a = i + d6[qf][0], bb = j + d6[qf][1], e = k + d6[qf][2];
+                        if (a < 0 || bb < 0 || e < 0 || a >= n[0] || bb >= n[1] || e >= n[2]) continue;
+                        if (!(L.flags0[L.dense_index(a, bb, e)] & (F_ACTIVE | F_INTERFACE)) || !on_plane1(a, bb, e))
+                            continue;
+                        const long long sl = L.tile_slot(a, bb, e);
+                        if (sl < 0 || sl > INT32_MAX) throw Error(HDD_ERR_INTERNAL, "face neighbour outside the tile layout");
+                        nb6[qf] = (int)sl;
+                        any = true;
+                    }
+                    if (!any) continue;
+                    const long long sc = L.tile_slot(i, j, k);
+                    if (sc < 0) throw Error(HDD_ERR_INTERNAL, "face cell outside the tile layout");
+                    fslot.push_back(sc);
+                    fnb.insert(fnb.end(), nb6, nb6 + 6);
+                }
+        n_face = (int)fslot.size();
+        face_slot.upload(fslot.data(), fslot.size(), stream);
+        face_nb.upload(fnb.data(), fnb.size(), stream);
+        iface2_slot.upload(slot2.data(), slot2.size(), stream);
+        iface2_nb_ir.upload(nb_ir.data(), nb_ir.size(), stream);
+        iface2_nb_ri.upload(nb_ri.data(), nb_ri.size(), stream);
+        const int n2 = ih2.n_iface.empty() ? 0 : ih2.n_iface[0];
+        if (n2 > 0) sigma2.setup(ih2, opts.sigma_smoothing, stream, opts.coarse_solve == HDD_COARSE_EXACT);
+        else sigma2.release();
+        w0.sig2 = sigma2.primary();
+        w0.sig2.set_grid_div(std::max(1, opts.solve_share));
+        w0.own_sig2 = false;
     }
     iface_slot.upload(slot.data(), slot.size(), stream);
     iface_nb.upload(nbs.data(), nbs.size(), stream);
@@ -252,6 +338,16 @@ void Solver::alloc_vectors(Work& w) {
     for (DevBuf<float>* v : {&w.x, &w.b, &w.r, &w.z, &w.s, &w.q}) { v->alloc(N * k); v->zero(w.stream); }
     if (opts.precision_mode == HDD_PRECISION_MIXED) w.xd.alloc(N * k);
     else w.xd.release();
+    if (opts.multilevel) w.hr.alloc(N * k);
+    else w.hr.release();
+    for (int l = 0; l < kMaxLevels; ++l) {
+        const bool on = L.global_vcycle && l < L.opt.vlevels;
+        const size_t c = on ? (size_t)L.g_dims[l][0] * L.g_dims[l][1] * L.g_dims[l][2] : 0;
+        for (DevBuf<float>* v : {&w.gu[l], &w.gb[l], &w.gr[l]}) {
+            if (on) { v->alloc(c); v->zero(w.stream); }
+            else v->release();
+        }
+    }
     w.partial.alloc(P * k);
     w.partial_max.alloc(P * k);
     w.sums.alloc(8 * k);
@@ -263,7 +359,7 @@ void Solver::alloc_vectors(Work& w) {
 }
 
 int Solver::max_batch() const {
-    if (!initialized) return 1;
+    if (!initialized || opts.multilevel || L.global_vcycle) return 1;
     return sigma.lv.empty() ? 4 : sigma.max_rhs();
 }
 
@@ -282,6 +378,11 @@ std::unique_ptr<Work> Solver::make_work(int k) {
         w->sig.set_grid_div(std::max(1, opts.solve_share));
         w->own_sig = true;
     }
+    if (!sigma2.lv.empty()) {
+        sigma2.alloc_scratch(w->sig2, w->stream, k);
+        w->sig2.set_grid_div(std::max(1, opts.solve_share));
+        w->own_sig2 = true;
+    }
     sync(*w);
     return w;
 }
@@ -289,10 +390,12 @@ std::unique_ptr<Work> Solver::make_work(int k) {
 size_t Solver::work_bytes(int k) const {
     const size_t nt = L.tiles.size(), N = nt * (size_t)L.tile_cells;
     const size_t P = std::max<size_t>({nt, (size_t)laplace_partials(geom()), (size_t)1});
-    size_t t = std::max<size_t>(L.cell_count(), 1) * 4 + 6 * std::max<size_t>(N, 1) * 4 * k;
+    size_t t = std::max<size_t>(L.cell_count(), 1) * 4 + (opts.multilevel ? 7 : 6) * std::max<size_t>(N, 1) * 4 * k;
     if (opts.precision_mode == HDD_PRECISION_MIXED) t += std::max<size_t>(N, 1) * 8 * k;
     t += (P * 12 + 128 + sizeof(PcgScalars) + 12) * k;
-    return t + sigma.scratch_bytes(k);
+    if (L.global_vcycle)
+        for (int l = 0; l < L.opt.vlevels; ++l) t += 12 * (size_t)L.g_dims[l][0] * L.g_dims[l][1] * L.g_dims[l][2];
+    return t + sigma.scratch_bytes(k) + (sigma2.lv.empty() ? 0 : sigma2.scratch_bytes(k));
 }
 
 void Solver::set_rhs(Work& w, const float* rhs) {
@@ -349,8 +452,36 @@ VcycleArgs Solver::vcycle_args(float* u, const float* bb, int halo_from_u, int z
     return a;
 }
 
-void Solver::run_vcycle(Work& w, float* u, const float* bb, int halo_from_u, int zero_init, int nv) {
+void Solver::run_vcycle(Work& w, float* u, const float* bb, int halo_from_u, int zero_init, int nv,
+                        const float* r_halo) {
     VcycleArgs a = vcycle_args(u, bb, halo_from_u, zero_init, nv);
+    a.r_halo = r_halo;
+    if (L.global_vcycle) {
+        // Coarse levels couple the boxes: the whole-grid V-cycle (one system).
+        if (w.k > 1) throw Error(HDD_ERR_INTERNAL, "whole-grid V-cycle with a batched context");
+        GlobalVcycleArgs ga;
+        std::memset(&ga, 0, sizeof(ga));
+        ga.levels = L.opt.vlevels;
+        for (int l = 0; l < ga.levels; ++l) {
+            for (int q = 0; q < 3; ++q) ga.dims[l][q] = L.g_dims[l][q];
+            ga.f[l] = gflags[l].p;
+            ga.u[l] = w.gu[l].p;
+            ga.b[l] = w.gb[l].p;
+            ga.r[l] = w.gr[l].p;
+        }
+        ga.n_vcycles = nv;
+        ga.interior_itr = a.interior_itr;
+        ga.boundary_itr = a.boundary_itr;
+        ga.bottom_itr = a.bottom_itr;
+        ga.halo_from_u = halo_from_u;
+        ga.zero_init = zero_init;
+        std::memcpy(ga.w.inv_diag, a.inv_diag, sizeof(a.inv_diag));
+        std::memcpy(ga.w.restrict_w, a.restrict_w, sizeof(a.restrict_w));
+        std::memcpy(ga.w.prolong_w, a.prolong_w, sizeof(a.prolong_w));
+        Tm tm(this, w, 0, vcycle_bytes);
+        w.launches += launch_vcycle_global(ga, geom(), tile_xyz.p, u, bb, r_halo, w.stream);
+        return;
+    }
     if (w.k > 1) {
         a.nslots = w.k;
         a.slot_stride = w.vstride;
@@ -407,6 +538,10 @@ void Solver::apply_preconditioner(Work& w, const float* rr, float* zz) {
 }
 
 void Solver::apply_preconditioner_launches(Work& w, const float* rr, float* zz) {
+    if (opts.multilevel) {
+        two_level_launches(w, rr, zz);
+        return;
+    }
     NvtxRange range("Apply_Preconditioner");
     const TileGeom g = geom();
     {
@@ -439,6 +574,121 @@ void Solver::apply_preconditioner_launches(Work& w, const float* rr, float* zz) 
     run_vcycle(w, zz, rr, 1, 1, opts.nVcycles);
 }
 
+void Solver::build_two_level_interfaces() {
+    // Two-level DD (demos/Domain_Decomposition_CPU_Only_Two_Levels, "TWO/"):
+    // the first-level interface system is assembled on boxes of sub_size from
+    // the caller's flags (TWO/SPGrid_Domain_Decomposition_Solver/SPGrid_Subdomain_Splitter.h:53-160).
+    // The second-level systems, one per first-level subdomain (:168-193),
+    // are stacked into one block-diagonal system (build_second_level).
+    DomainLayout Lf;
+    Lf.opt = L.opt;
+    for (int a = 0; a < 3; ++a) Lf.opt.sub[a] = opts.sub_size[a];
+    Lf.flags_in = flags_in;
+    build_interface(Lf, opts.sigma_levels, ih);
+    build_second_level(Lf, opts.sub_size, opts.sigma_levels, ih2);
+}
+
+// Subdomain_DD (TWO/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Decomposition_Preconditioner.h:127-181;
+// its residual prints dropped): a DD solve inside every first-level
+// subdomain, the first-level interface values in zz as its boundary data.
+// On entry zz holds only first-level interface values (zero the first time).
+//
+// The reference computes Laplace_ir_Subdomain into its tmp channel and runs
+// the first V-cycles on that channel without clearing it; its restriction
+// reads the channel at the boxes' face cells, where the V-cycle computes no
+// residual, so at the second-level interface cells it restricts those
+// values.  They are zero on the first call (zz is zero) and are passed to the
+// V-cycle as its face residual (hr) on the second, for the same result.
+// (Every Active|Interface cell off the first-level planes gets a value; only
+// those on box faces are read, and only those next to a first-level plane
+// are nonzero: face_slot.)
+void Solver::subdomain_dd(Work& w, const float* rr, float* zz, bool second) {
+    const TileGeom g = geom();
+    const int n2 = ih2.n_iface.empty() ? 0 : ih2.n_iface[0];
+    const int n1 = ih.n_iface.empty() ? 0 : ih.n_iface[0];
+    {
+        // b2 = Laplace_ir_Subdomain(zz) at the second-level interface cells.
+        Tm tm(this, w, 3);
+        cuda_check(launch_interface_gather(g, iface2_slot.p, iface2_nb_ir.p, n2, rr, zz, w.sig2.b0(), w.stream,
+                                           Batch(), 0, kGatherIr), "gather ir");
+        count(w);
+        if (second && n_face > 0) {
+            cuda_check(cudaMemsetAsync(w.hr.p, 0, sizeof(float) * w.vstride, w.stream), "memset hr");
+            cuda_check(launch_interface_gather(g, face_slot.p, face_nb.p, n_face, rr, zz, w.hr.p, w.stream, Batch(), 0,
+                                               kGatherIrTiled), "gather ir faces");
+            count(w);
+        }
+    }
+    run_vcycle(w, zz, rr, 1, 1, opts.nVcycles, second && n_face > 0 ? w.hr.p : nullptr);
+    if (n2 > 0) {
+        {
+            // b2 += rr - A_ri zz (Laplace_ri, then Accumulate_To_Eigen_Array).
+            Tm tm(this, w, 3);
+            cuda_check(launch_interface_gather(g, iface2_slot.p, iface2_nb_ri.p, n2, rr, zz, w.sig2.b0(), w.stream,
+                                               Batch(), 0, kGatherRiAdd), "gather ri");
+            count(w);
+        }
+        NvtxRange sigma_range("Sigma_V_Cycle (second level)");
+        Tm tm(this, w, 4);
+        cuda_check(cudaMemsetAsync(w.sig2.u0(), 0, sizeof(float) * w.sig2.lv[0].si, w.stream), "memset u2");
+        for (int i = 0; i < opts.sigma_mg; ++i) sigma2.vcycle(w.sig2, w.stream, w.launches, &w == &w0 ? &hook : nullptr);
+    }
+    {
+        // zz = 0, then the first- and second-level interface values.
+        Tm tm(this, w, 3);
+        cuda_check(cudaMemsetAsync(zz, 0, sizeof(float) * w.vstride, w.stream), "memset z");
+        cuda_check(launch_interface_scatter(iface_slot.p, n1, w.sig.u0(), zz, w.stream), "scatter u1");
+        cuda_check(launch_interface_scatter(iface2_slot.p, n2, w.sig2.u0(), zz, w.stream), "scatter u2");
+        count(w, 2);
+    }
+    run_vcycle(w, zz, rr, 1, 1, opts.nVcycles);
+}
+
+// Apply_Preconditioner with multilevel
+// (TWO/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Decomposition_Preconditioner.h:182-230):
+// Subdomain_DD in place of each V-cycle pass, the first-level interface
+// right-hand side from Laplace_ri_Subdomain.
+void Solver::two_level_launches(Work& w, const float* rr, float* zz) {
+    NvtxRange range("Apply_Preconditioner (two-level)");
+    const TileGeom g = geom();
+    const int n1 = ih.n_iface.empty() ? 0 : ih.n_iface[0];
+    cuda_check(cudaMemsetAsync(zz, 0, sizeof(float) * w.vstride, w.stream), "memset z");
+    if (n1 > 0) cuda_check(cudaMemsetAsync(w.sig.u0(), 0, sizeof(float) * w.sig.lv[0].si, w.stream), "memset u1");
+    subdomain_dd(w, rr, zz, false);
+    if (n1 > 0) {
+        {
+            Tm tm(this, w, 3);
+            cuda_check(launch_interface_gather(g, iface_slot.p, iface_nb.p, n1, rr, zz, w.sig.b0(), w.stream),
+                       "gather ri_subdomain");
+            count(w);
+        }
+        NvtxRange sigma_range("Sigma_V_Cycle");
+        Tm tm(this, w, 4);
+        cuda_check(cudaMemsetAsync(w.sig.u0(), 0, sizeof(float) * w.sig.lv[0].si, w.stream), "memset u1");
+        for (int i = 0; i < opts.sigma_mg; ++i) sigma.vcycle(w.sig, w.stream, w.launches, &w == &w0 ? &hook : nullptr);
+    }
+    {
+        Tm tm(this, w, 3);
+        cuda_check(cudaMemsetAsync(zz, 0, sizeof(float) * w.vstride, w.stream), "memset z");
+        cuda_check(launch_interface_scatter(iface_slot.p, n1, w.sig.u0(), zz, w.stream), "scatter u1");
+        count(w);
+    }
+    subdomain_dd(w, rr, zz, true);
+}
+
+int Solver::wait_error(Work& w) {
+    int e[2] = {0, 0};
+    if (w.sig.err) cuda_check(cudaMemcpyAsync(&e[0], w.sig.err, sizeof(int), cudaMemcpyDeviceToHost, w.stream), "D2H");
+    if (w.sig2.err) cuda_check(cudaMemcpyAsync(&e[1], w.sig2.err, sizeof(int), cudaMemcpyDeviceToHost, w.stream), "D2H");
+    sync(w);
+    return e[0] | e[1];
+}
+
+void Solver::clear_wait_errors(Work& w) {
+    SigmaGpu::clear_error(w.sig, w.stream);
+    if (w.sig2.err) SigmaGpu::clear_error(w.sig2, w.stream);
+}
+
 void Solver::solve(Work& w, hdd_result* res) {
     if (!initialized) throw Error(HDD_ERR_NOT_INITIALIZED, "initialize_preconditioner not called");
     NvtxRange range("solve");
@@ -454,7 +704,7 @@ void Solver::solve(Work& w, hdd_result* res) {
     w.x.zero(w.stream);
     w.xd.zero(w.stream);
     double* xdp = mode == 1 ? w.xd.p : nullptr;
-    SigmaGpu::clear_error(w.sig, w.stream);
+    clear_wait_errors(w);
     cudaEvent_t e0, e1;
     cuda_check(cudaEventCreate(&e0), "event");
     cuda_check(cudaEventCreate(&e1), "event");
@@ -528,10 +778,13 @@ void Solver::solve(Work& w, hdd_result* res) {
         cuda_check(launch_reduce_max(w.partial_max.p, nt, w.scalars_f.p, w.stream), "reduce"); count(w);
         cuda_check(cudaMemcpyAsync(&rmax, w.scalars_f.p, sizeof(float), cudaMemcpyDeviceToHost, w.stream), "D2H");
         cuda_check(cudaMemcpyAsync(&hs, w.scal.p, sizeof(hs), cudaMemcpyDeviceToHost, w.stream), "D2H");
-        int herr = 0;
+        int herr = 0, herr2 = 0;
         if (w.sig.err)
             cuda_check(cudaMemcpyAsync(&herr, w.sig.err, sizeof(int), cudaMemcpyDeviceToHost, w.stream), "D2H");
+        if (w.sig2.err)
+            cuda_check(cudaMemcpyAsync(&herr2, w.sig2.err, sizeof(int), cudaMemcpyDeviceToHost, w.stream), "D2H");
         sync(w);
+        herr |= herr2;
         w.history.push_back((double)rmax);
         w.alphas.push_back(mode == 1 ? hs.alpha_d : (double)hs.alpha);
         w.betas.push_back(first ? 0.0 : (mode == 1 ? hs.beta_d : (double)hs.beta));
@@ -701,7 +954,7 @@ void Solver::solve_batch(Work& w, BatchFeeder& feed) {
         h_active[j] = 1;
         if (stop_test(j)) return;
     };
-    SigmaGpu::clear_error(w.sig, w.stream);
+    clear_wait_errors(w);
     // A failure of a device call ends every request the batch holds with its
     // status, then propagates.
     auto fail_all = [&](hdd_status st) {
@@ -778,10 +1031,13 @@ void Solver::solve_batch(Work& w, BatchFeeder& feed) {
         }
         cuda_check(cudaMemcpyAsync(h_scal.data(), w.scal.p, K * sizeof(PcgScalars), cudaMemcpyDeviceToHost, w.stream),
                    "D2H");
-        int herr = 0;
+        int herr = 0, herr2 = 0;
         if (w.sig.err)
             cuda_check(cudaMemcpyAsync(&herr, w.sig.err, sizeof(int), cudaMemcpyDeviceToHost, w.stream), "D2H");
+        if (w.sig2.err)
+            cuda_check(cudaMemcpyAsync(&herr2, w.sig2.err, sizeof(int), cudaMemcpyDeviceToHost, w.stream), "D2H");
         sync(w);
+        herr |= herr2;
         for (int j = 0; j < K; ++j) {
             Sys& S = sys[j];
             if (!S.busy) continue;
@@ -794,7 +1050,7 @@ void Solver::solve_batch(Work& w, BatchFeeder& feed) {
             if (h_scal[j].status != 0 || !std::isfinite(S.rmax)) { finish(j, HDD_ERR_BREAKDOWN); continue; }
             stop_test(j);
         }
-        if (herr != 0) SigmaGpu::clear_error(w.sig, w.stream);
+        if (herr != 0) clear_wait_errors(w);
     }
     } catch (const Error& e) {
         cudaStreamSynchronize(w.stream);
@@ -846,7 +1102,7 @@ void Solver::apply_preconditioner_dense(const float* rin, float* zout) {
     dense_to_tiles(L, rin, t.data());
     cuda_check(cudaMemcpyAsync(w0.r.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "H2D");
     w0.z.zero(stream);
-    sigma.clear_error(stream);
+    clear_wait_errors(w0);
     apply_preconditioner(w0, w0.r.p, w0.z.p);
     cuda_check(launch_project(geom(), w0.z.p, stream), "project"); count(w0);
     cuda_check(cudaMemcpyAsync(t.data(), w0.z.p, t.size() * sizeof(float), cudaMemcpyDeviceToHost, stream), "D2H");
@@ -961,7 +1217,7 @@ void Solver::interface_solve_batch(int kind, int level, int nrhs, const float* b
 }
 
 void Solver::check_waits(Work& w) {
-    if (SigmaGpu::error_flag(w.sig, w.stream))
+    if (wait_error(w))
         throw Error(HDD_ERR_TIMEOUT, "a bounded device wait in the sigma solve gave up; results are invalid");
 }
 

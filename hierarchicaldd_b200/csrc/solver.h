@@ -83,6 +83,8 @@ struct Work {
     int pstride = 0;
     DevBuf<int> active, first, replace;
     DevBuf<float> x, b, r, z, s, q;
+    DevBuf<float> hr;       // two-level DD: the V-cycle's lower-face residual input
+    DevBuf<float> gu[kMaxLevels], gb[kMaxLevels], gr[kMaxLevels];  // whole-grid V-cycle levels
     DevBuf<double> xd;      // precision form: the FP64 iterate (x is its FP32 rounding)
     DevBuf<float> dense;    // staging buffer in the caller's dense layout
     DevBuf<double> partial, sums;
@@ -90,6 +92,8 @@ struct Work {
     DevBuf<PcgScalars> scal;
     SigmaScratch sig;
     bool own_sig = false;
+    SigmaScratch sig2;      // two-level DD: the second-level interface solver's vectors
+    bool own_sig2 = false;
     // CUDA graph of one preconditioner application (on buffers pc_r -> pc_z)
     // and the kernel launches it holds; dropped when a launch parameter
     // changes (re-initialisation, the wait limit).
@@ -112,10 +116,12 @@ struct Work {
     void release_graphs();
     size_t bytes() const {
         size_t t = 0;
-        for (const DevBuf<float>* v : {&x, &b, &r, &z, &s, &q, &dense, &partial_max, &scalars_f}) t += v->n * sizeof(float);
+        for (const DevBuf<float>* v : {&x, &b, &r, &z, &s, &q, &hr, &dense, &partial_max, &scalars_f})
+            t += v->n * sizeof(float);
+        for (int l = 0; l < kMaxLevels; ++l) t += (gu[l].n + gb[l].n + gr[l].n) * sizeof(float);
         t += (partial.n + sums.n + xd.n) * sizeof(double) + scal.n * sizeof(PcgScalars);
         t += (active.n + first.n + replace.n) * sizeof(int);
-        return t + (own_sig ? sig.bytes : 0);
+        return t + (own_sig ? sig.bytes : 0) + (own_sig2 ? sig2.bytes : 0);
     }
     // The launch description of all k systems (a plain single system for k = 1).
     Batch batch() const {
@@ -155,11 +161,27 @@ struct Solver {
     DevBuf<uint16_t> tflags;
     DevBuf<int> tile_nbr, box_tile, box_nb, tile_xyz;
     DevBuf<uint8_t> box_flags;
+    DevBuf<uint8_t> gflags[kMaxLevels];  // whole-grid V-cycle: compact8 flags per level
     // Level-0 interface DOFs (sigma level 0 order).
     DevBuf<long long> iface_slot;
     DevBuf<int> iface_nb;
     SigmaGpu sigma;
     InterfaceHost ih;
+    // Two-level DD (opts.multilevel): the second-level interface system (all
+    // first-level subdomains' systems as one block-diagonal system), its
+    // cells' slots and the neighbour lists of its three gathers.  iface_nb
+    // then lists, for the first-level interface cells, the neighbours off the
+    // first-level planes (Laplace_ri_Subdomain).
+    SigmaGpu sigma2;
+    InterfaceHost ih2;
+    DevBuf<long long> iface2_slot;
+    DevBuf<int> iface2_nb_ir, iface2_nb_ri;
+    // The cells where Laplace_ir_Subdomain can leave a nonzero value on a
+    // V-cycle box face: Interface cells off the first-level planes with a
+    // first-level plane neighbour; their slots and those neighbours.
+    DevBuf<long long> face_slot;
+    DevBuf<int> face_nb;
+    int n_face = 0;
     int iomode = HDD_IOMODE_NEITHER;  // interface dump / reload at initialize()
     std::string io_dir;
     double setup_ms = 0;
@@ -259,9 +281,15 @@ struct Solver {
     // Device pieces.
     TileGeom geom() const;
     VcycleArgs vcycle_args(float* u, const float* bb, int halo_from_u, int zero_init, int nv) const;
-    void run_vcycle(Work& w, float* u, const float* bb, int halo_from_u, int zero_init, int nv);
+    void run_vcycle(Work& w, float* u, const float* bb, int halo_from_u, int zero_init, int nv,
+                    const float* r_halo = nullptr);
     void apply_preconditioner(Work& w, const float* rr, float* zz);   // device tiled vectors (graph replay)
     void apply_preconditioner_launches(Work& w, const float* rr, float* zz);
+    void build_two_level_interfaces();
+    void two_level_launches(Work& w, const float* rr, float* zz);
+    void subdomain_dd(Work& w, const float* rr, float* zz, bool second);
+    int wait_error(Work& w);   // the contexts' bounded-wait error words (0: none)
+    void clear_wait_errors(Work& w);
     void release_graphs() { w0.release_graphs(); }
     void alloc_vectors(Work& w);
     static void count(Work& w, int n = 1) { w.launches += n; }
@@ -271,9 +299,11 @@ struct Solver {
     // first context).
     size_t device_bytes() const {
         size_t t = tflags.n * sizeof(uint16_t) + box_flags.n;
-        for (const DevBuf<int>* v : {&tile_nbr, &box_tile, &box_nb, &tile_xyz, &iface_nb}) t += v->n * sizeof(int);
-        t += iface_slot.n * sizeof(long long);
-        return t + sigma.device_bytes + w0.bytes();
+        for (int l = 0; l < kMaxLevels; ++l) t += gflags[l].n;
+        for (const DevBuf<int>* v : {&tile_nbr, &box_tile, &box_nb, &tile_xyz, &iface_nb, &iface2_nb_ir, &iface2_nb_ri})
+            t += v->n * sizeof(int);
+        t += (iface_slot.n + iface2_slot.n + face_slot.n) * sizeof(long long) + face_nb.n * sizeof(int);
+        return t + sigma.device_bytes + sigma2.device_bytes + w0.bytes();
     }
     // Device bytes a further context of this domain allocates.
     size_t work_bytes(int k = 1) const;

@@ -10,6 +10,10 @@
 // "rhs" modes read the fluids simulation format, which this library does not
 // implement, and exit with HDD_ERR_UNSUPPORTED.  -iomode output / input dump
 // or reload the interface matrices in the -o directory (main.cpp:315).
+// -multilevel yes|no is the two-level demo's flag
+// (demos/Domain_Decomposition_CPU_Only_Two_Levels/Test_Bench_3D/main.cpp:251-257):
+// "yes" solves every subdomain by a DD at sub_size/2; that demo has no
+// -iomode, so with -multilevel yes it defaults to neither.
 //
 // Flags of this library only: -tol x and -relative_tol 0|1 (the stop test;
 // default 1e-6 relative, the reference's is -tol 1e-5 -relative_tol 0),
@@ -37,7 +41,8 @@ struct Args {
     int threads = 0, vlevels = 3, sigma_levels = 3, sigma_smoothing = 3, sigma_mg = 1;
     int interior = 1, boundary = 3, nvcycles = 1, frame = 0;
     int origin[3] = {0, 0, 0};
-    std::string dir, out = "output", mode = "velocity", iomode = "output";
+    std::string dir, out = "output", mode = "velocity", iomode = "output", multilevel = "no";
+    bool iomode_given = false;
     double tol = 1e-6;
     int relative_tol = 1, max_iters = 5000, device = 0;
     std::string precision = "reference", solution;
@@ -50,7 +55,7 @@ void usage(FILE* f) {
                  "       [-nVcycles n] [-threads n] [-frame n] [-origin n n n] -d dir [-o dir]\n"
                  "       [-mode no_convertion|velocity|rhs] [-iomode output|input|neither]\n"
                  "       [-tol x] [-relative_tol 0|1] [-precision reference|mixed] [-max_iters n]\n"
-                 "       [-device n] [-solution file]\n");
+                 "       [-device n] [-solution file] [-multilevel yes|no]\n");
 }
 
 bool parse_int(const char* s, int& v) {
@@ -102,7 +107,11 @@ int parse(int argc, char** argv, Args& a) {
         else if (f == "-d") ok = next(a.dir);
         else if (f == "-o") ok = next(a.out);
         else if (f == "-mode") ok = next(a.mode);
-        else if (f == "-iomode") ok = next(a.iomode);
+        else if (f == "-iomode") {
+            ok = next(a.iomode);
+            a.iomode_given = true;
+        }
+        else if (f == "-multilevel") ok = next(a.multilevel);
         else if (f == "-relative_tol") ok = next_int(a.relative_tol);
         else if (f == "-max_iters") ok = next_int(a.max_iters);
         else if (f == "-device") ok = next_int(a.device);
@@ -121,6 +130,11 @@ int parse(int argc, char** argv, Args& a) {
             return 2;
         }
     }
+    if (a.multilevel != "yes" && a.multilevel != "no") {
+        std::fprintf(stderr, "-multilevel must be yes or no\n");
+        return 2;
+    }
+    if (a.multilevel == "yes" && !a.iomode_given) a.iomode = "neither";
     if (a.iomode != "output" && a.iomode != "input" && a.iomode != "neither") {
         std::fprintf(stderr, "-iomode must be output, input or neither\n");
         return 2;
@@ -187,6 +201,7 @@ int main(int argc, char** argv) {
     o.max_iters = a.max_iters;
     o.precision_mode = a.precision == "mixed" ? HDD_PRECISION_MIXED : HDD_PRECISION_REFERENCE;
     o.device = a.device;
+    o.multilevel = a.multilevel == "yes" ? 1 : 0;
 
     hdd_solver* h = nullptr;
     auto fail = [&](const char* what, hdd_status st) {

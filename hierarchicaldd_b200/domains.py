@@ -78,8 +78,8 @@ def reference_generator(size, delta) -> Domain:
     Active face neighbour are exterior too, and face bits follow Flaging.  The
     reference's shipped 2D output (256 x 256) decodes to exactly this.
 
-    The solver's GPU path rejects these inputs (exterior cells touch Active
-    ones); the oracle accepts them."""
+    Exterior cells touch Active ones here, which couples subdomain boxes at the
+    coarse V-cycle levels: the solver runs its whole-grid V-cycle for them."""
     n = tuple(int(v) for v in size)
     grids = np.ogrid[tuple(slice(0, v) for v in n)]
     d2 = np.float32(0)
@@ -224,6 +224,27 @@ def profile_case() -> Domain:
     return Domain(d.size, d.flags, d.rhs, d.sub_size, "p128_128cube_sub32", d.meta)
 
 
+# The two-level demo's Test_Bench defaults
+# (demos/Domain_Decomposition_CPU_Only_Two_Levels/Test_Bench_3D/main.cpp:236-251)
+# with -multilevel yes: 64^3 subdomains, each solved by a DD of 32^3 boxes.
+TWO_LEVEL_DEFAULTS = dict(vlevels=3, nVcycles=1, interior_smoothing=1, boundary_smoothing=3,
+                          sigma_levels=3, sigma_smoothing=3, sigma_mg=1, multilevel=True)
+
+
+def two_level_case() -> Domain:
+    """128^3 cells (size 129), centred Dirichlet sphere r=24, U[-1, 1] right-hand
+    side (Philox seed 11), 64^3 subdomains, two-level DD at the demo's defaults."""
+    d = small(128, 64, 24, seed=11)
+    return Domain(d.size, d.flags, d.rhs, d.sub_size, "tl128_128cube_sub64_two_level", dict(TWO_LEVEL_DEFAULTS))
+
+
+def config2_two_level() -> Domain:
+    """The 256^3 workload's domain and right-hand side (config2) solved by
+    two-level DD at the demo's defaults: 64^3 subdomains split into 32^3 boxes."""
+    d = config2()
+    return Domain(d.size, d.flags, d.rhs, (64, 64, 64), "c2_256cube_sub64_two_level", dict(TWO_LEVEL_DEFAULTS))
+
+
 SERVING_SIDES = (64, 96, 128, 192)
 
 
@@ -306,4 +327,4 @@ def to_pages(flags: np.ndarray, *fields: np.ndarray):
 
 
 CONFIGS = {"c1": config1, "c2": config2, "c3": config3, "p128": profile_case, "c5": config5,
-           "c5_half": lambda: config5(2)}
+           "c5_half": lambda: config5(2), "c2ml": config2_two_level, "tl128": two_level_case}

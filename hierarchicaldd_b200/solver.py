@@ -82,11 +82,14 @@ class SPGrid_Domain_Decomposition_Solver:
                                   tol=1e-6, relative_tol=True, max_iters=5000, min_iters=0,
                                   precision_mode=_lib.PRECISION_REFERENCE, true_residual_every=20,
                                   iomode="neither", dump_directory="matrices_dump",
-                                  coarse_solve=_lib.COARSE_REFERENCE, solve_share=0):
+                                  coarse_solve=_lib.COARSE_REFERENCE, solve_share=0, multilevel=False):
         """Setup with the reference's arguments (SPGrid_Domain_Decomposition_Solver.h:121).
         ``iomode`` "output" writes the interface matrices to ``dump_directory`` in the
         reference's dump layout, "input" reads them from there instead of assembling
-        (the reference defaults to "output"; this mirror to "neither")."""
+        (the reference defaults to "output"; this mirror to "neither").  ``multilevel``
+        is the two-level demo's last argument (Domain_Decomposition_CPU_Only_Two_Levels,
+        SPGrid_Domain_Decomposition_Solver.h:124): every subdomain is solved by a DD
+        at subdomain_size/2 instead of by V-cycles."""
         if iomode not in _lib.IOMODES:
             raise HddError(1, f"iomode must be one of {sorted(_lib.IOMODES)}, not {iomode!r}")
         o = hdd_options()
@@ -112,6 +115,7 @@ class SPGrid_Domain_Decomposition_Solver:
         o.precision_mode, o.true_residual_every = int(precision_mode), int(true_residual_every)
         o.coarse_solve = int(coarse_solve)
         o.solve_share = int(solve_share)
+        o.multilevel = 1 if multilevel else 0
         o.device = self.device
         self.options = o
         self.close()

@@ -68,6 +68,11 @@ typedef struct {
     int solve_share;        /* persistent interface solves use 1/solve_share of the device's
                                resident CTAs (0 or 1 = all), leaving room for concurrent solves;
                                results do not depend on it */
+    int multilevel;         /* reference -multilevel (demos/Domain_Decomposition_CPU_Only_Two_Levels,
+                               SPGrid_Domain_Decomposition_Preconditioner.h:127-230): 1 = two-level
+                               DD, each subdomain solved by a DD of its own at sub_size/2 (its
+                               interface system and V-cycles on boxes of sub_size/2) instead of
+                               V-cycles; one system per solve context */
 } hdd_options;
 
 /* Coarsest interface (sigma) level.  The reference runs 200 smoothing steps

@@ -31,6 +31,7 @@ struct SolverBase {
     Dims d0;
     int sub[3];
     int vlevels, nvcycles, interior, boundary, sigma_levels, sigma_smoothing, sigma_mg;
+    int multilevel = 0;  // two-level DD (the Two_Levels demo's -multilevel yes)
     std::vector<uint32_t> flags_in;
     virtual int num_levels() const = 0;
     virtual const Dims& level_dims(int l) const = 0;
@@ -43,6 +44,10 @@ struct Solver : SolverBase {
     InterfaceSystem<T> sys;
     SigmaSolver<T> sigma;
     std::vector<T> k_tmp;  // preconditioner tmp channel (CG_SYSTEM's preconditioner_tmp_field)
+    // Two-level DD: one interface system per first-level subdomain box, on
+    // the box split at sub/2 (iface_map in global cells).
+    std::vector<std::unique_ptr<InterfaceSystem<T>>> sys2;
+    std::vector<std::unique_ptr<SigmaSolver<T>>> sigma2;
 
     int num_levels() const override { return (int)lv.size(); }
     const Dims& level_dims(int l) const override { return lv[l].d; }
@@ -59,10 +64,22 @@ struct Solver : SolverBase {
         };
         build_interface_system<T>(d0, flags_in.data(), sub, sigma_levels, sys);
         stamp("interface system");
+        // Two-level: the V-cycles run on boxes of sub/2, whose planes (both
+        // levels) are Interface (TWO/SPGrid_Domain_Decomposition_Solver/
+        // SPGrid_Domain_Decomposition_Solver.h:124-158).
+        int vsub[3] = {sub[0], sub[1], sub[2]};
+        if (multilevel) {
+            for (int a = 0; a < 3; ++a) {
+                if (sub[a] % 2) throw std::runtime_error("two-level DD needs an even sub_size");
+                vsub[a] = sub[a] / 2;
+            }
+            setup_second_level();
+            stamp("second-level interface systems");
+        }
         lv.resize(vlevels);
         lv[0].d = d0;
         lv[0].flags = flags_in;
-        divide_domain(d0, lv[0].flags.data(), sub);
+        divide_domain(d0, lv[0].flags.data(), vsub);
         flag_faces(d0, lv[0].flags.data());
         for (int l = 0; l + 1 < vlevels; ++l) {
             for (int a = 0; a < 3; ++a) lv[l + 1].d.n[a] = lv[l].d.n[a] / 2 + 1;
@@ -84,6 +101,113 @@ struct Solver : SolverBase {
         k_tmp.assign(d0.count(), T(0));
     }
 
+    // TWO/SPGrid_Domain_Decomposition_Solver/SPGrid_Subdomain_Splitter.h:168-193:
+    // each first-level subdomain box [lo, lo + sub] gets the caller's flags
+    // with its Active cells on first-level planes made Dirichlet
+    // (Domain_Divider with clear_flag, TWO/.../SPGrid_Domain_Divider_Helper.h:61-72),
+    // split again at sub/2 into its own interface system.  The box is built
+    // as a local grid whose origin is a multiple of sub, so plane tests on
+    // local indices equal those on global ones.
+    void setup_second_level() {
+        int ns[3], sub2[3];
+        number_of_subdomains(d0.n, sub, ns);
+        for (int a = 0; a < 3; ++a) sub2[a] = sub[a] / 2;
+        sys2.clear();
+        sigma2.clear();
+        for (int si = 0; si < ns[0]; ++si)
+            for (int sj = 0; sj < ns[1]; ++sj)
+                for (int sk = 0; sk < ns[2]; ++sk) {
+                    const int lo[3] = {si * sub[0], sj * sub[1], sk * sub[2]};
+                    Dims ld;
+                    for (int a = 0; a < 3; ++a) ld.n[a] = std::min(sub[a] + 1, d0.n[a] - lo[a]);
+                    std::vector<uint32_t> lf(ld.count(), 0u);
+                    for (int i = 0; i < ld.n[0]; ++i)
+                        for (int j = 0; j < ld.n[1]; ++j)
+                            for (int k = 0; k < ld.n[2]; ++k) {
+                                uint32_t f = flags_in[d0.at(lo[0] + i, lo[1] + j, lo[2] + k)];
+                                if ((f & ACTIVE) && (i % sub[0] == 0 || j % sub[1] == 0 || k % sub[2] == 0))
+                                    f = DIRICHLET;
+                                lf[ld.at(i, j, k)] = f;
+                            }
+                    std::unique_ptr<InterfaceSystem<T>> sy(new InterfaceSystem<T>());
+                    build_interface_system<T>(ld, lf.data(), sub2, sigma_levels, *sy);
+                    if (sy->n_iface.empty() || sy->n_iface[0] == 0) continue;
+                    for (auto& c : sy->iface_map)
+                        for (int a = 0; a < 3; ++a) c[a] += lo[a];
+                    std::unique_ptr<SigmaSolver<T>> sg(new SigmaSolver<T>());
+                    sg->initialize(*sy, sigma_smoothing);
+                    sys2.push_back(std::move(sy));
+                    sigma2.push_back(std::move(sg));
+                }
+    }
+
+    // b[i] = v at the map's Interface cells (EIGEN_INTERFACE::Copy_To_Eigen_Array),
+    // or b[i] += v (TWO/Interface_Solver/EIGEN_INTERFACE.cpp:33-50, Accumulate_To_Eigen_Array).
+    void to_interface(const std::vector<std::array<int, 3>>& map, std::vector<T>& b, const T* v, bool acc) const {
+        const uint32_t* f = lv[0].flags.data();
+        for (size_t i = 0; i < map.size(); ++i) {
+            const size_t x = d0.at(map[i][0], map[i][1], map[i][2]);
+            if (!(f[x] & INTERFACE)) continue;
+            if (acc) b[i] += v[x];
+            else b[i] = v[x];
+        }
+    }
+    void from_interface(const std::vector<std::array<int, 3>>& map, const std::vector<T>& u, T* v) const {
+        const uint32_t* f = lv[0].flags.data();
+        for (size_t i = 0; i < map.size(); ++i) {
+            const size_t x = d0.at(map[i][0], map[i][1], map[i][2]);
+            if (f[x] & INTERFACE) v[x] = u[i];
+        }
+    }
+
+    // TWO/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Decomposition_Preconditioner.h:127-181
+    // (Subdomain_DD; residual prints dropped): a DD solve inside every
+    // first-level subdomain with the first-level interface values in result
+    // as its boundary data.
+    void subdomain_dd(T* result, const T* rhs, T* tmp) {
+        const size_t n = d0.count();
+        const uint32_t* f = lv[0].flags.data();
+        for (auto& sg : sigma2) std::fill(sg->b[0].begin(), sg->b[0].end(), T(0));
+        std::fill(tmp, tmp + n, T(0));
+        laplace_ir_subdomain<T>(d0, f, result, tmp, sub);
+        for (size_t s = 0; s < sys2.size(); ++s) to_interface(sys2[s]->iface_map, sigma2[s]->b[0], tmp, false);
+        for (int i = 0; i < nvcycles; ++i) v_cycle<T>(lv, result, tmp, rhs, interior, boundary);
+        std::copy(rhs, rhs + n, tmp);
+        laplace_ri<T>(d0, f, result, tmp);
+        for (size_t s = 0; s < sys2.size(); ++s) {
+            to_interface(sys2[s]->iface_map, sigma2[s]->b[0], tmp, true);
+            std::fill(sigma2[s]->u[0].begin(), sigma2[s]->u[0].end(), T(0));
+            for (int i = 0; i < sigma_mg; ++i) sigma2[s]->v_cycle();
+        }
+        std::fill(result, result + n, T(0));
+        std::fill(tmp, tmp + n, T(0));
+        from_interface(sys.iface_map, sigma.u[0], result);
+        for (size_t s = 0; s < sys2.size(); ++s) from_interface(sys2[s]->iface_map, sigma2[s]->u[0], result);
+        for (int i = 0; i < nvcycles; ++i) v_cycle<T>(lv, result, tmp, rhs, interior, boundary);
+    }
+
+    // TWO/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Decomposition_Preconditioner.h:182-230
+    // with multilevel: the subdomain V-cycles replaced by Subdomain_DD, and the
+    // first-level interface right-hand side from Laplace_ri_Subdomain.
+    void apply_two_level(T* result, const T* rhs, T* tmp) {
+        const size_t n = d0.count();
+        const uint32_t* f = lv[0].flags.data();
+        std::fill(sigma.u[0].begin(), sigma.u[0].end(), T(0));
+        std::fill(result, result + n, T(0));
+        std::fill(tmp, tmp + n, T(0));
+        subdomain_dd(result, rhs, tmp);
+        std::copy(rhs, rhs + n, tmp);
+        laplace_ri_subdomain<T>(d0, f, result, tmp, sub);
+        std::fill(sigma.b[0].begin(), sigma.b[0].end(), T(0));
+        to_interface(sys.iface_map, sigma.b[0], tmp, false);
+        std::fill(sigma.u[0].begin(), sigma.u[0].end(), T(0));
+        for (int i = 0; i < sigma_mg; ++i) sigma.v_cycle();
+        std::fill(result, result + n, T(0));
+        std::fill(tmp, tmp + n, T(0));
+        from_interface(sys.iface_map, sigma.u[0], result);
+        subdomain_dd(result, rhs, tmp);
+    }
+
     void project(T* v) const {
         const uint32_t* f = lv[0].flags.data();
         for (size_t x = 0; x < d0.count(); ++x)
@@ -92,6 +216,7 @@ struct Solver : SolverBase {
 
     // SPGrid_Domain_Decomposition_Preconditioner.h:88-128 (debug residual prints dropped).
     void apply_preconditioner(T* result, const T* rhs, T* tmp) {
+        if (multilevel) { apply_two_level(result, rhs, tmp); return; }
         const size_t n = d0.count();
         const uint32_t* f = lv[0].flags.data();
         std::fill(result, result + n, T(0));
@@ -217,9 +342,9 @@ Solver<T>& S(Handle* h) { return *static_cast<Solver<T>*>(h->s.get()); }
 
 extern "C" {
 
-void* hddo_create(const int size[3], const int sub[3], const uint32_t* flags, int vlevels, int nvcycles,
-                  int interior, int boundary, int sigma_levels, int sigma_smoothing, int sigma_mg,
-                  int use_double, char* err, int errlen) {
+void* hddo_create_ml(const int size[3], const int sub[3], const uint32_t* flags, int vlevels, int nvcycles,
+                     int interior, int boundary, int sigma_levels, int sigma_smoothing, int sigma_mg,
+                     int use_double, int multilevel, char* err, int errlen) {
     Handle* h = new Handle();
     h->dbl = use_double != 0;
     try {
@@ -234,6 +359,7 @@ void* hddo_create(const int size[3], const int sub[3], const uint32_t* flags, in
         base->sigma_levels = sigma_levels;
         base->sigma_smoothing = sigma_smoothing;
         base->sigma_mg = sigma_mg;
+        base->multilevel = multilevel;
         base->flags_in.assign(flags, flags + base->d0.count());
         if (h->dbl) S<double>(h).setup(); else S<float>(h).setup();
     } catch (const std::exception& e) {
@@ -242,6 +368,61 @@ void* hddo_create(const int size[3], const int sub[3], const uint32_t* flags, in
         return nullptr;
     }
     return h;
+}
+
+void* hddo_create(const int size[3], const int sub[3], const uint32_t* flags, int vlevels, int nvcycles,
+                  int interior, int boundary, int sigma_levels, int sigma_smoothing, int sigma_mg,
+                  int use_double, char* err, int errlen) {
+    return hddo_create_ml(size, sub, flags, vlevels, nvcycles, interior, boundary, sigma_levels, sigma_smoothing,
+                          sigma_mg, use_double, 0, err, errlen);
+}
+
+// Second-level interface systems of a two-level solver: their count, and
+// each one's level-0 interface size.
+int hddo_num_second_level(void* hp) {
+    Handle* h = static_cast<Handle*>(hp);
+    return DISPATCH(h, (int)s.sys2.size());
+}
+int hddo_second_level_interface(void* hp, int i) {
+    Handle* h = static_cast<Handle*>(hp);
+    return DISPATCH(h, s.sys2[i]->n_iface[0]);
+}
+// Second-level system i: interface DOF count of a level, level-0 interface
+// cells (global), and its matrices as hddo_matrix_shape / hddo_matrix_get.
+int hddo_sl_num_interface(void* hp, int i, int level) {
+    Handle* h = static_cast<Handle*>(hp);
+    return DISPATCH(h, level < (int)s.sys2[i]->n_iface.size() ? s.sys2[i]->n_iface[level] : -1);
+}
+void hddo_sl_interface_map(void* hp, int i, int* out) {
+    Handle* h = static_cast<Handle*>(hp);
+    DISPATCH(h, ([&] { const auto& m = s.sys2[i]->iface_map;
+                       for (size_t r = 0; r < m.size(); ++r)
+                           for (int a = 0; a < 3; ++a) out[3 * r + a] = m[r][a];
+                       return 0; })());
+}
+int hddo_sl_num_subdomains(void* hp, int i) {
+    Handle* h = static_cast<Handle*>(hp);
+    return DISPATCH(h, s.sys2[i]->n_sub);
+}
+int hddo_sl_matrix_shape(void* hp, int i, int kind, int level, int sub, int* rows, int* cols, int* nnz) {
+    Handle* h = static_cast<Handle*>(hp);
+    return DISPATCH(h, ([&] {
+        const auto& y = *s.sys2[i];
+        const auto* m = kind == 0 ? &y.Arr[level] : kind == 1 ? &y.Aii[level][sub]
+                      : kind == 2 ? &y.Air[level][sub] : &y.Prr[level];
+        *rows = m->rows; *cols = m->cols; *nnz = (int)m->col.size();
+        return 0; })());
+}
+int hddo_sl_matrix_get(void* hp, int i, int kind, int level, int sub, int* ptr, int* col, double* val) {
+    Handle* h = static_cast<Handle*>(hp);
+    return DISPATCH(h, ([&] {
+        const auto& y = *s.sys2[i];
+        const auto* m = kind == 0 ? &y.Arr[level] : kind == 1 ? &y.Aii[level][sub]
+                      : kind == 2 ? &y.Air[level][sub] : &y.Prr[level];
+        std::copy(m->ptr.begin(), m->ptr.end(), ptr);
+        std::copy(m->col.begin(), m->col.end(), col);
+        for (size_t r = 0; r < m->val.size(); ++r) val[r] = (double)m->val[r];
+        return 0; })());
 }
 
 void hddo_destroy(void* hp) { delete static_cast<Handle*>(hp); }

@@ -250,6 +250,50 @@ void laplace_ri(const Dims& d, const uint32_t* f, const T* u, T* lu) {
             }
 }
 
+static inline bool on_plane(int i, int j, int k, const int sub[3]) {
+    return i % sub[0] == 0 || j % sub[1] == 0 || k % sub[2] == 0;
+}
+
+template <class T>
+void laplace_ri_subdomain(const Dims& d, const uint32_t* f, const T* u, T* lu, const int sub[3]) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < d.n[0]; ++i)
+        for (int j = 0; j < d.n[1]; ++j)
+            for (int k = 0; k < d.n[2]; ++k) {
+                size_t x = d.at(i, j, k);
+                uint32_t fl = f[x];
+                if (!(fl & (ACTIVE | INTERFACE)) || !on_plane(i, j, k, sub)) continue;
+                double result = 0.;
+                for (int face = 0; face < 6; ++face)
+                    if (fl & (FACE_MX << face)) {
+                        int a = i + FACE_D[face][0], b = j + FACE_D[face][1], c = k + FACE_D[face][2];
+                        if (!(flag_at(d, f, a, b, c) & (ACTIVE | INTERFACE)) || on_plane(a, b, c, sub)) continue;
+                        result -= (double)u[d.at(a, b, c)];
+                    }
+                lu[x] -= (T)result;
+            }
+}
+
+template <class T>
+void laplace_ir_subdomain(const Dims& d, const uint32_t* f, const T* u, T* lu, const int sub[3]) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < d.n[0]; ++i)
+        for (int j = 0; j < d.n[1]; ++j)
+            for (int k = 0; k < d.n[2]; ++k) {
+                size_t x = d.at(i, j, k);
+                uint32_t fl = f[x];
+                if (!(fl & (ACTIVE | INTERFACE)) || on_plane(i, j, k, sub)) continue;
+                double result = 0.;
+                for (int face = 0; face < 6; ++face)
+                    if (fl & (FACE_MX << face)) {
+                        int a = i + FACE_D[face][0], b = j + FACE_D[face][1], c = k + FACE_D[face][2];
+                        if (!(flag_at(d, f, a, b, c) & (ACTIVE | INTERFACE)) || !on_plane(a, b, c, sub)) continue;
+                        result -= (double)u[d.at(a, b, c)];
+                    }
+                lu[x] = -(T)result;
+            }
+}
+
 #define ORACLE_INST(T)                                                                          \
     template void residual<T>(const Dims&, const uint32_t*, const T*, T*, const T*);            \
     template void correction<T>(const Dims&, const uint32_t*, T*, const T*, bool, bool);        \
@@ -257,7 +301,9 @@ void laplace_ri(const Dims& d, const uint32_t* f, const T* u, T* lu) {
     template void prolongation<T>(const Dims&, const uint32_t*, T*, const Dims&, const T*);     \
     template void v_cycle<T>(std::vector<MGLevel<T>>&, T*, T*, const T*, int, int);             \
     template void laplace_ai<T>(const Dims&, const uint32_t*, const T*, T*);                    \
-    template void laplace_ri<T>(const Dims&, const uint32_t*, const T*, T*);
+    template void laplace_ri<T>(const Dims&, const uint32_t*, const T*, T*);                    \
+    template void laplace_ri_subdomain<T>(const Dims&, const uint32_t*, const T*, T*, const int*); \
+    template void laplace_ir_subdomain<T>(const Dims&, const uint32_t*, const T*, T*, const int*);
 ORACLE_INST(float)
 ORACLE_INST(double)
 

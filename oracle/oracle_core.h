@@ -132,4 +132,18 @@ void laplace_ai(const Dims& d, const uint32_t* f, const T* u, T* lu);
 template <class T>
 void laplace_ri(const Dims& d, const uint32_t* f, const T* u, T* lu);
 
+// Two-level DD (demos/Domain_Decomposition_CPU_Only_Two_Levels, "TWO/"):
+// a cell is on a first-level plane when any index is a multiple of sub.
+// TWO/SPGrid_Library/SPGrid_Laplace_Legacy.h:120-178 (Laplace_ri_Subdomain):
+// at Active|Interface cells on a first-level plane, Lu -= (T)(-sum over
+// active-face Active|Interface neighbours off the planes of u_n).
+template <class T>
+void laplace_ri_subdomain(const Dims& d, const uint32_t* f, const T* u, T* lu, const int sub[3]);
+
+// TWO/SPGrid_Library/SPGrid_Laplace_Legacy.h:232-290 (Laplace_ir_Subdomain):
+// at Active|Interface cells off the first-level planes, Lu = -(T)(-sum over
+// active-face Active|Interface neighbours on the planes of u_n).
+template <class T>
+void laplace_ir_subdomain(const Dims& d, const uint32_t* f, const T* u, T* lu, const int sub[3]);
+
 }  // namespace oracle

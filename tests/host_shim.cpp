@@ -58,6 +58,34 @@ void* shim_build(const int size[3], const int sub[3], int vlevels, int sigma_lev
     }
 }
 
+// The product's two-level second-level interface system: every first-level
+// subdomain's system (first-level planes made Dirichlet, boxes of sub/2),
+// stacked block-diagonally.  NULL on error.
+void* shim_build_second_level(const int size[3], const int sub[3], int sigma_levels, const uint32_t* flags,
+                              char* err, int errlen) {
+    Shim* s = new Shim();
+    try {
+        for (int a = 0; a < 3; ++a) { s->L.opt.size[a] = size[a]; s->L.opt.sub[a] = sub[a]; }
+        s->L.opt.sigma_levels = sigma_levels;
+        s->L.flags_in.assign(flags, flags + (size_t)size[0] * size[1] * size[2]);
+        build_second_level(s->L, sub, sigma_levels, s->ih);
+        return s;
+    } catch (const std::exception& e) {
+        if (err && errlen > 0) { std::strncpy(err, e.what(), errlen - 1); err[errlen - 1] = 0; }
+        delete s;
+        return nullptr;
+    }
+}
+
+// 1 when the layout runs the whole-grid V-cycle (coarse levels couple boxes).
+int shim_global_vcycle(void* h) { return static_cast<Shim*>(h)->L.global_vcycle ? 1 : 0; }
+
+// Interface DOF count of a level.
+int shim_num_interface(void* h, int level) {
+    const InterfaceHost& ih = static_cast<Shim*>(h)->ih;
+    return level >= 0 && level < (int)ih.n_iface.size() ? ih.n_iface[level] : -1;
+}
+
 void shim_free(void* h) { delete static_cast<Shim*>(h); }
 
 // Factors a matrix of ncomp disconnected path graphs of csize vertices each

@@ -32,6 +32,15 @@ def lib():
         vp, ip, up, dp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_uint32), C.POINTER(C.c_double)
         L.hddo_create.restype = vp
         L.hddo_create.argtypes = [ip, ip, up] + [C.c_int] * 8 + [C.c_char_p, C.c_int]
+        L.hddo_create_ml.restype = vp
+        L.hddo_create_ml.argtypes = [ip, ip, up] + [C.c_int] * 9 + [C.c_char_p, C.c_int]
+        L.hddo_num_second_level.argtypes = [vp]
+        L.hddo_second_level_interface.argtypes = [vp, C.c_int]
+        L.hddo_sl_num_interface.argtypes = [vp, C.c_int, C.c_int]
+        L.hddo_sl_interface_map.argtypes = [vp, C.c_int, ip]
+        L.hddo_sl_num_subdomains.argtypes = [vp, C.c_int]
+        L.hddo_sl_matrix_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, ip]
+        L.hddo_sl_matrix_get.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, dp]
         L.hddo_destroy.argtypes = [vp]
         L.hddo_num_levels.argtypes = [vp]
         L.hddo_level_dims.argtypes = [vp, C.c_int, ip]
@@ -66,7 +75,7 @@ class Oracle:
 
     def __init__(self, size, sub_size, flags, vlevels=3, nVcycles=1, interior_smoothing=1,
                  boundary_smoothing=3, sigma_levels=3, sigma_smoothing=3, sigma_mg=1,
-                 dtype=np.float32):
+                 dtype=np.float32, multilevel=False):
         L = lib()
         self.size = tuple(int(s) for s in size)
         self.dtype = np.dtype(dtype)
@@ -75,9 +84,9 @@ class Oracle:
         sz = (C.c_int * 3)(*self.size)
         sb = (C.c_int * 3)(*[int(s) for s in sub_size])
         err = C.create_string_buffer(512)
-        self.h = L.hddo_create(sz, sb, _p(flags, C.c_uint32), vlevels, nVcycles, interior_smoothing,
-                               boundary_smoothing, sigma_levels, sigma_smoothing, sigma_mg,
-                               1 if self.dtype == np.float64 else 0, err, 512)
+        self.h = L.hddo_create_ml(sz, sb, _p(flags, C.c_uint32), vlevels, nVcycles, interior_smoothing,
+                                  boundary_smoothing, sigma_levels, sigma_smoothing, sigma_mg,
+                                  1 if self.dtype == np.float64 else 0, 1 if multilevel else 0, err, 512)
         if not self.h:
             raise RuntimeError("oracle setup failed: " + err.value.decode())
 
@@ -108,6 +117,29 @@ class Oracle:
 
     def num_interface(self, level=0):
         return lib().hddo_num_interface(self.h, level)
+
+    def second_level_sizes(self):
+        """Level-0 interface sizes of a two-level solver's per-subdomain systems."""
+        return [lib().hddo_second_level_interface(self.h, i) for i in range(lib().hddo_num_second_level(self.h))]
+
+    def second_level_map(self, i):
+        """Level-0 interface cells (global) of second-level system i."""
+        n = lib().hddo_sl_num_interface(self.h, i, 0)
+        out = np.zeros((n, 3), np.int32)
+        lib().hddo_sl_interface_map(self.h, i, _p(out, C.c_int))
+        return out
+
+    def second_level_matrix(self, i, kind, level, sub=0):
+        """Matrix of second-level system i, as matrix()."""
+        import scipy.sparse as sp
+        k = {"Arr": 0, "Aii": 1, "Air": 2, "Prr": 3}[kind]
+        r, c, nnz = C.c_int(), C.c_int(), C.c_int()
+        lib().hddo_sl_matrix_shape(self.h, i, k, level, sub, C.byref(r), C.byref(c), C.byref(nnz))
+        ptr = np.zeros(r.value + 1, np.int32)
+        col = np.zeros(nnz.value, np.int32)
+        val = np.zeros(nnz.value, np.float64)
+        lib().hddo_sl_matrix_get(self.h, i, k, level, sub, _p(ptr, C.c_int), _p(col, C.c_int), _p(val, C.c_double))
+        return sp.csr_matrix((val, col, ptr), shape=(r.value, c.value))
 
     def interface_map(self):
         n = self.num_interface(0)

@@ -28,6 +28,10 @@ def load_shim():
     L.shim_build.restype = C.c_void_p
     L.shim_build.argtypes = [ip, ip, C.c_int, C.c_int, C.POINTER(C.c_uint32), C.c_char_p, C.c_int]
     L.shim_free.argtypes = [C.c_void_p]
+    L.shim_build_second_level.restype = C.c_void_p
+    L.shim_build_second_level.argtypes = [ip, ip, C.c_int, C.POINTER(C.c_uint32), C.c_char_p, C.c_int]
+    L.shim_num_interface.argtypes = [C.c_void_p, C.c_int]
+    L.shim_global_vcycle.argtypes = [C.c_void_p]
     L.shim_num_subdomains.argtypes = [C.c_void_p]
     L.shim_matrix_shape.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, ip]
     L.shim_matrix_get.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, ip, ip, C.POINTER(C.c_double)]

@@ -43,6 +43,20 @@ def test_options_default_match_test_bench(hdd_lib):
     assert o.vlevels == 3 and o.nVcycles == 1 and o.interior_smoothing == 1 and o.boundary_smoothing == 3
     assert o.sigma_levels == 3 and o.sigma_smoothing == 3 and o.sigma_mg == 1
     assert o.max_iters == 5000 and o.relative_tol == 1 and abs(o.tol - 1e-6) < 1e-18
+    assert o.multilevel == 0  # -multilevel no
+
+
+@pytest.mark.parametrize("multilevel,sub,status", [(2, 64, 1), (1, 15, 1), (1, 24, 5), (1, 128, 5)])
+def test_two_level_options_are_checked_before_any_gpu_call(hdd_lib, multilevel, sub, status):
+    """multilevel must be 0 or 1; two-level DD needs an even sub_size whose half
+    is a V-cycle box size (8, 16, 32): refused before the device is touched."""
+    o = _lib.hdd_options()
+    hdd_lib.hdd_options_default(C.byref(o))
+    o.multilevel = multilevel
+    for a in range(3):
+        o.sub_size[a] = sub
+    h = C.c_void_p()
+    assert hdd_lib.hdd_create(C.byref(o), C.byref(h)) == status and not h.value
 
 
 def test_status_strings(hdd_lib):

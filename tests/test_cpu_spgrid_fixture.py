@@ -8,9 +8,9 @@ artifact the reference ships: the 2D directory written by Create_2D_Domain
   the digests in tests/golden/spgrid2d_fixture.json (made by
   tests/golden/make_spgrid2d_golden.py), and against the directory itself
   where the reference tree is present;
-* the generator's Neumann bubble in 3D: the oracle solves it, the product's
-  host setup rejects it with a status (its per-subdomain V-cycle boxes would
-  couple at coarse levels).
+* the generator's Neumann bubble in 3D: the oracle solves it; the product's
+  host setup takes it with the whole-grid V-cycle (its subdomain boxes couple
+  at coarse levels) and assembles the oracle's interface matrices bit for bit.
 """
 import ctypes as C
 import hashlib
@@ -63,8 +63,11 @@ def test_reference_2d_directory_decodes_to_the_generator():
     assert np.array_equal(data, d.rhs)
 
 
-def test_neumann_bubble_3d_oracle_solves_product_rejects():
-    from test_cpu_host import shim as shim_fixture
+def test_neumann_bubble_3d_oracle_solves_product_accepts():
+    """The generator's Neumann bubble couples subdomain boxes at coarse V-cycle
+    levels: the oracle solves it, and the product's layout takes it with the
+    whole-grid V-cycle and assembles the same interface matrices bit for bit."""
+    from test_cpu_host import matrix, shim as shim_fixture
     d = domains.reference_generator((35, 35, 35), (4, 16, 16))
     assert np.any(d.flags == 0) and d.n_active > 0
     o = Oracle(d.size, (8, 8, 8), d.flags, vlevels=3, nVcycles=1, interior_smoothing=3, boundary_smoothing=3,
@@ -77,4 +80,22 @@ def test_neumann_bubble_3d_oracle_solves_product_rejects():
     flags = np.ascontiguousarray(d.flags, np.uint32)
     err = C.create_string_buffer(512)
     h = lib.shim_build(size, sub, 3, 2, flags.ctypes.data_as(C.POINTER(C.c_uint32)), err, 512)
-    assert not h and b"exterior cells face-adjacent to Active cells" in err.value
+    assert h, err.value
+    try:
+        assert lib.shim_global_vcycle(h) == 1
+        # A Dirichlet-sphere domain keeps the per-box V-cycle.
+        ds = domains.small(32, 8, 6, seed=1)
+        fs = np.ascontiguousarray(ds.flags, np.uint32)
+        hs = lib.shim_build((C.c_int * 3)(*ds.size), sub, 3, 2, fs.ctypes.data_as(C.POINTER(C.c_uint32)), err, 512)
+        assert hs, err.value
+        assert lib.shim_global_vcycle(hs) == 0
+        lib.shim_free(hs)
+        for l in range(2):
+            a, b = matrix(lib, h, 0, l), o.matrix("Arr", l)
+            assert a.shape == b.shape and (a != b).nnz == 0, l
+            for sd in range(lib.shim_num_subdomains(h)):
+                for kind, name in ((1, "Aii"), (2, "Air")):
+                    a, b = matrix(lib, h, kind, l, sd), o.matrix(name, l, sd)
+                    assert a.shape == b.shape and (a != b).nnz == 0, (name, l, sd)
+    finally:
+        lib.shim_free(h)

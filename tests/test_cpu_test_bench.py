@@ -28,12 +28,12 @@ def test_help_lists_the_reference_flags(cli):
     assert p.returncode == 0
     for flag in ("-size", "-sub_size", "-vlevels", "-sigma_levels", "-sigma_smoothing", "-sigma_mg",
                  "-interior_smoothing", "-boundary_smoothing", "-nVcycles", "-threads", "-d", "-o", "-mode",
-                 "-iomode"):
+                 "-iomode", "-multilevel"):
         assert flag in p.stdout, flag
 
 
 @pytest.mark.parametrize("args", [("-bogus",), ("-size", "33", "33"), ("-vlevels", "x"), ("-iomode", "both"),
-                                  ("-precision", "half"), ("-mode", "no_convertion")])
+                                  ("-precision", "half"), ("-mode", "no_convertion"), ("-multilevel", "maybe")])
 def test_usage_errors_exit_2(cli, args):
     p = run(cli, *args)
     assert p.returncode == 2 and "usage" in p.stderr, (args, p.stderr)

@@ -1,0 +1,180 @@
+"""Two-level DD (the reference's -multilevel yes,
+demos/Domain_Decomposition_CPU_Only_Two_Levels) on the GPU, through the C ABI,
+against the oracle's two-level restatement:
+
+* the V-cycles run on boxes of sub/2 and are bit-exact against the oracle's;
+* the two-level preconditioner matches the oracle within 1e-4 relative
+  max-norm (the sigma solves' FP32 rounding, as for one level);
+* PCG iterations within +-1 of the FP32 oracle's, the true residual, and the
+  solution within 1e-5 relative L2 of the FP32 oracle's, on small and ragged
+  domains;
+* the demo's own defaults (64^3 subdomains, so 32^3 V-cycle boxes on the
+  cluster kernel, vlevels 3, smoothing 1/3, sigma_levels 3) at 128^3 and at the
+  256^3 workload's domain, against the oracle's full solves in
+  tests/golden/two_level_oracle.npz (tests/golden/make_two_level_fixture.py);
+* the solve server takes two-level domains (one system per context, whatever
+  its batch option) and returns the same bits as a solo solve.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from hierarchicaldd_b200 import domains
+from hierarchicaldd_b200.domains import ACTIVE, INTERFACE
+from oracle_ffi import Oracle
+
+pytestmark = pytest.mark.gpu
+
+PRECOND_RTOL = 1e-4
+FIXTURE = os.path.join(ROOT, "tests", "golden", "two_level_oracle.npz")
+
+
+def _meta(d, **over):
+    m = dict(d.meta, multilevel=True)
+    m.update(over)
+    return m
+
+
+def make_solver(d, m, **kw):
+    from hierarchicaldd_b200.solver import SPGrid_Domain_Decomposition_Solver
+    s = SPGrid_Domain_Decomposition_Solver()
+    s.Set_Domain(d.flags, d.rhs)
+    s.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"],
+                                m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"],
+                                m["sigma_mg"], multilevel=True, **kw)
+    return s
+
+
+def make_oracle(d, m, dtype=np.float32):
+    return Oracle(d.size, d.sub_size, d.flags, vlevels=m["vlevels"], nVcycles=m["nVcycles"],
+                  interior_smoothing=m["interior_smoothing"], boundary_smoothing=m["boundary_smoothing"],
+                  sigma_levels=m["sigma_levels"], sigma_smoothing=m["sigma_smoothing"], sigma_mg=m["sigma_mg"],
+                  dtype=dtype, multilevel=True)
+
+
+def rel_inf(a, b):
+    return float(np.max(np.abs(a.astype(np.float64) - b)) / max(np.max(np.abs(b)), 1e-30))
+
+
+CASES = [(32, 16, 6), ((40, 36, 44), 16, 6), (64, 16, 12)]
+
+
+@pytest.mark.parametrize("n,sub,radius", CASES)
+def test_two_level_vcycle_preconditioner_and_pcg(n, sub, radius):
+    d = domains.small(n, sub, radius, seed=5)
+    m = _meta(d, sigma_levels=2)
+    s = make_solver(d, m)
+    o = make_oracle(d, m)
+    try:
+        f0 = o.level_flags(0)
+        rng = np.random.default_rng(12)
+        # V-cycles on boxes of sub/2: bit-exact.
+        u = rng.standard_normal(d.size).astype(np.float32)
+        u[(f0 & (ACTIVE | INTERFACE)) == 0] = 0
+        b = rng.standard_normal(d.size).astype(np.float32)
+        b[(f0 & ACTIVE) == 0] = 0
+        ug = s.V_Cycle(u, b, 1)
+        uo, _ = o.vcycle(u, np.zeros_like(u), b)
+        assert np.array_equal(ug, uo), np.max(np.abs(ug - uo))
+        # The two-level preconditioner.
+        r = rng.standard_normal(d.size).astype(np.float32)
+        r[(f0 & (ACTIVE | INTERFACE)) == 0] = 0
+        assert rel_inf(s.Apply_Preconditioner(r), o.apply_preconditioner(r)) < PRECOND_RTOL
+        # PCG.
+        res = s.Solve()
+        xo, it_o, info = o.solve(d.rhs, tol=1e-6)
+        assert res["converged"] == 1
+        assert abs(res["iterations"] - it_o) <= 1, (res["iterations"], it_o)
+        assert res["true_residual_inf"] <= max(2e-6, 2 * info["true_res_inf"] / info["b_inf"])
+        x = s.Solution()
+        assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-5
+    finally:
+        s.close()
+
+
+def _fixture():
+    if not os.path.exists(FIXTURE):
+        pytest.skip("tests/golden/two_level_oracle.npz missing (tests/golden/make_two_level_fixture.py)")
+    return np.load(FIXTURE)
+
+
+def test_two_level_demo_defaults_128():
+    """The demo's defaults at 128^3: iteration parity with the FP32 oracle, its
+    max|r| history to 1 % over the first 10 iterations, and the solution of the
+    precision form at 1e-8 within 1e-5 relative L2 of the FP64 oracle's."""
+    g = _fixture()
+    d = domains.two_level_case()
+    m = d.meta
+    s = make_solver(d, m)
+    try:
+        res = s.Solve()
+        assert res["converged"] == 1
+        it_o = int(g["tl128_iterations_fp32"])
+        assert abs(res["iterations"] - it_o) <= 1, (res["iterations"], it_o)
+        h = s.Residual_History()
+        ho = g["tl128_history_fp32"]
+        k = min(10, len(h), len(ho))
+        assert np.all(np.abs(h[:k] - ho[:k]) <= 0.01 * ho[:k]), (h[:k], ho[:k])
+        s.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"],
+                                    m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"],
+                                    m["sigma_mg"], multilevel=True, tol=1e-8, precision_mode=1)
+        res8 = s.Solve()
+        assert res8["converged"] == 1
+        st = int(g["stride"])
+        x = s.Solution_F64()[::st, ::st, ::st]
+        x64 = g["tl128_x64_sub"].astype(np.float64)
+        assert np.linalg.norm(x - x64) / np.linalg.norm(x64) < 1e-5
+    finally:
+        s.close()
+
+
+def test_two_level_256_workload_iterations():
+    """The 256^3 workload's domain under two-level DD at the demo's defaults:
+    iteration parity with the FP32 oracle and the true residual."""
+    g = _fixture()
+    d = domains.config2_two_level()
+    s = make_solver(d, d.meta)
+    try:
+        res = s.Solve()
+        assert res["converged"] == 1
+        it_o = int(g["c2ml_iterations_fp32"])
+        assert abs(res["iterations"] - it_o) <= 1, (res["iterations"], it_o)
+        assert res["true_residual_inf"] <= 1e-5
+    finally:
+        s.close()
+
+
+def test_server_two_level_domain_equals_solo():
+    from hierarchicaldd_b200.server import SolveServer, make_options
+    d = domains.small(48, 16, 9, seed=8)
+    m = _meta(d, sigma_levels=2)
+    opts = make_options(d.size, d.sub_size, **{k: v for k, v in m.items() if k != "multilevel"},
+                        multilevel=1, tol=1e-6)
+    rng = np.random.default_rng(3)
+    rhs = []
+    for _ in range(3):
+        r = rng.uniform(-1, 1, d.size).astype(np.float32)
+        r[(d.flags & ACTIVE) == 0] = 0
+        rhs.append(r)
+    solo = []
+    s = make_solver(d, m, tol=1e-6)
+    try:
+        for r in rhs:
+            s.Set_RHS(r)
+            s.Solve()
+            solo.append(s.Solution())
+    finally:
+        s.close()
+    srv = SolveServer(slots=2, batch=4)
+    try:
+        dom = srv.add_domain(d.flags, opts)
+        assert srv.wait_domain(dom)
+        ids = [srv.submit(dom, r) for r in rhs]
+        for i, rid in enumerate(ids):
+            st, res, x, _ = srv.poll(rid, dom)
+            assert st == 0 and res["converged"] == 1
+            assert np.array_equal(x, solo[i])
+    finally:
+        srv.close()
