@@ -64,6 +64,9 @@ SIGNATURES = {
     "hdd_options_default": (None, [C.POINTER(hdd_options)]),
     "hdd_create": (C.c_int, [C.POINTER(hdd_options), C.POINTER(C.c_void_p)]),
     "hdd_set_domain_dense": (C.c_int, [_vp, C.POINTER(C.c_uint32), _fp]),
+    "hdd_velocity_divergence_dense": (C.c_int, [_vp, C.POINTER(C.c_uint32), _fp, _fp, _fp, C.c_float,
+                                                C.POINTER(C.c_uint32), _fp]),
+    "hdd_set_domain_velocity_dense": (C.c_int, [_vp, C.POINTER(C.c_uint32), _fp, _fp, _fp, C.c_float]),
     "hdd_load_spgrid_dir": (C.c_int, [_vp, C.c_char_p]),
     "hdd_set_domain_pages": (C.c_int, [_vp, C.c_longlong, _ip, C.POINTER(C.c_uint32), _fp]),
     "hdd_set_rhs_pages": (C.c_int, [_vp, C.c_longlong, _ip, _fp]),

@@ -32,6 +32,7 @@ SOURCES = [
     "sn_solve.cu",
     "solver.cu",
     "noalloc.cu",
+    "velocity.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -1,4 +1,5 @@
 // C ABI (include/hdd.h): status codes instead of exceptions, opaque handles.
+#include <cmath>
 #include <cstring>
 #include <fstream>
 #include <new>
@@ -8,6 +9,7 @@
 
 #include "noalloc.h"
 #include "solver.h"
+#include "velocity.h"
 
 using hdd::Error;
 using hdd::Solver;
@@ -120,6 +122,49 @@ hdd_status hdd_create(const hdd_options* opts, hdd_solver** out) {
 hdd_status hdd_set_domain_dense(hdd_solver* s, const uint32_t* flags, const float* rhs) {
     if (!flags || !rhs) return HDD_ERR_INVALID_ARGUMENT;
     return guard(s, [&](Solver& v) { v.set_domain(flags, rhs); });
+}
+
+namespace {
+// Runs the velocity conversion on the solver's device into host flags/rhs.
+void velocity_to_domain(Solver& v, const uint32_t* ff, const float* u, const float* vv, const float* w, float dx,
+                        uint32_t* flags_out, float* rhs_out) {
+    if (!(dx > 0.0f) || !std::isfinite(dx)) throw Error(HDD_ERR_INVALID_ARGUMENT, "dx must be positive and finite");
+    hdd::cuda_check(cudaSetDevice(v.opts.device), "cudaSetDevice");
+    const size_t N = (size_t)v.opts.size[0] * v.opts.size[1] * v.opts.size[2];
+    hdd::DevBuf<uint32_t> dff, dfo;
+    hdd::DevBuf<float> du, dv, dw, dr;
+    cudaStream_t st = v.stream;
+    dff.upload(ff, N, st);
+    du.upload(u, N, st);
+    dv.upload(vv, N, st);
+    dw.upload(w, N, st);
+    dfo.alloc(N);
+    dr.alloc(N);
+    hdd::cuda_check(hdd::launch_velocity_divergence(v.opts.size, dff.p, du.p, dv.p, dw.p, dx, dfo.p, dr.p, st),
+                    "velocity divergence");
+    v.count(v.w0);
+    hdd::cuda_check(cudaMemcpyAsync(flags_out, dfo.p, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "D2H");
+    hdd::cuda_check(cudaMemcpyAsync(rhs_out, dr.p, N * sizeof(float), cudaMemcpyDeviceToHost, st), "D2H");
+    v.sync();
+}
+}  // namespace
+
+hdd_status hdd_velocity_divergence_dense(hdd_solver* s, const uint32_t* fluid_flags, const float* u, const float* v,
+                                         const float* w, float dx, uint32_t* flags_out, float* rhs_out) {
+    if (!fluid_flags || !u || !v || !w || !flags_out || !rhs_out) return HDD_ERR_INVALID_ARGUMENT;
+    return guard(s, [&](Solver& sv) { velocity_to_domain(sv, fluid_flags, u, v, w, dx, flags_out, rhs_out); });
+}
+
+hdd_status hdd_set_domain_velocity_dense(hdd_solver* s, const uint32_t* fluid_flags, const float* u, const float* v,
+                                         const float* w, float dx) {
+    if (!fluid_flags || !u || !v || !w) return HDD_ERR_INVALID_ARGUMENT;
+    return guard(s, [&](Solver& sv) {
+        const size_t N = (size_t)sv.opts.size[0] * sv.opts.size[1] * sv.opts.size[2];
+        std::vector<uint32_t> f(N);
+        std::vector<float> b(N);
+        velocity_to_domain(sv, fluid_flags, u, v, w, dx, f.data(), b.data());
+        sv.set_domain(std::move(f), std::move(b));
+    });
 }
 
 hdd_status hdd_set_domain_pages(hdd_solver* s, long long n_pages, const int32_t* page_origin,

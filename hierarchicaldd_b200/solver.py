@@ -38,6 +38,7 @@ class SPGrid_Domain_Decomposition_Solver:
         self.spgrid_dir = None
         self.spgrid_size = None
         self.pages = None
+        self.velocity = None
         self.last_result = None
         self.options = None
 
@@ -54,6 +55,7 @@ class SPGrid_Domain_Decomposition_Solver:
         self.spgrid_dir = base_dir
         self.flags = self.rhs = None
         self.pages = None
+        self.velocity = None
 
     def Set_Domain_Pages(self, page_origin: np.ndarray, flags: np.ndarray, rhs: np.ndarray):
         """SPGrid pages of 4x8x8 cells, as Convert/Copy read them from an SPGrid
@@ -67,12 +69,28 @@ class SPGrid_Domain_Decomposition_Solver:
         self.size = None
         self.spgrid_dir = None
         self.flags = self.rhs = None
+        self.velocity = None
 
     def Set_Domain(self, flags: np.ndarray, rhs: np.ndarray):
         """Dense flags (uint32, reference bits) and right-hand side (float32)."""
         self.size = tuple(int(v) for v in flags.shape)
         self.flags = np.ascontiguousarray(flags, np.uint32)
         self.rhs = np.ascontiguousarray(rhs, np.float32)
+        self.spgrid_dir = None
+        self.pages = None
+        self.velocity = None
+
+    def Set_Domain_Velocity(self, fluid_flags: np.ndarray, u: np.ndarray, v: np.ndarray, w: np.ndarray,
+                            dx: float):
+        """The Test_Bench "velocity" mode on a uniform grid (Test_Bench_3D/main.cpp:317-324):
+        the right-hand side is the divergence of the face velocities (u on each
+        cell's -x face, v, w likewise) and the flags are converted from the
+        SPGrid_Fluids bits, on the GPU when Initialize_Preconditioner loads the
+        domain (hdd_set_domain_velocity_dense)."""
+        self.size = tuple(int(x) for x in fluid_flags.shape)
+        f32 = lambda a: np.ascontiguousarray(a, np.float32)
+        self.velocity = (np.ascontiguousarray(fluid_flags, np.uint32), f32(u), f32(v), f32(w), float(dx))
+        self.flags = self.rhs = None
         self.spgrid_dir = None
         self.pages = None
 
@@ -128,6 +146,10 @@ class SPGrid_Domain_Decomposition_Solver:
             origin, flags, rhs = self.pages
             self._check(self.lib.hdd_set_domain_pages(self.h, origin.shape[0], _ip(origin),
                                                       flags.ctypes.data_as(C.POINTER(C.c_uint32)), _fp(rhs)))
+        elif self.velocity is not None:
+            ff, u, v, w, dx = self.velocity
+            self._check(self.lib.hdd_set_domain_velocity_dense(self.h, ff.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                                               _fp(u), _fp(v), _fp(w), dx))
         else:
             self._check(self.lib.hdd_set_domain_dense(self.h, self.flags.ctypes.data_as(C.POINTER(C.c_uint32)),
                                                       _fp(self.rhs)))

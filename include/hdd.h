@@ -113,6 +113,23 @@ hdd_status hdd_create(const hdd_options* opts, hdd_solver** out);
  * loads cell flags and the right-hand side b. */
 hdd_status hdd_set_domain_dense(hdd_solver* s, const uint32_t* flags, const float* rhs);
 
+/* The Test_Bench "velocity" mode on a uniform grid (GPU/Test_Bench_3D/main.cpp:317-324):
+ * GRID_HIERARCHY_PROJECTION::Compute_Divergence of the face velocities u, v, w
+ * (Divergence_Helper, scale (1/dx)^3 * (-dx^2)) at Interior|Ghost fluid cells,
+ * then Convert's flags (fluid Dirichlet 0x2 -> Dirichlet, else fluid Active 0x8
+ * -> Active, else exterior; SPGrid_Convertor.h:213-236), computed on the GPU.
+ * fluid_flags use the SPGrid_Fluids bits (Interior 0x1, Dirichlet 0x2, Ghost 0x4,
+ * Active 0x8, face X/Y/Z valid 0x10/0x20/0x40); u[c] is the velocity on cell c's
+ * -x face (v, w likewise), all dense over opts.size cells.
+ * hdd_velocity_divergence_dense writes the converted flags and the right-hand
+ * side to flags_out and rhs_out; hdd_set_domain_velocity_dense loads them as
+ * hdd_set_domain_dense would.  The adaptive multi-level SPGrid_Fluids hierarchy
+ * (its ghost-value accumulation across levels) is not implemented. */
+hdd_status hdd_velocity_divergence_dense(hdd_solver* s, const uint32_t* fluid_flags, const float* u, const float* v,
+                                         const float* w, float dx, uint32_t* flags_out, float* rhs_out);
+hdd_status hdd_set_domain_velocity_dense(hdd_solver* s, const uint32_t* fluid_flags, const float* u, const float* v,
+                                         const float* w, float dx);
+
 /* Sparse input in SPGrid pages, for callers holding an SPGrid allocator:
  * replaces Convert / Copy (SPGrid_Domain_Decomposition_Solver.h:73-105 of the
  * CPU demo), which read the flags and right-hand side channels page by page.

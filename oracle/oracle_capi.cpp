@@ -425,6 +425,50 @@ int hddo_sl_matrix_get(void* hp, int i, int kind, int level, int sub, int* ptr, 
         return 0; })());
 }
 
+// The Test_Bench "velocity" mode on a uniform (single-level) grid:
+//   PB/Common_Libraries/SPGrid_Fluids/Projection/Divergence_Helper.cpp:150-240 (3D
+//   Run_Index_Range): at Interior|Ghost cells, result (T) starts at 0 and takes
+//   -= scale * u_face(cell) when the cell's face is valid, += scale *
+//   u_face(cell + e) when the neighbour's is, for x, y, z in turn, each in double
+//   and rounded to T;
+//   GRID_HIERARCHY_PROJECTION.h:31-42 (OLD_SCALING): scale = (1/dx)^3 * (-dx * dx)
+//   with one_over_dX = 1/dX in T;
+//   GPU/SPGrid_Domain_Decomposition_Solver/SPGrid_Convertor.h:213-236: the
+//   solver's flags are Dirichlet where the fluid cell is Dirichlet, else
+//   Active where it is Active, else exterior.
+// Fluid flag bits (FLUIDS_SIMULATION_FLAGS.h:13-25): Interior 0x1, Dirichlet
+// 0x2, Ghost 0x4, Active 0x8, face X/Y/Z valid 0x10/0x20/0x40.  Arrays are
+// dense x-slowest over size[0..2] cells; a neighbour outside the grid counts
+// as invalid.
+void hddo_velocity_divergence(const int size[3], const uint32_t* fflags, const float* u, const float* v,
+                              const float* w, float dx, uint32_t* flags_out, float* rhs_out) {
+    const Dims d{{size[0], size[1], size[2]}};
+    const float odx = 1.0f / dx;
+    const double scale = ((double)odx * (double)odx * (double)odx) * ((double)(-1.) * (double)dx * (double)dx);
+    const float* vel[3] = {u, v, w};
+    const uint32_t valid[3] = {0x10u, 0x20u, 0x40u};
+    for (int i = 0; i < d.n[0]; ++i)
+        for (int j = 0; j < d.n[1]; ++j)
+            for (int k = 0; k < d.n[2]; ++k) {
+                const size_t x = d.at(i, j, k);
+                const uint32_t f = fflags[x];
+                flags_out[x] = (f & 0x2u) ? DIRICHLET : ((f & 0x8u) ? ACTIVE : 0u);
+                float result = 0;
+                if (f & (0x1u | 0x4u)) {
+                    for (int a = 0; a < 3; ++a) {
+                        const int ni = i + (a == 0), nj = j + (a == 1), nk = k + (a == 2);
+                        const bool in = ni < d.n[0] && nj < d.n[1] && nk < d.n[2];
+                        const uint32_t fp = in ? fflags[d.at(ni, nj, nk)] : 0u;
+                        const double cur = (double)vel[a][x];
+                        const double plus = in ? (double)vel[a][d.at(ni, nj, nk)] : 0.0;
+                        if (f & valid[a]) result = (float)((double)result - scale * cur);
+                        if (fp & valid[a]) result = (float)((double)result + scale * plus);
+                    }
+                }
+                rhs_out[x] = result;
+            }
+}
+
 void hddo_destroy(void* hp) { delete static_cast<Handle*>(hp); }
 
 int hddo_num_levels(void* hp) { return static_cast<Handle*>(hp)->s->num_levels(); }

@@ -36,6 +36,7 @@ def lib():
         L.hddo_create_ml.argtypes = [ip, ip, up] + [C.c_int] * 9 + [C.c_char_p, C.c_int]
         L.hddo_num_second_level.argtypes = [vp]
         L.hddo_second_level_interface.argtypes = [vp, C.c_int]
+        L.hddo_velocity_divergence.argtypes = [ip, up, vp, vp, vp, C.c_float, up, vp]
         L.hddo_sl_num_interface.argtypes = [vp, C.c_int, C.c_int]
         L.hddo_sl_interface_map.argtypes = [vp, C.c_int, ip]
         L.hddo_sl_num_subdomains.argtypes = [vp, C.c_int]
@@ -68,6 +69,19 @@ def lib():
 
 def _p(a, t):
     return a.ctypes.data_as(C.POINTER(t))
+
+
+def velocity_divergence(fluid_flags, u, v, w, dx):
+    """The oracle's velocity -> divergence right-hand side and converted flags
+    (the Test_Bench "velocity" mode on a uniform grid): (flags, rhs)."""
+    ff = np.ascontiguousarray(fluid_flags, np.uint32)
+    f32 = [np.ascontiguousarray(a, np.float32) for a in (u, v, w)]
+    flags = np.zeros(ff.shape, np.uint32)
+    rhs = np.zeros(ff.shape, np.float32)
+    size = (C.c_int * 3)(*ff.shape)
+    lib().hddo_velocity_divergence(size, _p(ff, C.c_uint32), f32[0].ctypes.data, f32[1].ctypes.data,
+                                   f32[2].ctypes.data, float(dx), _p(flags, C.c_uint32), rhs.ctypes.data)
+    return flags, rhs
 
 
 class Oracle:
