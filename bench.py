@@ -203,9 +203,9 @@ def oracle_iterations(cfg):
             return int(np.load(path)["iterations_fp32"]), "tests/golden/c2_oracle.npz (full FP32 oracle solve)"
     if cfg in ("c2ml", "tl128"):
         path = os.path.join(ROOT, "tests", "golden", "two_level_oracle.npz")
-        if os.path.exists(path):
-            return (int(np.load(path)[f"{cfg}_iterations_fp32"]),
-                    "tests/golden/two_level_oracle.npz (full FP32 oracle solve)")
+        key = f"{cfg}_iterations_fp32"
+        if os.path.exists(path) and key in np.load(path).files:
+            return int(np.load(path)[key]), "tests/golden/two_level_oracle.npz (full FP32 oracle solve)"
     return None, None
 
 
