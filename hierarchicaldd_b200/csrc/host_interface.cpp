@@ -43,22 +43,8 @@ enum : uint32_t {
 typedef std::array<int, 3> I3;
 typedef std::array<float, 64> M8;
 
-// SPGrid page order (4x8x8 pages of a 16-byte struct, interleaved page bits):
-// the order in which the reference walks hierarchy cells.
-inline uint64_t spread_bits(uint64_t v, uint64_t mask) {
-    uint64_t r = 0;
-    for (uint64_t bit = 1; mask; bit <<= 1) {
-        const uint64_t low = mask & (~mask + 1);
-        if (v & bit) r |= low;
-        mask &= mask - 1;
-    }
-    return r;
-}
-inline uint64_t page_key(const I3& c) {
-    return spread_bits((uint64_t)c[0], 0x9249249249249000ull | 0x300ull) |
-           spread_bits((uint64_t)c[1], 0x4924924924924000ull | 0x0e0ull) |
-           spread_bits((uint64_t)c[2], 0x2492492492492000ull | 0x01cull);
-}
+// SPGrid page order: the order in which the reference walks hierarchy cells.
+inline uint64_t page_key(const I3& c) { return spgrid_address(c[0], c[1], c[2]); }
 
 struct Stride {
     int lo[3];

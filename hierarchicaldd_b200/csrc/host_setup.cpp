@@ -36,6 +36,41 @@ void divide_domain(const int size[3], const int sub[3], uint32_t* f) {
             }
 }
 
+void downsample_topology(const int fd[3], const uint32_t* fine, const int cd[3], uint32_t* coarse) {
+    // The reference visits the fine cells page by page in SPGrid address
+    // order, and within a page x-slowest; coarse cell c = (f+1)/2.  While c is
+    // unset (no Dirichlet, Active or Interface bit), an Active child sets it
+    // Active and a Dirichlet child sets it Dirichlet (an Interface child
+    // without the Dirichlet bit leaves it unset); once set, a Dirichlet or
+    // Interface child makes it Dirichlet.  So an Interface child seen before
+    // the first Active one does not count.
+    std::fill(coarse, coarse + (size_t)cd[0] * cd[1] * cd[2], 0u);
+    const int np[3] = {(fd[0] + 3) / 4, (fd[1] + 7) / 8, (fd[2] + 7) / 8};
+    std::vector<std::pair<uint64_t, int>> pages;
+    pages.reserve((size_t)np[0] * np[1] * np[2]);
+    for (int a = 0; a < np[0]; ++a)
+        for (int b = 0; b < np[1]; ++b)
+            for (int c = 0; c < np[2]; ++c)
+                pages.push_back({spgrid_address(4 * a, 8 * b, 8 * c), (a * np[1] + b) * np[2] + c});
+    std::sort(pages.begin(), pages.end());
+    for (const auto& pg : pages) {
+        const int a = pg.second / (np[1] * np[2]), b = (pg.second / np[2]) % np[1], c = pg.second % np[2];
+        for (int x = 4 * a; x < std::min(4 * a + 4, fd[0]); ++x)
+            for (int y = 8 * b; y < std::min(8 * b + 8, fd[1]); ++y)
+                for (int z = 8 * c; z < std::min(8 * c + 8, fd[2]); ++z) {
+                    const uint32_t v = fine[at3(fd, x, y, z)];
+                    if (!v) continue;
+                    uint32_t& o = coarse[at3(cd, (x + 1) / 2, (y + 1) / 2, (z + 1) / 2)];
+                    if (!(o & (F_DIRICHLET | F_ACTIVE | F_INTERFACE))) {
+                        if (v & F_ACTIVE) o |= F_ACTIVE;
+                        else if (v & (F_DIRICHLET | F_INTERFACE)) o |= (v & F_DIRICHLET);
+                        continue;
+                    }
+                    if (v & (F_DIRICHLET | F_INTERFACE)) o = F_DIRICHLET;
+                }
+    }
+}
+
 void clear_planes(const int size[3], const int sub[3], uint32_t* f) {
     // Domain_Divider with clear_flag (two-level demo,
     // TWO/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Divider_Helper.h:61-72):
@@ -186,10 +221,9 @@ void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& L) {
                 if (s >= 0) L.tile_flags[s] = compact16(L.flags0[at3(n, i, j, k)]);
             }
 
-    // Whole-grid levels (CPU/SPGrid_Domain_Decomposition_Solver/SPGrid_V_Cycle_Topology.h:35-178):
-    // level l+1 has n/2+1 cells per axis; a coarse cell is Dirichlet if a
-    // child (2c-1, 2c) is Dirichlet or Interface, else Active if a child is
-    // Active; then Flaging and Flaging_Boundary.
+    // Whole-grid levels (CPU/SPGrid_Library/SPGrid_V_Cycle_Topology.h:35-178):
+    // level l+1 has n/2+1 cells per axis, downsampled from level l
+    // (downsample_topology), then Flaging and Flaging_Boundary.
     const int V = opt.vlevels;
     L.g_dims.assign(V, {0, 0, 0});
     L.g_flags.assign(V, {});
@@ -200,14 +234,7 @@ void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& L) {
             if (l > 0) {
                 const std::array<int, 3> cd = {fd[0] / 2 + 1, fd[1] / 2 + 1, fd[2] / 2 + 1};
                 coarse.assign((size_t)cd[0] * cd[1] * cd[2], 0u);
-                for (int i = 0; i < fd[0]; ++i)
-                    for (int j = 0; j < fd[1]; ++j)
-                        for (int k = 0; k < fd[2]; ++k) {
-                            const uint32_t v = fine[at3(fd.data(), i, j, k)];
-                            uint32_t& c = coarse[at3(cd.data(), (i + 1) / 2, (j + 1) / 2, (k + 1) / 2)];
-                            if (v & (F_DIRICHLET | F_INTERFACE)) c = F_DIRICHLET;
-                            else if ((v & F_ACTIVE) && c != F_DIRICHLET) c = F_ACTIVE;
-                        }
+                downsample_topology(fd.data(), fine.data(), cd.data(), coarse.data());
                 flag_faces(cd.data(), coarse.data());
                 flag_boundary(cd.data(), coarse.data());
                 fine.swap(coarse);
@@ -255,66 +282,34 @@ void build_layout(const Options& opt, const uint32_t* flags, DomainLayout& L) {
                 L.boxes.push_back(bx);
             }
     L.box_flags.assign(L.boxes.size() * L.box_stride, 0);
-    // Set inside the parallel loop: a box level that is not the whole grid's.
+    // Per-box levels: the whole grid's levels inside each box.  The per-box
+    // V-cycle keeps a coarse box's face cells at zero, which is the whole
+    // grid's V-cycle unless one of them is Active; then the boxes couple and
+    // the whole-grid V-cycle runs (set inside the parallel loop).
     int coupled = 0;
 #pragma omp parallel for schedule(dynamic)
     for (long long bi = 0; bi < (long long)L.boxes.size(); ++bi) {
         const Box& bx = L.boxes[bi];
         uint8_t* rec = L.box_flags.data() + bi * L.box_stride;
-        // Level 0: reference flags of the box [o, o+sub] (cells outside the grid are 0).
-        std::vector<uint32_t> fine, coarse;
-        int fe[3] = {L.level_e[0], L.level_e[1], L.level_e[2]};
-        fine.assign((size_t)fe[0] * fe[1] * fe[2], 0u);
-        for (int x = 0; x < fe[0]; ++x)
-            for (int y = 0; y < fe[1]; ++y)
-                for (int z = 0; z < fe[2]; ++z) {
-                    int gi = bx.k[0] * opt.sub[0] + x, gj = bx.k[1] * opt.sub[1] + y, gk = bx.k[2] * opt.sub[2] + z;
-                    if (in3(n, gi, gj, gk)) fine[at3(fe, x, y, z)] = L.flags0[at3(n, gi, gj, gk)];
-                }
-        for (size_t x = 0; x < fine.size(); ++x) rec[x] = compact8(fine[x]);
-        for (int l = 1; l < V; ++l) {
-            int ce[3] = {L.level_e[3 * l], L.level_e[3 * l + 1], L.level_e[3 * l + 2]};
-            coarse.assign((size_t)ce[0] * ce[1] * ce[2], 0u);
-            // V_Cycle_Topology.h:35-67: Dirichlet if any child is Dirichlet|Interface,
-            // else Active if any child is Active.  Children of c are 2c-1 and 2c.
-            for (int x = 0; x < ce[0]; ++x)
-                for (int y = 0; y < ce[1]; ++y)
-                    for (int z = 0; z < ce[2]; ++z) {
-                        uint32_t out = 0;
-                        for (int ci = 0; ci < 8; ++ci) {
-                            int fx = 2 * x - 1 + (ci >> 2), fy = 2 * y - 1 + ((ci >> 1) & 1), fz = 2 * z - 1 + (ci & 1);
-                            if (!in3(fe, fx, fy, fz)) continue;
-                            uint32_t v = fine[at3(fe, fx, fy, fz)];
-                            if (v & (F_DIRICHLET | F_INTERFACE)) out = F_DIRICHLET;
-                            else if ((v & F_ACTIVE) && out != F_DIRICHLET) out = F_ACTIVE;
-                        }
-                        coarse[at3(ce, x, y, z)] = out;
-                    }
-            flag_faces(ce, coarse.data());
-            flag_boundary(ce, coarse.data());
-            // The box's level must be the whole grid's inside the box (flags,
-            // faces, Boundary band), and its box-face cells, which the
-            // per-box V-cycle keeps at zero, must not be Active there.
+        for (int l = 0; l < V; ++l) {
+            const int ce[3] = {L.level_e[3 * l], L.level_e[3 * l + 1], L.level_e[3 * l + 2]};
             const std::array<int, 3>& gd = L.g_dims[l];
             const std::vector<uint8_t>& gf = L.g_flags[l];
             const int o[3] = {bx.k[0] * (opt.sub[0] >> l), bx.k[1] * (opt.sub[1] >> l), bx.k[2] * (opt.sub[2] >> l)};
+            uint8_t* dst = rec + L.level_off[l];
             for (int x = 0; x < ce[0]; ++x)
                 for (int y = 0; y < ce[1]; ++y)
                     for (int z = 0; z < ce[2]; ++z) {
                         const int gx = o[0] + x, gy = o[1] + y, gz = o[2] + z;
-                        const bool halo = x == 0 || y == 0 || z == 0 || x == ce[0] - 1 || y == ce[1] - 1 || z == ce[2] - 1;
                         const bool inside = gx < gd[0] && gy < gd[1] && gz < gd[2];
                         const uint8_t g = inside ? gf[at3(gd.data(), gx, gy, gz)] : 0;
-                        const bool bad = halo ? (g & C_ACTIVE) != 0 : g != compact8(coarse[at3(ce, x, y, z)]);
-                        if (bad) {
+                        dst[at3(ce, x, y, z)] = g;
+                        const bool halo = x == 0 || y == 0 || z == 0 || x == ce[0] - 1 || y == ce[1] - 1 || z == ce[2] - 1;
+                        if (l > 0 && halo && (g & C_ACTIVE)) {
 #pragma omp atomic write
                             coupled = 1;
                         }
                     }
-            uint8_t* dst = rec + L.level_off[l];
-            for (size_t x = 0; x < coarse.size(); ++x) dst[x] = compact8(coarse[x]);
-            fine.swap(coarse);
-            for (int a = 0; a < 3; ++a) fe[a] = ce[a];
         }
     }
     L.global_vcycle = coupled != 0;

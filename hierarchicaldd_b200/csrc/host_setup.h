@@ -16,6 +16,25 @@
 
 namespace hdd {
 
+// SPGrid_Mask<4,2,3> addresses (4 x 8 x 8-cell pages of a 16-byte struct,
+// page coordinates bit-interleaved above 4 KB, cell (x, y, z) of a page at
+// (x * 8 + y) * 8 + z, SPGrid_Mask.h:25-31): the order in which the
+// reference's block iterators walk cells.
+inline uint64_t spgrid_spread_bits(uint64_t v, uint64_t mask) {
+    uint64_t r = 0;
+    for (uint64_t bit = 1; mask; bit <<= 1) {
+        const uint64_t low = mask & (~mask + 1);
+        if (v & bit) r |= low;
+        mask &= mask - 1;
+    }
+    return r;
+}
+inline uint64_t spgrid_address(int x, int y, int z) {
+    return spgrid_spread_bits((uint64_t)x, 0x9249249249249000ull | 0x300ull) |
+           spgrid_spread_bits((uint64_t)y, 0x4924924924924000ull | 0x0e0ull) |
+           spgrid_spread_bits((uint64_t)z, 0x2492492492492000ull | 0x01cull);
+}
+
 struct Options {
     int size[3];
     int sub[3];
@@ -95,6 +114,11 @@ void pages_to_dense(const int size[3], long long n, const int32_t* origin, const
 void pages_to_dense(const int size[3], long long n, const int32_t* origin, const float* values, float* dense);
 // Gathers the same pages from a dense grid (0 outside the grid).
 void dense_to_pages(const int size[3], long long n, const int32_t* origin, const float* dense, float* values);
+
+// V_Cycle_Topology::Topology_Downsample (CPU/SPGrid_Library/SPGrid_V_Cycle_Topology.h:35-67):
+// coarse flags of size cd from fine flags of size fd (cells visited in SPGrid
+// address order; the result depends on it).
+void downsample_topology(const int fd[3], const uint32_t* fine, const int cd[3], uint32_t* coarse);
 
 // Level-0 flag pipeline pieces (same semantics as the reference passes).
 void divide_domain(const int size[3], const int sub[3], uint32_t* f);

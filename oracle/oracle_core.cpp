@@ -75,16 +75,50 @@ void divide_domain(const Dims& d, uint32_t* f, const int sub[3]) {
             }
 }
 
+// SPGrid_Mask<4,2,3> (PB/Common_Libraries/SPGrid/Core/SPGrid_Mask.h): 4 x 8 x 8-cell
+// pages whose coordinates are bit-interleaved above the 4 KB page, cells of a
+// page x-slowest.  The address of page (a, b, c), as a sort key.
+// Page bit k of x sits at address bit 12 + 3k, of z at 13 + 3k, of y at 14 + 3k.
+static uint64_t page_address(int a, int b, int c) {
+    const uint64_t v[3] = {(uint64_t)a, (uint64_t)b, (uint64_t)c};
+    const int lane[3] = {0, 2, 1};
+    uint64_t key = 0;
+    for (int bit = 0; bit < 17; ++bit)
+        for (int axis = 0; axis < 3; ++axis)
+            if (v[axis] >> bit & 1u) key |= 1ull << (12 + 3 * bit + lane[axis]);
+    return key;
+}
+
 void downsample_topology(const Dims& fd, const uint32_t* ff, const Dims& cd, uint32_t* cf) {
+    // SPGrid_V_Cycle_Topology.h:35-67 (Topology_Downsample): the fine cells are
+    // visited page by page in address order, x-slowest inside a page; coarse
+    // cell (f+1)/2.  An unset coarse cell (no Dirichlet, Active or Interface
+    // bit) becomes Active on an Active child, Dirichlet on a Dirichlet child,
+    // and stays unset on an Interface child; a set one becomes Dirichlet on a
+    // Dirichlet or Interface child.
     std::fill(cf, cf + cd.count(), 0u);
-    for (int i = 0; i < fd.n[0]; ++i)
-        for (int j = 0; j < fd.n[1]; ++j)
-            for (int k = 0; k < fd.n[2]; ++k) {
-                uint32_t fl = ff[fd.at(i, j, k)];
-                uint32_t& c = cf[cd.at((i + 1) / 2, (j + 1) / 2, (k + 1) / 2)];
-                if (fl & (DIRICHLET | INTERFACE)) c = DIRICHLET;
-                else if ((fl & ACTIVE) && c != DIRICHLET) c = ACTIVE;
-            }
+    const int np[3] = {(fd.n[0] + 3) / 4, (fd.n[1] + 7) / 8, (fd.n[2] + 7) / 8};
+    std::vector<std::pair<uint64_t, long long>> pages;
+    for (int a = 0; a < np[0]; ++a)
+        for (int b = 0; b < np[1]; ++b)
+            for (int c = 0; c < np[2]; ++c) pages.push_back({page_address(a, b, c), ((long long)a * np[1] + b) * np[2] + c});
+    std::sort(pages.begin(), pages.end());
+    for (const auto& pg : pages) {
+        const int a = (int)(pg.second / ((long long)np[1] * np[2])), b = (int)(pg.second / np[2] % np[1]),
+                  c = (int)(pg.second % np[2]);
+        for (int i = 4 * a; i < 4 * a + 4 && i < fd.n[0]; ++i)
+            for (int j = 8 * b; j < 8 * b + 8 && j < fd.n[1]; ++j)
+                for (int k = 8 * c; k < 8 * c + 8 && k < fd.n[2]; ++k) {
+                    const uint32_t fl = ff[fd.at(i, j, k)];
+                    uint32_t& o = cf[cd.at((i + 1) / 2, (j + 1) / 2, (k + 1) / 2)];
+                    if (!(o & (DIRICHLET | ACTIVE | INTERFACE))) {
+                        if (fl & ACTIVE) o |= ACTIVE;
+                        else if (fl & (DIRICHLET | INTERFACE)) o |= (fl & DIRICHLET);
+                        continue;
+                    }
+                    if (fl & (DIRICHLET | INTERFACE)) o = DIRICHLET;
+                }
+    }
 }
 
 template <class T>

@@ -82,9 +82,11 @@ void flag_boundary(const Dims& d, uint32_t* f);
 void divide_domain(const Dims& d, uint32_t* f, const int sub[3]);
 void number_of_subdomains(const int size[3], const int sub[3], int out[3]);
 
-// CPU/SPGrid_Domain_Decomposition_Solver/SPGrid_V_Cycle_Topology.h:35-67:
-// coarse cell = Dirichlet if any child (fine (c*2-1 .. c*2)) is
-// Dirichlet|Interface, else Active if any child is Active.
+// CPU/SPGrid_Library/SPGrid_V_Cycle_Topology.h:35-67 (Topology_Downsample):
+// children (fine c*2-1 .. c*2) visited in SPGrid address order; an unset
+// coarse cell takes Active from an Active child and Dirichlet from a
+// Dirichlet one (an Interface child leaves it unset); a set one becomes
+// Dirichlet on a Dirichlet or Interface child.
 void downsample_topology(const Dims& fd, const uint32_t* ff, const Dims& cd, uint32_t* cf);
 
 // ----------------------------------------------------------------------------

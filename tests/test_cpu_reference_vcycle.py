@@ -1,0 +1,84 @@
+"""The oracle pinned to the reference's own code: the reference's CPU V-cycle,
+V-cycle topology, Flaging and Domain_Divider (CPU/SPGrid_Library/SPGrid_V_Cycle_Helper.h,
+SPGrid_V_Cycle_Topology.h, SPGrid_Flag_Helper.h, CPU/SPGrid_Domain_Decomposition_Solver/
+SPGrid_Domain_Divider_Helper.h), compiled from the reference tree by
+oracle/Makefile.ref into oracle/_ref/libref_vcycle.so (driver: oracle/ref_vcycle.cpp),
+give bit for bit the oracle's flags at every V-cycle level and its V-cycle
+result, on sphere domains, a ragged grid and the reference generator's own
+Neumann-bubble domain (whose coarse levels depend on the order in which the
+reference visits the fine cells).  The GPU path is bit-exact against the
+oracle on the same operations (tests/test_gpu_parity.py, test_gpu_bubble.py).
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from hierarchicaldd_b200 import domains
+from hierarchicaldd_b200.domains import ACTIVE, INTERFACE
+from oracle_ffi import Oracle
+
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libref_vcycle.so")
+
+
+@pytest.fixture(scope="module")
+def ref():
+    tree = os.environ.get("HDD_REFERENCE_ROOT")
+    if tree and os.path.isdir(tree):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "-f", "Makefile.ref", "REF=" + tree],
+                       check=True)
+    if not os.path.exists(REF_SO):
+        pytest.skip("oracle/_ref/libref_vcycle.so not built (needs the reference tree, HDD_REFERENCE_ROOT)")
+    L = C.CDLL(REF_SO)
+    ip, up, fp = C.POINTER(C.c_int), C.POINTER(C.c_uint32), C.POINTER(C.c_float)
+    L.refv_vcycle.argtypes = [ip, ip, up, C.c_int, C.c_int, C.c_int, fp, fp, up, fp]
+    return L
+
+
+def ref_vcycle(L, d, sub, levels, interior, boundary, u, b):
+    sizes, n = [], list(d.size)
+    for _ in range(levels):
+        sizes.append(tuple(n))
+        n = [x // 2 + 1 for x in n]
+    lf = np.zeros(sum(int(np.prod(s)) for s in sizes), np.uint32)
+    out = np.zeros(d.size, np.float32)
+    f = np.ascontiguousarray(d.flags, np.uint32)
+    L.refv_vcycle((C.c_int * 3)(*d.size), (C.c_int * 3)(*sub), f.ctypes.data_as(C.POINTER(C.c_uint32)), levels,
+                  interior, boundary, u.ctypes.data_as(C.POINTER(C.c_float)), b.ctypes.data_as(C.POINTER(C.c_float)),
+                  lf.ctypes.data_as(C.POINTER(C.c_uint32)), out.ctypes.data_as(C.POINTER(C.c_float)))
+    levels_out, o = [], 0
+    for s in sizes:
+        c = int(np.prod(s))
+        levels_out.append(lf[o:o + c].reshape(s))
+        o += c
+    return levels_out, out
+
+
+CASES = [("sphere 32^3, sub 8", lambda: domains.small(32, 8, 6, seed=1), (8,) * 3, 3, 3),
+         ("sphere 48^3, sub 16", lambda: domains.small(48, 16, 8, seed=7), (16,) * 3, 3, 1),
+         ("ragged 40x36x44, sub 8", lambda: domains.small((40, 36, 44), 8, 6, seed=4), (8,) * 3, 3, 3),
+         ("generator bubble 35^3, sub 8", lambda: domains.reference_generator((35, 35, 35), (4, 16, 16)), (8,) * 3,
+          3, 3),
+         ("generator bubble 65^3, sub 16", lambda: domains.reference_generator((65, 65, 65), (8, 32, 32)),
+          (16,) * 3, 3, 1)]
+
+
+@pytest.mark.parametrize("name,make,sub,levels,interior", CASES, ids=[c[0] for c in CASES])
+def test_reference_vcycle_equals_oracle(ref, name, make, sub, levels, interior):
+    d = make()
+    o = Oracle(d.size, sub, d.flags, vlevels=levels, nVcycles=1, interior_smoothing=interior, boundary_smoothing=3,
+               sigma_levels=2, sigma_smoothing=3, sigma_mg=1)
+    f0 = o.level_flags(0)
+    rng = np.random.default_rng(3)
+    u = rng.standard_normal(d.size).astype(np.float32)
+    u[(f0 & (ACTIVE | INTERFACE)) == 0] = 0
+    b = rng.standard_normal(d.size).astype(np.float32)
+    b[(f0 & ACTIVE) == 0] = 0
+    lf, ur = ref_vcycle(ref, d, sub, levels, interior, 3, u, b)
+    for l in range(levels):
+        assert np.array_equal(lf[l], o.level_flags(l)), (name, l)
+    uo, _ = o.vcycle(u, np.zeros_like(u), b)
+    assert np.array_equal(ur.view(np.uint32), uo.view(np.uint32)), (name, float(np.max(np.abs(ur - uo))))
