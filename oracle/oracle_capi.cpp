@@ -534,6 +534,16 @@ void hddo_apply_preconditioner(void* hp, const void* rhs, void* result) {
         return 0; })());
 }
 
+// lu (in/out) after Laplace_ri(u) on the level-0 flags (the interface
+// right-hand side step of Apply_Preconditioner).
+void hddo_laplace_ri(void* hp, const void* u, void* lu) {
+    Handle* h = static_cast<Handle*>(hp);
+    DISPATCH(h, ([&] {
+        using T = typename std::remove_reference<decltype(s.lv[0].u[0])>::type;
+        laplace_ri<T>(s.d0, s.lv[0].flags.data(), (const T*)u, (T*)lu);
+        return 0; })());
+}
+
 // y = project(A x) with the CG system's Laplacian.
 void hddo_multiply(void* hp, const void* x, void* y) {
     Handle* h = static_cast<Handle*>(hp);

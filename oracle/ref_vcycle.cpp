@@ -10,6 +10,9 @@
 //   CPU/SPGrid_Library/SPGrid_V_Cycle_Topology.h (V_Cycle_Topology: Initialize, Flaging)
 //   CPU/SPGrid_Library/SPGrid_V_Cycle_Helper.h (V_Cycle_Helper::v_cycle) and the
 //   Residual/Correction/Restriction/Prolongation legacy stencils it calls,
+//   CPU/SPGrid_Domain_Decomposition_Solver/SPGrid_Gemini_Arithmetic_Helpers.h (SPGrid_Laplace,
+//   the operator of CG_SYSTEM::Multiply) and CPU/SPGrid_Library/SPGrid_Laplace_Legacy.h
+//   (Laplace_ri, the interface right-hand side of Apply_Preconditioner),
 // in the order CPU/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Decomposition_Solver.h:121-155
 // runs them (divider, Flaging, topology).  The SPGrid containers come from
 // PB/Common_Libraries/SPGrid.  PhysBAM's logging and debug-reporting functions,
@@ -44,7 +47,9 @@ using namespace SPGrid;
 #define Packed_Offset template Packed_Offset
 #include "SPGrid_V_Cycle_Helper.h"
 #include "SPGrid_V_Cycle_Topology.h"
+#include "SPGrid_Laplace_Legacy.h"
 #include "SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Divider_Helper.h"
+#include "SPGrid_Domain_Decomposition_Solver/SPGrid_Gemini_Arithmetic_Helpers.h"
 #undef Packed_OffsetXdim
 #undef Packed_OffsetYdim
 #undef Packed_OffsetZdim
@@ -144,6 +149,57 @@ int refv_vcycle(const int size[3], const int sub[3], const uint32_t* flags_in, i
                 const std_array<unsigned int, 3> c(i, j, k);
                 const size_t x = ((size_t)i * size[1] + j) * size[2] + k;
                 u_out[x] = set.IsPageActive(c) ? u(c) : 0.0f;
+            }
+    return 0;
+}
+
+// The CG operator and the interface gather on the same domain (built as
+// refv_vcycle does): lu_out = SPGrid_Laplace(u) at Active|Interface cells
+// (CG_SYSTEM.cpp:28-44, before Project; other cells 0), and ri_out =
+// b_in with Laplace_ri(u) applied (Lu -= (T)(-sum of Active neighbours) at
+// Interface cells; other cells keep b).  Returns 0.
+int refv_laplace(const int size[3], const int sub[3], const uint32_t* flags_in, const float* u_in, const float* b_in,
+                 float* lu_out, float* ri_out) {
+    typedef VECTOR<int, 3> T_INDEX;
+    std_array<int, 3> sz(size[0], size[1], size[2]);
+    Alloc allocator(sz);
+    Set set(allocator.Get_Array(&T_STRUCT::flags));
+    for (int i = 0; i < size[0]; ++i)
+        for (int j = 0; j < size[1]; ++j)
+            for (int k = 0; k < size[2]; ++k) {
+                const uint32_t f = flags_in[((size_t)i * size[1] + j) * size[2] + k];
+                if (f) set.Mask(std_array<unsigned int, 3>(i, j, k), f);
+            }
+    set.Refresh_Block_Offsets();
+    SPGrid_Computations::Domain_Divider<T_STRUCT, 3>(allocator, set.Get_Blocks(), &T_STRUCT::flags, set,
+                                                     T_INDEX(size[0], size[1], size[2]), T_INDEX(),
+                                                     T_INDEX(sub[0], sub[1], sub[2]));
+    SPGrid_Computations::Flaging<T_STRUCT, 3>(allocator, set.Get_Blocks(), &T_STRUCT::flags, set);
+    Alloc::Array<float>::type u = allocator.Get_Array(&T_STRUCT::ch0), lu = allocator.Get_Array(&T_STRUCT::ch1),
+                              t = allocator.Get_Array(&T_STRUCT::ch2);
+    for (int i = 0; i < size[0]; ++i)
+        for (int j = 0; j < size[1]; ++j)
+            for (int k = 0; k < size[2]; ++k) {
+                const std_array<unsigned int, 3> c(i, j, k);
+                if (!set.IsPageActive(c)) continue;
+                const size_t x = ((size_t)i * size[1] + j) * size[2] + k;
+                u(c) = u_in[x];
+                lu(c) = 0.0f;
+                t(c) = b_in[x];
+            }
+    SPGrid_Computations::SPGrid_Laplace<T_STRUCT, float, unsigned, 3>(
+        allocator, set.Get_Blocks(), allocator, allocator, &T_STRUCT::ch0, &T_STRUCT::ch1, &T_STRUCT::flags,
+        SPGrid_Solver_Cell_Type_Active | SPGrid_Solver_Cell_Type_Interface);
+    SPGrid_Computations::Laplace_ri<T_STRUCT, float, unsigned, 3>(allocator, set.Get_Blocks(), &T_STRUCT::ch0,
+                                                                  &T_STRUCT::ch2, &T_STRUCT::flags);
+    for (int i = 0; i < size[0]; ++i)
+        for (int j = 0; j < size[1]; ++j)
+            for (int k = 0; k < size[2]; ++k) {
+                const std_array<unsigned int, 3> c(i, j, k);
+                const size_t x = ((size_t)i * size[1] + j) * size[2] + k;
+                const bool on = set.IsPageActive(c);
+                lu_out[x] = on ? lu(c) : 0.0f;
+                ri_out[x] = on ? t(c) : b_in[x];
             }
     return 0;
 }

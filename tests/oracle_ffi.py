@@ -54,6 +54,7 @@ def lib():
         L.hddo_vcycle.argtypes = [vp, vp, vp, vp]
         L.hddo_apply_preconditioner.argtypes = [vp, vp, vp]
         L.hddo_multiply.argtypes = [vp, vp, vp]
+        L.hddo_laplace_ri.argtypes = [vp, vp, vp]
         L.hddo_sigma_vcycle.argtypes = [vp, vp, vp]
         L.hddo_sigma_smooth.argtypes = [vp, C.c_int, vp, vp]
         L.hddo_solve.restype = C.c_int
@@ -177,6 +178,13 @@ class Oracle:
         u = self._vec(u); r = self._vec(r); b = self._vec(b)
         lib().hddo_vcycle(self.h, u.ctypes.data, r.ctypes.data, b.ctypes.data)
         return u, r
+
+    def laplace_ri(self, u, lu):
+        """lu after Laplace_ri(u) (the interface right-hand side step)."""
+        u = self._vec(u)
+        lu = self._vec(lu)
+        lib().hddo_laplace_ri(self.h, u.ctypes.data, lu.ctypes.data)
+        return lu
 
     def apply_preconditioner(self, rhs):
         rhs = self._vec(rhs)

@@ -1,5 +1,6 @@
 """The oracle pinned to the reference's own code: the reference's CPU V-cycle,
-V-cycle topology, Flaging and Domain_Divider (CPU/SPGrid_Library/SPGrid_V_Cycle_Helper.h,
+V-cycle topology, Flaging, Domain_Divider, CG Laplacian (SPGrid_Laplace) and
+interface gather (Laplace_ri) (CPU/SPGrid_Library/SPGrid_V_Cycle_Helper.h,
 SPGrid_V_Cycle_Topology.h, SPGrid_Flag_Helper.h, CPU/SPGrid_Domain_Decomposition_Solver/
 SPGrid_Domain_Divider_Helper.h), compiled from the reference tree by
 oracle/Makefile.ref into oracle/_ref/libref_vcycle.so (driver: oracle/ref_vcycle.cpp),
@@ -35,7 +36,18 @@ def ref():
     L = C.CDLL(REF_SO)
     ip, up, fp = C.POINTER(C.c_int), C.POINTER(C.c_uint32), C.POINTER(C.c_float)
     L.refv_vcycle.argtypes = [ip, ip, up, C.c_int, C.c_int, C.c_int, fp, fp, up, fp]
+    L.refv_laplace.argtypes = [ip, ip, up, fp, fp, fp, fp]
     return L
+
+
+def ref_laplace(L, d, sub, u, b):
+    lu = np.zeros(d.size, np.float32)
+    ri = np.zeros(d.size, np.float32)
+    f = np.ascontiguousarray(d.flags, np.uint32)
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+    L.refv_laplace((C.c_int * 3)(*d.size), (C.c_int * 3)(*sub), f.ctypes.data_as(C.POINTER(C.c_uint32)), fp(u),
+                   fp(b), fp(lu), fp(ri))
+    return lu, ri
 
 
 def ref_vcycle(L, d, sub, levels, interior, boundary, u, b):
@@ -82,3 +94,19 @@ def test_reference_vcycle_equals_oracle(ref, name, make, sub, levels, interior):
         assert np.array_equal(lf[l], o.level_flags(l)), (name, l)
     uo, _ = o.vcycle(u, np.zeros_like(u), b)
     assert np.array_equal(ur.view(np.uint32), uo.view(np.uint32)), (name, float(np.max(np.abs(ur - uo))))
+
+
+@pytest.mark.parametrize("name,make,sub,levels,interior", CASES, ids=[c[0] for c in CASES])
+def test_reference_laplacian_and_interface_gather_equal_oracle(ref, name, make, sub, levels, interior):
+    """CG_SYSTEM::Multiply's SPGrid_Laplace and Apply_Preconditioner's Laplace_ri."""
+    d = make()
+    o = Oracle(d.size, sub, d.flags, vlevels=levels, nVcycles=1, interior_smoothing=interior, boundary_smoothing=3,
+               sigma_levels=2, sigma_smoothing=3, sigma_mg=1)
+    f0 = o.level_flags(0)
+    rng = np.random.default_rng(8)
+    u = rng.standard_normal(d.size).astype(np.float32)
+    u[(f0 & (ACTIVE | INTERFACE)) == 0] = 0
+    b = rng.standard_normal(d.size).astype(np.float32)
+    lu_ref, ri_ref = ref_laplace(ref, d, sub, u, b)
+    assert np.array_equal(o.multiply(u).view(np.uint32), lu_ref.view(np.uint32)), name
+    assert np.array_equal(o.laplace_ri(u, b).view(np.uint32), ri_ref.view(np.uint32)), name
