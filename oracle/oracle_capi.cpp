@@ -544,6 +544,18 @@ void hddo_laplace_ri(void* hp, const void* u, void* lu) {
         return 0; })());
 }
 
+// lu (in/out) after Laplace_ri_Subdomain (which 0) or Laplace_ir_Subdomain
+// (which 1) of u at the solver's sub_size, on the level-0 flags (two-level
+// DD's couplings).
+void hddo_laplace_subdomain(void* hp, int which, const void* u, void* lu) {
+    Handle* h = static_cast<Handle*>(hp);
+    DISPATCH(h, ([&] {
+        using T = typename std::remove_reference<decltype(s.lv[0].u[0])>::type;
+        if (which == 0) laplace_ri_subdomain<T>(s.d0, s.lv[0].flags.data(), (const T*)u, (T*)lu, s.sub);
+        else laplace_ir_subdomain<T>(s.d0, s.lv[0].flags.data(), (const T*)u, (T*)lu, s.sub);
+        return 0; })());
+}
+
 // y = project(A x) with the CG system's Laplacian.
 void hddo_multiply(void* hp, const void* x, void* y) {
     Handle* h = static_cast<Handle*>(hp);

@@ -55,6 +55,7 @@ def lib():
         L.hddo_apply_preconditioner.argtypes = [vp, vp, vp]
         L.hddo_multiply.argtypes = [vp, vp, vp]
         L.hddo_laplace_ri.argtypes = [vp, vp, vp]
+        L.hddo_laplace_subdomain.argtypes = [vp, C.c_int, vp, vp]
         L.hddo_sigma_vcycle.argtypes = [vp, vp, vp]
         L.hddo_sigma_smooth.argtypes = [vp, C.c_int, vp, vp]
         L.hddo_solve.restype = C.c_int
@@ -184,6 +185,13 @@ class Oracle:
         u = self._vec(u)
         lu = self._vec(lu)
         lib().hddo_laplace_ri(self.h, u.ctypes.data, lu.ctypes.data)
+        return lu
+
+    def laplace_subdomain(self, which, u, lu):
+        """lu after Laplace_ri_Subdomain ("ri") or Laplace_ir_Subdomain ("ir") of u."""
+        u = self._vec(u)
+        lu = self._vec(lu)
+        lib().hddo_laplace_subdomain(self.h, {"ri": 0, "ir": 1}[which], u.ctypes.data, lu.ctypes.data)
         return lu
 
     def apply_preconditioner(self, rhs):

@@ -1,6 +1,7 @@
 """The oracle pinned to the reference's own code: the reference's CPU V-cycle,
-V-cycle topology, Flaging, Domain_Divider, CG Laplacian (SPGrid_Laplace) and
-interface gather (Laplace_ri) (CPU/SPGrid_Library/SPGrid_V_Cycle_Helper.h,
+V-cycle topology, Flaging, Domain_Divider, CG Laplacian (SPGrid_Laplace),
+interface gather (Laplace_ri) and the two-level demo's subdomain couplings
+(Laplace_ri_Subdomain, Laplace_ir_Subdomain, oracle/_ref/libref_two_level.so) (CPU/SPGrid_Library/SPGrid_V_Cycle_Helper.h,
 SPGrid_V_Cycle_Topology.h, SPGrid_Flag_Helper.h, CPU/SPGrid_Domain_Decomposition_Solver/
 SPGrid_Domain_Divider_Helper.h), compiled from the reference tree by
 oracle/Makefile.ref into oracle/_ref/libref_vcycle.so (driver: oracle/ref_vcycle.cpp),
@@ -23,6 +24,7 @@ from hierarchicaldd_b200.domains import ACTIVE, INTERFACE
 from oracle_ffi import Oracle
 
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libref_vcycle.so")
+REF2_SO = os.path.join(ROOT, "oracle", "_ref", "libref_two_level.so")
 
 
 @pytest.fixture(scope="module")
@@ -110,3 +112,31 @@ def test_reference_laplacian_and_interface_gather_equal_oracle(ref, name, make, 
     lu_ref, ri_ref = ref_laplace(ref, d, sub, u, b)
     assert np.array_equal(o.multiply(u).view(np.uint32), lu_ref.view(np.uint32)), name
     assert np.array_equal(o.laplace_ri(u, b).view(np.uint32), ri_ref.view(np.uint32)), name
+
+
+@pytest.mark.parametrize("n,sub,radius,kind", [(32, 16, 6, "sphere"), ((40, 36, 44), 16, 6, "sphere"),
+                                               (64, 16, 0, "bubble")])
+def test_reference_two_level_couplings_equal_oracle(ref, n, sub, radius, kind):
+    """The two-level demo's Laplace_ri_Subdomain and Laplace_ir_Subdomain
+    (TWO/SPGrid_Library/SPGrid_Laplace_Legacy.h:120-178, 232-290)."""
+    if not os.path.exists(REF2_SO):
+        pytest.skip("oracle/_ref/libref_two_level.so not built")
+    L = C.CDLL(REF2_SO)
+    d = (domains.small(n, sub, radius, seed=2) if kind == "sphere"
+         else domains.reference_generator((n + 1,) * 3, (8, n // 2, n // 2)))
+    s3 = (sub,) * 3
+    o = Oracle(d.size, s3, d.flags, vlevels=3, nVcycles=1, interior_smoothing=1, boundary_smoothing=3,
+               sigma_levels=2, sigma_smoothing=3, sigma_mg=1, multilevel=True)
+    rng = np.random.default_rng(9)
+    f0 = o.level_flags(0)
+    u = rng.standard_normal(d.size).astype(np.float32)
+    u[(f0 & (ACTIVE | INTERFACE)) == 0] = 0
+    b = rng.standard_normal(d.size).astype(np.float32)
+    ri = np.zeros(d.size, np.float32)
+    ir = np.zeros(d.size, np.float32)
+    f = np.ascontiguousarray(d.flags, np.uint32)
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+    L.reft_subdomain_couplings((C.c_int * 3)(*d.size), (C.c_int * 3)(*s3), f.ctypes.data_as(C.POINTER(C.c_uint32)),
+                               fp(u), fp(b), fp(ri), fp(ir))
+    assert np.array_equal(o.laplace_subdomain("ri", u, b).view(np.uint32), ri.view(np.uint32))
+    assert np.array_equal(o.laplace_subdomain("ir", u, np.zeros_like(u)).view(np.uint32), ir.view(np.uint32))
