@@ -35,7 +35,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -670,6 +673,13 @@ int occupancy_nt(int k, size_t smf, size_t smb) {
 void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::vector<int>& offsets, cudaStream_t s,
                       int* shared_err) {
     release();
+    const bool verbose = std::getenv("HDD_VERBOSE") != nullptr;
+    const auto t_start = std::chrono::steady_clock::now();
+    auto stamp = [&](const char* what) {
+        if (verbose)
+            std::fprintf(stderr, "[hdd setup]   plan (%zu factors): %s at %.3f s\n", factors.size(), what,
+                         std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count());
+    };
     std::vector<int> col0, ncol, nrow, rows, child_ptr{0}, child, relmap, perm, height, depth, parent_g;
     std::vector<long long> rows_off, relmap_off, upd_off, fw_off;
     n = 0;
@@ -800,41 +810,112 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
     n_fwd = (int)ftasks.size();
     n_bwd = (int)btasks.size();
     n_ctr = 2 + 2 * nsn + nchunk;
-    std::vector<float> fw((size_t)std::max<long long>(fw_total, 4), 0.0f);
+    stamp("fronts and tasks");
+    // Coefficient blocks (FP64 -> FP32, padding rows zero), packed front by
+    // front into two pinned staging buffers in turn, each copied to the device
+    // while the next is packed: the gigabytes of a level-0 plan then cross at
+    // pinned-copy speed and the packing overlaps the copy.
+    size_t bytes_fw = 0;
+    {
+        const long long total = std::max<long long>(fw_total, 4);
+        d_fw = nullptr;
+        if (cudaMalloc(&d_fw, (size_t)total * sizeof(float)) != cudaSuccess)
+            throw Error(HDD_ERR_OUT_OF_MEMORY, "cudaMalloc: supernodal coefficients");
+        long long biggest = 4;
+        for (int g = 0; g < nsn; ++g) biggest = std::max(biggest, (long long)((ncol[g] + nrow[g] + 3) & ~3) * ncol[g]);
+        // Floats per staging buffer: 32 MB (pinning costs about as much as the
+        // copy, so the buffers stay small), or the largest front.
+        const long long chunk = std::max<long long>(biggest, 8ll << 20);
+        float* stage[2] = {nullptr, nullptr};
+        cudaEvent_t copied[2] = {nullptr, nullptr};
+        auto cleanup = [&]() {
+            for (int i = 0; i < 2; ++i) {
+                if (copied[i]) { cudaEventSynchronize(copied[i]); cudaEventDestroy(copied[i]); }
+                if (stage[i]) cudaFreeHost(stage[i]);
+            }
+        };
+        try {
+            for (int i = 0; i < 2; ++i) {
+                dev::ck(cudaMallocHost(&stage[i], (size_t)std::min(chunk, total) * sizeof(float)), "pinned staging");
+                dev::ck(cudaEventCreateWithFlags(&copied[i], cudaEventDisableTiming), "event");
+            }
+            int g0 = 0, buf = 0;
+            bool used[2] = {false, false};
+            while (g0 < nsn) {
+                // Fronts g0 .. g1-1 fill this chunk (at least one front).
+                int g1 = g0 + 1;
+                while (g1 < nsn && fw_off[g1] + (long long)((ncol[g1] + nrow[g1] + 3) & ~3) * ncol[g1] -
+                                           fw_off[g0] <= chunk)
+                    ++g1;
+                const long long base = fw_off[g0];
+                const long long end = g1 < nsn ? fw_off[g1] : fw_total;
+                if (used[buf]) dev::ck(cudaEventSynchronize(copied[buf]), "staging reuse");
+                float* st = stage[buf];
 #pragma omp parallel for schedule(dynamic)
-    for (int g = 0; g < nsn; ++g) {
-        const SnFactor& F = *factors[where[g].first];
-        const BlockVec& W = F.Fw[where[g].second];  // m x nj, col-major
-        const int nj = ncol[g], m = nj + nrow[g], ld = (m + 3) & ~3;
-        float* dst = &fw[(size_t)fw_off[g]];
-        for (int c = 0; c < nj; ++c)
-            for (int r = 0; r < m; ++r) dst[(size_t)c * ld + r] = (float)W[(size_t)c * m + r];
+                for (int g = g0; g < g1; ++g) {
+                    const SnFactor& F = *factors[where[g].first];
+                    const BlockVec& W = F.Fw[where[g].second];  // m x nj, col-major
+                    const int nj = ncol[g], m = nj + nrow[g], ld = (m + 3) & ~3;
+                    float* dst = st + (fw_off[g] - base);
+                    for (int c = 0; c < nj; ++c) {
+                        for (int r = 0; r < m; ++r) dst[(size_t)c * ld + r] = (float)W[(size_t)c * m + r];
+                        for (int r = m; r < ld; ++r) dst[(size_t)c * ld + r] = 0.0f;
+                    }
+                }
+                if (end > base)
+                    dev::ck(cudaMemcpyAsync(d_fw + base, st, (size_t)(end - base) * sizeof(float),
+                                            cudaMemcpyHostToDevice, s), "coefficient upload");
+                dev::ck(cudaEventRecord(copied[buf], s), "event");
+                used[buf] = true;
+                buf ^= 1;
+                g0 = g1;
+            }
+            if (fw_total < total)  // an empty plan's placeholder
+                dev::ck(cudaMemsetAsync(d_fw + fw_total, 0, (size_t)(total - fw_total) * sizeof(float), s), "memset");
+        } catch (...) {
+            cleanup();
+            throw;
+        }
+        cleanup();
+        bytes_fw = (size_t)total * sizeof(float);
     }
+    stamp("coefficients packed and uploaded");
     // Children lists and relative maps (child row -> position in parent's front).
     relmap_off.assign(nsn, 0);
     for (int g = 0; g < nsn; ++g) {
         for (int c : kids[g]) child.push_back(c);
         child_ptr.push_back((int)child.size());
     }
-    for (int g = 0; g < nsn; ++g) {
-        relmap_off[g] = (long long)relmap.size();
-        const int p = parent_g[g];
-        if (p < 0) continue;
-        const int pc0 = col0[p], pnj = ncol[p];
-        const int* prow = rows.data() + rows_off[p];
-        const int pnr = nrow[p];
-        const int* crow = rows.data() + rows_off[g];
-        for (int kq = 0; kq < nrow[g]; ++kq) {
-            const int r = crow[kq];
-            int posn;
-            if (r >= pc0 && r < pc0 + pnj) posn = r - pc0;
-            else {
-                const int* it = std::lower_bound(prow, prow + pnr, r);
-                if (it == prow + pnr || *it != r) throw Error(HDD_ERR_INTERNAL, "supernode row not in parent front");
-                posn = pnj + (int)(it - prow);
-            }
-            relmap.push_back(posn);
+    {
+        long long total = 0;
+        for (int g = 0; g < nsn; ++g) {
+            relmap_off[g] = total;
+            if (parent_g[g] >= 0) total += nrow[g];
         }
+        relmap.resize((size_t)total);
+        int bad = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(| : bad)
+        for (int g = 0; g < nsn; ++g) {
+            const int p = parent_g[g];
+            if (p < 0) continue;
+            const int pc0 = col0[p], pnj = ncol[p];
+            const int* prow = rows.data() + rows_off[p];
+            const int pnr = nrow[p];
+            const int* crow = rows.data() + rows_off[g];
+            int* out = relmap.data() + relmap_off[g];
+            for (int kq = 0; kq < nrow[g]; ++kq) {
+                const int r = crow[kq];
+                int posn = 0;
+                if (r >= pc0 && r < pc0 + pnj) posn = r - pc0;
+                else {
+                    const int* it = std::lower_bound(prow, prow + pnr, r);
+                    if (it == prow + pnr || *it != r) bad = 1;
+                    else posn = pnj + (int)(it - prow);
+                }
+                out[kq] = posn;
+            }
+        }
+        if (bad) throw Error(HDD_ERR_INTERNAL, "supernode row not in parent front");
     }
     // Gather lists (the relative maps inverted per parent position, children
     // in their order).
@@ -842,33 +923,40 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
     std::vector<long long> gp_off(nsn, 0), ge_off(nsn, 0);
     std::vector<int> gptr, gent;
     {
-        std::vector<int> cnt;
+        long long np = 0, ne = 0;
+        for (int g = 0; g < nsn; ++g) {
+            gp_off[g] = np;
+            ge_off[g] = ne;
+            np += ncol[g] + nrow[g] + 1;
+            for (int c = child_ptr[g]; c < child_ptr[g + 1]; ++c) ne += nrow[child[c]];
+        }
+        gptr.resize((size_t)np);
+        gent.resize((size_t)ne);
+#pragma omp parallel for schedule(dynamic, 64)
         for (int g = 0; g < nsn; ++g) {
             const int m = ncol[g] + nrow[g];
-            gp_off[g] = (long long)gptr.size();
-            ge_off[g] = (long long)gent.size();
-            cnt.assign(m + 1, 0);
+            int* cnt = gptr.data() + gp_off[g];  // m + 1 entries
+            std::fill(cnt, cnt + m + 1, 0);
             for (int c = child_ptr[g]; c < child_ptr[g + 1]; ++c) {
                 const int C = child[c];
                 for (int k = 0; k < nrow[C]; ++k) ++cnt[relmap[relmap_off[C] + k] + 1];
             }
             for (int q = 0; q < m; ++q) cnt[q + 1] += cnt[q];
-            const size_t base = gent.size();
-            gent.resize(base + (size_t)cnt[m]);
-            gptr.insert(gptr.end(), cnt.begin(), cnt.end());
-            std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+            std::vector<int> fill(cnt, cnt + m);
+            int* ent = gent.data() + ge_off[g];
             for (int c = child_ptr[g]; c < child_ptr[g + 1]; ++c) {
                 const int C = child[c];
                 for (int k = 0; k < nrow[C]; ++k) {
                     const int q = relmap[relmap_off[C] + k];
-                    gent[base + fill[q]++] = (int)(upd_off[C] + k);
+                    ent[fill[q]++] = (int)(upd_off[C] + k);
                 }
             }
         }
     }
+    stamp("relative maps and gather lists");
     if (forward_smem(max_front, 1, nt) > 200 * 1024)
         throw Error(HDD_ERR_UNSUPPORTED, "supernodal front too large for shared memory: " + std::to_string(max_front));
-    bytes = 0;
+    bytes = bytes_fw;
     d_col0 = dev::upload(col0, s, bytes);
     d_ncol = dev::upload(ncol, s, bytes);
     d_nrow = dev::upload(nrow, s, bytes);
@@ -892,7 +980,7 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
     d_bwd = dev::upload(btasks, s, bytes);
     d_bfwd = dev::upload(bfwd.empty() ? std::vector<int>{0} : bfwd, s, bytes);
     d_bbwd = dev::upload(bbwd.empty() ? std::vector<int>{0} : bbwd, s, bytes);
-    d_fw = dev::upload(fw, s, bytes);
+    stamp("uploads issued");
     part_len = std::max<long long>(part_total, 1);
     upd_len = std::max<long long>(upd_total, 1);
     {
@@ -902,6 +990,7 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
         d_err = sc.err;
         own_err = sc.own_err;
     }
+    stamp("scratch allocated");
     // A front with a parent, for stall_dependency (the wait of its parent's
     // forward tasks on it can be made unsatisfiable).
     stall_front = -1;
@@ -927,7 +1016,9 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
         kmax = k;
     }
     grid = grids[0];
+    stamp("grids sized");
     dev::ck(cudaStreamSynchronize(s), "plan upload");
+    stamp("uploaded");
 }
 
 void SolvePlan::release() {
