@@ -513,8 +513,9 @@ template <int K, int NT>
 __global__ void __launch_bounds__(NT, min_blocks(K, NT))
     sn_backward_kernel(PlanView P, const SnTask* __restrict__ tasks, int ntasks, float* __restrict__ x_old) {
     extern __shared__ double g[];  // [y_J; x_R] x K, m4 x K entries (zero padding rows)
-    __shared__ int s_ticket;
+    __shared__ int s_ticket, s_last;
     int* done = P.ctr + 2 + P.nsn;
+    int* chunk_ctr = P.ctr + 2 + 2 * P.nsn;
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     for (;;) {
         if (tid == 0) s_ticket = atomicAdd(P.ctr + 1, 1);
@@ -530,7 +531,11 @@ __global__ void __launch_bounds__(NT, min_blocks(K, NT))
         const int J = T.front, nj = P.ncol[J], m = nj + P.nrow[J], c0 = P.col0[J];
         const int m4 = (m + 3) & ~3;
         const int a0 = T.r0, na = T.rows;
-        const int rs = a0;  // a multiple of kBC: the first row any column of the block needs
+        // This task's rows [rlo, rhi): all rows from a0 (the first any of its
+        // columns needs, a multiple of 4), or one chunk of them when a tall
+        // column block is split (chunks start at multiples of 4; partial sums
+        // of the chunks are added in chunk order by the last one to finish).
+        const int rlo = T.c0, rhi = T.c0 + T.ncols;
         const int* rows = P.rows + P.rows_off[J];
         const size_t ld = (size_t)m4;
         const float* A = P.fw + P.fw_off[J];
@@ -543,14 +548,16 @@ __global__ void __launch_bounds__(NT, min_blocks(K, NT))
         // Row quads wholly below nj (the L_JJ^{-T} y part) need only this
         // front's forward result, so they are summed before waiting on the
         // parent; each lane adds its quads in ascending order.
-        for (int i = rs + tid; i < nj; i += NT)  // from the forward launch
+        const int yhi = min(rhi, nj);
+        for (int i = rlo + tid; i < yhi; i += NT)  // from the forward launch
 #pragma unroll
             for (int j = 0; j < K; ++j) g[(size_t)i * K + j] = P.ynew[j * P.ld_n + c0 + i];
-        for (int i = m + tid; i < m4; i += NT)  // padding rows
+        if (rhi == m)
+            for (int i = m + tid; i < m4; i += NT)  // padding rows
 #pragma unroll
-            for (int j = 0; j < K; ++j) g[(size_t)i * K + j] = 0.0;
+                for (int j = 0; j < K; ++j) g[(size_t)i * K + j] = 0.0;
         __syncthreads();
-        int r = rs + 4 * lane;
+        int r = rlo + 4 * lane;
         auto quad = [&](int rr) {
             double gg[K][4];
 #pragma unroll
@@ -574,22 +581,27 @@ __global__ void __launch_bounds__(NT, min_blocks(K, NT))
         };
         if (amin < a0 + na) {
 #pragma unroll 2
-            for (; r + 4 <= nj; r += 128) quad(r);
+            for (; r + 4 <= yhi; r += 128) quad(r);
         }
-        if (tid == 0) {
-            const int p = P.parent[J];
-            if (p >= 0 && !wait_at_least(done + p, P.ntb[p], P.err, P.spin_limit)) atomicExch(P.err, 1);
-        }
-        __syncthreads();
-        for (int i = max(rs, nj) + tid; i < m; i += NT) {
-            const int tr = rows[i - nj];
+        if (rhi > nj) {
+            // The update rows need the parent's solution.
+            if (tid == 0) {
+                const int p = P.parent[J];
+                if (p >= 0 && !wait_at_least(done + p, P.ntb[p], P.err, P.spin_limit)) atomicExch(P.err, 1);
+            }
+            __syncthreads();
+            for (int i = max(rlo, nj) + tid; i < rhi; i += NT) {
+                const int tr = rows[i - nj];
 #pragma unroll
-            for (int j = 0; j < K; ++j) g[(size_t)i * K + j] = __ldcg(P.xnew + j * P.ld_n + tr);
+                for (int j = 0; j < K; ++j) g[(size_t)i * K + j] = __ldcg(P.xnew + j * P.ld_n + tr);
+            }
+            __syncthreads();
         }
-        __syncthreads();
+        // The rest: the update rows, and the quad that straddles nj (its rows
+        // past m are the zero padding).
         if (amin < a0 + na) {
 #pragma unroll 2
-            for (; r < m; r += 128) quad(r);
+            for (; r < rhi; r += 128) quad(r);
         }
 #pragma unroll
         for (int j = 0; j < K; ++j)
@@ -597,17 +609,44 @@ __global__ void __launch_bounds__(NT, min_blocks(K, NT))
             for (int jj = 0; jj < 4; ++jj)
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) s4[j][jj] += __shfl_xor_sync(0xffffffffu, s4[j][jj], o);
-        if (lane == 0) {
+        auto write_x = [&](int a, int j, double v) {
+            P.xnew[j * P.ld_n + c0 + a] = v;
+            x_old[j * P.ld_x + P.perm[c0 + a]] = (float)v;
+        };
+        if (T.nk == 1) {
+            if (lane == 0) {
 #pragma unroll
-            for (int jj = 0; jj < 4; ++jj) {
-                const int a = amin + warps_of(NT) * jj;
-                if (a < a0 + na) {
-                    const int po = P.perm[c0 + a];
+                for (int jj = 0; jj < 4; ++jj) {
+                    const int a = amin + warps_of(NT) * jj;
+                    if (a < a0 + na)
 #pragma unroll
-                    for (int j = 0; j < K; ++j) {
-                        P.xnew[j * P.ld_n + c0 + a] = s4[j][jj];
-                        x_old[j * P.ld_x + po] = (float)s4[j][jj];
-                    }
+                        for (int j = 0; j < K; ++j) write_x(a, j, s4[j][jj]);
+                }
+            }
+        } else {
+            // Partial sums of this chunk: column (a - a0) of chunk k.
+            if (lane == 0) {
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj) {
+                    const int a = amin + warps_of(NT) * jj;
+                    if (a < a0 + na)
+#pragma unroll
+                        for (int j = 0; j < K; ++j)
+                            P.part[j * P.ld_part + T.part + (size_t)T.k * bc_of(NT) + (a - a0)] = s4[j][jj];
+                }
+            }
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) s_last = (atomicAdd(chunk_ctr + T.chunk, 1) == T.nk - 1);
+            __syncthreads();
+            if (s_last) {
+                __threadfence();
+                for (int q = tid; q < na * K; q += NT) {
+                    const int c = q / K, j = q - c * K;
+                    const double* pj = P.part + j * P.ld_part + T.part + c;
+                    double v = 0.0;
+                    for (int k = 0; k < T.nk; ++k) v += __ldcg(pj + (size_t)k * bc_of(NT));
+                    write_x(a0 + c, j, v);
                 }
             }
         }
@@ -708,6 +747,9 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
     if (nsn == 0) return;
     nt = factors.size() >= 2 ? kNTInterior : kNTInterface;
     const int kWarps = warps_of(nt), kBC = bc_of(nt);
+    // Rows per backward task: about 16K coefficients per task, as a forward
+    // task's 128 x 128 block (512 rows of 32 columns, 2048 of 8).
+    const int kBRows = 16384 / kBC;
     height.assign(nsn, 0);
     depth.assign(nsn, 0);
     for (int g = 0; g < nsn; ++g)
@@ -792,12 +834,24 @@ void SolvePlan::build(const std::vector<const SnFactor*>& factors, const std::ve
             if ((int)bbwd.size() - bfirst == kWarps) flush(btasks, bbwd, bfirst);
             continue;
         }
+        // Column blocks of kBC columns over rows a0 .. m-1; a tall block is
+        // split into row chunks of kBRows (c0, ncols: the chunk's rows) whose
+        // partial sums the last chunk adds, so that the wide update part of a
+        // tall front is read by several CTAs at once.
         for (int a0 = 0; a0 < nj; a0 += kBC) {
-            SnTask t;
-            t.front = g; t.r0 = a0; t.rows = std::min(kBC, nj - a0); t.c0 = 0; t.ncols = 0;
-            t.k = 0; t.nk = 1; t.chunk = -1; t.part = 0;
-            btasks.push_back(t);
-            ++ntb[g];
+            const int span = m - a0;
+            const int nk = std::max(1, (span + kBRows - 1) / kBRows);
+            const int chunk = nk > 1 ? nchunk++ : -1;
+            const long long part = nk > 1 ? part_total : 0;
+            if (nk > 1) part_total += (long long)nk * kBC;
+            for (int k = 0; k < nk; ++k) {
+                SnTask t;
+                t.front = g; t.r0 = a0; t.rows = std::min(kBC, nj - a0);
+                t.c0 = a0 + k * kBRows; t.ncols = std::min(kBRows, m - t.c0);
+                t.k = k; t.nk = nk; t.chunk = chunk; t.part = part;
+                btasks.push_back(t);
+                ++ntb[g];
+            }
         }
     }
     flush(btasks, bbwd, bfirst);
