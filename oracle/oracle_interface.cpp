@@ -476,7 +476,9 @@ struct Stride1D {
 typedef std::array<Stride1D, 3> Stride3;
 
 // CPU/Interface_Solver/STRIDE_GENERATOR.h:23-54.
-static int generate_adaptive_stride(const I3& lo, const I3& hi, Stride3& q) {
+// filled (optional): per axis, how many entries the fill wrote (counts + 1
+// when the adaptation sequence tiles the range exactly).
+static int generate_adaptive_stride(const I3& lo, const I3& hi, Stride3& q, int* filled = nullptr) {
     int level = INT_MAX;
     for (int a = 0; a < 3; ++a) {
         int counts = hi[a] - lo[a], axis_level = 0;
@@ -509,11 +511,29 @@ static int generate_adaptive_stride(const I3& lo, const I3& hi, Stride3& q) {
             st.pop_back();
             for (int i = 0; i < cs; ++i) put(cs);
         }
+        if (filled) filled[a] = cnt - 1;
         q[a].q.resize(counts + 1);
         for (int v : q[a].q)
             if (v <= 0) throw std::runtime_error("oracle: stride array not filled");
         level = std::min(level, axis_level);
     }
+    return level;
+}
+
+// The strides of the box [lo, hi] per axis, axis 0 first (hi - lo + 1
+// entries each), into q_out; filled[3] as above.  Returns the adaptation
+// level, or -1 if an axis was not filled.
+extern "C" int hddo_adaptive_stride(const int lo[3], const int hi[3], int* q_out, int filled[3]) {
+    Stride3 q;
+    int level;
+    try {
+        level = generate_adaptive_stride(I3{lo[0], lo[1], lo[2]}, I3{hi[0], hi[1], hi[2]}, q, filled);
+    } catch (const std::exception&) {
+        return -1;
+    }
+    size_t o = 0;
+    for (int a = 0; a < 3; ++a)
+        for (int v : q[a].q) q_out[o++] = v;
     return level;
 }
 

@@ -13,6 +13,8 @@
 //   CPU/SPGrid_Domain_Decomposition_Solver/SPGrid_Gemini_Arithmetic_Helpers.h (SPGrid_Laplace,
 //   the operator of CG_SYSTEM::Multiply) and CPU/SPGrid_Library/SPGrid_Laplace_Legacy.h
 //   (Laplace_ri, the interface right-hand side of Apply_Preconditioner),
+//   CPU/Interface_Solver/STRIDE_GENERATOR.h (Generate_Adaptive_Stride, the graded
+//   node spacing of the interface hierarchy),
 // in the order CPU/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Decomposition_Solver.h:121-155
 // runs them (divider, Flaging, topology).  The SPGrid containers come from
 // PB/Common_Libraries/SPGrid.  PhysBAM's logging and debug-reporting functions,
@@ -50,6 +52,7 @@ using namespace SPGrid;
 #include "SPGrid_Laplace_Legacy.h"
 #include "SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Divider_Helper.h"
 #include "SPGrid_Domain_Decomposition_Solver/SPGrid_Gemini_Arithmetic_Helpers.h"
+#include "Interface_Solver/STRIDE_GENERATOR.h"
 #undef Packed_OffsetXdim
 #undef Packed_OffsetYdim
 #undef Packed_OffsetZdim
@@ -202,6 +205,20 @@ int refv_laplace(const int size[3], const int sub[3], const uint32_t* flags_in, 
                 ri_out[x] = on ? t(c) : b_in[x];
             }
     return 0;
+}
+
+// STRIDE_GENERATOR<3>::Generate_Adaptive_Stride over the box [lo, hi]: the
+// stride of every index per axis, axis 0 first (hi - lo + 1 entries each),
+// into q_out.  Returns the adaptation level.
+int refv_adaptive_stride(const int lo[3], const int hi[3], int* q_out) {
+    typedef VECTOR<int, 3> T_INDEX;
+    RANGE<T_INDEX> range(T_INDEX(lo[0], lo[1], lo[2]), T_INDEX(hi[0], hi[1], hi[2]));
+    VECTOR<ARRAY<int, VECTOR<int, 1> >, 3> q;
+    const int level = STRIDE_GENERATOR<3>::Generate_Adaptive_Stride(range, q);
+    size_t o = 0;
+    for (int a = 1; a <= 3; ++a)
+        for (int i = lo[a - 1]; i <= hi[a - 1]; ++i) q_out[o++] = q(a)(i);
+    return level;
 }
 
 }  // extern "C"

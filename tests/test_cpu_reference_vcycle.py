@@ -1,6 +1,7 @@
 """The oracle pinned to the reference's own code: the reference's CPU V-cycle,
 V-cycle topology, Flaging, Domain_Divider, CG Laplacian (SPGrid_Laplace),
-interface gather (Laplace_ri) and the two-level demo's subdomain couplings
+interface gather (Laplace_ri), the interface hierarchy's adaptive strides
+(STRIDE_GENERATOR) and the two-level demo's subdomain couplings
 (Laplace_ri_Subdomain, Laplace_ir_Subdomain, oracle/_ref/libref_two_level.so) (CPU/SPGrid_Library/SPGrid_V_Cycle_Helper.h,
 SPGrid_V_Cycle_Topology.h, SPGrid_Flag_Helper.h, CPU/SPGrid_Domain_Decomposition_Solver/
 SPGrid_Domain_Divider_Helper.h), compiled from the reference tree by
@@ -39,6 +40,7 @@ def ref():
     ip, up, fp = C.POINTER(C.c_int), C.POINTER(C.c_uint32), C.POINTER(C.c_float)
     L.refv_vcycle.argtypes = [ip, ip, up, C.c_int, C.c_int, C.c_int, fp, fp, up, fp]
     L.refv_laplace.argtypes = [ip, ip, up, fp, fp, fp, fp]
+    L.refv_adaptive_stride.argtypes = [ip, ip, ip]
     return L
 
 
@@ -140,3 +142,25 @@ def test_reference_two_level_couplings_equal_oracle(ref, n, sub, radius, kind):
                                fp(u), fp(b), fp(ri), fp(ir))
     assert np.array_equal(o.laplace_subdomain("ri", u, b).view(np.uint32), ri.view(np.uint32))
     assert np.array_equal(o.laplace_subdomain("ir", u, np.zeros_like(u)).view(np.uint32), ir.view(np.uint32))
+
+
+def test_reference_adaptive_stride_equals_oracle(ref):
+    """STRIDE_GENERATOR<3>::Generate_Adaptive_Stride (CPU/Interface_Solver/STRIDE_GENERATOR.h:23-54),
+    the graded node spacing of the interface hierarchy, against the oracle's restatement for every
+    box extent 2..129 and two box origins.  (Extent 1 writes one entry past the array in both.)"""
+    from oracle_ffi import lib as oracle_lib
+    O = oracle_lib()
+    O.hddo_adaptive_stride.restype = C.c_int
+    ip = C.POINTER(C.c_int)
+    for n in range(2, 130):
+        for lo in [(0, 0, 0), (8, 16, 24)]:
+            lo3 = (C.c_int * 3)(*lo)
+            hi3 = (C.c_int * 3)(*(x + n for x in lo))
+            q_o = np.zeros(3 * (n + 1), np.int32)
+            q_r = np.zeros_like(q_o)
+            filled = (C.c_int * 3)()
+            lv_o = O.hddo_adaptive_stride(lo3, hi3, q_o.ctypes.data_as(ip), filled)
+            lv_r = ref.refv_adaptive_stride(lo3, hi3, q_r.ctypes.data_as(ip))
+            assert list(filled) == [n + 1] * 3, (n, list(filled))
+            assert lv_o == lv_r, (n, lo, lv_o, lv_r)
+            assert np.array_equal(q_o, q_r), (n, lo)
