@@ -130,9 +130,25 @@ def job_throughput(world, steps, seconds):
     return world * steps / seconds
 
 
+# The sparse sphere-union workloads are built and handed over as SPGrid pages,
+# so the host never holds dense arrays of their 1024^3 (or 512^3) box.
+PAGED = {"c5": 1, "c5_half": 2}
+
+
 def workload(cfg):
     from hierarchicaldd_b200 import domains
+    if cfg in PAGED:
+        return domains.config5_pages(PAGED[cfg])
     return domains.CONFIGS[cfg]()
+
+
+def set_domain(s, d):
+    """Hands domain d to solver s: as SPGrid pages when it is paged, else dense."""
+    from hierarchicaldd_b200.domains import PagedDomain
+    if isinstance(d, PagedDomain):
+        s.Set_Domain_Pages(d.origin, d.flags, d.rhs)
+    else:
+        s.Set_Domain(d.flags, d.rhs)
 
 
 PHASES = ["vcycle", "laplace", "pcg_vector", "interface", "sigma_vcycle", "dense_tile_copy",
@@ -146,7 +162,7 @@ def one_solve(args):
     d = workload(args.config)
     m = d.meta
     s = SPGrid_Domain_Decomposition_Solver()
-    s.Set_Domain(d.flags, d.rhs)
+    set_domain(s, d)
     t0 = time.time()
     s.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"],
                                 m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"],
@@ -638,13 +654,13 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from hierarchicaldd_b200 import _lib
-    from hierarchicaldd_b200.domains import ACTIVE
+    from hierarchicaldd_b200.domains import ACTIVE, PagedDomain
     from hierarchicaldd_b200.solver import SPGrid_Domain_Decomposition_Solver
 
     d = workload(args.config)
     m = d.meta
     s = SPGrid_Domain_Decomposition_Solver(device=local_rank)
-    s.Set_Domain(d.flags, d.rhs)
+    set_domain(s, d)
     t0 = time.time()
     s.Initialize_Preconditioner(m["vlevels"], d.size, d.sub_size, m["sigma_levels"], m["nVcycles"],
                                 m["interior_smoothing"], m["boundary_smoothing"], m["sigma_smoothing"],
@@ -680,20 +696,30 @@ def main():
     total_ms = max_over_ranks(float(dev_ms.sum()), dist, "cuda")
     value = job_throughput(world, args.steps, total_ms / 1000.0)
 
-    # End to end through the C ABI with pinned host buffers: H2D of b, solve, D2H of x.
-    cells = int(np.prod(d.size))
+    # End to end through the C ABI with pinned host buffers: H2D of b, solve,
+    # D2H of x (dense arrays of the box, or the SPGrid pages of a paged domain).
+    paged = isinstance(d, PagedDomain)
+    cells = int(d.rhs.size) if paged else int(np.prod(d.size))
     pin_b = torch.empty(cells, dtype=torch.float32, pin_memory=True)
     pin_x = torch.empty(cells, dtype=torch.float32, pin_memory=True)
     pin_b.numpy()[:] = d.rhs.ravel()
     lib = _lib.load()
     fp = lambda t: C.cast(t.data_ptr(), C.POINTER(C.c_float))
+    if paged:
+        origin = np.ascontiguousarray(d.origin, np.int32)
+        op = origin.ctypes.data_as(C.POINTER(C.c_int))
+        set_rhs = lambda: lib.hdd_set_rhs_pages(s.h, origin.shape[0], op, fp(pin_b))
+        get_x = lambda: lib.hdd_get_solution_pages(s.h, origin.shape[0], op, fp(pin_x))
+    else:
+        set_rhs = lambda: lib.hdd_set_rhs_dense(s.h, fp(pin_b))
+        get_x = lambda: lib.hdd_get_solution_dense(s.h, fp(pin_x))
     barrier()
     t_e2e = time.perf_counter()
     for _ in range(args.steps):
-        st = lib.hdd_set_rhs_dense(s.h, fp(pin_b))
+        st = set_rhs()
         assert st == 0, st
         s.Solve()
-        st = lib.hdd_get_solution_dense(s.h, fp(pin_x))
+        st = get_x()
         assert st == 0, st
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t_e2e     # host copies are part of this step, so host time

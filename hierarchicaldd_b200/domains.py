@@ -215,6 +215,93 @@ def config5(scale: int = 1) -> Domain:
                        sigma_smoothing=3, sigma_mg=1, precision_mode=1, true_residual_every=20))
 
 
+@dataclass
+class PagedDomain:
+    """A domain held only as SPGrid pages (4 x 8 x 8 cells), as
+    hdd_set_domain_pages takes it: origin (n, 3), flags and rhs (n, 256) with
+    cell (x, y, z) of a page at (x*8 + y)*8 + z; pages without a non-zero flag
+    are absent."""
+    size: tuple
+    origin: np.ndarray   # int32 (n, 3)
+    flags: np.ndarray    # uint32 (n, 256)
+    rhs: np.ndarray      # float32 (n, 256)
+    sub_size: tuple
+    name: str
+    meta: dict = field(default_factory=dict)
+
+
+def _slab_pages(a: np.ndarray, x0: int, yz: tuple, keep=None):
+    """The x-slab a (cells x0 .. x0 + a.shape[0], x0 a multiple of 4) as pages:
+    (the page indices kept within the slab, their origins, the page arrays),
+    in to_pages() order.  keep None keeps the pages with a non-zero cell."""
+    px, py, pz = -(-a.shape[0] // 4) * 4, -(-yz[0] // 8) * 8, -(-yz[1] // 8) * 8
+    p = np.zeros((px, py, pz), a.dtype)
+    p[:a.shape[0], :yz[0], :yz[1]] = a
+    nb = (px // 4, py // 8, pz // 8)
+    b = p.reshape(nb[0], 4, nb[1], 8, nb[2], 8).transpose(0, 2, 4, 1, 3, 5).reshape(-1, 256)
+    if keep is None:
+        keep = np.flatnonzero(b.any(axis=1))
+    origin = np.stack(np.unravel_index(keep, nb), axis=1) * np.array([4, 8, 8])
+    origin[:, 0] += x0
+    return keep, origin.astype(np.int32), b[keep]
+
+
+def config5_pages(scale: int = 1) -> PagedDomain:
+    """config5(scale) built as SPGrid pages without dense flag or right-hand
+    side arrays of the box: the same spheres, rules and random draws, so its
+    pages equal to_pages() of config5(scale) bit for bit.  Only the union
+    mask of the box is dense (1 byte a cell, 1.1 GB at full scale); flags are
+    made 64-cell x-slab by x-slab (with a 3-cell halo, the reach of the
+    interior, exterior and face-bit rules) and kept as pages, and the
+    right-hand side is drawn in one piece (8 bytes an Active cell) and spread
+    into the pages slab by slab in the box's x-slowest order."""
+    n = 1024 // scale
+    size = (n + 1,) * 3
+    rng = np.random.Generator(np.random.Philox(5))
+    union = np.zeros(size, bool)
+    for _ in range(64):
+        c = rng.uniform(0, n, 3)
+        r = rng.uniform(40, 120) / scale
+        lo = np.maximum(np.floor(c - r).astype(int), 0)
+        hi = np.minimum(np.ceil(c + r).astype(int) + 1, n + 1)
+        i, j, k = np.ogrid[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]]
+        union[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] |= (i - c[0]) ** 2 + (j - c[1]) ** 2 + (k - c[2]) ** 2 <= r * r
+    X, yz = size[0], size[1:]
+    slabs = []   # (x0, depth, kept page indices, origins, flag pages, packed Active mask)
+    total = 0
+    for x0 in range(0, X, 64):
+        x1 = min(x0 + 64, X)
+        w0, w1 = max(x0 - 3, 0), min(x1 + 3, X)
+        u = union[w0:w1]
+        interior = u.copy()
+        for axis in range(3):
+            for step in (-1, 1):
+                interior &= _neighbour(u, axis, step)
+        fl = _finish(interior, u & ~interior)[x0 - w0:x1 - w0]
+        act = (fl & ACTIVE) != 0
+        total += int(np.count_nonzero(act))
+        keep, origin, fpages = _slab_pages(fl, x0, yz)
+        slabs.append((x0, x1 - x0, keep, origin, fpages, np.packbits(act)))
+    del union
+    vals = rng.uniform(0, 1, total)
+    mean = vals.mean()
+    rpages, off = [], 0
+    for x0, depth, keep, _, _, packed in slabs:
+        act = np.unpackbits(packed, count=depth * yz[0] * yz[1]).astype(bool).reshape(depth, *yz)
+        cnt = int(np.count_nonzero(act))
+        r = np.zeros(act.shape, np.float32)
+        r[act] = (vals[off:off + cnt] - mean).astype(np.float32)
+        off += cnt
+        rpages.append(_slab_pages(r, x0, yz, keep)[2])
+    origin = np.concatenate([sl[3] for sl in slabs]).astype(np.int32)
+    flags = np.concatenate([sl[4] for sl in slabs]).astype(np.uint32)
+    rhs = np.concatenate(rpages).astype(np.float32)
+    tag = f"c5_{n}box_sparse_sub32" if scale > 1 else "c5_1024box_sparse_sub32"
+    return PagedDomain(size, origin, flags, rhs, (32, 32, 32), tag,
+                       dict(vlevels=5, nVcycles=1, interior_smoothing=3, boundary_smoothing=3, sigma_levels=4,
+                            sigma_smoothing=3, sigma_mg=1, precision_mode=1, true_residual_every=20))
+
+
 def profile_case() -> Domain:
     """128^3 cells (size 129), centred Dirichlet sphere r=24, 32^3 subdomains:
     the 256^3 workload's kernels (sub 32, vlevels 4, smoothing 4/4) on an eighth
