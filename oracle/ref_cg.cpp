@@ -6,7 +6,7 @@
 //
 // Reference code run here (nothing of it is copied):
 //   PB/Public_Library/PhysBAM_Tools/Krylov_Solvers/CONJUGATE_GRADIENT.cpp:22-67 (Solve),
-//   KRYLOV_SOLVER.cpp, KRYLOV_VECTOR_BASE.cpp and KRYLOV_SYSTEM_BASE.cpp:100-107
+//   KRYLOV_SOLVER.cpp, KRYLOV_VECTOR_BASE.cpp and KRYLOV_SYSTEM_BASE.cpp:100-106
 //   (Precondition: Apply_Preconditioner, then Project and Project_Nullspace),
 //   CPU/SPGrid_Domain_Decomposition_Solver/CG_VECTOR.cpp (the vector updates,
 //   SPGrid_Gemini_Arithmetic_Helpers.h SPGrid_Copy / SPGrid_Copy2 / SPGrid_Minus_Equal),
@@ -15,14 +15,14 @@
 // CPU/SPGrid_Domain_Decomposition_Solver/CG_SYSTEM.cpp cannot be compiled
 // here (its header pulls in the whole preconditioner, which needs Eigen and
 // MKL), so the system class below restates its members: Multiply calls
-// SPGrid_Laplace as CG_SYSTEM.cpp:28-44 does; Inner_Product is the FP64 sum
-// of FP32 products over the set's blocks in block order (CG_SYSTEM.cpp:48-70);
-// Convergence_Norm the max |v| (:74-93); Project zeroes cells that are
-// neither Active nor Interface (:97-118); Set_Boundary_Conditions and
-// Project_Nullspace do nothing (:122-135); Apply_Preconditioner calls the
+// SPGrid_Laplace as CG_SYSTEM.cpp:29-44 does; Inner_Product is the FP64 sum
+// of FP32 products over the set's blocks in block order (CG_SYSTEM.cpp:50-73);
+// Convergence_Norm the max |v| (:78-96); Project zeroes cells that are
+// neither Active nor Interface (:101-119); Set_Boundary_Conditions and
+// Project_Nullspace do nothing (:124-133); Apply_Preconditioner calls the
 // preconditioner it is given (the oracle's, by function pointer) on dense
 // copies.  The system is built as
-// CPU/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Decomposition_Solver.h:165-193
+// CPU/SPGrid_Domain_Decomposition_Solver/SPGrid_Domain_Decomposition_Solver.h:165-194
 // builds it: KRYLOV_SYSTEM_BASE(false,false) with use_preconditioner then set.
 #include <cstdint>
 #include <cstdio>
