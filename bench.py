@@ -130,8 +130,9 @@ def job_throughput(world, steps, seconds):
     return world * steps / seconds
 
 
-# The sparse sphere-union workloads are built and handed over as SPGrid pages,
-# so the host never holds dense arrays of their 1024^3 (or 512^3) box.
+# The sparse sphere-union workloads are built and handed over as SPGrid pages:
+# the generator and the caller hold no dense arrays of their 1024^3 (or 512^3)
+# box (the library's setup still expands the pages over the box internally).
 PAGED = {"c5": 1, "c5_half": 2}
 
 
