@@ -67,6 +67,24 @@ CASES = [("sphere 32^3, sub 8", lambda: domains.small(32, 8, 6, seed=1), 8, Fals
          ("two-level sphere 32^3, sub 16", lambda: domains.small(32, 16, 6, seed=2), 16, True)]
 
 
+def test_reference_cg_equals_oracle_pcg_on_the_64cube_workload(refcg):
+    """The 64^3 sub-16 workload at its own settings and right-hand side (a unit
+    point source), relative stop at 1e-6 expressed as PhysBAM's absolute one."""
+    d = domains.config1()
+    m = d.meta
+    o = Oracle(d.size, d.sub_size, d.flags, vlevels=m["vlevels"], nVcycles=m["nVcycles"],
+               interior_smoothing=m["interior_smoothing"], boundary_smoothing=m["boundary_smoothing"],
+               sigma_levels=m["sigma_levels"], sigma_smoothing=m["sigma_smoothing"], sigma_mg=m["sigma_mg"])
+    f0 = o.level_flags(0)
+    b = np.where((f0 & (ACTIVE | INTERFACE)) != 0, d.rhs, 0).astype(np.float32)
+    tol = float(np.float32(1e-6 * float(np.abs(b).max())))
+    x_o, it_o, info = o.solve(b, tol=tol, relative=False, max_it=200)
+    x_r, it_r, hist_r = ref_solve(refcg, o, f0, b, tol, 200)
+    assert it_r == it_o and 0 < it_o < 200, (it_r, it_o)
+    assert np.array_equal(hist_r[:it_r + 1], info["history"][:it_o + 1])
+    assert np.array_equal(x_r.view(np.uint32), x_o.view(np.uint32))
+
+
 @pytest.mark.parametrize("name,make,sub,multilevel", CASES, ids=[c[0] for c in CASES])
 def test_reference_cg_equals_oracle_pcg(refcg, name, make, sub, multilevel):
     d = make()
